@@ -1,0 +1,199 @@
+// is_analysis.cuh - open-loop analysis kernel: every block shape at every aligned position of a superblock.
+//
+// One CTA per 64x64 SB (8 warps).  The CTA stages the SB's source tile with its edges - rows sby-1 .. sby+63,
+// columns sbx-16 .. sbx+127 - in shared memory with 128-bit loads (every edge an open-loop block can read: the
+// above-right reach of a block at the SB's top row is 2W <= 128 columns; below-left never leaves the SB's rows).
+// Warps then take blocks from the SB's task list (largest shapes first) and run, per block, the search of the
+// reference's k_analysis (encoder/src/k_analysis.cuh:496-689):
+//   edges from the source (haveAR / haveBL by the Z-order guess), DC value,
+//   SATD screening of the 13 modes, then +-1..3 around the two best directional modes (bsize >= 8x8),
+//   top-4 by SATD * 2^14 + sqrt(lambda) * mode bits, exact-rate RD of the top-4 with DCT_DCT, tx-type search of the
+//   winner, -> BlockRes {J, candidates best first, tx}.
+#pragma once
+#include "is_dev.cuh"
+#include "is_frame.cuh"
+
+namespace is {
+
+constexpr int AN_WARPS = 12;
+constexpr int AN_TASKS = 849;                 // blocks of all 19 shapes in one SB
+__constant__ uint8_t c_anTask[AN_TASKS][3];   // (bsize, x4, y4) sorted by area descending, then shape, then raster
+
+template <typename Px> struct AnSmem {
+    static constexpr int TW = 144, TH = 65;   // tile: columns sbx-16 .. sbx+127, rows sby-1 .. sby+63
+    Px tile[TH * TW];
+    struct Warp {
+        int16_t res[64 * 64];                 // residual of an evaluation (its levels reuse the same bytes)
+        int32_t tmp[32 * 65];
+        Px ea[EDGE_LEN], el[EDGE_LEN];
+        int satd[32];
+        int cand[32];
+    } w[AN_WARPS];
+    int next;
+};
+
+// open-loop "decoded before (x, y)" guess (the reference's ol_decoded, dev_common.cuh:153-163): previous SB row and
+// left SB as the spec's BlockDecoded init, Z-order inside the SB; luma pixel units, tile box in pixels
+__device__ __forceinline__ int zorder16(int x, int y) {
+    int z = 0;
+#pragma unroll
+    for (int b = 0; b < 4; b++) z |= (((x >> b) & 1) << (2 * b)) | (((y >> b) & 1) << (2 * b + 1));
+    return z;
+}
+__device__ __forceinline__ bool ol_decoded(int px, int py, int x, int y, int tx0, int ty0, int tx1, int ty1) {
+    if (px < tx0 || py < ty0 || px >= tx1 || py >= ty1) return false;
+    const int sbx = x & ~63, sby = y & ~63;
+    if (py < sby) return true;
+    if (px < sbx) return py < sby + 64;
+    if (px >= sbx + 64 || py >= sby + 64) return false;
+    return zorder16(((px - sbx) >> 2) & 15, ((py - sby) >> 2) & 15) < zorder16(((x - sbx) >> 2) & 15, ((y - sby) >> 2) & 15);
+}
+
+template <int BD, typename Px>
+__device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, typename AnSmem<Px>::Warp &S, int bs, int x, int y, int sbx,
+                                      int sby, int tx0, int ty0, int tx1, int ty1) {
+    constexpr int TW = AnSmem<Px>::TW;
+    const int lane = lane_id();
+    const int txSz = AV1G_T(Max_Tx_Size_Rect)[bs];
+    const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
+    const int maxX = F.MiCols * 4 - 1, maxY = F.MiRows * 4 - 1;
+    const int haveL = x > tx0, haveA = y > ty0;
+    const int haveAR = ol_decoded(x + W, y - 1, x, y, tx0, ty0, tx1, ty1), haveBL = ol_decoded(x - 1, y + H, x, y, tx0, ty0, tx1, ty1);
+    // tile-local coordinates (tile column 0 = sbx - 16, row 0 = sby - 1)
+    const int lx = x - sbx + 16, ly = y - sby + 1;
+    Px *A = S.ea + EDGE_OFF, *L = S.el + EDGE_OFF;
+    build_edges<BD>(tile, TW, lx, ly, W, H, haveL, haveA, haveAR, haveBL, maxX - sbx + 16, maxY - sby + 1, A, L, lane, 32);
+    __syncwarp();
+    const int dcv = warp_dc<BD>(A, L, haveL, haveA, lw, lh);
+    const Px *src = tile + ly * TW + lx;
+    const uint16_t *C = g_cost[F.qctx];
+    auto mbits = [&](int c) -> int {
+        const int m = cand_mode(c);
+        int b = c_avgY[m];
+        if (bs >= AV1G_BLOCK_8X8 && is_dir(m)) b += C[ci_angle(m - AV1G_V_PRED) + cand_delta(c) + 3];
+        return b;
+    };
+    // ---- SATD screening of candidates [c0, c1): (candidate, 4x4 sub-block) items over the lanes ----
+    const int nsx = W >> 2, lnsx = lw - 2, nsub = (W >> 2) * (H >> 2), lnsub = lw + lh - 4;
+    auto screen = [&](int c0, int c1) {
+        const int items = (c1 - c0) * nsub;
+        for (int it0 = 0; it0 < items; it0 += 32) {
+            const int it = it0 + lane;
+            const int ci = c0 + (it >> lnsub);
+            int t = 0;
+            if (it < items) {
+                const int sb = it & (nsub - 1), sx = (sb & (nsx - 1)) * 4, sy = (sb >> lnsx) * 4;
+                const int c = S.cand[ci], m = cand_mode(c), pa = pangle(m, cand_delta(c));
+                int d[16];
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        d[i * 4 + j] = (int)src[(sy + i) * TW + sx + j] - pred_px(m, pa, sy + i, sx + j, lw, lh, A, L, dcv);
+                t = hadamard4_sum(d);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                if (o < nsub) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (it < items && (lane & (nsub - 1)) == 0) S.satd[ci] += t;
+            __syncwarp();
+        }
+    };
+    S.satd[lane] = 0;
+    S.cand[lane] = lane < 13 ? cand_pack(lane, 0) : 0;
+    __syncwarp();
+    screen(0, 13);
+    i64 js = lane < 13 ? ((i64)S.satd[lane] << 14) + F.sqlam * mbits(S.cand[lane]) : INF;
+    if (bs >= AV1G_BLOCK_8X8) {
+        const i64 jd = (lane >= AV1G_V_PRED && lane <= AV1G_D67_PRED) ? js : INF;
+        const int b0 = warp_argmin(jd, lane);
+        const int b1 = warp_argmin(lane == b0 ? INF : jd, lane);
+        if (lane < 12) {
+            const int m = lane < 6 ? b0 : b1, k = lane % 6;
+            S.cand[13 + lane] = cand_pack(m, k < 3 ? -(k + 1) : (k - 2));
+        }
+        __syncwarp();
+        screen(13, 25);
+        if (lane >= 13 && lane < 25) js = ((i64)S.satd[lane] << 14) + F.sqlam * mbits(S.cand[lane]);
+    }
+    int top[K_TOP];
+    int nK = 0;
+#pragma unroll
+    for (int k = 0; k < K_TOP; k++) {
+        top[k] = warp_argmin(js, lane);
+        if (top[k] >= 0) nK = k + 1;
+        if (lane == top[k]) js = INF;
+    }
+    // ---- RD of the top-K with DCT_DCT, then the tx types of the winner ----
+    const int set = tx_set_intra(txSz);
+    const bool hasC = has_chroma(bs, y >> 2, x >> 2, F.ssx);
+    const int overhead = (hasC ? UV_OVERHEAD : 0) + c_avgSkip0;
+    i64 bestJ = INF;
+    int bestK = 0, bestTx = AV1G_DCT_DCT;
+    const int nSteps = nK + (set != AV1G_TX_SET_DCTONLY ? 15 : 0);
+    for (int st = 0; st < nSteps; st++) {
+        const int k = st < nK ? st : bestK, t = st < nK ? AV1G_DCT_DCT : st - nK + 1;
+        if (t != AV1G_DCT_DCT && !tx_in_set(set, t)) continue;
+        const int c = S.cand[top[k]], m = cand_mode(c);
+        const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, C};
+        const EvalOut o = rc_eval<BD, Px>(txSz, res_mode<Px>(src, TW, A, L, m, cand_delta(c), lw, lh, dcv), e, S.res, S.tmp, S.res);
+        const i64 J = o.D + F.lam * (o.R + mbits(c) + overhead);
+        if (J < bestJ) {
+            bestJ = J;
+            if (st < nK) bestK = k; else bestTx = t;
+        }
+    }
+    if (lane == 0) {
+        BlockRes r;
+        r.J = bestJ;
+        r.tx = (uint8_t)bestTx;
+        int n = 0;
+        r.cand[n++] = (uint8_t)S.cand[top[bestK]];
+        for (int k = 0; k < nK; k++) if (k != bestK) r.cand[n++] = (uint8_t)S.cand[top[k]];
+        for (int k = n; k < 4; k++) r.cand[k] = 0;
+        r.ncand = (uint8_t)n;
+        r.pad[0] = r.pad[1] = 0;
+        F.blk[F.shOff[bs] + (uint32_t)(y / H) * F.shNbx[bs] + x / W] = r;
+    }
+    __syncwarp();
+}
+
+template <int BD>
+__global__ void __launch_bounds__(AN_WARPS * 32, 1) k_analysis(const FrameDesc *__restrict__ Fp) {
+    typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    AnSmem<Px> &S = *reinterpret_cast<AnSmem<Px> *>(smem_raw);
+    const FrameDesc &F = *Fp;
+    const int sb = blockIdx.x, sbr = sb / F.sbCols, sbc = sb % F.sbCols;
+    const int sbx = sbc * 64, sby = sbr * 64;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // stage the SB tile with 128-bit loads (rows and the tile's first column are 16-byte aligned by the layout)
+    {
+        constexpr int V = AnSmem<Px>::TW * (int)sizeof(Px) / 16;   // uint4 per tile row
+        const Px *s0 = (const Px *)F.src[0] + (size_t)(sby - 1) * F.spitch[0] + (sbx - 16);
+        for (int k = tid; k < AnSmem<Px>::TH * V; k += AN_WARPS * 32) {
+            const int r = k / V, c = k % V;
+            reinterpret_cast<uint4 *>(S.tile + r * AnSmem<Px>::TW)[c] = __ldg(reinterpret_cast<const uint4 *>(s0 + (size_t)r * F.spitch[0]) + c);
+        }
+        if (tid == 0) S.next = AN_WARPS;
+    }
+    __syncthreads();
+    // the tile containing this SB (pixels)
+    int tc = 0, tr = 0;
+    while (tc + 1 < F.tileCols && sbx >= F.tileColStart[tc + 1] * 4) tc++;
+    while (tr + 1 < F.tileRows && sby >= F.tileRowStart[tr + 1] * 4) tr++;
+    const int tx0 = F.tileColStart[tc] * 4, tx1 = F.tileColStart[tc + 1] * 4, ty0 = F.tileRowStart[tr] * 4, ty1 = F.tileRowStart[tr + 1] * 4;
+    const int FW = F.MiCols * 4, FH = F.MiRows * 4;
+    int t = warp;
+    while (t < AN_TASKS) {
+        const int bs = c_anTask[t][0], x = sbx + c_anTask[t][1] * 4, y = sby + c_anTask[t][2] * 4;
+        if (x < FW && y < FH) {
+            an_block<BD, Px>(F, S.tile, S.w[warp], bs, x, y, sbx, sby, tx0, ty0, tx1, ty1);
+        }
+        int n = 0;
+        if (lane == 0) n = atomicAdd(&S.next, 1);
+        t = __shfl_sync(0xffffffffu, n, 0);
+    }
+}
+
+}  // namespace is

@@ -1,0 +1,552 @@
+// is_api.cu - host orchestration of the B200 intra search and its C ABI (include/is_api.h).
+//
+// One encode = one stream-ordered sequence (the reference's GpEncoder::encode, encoder/src/pipeline.cpp:323-1180):
+//   upload / pad   the caller's planes into the padded workspace planes (cudaMemcpy2DAsync + k_pad)
+//   analysis       k_analysis: one CTA per SB, every shape and position
+//   dp             k_dp: one thread per SB
+//   closed loop    k_recon: persistent cooperative wavefront (one CTA per SM)
+//   pack           k_pack_scan + k_pack: DecisionRecord arrays in decode order
+// The workspace is one device allocation per handle, grown when a larger image arrives and reused otherwise.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "is_api.h"
+#include "is_dev.cuh"
+#include "is_frame.cuh"
+#include "is_analysis.cuh"
+#include "is_dp.cuh"
+#include "is_recon.cuh"
+
+using namespace is;
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------------------------
+// fixed-point tables (the same definitions as the reference's gp_init_tables, k_misc.cu:505-621, in 1/256 bit)
+// ---------------------------------------------------------------------------------------------------------------
+struct HostTables {
+    std::vector<uint16_t> cost[4];
+    int avgY[13];
+    int avgPart[5][10];
+    int avgSkip0;
+};
+
+int bits_fx(double p) { return (int)llround(-std::log2(p) * 256.0); }
+
+template <typename Arr>
+void cost_of_field(const av1g_cdfs &c, const Arr &field, uint16_t *out) {
+    typedef typename std::remove_reference<Arr>::type T;
+    constexpr size_t L = std::extent<T, std::rank<T>::value - 1>::value;   // symbols + 1 (adaptation counter)
+    const uint16_t *p = reinterpret_cast<const uint16_t *>(&field);
+    const size_t base = (size_t)(p - reinterpret_cast<const uint16_t *>(&c));
+    for (size_t b = 0; b < sizeof(T) / 2; b += L)
+        for (size_t s = 0; s + 1 < L; s++) {
+            const double lo = s ? p[b + s - 1] : 0.0, hi = p[b + s];
+            out[base + b + s] = (uint16_t)bits_fx(std::max((hi - lo) / 32768.0, 1.0 / 32768.0));
+        }
+}
+
+const HostTables &host_tables() {
+    static HostTables T;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const int qrep[4] = {20, 60, 120, 255};   // a base_q_idx of each coefficient-CDF q-context
+        for (int qc = 0; qc < 4; qc++) {
+            av1g_cdfs c;
+            av1g_cdfs_init(&c, qrep[qc]);
+            T.cost[qc].assign(NCDF, 0);
+            uint16_t *o = T.cost[qc].data();
+            cost_of_field(c, c.y_mode, o); cost_of_field(c, c.uv_mode_cfl_not_allowed, o); cost_of_field(c, c.uv_mode_cfl_allowed, o);
+            cost_of_field(c, c.angle_delta, o); cost_of_field(c, c.partition_w8, o); cost_of_field(c, c.partition_w16, o);
+            cost_of_field(c, c.partition_w32, o); cost_of_field(c, c.partition_w64, o); cost_of_field(c, c.tx_8x8, o);
+            cost_of_field(c, c.tx_16x16, o); cost_of_field(c, c.tx_32x32, o); cost_of_field(c, c.tx_64x64, o);
+            cost_of_field(c, c.skip, o); cost_of_field(c, c.filter_intra_mode, o); cost_of_field(c, c.filter_intra, o);
+            cost_of_field(c, c.intra_tx_set1, o); cost_of_field(c, c.intra_tx_set2, o); cost_of_field(c, c.cfl_sign, o);
+            cost_of_field(c, c.cfl_alpha, o); cost_of_field(c, c.txb_skip, o); cost_of_field(c, c.eob_pt_16, o);
+            cost_of_field(c, c.eob_pt_32, o); cost_of_field(c, c.eob_pt_64, o); cost_of_field(c, c.eob_pt_128, o);
+            cost_of_field(c, c.eob_pt_256, o); cost_of_field(c, c.eob_pt_512, o); cost_of_field(c, c.eob_pt_1024, o);
+            cost_of_field(c, c.eob_extra, o); cost_of_field(c, c.dc_sign, o); cost_of_field(c, c.coeff_base_eob, o);
+            cost_of_field(c, c.coeff_base, o); cost_of_field(c, c.coeff_br, o);
+            if (qc) continue;
+            for (int m = 0; m < 13; m++) {   // y_mode averaged over its 5 x 5 contexts
+                double p = 0;
+                for (int a = 0; a < 5; a++)
+                    for (int l = 0; l < 5; l++) p += (c.y_mode[a][l][m] - (m ? c.y_mode[a][l][m - 1] : 0)) / 32768.0;
+                T.avgY[m] = bits_fx(std::max(p / 25.0, 1e-6));
+            }
+            for (int b = 0; b < 5; b++)
+                for (int p = 0; p < 10; p++) T.avgPart[b][p] = 20 * 256;
+            for (int bsl = 1; bsl <= 4; bsl++) {   // partition averaged over its 4 contexts
+                const int N = bsl == 1 ? 4 : 10;
+                for (int p = 0; p < N; p++) {
+                    double pr = 0;
+                    for (int ctx = 0; ctx < 4; ctx++) {
+                        const uint16_t *cd = bsl == 1 ? c.partition_w8[ctx] : bsl == 2 ? c.partition_w16[ctx]
+                                           : bsl == 3 ? c.partition_w32[ctx] : c.partition_w64[ctx];
+                        pr += (cd[p] - (p ? cd[p - 1] : 0)) / 32768.0;
+                    }
+                    T.avgPart[bsl][p] = bits_fx(std::max(pr / 4.0, 1e-6));
+                }
+            }
+            double ps = 0;
+            for (int ctx = 0; ctx < 3; ctx++) ps += c.skip[ctx][0] / 32768.0;
+            T.avgSkip0 = bits_fx(ps / 3.0);
+        }
+    });
+    return T;
+}
+
+// libaom-style lambda (the reference's gp_lambda, dev_common.cuh:99-107), fixed point 1/256
+void lambda_fx(int qidx, int bd, long long *lam, long long *sq) {
+    const int q = AV1G_T(Dc_Qlookup)[(bd - 8) >> 1][std::min(255, std::max(0, qidx))];
+    double rd = (double)q * q * (3.3 + 0.0015 * q);
+    int w = ((255 - qidx) * 3) / 4;
+    w = w < 0 ? 0 : w > 72 ? 72 : w;
+    rd = rd * (128 + w) / 128.0;
+    const double l = rd / 2048.0;
+    *lam = llround(l * 256.0);
+    *sq = llround(std::sqrt(l) * 256.0);
+}
+
+// spec 5.9.15 tile_info with uniform spacing at the minimum legal tiling (the reference's compute_tiles,
+// av1core/src/encoder.cpp:56-92): returns cols, rows and the starts in mi units
+int tile_log2(int blk, int target) { int k = 0; while ((blk << k) < target) k++; return k; }
+void min_tiles(int W, int H, std::vector<int> &cs, std::vector<int> &rs) {
+    const int MiCols = 2 * ((W + 7) >> 3), MiRows = 2 * ((H + 7) >> 3);
+    const int sbCols = (MiCols + 15) >> 4, sbRows = (MiRows + 15) >> 4;
+    const int maxTileWidthSb = 4096 >> 6, maxTileAreaSb = (4096 * 2304) >> 12;
+    const int minLog2TileCols = tile_log2(maxTileWidthSb, sbCols);
+    const int maxLog2TileRows = tile_log2(1, std::min(sbRows, 64));
+    const int minLog2Tiles = std::max(minLog2TileCols, tile_log2(maxTileAreaSb, sbRows * sbCols));
+    const int colsLog2 = minLog2TileCols;
+    const int tileWidthSb = (sbCols + (1 << colsLog2) - 1) >> colsLog2;
+    cs.clear();
+    for (int s = 0; s < sbCols; s += tileWidthSb) cs.push_back(s << 4);
+    cs.push_back(MiCols);
+    int rowsLog2 = std::max(minLog2Tiles - colsLog2, 0);
+    for (;; rowsLog2++) {
+        const int tileHeightSb = (sbRows + (1 << rowsLog2) - 1) >> rowsLog2;
+        if (tileWidthSb * tileHeightSb <= maxTileAreaSb || rowsLog2 >= maxLog2TileRows) {
+            rs.clear();
+            for (int s = 0; s < sbRows; s += tileHeightSb) rs.push_back(s << 4);
+            rs.push_back(MiRows);
+            return;
+        }
+    }
+}
+
+// analysis task list of one SB: (bsize, x4, y4) for every shape, largest area first
+std::vector<uint8_t> an_tasks() {
+    std::vector<int> shapes;
+    for (int s = 0; s < AV1G_BLOCK_INVALID; s++) if (!(s >= 13 && s <= 15)) shapes.push_back(s);
+    std::stable_sort(shapes.begin(), shapes.end(), [](int a, int b) {
+        return AV1G_T(Num_4x4_Blocks_Wide)[a] * AV1G_T(Num_4x4_Blocks_High)[a] > AV1G_T(Num_4x4_Blocks_Wide)[b] * AV1G_T(Num_4x4_Blocks_High)[b];
+    });
+    std::vector<uint8_t> t;
+    for (int s : shapes) {
+        const int w4 = AV1G_T(Num_4x4_Blocks_Wide)[s], h4 = AV1G_T(Num_4x4_Blocks_High)[s];
+        for (int y = 0; y < 16; y += h4)
+            for (int x = 0; x < 16; x += w4) { t.push_back((uint8_t)s); t.push_back((uint8_t)x); t.push_back((uint8_t)y); }
+    }
+    return t;
+}
+
+// pad kernel: replicate the last visible column / row of a plane over the padded area (right, then bottom)
+template <typename Px>
+__global__ void k_pad(Px *plane, int pitch, int vw, int vh, int pw, int ph) {
+    const int y = blockIdx.y;
+    if (y < vh) {
+        const Px v = plane[(size_t)y * pitch + vw - 1];
+        for (int x = vw + threadIdx.x; x < pw; x += blockDim.x) plane[(size_t)y * pitch + x] = v;
+    } else if (y < ph) {
+        const Px *s = plane + (size_t)(vh - 1) * pitch;
+        for (int x = threadIdx.x; x < pw; x += blockDim.x) plane[(size_t)y * pitch + x] = s[x];
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------------------------------------------
+struct is_handle {
+    is_params p;
+    int device = 0, nSm = 0, rcGrid = 0;
+    cudaStream_t own = nullptr;
+    std::string err;
+    // workspace
+    void *arena = nullptr;
+    size_t arenaBytes = 0;
+    FrameDesc F;                 // host copy of the descriptor (device pointers)
+    FrameDesc *dF = nullptr;     // device copy
+    FrameDesc *hFpinned = nullptr;
+    int nSb = 0;
+    int geomW = -1, geomH = -1;
+    size_t smemAn = 0, smemRc = 0;
+    // last result
+    bool have = false;
+    uint32_t nBlocks = 0, nTxb = 0;
+    uint64_t nCoeffs = 0;
+    int qidx = 0;
+    is_times times;
+    cudaEvent_t ev[6];
+    void *hostSmall = nullptr;   // pinned 64 bytes for the counts / error readback
+    int setErr(int code, const char *fmt, ...) {
+        char b[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(b, sizeof b, fmt, ap);
+        va_end(ap);
+        err = b;
+        return code;
+    }
+};
+
+#define IS_CK(call)                                                                                 \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return h->setErr(e_ == cudaErrorMemoryAllocation ? IS_ERR_OOM : IS_ERR_CUDA, \
+                                                "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+namespace {
+
+std::once_flag g_upload_once[64];
+int g_upload_rc[64];
+
+int upload_tables(int dev) {
+    std::call_once(g_upload_once[dev & 63], [dev] {
+        const HostTables &T = host_tables();
+        std::vector<uint16_t> all((size_t)4 * NCDF);
+        for (int q = 0; q < 4; q++) memcpy(all.data() + (size_t)q * NCDF, T.cost[q].data(), NCDF * 2);
+        const std::vector<uint8_t> tasks = an_tasks();
+        cudaError_t e = cudaMemcpyToSymbol(g_cost, all.data(), all.size() * 2);
+        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgY, T.avgY, sizeof T.avgY);
+        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgPart, T.avgPart, sizeof T.avgPart);
+        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgSkip0, &T.avgSkip0, sizeof T.avgSkip0);
+        if (e == cudaSuccess && tasks.size() == (size_t)AN_TASKS * 3) e = cudaMemcpyToSymbol(c_anTask, tasks.data(), tasks.size());
+        else if (e == cudaSuccess) e = cudaErrorInvalidValue;
+        g_upload_rc[dev & 63] = e == cudaSuccess ? 0 : (int)e;
+    });
+    return g_upload_rc[dev & 63];
+}
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// host self-check: the compile-time row shifts agree with the spec table (the forward scale depends on them)
+template <int W, int H> bool rowshift_ok() { return TxDims<W, H>::rowShift == AV1G_T(Transform_Row_Shift)[TxDims<W, H>::size]; }
+bool tables_consistent() {
+    bool ok = true;
+#define IS_CHK(W_, H_) ok = ok && rowshift_ok<W_, H_>()
+    for (int t = 0; t < 19; t++) { IS_TX_SWITCH(t, IS_CHK) }
+#undef IS_CHK
+    return ok;
+}
+
+// lay out the workspace for an image of W x H (8-bit 4:2:0); returns bytes needed, fills F's pointers if base != 0
+size_t layout(int W, int H, uint8_t *base, FrameDesc &F, int &nSb) {
+    F.W = W; F.H = H;
+    F.MiCols = 2 * ((W + 7) >> 3); F.MiRows = 2 * ((H + 7) >> 3);
+    F.sbCols = (F.MiCols + 15) >> 4; F.sbRows = (F.MiRows + 15) >> 4;
+    F.ssx = F.ssy = 1; F.bd = 8;
+    nSb = F.sbCols * F.sbRows;
+    size_t at = 0;
+    auto take = [&](size_t bytes) -> uint8_t * { uint8_t *p = base ? base + at : nullptr; at += align256(bytes); return p; };
+    for (int p = 0; p < 3; p++) {
+        const int ss = p ? 1 : 0;
+        const int pw = (((F.sbCols + 1) * 64) >> ss) + SRC_MARGIN_X, ph = ((F.sbRows * 64) >> ss) + SRC_MARGIN_Y;
+        const int pitch = (pw + 15) & ~15;
+        uint8_t *s = take((size_t)pitch * ph), *r = take((size_t)pitch * ph);
+        F.spitch[p] = F.rpitch[p] = pitch;
+        F.src[p] = s ? s + (size_t)SRC_MARGIN_Y * pitch + SRC_MARGIN_X : nullptr;
+        F.rec[p] = r ? r + (size_t)SRC_MARGIN_Y * pitch + SRC_MARGIN_X : nullptr;
+    }
+    F.mYMode = take((size_t)F.MiCols * F.MiRows);
+    for (int p = 0; p < 3; p++) {
+        const size_t n = (size_t)(F.MiCols >> (p ? 1 : 0)) * (F.MiRows >> (p ? 1 : 0));
+        F.cLvl[p] = take(n);
+        F.cDc[p] = take(n);
+    }
+    uint32_t off = 0;
+    for (int s = 0; s < 22; s++) {
+        F.shNbx[s] = F.shNby[s] = 0;
+        F.shOff[s] = off;
+        if (s >= AV1G_BLOCK_INVALID || (s >= 13 && s <= 15)) continue;
+        const int w = 4 * AV1G_T(Num_4x4_Blocks_Wide)[s], h = 4 * AV1G_T(Num_4x4_Blocks_High)[s];
+        F.shNbx[s] = (F.MiCols * 4 + w - 1) / w;
+        F.shNby[s] = (F.MiRows * 4 + h - 1) / h;
+        off += (uint32_t)(F.shNbx[s] * F.shNby[s]);
+    }
+    F.blk = (BlockRes *)take((size_t)off * sizeof(BlockRes));
+    F.leaves = (Leaf *)take((size_t)nSb * SB_MAX_LEAVES * sizeof(Leaf));
+    F.nLeaves = (uint16_t *)take((size_t)nSb * 2);
+    F.oBlocks = (av1g_block *)take((size_t)nSb * SB_MAX_LEAVES * sizeof(av1g_block));
+    F.oBlockTxb = (uint16_t *)take((size_t)nSb * SB_MAX_LEAVES * 2);
+    F.oTxb = (av1g_txb *)take((size_t)nSb * SB_MAX_TXB * sizeof(av1g_txb));
+    F.oCoeffs = (int16_t *)take((size_t)nSb * SB_MAX_COEF * 2);
+    F.sbCount = (SbCount *)take((size_t)nSb * sizeof(SbCount));
+    F.sbOrder = (const uint32_t *)take((size_t)nSb * 4);
+    F.sbDone = (int *)take((size_t)nSb * 4);
+    F.queue = (int *)take(4);
+    F.err = (int *)take(4);
+    F.sbDecodeOrder = (uint32_t *)take((size_t)nSb * 4);
+    F.offBlk = (uint32_t *)take((size_t)(nSb + 1) * 4);
+    F.offTxb = (uint32_t *)take((size_t)(nSb + 1) * 4);
+    F.offCoef = (uint64_t *)take((size_t)(nSb + 1) * 8);
+    F.recBlocks = (av1g_block *)take((size_t)nSb * SB_MAX_LEAVES * sizeof(av1g_block));
+    F.recBlockTxb = (uint32_t *)take(((size_t)nSb * SB_MAX_LEAVES + 1) * 4);
+    F.recTxb = (av1g_txb *)take((size_t)nSb * SB_MAX_TXB * sizeof(av1g_txb));
+    F.recCoeffs = (int16_t *)take((size_t)nSb * SB_MAX_COEF * 2);
+    take(sizeof(FrameDesc));   // the device copy of the descriptor
+    return at;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------------------------------
+extern "C" {
+
+int is_create(const is_params *p, is_handle **out) {
+    if (!p || !out) return IS_ERR_INVALID;
+    if (p->bit_depth != 8 || p->chroma_444 != 0) return IS_ERR_INVALID;
+    is_handle *h = new is_handle();
+    h->p = *p;
+    h->device = p->device;
+    auto fail = [&](int rc) { is_destroy(h); *out = nullptr; return rc; };
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(IS_ERR_CUDA);
+    if (!tables_consistent()) return fail(IS_ERR_INVALID);
+    if (upload_tables(h->device)) return fail(IS_ERR_CUDA);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) return fail(IS_ERR_CUDA);
+    h->nSm = prop.multiProcessorCount;
+    h->smemAn = sizeof(AnSmem<uint8_t>);
+    h->smemRc = sizeof(RcSmem<uint8_t>);
+    if (cudaFuncSetAttribute(k_analysis<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemAn) != cudaSuccess) return fail(IS_ERR_CUDA);
+    if (cudaFuncSetAttribute(k_recon<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemRc) != cudaSuccess) return fail(IS_ERR_CUDA);
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_recon<8>, RC_WARPS * 32, h->smemRc) != cudaSuccess || per < 1) return fail(IS_ERR_CUDA);
+    h->rcGrid = per * h->nSm;
+    if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess) return fail(IS_ERR_CUDA);
+    for (auto &e : h->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return fail(IS_ERR_CUDA);
+    if (cudaMallocHost(&h->hostSmall, 64) != cudaSuccess) return fail(IS_ERR_OOM);
+    if (cudaMallocHost(&h->hFpinned, sizeof(FrameDesc)) != cudaSuccess) return fail(IS_ERR_OOM);
+    memset(&h->times, 0, sizeof h->times);
+    *out = h;
+    return IS_OK;
+}
+
+void is_destroy(is_handle *h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->own) cudaStreamSynchronize(h->own);
+    if (h->arena) cudaFree(h->arena);
+    for (auto &e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->own) cudaStreamDestroy(h->own);
+    if (h->hostSmall) cudaFreeHost(h->hostSmall);
+    if (h->hFpinned) cudaFreeHost(h->hFpinned);
+    delete h;
+}
+
+const char *is_last_error(const is_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+static int prepare(is_handle *h, const is_frame *f) {
+    if (!f || f->width < 1 || f->height < 1 || f->width > 16384 || f->height > 16384 || f->qindex < 1 || f->qindex > 255)
+        return h->setErr(IS_ERR_INVALID, "invalid frame (size %dx%d, qindex %d)", f ? f->width : 0, f ? f->height : 0, f ? f->qindex : 0);
+    FrameDesc F;
+    memset(&F, 0, sizeof F);
+    int nSb = 0;
+    const size_t need = layout(f->width, f->height, nullptr, F, nSb);
+    if (need > h->arenaBytes) {
+        if (h->arena) { cudaStreamSynchronize(h->own); cudaFree(h->arena); h->arena = nullptr; h->arenaBytes = 0; }
+        IS_CK(cudaMalloc(&h->arena, need));
+        h->arenaBytes = need;
+        h->geomW = -1;
+    }
+    memset(&F, 0, sizeof F);
+    layout(f->width, f->height, (uint8_t *)h->arena, F, nSb);
+    h->dF = (FrameDesc *)((uint8_t *)h->arena + need - align256(sizeof(FrameDesc)));
+    // tiles, wavefront order, decode order
+    std::vector<int> cs, rs;
+    min_tiles(f->width, f->height, cs, rs);
+    if (cs.size() > 65 || rs.size() > 65) return h->setErr(IS_ERR_INVALID, "too many tiles");
+    F.tileCols = (int)cs.size() - 1; F.tileRows = (int)rs.size() - 1;
+    for (size_t i = 0; i < cs.size(); i++) F.tileColStart[i] = cs[i];
+    for (size_t i = 0; i < rs.size(); i++) F.tileRowStart[i] = rs[i];
+    F.qidx = f->qindex;
+    F.qctx = av1g_coeff_cdf_q_ctx(f->qindex);
+    lambda_fx(f->qindex, 8, &F.lam, &F.sqlam);
+    F.dcQ = AV1G_T(Dc_Qlookup)[0][f->qindex];
+    F.acQ = AV1G_T(Ac_Qlookup)[0][f->qindex];
+    if (h->geomW != f->width || h->geomH != f->height) {
+        std::vector<uint32_t> order, dec;
+        struct J { uint32_t sb; int step; };
+        std::vector<J> js;
+        for (int tr = 0; tr < F.tileRows; tr++)
+            for (int tc = 0; tc < F.tileCols; tc++) {
+                const int r0 = rs[tr] >> 4, r1 = (rs[tr + 1] + 15) >> 4, c0 = cs[tc] >> 4, c1 = (cs[tc + 1] + 15) >> 4;
+                for (int r = r0; r < r1; r++)
+                    for (int c = c0; c < c1; c++) {
+                        js.push_back(J{(uint32_t)(r * F.sbCols + c), (c - c0) + 2 * (r - r0)});
+                        dec.push_back((uint32_t)(r * F.sbCols + c));
+                    }
+            }
+        std::stable_sort(js.begin(), js.end(), [](const J &a, const J &b) { return a.step < b.step; });
+        for (auto &j : js) order.push_back(j.sb);
+        IS_CK(cudaMemcpy((void *)F.sbOrder, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
+        IS_CK(cudaMemcpy(F.sbDecodeOrder, dec.data(), dec.size() * 4, cudaMemcpyHostToDevice));
+        h->geomW = f->width;
+        h->geomH = f->height;
+    }
+    h->F = F;
+    h->nSb = nSb;
+    h->qidx = f->qindex;
+    return IS_OK;
+}
+
+static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) {
+    FrameDesc &F = h->F;
+    const int nSb = h->nSb;
+    IS_CK(cudaEventRecord(h->ev[0], st));
+    // descriptor (pinned staging so the copy stays asynchronous)
+    IS_CK(cudaStreamSynchronize(st));   // the pinned staging copy of a previous encode must be consumed
+    *h->hFpinned = F;
+    IS_CK(cudaMemcpyAsync(h->dF, h->hFpinned, sizeof(FrameDesc), cudaMemcpyHostToDevice, st));
+    // planes into the padded workspace
+    for (int p = 0; p < 3; p++) {
+        const int ss = p ? 1 : 0;
+        const int vw = (f->width + ss) >> ss, vh = (f->height + ss) >> ss;
+        uint8_t *dst = const_cast<uint8_t *>(F.src[p]);
+        IS_CK(cudaMemcpy2DAsync(dst, F.spitch[p], f->planes[p], f->pitch[p], vw, vh,
+                                fromHost ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+        const int pw = ((F.sbCols + 1) * 64) >> ss, ph = (F.sbRows * 64) >> ss;
+        k_pad<uint8_t><<<dim3(1, ph), 128, 0, st>>>(dst, F.spitch[p], vw, vh, pw, ph);
+    }
+    IS_CK(cudaMemsetAsync(F.sbDone, 0, (size_t)nSb * 4, st));
+    IS_CK(cudaMemsetAsync(F.queue, 0, 4, st));
+    IS_CK(cudaMemsetAsync(F.err, 0, 4, st));
+    IS_CK(cudaEventRecord(h->ev[1], st));
+    k_analysis<8><<<nSb, AN_WARPS * 32, h->smemAn, st>>>(h->dF);
+    IS_CK(cudaGetLastError());
+    IS_CK(cudaEventRecord(h->ev[2], st));
+    k_dp<<<(nSb + 63) / 64, 64, 0, st>>>(h->dF, nSb);
+    IS_CK(cudaGetLastError());
+    IS_CK(cudaEventRecord(h->ev[3], st));
+    {
+        const FrameDesc *a0 = h->dF;
+        int a1 = nSb;
+        void *args[2] = {(void *)&a0, (void *)&a1};
+        const int grid = std::min(h->rcGrid, nSb);
+        IS_CK(cudaLaunchCooperativeKernel((const void *)k_recon<8>, dim3(grid), dim3(RC_WARPS * 32), args, h->smemRc, st));
+    }
+    IS_CK(cudaEventRecord(h->ev[4], st));
+    k_pack_scan<<<1, 1024, 0, st>>>(h->dF, nSb);
+    k_pack<<<nSb, 256, 0, st>>>(h->dF, nSb);
+    IS_CK(cudaGetLastError());
+    IS_CK(cudaEventRecord(h->ev[5], st));
+    // counts + error status
+    uint32_t *hs = (uint32_t *)h->hostSmall;
+    IS_CK(cudaMemcpyAsync(hs, F.offBlk + nSb, 4, cudaMemcpyDeviceToHost, st));
+    IS_CK(cudaMemcpyAsync(hs + 1, F.offTxb + nSb, 4, cudaMemcpyDeviceToHost, st));
+    IS_CK(cudaMemcpyAsync(hs + 2, F.offCoef + nSb, 8, cudaMemcpyDeviceToHost, st));
+    IS_CK(cudaMemcpyAsync(hs + 4, F.err, 4, cudaMemcpyDeviceToHost, st));
+    IS_CK(cudaStreamSynchronize(st));
+    if (hs[4]) {
+        h->have = false;
+        return h->setErr(IS_ERR_TIMEOUT, "closed loop reported error %u (dependency wait budget exhausted)", hs[4]);
+    }
+    h->nBlocks = hs[0];
+    h->nTxb = hs[1];
+    memcpy(&h->nCoeffs, hs + 2, 8);
+    float ms[6];
+    for (int i = 1; i < 6; i++) IS_CK(cudaEventElapsedTime(&ms[i], h->ev[i - 1], h->ev[i]));
+    h->times.upload = ms[1]; h->times.analysis = ms[2]; h->times.dp = ms[3]; h->times.recon = ms[4]; h->times.pack = ms[5];
+    h->times.total = ms[1] + ms[2] + ms[3] + ms[4] + ms[5];
+    h->times.sbs = (uint32_t)nSb;
+    h->times.blocks = h->nBlocks;
+    h->have = true;
+    return IS_OK;
+}
+
+int is_encode_device(is_handle *h, const is_frame *f, void *stream) {
+    if (!h) return IS_ERR_INVALID;
+    IS_CK(cudaSetDevice(h->device));
+    const int rc = prepare(h, f);
+    if (rc) return rc;
+    return run(h, stream ? (cudaStream_t)stream : h->own, f, false);
+}
+
+int is_encode_host(is_handle *h, const is_frame *f, void *stream) {
+    if (!h) return IS_ERR_INVALID;
+    IS_CK(cudaSetDevice(h->device));
+    const int rc = prepare(h, f);
+    if (rc) return rc;
+    return run(h, stream ? (cudaStream_t)stream : h->own, f, true);
+}
+
+int is_record_counts(const is_handle *h, uint32_t *nb, uint32_t *nt, uint64_t *nc) {
+    if (!h || !h->have) return IS_ERR_STATE;
+    if (nb) *nb = h->nBlocks;
+    if (nt) *nt = h->nTxb;
+    if (nc) *nc = h->nCoeffs;
+    return IS_OK;
+}
+
+int is_record_copy(is_handle *h, av1g_frame_params *fp, av1g_block *blocks, uint32_t *block_txb, av1g_txb *txb, int16_t *coeffs,
+                   void *recon[3], const int32_t recon_pitch[3]) {
+    if (!h || !h->have) return IS_ERR_STATE;
+    IS_CK(cudaSetDevice(h->device));
+    const FrameDesc &F = h->F;
+    cudaStream_t st = h->own;
+    if (fp) {
+        memset(fp, 0, sizeof *fp);
+        fp->version = AV1G_DECISIONS_VERSION;
+        fp->width = (uint32_t)F.W; fp->height = (uint32_t)F.H;
+        fp->base_q_idx = (uint8_t)h->qidx;
+        fp->tile_cols_log2 = -1; fp->tile_rows_log2 = -1;
+        fp->qm_y = fp->qm_u = fp->qm_v = 15;
+        fp->chroma_format = AV1G_CHROMA_420;
+        fp->bit_depth = 8;
+    }
+    if (blocks) IS_CK(cudaMemcpyAsync(blocks, F.recBlocks, (size_t)h->nBlocks * sizeof(av1g_block), cudaMemcpyDeviceToHost, st));
+    if (block_txb) IS_CK(cudaMemcpyAsync(block_txb, F.recBlockTxb, ((size_t)h->nBlocks + 1) * 4, cudaMemcpyDeviceToHost, st));
+    if (txb) IS_CK(cudaMemcpyAsync(txb, F.recTxb, (size_t)h->nTxb * sizeof(av1g_txb), cudaMemcpyDeviceToHost, st));
+    if (coeffs) IS_CK(cudaMemcpyAsync(coeffs, F.recCoeffs, (size_t)h->nCoeffs * 2, cudaMemcpyDeviceToHost, st));
+    for (int p = 0; p < 3; p++) {
+        if (!recon || !recon[p]) continue;
+        const int ss = p ? 1 : 0;
+        const int vw = (F.W + ss) >> ss, vh = (F.H + ss) >> ss;
+        IS_CK(cudaMemcpy2DAsync(recon[p], recon_pitch ? recon_pitch[p] : vw, F.rec[p], F.rpitch[p], vw, vh, cudaMemcpyDeviceToHost, st));
+    }
+    IS_CK(cudaStreamSynchronize(st));
+    return IS_OK;
+}
+
+int is_record_device(const is_handle *h, const av1g_block **blocks, const uint32_t **block_txb, const av1g_txb **txb, const int16_t **coeffs) {
+    if (!h || !h->have) return IS_ERR_STATE;
+    if (blocks) *blocks = h->F.recBlocks;
+    if (block_txb) *block_txb = h->F.recBlockTxb;
+    if (txb) *txb = h->F.recTxb;
+    if (coeffs) *coeffs = h->F.recCoeffs;
+    return IS_OK;
+}
+
+int is_times_get(const is_handle *h, is_times *t) {
+    if (!h || !t) return IS_ERR_INVALID;
+    *t = h->times;
+    return IS_OK;
+}
+
+}  // extern "C"
+
+#include "is_testapi.cuh"

@@ -1,0 +1,732 @@
+// is_dev.cuh - device building blocks of the B200 intra search (sm_100a).
+//
+// Everything here is integer arithmetic on the INT32 pipes; warp primitives (shuffles, ballots) do the reductions.
+//   - spec geometry rules (block / tx sizes, tx sets, scans, chroma ownership) over the AV1 spec tables of av1core's
+//     spec_tables.h (data only; av1core's dsp.h / blockinfo.h functions are not used by the product)
+//   - intra prediction of one sample (spec 7.11.2, intra edge filter off) and edge preparation from a plane
+//   - the forward 2-D transform: transposed spec butterfly networks (txfm_gen.cuh), one lane per column, then one lane
+//     per row, registers only
+//   - dead-zone quantiser, transform-domain distortion and the exact coefficient rate with every in-block context
+//   - the exact inverse transform with the spec's conformance checks (for the reconstruction)
+// Fixed-point conventions (shared with the CPU oracle, which restates them independently): coefficients carry FB = 3
+// fractional bits; D is pixel SSE * 2^16; R is in 1/256 bit; lambda in 1/256; J = D + lambda * R (int64).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <type_traits>
+#include "av1g/decisions.h"
+#include "av1g/enums_gen.h"
+#include "av1g/spec_tables.h"
+#include "av1g/cdfctx.h"
+#include "txfm_gen.cuh"
+
+namespace is {
+
+typedef long long i64;
+constexpr i64 INF = 1LL << 60;
+constexpr int FB = 3;
+constexpr int NCDF = (int)(sizeof(av1g_cdfs) / 2);
+// plain-form knobs (reference GpConfig defaults, encoder/src/pipeline.cpp:41-76)
+constexpr int K_TOP = 4, K_RECHECK = 2, UV_K = 2;
+constexpr int UV_OVERHEAD = 384;   // uvOverheadBits 1.5 in 1/256 bit
+constexpr int EDGE_OFF = 16, EDGE_LEN = 16 + 2 * 64 + 16;
+
+// ---- fixed-point tables (host-built, uploaded once per process) ----
+__device__ uint16_t g_cost[4][NCDF];   // -log2(p) * 256 of every CDF symbol of av1g_cdfs, per coefficient q-context
+__constant__ int c_avgY[13];           // y_mode bits averaged over its 25 contexts
+__constant__ int c_avgPart[5][10];     // partition bits averaged over contexts, per block-size level
+__constant__ int c_avgSkip0;           // skip = 0 averaged over contexts
+
+// ---- index of an entry of av1g_cdfs (uint16 units) ----
+#define IS_CB(f) ((int)(offsetof(av1g_cdfs, f) / 2))
+#define IS_CD(f, d) ((int)std::extent<decltype(av1g_cdfs::f), d>::value)
+__device__ __forceinline__ int ci_y_mode(int a, int l) { return IS_CB(y_mode) + (a * IS_CD(y_mode, 1) + l) * IS_CD(y_mode, 2); }
+__device__ __forceinline__ int ci_uv_cfl(int y) { return IS_CB(uv_mode_cfl_allowed) + y * IS_CD(uv_mode_cfl_allowed, 1); }
+__device__ __forceinline__ int ci_uv_nocfl(int y) { return IS_CB(uv_mode_cfl_not_allowed) + y * IS_CD(uv_mode_cfl_not_allowed, 1); }
+__device__ __forceinline__ int ci_angle(int m) { return IS_CB(angle_delta) + m * IS_CD(angle_delta, 1); }
+__device__ __forceinline__ int ci_set1(int s, int d) { return IS_CB(intra_tx_set1) + (s * IS_CD(intra_tx_set1, 1) + d) * IS_CD(intra_tx_set1, 2); }
+__device__ __forceinline__ int ci_set2(int s, int d) { return IS_CB(intra_tx_set2) + (s * IS_CD(intra_tx_set2, 1) + d) * IS_CD(intra_tx_set2, 2); }
+__device__ __forceinline__ int ci_cfl_sign() { return IS_CB(cfl_sign); }
+__device__ __forceinline__ int ci_cfl_alpha(int c) { return IS_CB(cfl_alpha) + c * IS_CD(cfl_alpha, 1); }
+__device__ __forceinline__ int ci_txb_skip(int a, int b) { return IS_CB(txb_skip) + (a * IS_CD(txb_skip, 1) + b) * IS_CD(txb_skip, 2); }
+__device__ __forceinline__ int ci_eob_pt(int ms, int p, int c) {
+    switch (ms) {
+    case 0: return IS_CB(eob_pt_16) + (p * 2 + c) * IS_CD(eob_pt_16, 2);
+    case 1: return IS_CB(eob_pt_32) + (p * 2 + c) * IS_CD(eob_pt_32, 2);
+    case 2: return IS_CB(eob_pt_64) + (p * 2 + c) * IS_CD(eob_pt_64, 2);
+    case 3: return IS_CB(eob_pt_128) + (p * 2 + c) * IS_CD(eob_pt_128, 2);
+    case 4: return IS_CB(eob_pt_256) + (p * 2 + c) * IS_CD(eob_pt_256, 2);
+    case 5: return IS_CB(eob_pt_512) + p * IS_CD(eob_pt_512, 1);
+    default: return IS_CB(eob_pt_1024) + p * IS_CD(eob_pt_1024, 1);
+    }
+}
+__device__ __forceinline__ int ci_eob_extra(int s, int p, int k) {
+    return IS_CB(eob_extra) + ((s * IS_CD(eob_extra, 1) + p) * IS_CD(eob_extra, 2) + k) * IS_CD(eob_extra, 3);
+}
+__device__ __forceinline__ int ci_dc_sign(int p, int c) { return IS_CB(dc_sign) + (p * IS_CD(dc_sign, 1) + c) * IS_CD(dc_sign, 2); }
+__device__ __forceinline__ int ci_base_eob(int s, int p, int c) {
+    return IS_CB(coeff_base_eob) + ((s * IS_CD(coeff_base_eob, 1) + p) * IS_CD(coeff_base_eob, 2) + c) * IS_CD(coeff_base_eob, 3);
+}
+__device__ __forceinline__ int ci_base(int s, int p, int c) {
+    return IS_CB(coeff_base) + ((s * IS_CD(coeff_base, 1) + p) * IS_CD(coeff_base, 2) + c) * IS_CD(coeff_base, 3);
+}
+__device__ __forceinline__ int ci_br(int s, int p, int c) {
+    return IS_CB(coeff_br) + ((s * IS_CD(coeff_br, 1) + p) * IS_CD(coeff_br, 2) + c) * IS_CD(coeff_br, 3);
+}
+
+// ---- warp helpers ----
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ int warp_sum(int v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ i64 warp_sum64(i64 v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ int warp_max(int v) {
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+// index of the smallest (v, i) over the warp; the first of equal values (a serial scan's pick); -1 if all are >= INF
+__device__ __forceinline__ int warp_argmin(i64 v, int i) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const i64 ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+        if (ov < v || (ov == v && oi < i)) { v = ov; i = oi; }
+    }
+    return v < INF ? i : -1;
+}
+
+// ---- geometry (spec tables) ----
+__device__ __forceinline__ int bw4(int bs) { return AV1G_T(Num_4x4_Blocks_Wide)[bs]; }
+__device__ __forceinline__ int bh4(int bs) { return AV1G_T(Num_4x4_Blocks_High)[bs]; }
+__device__ __forceinline__ int txw(int t) { return AV1G_T(Tx_Width)[t]; }
+__device__ __forceinline__ int txh(int t) { return AV1G_T(Tx_Height)[t]; }
+__device__ __forceinline__ bool is_dir(int m) { return m >= AV1G_V_PRED && m <= AV1G_D67_PRED; }
+__device__ __forceinline__ int cand_mode(int c) { return c >> 3; }
+__device__ __forceinline__ int cand_delta(int c) { return (c & 7) - 3; }
+__device__ __forceinline__ int cand_pack(int m, int d) { return (m << 3) | (d + 3); }
+__device__ __forceinline__ int pangle(int m, int d) { return is_dir(m) ? AV1G_T(Mode_To_Angle)[m] + d * AV1G_ANGLE_STEP : 0; }
+
+// get_tx_set() for intra (spec 5.11.48), reduced_tx_set = 0
+__device__ __forceinline__ int tx_set_intra(int txSz) {
+    const int up = AV1G_T(Tx_Size_Sqr_Up)[txSz];
+    if (up >= AV1G_TX_32X32) return AV1G_TX_SET_DCTONLY;
+    if (AV1G_T(Tx_Size_Sqr)[txSz] == AV1G_TX_16X16) return AV1G_TX_SET_INTRA_2;
+    return AV1G_TX_SET_INTRA_1;
+}
+__device__ __forceinline__ bool tx_in_set(int set, int t) { return AV1G_T(Tx_Type_In_Set_Intra)[set][t] != 0; }
+// 1-D kinds of a 2-D type: 0 DCT, 1 ADST, 2 identity (no FLIPADST occurs in the intra sets)
+__device__ __forceinline__ int col_kind(int t) {
+    return (t == AV1G_DCT_DCT || t == AV1G_DCT_ADST || t == AV1G_V_DCT) ? 0 : (t == AV1G_IDTX || t == AV1G_H_DCT) ? 2 : 1;
+}
+__device__ __forceinline__ int row_kind(int t) {
+    return (t == AV1G_DCT_DCT || t == AV1G_ADST_DCT || t == AV1G_H_DCT) ? 0 : (t == AV1G_IDTX || t == AV1G_V_DCT) ? 2 : 1;
+}
+__device__ __forceinline__ int tx_class(int t) {
+    return t == AV1G_V_DCT ? AV1G_TX_CLASS_VERT : t == AV1G_H_DCT ? AV1G_TX_CLASS_HORIZ : AV1G_TX_CLASS_2D;
+}
+// chroma type (spec compute_tx_type for plane > 0): Mode_To_Txfm if in the set, else DCT_DCT
+__device__ __forceinline__ int chroma_tx_type(int uvTx, int uvMode) {
+    if (AV1G_T(Tx_Size_Sqr_Up)[uvTx] > AV1G_TX_32X32) return AV1G_DCT_DCT;
+    const int t = AV1G_T(Mode_To_Txfm)[uvMode];
+    return tx_in_set(tx_set_intra(uvTx), t) ? t : AV1G_DCT_DCT;
+}
+// get_scan() (spec 5.11.41), intra types only (no flips)
+__device__ __forceinline__ const uint16_t *get_scan(int txSz, int txType) {
+    if (txSz == AV1G_TX_16X64) return AV1G_T(Default_Scan_16x32);
+    if (txSz == AV1G_TX_64X16) return AV1G_T(Default_Scan_32x16);
+    if (AV1G_T(Tx_Size_Sqr_Up)[txSz] == AV1G_TX_64X64) return AV1G_T(Default_Scan_32x32);
+    const int cls = txType == AV1G_IDTX ? AV1G_TX_CLASS_2D : tx_class(txType);
+    if (cls == AV1G_TX_CLASS_VERT) {
+        switch (txSz) {
+        case AV1G_TX_4X4: return AV1G_T(Mrow_Scan_4x4);
+        case AV1G_TX_4X8: return AV1G_T(Mrow_Scan_4x8);
+        case AV1G_TX_8X4: return AV1G_T(Mrow_Scan_8x4);
+        case AV1G_TX_8X8: return AV1G_T(Mrow_Scan_8x8);
+        case AV1G_TX_8X16: return AV1G_T(Mrow_Scan_8x16);
+        case AV1G_TX_16X8: return AV1G_T(Mrow_Scan_16x8);
+        case AV1G_TX_16X16: return AV1G_T(Mrow_Scan_16x16);
+        case AV1G_TX_4X16: return AV1G_T(Mrow_Scan_4x16);
+        default: return AV1G_T(Mrow_Scan_16x4);
+        }
+    }
+    if (cls == AV1G_TX_CLASS_HORIZ) {
+        switch (txSz) {
+        case AV1G_TX_4X4: return AV1G_T(Mcol_Scan_4x4);
+        case AV1G_TX_4X8: return AV1G_T(Mcol_Scan_4x8);
+        case AV1G_TX_8X4: return AV1G_T(Mcol_Scan_8x4);
+        case AV1G_TX_8X8: return AV1G_T(Mcol_Scan_8x8);
+        case AV1G_TX_8X16: return AV1G_T(Mcol_Scan_8x16);
+        case AV1G_TX_16X8: return AV1G_T(Mcol_Scan_16x8);
+        case AV1G_TX_16X16: return AV1G_T(Mcol_Scan_16x16);
+        case AV1G_TX_4X16: return AV1G_T(Mcol_Scan_4x16);
+        default: return AV1G_T(Mcol_Scan_16x4);
+        }
+    }
+    switch (txSz) {
+    case AV1G_TX_4X4: return AV1G_T(Default_Scan_4x4);
+    case AV1G_TX_4X8: return AV1G_T(Default_Scan_4x8);
+    case AV1G_TX_8X4: return AV1G_T(Default_Scan_8x4);
+    case AV1G_TX_8X8: return AV1G_T(Default_Scan_8x8);
+    case AV1G_TX_8X16: return AV1G_T(Default_Scan_8x16);
+    case AV1G_TX_16X8: return AV1G_T(Default_Scan_16x8);
+    case AV1G_TX_16X16: return AV1G_T(Default_Scan_16x16);
+    case AV1G_TX_16X32: return AV1G_T(Default_Scan_16x32);
+    case AV1G_TX_32X16: return AV1G_T(Default_Scan_32x16);
+    case AV1G_TX_4X16: return AV1G_T(Default_Scan_4x16);
+    case AV1G_TX_16X4: return AV1G_T(Default_Scan_16x4);
+    case AV1G_TX_8X32: return AV1G_T(Default_Scan_8x32);
+    case AV1G_TX_32X8: return AV1G_T(Default_Scan_32x8);
+    default: return AV1G_T(Default_Scan_32x32);
+    }
+}
+__device__ __forceinline__ int dq_denom(int txSz) {
+    if (txSz == AV1G_TX_32X32 || txSz == AV1G_TX_16X32 || txSz == AV1G_TX_32X16 || txSz == AV1G_TX_16X64 || txSz == AV1G_TX_64X16) return 2;
+    if (txSz == AV1G_TX_64X64 || txSz == AV1G_TX_32X64 || txSz == AV1G_TX_64X32) return 4;
+    return 1;
+}
+// spec 7.12.3 step 1 without quantizer matrices: (|l q| & 0xFFFFFF) / den, signed, clamped to 2^(7 + BitDepth)
+template <int BD> __device__ __forceinline__ int dequant(int l, int q, int den) {
+    const int dq = l * q;
+    int a = (dq < 0 ? -dq : dq) & 0xFFFFFF;
+    a /= den;
+    if (dq < 0) a = -a;
+    return min(max(a, -(1 << (7 + BD))), (1 << (7 + BD)) - 1);
+}
+// HasChroma (spec decode_block); 4:2:0 when ss = 1
+__device__ __forceinline__ bool has_chroma(int bs, int mi_row, int mi_col, int ss) {
+    if (ss && bh4(bs) == 1 && (mi_row & 1) == 0) return false;
+    if (ss && bw4(bs) == 1 && (mi_col & 1) == 0) return false;
+    return true;
+}
+__device__ __forceinline__ int uv_bsize(int bs, int ss) { return AV1G_T(Subsampled_Size)[bs][ss][ss]; }
+__device__ __forceinline__ int uv_tx_size(int bs, int ss) {
+    const int t = AV1G_T(Max_Tx_Size_Rect)[uv_bsize(bs, ss)];
+    const int w = txw(t), h = txh(t);
+    if (w == 64 || h == 64) return w == 16 ? AV1G_TX_16X32 : h == 16 ? AV1G_TX_32X16 : AV1G_TX_32X32;
+    return t;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// intra prediction of one sample (spec 7.11.2.2 / .4 / .5 / .6, edge filter and upsampling off).  A / L point at
+// AboveRow[0] / LeftCol[0] (index -1 valid).
+// ---------------------------------------------------------------------------------------------------------------
+template <typename P>
+__device__ __forceinline__ int pred_px(int mode, int pAng, int i, int j, int lw, int lh, const P *A, const P *L, int dcv) {
+    const int w = 1 << lw, h = 1 << lh;
+    if (mode == AV1G_DC_PRED) return dcv;
+    if (is_dir(mode)) {
+        if (pAng == 90) return A[j];
+        if (pAng == 180) return L[i];
+        if (pAng < 90) {
+            const int dx = AV1G_T(Dr_Intra_Derivative)[pAng];
+            const int idx = (i + 1) * dx, base = (idx >> 6) + j, sh = (idx >> 1) & 0x1F;
+            const int maxBaseX = w + h - 1;
+            return base < maxBaseX ? (A[base] * (32 - sh) + A[base + 1] * sh + 16) >> 5 : A[maxBaseX];
+        }
+        if (pAng < 180) {
+            const int dx = AV1G_T(Dr_Intra_Derivative)[180 - pAng];
+            int idx = (j << 6) - (i + 1) * dx;
+            int base = idx >> 6;
+            if (base >= -1) {
+                const int sh = (idx >> 1) & 0x1F;
+                return (A[base] * (32 - sh) + A[base + 1] * sh + 16) >> 5;
+            }
+            const int dy = AV1G_T(Dr_Intra_Derivative)[pAng - 90];
+            idx = (i << 6) - (j + 1) * dy;
+            base = idx >> 6;
+            const int sh = (idx >> 1) & 0x1F;
+            return (L[base] * (32 - sh) + L[base + 1] * sh + 16) >> 5;
+        }
+        const int dy = AV1G_T(Dr_Intra_Derivative)[270 - pAng];
+        const int idx = (j + 1) * dy, base = (idx >> 6) + i, sh = (idx >> 1) & 0x1F;
+        return (L[base] * (32 - sh) + L[base + 1] * sh + 16) >> 5;
+    }
+    if (mode == AV1G_PAETH_PRED) {
+        const int a = A[j], l = L[i], tl = A[-1], base = a + l - tl;
+        const int pL = abs(base - l), pT = abs(base - a), pTL = abs(base - tl);
+        return (pL <= pT && pL <= pTL) ? l : pT <= pTL ? a : tl;
+    }
+    const uint8_t *wx = lw == 2 ? AV1G_T(Sm_Weights_Tx_4x4) : lw == 3 ? AV1G_T(Sm_Weights_Tx_8x8) : lw == 4 ? AV1G_T(Sm_Weights_Tx_16x16)
+                      : lw == 5 ? AV1G_T(Sm_Weights_Tx_32x32) : AV1G_T(Sm_Weights_Tx_64x64);
+    const uint8_t *wy = lh == 2 ? AV1G_T(Sm_Weights_Tx_4x4) : lh == 3 ? AV1G_T(Sm_Weights_Tx_8x8) : lh == 4 ? AV1G_T(Sm_Weights_Tx_16x16)
+                      : lh == 5 ? AV1G_T(Sm_Weights_Tx_32x32) : AV1G_T(Sm_Weights_Tx_64x64);
+    if (mode == AV1G_SMOOTH_PRED)
+        return (wy[i] * A[j] + (256 - wy[i]) * L[h - 1] + wx[j] * L[i] + (256 - wx[j]) * A[w - 1] + 256) >> 9;
+    if (mode == AV1G_SMOOTH_V_PRED) return (wy[i] * A[j] + (256 - wy[i]) * L[h - 1] + 128) >> 8;
+    return (wx[j] * L[i] + (256 - wx[j]) * A[w - 1] + 128) >> 8;   // SMOOTH_H
+}
+
+// AboveRow / LeftCol preparation (spec 7.11.2, "intra edge" arrays): lanes t = 0..nt-1 of a group fill
+// A[-1 .. w+h-1] / L[-1 .. w+h-1] from a plane (pointer at sample (0, 0), pitch in samples).
+template <int BD, typename P>
+__device__ __forceinline__ void build_edges(const P *plane, int pitch, int x, int y, int w, int h, int haveL, int haveA, int haveAR,
+                                            int haveBL, int maxX, int maxY, P *A, P *L, int t, int nt) {
+    const int n = w + h;
+    const int alim = min(x + (haveAR ? 2 * w : w) - 1, maxX), llim = min(y + (haveBL ? 2 * h : h) - 1, maxY);
+    for (int i = t; i < n; i += nt) {
+        P a, l;
+        if (haveA) a = plane[(size_t)(y - 1) * pitch + min(x + i, alim)];
+        else a = haveL ? plane[(size_t)y * pitch + x - 1] : (P)((1 << (BD - 1)) - 1);
+        if (haveL) l = plane[(size_t)min(y + i, llim) * pitch + x - 1];
+        else l = haveA ? plane[(size_t)(y - 1) * pitch + x] : (P)((1 << (BD - 1)) + 1);
+        A[i] = a;
+        L[i] = l;
+    }
+    if (t == 0) {
+        P c;
+        if (haveA && haveL) c = plane[(size_t)(y - 1) * pitch + x - 1];
+        else if (haveA) c = plane[(size_t)(y - 1) * pitch + x];
+        else if (haveL) c = plane[(size_t)y * pitch + x - 1];
+        else c = (P)(1 << (BD - 1));
+        A[-1] = c;
+        L[-1] = c;
+    }
+}
+// DC value (spec 7.11.2.5), sums over the warp
+template <int BD, typename P>
+__device__ __forceinline__ int warp_dc(const P *A, const P *L, int haveL, int haveA, int lw, int lh) {
+    const int w = 1 << lw, h = 1 << lh, lane = lane_id();
+    int sa = 0, sl = 0;
+    for (int k = lane; k < w; k += 32) sa += A[k];
+    for (int k = lane; k < h; k += 32) sl += L[k];
+    sa = warp_sum(sa);
+    sl = warp_sum(sl);
+    if (haveL && haveA) return (sa + sl + ((w + h) >> 1)) / (w + h);
+    if (haveL) return min((sl + (h >> 1)) >> lh, (1 << BD) - 1);
+    if (haveA) return min((sa + (w >> 1)) >> lw, (1 << BD) - 1);
+    return 1 << (BD - 1);
+}
+
+// 4x4 Hadamard: sum of |coefficients| (the reference's SATD proxy, 4 x the orthonormal SATD)
+__device__ __forceinline__ int hadamard4_sum(int *d) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int *r = d + 4 * i;
+        const int s0 = r[0] + r[1], s1 = r[0] - r[1], s2 = r[2] + r[3], s3 = r[2] - r[3];
+        r[0] = s0 + s2; r[1] = s1 + s3; r[2] = s0 - s2; r[3] = s1 - s3;
+    }
+    int sum = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int s0 = d[j] + d[4 + j], s1 = d[j] - d[4 + j], s2 = d[8 + j] + d[12 + j], s3 = d[8 + j] - d[12 + j];
+        sum += abs(s0 + s2) + abs(s1 + s3) + abs(s0 - s2) + abs(s1 - s3);
+    }
+    return sum;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// forward 2-D transform (warp): columns on lanes, then rows on lanes, all in registers.  Shifts (the range rule):
+// s0 = 17 - BD - log2 H keeps every column intermediate inside int32 rotations, s1 = log2 W the row inputs,
+// s2 brings the result to the dequantisation domain with FB fractional bits:
+//     DQ = M_H^T R M_W 2^(rowShift + 4) / (H W / 4) / rect   (rect: a further x 5793 / 4096 for 2:1 sizes)
+// ---------------------------------------------------------------------------------------------------------------
+template <int N> __device__ __forceinline__ void fwd1d(int kind, int32_t *T) {
+    if (N >= 32 || kind == 0) {
+        if constexpr (N == 4) fwd_dct4(T);
+        else if constexpr (N == 8) fwd_dct8(T);
+        else if constexpr (N == 16) fwd_dct16(T);
+        else if constexpr (N == 32) fwd_dct32(T);
+        else fwd_dct64(T);
+    } else if (kind == 1) {
+        if constexpr (N == 4) fwd_adst4(T);
+        else if constexpr (N == 8) fwd_adst8(T);
+        else if constexpr (N == 16) fwd_adst16(T);
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            if constexpr (N == 4) T[i] = (T[i] * 5793 + 2048) >> 12;
+            else if constexpr (N == 8) T[i] = T[i] * 2;
+            else T[i] = (T[i] * 11586 + 2048) >> 12;
+        }
+    }
+}
+template <int W, int H> struct TxDims {
+    static constexpr int lw = W == 4 ? 2 : W == 8 ? 3 : W == 16 ? 4 : W == 32 ? 5 : 6;
+    static constexpr int lh = H == 4 ? 2 : H == 8 ? 3 : H == 16 ? 4 : H == 32 ? 5 : 6;
+    static constexpr int tw = W > 32 ? 32 : W, th = H > 32 ? 32 : H, n = tw * th;
+    static constexpr int TS = W + 1;   // coefficient row stride in the scratch (odd: conflict-free row reads)
+    static constexpr bool rect = (lw - lh == 1 || lh - lw == 1);
+    static constexpr int size = W == H ? (W == 4 ? AV1G_TX_4X4 : W == 8 ? AV1G_TX_8X8 : W == 16 ? AV1G_TX_16X16 : W == 32 ? AV1G_TX_32X32 : AV1G_TX_64X64)
+                              : (W == 4 && H == 8) ? AV1G_TX_4X8 : (W == 8 && H == 4) ? AV1G_TX_8X4 : (W == 8 && H == 16) ? AV1G_TX_8X16
+                              : (W == 16 && H == 8) ? AV1G_TX_16X8 : (W == 16 && H == 32) ? AV1G_TX_16X32 : (W == 32 && H == 16) ? AV1G_TX_32X16
+                              : (W == 32 && H == 64) ? AV1G_TX_32X64 : (W == 64 && H == 32) ? AV1G_TX_64X32 : (W == 4 && H == 16) ? AV1G_TX_4X16
+                              : (W == 16 && H == 4) ? AV1G_TX_16X4 : (W == 8 && H == 32) ? AV1G_TX_8X32 : (W == 32 && H == 8) ? AV1G_TX_32X8
+                              : (W == 16 && H == 64) ? AV1G_TX_16X64 : AV1G_TX_64X16;
+    static constexpr int rowShift = (size == AV1G_TX_4X4 || size == AV1G_TX_4X8 || size == AV1G_TX_8X4) ? 0
+                                  : (size == AV1G_TX_16X16 || size == AV1G_TX_32X32 || size == AV1G_TX_64X64 || size == AV1G_TX_8X32 ||
+                                     size == AV1G_TX_32X8 || size == AV1G_TX_16X64 || size == AV1G_TX_64X16) ? 2 : 1;
+    static constexpr int E = rowShift + 4 + FB - (lw + lh - 2);
+    // distortion: pixel SSE = sum (DQ - dequant)^2 2^-(2 FB + k)
+    static constexpr int k = 2 * (rowShift + 4) - (lw + lh - 2) + (rect ? 1 : 0);
+    static constexpr int dsh = 16 - 2 * FB - k;
+};
+
+// Residual source of an evaluation: src - prediction (a mode with edges, or CfL), computed per sample; or a given
+// residual array (kernel tests).
+template <typename P>
+struct ResFn {
+    const P *src;        // sample (0, 0) of the block
+    int sp;
+    const P *A, *L;      // edges (index 0 = AboveRow[0] / LeftCol[0])
+    int mode, pAng, lw, lh, dcv;
+    const int16_t *cfl;  // CfL luma values (nullptr: not CfL), row stride 1 << lw
+    int alpha, avg, maxv;
+    const int32_t *arr;  // residual array (H x W row-major) instead of src - prediction
+    __device__ __forceinline__ int pred(int i, int j) const {
+        if (cfl) {
+            const int v = alpha * (cfl[(i << lw) + j] - avg);
+            const int s = v >= 0 ? (v + 32) >> 6 : -((-v + 32) >> 6);
+            return min(max(dcv + s, 0), maxv);
+        }
+        return pred_px(mode, pAng, i, j, lw, lh, A, L, dcv);
+    }
+    __device__ __forceinline__ int operator()(int i, int j) const { return arr ? arr[(i << lw) + j] : (int)src[i * sp + j] - pred(i, j); }
+};
+template <typename P>
+__device__ __forceinline__ ResFn<P> res_mode(const P *src, int sp, const P *A, const P *L, int mode, int delta, int lw, int lh, int dcv) {
+    return ResFn<P>{src, sp, A, L, mode, pangle(mode, delta), lw, lh, dcv, nullptr, 0, 0, 0, nullptr};
+}
+template <typename P>
+__device__ __forceinline__ ResFn<P> res_cfl(const P *src, int sp, int lw, int lh, int dcv, const int16_t *cfl, int alpha, int avg, int maxv) {
+    return ResFn<P>{src, sp, nullptr, nullptr, AV1G_DC_PRED, 0, lw, lh, dcv, cfl, alpha, avg, maxv, nullptr};
+}
+
+// forward 2-D transform of the residual res (H x W int16, row-major, shared memory) into tmp (th x tw, row stride TS)
+template <int W, int H, int BD>
+__device__ __forceinline__ void warp_fwd(const int16_t *res, int txType, int32_t *tmp) {
+    typedef TxDims<W, H> D;
+    constexpr int s0 = (17 - BD - D::lh) > 0 ? (17 - BD - D::lh) : 0, s1 = D::lw, s2 = s0 - s1 - D::E;
+    const int lane = lane_id();
+    const int ck = col_kind(txType), rk = row_kind(txType);
+    for (int j = lane; j < W; j += 32) {
+        int32_t T[H];
+#pragma unroll
+        for (int i = 0; i < H; i++) T[i] = (int32_t)res[i * W + j] * (1 << s0);
+        fwd1d<H>(ck, T);
+#pragma unroll
+        for (int i = 0; i < D::th; i++) tmp[i * D::TS + j] = (T[i] + (1 << (s1 - 1))) >> s1;
+    }
+    __syncwarp();
+    for (int i = lane; i < D::th; i += 32) {
+        int32_t T[W];
+#pragma unroll
+        for (int j = 0; j < W; j++) T[j] = tmp[i * D::TS + j];
+        fwd1d<W>(rk, T);
+#pragma unroll
+        for (int j = 0; j < D::tw; j++) {
+            int32_t v = T[j];
+            if (D::rect) v = (v * 5793 + 2048) >> 12;
+            if constexpr (s2 > 0) v = (v + (1 << (s2 - 1))) >> s2;
+            else if constexpr (s2 < 0) v = v * (1 << -s2);
+            tmp[i * D::TS + j] = v;
+        }
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// quantisation + distortion + exact rate (warp)
+// ---------------------------------------------------------------------------------------------------------------
+struct EvalIn {
+    int txType, plane, skipCtx, dcCtx, intraDir, dcQ, acQ;
+    const uint16_t *C;   // cost table of the image's q-context
+};
+struct EvalOut { i64 D, R; int eob; };
+
+__device__ __forceinline__ int tx_index_in_set(int set, int t) {
+    if (set == AV1G_TX_SET_INTRA_1) { for (int i = 0; i < 7; i++) if (AV1G_T(Tx_Type_Intra_Inv_Set1)[i] == t) return i; }
+    else { for (int i = 0; i < 5; i++) if (AV1G_T(Tx_Type_Intra_Inv_Set2)[i] == t) return i; }
+    return 0;
+}
+
+// txb_skip, tx type, eob position bits
+__device__ __noinline__ i64 base_bits(int txSz, const EvalIn &e, int eob) {
+    const int txSzCtx = (AV1G_T(Tx_Size_Sqr)[txSz] + AV1G_T(Tx_Size_Sqr_Up)[txSz] + 1) >> 1;
+    const uint16_t *C = e.C;
+    if (eob == 0) return C[ci_txb_skip(txSzCtx, e.skipCtx) + 1];
+    i64 b = C[ci_txb_skip(txSzCtx, e.skipCtx)];
+    const int ptype = e.plane > 0;
+    if (e.plane == 0) {
+        const int set = tx_set_intra(txSz);
+        if (set > 0) {
+            const int sqr = AV1G_T(Tx_Size_Sqr)[txSz], idx = tx_index_in_set(set, e.txType);
+            b += set == AV1G_TX_SET_INTRA_1 ? C[ci_set1(sqr, e.intraDir) + idx] : C[ci_set2(sqr, e.intraDir) + idx];
+        }
+    }
+    const int ms = min((int)AV1G_T(Tx_Width_Log2)[txSz], 5) + min((int)AV1G_T(Tx_Height_Log2)[txSz], 5) - 4;
+    const int eobPt = eob <= 2 ? eob : 2 + (31 - __clz(eob - 1));
+    b += C[ci_eob_pt(ms, ptype, tx_class(e.txType) == AV1G_TX_CLASS_2D ? 0 : 1) + eobPt - 1];
+    if (eobPt >= 3) {
+        const int rem = eob - ((1 << (eobPt - 2)) + 1);
+        b += C[ci_eob_extra(txSzCtx, ptype, eobPt - 3) + ((rem >> (eobPt - 3)) & 1)];
+        b += (eobPt - 3) * 256;
+    }
+    return b;
+}
+
+// bits of the coefficient at scan position c < eob (levels q natural order, row stride = adjusted width)
+__device__ __forceinline__ int coeff_bits(int c, int eob, const int16_t *q, const uint16_t *scan, int txSz, int txClass, int ptype,
+                                          int dcCtx, const uint16_t *C) {
+    const int txSzCtx = (AV1G_T(Tx_Size_Sqr)[txSz] + AV1G_T(Tx_Size_Sqr_Up)[txSz] + 1) >> 1;
+    const int adj = AV1G_T(Adjusted_Tx_Size)[txSz];
+    const int bwl = AV1G_T(Tx_Width_Log2)[adj];
+    const int width = 1 << bwl, height = AV1G_T(Tx_Height)[adj];
+    const int pos = scan[c];
+    const int qv = q[pos], v = abs(qv), level = min(v, 15);
+    const int row = pos >> bwl, col = pos - (row << bwl);
+    int b;
+    if (c == eob - 1) {
+        const int area = height << bwl;
+        const int bctx = c == 0 ? 0 : c <= area / 8 ? 1 : c <= area / 4 ? 2 : 3;
+        b = C[ci_base_eob(txSzCtx, ptype, bctx) + min(level, 3) - 1];
+    } else {
+        int mag = 0;
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            const int rr = row + AV1G_T(Sig_Ref_Diff_Offset)[txClass][k][0], cc = col + AV1G_T(Sig_Ref_Diff_Offset)[txClass][k][1];
+            if (rr < height && cc < width) mag += min(abs((int)q[(rr << bwl) + cc]), 3);
+        }
+        int bctx = min((mag + 1) >> 1, 4);
+        if (txClass == AV1G_TX_CLASS_2D) bctx = (row == 0 && col == 0) ? 0 : bctx + AV1G_T(Coeff_Base_Ctx_Offset)[txSz][min(row, 4)][min(col, 4)];
+        else bctx += AV1G_T(Coeff_Base_Pos_Ctx_Offset)[min(txClass == AV1G_TX_CLASS_VERT ? row : col, 2)];
+        b = C[ci_base(txSzCtx, ptype, bctx) + min(level, 3)];
+    }
+    if (level > 2) {
+        int mag = 0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const int rr = row + AV1G_T(Mag_Ref_Offset_With_Tx_Class)[txClass][k][0], cc = col + AV1G_T(Mag_Ref_Offset_With_Tx_Class)[txClass][k][1];
+            if (rr < height && cc < width) mag += min(abs((int)q[rr * width + cc]), 15);
+        }
+        mag = min((mag + 1) >> 1, 6);
+        const int brctx = pos == 0 ? mag
+                        : txClass == AV1G_TX_CLASS_2D ? ((row < 2 && col < 2) ? mag + 7 : mag + 14)
+                        : txClass == AV1G_TX_CLASS_HORIZ ? (col == 0 ? mag + 7 : mag + 14) : (row == 0 ? mag + 7 : mag + 14);
+        const int cid = ci_br(min(txSzCtx, (int)AV1G_TX_32X32), ptype, brctx);
+        int rem = level - 3;
+        for (int i = 0; i < 4; i++) {
+            const int k = min(rem, 3);
+            b += C[cid + k];
+            rem -= k;
+            if (k < 3) break;
+        }
+    }
+    if (v) {
+        b += c == 0 ? C[ci_dc_sign(ptype, dcCtx) + (qv < 0)] : 256;
+        if (v > 14) b += (2 * (31 - __clz(v - 14)) + 1) * 256;
+    }
+    return b;
+}
+
+// quantise the coefficients in tmp (th x tw, row stride TS) into q (tw x th natural order), distortion, rate.
+// zbin 21/32, rounding 3/8 of the step (the reference's 0.656 / 0.375), levels capped at 16383.
+template <int W, int H, int BD>
+__device__ __forceinline__ EvalOut warp_quant_rate(const int32_t *tmp, int16_t *q, const EvalIn &e, i64 resE) {
+    typedef TxDims<W, H> D;
+    constexpr int txSz = D::size;
+    const int lane = lane_id();
+    const int den = dq_denom(txSz);
+    i64 dist = 0, kept = 0;
+    for (int idx = lane; idx < D::n; idx += 32) {
+        const int i = idx / D::tw, j = idx % D::tw;
+        const int v = tmp[i * D::TS + j];
+        const int step = idx == 0 ? e.dcQ : e.acQ;
+        const int a = abs(v) * den, S = step << FB;
+        int l = 0;
+        if (a * 32 >= 21 * S) l = min((8 * a + 3 * S) / (8 * S), 16383);
+        const int qv = v < 0 ? -l : l;
+        q[idx] = (int16_t)qv;
+        const int dq = l ? dequant<BD>(qv, step, den) * (1 << FB) : 0;
+        const i64 d = (i64)(v - dq);
+        dist += d * d;
+        kept += (i64)v * v;
+    }
+    dist = warp_sum64(dist);
+    __syncwarp();
+    const uint16_t *scan = get_scan(txSz, e.txType);
+    int last = 0;
+    for (int c = lane; c < D::n; c += 32)
+        if (q[scan[c]]) last = c + 1;
+    const int eob = warp_max(last);
+    i64 bits = 0;
+    if (eob > 0) {
+        const int cls = tx_class(e.txType);
+        int b = 0;
+        for (int c = lane; c < eob; c += 32) b += coeff_bits(c, eob, q, scan, txSz, cls, e.plane > 0, e.dcCtx, e.C);
+        bits = warp_sum(b);
+    }
+    bits += base_bits(txSz, e, eob);
+    EvalOut o;
+    o.D = dist << D::dsh;
+    if (W == 64 || H == 64) {
+        kept = warp_sum64(kept);
+        const i64 extra = (resE << 16) - (kept << D::dsh);
+        o.D += extra > 0 ? extra : 0;
+    }
+    o.R = bits;
+    o.eob = eob;
+    return o;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// exact inverse transform (spec 7.13.3, Lossless = 0) + conformance flags.  Rows on lanes, then columns on lanes
+// (warp), residual rows stored in res (H x W int32 scratch).
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t inv_adst4(int32_t *T, int r) {   // spec 7.13.2.6 with its range checks
+    const i64 s0 = 1321LL * T[0], s1 = 2482LL * T[0], s2 = 3344LL * T[1], s3 = 3803LL * T[2], s4 = 1321LL * T[2];
+    const i64 s5 = 2482LL * T[3], s6 = 3803LL * T[3];
+    const i64 a7 = (i64)T[0] - T[2], b7 = a7 + T[3];
+    uint32_t e = 0;
+    auto chk = [&](i64 v, int bits) { if (v < -(1LL << (bits - 1)) || v > (1LL << (bits - 1)) - 1) e |= 2; };
+    chk(a7, r + 1); chk(b7, r);
+    chk(s0, r + 12); chk(s1, r + 12); chk(s2, r + 12); chk(s3, r + 12); chk(s4, r + 12); chk(s5, r + 12); chk(s6, r + 12);
+    i64 t0 = s0 + s3, t1 = s1 - s4, t3 = s2, t2 = 3344LL * b7;
+    chk(t0, r + 12); chk(t1, r + 12); chk(t2, r + 12);
+    t0 += s5; t1 -= s6;
+    chk(t0, r + 12); chk(t1, r + 12);
+    const i64 x0 = t0 + t3, x1 = t1 + t3, x2 = t2;
+    i64 x3 = t0 + t1;
+    chk(x3, r + 12);
+    x3 -= t3;
+    chk(x0, r + 12); chk(x1, r + 12); chk(x2, r + 12); chk(x3, r + 12);
+    T[0] = (int32_t)((x0 + 2048) >> 12); T[1] = (int32_t)((x1 + 2048) >> 12);
+    T[2] = (int32_t)((x2 + 2048) >> 12); T[3] = (int32_t)((x3 + 2048) >> 12);
+    return e;
+}
+template <int N> __device__ __forceinline__ uint32_t inv1d(int kind, int32_t *T, int r) {
+    if (N >= 32 || kind == 0) {
+        if constexpr (N == 4) return inv_dct4(T, r);
+        else if constexpr (N == 8) return inv_dct8(T, r);
+        else if constexpr (N == 16) return inv_dct16(T, r);
+        else if constexpr (N == 32) return inv_dct32(T, r);
+        else return inv_dct64(T, r);
+    } else if (kind == 1) {
+        if constexpr (N == 4) return inv_adst4(T, r);
+        else if constexpr (N == 8) return inv_adst8(T, r);
+        else if constexpr (N == 16) return inv_adst16(T, r);
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            if constexpr (N == 4) T[i] = (int32_t)(((i64)T[i] * 5793 + 2048) >> 12);
+            else if constexpr (N == 8) T[i] = T[i] * 2;
+            else T[i] = (int32_t)(((i64)T[i] * 11586 + 2048) >> 12);
+        }
+    }
+    return 0;
+}
+
+// levels q (tw x th) -> residual res (H x W row-major) of the spec's 2-D inverse; returns the OR of the flags.  The
+// row outputs are clamped to colClampRange (16 bits at 8 and 10 bits) and the final residual is within 12 bits, so int16
+// holds both.
+template <int W, int H, int BD>
+__device__ __forceinline__ uint32_t warp_inverse(const int16_t *q, int txType, int dcQ, int acQ, int16_t *res) {
+    typedef TxDims<W, H> D;
+    constexpr int rowR = BD + 8, colR = (BD + 6) > 16 ? BD + 6 : 16;
+    const int lane = lane_id();
+    const int den = dq_denom(D::size);
+    const int ck = col_kind(txType), rk = row_kind(txType);
+    uint32_t err = 0;
+    for (int i = lane; i < H; i += 32) {
+        int32_t T[W];
+        bool nz = false;
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            int v = 0;
+            if (i < D::th && j < D::tw) {
+                const int l = q[i * D::tw + j];
+                v = l ? dequant<BD>(l, (i == 0 && j == 0) ? dcQ : acQ, den) : 0;
+            }
+            T[j] = v;
+            nz |= v != 0;
+        }
+        if (!nz) {
+#pragma unroll
+            for (int j = 0; j < W; j++) res[i * W + j] = 0;
+            continue;
+        }
+        if (D::rect) {
+#pragma unroll
+            for (int j = 0; j < W; j++) T[j] = (int32_t)(((i64)T[j] * 2896 + 2048) >> 12);
+        }
+        err |= inv1d<W>(rk, T, rowR);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            int32_t v = D::rowShift ? (int32_t)(((i64)T[j] + (1 << (D::rowShift - 1))) >> D::rowShift) : T[j];
+            res[i * W + j] = (int16_t)min(max(v, -(1 << (colR - 1))), (1 << (colR - 1)) - 1);
+        }
+    }
+    __syncwarp();
+    for (int j = lane; j < W; j += 32) {
+        int32_t T[H];
+#pragma unroll
+        for (int i = 0; i < H; i++) T[i] = res[i * W + j];
+        err |= inv1d<H>(ck, T, colR);
+#pragma unroll
+        for (int i = 0; i < H; i++) res[i * W + j] = (int16_t)(((i64)T[i] + 8) >> 4);
+    }
+    __syncwarp();
+    return (uint32_t)warp_max((int)err);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// runtime dispatch over the 19 tx sizes
+// ---------------------------------------------------------------------------------------------------------------
+// one evaluation of any tx size (warp): residual into res (lanes over samples), forward transform, quantisation,
+// rate, distortion.  res: H x W int16 scratch, tmp: 32 x 65 int32 scratch, q: the levels (may alias res).
+#define IS_TX_SWITCH(txSz, M)            \
+    switch (txSz) {                      \
+    case AV1G_TX_4X4: M(4, 4); break;    \
+    case AV1G_TX_8X8: M(8, 8); break;    \
+    case AV1G_TX_16X16: M(16, 16); break; \
+    case AV1G_TX_32X32: M(32, 32); break; \
+    case AV1G_TX_64X64: M(64, 64); break; \
+    case AV1G_TX_4X8: M(4, 8); break;    \
+    case AV1G_TX_8X4: M(8, 4); break;    \
+    case AV1G_TX_8X16: M(8, 16); break;  \
+    case AV1G_TX_16X8: M(16, 8); break;  \
+    case AV1G_TX_16X32: M(16, 32); break; \
+    case AV1G_TX_32X16: M(32, 16); break; \
+    case AV1G_TX_32X64: M(32, 64); break; \
+    case AV1G_TX_64X32: M(64, 32); break; \
+    case AV1G_TX_4X16: M(4, 16); break;  \
+    case AV1G_TX_16X4: M(16, 4); break;  \
+    case AV1G_TX_8X32: M(8, 32); break;  \
+    case AV1G_TX_32X8: M(32, 8); break;  \
+    case AV1G_TX_16X64: M(16, 64); break; \
+    default: M(64, 16); break;           \
+    }
+
+}  // namespace is
+
+namespace is {
+template <int BD, typename Px>
+__device__ __noinline__ EvalOut rc_eval(int txSz, const ResFn<Px> &rf, const EvalIn &e, int16_t *res, int32_t *tmp, int16_t *q) {
+    const int lane = lane_id();
+    const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W);
+    i64 en = 0;
+    for (int p = lane; p < W * H; p += 32) {
+        const int r = rf(p >> lw, p & (W - 1));
+        res[p] = (int16_t)r;
+        en += r * r;
+    }
+    __syncwarp();
+    const i64 resE = (W == 64 || H == 64) ? warp_sum64(en) : 0;
+    EvalOut o;
+#define IS_RC_EVAL(W_, H_) { warp_fwd<W_, H_, BD>(res, e.txType, tmp); o = warp_quant_rate<W_, H_, BD>(tmp, q, e, resE); }
+    IS_TX_SWITCH(txSz, IS_RC_EVAL)
+#undef IS_RC_EVAL
+    return o;
+}
+template <int BD>
+__device__ __noinline__ uint32_t rc_inverse(int txSz, const int16_t *q, int txType, int dcQ, int acQ, int16_t *res) {
+    uint32_t e = 0;
+#define IS_RC_INV(W_, H_) e = warp_inverse<W_, H_, BD>(q, txType, dcQ, acQ, res)
+    IS_TX_SWITCH(txSz, IS_RC_INV)
+#undef IS_RC_INV
+    return e;
+}
+}  // namespace is

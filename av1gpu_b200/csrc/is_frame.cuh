@@ -1,0 +1,72 @@
+// is_frame.cuh - the per-image descriptor shared by the host orchestration and the kernels, and the HBM layout.
+//
+// HBM layout of one image (all in one workspace, 256-byte aligned sub-buffers):
+//   src[p], rec[p]   planes with a margin of SRC_MARGIN_Y rows above and SRC_MARGIN_X samples left of sample (0, 0),
+//                    padded by edge replication to the 64x64 SB grid plus one SB column, pitch a multiple of 16 bytes,
+//                    so a superblock tile and its edges are always in bounds for 128-bit loads.
+//   blk              analysis records, shape-major: blk[shOff[s] + by * shNbx[s] + bx] (16 bytes)
+//   leaves / nLeaves DP output, 256 slots per SB
+//   mYMode, cLvl, cDc  4x4 context maps (luma MiRows x MiCols, chroma (MiRows >> ss) x (MiCols >> ss))
+//   oBlocks / oTxb / oCoeffs  closed-loop output slots per SB (compacted into the DecisionRecord by k_pack)
+#pragma once
+#include <stdint.h>
+#include "av1g/decisions.h"
+
+namespace is {
+
+constexpr int SRC_MARGIN_X = 16, SRC_MARGIN_Y = 1;
+constexpr int SB_MAX_LEAVES = 256;
+constexpr int SB_MAX_TXB = 768;      // luma 256 + chroma 2 x 256 (4:4:4 bound)
+constexpr int SB_MAX_COEF = 12288;   // 3 x 64 x 64
+
+struct BlockRes {      // analysis result of one (shape, position): 16 bytes
+    long long J;       // best open-loop RD cost (J units)
+    uint8_t cand[4];   // candidates (mode << 3 | delta + 3), best first
+    uint8_t ncand;
+    uint8_t tx;        // best tx type of cand[0]
+    uint8_t pad[2];
+};
+struct Leaf { uint8_t bsize, x4, y4, pad; };
+struct SbCount { uint32_t nBlocks, nTxb, nCoeffs, pad; };
+
+struct FrameDesc {
+    int W, H, MiCols, MiRows, sbCols, sbRows, ssx, ssy, bd, qidx, qctx;
+    int tileCols, tileRows;
+    int tileColStart[65], tileRowStart[65];   // mi units, [n] = MiCols / MiRows
+    const uint8_t *src[3];                    // sample (0, 0); samples of the bit depth
+    int spitch[3];                            // in samples
+    uint8_t *rec[3];
+    int rpitch[3];
+    uint8_t *mYMode, *cLvl[3], *cDc[3];
+    BlockRes *blk;
+    uint32_t shOff[22];
+    int shNbx[22], shNby[22];
+    long long lam, sqlam;                     // lambda, sqrt(lambda) in 1/256
+    int dcQ, acQ;
+    Leaf *leaves;                             // [nSb * 256]
+    uint16_t *nLeaves;                        // [nSb]
+    av1g_block *oBlocks;                      // [nSb * 256]
+    uint16_t *oBlockTxb;                      // [nSb * 256] first txb (SB-local) of each block
+    av1g_txb *oTxb;                           // [nSb * SB_MAX_TXB] (coeff_off SB-local)
+    int16_t *oCoeffs;                         // [nSb * SB_MAX_COEF]
+    SbCount *sbCount;                         // [nSb]
+    const uint32_t *sbOrder;                  // [nSb] SBs sorted by wavefront step (tile-local c + 2 r)
+    int *sbDone;                              // [nSb] 1 once the SB's reconstruction and maps are complete
+    int *queue;                               // [1] next index into sbOrder
+    int *err;                                 // [1] error status (0 = ok)
+    // pack output (DecisionRecord arrays in decode order) and per-SB offsets
+    uint32_t *sbDecodeOrder;                  // [nSb] SBs in decode order (tiles raster, SB raster inside a tile)
+    uint32_t *offBlk, *offTxb;                // [nSb + 1] exclusive prefix sums in decode order
+    uint64_t *offCoef;                        // [nSb + 1]
+    av1g_block *recBlocks;
+    uint32_t *recBlockTxb;
+    av1g_txb *recTxb;
+    int16_t *recCoeffs;
+};
+
+// error codes written to FrameDesc::err by the kernels
+constexpr int KERR_WAIT_SB = 1;      // a wavefront dependency wait ran out of its iteration budget
+constexpr int KERR_WAIT_LEAF = 2;    // an intra-SB leaf dependency wait ran out
+constexpr int KERR_CAPACITY = 3;     // per-SB output slots exceeded
+
+}  // namespace is

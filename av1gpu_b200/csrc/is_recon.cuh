@@ -1,0 +1,611 @@
+// is_recon.cuh - closed-loop decision + reconstruction: a persistent, dependency-driven SB wavefront.
+//
+// Grid: one CTA per SM (co-resident, cooperative launch), 8 warps.  CTAs take superblocks from a global queue ordered
+// by wavefront step (tile-local col + 2 row: the left and above-right SBs of an SB come earlier), wait - with a bounded
+// spin on an acquire load - for those two SBs to be complete, and run the SB.  Inside an SB the leaves (the DP's
+// blocks in decode order) are claimed by warps in decode order; a warp waits only for the earlier leaves whose area
+// meets its leaf's neighbourhood (edges, above-right / below-left reach, coefficient and mode contexts, 4:2:0 chroma
+// pairs), so independent leaves run concurrently while every leaf still sees exactly the state of a sequential
+// decode-order pass.  Per leaf (one warp; the reference's rc_luma / rc_chroma, encoder/src/k_recon.cuh:822-1686):
+//   luma    real edges from the reconstruction, exact contexts; pass 1 = the analysis' top-2 with DCT_DCT (+ its winner
+//           with its tx type), pass 2 = the other tx types of the pass-1 winner; final levels -> exact inverse (with the
+//           conformance repair) -> reconstruction, record
+//   chroma  CfL luma from the reconstruction, least-squares alpha + +-1 refinement; SATD screening of 13 UV modes
+//           (+ +-1..3 around the best directional one); top-2 + CfL through the exact RD of U and V; final U, V
+// The BlockDecoded state of the spec is derived from a per-4x4 map of the leaf index (a unit is decoded for leaf li
+// iff its leaf index is below li), the SB border rules of clear_block_decoded_flags outside it.
+#pragma once
+#include "is_dev.cuh"
+#include "is_frame.cuh"
+
+namespace is {
+
+constexpr int RC_WARPS = 8;
+// bounded spins: a wait that runs out records an error and moves on instead of hanging, and once any error is recorded
+// no further wait starts (the kernel then finishes with wrong data, which the host discards)
+constexpr int SB_WAIT_ITERS = 1 << 20;
+constexpr int LEAF_WAIT_ITERS = 1 << 20;
+
+template <typename Px> struct RcSmem {
+    uint8_t ordmap[16][16];        // leaf index covering each luma 4x4 unit of the SB (255: none)
+    int leafDone[SB_MAX_LEAVES];
+    Leaf lv[SB_MAX_LEAVES];
+    uint16_t leafTxb[SB_MAX_LEAVES + 1];
+    uint16_t leafCoef[SB_MAX_LEAVES + 1];
+    int next, sbIdx;
+    struct Warp {
+        int16_t res[64 * 64];      // residual of an evaluation; the inverse transform's residual
+        int32_t tmp[32 * 65];      // forward-transform scratch
+        int16_t qa[2][1024], qb[2][1024];   // levels: candidate / best (chroma: U, V)
+        Px ea[3][EDGE_LEN], el[3][EDGE_LEN];
+        int16_t cfl[256];
+        int satd[32];
+        int cand[32];
+    } w[RC_WARPS];
+};
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) { asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
+
+// exact inverse + reconstruction of a tx block (warp), the levels halved until conformant (AV1G_ENC_FIX_RANGE's
+// repair, the reference's cta_inverse_add, k_recon.cuh:140-197); writes prediction + residual into the plane
+template <int BD, typename Px>
+__device__ void rc_reconstruct(int txSz, int txType, int16_t *q, int dcQ, int acQ, const ResFn<Px> &rf, Px *dst, int pitch, int16_t *res) {
+    const int lane = lane_id();
+    const int W = txw(txSz), H = txh(txSz), n = min(W, 32) * min(H, 32);
+    bool any = false;
+    for (;;) {
+        int nz = 0;
+        for (int i = lane; i < n; i += 32) nz |= q[i] != 0;
+        if (!__any_sync(0xffffffffu, nz)) { any = false; break; }
+        const uint32_t err = rc_inverse<BD>(txSz, q, txType, dcQ, acQ, res);
+        if (!err) { any = true; break; }
+        for (int i = lane; i < n; i += 32) q[i] = (int16_t)(q[i] / 2);
+        __syncwarp();
+    }
+    const int lw = 31 - __clz(W);
+    for (int p = lane; p < W * H; p += 32) {
+        const int i = p >> lw, j = p & (W - 1);
+        int v = rf.pred(i, j) + (any ? res[p] : 0);
+        v = min(max(v, 0), (1 << BD) - 1);
+        dst[(size_t)i * pitch + j] = (Px)v;
+    }
+    __syncwarp();
+}
+
+// record a finished tx block: eob, culLevel / dc category into the context maps, the txb entry and its levels
+template <typename Px>
+__device__ int rc_record(const FrameDesc &F, int sb, int plane, int txSz, int txType, int x4, int y4, const int16_t *q, int txbIdx, int coefOff) {
+    const int lane = lane_id();
+    const int W = txw(txSz), H = txh(txSz), n = min(W, 32) * min(H, 32);
+    const uint16_t *scan = get_scan(txSz, txType);
+    int last = 0;
+    for (int c = lane; c < n; c += 32) if (q[scan[c]]) last = c + 1;
+    const int eob = warp_max(last);
+    int cul = 0;
+    for (int c = lane; c < eob; c += 32) cul += abs((int)q[scan[c]]);
+    cul = min(warp_sum(cul), 63);
+    const int dcCat = q[0] < 0 ? 1 : q[0] > 0 ? 2 : 0;
+    const int ss = plane ? F.ssx : 0;
+    const int stride = F.MiCols >> ss, rows = F.MiRows >> ss;
+    const int w4 = W >> 2, h4 = H >> 2;
+    for (int k = lane; k < w4 * h4; k += 32) {
+        const int yy = y4 + k / w4, xx = x4 + k % w4;
+        if (yy < rows && xx < stride) {
+            F.cLvl[plane][(size_t)yy * stride + xx] = (uint8_t)(eob ? cul : 0);
+            F.cDc[plane][(size_t)yy * stride + xx] = (uint8_t)(eob ? dcCat : 0);
+        }
+    }
+    int16_t *oc = F.oCoeffs + (size_t)sb * SB_MAX_COEF + coefOff;
+    for (int i = lane; i < n; i += 32) oc[i] = q[i];
+    if (lane == 0) {
+        av1g_txb t;
+        t.coeff_off = (uint32_t)coefOff;
+        t.x4 = (uint16_t)x4; t.y4 = (uint16_t)y4;
+        t.plane = (uint8_t)plane; t.tx_size = (uint8_t)txSz;
+        t.tx_type = (uint8_t)(plane == 0 && eob == 0 ? AV1G_DCT_DCT : txType);
+        t.flags = 0; t.eob = (uint16_t)eob; t.reserved = 0;
+        F.oTxb[(size_t)sb * SB_MAX_TXB + txbIdx] = t;
+    }
+    __syncwarp();
+    return eob;
+}
+
+// txb skip / dc-sign contexts from the 4x4 maps (spec get_tx_size_context and the reference's txb_ctx,
+// k_recon.cuh:204-238): lane k reads above entry k and left entry k (w4, h4 <= 16)
+__device__ __forceinline__ void rc_txb_ctx(const FrameDesc &F, int plane, int txSz, int x4, int y4, int bsize, int tileX4, int tileY4,
+                                           int *skipCtx, int *dcCtx) {
+    const int lane = lane_id();
+    const int ss = plane ? F.ssx : 0;
+    const int stride = F.MiCols >> ss, maxX4 = F.MiCols >> ss, maxY4 = F.MiRows >> ss;
+    const bool hasAbove = y4 > (tileY4 >> ss), hasLeft = x4 > (tileX4 >> ss);
+    const int w = txw(txSz), h = txh(txSz), w4 = w >> 2, h4 = h >> 2;
+    const bool a = hasAbove && lane < w4 && x4 + lane < maxX4, l = hasLeft && lane < h4 && y4 + lane < maxY4;
+    const int la = a ? F.cLvl[plane][(size_t)(y4 - 1) * stride + x4 + lane] : 0, da = a ? F.cDc[plane][(size_t)(y4 - 1) * stride + x4 + lane] : 0;
+    const int ll = l ? F.cLvl[plane][(size_t)(y4 + lane) * stride + x4 - 1] : 0, dl = l ? F.cDc[plane][(size_t)(y4 + lane) * stride + x4 - 1] : 0;
+    const bool nzA = __any_sync(0xffffffffu, plane ? (la | da) != 0 : la != 0);
+    const bool nzL = __any_sync(0xffffffffu, plane ? (ll | dl) != 0 : ll != 0);
+    const int dcSign = warp_sum((da == 2) - (da == 1) + (dl == 2) - (dl == 1));
+    *dcCtx = dcSign < 0 ? 1 : dcSign > 0 ? 2 : 0;
+    if (plane == 0) {
+        const bool gtA = __any_sync(0xffffffffu, la > 3), gtL = __any_sync(0xffffffffu, ll > 3);
+        if (4 * bw4(bsize) == w && 4 * bh4(bsize) == h) *skipCtx = 0;
+        else if (!nzA && !nzL) *skipCtx = 1;
+        else if (!nzA || !nzL) *skipCtx = 2 + (gtA || gtL);
+        else if (!gtA && !gtL) *skipCtx = 4;
+        else if (!gtA || !gtL) *skipCtx = 5;
+        else *skipCtx = 6;
+    } else {
+        const int ub = uv_bsize(bsize, ss);
+        *skipCtx = (int)nzA + (int)nzL + 7 + ((16 * bw4(ub) * bh4(ub) > w * h) ? 3 : 0);
+    }
+}
+
+template <int BD, typename Px>
+__device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::Warp &Wp, int sb, int sbr, int sbc, int li,
+                        int tR0, int tR1, int tC0, int tC1) {
+    const int lane = lane_id();
+    const Leaf lf = S.lv[li];
+    const int bsize = lf.bsize;
+    const int sbx = sbc * 64, sby = sbr * 64;
+    const int x = sbx + lf.x4 * 4, y = sby + lf.y4 * 4, mi_row = y >> 2, mi_col = x >> 2;
+    const int bw = bw4(bsize), bh = bh4(bsize);
+    const int ss = F.ssx;
+    // ---- wait for the earlier leaves of the neighbourhood ----
+    {
+        const int r0 = max(0, lf.y4 - 2), r1 = min(16, lf.y4 + max(2 * bh, 4));
+        const int c0 = max(0, lf.x4 - 2), c1 = min(16, lf.x4 + max(2 * bw, 4));
+        const int nc = c1 - c0, nu = (r1 - r0) * nc;
+        bool ok = true;
+        for (int u = lane; u < nu; u += 32) {
+            const int o = S.ordmap[r0 + u / nc][c0 + u % nc];
+            if (o < li) {
+                int it = 0;
+                while (!*(volatile int *)&S.leafDone[o]) {
+                    if (++it > LEAF_WAIT_ITERS || *(volatile int *)F.err) { ok = false; break; }
+                    __nanosleep(32);
+                }
+            }
+        }
+        if (!__all_sync(0xffffffffu, ok) && lane == 0) atomicExch(F.err, KERR_WAIT_LEAF);
+        __threadfence_block();
+        __syncwarp();
+    }
+    const int availU = mi_row - 1 >= tR0, availL = mi_col - 1 >= tC0;
+    const bool hasC = has_chroma(bsize, mi_row, mi_col, ss);
+    const int availUC = (ss && bh == 1) ? (mi_row - 2 >= tR0) : availU;
+    const int availLC = (ss && bw == 1) ? (mi_col - 2 >= tC0) : availL;
+    const uint16_t *C = g_cost[F.qctx];
+    const int txbBase = S.leafTxb[li], coefBase = S.leafCoef[li];
+    // BlockDecoded of a 4x4 unit (SB-relative, plane units; ps = 0 luma, ss chroma) for this leaf
+    auto decoded = [&](int ps, int yy, int xx) -> bool {
+        const int sz = 16 >> ps;
+        const int sbW4 = (tC1 - sbc * 16) >> ps, sbH4 = (tR1 - sbr * 16) >> ps;
+        if (yy < 0) return xx < sbW4;
+        if (xx < 0) return yy < sbH4 && yy != sz;
+        if (yy >= sz || xx >= sz) return false;
+        const int o = ps ? S.ordmap[(yy << ps) + 1][(xx << ps) + 1] : S.ordmap[yy][xx];
+        return o < li;
+    };
+    // ================= luma =================
+    int yMode, yDelta, eobY;
+    {
+        const int txSz = AV1G_T(Max_Tx_Size_Rect)[bsize];
+        const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
+        const int haveAR = decoded(0, lf.y4 - 1, lf.x4 + (W >> 2)), haveBL = decoded(0, lf.y4 + (H >> 2), lf.x4 - 1);
+        Px *A = Wp.ea[0] + EDGE_OFF, *L = Wp.el[0] + EDGE_OFF;
+        const Px *rec = (const Px *)F.rec[0];
+        build_edges<BD>(rec, F.rpitch[0], x, y, W, H, availL, availU, haveAR, haveBL, F.MiCols * 4 - 1, F.MiRows * 4 - 1, A, L, lane, 32);
+        __syncwarp();
+        const int dcv = warp_dc<BD>(A, L, availL, availU, lw, lh);
+        const BlockRes br = F.blk[F.shOff[bsize] + (uint32_t)(y / H) * F.shNbx[bsize] + x / W];
+        int skipCtx, dcCtx;
+        rc_txb_ctx(F, 0, txSz, x >> 2, y >> 2, bsize, tC0, tR0, &skipCtx, &dcCtx);
+        const int am = AV1G_T(Intra_Mode_Context)[availU ? F.mYMode[(size_t)(mi_row - 1) * F.MiCols + mi_col] : AV1G_DC_PRED];
+        const int lm = AV1G_T(Intra_Mode_Context)[availL ? F.mYMode[(size_t)mi_row * F.MiCols + mi_col - 1] : AV1G_DC_PRED];
+        auto mbits = [&](int c) -> int {
+            const int m = cand_mode(c);
+            int b = C[ci_y_mode(am, lm) + m];
+            if (bsize >= AV1G_BLOCK_8X8 && is_dir(m)) b += C[ci_angle(m - AV1G_V_PRED) + cand_delta(c) + 3];
+            return b;
+        };
+        const Px *src = (const Px *)F.src[0] + (size_t)y * F.spitch[0] + x;
+        auto rfOf = [&](int c) {
+            const int m = cand_mode(c);
+            return res_mode<Px>(src, F.spitch[0], A, L, m, cand_delta(c), lw, lh, dcv);
+        };
+        const int set = tx_set_intra(txSz);
+        int16_t *cur = Wp.qa[0], *best = Wp.qb[0];
+        i64 bestJ = INF;
+        int bestC = br.cand[0], bestT = br.tx;
+        bool have = false;
+        auto run = [&](int c, int t) {
+            const EvalIn e{t, 0, skipCtx, dcCtx, cand_mode(c), F.dcQ, F.acQ, C};
+            const EvalOut o = rc_eval<BD, Px>(txSz, rfOf(c), e, Wp.res, Wp.tmp, cur);
+            const i64 J = o.D + F.lam * (o.R + mbits(c));
+            if (J < bestJ) {
+                bestJ = J; bestC = c; bestT = t; have = true;
+                int16_t *s = cur; cur = best; best = s;
+            }
+        };
+        const int nc = max(1, min((int)br.ncand, K_RECHECK));
+        const int nT1 = nc + (br.tx != AV1G_DCT_DCT ? 1 : 0);
+        const bool skip1 = nT1 == 1;
+        if (!skip1) {
+            for (int k = 0; k < nc; k++) run(br.cand[k], AV1G_DCT_DCT);
+            if (br.tx != AV1G_DCT_DCT) run(br.cand[0], br.tx);
+        } else {
+            bestC = br.cand[0]; bestT = AV1G_DCT_DCT;
+        }
+        if (set != AV1G_TX_SET_DCTONLY) {
+            const int c1 = bestC;
+            const bool isC0 = c1 == br.cand[0];
+            for (int t = 0; t < 16; t++) {
+                if (!tx_in_set(set, t)) continue;
+                if (!skip1 && (t == AV1G_DCT_DCT || (isC0 && t == br.tx))) continue;
+                run(c1, t);
+            }
+        }
+        if (!have) {   // one candidate, DCT only: its levels
+            const EvalIn e{bestT, 0, skipCtx, dcCtx, cand_mode(bestC), F.dcQ, F.acQ, C};
+            rc_eval<BD, Px>(txSz, rfOf(bestC), e, Wp.res, Wp.tmp, best);
+        }
+        Px *dst = (Px *)F.rec[0] + (size_t)y * F.rpitch[0] + x;
+        rc_reconstruct<BD, Px>(txSz, bestT, best, F.dcQ, F.acQ, rfOf(bestC), dst, F.rpitch[0], Wp.res);
+        eobY = rc_record<Px>(F, sb, 0, txSz, bestT, x >> 2, y >> 2, best, txbBase, coefBase);
+        yMode = cand_mode(bestC);
+        yDelta = cand_delta(bestC);
+        // y mode map (the context of later blocks)
+        for (int k = lane; k < bw * bh; k += 32) {
+            const int r = mi_row + k / bw, c = mi_col + k % bw;
+            if (r < F.MiRows && c < F.MiCols) F.mYMode[(size_t)r * F.MiCols + c] = (uint8_t)yMode;
+        }
+    }
+    // ================= chroma =================
+    int uv = 0, duv = 0, aU = 0, aV = 0, eobU = 0, eobV = 0;
+    if (hasC) {
+        const int txSz = uv_tx_size(bsize, ss);
+        const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
+        const int cx = (mi_col >> ss) * 4, cy = (mi_row >> ss) * 4, cx4 = cx >> 2, cy4 = cy >> 2;
+        const int csr = (mi_row & 15) >> ss, csc = (mi_col & 15) >> ss;
+        const int haveAR = decoded(ss, csr - 1, csc + (W >> 2)), haveBL = decoded(ss, csr + (H >> 2), csc - 1);
+        const int maxX = ((F.MiCols * 4) >> ss) - 1, maxY = ((F.MiRows * 4) >> ss) - 1;
+        Px *A[3], *L[3];
+        int dcv[3];
+        for (int pl = 1; pl <= 2; pl++) {
+            A[pl] = Wp.ea[pl] + EDGE_OFF; L[pl] = Wp.el[pl] + EDGE_OFF;
+            build_edges<BD>((const Px *)F.rec[pl], F.rpitch[pl], cx, cy, W, H, availLC, availUC, haveAR, haveBL, maxX, maxY, A[pl], L[pl], lane, 32);
+        }
+        __syncwarp();
+        for (int pl = 1; pl <= 2; pl++) dcv[pl] = warp_dc<BD>(A[pl], L[pl], availLC, availUC, lw, lh);
+        const Px *sP[3] = {nullptr, (const Px *)F.src[1] + (size_t)cy * F.spitch[1] + cx, (const Px *)F.src[2] + (size_t)cy * F.spitch[2] + cx};
+        const bool cflAllowed = bw <= 8 && bh <= 8;
+        auto uvbits = [&](int m) -> int { return cflAllowed ? C[ci_uv_cfl(yMode) + m] : C[ci_uv_nocfl(yMode) + m]; };
+        auto uvcbits = [&](int c) -> int {
+            const int m = cand_mode(c);
+            int b = uvbits(m);
+            if (bsize >= AV1G_BLOCK_8X8 && is_dir(m)) b += C[ci_angle(m - AV1G_V_PRED) + cand_delta(c) + 3];
+            return b;
+        };
+        // ---- CfL (spec 7.11.5 luma values; least-squares alpha, then the best of alpha - 1 .. + 1 by SSE) ----
+        int alpha[3] = {0, 0, 0}, cflAvg = 0;
+        if (cflAllowed) {
+            const int maxLumaW = x + 4 * bw, maxLumaH = y + 4 * bh;   // tx_depth 0: one luma tx block, starting inside
+            const Px *luma = (const Px *)F.rec[0];
+            const int lp = F.rpitch[0];
+            int sum = 0;
+            for (int p = lane; p < W * H; p += 32) {
+                const int i = p >> lw, j = p & (W - 1);
+                int v;
+                if (ss) {
+                    const int ly = min((cy + i) << 1, maxLumaH - 2), lx = min((cx + j) << 1, maxLumaW - 2);
+                    v = (luma[(size_t)ly * lp + lx] + luma[(size_t)ly * lp + lx + 1] + luma[(size_t)(ly + 1) * lp + lx] + luma[(size_t)(ly + 1) * lp + lx + 1]) << 1;
+                } else {
+                    v = luma[(size_t)min(cy + i, maxLumaH - 1) * lp + min(cx + j, maxLumaW - 1)] << 3;
+                }
+                Wp.cfl[p] = (int16_t)v;
+                sum += v;
+            }
+            sum = warp_sum(sum);
+            cflAvg = (sum + (1 << (lw + lh - 1))) >> (lw + lh);
+            __syncwarp();
+            i64 num1 = 0, num2 = 0, den = 0;
+            for (int p = lane; p < W * H; p += 32) {
+                const int i = p >> lw, j = p & (W - 1);
+                const i64 l = Wp.cfl[p] - cflAvg;
+                num1 += l * ((int)sP[1][i * F.spitch[1] + j] - dcv[1]);
+                num2 += l * ((int)sP[2][i * F.spitch[2] + j] - dcv[2]);
+                den += l * l;
+            }
+            num1 = warp_sum64(num1); num2 = warp_sum64(num2); den = warp_sum64(den);
+            for (int pl = 1; pl <= 2; pl++) {
+                const i64 num = pl == 1 ? num1 : num2;
+                int a = 0;
+                if (den > 0) {
+                    const i64 n = 64 * num;
+                    a = (int)(n >= 0 ? (2 * n + den) / (2 * den) : -((-2 * n + den) / (2 * den)));
+                }
+                a = max(-16, min(16, a));
+                i64 sse[3] = {0, 0, 0};
+                for (int p = lane; p < W * H; p += 32) {
+                    const int i = p >> lw, j = p & (W - 1);
+                    const int l = Wp.cfl[p] - cflAvg, s = sP[pl][i * F.spitch[pl] + j];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        const int ak = max(-16, min(16, a + k - 1));
+                        const int v = ak * l, sc = v >= 0 ? (v + 32) >> 6 : -((-v + 32) >> 6);
+                        const int pr = min(max(dcv[pl] + sc, 0), (1 << BD) - 1);
+                        sse[k] += (i64)(s - pr) * (s - pr);
+                    }
+                }
+                for (int k = 0; k < 3; k++) sse[k] = warp_sum64(sse[k]);
+                int bk = 1;
+                for (int k = 0; k < 3; k++) if (sse[k] < sse[bk]) bk = k;
+                alpha[pl] = max(-16, min(16, a + bk - 1));
+            }
+        }
+        // ---- SATD screening of the UV modes over U and V ----
+        const int nsx = W >> 2, nsub2 = 2 * (W >> 2) * (H >> 2);   // items per candidate: U then V 4x4 sub-blocks
+        auto screen = [&](int c0, int c1) {
+            const int items = (c1 - c0) * nsub2;
+            for (int it0 = 0; it0 < items; it0 += 32) {
+                const int it = it0 + lane;
+                const int ci = c0 + it / nsub2;
+                int t = 0;
+                if (it < items) {
+                    const int r = it % nsub2, pl = 1 + (r >= (nsub2 >> 1)), sbk = r % (nsub2 >> 1);
+                    const int sx = (sbk % nsx) * 4, sy = (sbk / nsx) * 4;
+                    const int c = Wp.cand[ci], m = cand_mode(c), pa = pangle(m, cand_delta(c));
+                    int d[16];
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            d[i * 4 + j] = (int)sP[pl][(sy + i) * F.spitch[pl] + sx + j] - pred_px(m, pa, sy + i, sx + j, lw, lh, A[pl], L[pl], dcv[pl]);
+                    t = hadamard4_sum(d);
+                }
+                for (int o = 16; o > 0; o >>= 1)
+                    if (o < nsub2) t += __shfl_xor_sync(0xffffffffu, t, o);
+                if (it < items && (lane & (nsub2 - 1)) == 0) Wp.satd[ci] += t;
+                __syncwarp();
+            }
+        };
+        Wp.satd[lane] = 0;
+        Wp.cand[lane] = lane < 13 ? cand_pack(lane, 0) : 0;
+        __syncwarp();
+        screen(0, 13);
+        i64 js = lane < 13 ? ((i64)Wp.satd[lane] << 14) + F.sqlam * uvcbits(Wp.cand[lane]) : INF;
+        if (bsize >= AV1G_BLOCK_8X8) {
+            const int bm = warp_argmin((lane >= AV1G_V_PRED && lane <= AV1G_D67_PRED) ? js : INF, lane);
+            if (lane < 6) Wp.cand[13 + lane] = cand_pack(bm, lane < 3 ? -(lane + 1) : (lane - 2));
+            __syncwarp();
+            screen(13, 19);
+            if (lane >= 13 && lane < 19) js = ((i64)Wp.satd[lane] << 14) + F.sqlam * uvcbits(Wp.cand[lane]);
+        }
+        int chosen[UV_K + 1], nch = 0;
+        for (int k = 0; k < UV_K; k++) {
+            const int b = warp_argmin(js, lane);
+            if (b < 0) break;
+            chosen[nch++] = Wp.cand[b];
+            if (lane == b) js = INF;
+        }
+        if (cflAllowed && (alpha[1] || alpha[2])) chosen[nch++] = 255;
+        int skipCtx[3], dcCtx[3];
+        for (int pl = 1; pl <= 2; pl++) rc_txb_ctx(F, pl, txSz, cx4, cy4, bsize, tC0, tR0, &skipCtx[pl], &dcCtx[pl]);
+        auto rfOf = [&](int pl, int c) {
+            if (c == 255) return res_cfl<Px>(sP[pl], F.spitch[pl], lw, lh, dcv[pl], Wp.cfl, alpha[pl], cflAvg, (1 << BD) - 1);
+            return res_mode<Px>(sP[pl], F.spitch[pl], A[pl], L[pl], cand_mode(c), cand_delta(c), lw, lh, dcv[pl]);
+        };
+        int16_t *cur[2] = {Wp.qa[0], Wp.qa[1]}, *best[2] = {Wp.qb[0], Wp.qb[1]};
+        i64 bJ = INF;
+        int bestC = cand_pack(AV1G_DC_PRED, 0);
+        for (int k = 0; k < nch; k++) {
+            const int c = chosen[k];
+            const int mode = c == 255 ? AV1G_UV_CFL_PRED : cand_mode(c);
+            const int txType = chroma_tx_type(txSz, mode);
+            i64 J = 0;
+            for (int pl = 1; pl <= 2; pl++) {
+                const EvalIn e{txType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, C};
+                const EvalOut o = rc_eval<BD, Px>(txSz, rfOf(pl, c), e, Wp.res, Wp.tmp, cur[pl - 1]);
+                J += o.D + F.lam * o.R;
+            }
+            int b;
+            if (c == 255) {
+                const int a1 = alpha[1], a2 = alpha[2];
+                const int sU = a1 == 0 ? 0 : a1 < 0 ? 1 : 2, sV = a2 == 0 ? 0 : a2 < 0 ? 1 : 2;
+                b = uvbits(AV1G_UV_CFL_PRED) + C[ci_cfl_sign() + sU * 3 + sV - 1];
+                if (sU) b += C[ci_cfl_alpha((sU - 1) * 3 + sV) + abs(a1) - 1];
+                if (sV) b += C[ci_cfl_alpha((sV - 1) * 3 + sU) + abs(a2) - 1];
+            } else {
+                b = uvcbits(c);
+            }
+            J += F.lam * b;
+            if (J < bJ) {
+                bJ = J; bestC = c;
+                for (int p = 0; p < 2; p++) { int16_t *s = cur[p]; cur[p] = best[p]; best[p] = s; }
+            }
+        }
+        const bool cfl = bestC == 255;
+        uv = cfl ? AV1G_UV_CFL_PRED : cand_mode(bestC);
+        const int uvType = chroma_tx_type(txSz, uv);
+        for (int pl = 1; pl <= 2; pl++) {
+            Px *dst = (Px *)F.rec[pl] + (size_t)cy * F.rpitch[pl] + cx;
+            rc_reconstruct<BD, Px>(txSz, uvType, best[pl - 1], F.dcQ, F.acQ, rfOf(pl, bestC), dst, F.rpitch[pl], Wp.res);
+            const int yt = AV1G_T(Max_Tx_Size_Rect)[bsize];
+            const int off = coefBase + min(txw(yt), 32) * min(txh(yt), 32) + (pl - 1) * min(W, 32) * min(H, 32);
+            const int e = rc_record<Px>(F, sb, pl, txSz, uvType, cx4, cy4, best[pl - 1], txbBase + pl, off);
+            if (pl == 1) eobU = e; else eobV = e;
+        }
+        duv = cfl ? 0 : cand_delta(bestC);
+        aU = cfl ? alpha[1] : 0;
+        aV = cfl ? alpha[2] : 0;
+    }
+    if (lane == 0) {
+        av1g_block b;
+        b.mi_row = (uint16_t)mi_row; b.mi_col = (uint16_t)mi_col;
+        b.bsize = (uint8_t)bsize;
+        b.skip = (uint8_t)((eobY == 0 && eobU == 0 && eobV == 0) ? 1 : 0);
+        b.tx_depth = 0;
+        b.y_mode = (uint8_t)yMode;
+        b.angle_delta_y = (int8_t)(bsize >= AV1G_BLOCK_8X8 && is_dir(yMode) ? yDelta : 0);
+        b.uv_mode = (uint8_t)(hasC ? uv : 0);
+        b.angle_delta_uv = (int8_t)(hasC && bsize >= AV1G_BLOCK_8X8 && is_dir(uv) ? duv : 0);
+        b.cfl_alpha_u = (int8_t)aU; b.cfl_alpha_v = (int8_t)aV;
+        b.filter_intra = 0; b.cdef_idx = 0; b.sb_qindex = 0;
+        F.oBlocks[(size_t)sb * SB_MAX_LEAVES + li] = b;
+        F.oBlockTxb[(size_t)sb * SB_MAX_LEAVES + li] = (uint16_t)txbBase;
+    }
+    __threadfence_block();
+    __syncwarp();
+    if (lane == 0) *(volatile int *)&S.leafDone[li] = 1;
+}
+
+template <int BD>
+__global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__restrict__ Fp, int nSb) {
+    typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    RcSmem<Px> &S = *reinterpret_cast<RcSmem<Px> *>(smem_raw);
+    const FrameDesc &F = *Fp;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (;;) {
+        if (tid == 0) S.sbIdx = atomicAdd(F.queue, 1);
+        __syncthreads();
+        const int idx = S.sbIdx;
+        if (idx >= nSb) break;
+        const int sb = (int)F.sbOrder[idx], sbr = sb / F.sbCols, sbc = sb % F.sbCols;
+        int tc = 0, tr = 0;
+        while (tc + 1 < F.tileCols && sbc * 16 >= F.tileColStart[tc + 1]) tc++;
+        while (tr + 1 < F.tileRows && sbr * 16 >= F.tileRowStart[tr + 1]) tr++;
+        const int tC0 = F.tileColStart[tc], tC1 = F.tileColStart[tc + 1], tR0 = F.tileRowStart[tr], tR1 = F.tileRowStart[tr + 1];
+        // wait for the left and the above-right (above at the tile's right edge) SBs of the same tile
+        if (tid == 0) {
+            const int sbC0 = tC0 >> 4, sbR0 = tR0 >> 4, sbC1 = (tC1 + 15) >> 4;
+            int dep[2], nd = 0;
+            if (sbc > sbC0) dep[nd++] = sb - 1;
+            if (sbr > sbR0) dep[nd++] = (sbr - 1) * F.sbCols + min(sbc + 1, sbC1 - 1);
+            for (int k = 0; k < nd; k++) {
+                int it = 0;
+                while (!ld_acquire(F.sbDone + dep[k])) {
+                    if (++it > SB_WAIT_ITERS) { atomicExch(F.err, KERR_WAIT_SB); break; }
+                    if (*(volatile int *)F.err) break;
+                    __nanosleep(128);
+                }
+            }
+        }
+        // leaves, the 4x4 leaf-index map, per-leaf output offsets
+        const int nl = F.nLeaves[sb];
+        if (tid < 256) { S.ordmap[tid >> 4][tid & 15] = 255; S.leafDone[tid] = 0; }
+        if (tid < nl) S.lv[tid] = F.leaves[(size_t)sb * SB_MAX_LEAVES + tid];
+        __syncthreads();
+        if (tid < nl) {
+            const Leaf l = S.lv[tid];
+            const int w4 = bw4(l.bsize), h4 = bh4(l.bsize);
+            for (int r = l.y4; r < min(16, l.y4 + h4); r++)
+                for (int c = l.x4; c < min(16, l.x4 + w4); c++) S.ordmap[r][c] = (uint8_t)tid;
+        }
+        if (tid == 0) {
+            int nt = 0, ncf = 0;
+            for (int i = 0; i < nl; i++) {
+                S.leafTxb[i] = (uint16_t)nt;
+                S.leafCoef[i] = (uint16_t)ncf;
+                const Leaf l = S.lv[i];
+                const int yt = AV1G_T(Max_Tx_Size_Rect)[l.bsize];
+                nt += 1;
+                ncf += min(txw(yt), 32) * min(txh(yt), 32);
+                if (has_chroma(l.bsize, sbr * 16 + l.y4, sbc * 16 + l.x4, F.ssx)) {
+                    const int ut = uv_tx_size(l.bsize, F.ssx);
+                    nt += 2;
+                    ncf += 2 * min(txw(ut), 32) * min(txh(ut), 32);
+                }
+            }
+            S.leafTxb[nl] = (uint16_t)nt;
+            S.leafCoef[nl] = (uint16_t)ncf;
+            S.next = RC_WARPS;
+        }
+        __syncthreads();
+        int li = warp;
+        while (li < nl) {
+            rc_leaf<BD, Px>(F, S, S.w[warp], sb, sbr, sbc, li, tR0, tR1, tC0, tC1);
+            int n = 0;
+            if (lane == 0) n = atomicAdd(&S.next, 1);
+            li = __shfl_sync(0xffffffffu, n, 0);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            SbCount c;
+            c.nBlocks = (uint32_t)nl; c.nTxb = S.leafTxb[nl]; c.nCoeffs = S.leafCoef[nl]; c.pad = 0;
+            F.sbCount[sb] = c;
+            __threadfence();
+            st_release(F.sbDone + sb, 1);
+        }
+    }
+}
+
+// ---- pack: per-SB slots -> DecisionRecord arrays in decode order ----
+__global__ void k_pack_scan(const FrameDesc *__restrict__ Fp, int nSb) {
+    // exclusive prefix sums of the per-SB counts over the decode order (one CTA of 1024 threads)
+    const FrameDesc &F = *Fp;
+    __shared__ uint32_t sB[1024], sT[1024];
+    __shared__ unsigned long long sC[1024];
+    const int tid = threadIdx.x;
+    const int per = (nSb + 1023) / 1024, i0 = min(nSb, tid * per), i1 = min(nSb, i0 + per);
+    uint32_t b = 0, t = 0;
+    unsigned long long c = 0;
+    for (int i = i0; i < i1; i++) {
+        const SbCount k = F.sbCount[F.sbDecodeOrder[i]];
+        b += k.nBlocks; t += k.nTxb; c += k.nCoeffs;
+    }
+    sB[tid] = b; sT[tid] = t; sC[tid] = c;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        uint32_t vb = 0, vt = 0;
+        unsigned long long vc = 0;
+        if (tid >= o) { vb = sB[tid - o]; vt = sT[tid - o]; vc = sC[tid - o]; }
+        __syncthreads();
+        sB[tid] += vb; sT[tid] += vt; sC[tid] += vc;
+        __syncthreads();
+    }
+    b = sB[tid] - b; t = sT[tid] - t; c = sC[tid] - c;
+    for (int i = i0; i < i1; i++) {
+        F.offBlk[i] = b; F.offTxb[i] = t; F.offCoef[i] = c;
+        const SbCount k = F.sbCount[F.sbDecodeOrder[i]];
+        b += k.nBlocks; t += k.nTxb; c += k.nCoeffs;
+    }
+    if (tid == 1023) { F.offBlk[nSb] = sB[1023]; F.offTxb[nSb] = sT[1023]; F.offCoef[nSb] = sC[1023]; }
+}
+
+__global__ void k_pack(const FrameDesc *__restrict__ Fp, int nSb) {
+    const FrameDesc &F = *Fp;
+    const int i = blockIdx.x;
+    if (i >= nSb) return;
+    const int sb = (int)F.sbDecodeOrder[i];
+    const SbCount k = F.sbCount[sb];
+    const uint32_t ob = F.offBlk[i], ot = F.offTxb[i];
+    const uint64_t oc = F.offCoef[i];
+    for (uint32_t j = threadIdx.x; j < k.nBlocks; j += blockDim.x) {
+        F.recBlocks[ob + j] = F.oBlocks[(size_t)sb * SB_MAX_LEAVES + j];
+        F.recBlockTxb[ob + j] = ot + F.oBlockTxb[(size_t)sb * SB_MAX_LEAVES + j];
+    }
+    for (uint32_t j = threadIdx.x; j < k.nTxb; j += blockDim.x) {
+        av1g_txb t = F.oTxb[(size_t)sb * SB_MAX_TXB + j];
+        t.coeff_off = (uint32_t)(oc + t.coeff_off);
+        F.recTxb[ot + j] = t;
+    }
+    // coefficients: 16-byte vectors (every tx block holds a multiple of 16 levels, SB slots are 16-byte aligned)
+    const uint4 *s = reinterpret_cast<const uint4 *>(F.oCoeffs + (size_t)sb * SB_MAX_COEF);
+    int16_t *d = F.recCoeffs + oc;
+    if ((oc & 7) == 0) {
+        uint4 *dv = reinterpret_cast<uint4 *>(d);
+        for (uint32_t j = threadIdx.x; j < k.nCoeffs / 8; j += blockDim.x) dv[j] = s[j];
+    } else {
+        const int16_t *ss = F.oCoeffs + (size_t)sb * SB_MAX_COEF;
+        for (uint32_t j = threadIdx.x; j < k.nCoeffs; j += blockDim.x) d[j] = ss[j];
+    }
+    if (i == nSb - 1 && threadIdx.x == 0) F.recBlockTxb[F.offBlk[nSb]] = F.offTxb[nSb];
+}
+
+}  // namespace is

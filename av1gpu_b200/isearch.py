@@ -1,0 +1,238 @@
+"""Host mirror of the reference's GpEncoder (encoder/src/pipeline.h:191-211) over libisearch.so's C ABI.
+
+    enc = Encoder(device=0)                 # GpEncoder::init
+    rec = enc.encode(planes, qindex)        # GpEncoder::encode with host planes (upload inside the call)
+    rec = enc.encode_device(tensors, q)     # device planes (torch CUDA uint8 tensors), GpFrameIn-style
+    rec.blocks, rec.block_txb, rec.txb, rec.coeffs, rec.recon   # av1core DecisionRecord + reconstruction
+
+Errors raise RuntimeError with the library's message (the reference returns -1 + a message, pipeline.cpp:31-39).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libisearch.so")
+
+# av1core DecisionRecord layouts (av1core/include/av1g/decisions.h:225-252), 16 bytes each
+BLOCK_DT = np.dtype([("mi_row", "<u2"), ("mi_col", "<u2"), ("bsize", "u1"), ("skip", "u1"), ("tx_depth", "u1"),
+                     ("y_mode", "u1"), ("angle_delta_y", "i1"), ("uv_mode", "u1"), ("angle_delta_uv", "i1"),
+                     ("cfl_alpha_u", "i1"), ("cfl_alpha_v", "i1"), ("filter_intra", "u1"), ("cdef_idx", "i1"),
+                     ("sb_qindex", "u1")])
+TXB_DT = np.dtype([("coeff_off", "<u4"), ("x4", "<u2"), ("y4", "<u2"), ("plane", "u1"), ("tx_size", "u1"),
+                   ("tx_type", "u1"), ("flags", "u1"), ("eob", "<u2"), ("reserved", "<u2")])
+
+IS_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "wavefront wait timeout",
+             -5: "no result"}
+
+
+class IsParams(C.Structure):
+    _fields_ = [("bit_depth", C.c_int32), ("chroma_444", C.c_int32), ("device", C.c_int32), ("reserved", C.c_int32 * 5)]
+
+
+class IsFrame(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("qindex", C.c_int32), ("pad", C.c_int32),
+                ("planes", C.c_void_p * 3), ("pitch", C.c_int32 * 3), ("pad2", C.c_int32)]
+
+
+class IsTimes(C.Structure):
+    _fields_ = [("upload", C.c_float), ("analysis", C.c_float), ("dp", C.c_float), ("recon", C.c_float),
+                ("pack", C.c_float), ("total", C.c_float), ("sbs", C.c_uint32), ("blocks", C.c_uint32)]
+
+
+# every entry point declared in include/is_api.h
+EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_encode_host", "is_record_counts",
+           "is_record_copy", "is_record_device", "is_times_get", "is_test_fwd_quant", "is_test_inverse",
+           "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables"]
+
+_lib = None
+
+
+def load_library():
+    """The CUDA library; raises if it was not built (there is no CPU path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libisearch.so missing: run `python -m av1gpu_b200.build` (the search has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.is_create.argtypes = [C.POINTER(IsParams), C.POINTER(vp)]
+    L.is_destroy.argtypes = [vp]
+    L.is_destroy.restype = None
+    L.is_last_error.argtypes = [vp]
+    L.is_last_error.restype = C.c_char_p
+    L.is_encode_device.argtypes = [vp, C.POINTER(IsFrame), vp]
+    L.is_encode_host.argtypes = [vp, C.POINTER(IsFrame), vp]
+    L.is_record_counts.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
+    L.is_record_copy.argtypes = [vp, vp, vp, vp, vp, vp, vp * 3, vp]
+    L.is_record_device.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]
+    L.is_times_get.argtypes = [vp, C.POINTER(IsTimes)]
+    L.is_test_fwd_quant.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp]
+    L.is_test_inverse.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, vp]
+    L.is_test_predict.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, vp, vp]
+    L.is_debug_analysis.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+    L.is_debug_leaves.argtypes = [vp, C.c_uint32, vp, vp, vp]
+    L.is_debug_tables.argtypes = [vp, C.c_int, vp, C.c_size_t, vp, vp, vp, C.c_int, C.POINTER(C.c_int64),
+                                  C.POINTER(C.c_int64)]
+    _lib = L
+    return L
+
+
+def host_tables(qctx, qindex=120):
+    """Fixed-point tables the library uploads (no GPU needed): cost table, avgY, avgPart, avgSkip0, lambda, sqrt."""
+    L = load_library()
+    n = L.is_debug_tables(None, qctx, None, 0, None, None, None, qindex, None, None)
+    cost = np.zeros(n, np.uint16)
+    y, p, s = np.zeros(13, np.int32), np.zeros(50, np.int32), np.zeros(1, np.int32)
+    lam, sq = C.c_int64(), C.c_int64()
+    L.is_debug_tables(None, qctx, cost.ctypes.data, n, y.ctypes.data, p.ctypes.data, s.ctypes.data, qindex,
+                      C.byref(lam), C.byref(sq))
+    return cost, y, p.reshape(5, 10), int(s[0]), lam.value, sq.value
+
+
+class Record:
+    """One encoded image: the DecisionRecord arrays (decode order) and the cropped reconstruction."""
+
+    def __init__(self, width, height, qindex, blocks, block_txb, txb, coeffs, recon, times):
+        self.width, self.height, self.qindex = width, height, qindex
+        self.blocks, self.block_txb, self.txb, self.coeffs = blocks, block_txb, txb, coeffs
+        self.recon = recon
+        self.times = times
+
+
+class Encoder:
+    """GpEncoder-shaped handle (one host thread at a time)."""
+
+    def __init__(self, device=0):
+        self.L = load_library()
+        p = IsParams()
+        p.bit_depth, p.chroma_444, p.device = 8, 0, device
+        h = C.c_void_p()
+        rc = self.L.is_create(C.byref(p), C.byref(h))
+        if rc != 0:
+            raise RuntimeError("is_create failed (%d: %s)" % (rc, IS_ERRORS.get(rc, "?")))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.is_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = self.L.is_last_error(self.h).decode(errors="replace")
+            raise RuntimeError("%s failed (%d: %s): %s" % (what, rc, IS_ERRORS.get(rc, "?"), msg))
+
+    @staticmethod
+    def _frame(width, height, qindex, ptrs, pitches):
+        f = IsFrame()
+        f.width, f.height, f.qindex = width, height, qindex
+        for p in range(3):
+            f.planes[p] = ptrs[p]
+            f.pitch[p] = pitches[p]
+        return f
+
+    def encode_host_async(self, planes, qindex, stream=None):
+        """Queue an encode of host planes (Y, U, V numpy uint8, C-contiguous); returns after the record sizes are known."""
+        y = planes[0]
+        f = self._frame(y.shape[1], y.shape[0], qindex, [p.ctypes.data for p in planes], [p.strides[0] for p in planes])
+        self._check(self.L.is_encode_host(self.h, C.byref(f), stream), "is_encode_host")
+        return f
+
+    def encode_device_async(self, planes, qindex, stream=None):
+        """Queue an encode of device planes (torch CUDA uint8 tensors, row-contiguous)."""
+        y = planes[0]
+        f = self._frame(y.shape[1], y.shape[0], qindex, [p.data_ptr() for p in planes], [p.stride(0) for p in planes])
+        self._check(self.L.is_encode_device(self.h, C.byref(f), stream), "is_encode_device")
+        return f
+
+    def counts(self):
+        nb, nt, nc = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        self._check(self.L.is_record_counts(self.h, C.byref(nb), C.byref(nt), C.byref(nc)), "is_record_counts")
+        return nb.value, nt.value, nc.value
+
+    def times(self):
+        t = IsTimes()
+        self._check(self.L.is_times_get(self.h, C.byref(t)), "is_times_get")
+        return {k: getattr(t, k) for k, _ in IsTimes._fields_}
+
+    def fetch(self, width, height, qindex, out=None):
+        """Copy the last record and reconstruction to host memory (numpy arrays, or the preallocated `out` dict)."""
+        nb, nt, nc = self.counts()
+        if out is None:
+            cw, ch = (width + 1) // 2, (height + 1) // 2
+            out = {"blocks": np.zeros(nb, BLOCK_DT), "block_txb": np.zeros(nb + 1, np.uint32),
+                   "txb": np.zeros(nt, TXB_DT), "coeffs": np.zeros(nc, np.int16),
+                   "recon": [np.zeros((height, width), np.uint8), np.zeros((ch, cw), np.uint8), np.zeros((ch, cw), np.uint8)]}
+        rp = (C.c_void_p * 3)(*[r.ctypes.data for r in out["recon"]])
+        pitches = (C.c_int32 * 3)(*[r.strides[0] for r in out["recon"]])
+        self._check(self.L.is_record_copy(self.h, None, out["blocks"].ctypes.data, out["block_txb"].ctypes.data,
+                                          out["txb"].ctypes.data, out["coeffs"].ctypes.data, rp, pitches),
+                    "is_record_copy")
+        return Record(width, height, qindex, out["blocks"][:nb], out["block_txb"][:nb + 1], out["txb"][:nt],
+                      out["coeffs"][:nc], out["recon"], self.times())
+
+    def encode(self, planes, qindex):
+        """Encode host planes end to end: upload, search, download of the record and the reconstruction."""
+        planes = [np.ascontiguousarray(p, np.uint8) for p in planes]
+        self.encode_host_async(planes, qindex)
+        return self.fetch(planes[0].shape[1], planes[0].shape[0], qindex)
+
+    def encode_device(self, planes, qindex):
+        self.encode_device_async(planes, qindex)
+        return self.fetch(planes[0].shape[1], planes[0].shape[0], qindex)
+
+    # ---- kernel-level entry points (parity tests) ----
+    def test_fwd_quant(self, res, tx_size, tx_type, plane, qindex, ctx):
+        res = np.ascontiguousarray(res, np.int32)
+        n = res.shape[0]
+        h, w = res.shape[1], res.shape[2]
+        nc = min(w, 32) * min(h, 32)
+        coef, lv = np.zeros((n, nc), np.int32), np.zeros((n, nc), np.int16)
+        D, R, eob = np.zeros(n, np.int64), np.zeros(n, np.int64), np.zeros(n, np.int32)
+        cx = np.array(ctx, np.int32)
+        self._check(self.L.is_test_fwd_quant(self.h, n, res.ctypes.data, tx_size, tx_type, plane, qindex, cx.ctypes.data,
+                                             coef.ctypes.data, lv.ctypes.data, D.ctypes.data, R.ctypes.data,
+                                             eob.ctypes.data), "is_test_fwd_quant")
+        return coef, lv, D, R, eob
+
+    def test_inverse(self, levels, tx_size, tx_type, qindex, w, h):
+        levels = np.ascontiguousarray(levels, np.int16)
+        n = levels.shape[0]
+        res, fl = np.zeros((n, h * w), np.int32), np.zeros(n, np.uint32)
+        self._check(self.L.is_test_inverse(self.h, n, levels.ctypes.data, tx_size, tx_type, qindex, res.ctypes.data,
+                                           fl.ctypes.data), "is_test_inverse")
+        return res.reshape(n, h, w), fl
+
+    def test_predict(self, plane, params):
+        plane = np.ascontiguousarray(plane, np.uint8)
+        params = np.ascontiguousarray(params, np.int32)
+        n = params.shape[0]
+        out = np.zeros((n, 4096), np.uint8)
+        self._check(self.L.is_test_predict(self.h, n, plane.ctypes.data, plane.shape[1], plane.shape[0],
+                                           params.ctypes.data, out.ctypes.data), "is_test_predict")
+        return out
+
+    def debug_analysis(self, bsize):
+        n = self.L.is_debug_analysis(self.h, bsize, None, None, None, None)
+        if n < 0:
+            raise RuntimeError("is_debug_analysis failed")
+        J, cand = np.zeros(n, np.int64), np.zeros((n, 4), np.uint8)
+        nc, tx = np.zeros(n, np.uint8), np.zeros(n, np.uint8)
+        self.L.is_debug_analysis(self.h, bsize, J.ctypes.data, cand.ctypes.data, nc.ctypes.data, tx.ctypes.data)
+        return J, cand, nc, tx
+
+    def debug_leaves(self, sb):
+        b, x, y = (np.zeros(256, np.uint8) for _ in range(3))
+        n = self.L.is_debug_leaves(self.h, sb, b.ctypes.data, x.ctypes.data, y.ctypes.data)
+        if n < 0:
+            raise RuntimeError("is_debug_leaves failed")
+        return b[:n].copy(), x[:n].copy(), y[:n].copy()

@@ -1,0 +1,109 @@
+/* include/is_api.h - C ABI of the B200 intra RD search (libisearch.so).
+ *
+ * The drop-in boundary for maddog107/av1gpu's per-superblock intra search.  The reference's boundary is the C++ class
+ * GpEncoder (encoder/src/pipeline.h:191-211): init(const GpConfig&, err) and encode(frames, out records, times, err,
+ * stream).  These entry points replace it with plain pointers and sizes:
+ *   is_create / is_destroy    <- GpEncoder::GpEncoder + GpEncoder::init            (pipeline.h:193-196, pipeline.cpp:221-298)
+ *   is_encode_device          <- GpEncoder::encode, device planes in              (pipeline.h:197-199, pipeline.cpp:323-1180)
+ *   is_encode_host            <- the same, host planes in (upload inside)          (av1gpu.cpp:690-843 upload + encode)
+ *   is_record_counts / _copy  <- GpFrameOut::record() + the record download       (pipeline.h:165-178, pipeline.cpp:829-1010)
+ *   is_record_device          <- GpDevRecords (records stay on the GPU)            (pipeline.h:197-199 `dev`)
+ * The output is av1core's DecisionRecord (av1core/include/av1g/decisions.h): blocks in decode order, the tx-block
+ * layout of av1g_layout(), quantised levels, plus the exact reconstruction, so av1g_encode() of the record reproduces
+ * the reconstruction sample for sample.
+ *
+ * Plain form only: the reference GpConfig defaults without the speed switches (all 19 shapes, all partitions,
+ * K 4 / Krecheck 2, tx-type search open and closed loop, angle deltas, CfL, uvK 2; edge filter, filter intra,
+ * palette, QM, delta-q off; minimum legal tiling; tx_mode_select 0).  8-bit 4:2:0.
+ *
+ * Status codes: IS_OK or a negative IS_ERR_*; is_last_error() returns the message of the last failure of a handle.
+ * A handle serves one host thread at a time (several handles may run concurrently on different streams).
+ */
+#ifndef IS_API_H
+#define IS_API_H
+#include <stddef.h>
+#include <stdint.h>
+#include "av1g/decisions.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IS_OK 0
+#define IS_ERR_INVALID -1   /* bad argument (size, qindex, bit depth, format) */
+#define IS_ERR_CUDA -2      /* a CUDA call failed (message in is_last_error) */
+#define IS_ERR_OOM -3       /* device allocation failed */
+#define IS_ERR_TIMEOUT -4   /* a wavefront dependency wait of the closed loop ran out of its budget (no hang) */
+#define IS_ERR_STATE -5     /* no encode result to read */
+
+typedef struct is_params {
+    int32_t bit_depth;      /* 8 */
+    int32_t chroma_444;     /* 0 (4:2:0) */
+    int32_t device;         /* CUDA device ordinal */
+    int32_t reserved[5];    /* 0 */
+} is_params;
+
+typedef struct is_handle is_handle;
+
+/* One image.  planes: Y, U, V of width x height (chroma ((width+1)/2) x ((height+1)/2)), pitch in samples.
+ * is_encode_device: device pointers; is_encode_host: host pointers (pinned memory gives the fastest upload). */
+typedef struct is_frame {
+    int32_t width, height;
+    int32_t qindex;         /* base_q_idx 1..255 */
+    int32_t pad;
+    const void *planes[3];
+    int32_t pitch[3];
+    int32_t pad2;
+} is_frame;
+
+/* Stage times of the last encode (ms, CUDA events on the handle's stream), cf. the reference's GpTimes
+ * (pipeline.h:180-189). */
+typedef struct is_times {
+    float upload, analysis, dp, recon, pack, total;
+    uint32_t sbs, blocks;
+} is_times;
+
+int is_create(const is_params *p, is_handle **out);
+void is_destroy(is_handle *h);
+const char *is_last_error(const is_handle *h);
+
+/* Run the search on one image; stream: a cudaStream_t (NULL = the handle's own stream).  Returns after the work is
+ * queued and the record sizes are known (one small device->host read). */
+int is_encode_device(is_handle *h, const is_frame *f, void *stream);
+int is_encode_host(is_handle *h, const is_frame *f, void *stream);
+
+int is_record_counts(const is_handle *h, uint32_t *n_blocks, uint32_t *n_txb, uint64_t *n_coeffs);
+/* Copy the last record (frame params, blocks, block_txb[n_blocks + 1], txb, coeffs) and the cropped
+ * reconstruction planes to host memory; any pointer may be NULL. */
+int is_record_copy(is_handle *h, av1g_frame_params *fp, av1g_block *blocks, uint32_t *block_txb, av1g_txb *txb,
+                   int16_t *coeffs, void *recon[3], const int32_t recon_pitch[3]);
+/* Device pointers of the last record (valid until the next encode on the handle). */
+int is_record_device(const is_handle *h, const av1g_block **blocks, const uint32_t **block_txb, const av1g_txb **txb,
+                     const int16_t **coeffs);
+int is_times_get(const is_handle *h, is_times *t);
+
+/* ---- kernel-level entry points for the parity tests (device primitives of av1core's dsp.h API) ---- */
+/* Forward 2-D transform (this project's integer transform) + quantisation + rate of n residual blocks of one tx
+ * size / type, host arrays: res [n][H*W] int32 -> coef [n][tw*th] (fixed point), levels [n][tw*th], D, R, eob per block.
+ * plane 0 luma, 1/2 chroma; ctx = (skipCtx, dcCtx, intraDir). */
+int is_test_fwd_quant(is_handle *h, int n, const int32_t *res, int tx_size, int tx_type, int plane, int qindex,
+                      const int32_t ctx[3], int32_t *coef, int16_t *levels, int64_t *D, int64_t *R, int32_t *eob);
+/* Exact inverse transform (av1g_dequant + av1g_inv_txfm2d semantics) of n level blocks: res [n][H*W], flags [n]. */
+int is_test_inverse(is_handle *h, int n, const int16_t *levels, int tx_size, int tx_type, int qindex, int32_t *res,
+                    uint32_t *flags);
+/* Intra prediction (av1g_build_edges + av1g_predict_intra semantics) of n blocks on an 8-bit plane (host, w x h):
+ * params [n][10] = {x, y, log2W, log2H, haveLeft, haveAbove, haveAR, haveBL, mode, delta}, out [n][64*64]. */
+int is_test_predict(is_handle *h, int n, const uint8_t *plane, int w, int hgt, const int32_t *params, uint8_t *out);
+/* Analysis records of one shape of the last encode: J, cand[4], ncand, tx per block; returns the count or < 0. */
+int is_debug_analysis(is_handle *h, int bsize, int64_t *J, uint8_t *cand, uint8_t *ncand, uint8_t *tx);
+/* Leaves of SB sb of the last encode (bsize, x4, y4); returns the count or < 0. */
+int is_debug_leaves(is_handle *h, uint32_t sb, uint8_t *bsize, uint8_t *x4, uint8_t *y4);
+/* Fixed-point tables as uploaded: cost table of q-context qctx (n entries), averaged bits, lambda of a qindex.  Host
+ * only: h may be NULL (no GPU needed).  Returns the cost-table size. */
+int is_debug_tables(is_handle *h, int qctx, uint16_t *cost, size_t cap, int32_t *avgY13, int32_t *avgPart50,
+                    int32_t *avgSkip0, int qindex, int64_t *lam, int64_t *sqrtlam);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -70,6 +70,9 @@ void orc_predict(const uint8_t *plane, int stride, int x, int y, int log2W, int 
  * 8-bit 4:2:0 only; returns decide seconds and encode seconds. */
 int orc_ref_engine(const orc_image *img, double *sec_decide, double *sec_encode);
 
+/* dc_q / ac_q of a qindex (spec 7.12.2 Dc_Qlookup / Ac_Qlookup). */
+void orc_qstep(int qindex, int bd, int *dcq, int *acq);
+
 /* orc_av1g_recon of a record given as arrays; the frame parameters are the plain form's for that picture. */
 int orc_av1g_recon_arrays(int width, int height, int qindex, int bd, int chroma_444, uint32_t n_blocks, av1g_block *blocks,
                           uint32_t *block_txb, uint32_t n_txb, av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs,

@@ -53,6 +53,7 @@ def lib():
         L.orc_avg_bits.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_lambda.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.orc_predict.argtypes = [C.c_void_p] + [C.c_int] * 13 + [C.c_void_p]
+        L.orc_qstep.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_ref_engine.argtypes = [C.POINTER(OrcImage), C.POINTER(C.c_double), C.POINTER(C.c_double)]
         _lib = L
     return _lib
@@ -197,3 +198,10 @@ def ref_engine_seconds(planes, qindex):
     if rc != 0:
         raise RuntimeError("ref_engine_encode failed: %d" % rc)
     return d.value, e.value
+
+
+def qstep(qindex, bit_depth=8):
+    """(dc_q, ac_q) of a qindex (av1core's spec tables)."""
+    d, a = C.c_int(), C.c_int()
+    lib().orc_qstep(qindex, bit_depth, C.byref(d), C.byref(a))
+    return d.value, a.value

@@ -1579,3 +1579,8 @@ extern "C" int orc_av1g_recon_arrays(int width, int height, int qindex, int bd, 
     rec.coeffs = coeffs;
     return orc_av1g_recon(&rec, recon, err, errlen, obu_bytes);
 }
+
+extern "C" void orc_qstep(int qindex, int bd, int *dcq, int *acq) {
+    *dcq = av1g_dc_q_bd(qindex, bd);
+    *acq = av1g_ac_q_bd(qindex, bd);
+}
