@@ -165,9 +165,9 @@ __global__ void k_pad(Px *plane, int pitch, int vw, int vh, int pw, int ph) {
     if (y < vh) {
         const Px v = plane[(size_t)y * pitch + vw - 1];
         for (int x = vw + threadIdx.x; x < pw; x += blockDim.x) plane[(size_t)y * pitch + x] = v;
-    } else if (y < ph) {
+    } else if (y < ph) {   // below the picture: the last visible row, itself extended by its last sample
         const Px *s = plane + (size_t)(vh - 1) * pitch;
-        for (int x = threadIdx.x; x < pw; x += blockDim.x) plane[(size_t)y * pitch + x] = s[x];
+        for (int x = threadIdx.x; x < pw; x += blockDim.x) plane[(size_t)y * pitch + x] = s[min(x, vw - 1)];
     }
 }
 

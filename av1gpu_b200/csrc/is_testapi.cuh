@@ -190,3 +190,56 @@ int is_debug_tables(is_handle *h, int qctx, uint16_t *cost, size_t cap, int32_t 
 }
 
 }  // extern "C"
+
+// ---- INT32 issue-rate probe (the roofline denominator of this integer path) ----
+// Every thread runs 8 independent chains of x = x * K + (y ^ C) (IMAD + LOP3: 2 INT32 instructions per link), the
+// shape of the search's arithmetic (multiply-adds, xors / selects); ops = 2 x 8 x iterations x threads.
+namespace {
+__global__ void __launch_bounds__(256) k_int32_probe(int iters, uint32_t *sink) {
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = threadIdx.x * (k + 1) + blockIdx.x;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int r = 0; r < 16; r++)
+#pragma unroll
+            for (int k = 0; k < 8; k++) v[k] = v[k] * 0x01000193u + (v[(k + 1) & 7] ^ 0x5bd1e995u);
+    }
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s ^= v[k];
+    if (s == 0x12345678u) sink[blockIdx.x] = s;   // keeps the chains alive
+}
+}  // namespace
+
+extern "C" int is_probe_int32(int device, double *gops, float *ms) {
+    if (cudaSetDevice(device) != cudaSuccess) return IS_ERR_CUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return IS_ERR_CUDA;
+    uint32_t *sink = nullptr;
+    if (cudaMalloc(&sink, 1 << 16) != cudaSuccess) return IS_ERR_OOM;
+    const int blocks = prop.multiProcessorCount * 8, iters = 512;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    k_int32_probe<<<blocks, 256>>>(iters, sink);   // warm-up (clocks, module load)
+    float best = 1e30f;
+    for (int rep = 0; rep < 5; rep++) {
+        cudaEventRecord(a);
+        k_int32_probe<<<blocks, 256>>>(iters, sink);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float t = 0;
+        cudaEventElapsedTime(&t, a, b);
+        best = t < best ? t : best;
+    }
+    const cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (e != cudaSuccess) return IS_ERR_CUDA;
+    const double ops = 2.0 * 8 * 16 * (double)iters * blocks * 256;
+    *gops = ops / (best * 1e-3) / 1e9;
+    *ms = best;
+    return IS_OK;
+}

@@ -44,7 +44,7 @@ class IsTimes(C.Structure):
 # every entry point declared in include/is_api.h
 EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_encode_host", "is_record_counts",
            "is_record_copy", "is_record_device", "is_times_get", "is_test_fwd_quant", "is_test_inverse",
-           "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables"]
+           "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32"]
 
 _lib = None
 
@@ -76,8 +76,18 @@ def load_library():
     L.is_debug_leaves.argtypes = [vp, C.c_uint32, vp, vp, vp]
     L.is_debug_tables.argtypes = [vp, C.c_int, vp, C.c_size_t, vp, vp, vp, C.c_int, C.POINTER(C.c_int64),
                                   C.POINTER(C.c_int64)]
+    L.is_probe_int32.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]
     _lib = L
     return L
+
+
+def probe_int32(device=0):
+    """Measured INT32 instruction throughput (Gop/s) and the probe kernel's time (ms)."""
+    g, ms = C.c_double(), C.c_float()
+    rc = load_library().is_probe_int32(device, C.byref(g), C.byref(ms))
+    if rc != 0:
+        raise RuntimeError("is_probe_int32 failed (%d)" % rc)
+    return g.value, ms.value
 
 
 def host_tables(qctx, qindex=120):

@@ -41,7 +41,6 @@ def _plane(rng, w, h, centre, spread, edges, cell=48):
         ph = rng.uniform(0, 2 * np.pi)
         out = out + a * np.sin(2 * np.pi * (xx * np.cos(th) + yy * np.sin(th)) / per + ph)
     if edges:            # oriented step edges, 2-40 per 256x256 area, each over a disc of radius 24-96
-        scale = 256.0 * (w / max(w, 1))
         for ay in range(0, h, 256):
             for ax in range(0, w, 256):
                 n = int(rng.integers(2, 41))
@@ -57,7 +56,6 @@ def _plane(rng, w, h, centre, spread, edges, cell=48):
                     px, py = xx[y0:y1, x0:x1] - ex, yy[y0:y1, x0:x1] - ey
                     m = (px * px + py * py < r * r) & (px * np.cos(th) + py * np.sin(th) > 0)
                     out[y0:y1, x0:x1] += amp * m
-    del scale
     return out
 
 

@@ -70,6 +70,10 @@ void orc_predict(const uint8_t *plane, int stride, int x, int y, int log2W, int 
  * 8-bit 4:2:0 only; returns decide seconds and encode seconds. */
 int orc_ref_engine(const orc_image *img, double *sec_decide, double *sec_encode);
 
+/* Algorithmic INT32 operations of the last search (the roofline numerator, cost model in plain_search.cpp):
+ * open-loop analysis and closed loop. */
+void orc_op_counts(const orc_result *r, uint64_t *analysis, uint64_t *closed);
+
 /* dc_q / ac_q of a qindex (spec 7.12.2 Dc_Qlookup / Ac_Qlookup). */
 void orc_qstep(int qindex, int bd, int *dcq, int *acq);
 

@@ -53,6 +53,7 @@ def lib():
         L.orc_avg_bits.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_lambda.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.orc_predict.argtypes = [C.c_void_p] + [C.c_int] * 13 + [C.c_void_p]
+        L.orc_op_counts.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.orc_qstep.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_ref_engine.argtypes = [C.POINTER(OrcImage), C.POINTER(C.c_double), C.POINTER(C.c_double)]
         _lib = L
@@ -110,6 +111,12 @@ class Result:
         b, x, y = (np.zeros(256, np.uint8) for _ in range(3))
         n = L.orc_leaves(self.h, sb, b.ctypes.data, x.ctypes.data, y.ctypes.data)
         return b[:n].copy(), x[:n].copy(), y[:n].copy()
+
+    def op_counts(self):
+        """Algorithmic INT32 operations of this search: (open-loop analysis, closed loop)."""
+        a, c = C.c_uint64(), C.c_uint64()
+        lib().orc_op_counts(self.h, C.byref(a), C.byref(c))
+        return a.value, c.value
 
     def __del__(self):
         try:

@@ -515,6 +515,52 @@ static void quant_rate(const int32_t *coef, const EvalIn &e, int16_t *q, EvalOut
 
 
 
+
+// ---------------------------------------------------------------------------------------------------------------
+// algorithmic INT32 operation count (the roofline numerator): every unit of work the search does is counted, each with
+// the integer operations (add / sub / mul / shift / min / max / abs / compare / select / table read) its definition
+// takes, counted from this file's code: a residual sample = its prediction + 1; a 4x4 Hadamard = 111; a forward
+// butterfly rotation = 10, an H step = 2, the ADST4 matrix = 36, an identity element = 2, plus 1 pre-shift and 2 for
+// the rounding of every input / output; quantisation 18 per coefficient, the eob scan 2; the rate 40 per coefficient up
+// to the eob (+25 when level > 2) and 60 per block; the inverse as the forward plus 6 per coefficient of dequantisation
+// and 3 per sample of reconstruction.  ops[0]: open-loop analysis, ops[1]: closed loop.
+// ---------------------------------------------------------------------------------------------------------------
+struct OpCounter { std::atomic<uint64_t> ops[2]; };
+static int pred_ops(int mode, int delta) {
+    if (mode == AV1G_DC_PRED) return 1;
+    if (mode == AV1G_PAETH_PRED) return 12;
+    if (mode == AV1G_SMOOTH_PRED) return 12;
+    if (mode == AV1G_SMOOTH_V_PRED || mode == AV1G_SMOOTH_H_PRED) return 7;
+    const int pa = AV1G_T(Mode_To_Angle)[mode] + delta * AV1G_ANGLE_STEP;
+    return (pa == 90 || pa == 180) ? 1 : 9;
+}
+static int fwd1d_ops(int kind, int n) {
+    static int cache[3][7];
+    static std::once_flag once;
+    std::call_once(once, [] {
+        for (int k = 0; k < 3; k++) for (int l = 2; l <= 6; l++) {
+            int c = 0;
+            if (k == AV1G_K_IDT) c = 2 * (1 << l);
+            else if (k == AV1G_K_ADST && l == 2) c = 36;
+            else if (k == AV1G_K_DCT || (k == AV1G_K_ADST && l <= 4)) {
+                const OpList L = k == AV1G_K_DCT ? idct_list(l) : iadst_list(l);
+                for (const Op &o : L.ops) c += o.t == 'B' ? 10 : o.t == 'H' ? 2 : 0;
+            }
+            cache[k][l] = c + 3 * (1 << l);
+        }
+    });
+    return cache[kind][n];
+}
+static uint64_t fwd2d_ops(int txSz, int txType) {
+    const int lw = AV1G_T(Tx_Width_Log2)[txSz], lh = AV1G_T(Tx_Height_Log2)[txSz];
+    const int W = 1 << lw, H = 1 << lh, th = std::min(H, 32), tw = std::min(W, 32);
+    return (uint64_t)W * fwd1d_ops(av1g_col_kind(txType), lh) + (uint64_t)th * fwd1d_ops(av1g_row_kind(txType), lw) + 3ull * tw * th;
+}
+static uint64_t eval_ops(int txSz, int txType, int eob, int nBig, int mode, int delta) {
+    const int W = AV1G_T(Tx_Width)[txSz], H = AV1G_T(Tx_Height)[txSz], n = std::min(W, 32) * std::min(H, 32);
+    return (uint64_t)W * H * (pred_ops(mode, delta) + 1) + fwd2d_ops(txSz, txType) + 20ull * n + 40ull * eob + 25ull * nBig + 60;
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // the search engine of one image
 // ---------------------------------------------------------------------------------------------------------------
@@ -580,6 +626,7 @@ struct Engine {
     std::vector<std::vector<Leaf>> leaves;
     std::vector<uint8_t> mYMode, cLvl[3], cDc[3];
     std::vector<SbOut> sbo;
+    OpCounter *ops = nullptr;
 
     TileBox tile_of(int x, int y) const {
         int c = 0, r = 0;
@@ -633,14 +680,22 @@ struct Engine {
     }
 
     // ---- one evaluation: residual -> forward transform -> quantise / rate / distortion ----
-    EvalOut eval(const int32_t *res, int txSz, int txType, int plane, int skipCtx, int dcCtx, int intraDir, i64 resE, int16_t *q) const {
+    EvalOut eval(const int32_t *res, int txSz, int txType, int plane, int skipCtx, int dcCtx, int intraDir, i64 resE, int16_t *q,
+                 int stage = -1, int mode = 0, int delta = 0) const {
         int32_t coef[1024];
         fwd2d(res, txSz, txType, BD, coef);
         EvalIn e{txSz, txType, plane, BD, dcQ[plane], acQ[plane], skipCtx, dcCtx, intraDir, C, resE};
         EvalOut o;
         quant_rate(coef, e, q, o);
+        if (ops && stage >= 0) {
+            const uint16_t *scan = av1g_get_scan(txSz, txType);
+            int big = 0;
+            for (int c = 0; c < o.eob; c++) big += std::abs((int)q[scan[c]]) > 2;
+            ops->ops[stage].fetch_add(eval_ops(txSz, txType, o.eob, big, mode, delta), std::memory_order_relaxed);
+        }
         return o;
     }
+    void count(int stage, uint64_t n) const { if (ops) ops->ops[stage].fetch_add(n, std::memory_order_relaxed); }
 
     // ---- open-loop analysis of one block (k_analysis.cuh:496-689) ----
     void analyse(int bs, int bx, int by) {
@@ -685,6 +740,7 @@ struct Engine {
                         satd += hadamard4_sum(d);
                     }
                 js[ci] = (satd << 14) + sqlam * mbits(cands[ci]);
+                count(0, (uint64_t)(w * h / 16) * (16 * (uint64_t)pred_ops(cand_mode(cands[ci]), cand_delta(cands[ci])) + 111) + 30);
             }
         };
         screen(0, 13);
@@ -734,7 +790,7 @@ struct Engine {
                     }
                 resK = k;
             }
-            const EvalOut o = eval(res.data(), txSz, t, 0, 0, 0, cand_mode(c), resE, q);
+            const EvalOut o = eval(res.data(), txSz, t, 0, 0, 0, cand_mode(c), resE, q, 0, cand_mode(c), cand_delta(c));
             const i64 J = o.D + lam * (o.R + mbits(c) + overhead);
             if (J < bestJ) {
                 bestJ = J;
@@ -924,6 +980,7 @@ struct Engine {
             for (int i = 0; i < n; i++) q[i] = (int16_t)(q[i] / 2);
         }
         av1g_add_residual<BD>(dst, pitch, res.data(), txSz, txType);
+        count(1, fwd2d_ops(txSz, txType) + 6ull * n + 3ull * W * H + (uint64_t)W * H * 4);
     }
 
     // record a finished tx block: eob, context maps, BlockDecoded, the txb entry (k_recon.cuh:686-730)
@@ -1064,7 +1121,7 @@ struct Engine {
         auto run = [&](const std::vector<Task> &ts) {
             for (const Task &tk : ts) {
                 const i64 e = residual(tk.c);
-                const EvalOut o = eval(res.data(), txSz, tk.t, 0, skipCtx, dcCtx, cand_mode(tk.c), e, q);
+                const EvalOut o = eval(res.data(), txSz, tk.t, 0, skipCtx, dcCtx, cand_mode(tk.c), e, q, 1, cand_mode(tk.c), cand_delta(tk.c));
                 const i64 J = o.D + lam * (o.R + mbits(tk.c));
                 if (J < bestJ) {
                     bestJ = J; bestC = tk.c; bestT = tk.t; have = true;
@@ -1090,7 +1147,7 @@ struct Engine {
         }
         if (!have) {   // a single candidate, DCT only: its levels
             const i64 e = residual(bestC);
-            eval(res.data(), txSz, bestT, 0, skipCtx, dcCtx, cand_mode(bestC), e, bestQ);
+            eval(res.data(), txSz, bestT, 0, skipCtx, dcCtx, cand_mode(bestC), e, bestQ, 1, cand_mode(bestC), cand_delta(bestC));
         }
         // final: prediction + exact inverse into the reconstruction, record
         Px *dst = rec[0].data() + (size_t)y * pw[0] + x;
@@ -1162,6 +1219,7 @@ struct Engine {
                     sum += v;
                 }
             cflAvg = (int)((sum + ((i64)1 << (lw + lh - 1))) >> (lw + lh));
+            count(1, (uint64_t)npx * (8 + 8 + 2 * 3 * 9));
             i64 den = 0, num[3] = {0, 0, 0};
             for (int i = 0; i < Ht; i++)
                 for (int j = 0; j < Wt; j++) {
@@ -1213,6 +1271,7 @@ struct Engine {
                         }
                 }
                 satd[ci] = t << 14;
+                count(1, 2 * (uint64_t)(npx / 16) * (16 * (uint64_t)pred_ops(cand_mode(uvc[ci]), cand_delta(uvc[ci])) + 111) + 30);
             }
         };
         screen(0, 13);
@@ -1272,7 +1331,8 @@ struct Engine {
             int16_t qq[3][1024];
             for (int pl = 1; pl <= 2; pl++) {
                 residual(pl, c);
-                const EvalOut o = eval(res.data(), txSz, txType, pl, skipCtx[pl], dcCtx[pl], 0, 0, q);
+                const EvalOut o = eval(res.data(), txSz, txType, pl, skipCtx[pl], dcCtx[pl], 0, 0, q, 1, c == 255 ? AV1G_SMOOTH_V_PRED : cand_mode(c),
+                                       c == 255 ? 0 : cand_delta(c));
                 J += o.D + lam * o.R;
                 memcpy(qq[pl], q, sizeof q);
             }
@@ -1376,14 +1436,21 @@ struct orc_result {
     std::vector<uint8_t> recon[3];   // cropped, bytes (8-bit) or uint16 pairs
     std::vector<orc::BlockRes> blk[22];
     std::vector<std::vector<orc::Leaf>> leaves;
+    uint64_t ops[2] = {0, 0};
 };
 
 template <int BD>
 static int encode_bd(const orc_image *img, int threads, orc_result *R) {
     typedef av1g_pixel_t(BD) Px;
     std::unique_ptr<orc::Engine<BD>> E(new orc::Engine<BD>());
+    orc::OpCounter cnt;
+    cnt.ops[0] = 0;
+    cnt.ops[1] = 0;
+    E->ops = &cnt;
     E->setup(*img);
     E->run(threads);
+    R->ops[0] = cnt.ops[0].load();
+    R->ops[1] = cnt.ops[1].load();
     memset(&R->fp, 0, sizeof R->fp);
     R->fp.version = AV1G_DECISIONS_VERSION;
     R->fp.width = (uint32_t)img->width;
@@ -1583,4 +1650,9 @@ extern "C" int orc_av1g_recon_arrays(int width, int height, int qindex, int bd, 
 extern "C" void orc_qstep(int qindex, int bd, int *dcq, int *acq) {
     *dcq = av1g_dc_q_bd(qindex, bd);
     *acq = av1g_ac_q_bd(qindex, bd);
+}
+
+extern "C" void orc_op_counts(const orc_result *r, uint64_t *analysis, uint64_t *closed) {
+    *analysis = r->ops[0];
+    *closed = r->ops[1];
 }
