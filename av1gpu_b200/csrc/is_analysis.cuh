@@ -15,20 +15,27 @@
 
 namespace is {
 
-constexpr int AN_WARPS = 12;
-constexpr int AN_TASKS = 849;                 // blocks of all 19 shapes in one SB
-__constant__ uint8_t c_anTask[AN_TASKS][3];   // (bsize, x4, y4) sorted by area descending, then shape, then raster
+// Two kernels share the block search: k_analysis for the 836 blocks of the shapes up to 32 samples a side (12 warps,
+// 2 CTAs per SM), k_analysis_big for the 13 blocks with a 64-sample side (4 warps with the larger scratch).
+constexpr int AN_WARPS = 12, ANB_WARPS = 4;
+constexpr int AN_TASKS = 836, ANB_TASKS = 13;
+constexpr int AN_BUF_INTS = 1088;             // evaluation scratch per warp: 32 / G tasks of H x (W + 1) int32 (<= 32x32)
+constexpr int ANB_BUF_INTS = 64 * 65;
+__constant__ uint8_t c_anTask[AN_TASKS][3];   // (bsize, x4, y4) largest area first, then shape, then raster
+__constant__ uint8_t c_anTaskBig[ANB_TASKS][3];
 
-template <typename Px> struct AnSmem {
+template <typename Px, int BUFI> struct AnWarp {
+    int32_t buf[BUFI];
+    int16_t q[1024];
+    i64 taskJ[8];
+    Px ea[EDGE_LEN], el[EDGE_LEN];
+    int satd[32];
+    int cand[32];
+};
+template <typename Px, int NW, int BUFI> struct AnSmem {
     static constexpr int TW = 144, TH = 65;   // tile: columns sbx-16 .. sbx+127, rows sby-1 .. sby+63
     Px tile[TH * TW];
-    struct Warp {
-        int16_t res[64 * 64];                 // residual of an evaluation (its levels reuse the same bytes)
-        int32_t tmp[32 * 65];
-        Px ea[EDGE_LEN], el[EDGE_LEN];
-        int satd[32];
-        int cand[32];
-    } w[AN_WARPS];
+    AnWarp<Px, BUFI> w[NW];
     int next;
 };
 
@@ -49,10 +56,10 @@ __device__ __forceinline__ bool ol_decoded(int px, int py, int x, int y, int tx0
     return zorder16(((px - sbx) >> 2) & 15, ((py - sby) >> 2) & 15) < zorder16(((x - sbx) >> 2) & 15, ((y - sby) >> 2) & 15);
 }
 
-template <int BD, typename Px>
-__device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, typename AnSmem<Px>::Warp &S, int bs, int x, int y, int sbx,
-                                      int sby, int tx0, int ty0, int tx1, int ty1) {
-    constexpr int TW = AnSmem<Px>::TW;
+template <int BD, typename Px, int BUFI>
+__device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp<Px, BUFI> &S, int bs, int x, int y, int sbx, int sby,
+                                      int tx0, int ty0, int tx1, int ty1) {
+    constexpr int TW = 144;
     const int lane = lane_id();
     const int txSz = AV1G_T(Max_Tx_Size_Rect)[bs];
     const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
@@ -124,23 +131,43 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, typena
         if (top[k] >= 0) nK = k + 1;
         if (lane == top[k]) js = INF;
     }
-    // ---- RD of the top-K with DCT_DCT, then the tx types of the winner ----
+    // ---- RD: the top-K with DCT_DCT, then the other types of the set for the winner; 32 / G tasks at a time, the
+    //      costs compared afterwards in evaluation order (strict <: the first of equal costs wins, as a serial loop) ----
     const int set = tx_set_intra(txSz);
     const bool hasC = has_chroma(bs, y >> 2, x >> 2, F.ssx);
     const int overhead = (hasC ? UV_OVERHEAD : 0) + c_avgSkip0;
+    const int G = grp_size(txSz), ng = 32 / G, grp = lane / G, g = lane & (G - 1);
+    const int bufInts = task_buf_ints(txSz), nq = min(W, 32) * min(H, 32);
+    int32_t *tb = S.buf + grp * bufInts;
+    int16_t *tq = S.q + grp * nq;
     i64 bestJ = INF;
     int bestK = 0, bestTx = AV1G_DCT_DCT;
-    const int nSteps = nK + (set != AV1G_TX_SET_DCTONLY ? 15 : 0);
-    for (int st = 0; st < nSteps; st++) {
-        const int k = st < nK ? st : bestK, t = st < nK ? AV1G_DCT_DCT : st - nK + 1;
-        if (t != AV1G_DCT_DCT && !tx_in_set(set, t)) continue;
+    // stage 1: candidates top[0 .. nK) with DCT_DCT
+    for (int r0 = 0; r0 < nK; r0 += ng) {
+        const int k = min(r0 + grp, nK - 1);   // groups past the end repeat the last task (their results are unused)
         const int c = S.cand[top[k]], m = cand_mode(c);
-        const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, C};
-        const EvalOut o = rc_eval<BD, Px>(txSz, res_mode<Px>(src, TW, A, L, m, cand_delta(c), lw, lh, dcv), e, S.res, S.tmp, S.res);
-        const i64 J = o.D + F.lam * (o.R + mbits(c) + overhead);
-        if (J < bestJ) {
-            bestJ = J;
-            if (st < nK) bestK = k; else bestTx = t;
+        const EvalIn e{AV1G_DCT_DCT, 0, 0, 0, m, F.dcQ, F.acQ, C};
+        const EvalOut o = grp_eval<BD, Px>(txSz, res_mode<Px>(src, TW, A, L, m, cand_delta(c), lw, lh, dcv), e, tb, tq, g, G);
+        if (g == 0 && r0 + grp < nK) S.taskJ[grp] = o.D + F.lam * (o.R + mbits(c) + overhead);
+        __syncwarp();
+        for (int t = 0; t < ng && r0 + t < nK; t++)
+            if (S.taskJ[t] < bestJ) { bestJ = S.taskJ[t]; bestK = r0 + t; }
+        __syncwarp();
+    }
+    // stage 2: the other tx types of the set for the winner
+    if (set != AV1G_TX_SET_DCTONLY) {
+        int types[8], nt = 0;
+        for (int t = 1; t < 16; t++) if (tx_in_set(set, t)) types[nt++] = t;
+        const int c = S.cand[top[bestK]], m = cand_mode(c);
+        for (int r0 = 0; r0 < nt; r0 += ng) {
+            const int tt = types[min(r0 + grp, nt - 1)];
+            const EvalIn e{tt, 0, 0, 0, m, F.dcQ, F.acQ, C};
+            const EvalOut o = grp_eval<BD, Px>(txSz, res_mode<Px>(src, TW, A, L, m, cand_delta(c), lw, lh, dcv), e, tb, tq, g, G);
+            if (g == 0 && r0 + grp < nt) S.taskJ[grp] = o.D + F.lam * (o.R + mbits(c) + overhead);
+            __syncwarp();
+            for (int t = 0; t < ng && r0 + t < nt; t++)
+                if (S.taskJ[t] < bestJ) { bestJ = S.taskJ[t]; bestTx = types[r0 + t]; }
+            __syncwarp();
         }
     }
     if (lane == 0) {
@@ -158,42 +185,51 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, typena
     __syncwarp();
 }
 
-template <int BD>
-__global__ void __launch_bounds__(AN_WARPS * 32, 1) k_analysis(const FrameDesc *__restrict__ Fp) {
+// one CTA per SB: stage the tile, then the warps take the blocks of the task list
+template <int BD, int NW, int BUFI, bool BIG>
+__device__ __forceinline__ void an_sb(const FrameDesc &F, unsigned char *smem_raw) {
     typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    AnSmem<Px> &S = *reinterpret_cast<AnSmem<Px> *>(smem_raw);
-    const FrameDesc &F = *Fp;
+    typedef AnSmem<Px, NW, BUFI> Sm;
+    Sm &S = *reinterpret_cast<Sm *>(smem_raw);
     const int sb = blockIdx.x, sbr = sb / F.sbCols, sbc = sb % F.sbCols;
     const int sbx = sbc * 64, sby = sbr * 64;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    // stage the SB tile with 128-bit loads (rows and the tile's first column are 16-byte aligned by the layout)
-    {
-        constexpr int V = AnSmem<Px>::TW * (int)sizeof(Px) / 16;   // uint4 per tile row
+    {   // the SB tile with 128-bit loads (rows and the tile's first column are 16-byte aligned by the layout)
+        constexpr int V = Sm::TW * (int)sizeof(Px) / 16;
         const Px *s0 = (const Px *)F.src[0] + (size_t)(sby - 1) * F.spitch[0] + (sbx - 16);
-        for (int k = tid; k < AnSmem<Px>::TH * V; k += AN_WARPS * 32) {
+        for (int k = tid; k < Sm::TH * V; k += NW * 32) {
             const int r = k / V, c = k % V;
-            reinterpret_cast<uint4 *>(S.tile + r * AnSmem<Px>::TW)[c] = __ldg(reinterpret_cast<const uint4 *>(s0 + (size_t)r * F.spitch[0]) + c);
+            reinterpret_cast<uint4 *>(S.tile + r * Sm::TW)[c] = __ldg(reinterpret_cast<const uint4 *>(s0 + (size_t)r * F.spitch[0]) + c);
         }
-        if (tid == 0) S.next = AN_WARPS;
+        if (tid == 0) S.next = NW;
     }
     __syncthreads();
-    // the tile containing this SB (pixels)
     int tc = 0, tr = 0;
     while (tc + 1 < F.tileCols && sbx >= F.tileColStart[tc + 1] * 4) tc++;
     while (tr + 1 < F.tileRows && sby >= F.tileRowStart[tr + 1] * 4) tr++;
     const int tx0 = F.tileColStart[tc] * 4, tx1 = F.tileColStart[tc + 1] * 4, ty0 = F.tileRowStart[tr] * 4, ty1 = F.tileRowStart[tr + 1] * 4;
     const int FW = F.MiCols * 4, FH = F.MiRows * 4;
+    constexpr int NT = BIG ? ANB_TASKS : AN_TASKS;
     int t = warp;
-    while (t < AN_TASKS) {
-        const int bs = c_anTask[t][0], x = sbx + c_anTask[t][1] * 4, y = sby + c_anTask[t][2] * 4;
-        if (x < FW && y < FH) {
-            an_block<BD, Px>(F, S.tile, S.w[warp], bs, x, y, sbx, sby, tx0, ty0, tx1, ty1);
-        }
+    while (t < NT) {
+        const uint8_t *tk = BIG ? c_anTaskBig[t] : c_anTask[t];
+        const int bs = tk[0], x = sbx + tk[1] * 4, y = sby + tk[2] * 4;
+        if (x < FW && y < FH) an_block<BD, Px, BUFI>(F, S.tile, S.w[warp], bs, x, y, sbx, sby, tx0, ty0, tx1, ty1);
         int n = 0;
         if (lane == 0) n = atomicAdd(&S.next, 1);
         t = __shfl_sync(0xffffffffu, n, 0);
     }
+}
+
+template <int BD>
+__global__ void __launch_bounds__(AN_WARPS * 32, 2) k_analysis(const FrameDesc *__restrict__ Fp) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    an_sb<BD, AN_WARPS, AN_BUF_INTS, false>(*Fp, smem_raw);
+}
+template <int BD>
+__global__ void __launch_bounds__(ANB_WARPS * 32, 2) k_analysis_big(const FrameDesc *__restrict__ Fp) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    an_sb<BD, ANB_WARPS, ANB_BUF_INTS, true>(*Fp, smem_raw);
 }
 
 }  // namespace is

@@ -142,10 +142,14 @@ void min_tiles(int W, int H, std::vector<int> &cs, std::vector<int> &rs) {
     }
 }
 
-// analysis task list of one SB: (bsize, x4, y4) for every shape, largest area first
-std::vector<uint8_t> an_tasks() {
+// analysis task lists of one SB: (bsize, x4, y4) for every shape, largest area first; big = shapes with a 64 side
+std::vector<uint8_t> an_tasks(bool big) {
     std::vector<int> shapes;
-    for (int s = 0; s < AV1G_BLOCK_INVALID; s++) if (!(s >= 13 && s <= 15)) shapes.push_back(s);
+    for (int s = 0; s < AV1G_BLOCK_INVALID; s++) {
+        if (s >= 13 && s <= 15) continue;
+        const bool b = AV1G_T(Num_4x4_Blocks_Wide)[s] == 16 || AV1G_T(Num_4x4_Blocks_High)[s] == 16;
+        if (b == big) shapes.push_back(s);
+    }
     std::stable_sort(shapes.begin(), shapes.end(), [](int a, int b) {
         return AV1G_T(Num_4x4_Blocks_Wide)[a] * AV1G_T(Num_4x4_Blocks_High)[a] > AV1G_T(Num_4x4_Blocks_Wide)[b] * AV1G_T(Num_4x4_Blocks_High)[b];
     });
@@ -189,7 +193,7 @@ struct is_handle {
     FrameDesc *hFpinned = nullptr;
     int nSb = 0;
     int geomW = -1, geomH = -1;
-    size_t smemAn = 0, smemRc = 0;
+    size_t smemAn = 0, smemAnBig = 0, smemRc = 0;
     // last result
     bool have = false;
     uint32_t nBlocks = 0, nTxb = 0;
@@ -226,29 +230,23 @@ int upload_tables(int dev) {
         const HostTables &T = host_tables();
         std::vector<uint16_t> all((size_t)4 * NCDF);
         for (int q = 0; q < 4; q++) memcpy(all.data() + (size_t)q * NCDF, T.cost[q].data(), NCDF * 2);
-        const std::vector<uint8_t> tasks = an_tasks();
+        const std::vector<uint8_t> tasks = an_tasks(false), tasksBig = an_tasks(true);
         cudaError_t e = cudaMemcpyToSymbol(g_cost, all.data(), all.size() * 2);
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgY, T.avgY, sizeof T.avgY);
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgPart, T.avgPart, sizeof T.avgPart);
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgSkip0, &T.avgSkip0, sizeof T.avgSkip0);
-        if (e == cudaSuccess && tasks.size() == (size_t)AN_TASKS * 3) e = cudaMemcpyToSymbol(c_anTask, tasks.data(), tasks.size());
-        else if (e == cudaSuccess) e = cudaErrorInvalidValue;
+        if (e == cudaSuccess && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3) {
+            e = cudaMemcpyToSymbol(c_anTask, tasks.data(), tasks.size());
+            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anTaskBig, tasksBig.data(), tasksBig.size());
+        } else if (e == cudaSuccess) {
+            e = cudaErrorInvalidValue;
+        }
         g_upload_rc[dev & 63] = e == cudaSuccess ? 0 : (int)e;
     });
     return g_upload_rc[dev & 63];
 }
 
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
-
-// host self-check: the compile-time row shifts agree with the spec table (the forward scale depends on them)
-template <int W, int H> bool rowshift_ok() { return TxDims<W, H>::rowShift == AV1G_T(Transform_Row_Shift)[TxDims<W, H>::size]; }
-bool tables_consistent() {
-    bool ok = true;
-#define IS_CHK(W_, H_) ok = ok && rowshift_ok<W_, H_>()
-    for (int t = 0; t < 19; t++) { IS_TX_SWITCH(t, IS_CHK) }
-#undef IS_CHK
-    return ok;
-}
 
 // lay out the workspace for an image of W x H (8-bit 4:2:0); returns bytes needed, fills F's pointers if base != 0
 size_t layout(int W, int H, uint8_t *base, FrameDesc &F, int &nSb) {
@@ -323,14 +321,15 @@ int is_create(const is_params *p, is_handle **out) {
     h->device = p->device;
     auto fail = [&](int rc) { is_destroy(h); *out = nullptr; return rc; };
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(IS_ERR_CUDA);
-    if (!tables_consistent()) return fail(IS_ERR_INVALID);
     if (upload_tables(h->device)) return fail(IS_ERR_CUDA);
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) return fail(IS_ERR_CUDA);
     h->nSm = prop.multiProcessorCount;
-    h->smemAn = sizeof(AnSmem<uint8_t>);
+    h->smemAn = sizeof(AnSmem<uint8_t, AN_WARPS, AN_BUF_INTS>);
+    h->smemAnBig = sizeof(AnSmem<uint8_t, ANB_WARPS, ANB_BUF_INTS>);
     h->smemRc = sizeof(RcSmem<uint8_t>);
     if (cudaFuncSetAttribute(k_analysis<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemAn) != cudaSuccess) return fail(IS_ERR_CUDA);
+    if (cudaFuncSetAttribute(k_analysis_big<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemAnBig) != cudaSuccess) return fail(IS_ERR_CUDA);
     if (cudaFuncSetAttribute(k_recon<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemRc) != cudaSuccess) return fail(IS_ERR_CUDA);
     int per = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_recon<8>, RC_WARPS * 32, h->smemRc) != cudaSuccess || per < 1) return fail(IS_ERR_CUDA);
@@ -436,6 +435,7 @@ static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) 
     IS_CK(cudaMemsetAsync(F.queue, 0, 4, st));
     IS_CK(cudaMemsetAsync(F.err, 0, 4, st));
     IS_CK(cudaEventRecord(h->ev[1], st));
+    k_analysis_big<8><<<nSb, ANB_WARPS * 32, h->smemAnBig, st>>>(h->dF);
     k_analysis<8><<<nSb, AN_WARPS * 32, h->smemAn, st>>>(h->dF);
     IS_CK(cudaGetLastError());
     IS_CK(cudaEventRecord(h->ev[2], st));

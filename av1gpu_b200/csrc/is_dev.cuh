@@ -319,10 +319,13 @@ __device__ __forceinline__ int hadamard4_sum(int *d) {
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// forward 2-D transform (warp): columns on lanes, then rows on lanes, all in registers.  Shifts (the range rule):
-// s0 = 17 - BD - log2 H keeps every column intermediate inside int32 rotations, s1 = log2 W the row inputs,
-// s2 brings the result to the dequantisation domain with FB fractional bits:
-//     DQ = M_H^T R M_W 2^(rowShift + 4) / (H W / 4) / rect   (rect: a further x 5793 / 4096 for 2:1 sizes)
+// 1-D transforms on a strided int32 vector in shared memory.  Each (kind, length) network exists ONCE in the binary
+// (the dispatchers are not inlined): the kernels' instruction footprint stays small enough for the instruction
+// caches, whatever mix of block sizes the warps of an SM are working on.
+//   forward: T = v << pre; the transposed spec network (txfm_gen.cuh); out i < nout: (rect: Round2(T * 5793, 12)),
+//            then Round2(., post) for post > 0 or << -post
+//   inverse: T = v (preRect: Round2(T * 2896, 12)); the spec network with its checks at r bits; out: Round2(., post),
+//            clamped to clampBits when nonzero
 // ---------------------------------------------------------------------------------------------------------------
 template <int N> __device__ __forceinline__ void fwd1d(int kind, int32_t *T) {
     if (N >= 32 || kind == 0) {
@@ -344,26 +347,54 @@ template <int N> __device__ __forceinline__ void fwd1d(int kind, int32_t *T) {
         }
     }
 }
-template <int W, int H> struct TxDims {
-    static constexpr int lw = W == 4 ? 2 : W == 8 ? 3 : W == 16 ? 4 : W == 32 ? 5 : 6;
-    static constexpr int lh = H == 4 ? 2 : H == 8 ? 3 : H == 16 ? 4 : H == 32 ? 5 : 6;
-    static constexpr int tw = W > 32 ? 32 : W, th = H > 32 ? 32 : H, n = tw * th;
-    static constexpr int TS = W + 1;   // coefficient row stride in the scratch (odd: conflict-free row reads)
-    static constexpr bool rect = (lw - lh == 1 || lh - lw == 1);
-    static constexpr int size = W == H ? (W == 4 ? AV1G_TX_4X4 : W == 8 ? AV1G_TX_8X8 : W == 16 ? AV1G_TX_16X16 : W == 32 ? AV1G_TX_32X32 : AV1G_TX_64X64)
-                              : (W == 4 && H == 8) ? AV1G_TX_4X8 : (W == 8 && H == 4) ? AV1G_TX_8X4 : (W == 8 && H == 16) ? AV1G_TX_8X16
-                              : (W == 16 && H == 8) ? AV1G_TX_16X8 : (W == 16 && H == 32) ? AV1G_TX_16X32 : (W == 32 && H == 16) ? AV1G_TX_32X16
-                              : (W == 32 && H == 64) ? AV1G_TX_32X64 : (W == 64 && H == 32) ? AV1G_TX_64X32 : (W == 4 && H == 16) ? AV1G_TX_4X16
-                              : (W == 16 && H == 4) ? AV1G_TX_16X4 : (W == 8 && H == 32) ? AV1G_TX_8X32 : (W == 32 && H == 8) ? AV1G_TX_32X8
-                              : (W == 16 && H == 64) ? AV1G_TX_16X64 : AV1G_TX_64X16;
-    static constexpr int rowShift = (size == AV1G_TX_4X4 || size == AV1G_TX_4X8 || size == AV1G_TX_8X4) ? 0
-                                  : (size == AV1G_TX_16X16 || size == AV1G_TX_32X32 || size == AV1G_TX_64X64 || size == AV1G_TX_8X32 ||
-                                     size == AV1G_TX_32X8 || size == AV1G_TX_16X64 || size == AV1G_TX_64X16) ? 2 : 1;
-    static constexpr int E = rowShift + 4 + FB - (lw + lh - 2);
-    // distortion: pixel SSE = sum (DQ - dequant)^2 2^-(2 FB + k)
-    static constexpr int k = 2 * (rowShift + 4) - (lw + lh - 2) + (rect ? 1 : 0);
-    static constexpr int dsh = 16 - 2 * FB - k;
+template <int N>
+__device__ __forceinline__ void fwd_mem_n(int kind, int32_t *p, int stride, int pre, int nout, int rect, int post) {
+    int32_t T[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) T[i] = p[i * stride] * (1 << pre);
+    fwd1d<N>(kind, T);
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        if (i < nout) {
+            int32_t v = T[i];
+            if (rect) v = (v * 5793 + 2048) >> 12;
+            v = post > 0 ? (v + (1 << (post - 1))) >> post : v * (1 << -post);
+            p[i * stride] = v;
+        }
+    }
+}
+__device__ __noinline__ void fwd1d_mem(int kind, int n, int32_t *p, int stride, int pre, int nout, int rect, int post) {
+    switch (n) {
+    case 4: fwd_mem_n<4>(kind, p, stride, pre, nout, rect, post); break;
+    case 8: fwd_mem_n<8>(kind, p, stride, pre, nout, rect, post); break;
+    case 16: fwd_mem_n<16>(kind, p, stride, pre, nout, rect, post); break;
+    case 32: fwd_mem_n<32>(0, p, stride, pre, nout, rect, post); break;
+    default: fwd_mem_n<64>(0, p, stride, pre, nout, rect, post); break;
+    }
+}
+
+// runtime geometry of a tx size: the forward transform's shifts (the range rule: s0 = 17 - BD - log2 H keeps every
+// column intermediate inside int32 rotations, s1 = log2 W the row inputs, s2 brings the result to the dequantisation
+// domain with FB fractional bits, DQ = M_H^T R M_W 2^(rowShift + 4) / (H W / 4) / rect) and the distortion scale
+// (pixel SSE = sum (DQ - dequant)^2 2^-(2 FB + k))
+struct TxRt {
+    int W, H, lw, lh, tw, th, ltw, n, TS, rowShift, rect, s0, s1, s2, dsh;
 };
+__device__ __forceinline__ TxRt tx_rt(int txSz, int bd) {
+    TxRt d;
+    d.W = txw(txSz); d.H = txh(txSz);
+    d.lw = AV1G_T(Tx_Width_Log2)[txSz]; d.lh = AV1G_T(Tx_Height_Log2)[txSz];
+    d.tw = min(d.W, 32); d.th = min(d.H, 32); d.ltw = min(d.lw, 5); d.n = d.tw * d.th;
+    d.TS = d.W + 1;
+    d.rowShift = AV1G_T(Transform_Row_Shift)[txSz];
+    d.rect = (d.lw - d.lh == 1 || d.lh - d.lw == 1) ? 1 : 0;
+    const int E = d.rowShift + 4 + FB - (d.lw + d.lh - 2);
+    d.s0 = max(0, 17 - bd - d.lh);
+    d.s1 = d.lw;
+    d.s2 = d.s0 - d.s1 - E;
+    d.dsh = 16 - 2 * FB - (2 * (d.rowShift + 4) - (d.lw + d.lh - 2) + d.rect);
+    return d;
+}
 
 // Residual source of an evaluation: src - prediction (a mode with edges, or CfL), computed per sample; or a given
 // residual array (kernel tests).
@@ -395,38 +426,27 @@ __device__ __forceinline__ ResFn<P> res_cfl(const P *src, int sp, int lw, int lh
     return ResFn<P>{src, sp, nullptr, nullptr, AV1G_DC_PRED, 0, lw, lh, dcv, cfl, alpha, avg, maxv, nullptr};
 }
 
-// forward 2-D transform of the residual res (H x W int16, row-major, shared memory) into tmp (th x tw, row stride TS)
-template <int W, int H, int BD>
-__device__ __forceinline__ void warp_fwd(const int16_t *res, int txType, int32_t *tmp) {
-    typedef TxDims<W, H> D;
-    constexpr int s0 = (17 - BD - D::lh) > 0 ? (17 - BD - D::lh) : 0, s1 = D::lw, s2 = s0 - s1 - D::E;
-    const int lane = lane_id();
-    const int ck = col_kind(txType), rk = row_kind(txType);
-    for (int j = lane; j < W; j += 32) {
-        int32_t T[H];
-#pragma unroll
-        for (int i = 0; i < H; i++) T[i] = (int32_t)res[i * W + j] * (1 << s0);
-        fwd1d<H>(ck, T);
-#pragma unroll
-        for (int i = 0; i < D::th; i++) tmp[i * D::TS + j] = (T[i] + (1 << (s1 - 1))) >> s1;
-    }
-    __syncwarp();
-    for (int i = lane; i < D::th; i += 32) {
-        int32_t T[W];
-#pragma unroll
-        for (int j = 0; j < W; j++) T[j] = tmp[i * D::TS + j];
-        fwd1d<W>(rk, T);
-#pragma unroll
-        for (int j = 0; j < D::tw; j++) {
-            int32_t v = T[j];
-            if (D::rect) v = (v * 5793 + 2048) >> 12;
-            if constexpr (s2 > 0) v = (v + (1 << (s2 - 1))) >> s2;
-            else if constexpr (s2 < 0) v = v * (1 << -s2);
-            tmp[i * D::TS + j] = v;
-        }
-    }
-    __syncwarp();
+// ---- lane groups: G lanes (a power of two) evaluate one task; reductions stay inside the aligned group ----
+__device__ __forceinline__ int grp_sum(int v, int G) {
+    for (int o = G >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
+__device__ __forceinline__ i64 grp_sum64(i64 v, int G) {
+    for (int o = G >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ int grp_max(int v, int G) {
+    for (int o = G >> 1; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+// lanes per evaluation task for a tx size in the analysis / closed loop: every task runs its column and row passes on
+// at least as many lanes as it has columns / rows, the warp holds 32 / G tasks
+__device__ __forceinline__ int grp_size(int txSz) {
+    const int W = txw(txSz), H = txh(txSz);
+    return (W >= 32 || H >= 32) ? 32 : max(max(W, H), 8);
+}
+// scratch of one task: int32 buffer H x (W + 1), levels tw x th
+__device__ __forceinline__ int task_buf_ints(int txSz) { return txh(txSz) * (txw(txSz) + 1); }
 
 // ---------------------------------------------------------------------------------------------------------------
 // quantisation + distortion + exact rate (warp)
@@ -522,18 +542,31 @@ __device__ __forceinline__ int coeff_bits(int c, int eob, const int16_t *q, cons
     return b;
 }
 
-// quantise the coefficients in tmp (th x tw, row stride TS) into q (tw x th natural order), distortion, rate.
-// zbin 21/32, rounding 3/8 of the step (the reference's 0.656 / 0.375), levels capped at 16383.
-template <int W, int H, int BD>
-__device__ __forceinline__ EvalOut warp_quant_rate(const int32_t *tmp, int16_t *q, const EvalIn &e, i64 resE) {
-    typedef TxDims<W, H> D;
-    constexpr int txSz = D::size;
-    const int lane = lane_id();
+// One evaluation (group of G lanes, all 32 lanes of the warp call it together with the same txSz): residual into
+// buf, forward transform in place (columns, then rows), dead-zone quantisation into q (zbin 21/32, rounding 3/8 of
+// the step, the reference's 0.656 / 0.375; levels capped at 16383), transform-domain distortion, exact rate.  The
+// coefficients stay in buf (th x tw, row stride W + 1).
+template <int BD, typename Px>
+__device__ __noinline__ EvalOut grp_eval(int txSz, const ResFn<Px> &rf, const EvalIn &e, int32_t *buf, int16_t *q, int g, int G) {
+    const TxRt d = tx_rt(txSz, BD);
+    const int ck = col_kind(e.txType), rk = row_kind(e.txType);
+    const bool big = d.W == 64 || d.H == 64;
+    i64 en = 0;
+    for (int j = g; j < d.W; j += G) {
+        for (int i = 0; i < d.H; i++) {
+            const int r = rf(i, j);
+            en += r * r;
+            buf[i * d.TS + j] = r;
+        }
+        fwd1d_mem(ck, d.H, buf + j, d.TS, d.s0, d.th, 0, d.s1);
+    }
+    __syncwarp();
+    for (int i = g; i < d.th; i += G) fwd1d_mem(rk, d.W, buf + i * d.TS, 1, 0, d.tw, d.rect, d.s2);
+    __syncwarp();
     const int den = dq_denom(txSz);
     i64 dist = 0, kept = 0;
-    for (int idx = lane; idx < D::n; idx += 32) {
-        const int i = idx / D::tw, j = idx % D::tw;
-        const int v = tmp[i * D::TS + j];
+    for (int idx = g; idx < d.n; idx += G) {
+        const int v = buf[(idx >> d.ltw) * d.TS + (idx & (d.tw - 1))];
         const int step = idx == 0 ? e.dcQ : e.acQ;
         const int a = abs(v) * den, S = step << FB;
         int l = 0;
@@ -541,33 +574,29 @@ __device__ __forceinline__ EvalOut warp_quant_rate(const int32_t *tmp, int16_t *
         const int qv = v < 0 ? -l : l;
         q[idx] = (int16_t)qv;
         const int dq = l ? dequant<BD>(qv, step, den) * (1 << FB) : 0;
-        const i64 d = (i64)(v - dq);
-        dist += d * d;
+        const i64 df = (i64)(v - dq);
+        dist += df * df;
         kept += (i64)v * v;
     }
-    dist = warp_sum64(dist);
+    dist = grp_sum64(dist, G);
     __syncwarp();
     const uint16_t *scan = get_scan(txSz, e.txType);
     int last = 0;
-    for (int c = lane; c < D::n; c += 32)
+    for (int c = g; c < d.n; c += G)
         if (q[scan[c]]) last = c + 1;
-    const int eob = warp_max(last);
-    i64 bits = 0;
-    if (eob > 0) {
-        const int cls = tx_class(e.txType);
-        int b = 0;
-        for (int c = lane; c < eob; c += 32) b += coeff_bits(c, eob, q, scan, txSz, cls, e.plane > 0, e.dcCtx, e.C);
-        bits = warp_sum(b);
-    }
-    bits += base_bits(txSz, e, eob);
+    const int eob = grp_max(last, G);
+    int b = 0;
+    const int cls = tx_class(e.txType);
+    for (int c = g; c < eob; c += G) b += coeff_bits(c, eob, q, scan, txSz, cls, e.plane > 0, e.dcCtx, e.C);
     EvalOut o;
-    o.D = dist << D::dsh;
-    if (W == 64 || H == 64) {
-        kept = warp_sum64(kept);
-        const i64 extra = (resE << 16) - (kept << D::dsh);
+    o.R = grp_sum(b, G) + base_bits(txSz, e, eob);
+    o.D = dist << d.dsh;
+    if (big) {
+        en = grp_sum64(en, G);
+        kept = grp_sum64(kept, G);
+        const i64 extra = (en << 16) - (kept << d.dsh);
         o.D += extra > 0 ? extra : 0;
     }
-    o.R = bits;
     o.eob = eob;
     return o;
 }
@@ -618,65 +647,63 @@ template <int N> __device__ __forceinline__ uint32_t inv1d(int kind, int32_t *T,
     }
     return 0;
 }
+template <int N>
+__device__ __forceinline__ uint32_t inv_mem_n(int kind, int32_t *p, int stride, int r, int preRect, int post, int clampBits) {
+    int32_t T[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        T[i] = p[i * stride];
+        if (preRect) T[i] = (int32_t)(((i64)T[i] * 2896 + 2048) >> 12);
+    }
+    const uint32_t e = inv1d<N>(kind, T, r);
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        int32_t v = post ? (int32_t)(((i64)T[i] + (1 << (post - 1))) >> post) : T[i];
+        if (clampBits) v = min(max(v, -(1 << (clampBits - 1))), (1 << (clampBits - 1)) - 1);
+        p[i * stride] = v;
+    }
+    return e;
+}
+__device__ __noinline__ uint32_t inv1d_mem(int kind, int n, int32_t *p, int stride, int r, int preRect, int post, int clampBits) {
+    switch (n) {
+    case 4: return inv_mem_n<4>(kind, p, stride, r, preRect, post, clampBits);
+    case 8: return inv_mem_n<8>(kind, p, stride, r, preRect, post, clampBits);
+    case 16: return inv_mem_n<16>(kind, p, stride, r, preRect, post, clampBits);
+    case 32: return inv_mem_n<32>(0, p, stride, r, preRect, post, clampBits);
+    default: return inv_mem_n<64>(0, p, stride, r, preRect, post, clampBits);
+    }
+}
 
-// levels q (tw x th) -> residual res (H x W row-major) of the spec's 2-D inverse; returns the OR of the flags.  The
-// row outputs are clamped to colClampRange (16 bits at 8 and 10 bits) and the final residual is within 12 bits, so int16
-// holds both.
-template <int W, int H, int BD>
-__device__ __forceinline__ uint32_t warp_inverse(const int16_t *q, int txType, int dcQ, int acQ, int16_t *res) {
-    typedef TxDims<W, H> D;
+// levels q (tw x th) -> residual in buf (H x W, row stride W + 1) of the spec's 2-D inverse (7.13.3, Lossless = 0:
+// dequantisation, row transforms at BitDepth + 8 bits with the 2:1 rectangular scaling, Round2 by the row shift,
+// clamp to colClampRange, column transforms, Round2(., 4)); returns the OR of the conformance flags (group)
+template <int BD>
+__device__ __noinline__ uint32_t grp_inverse(int txSz, const int16_t *q, int txType, int dcQ, int acQ, int32_t *buf, int g, int G) {
+    const TxRt d = tx_rt(txSz, BD);
     constexpr int rowR = BD + 8, colR = (BD + 6) > 16 ? BD + 6 : 16;
-    const int lane = lane_id();
-    const int den = dq_denom(D::size);
+    const int den = dq_denom(txSz);
     const int ck = col_kind(txType), rk = row_kind(txType);
+    for (int p = g; p < d.W * d.H; p += G) {
+        const int i = p >> d.lw, j = p & (d.W - 1);
+        int v = 0;
+        if (i < d.th && j < d.tw) {
+            const int l = q[i * d.tw + j];
+            v = l ? dequant<BD>(l, (i == 0 && j == 0) ? dcQ : acQ, den) : 0;
+        }
+        buf[i * d.TS + j] = v;
+    }
+    __syncwarp();
     uint32_t err = 0;
-    for (int i = lane; i < H; i += 32) {
-        int32_t T[W];
-        bool nz = false;
-#pragma unroll
-        for (int j = 0; j < W; j++) {
-            int v = 0;
-            if (i < D::th && j < D::tw) {
-                const int l = q[i * D::tw + j];
-                v = l ? dequant<BD>(l, (i == 0 && j == 0) ? dcQ : acQ, den) : 0;
-            }
-            T[j] = v;
-            nz |= v != 0;
-        }
-        if (!nz) {
-#pragma unroll
-            for (int j = 0; j < W; j++) res[i * W + j] = 0;
-            continue;
-        }
-        if (D::rect) {
-#pragma unroll
-            for (int j = 0; j < W; j++) T[j] = (int32_t)(((i64)T[j] * 2896 + 2048) >> 12);
-        }
-        err |= inv1d<W>(rk, T, rowR);
-#pragma unroll
-        for (int j = 0; j < W; j++) {
-            int32_t v = D::rowShift ? (int32_t)(((i64)T[j] + (1 << (D::rowShift - 1))) >> D::rowShift) : T[j];
-            res[i * W + j] = (int16_t)min(max(v, -(1 << (colR - 1))), (1 << (colR - 1)) - 1);
-        }
-    }
+    for (int i = g; i < d.H; i += G) err |= inv1d_mem(rk, d.W, buf + i * d.TS, 1, rowR, d.rect, d.rowShift, colR);
     __syncwarp();
-    for (int j = lane; j < W; j += 32) {
-        int32_t T[H];
-#pragma unroll
-        for (int i = 0; i < H; i++) T[i] = res[i * W + j];
-        err |= inv1d<H>(ck, T, colR);
-#pragma unroll
-        for (int i = 0; i < H; i++) res[i * W + j] = (int16_t)(((i64)T[i] + 8) >> 4);
-    }
+    for (int j = g; j < d.W; j += G) err |= inv1d_mem(ck, d.H, buf + j, d.TS, colR, 0, 4, 0);
     __syncwarp();
-    return (uint32_t)warp_max((int)err);
+    return (uint32_t)grp_max((int)err, G);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// runtime dispatch over the 19 tx sizes
+// runtime dispatch over the 19 tx sizes (host-side self-checks)
 // ---------------------------------------------------------------------------------------------------------------
-// one evaluation of any tx size (warp): residual into res (lanes over samples), forward transform, quantisation,
-// rate, distortion.  res: H x W int16 scratch, tmp: 32 x 65 int32 scratch, q: the levels (may alias res).
 #define IS_TX_SWITCH(txSz, M)            \
     switch (txSz) {                      \
     case AV1G_TX_4X4: M(4, 4); break;    \
@@ -700,33 +727,4 @@ __device__ __forceinline__ uint32_t warp_inverse(const int16_t *q, int txType, i
     default: M(64, 16); break;           \
     }
 
-}  // namespace is
-
-namespace is {
-template <int BD, typename Px>
-__device__ __noinline__ EvalOut rc_eval(int txSz, const ResFn<Px> &rf, const EvalIn &e, int16_t *res, int32_t *tmp, int16_t *q) {
-    const int lane = lane_id();
-    const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W);
-    i64 en = 0;
-    for (int p = lane; p < W * H; p += 32) {
-        const int r = rf(p >> lw, p & (W - 1));
-        res[p] = (int16_t)r;
-        en += r * r;
-    }
-    __syncwarp();
-    const i64 resE = (W == 64 || H == 64) ? warp_sum64(en) : 0;
-    EvalOut o;
-#define IS_RC_EVAL(W_, H_) { warp_fwd<W_, H_, BD>(res, e.txType, tmp); o = warp_quant_rate<W_, H_, BD>(tmp, q, e, resE); }
-    IS_TX_SWITCH(txSz, IS_RC_EVAL)
-#undef IS_RC_EVAL
-    return o;
-}
-template <int BD>
-__device__ __noinline__ uint32_t rc_inverse(int txSz, const int16_t *q, int txType, int dcQ, int acQ, int16_t *res) {
-    uint32_t e = 0;
-#define IS_RC_INV(W_, H_) e = warp_inverse<W_, H_, BD>(q, txType, dcQ, acQ, res)
-    IS_TX_SWITCH(txSz, IS_RC_INV)
-#undef IS_RC_INV
-    return e;
-}
 }  // namespace is

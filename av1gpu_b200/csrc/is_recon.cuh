@@ -34,9 +34,10 @@ template <typename Px> struct RcSmem {
     uint16_t leafCoef[SB_MAX_LEAVES + 1];
     int next, sbIdx;
     struct Warp {
-        int16_t res[64 * 64];      // residual of an evaluation; the inverse transform's residual
-        int32_t tmp[32 * 65];      // forward-transform scratch
-        int16_t qa[2][1024], qb[2][1024];   // levels: candidate / best (chroma: U, V)
+        int32_t buf[64 * 65];      // evaluation scratch (32 / G tasks) and the inverse transform's residual
+        int16_t q[1024];           // levels of the tasks of a round
+        int16_t qb[2][1024];       // best levels (chroma: U, V)
+        i64 taskJ[8];
         Px ea[3][EDGE_LEN], el[3][EDGE_LEN];
         int16_t cfl[256];
         int satd[32];
@@ -54,15 +55,15 @@ __device__ __forceinline__ void st_release(int *p, int v) { asm volatile("st.rel
 // exact inverse + reconstruction of a tx block (warp), the levels halved until conformant (AV1G_ENC_FIX_RANGE's
 // repair, the reference's cta_inverse_add, k_recon.cuh:140-197); writes prediction + residual into the plane
 template <int BD, typename Px>
-__device__ void rc_reconstruct(int txSz, int txType, int16_t *q, int dcQ, int acQ, const ResFn<Px> &rf, Px *dst, int pitch, int16_t *res) {
+__device__ void rc_reconstruct(int txSz, int txType, int16_t *q, int dcQ, int acQ, const ResFn<Px> &rf, Px *dst, int pitch, int32_t *buf) {
     const int lane = lane_id();
-    const int W = txw(txSz), H = txh(txSz), n = min(W, 32) * min(H, 32);
+    const int W = txw(txSz), H = txh(txSz), n = min(W, 32) * min(H, 32), TS = W + 1;
     bool any = false;
     for (;;) {
         int nz = 0;
         for (int i = lane; i < n; i += 32) nz |= q[i] != 0;
         if (!__any_sync(0xffffffffu, nz)) { any = false; break; }
-        const uint32_t err = rc_inverse<BD>(txSz, q, txType, dcQ, acQ, res);
+        const uint32_t err = grp_inverse<BD>(txSz, q, txType, dcQ, acQ, buf, lane, 32);
         if (!err) { any = true; break; }
         for (int i = lane; i < n; i += 32) q[i] = (int16_t)(q[i] / 2);
         __syncwarp();
@@ -70,7 +71,7 @@ __device__ void rc_reconstruct(int txSz, int txType, int16_t *q, int dcQ, int ac
     const int lw = 31 - __clz(W);
     for (int p = lane; p < W * H; p += 32) {
         const int i = p >> lw, j = p & (W - 1);
-        int v = rf.pred(i, j) + (any ? res[p] : 0);
+        int v = rf.pred(i, j) + (any ? buf[i * TS + j] : 0);
         v = min(max(v, 0), (1 << BD) - 1);
         dst[(size_t)i * pitch + j] = (Px)v;
     }
@@ -219,43 +220,56 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
             return res_mode<Px>(src, F.spitch[0], A, L, m, cand_delta(c), lw, lh, dcv);
         };
         const int set = tx_set_intra(txSz);
-        int16_t *cur = Wp.qa[0], *best = Wp.qb[0];
+        const int G = grp_size(txSz), ng = 32 / G, grp = lane / G, g = lane & (G - 1);
+        const int nq = min(W, 32) * min(H, 32);
+        int32_t *tb = Wp.buf + grp * task_buf_ints(txSz);
+        int16_t *tq = Wp.q + grp * nq;
+        int16_t *best = Wp.qb[0];
         i64 bestJ = INF;
         int bestC = br.cand[0], bestT = br.tx;
         bool have = false;
-        auto run = [&](int c, int t) {
-            const EvalIn e{t, 0, skipCtx, dcCtx, cand_mode(c), F.dcQ, F.acQ, C};
-            const EvalOut o = rc_eval<BD, Px>(txSz, rfOf(c), e, Wp.res, Wp.tmp, cur);
-            const i64 J = o.D + F.lam * (o.R + mbits(c));
-            if (J < bestJ) {
-                bestJ = J; bestC = c; bestT = t; have = true;
-                int16_t *s = cur; cur = best; best = s;
+        // tasks (candidate, tx type) in rounds of 32 / G; costs compared in task order (first of equal costs wins);
+        // the round's winner, if it beats the best so far, leaves its levels in `best`
+        auto run = [&](const int *tc, const int *tt, int n) {
+            for (int r0 = 0; r0 < n; r0 += ng) {
+                const int k = min(r0 + grp, n - 1);
+                const int c = tc[k], t = tt[k];
+                const EvalIn e{t, 0, skipCtx, dcCtx, cand_mode(c), F.dcQ, F.acQ, C};
+                const EvalOut o = grp_eval<BD, Px>(txSz, rfOf(c), e, tb, tq, g, G);
+                if (g == 0 && r0 + grp < n) Wp.taskJ[grp] = o.D + F.lam * (o.R + mbits(c));
+                __syncwarp();
+                int win = -1;
+                for (int u = 0; u < ng && r0 + u < n; u++)
+                    if (Wp.taskJ[u] < bestJ) { bestJ = Wp.taskJ[u]; bestC = tc[r0 + u]; bestT = tt[r0 + u]; win = u; have = true; }
+                if (win >= 0)
+                    for (int i = lane; i < nq; i += 32) best[i] = Wp.q[win * nq + i];
+                __syncwarp();
             }
         };
         const int nc = max(1, min((int)br.ncand, K_RECHECK));
-        const int nT1 = nc + (br.tx != AV1G_DCT_DCT ? 1 : 0);
-        const bool skip1 = nT1 == 1;
-        if (!skip1) {
-            for (int k = 0; k < nc; k++) run(br.cand[k], AV1G_DCT_DCT);
-            if (br.tx != AV1G_DCT_DCT) run(br.cand[0], br.tx);
-        } else {
-            bestC = br.cand[0]; bestT = AV1G_DCT_DCT;
-        }
+        int tc[8], tt[8], n1 = 0;
+        for (int k = 0; k < nc; k++) { tc[n1] = br.cand[k]; tt[n1] = AV1G_DCT_DCT; n1++; }
+        if (br.tx != AV1G_DCT_DCT) { tc[n1] = br.cand[0]; tt[n1] = br.tx; n1++; }
+        const bool skip1 = n1 == 1;
+        if (!skip1) run(tc, tt, n1);
+        else { bestC = br.cand[0]; bestT = AV1G_DCT_DCT; }
         if (set != AV1G_TX_SET_DCTONLY) {
             const int c1 = bestC;
             const bool isC0 = c1 == br.cand[0];
+            int n2 = 0;
             for (int t = 0; t < 16; t++) {
                 if (!tx_in_set(set, t)) continue;
                 if (!skip1 && (t == AV1G_DCT_DCT || (isC0 && t == br.tx))) continue;
-                run(c1, t);
+                tc[n2] = c1; tt[n2] = t; n2++;
             }
+            run(tc, tt, n2);
         }
         if (!have) {   // one candidate, DCT only: its levels
             const EvalIn e{bestT, 0, skipCtx, dcCtx, cand_mode(bestC), F.dcQ, F.acQ, C};
-            rc_eval<BD, Px>(txSz, rfOf(bestC), e, Wp.res, Wp.tmp, best);
+            grp_eval<BD, Px>(txSz, rfOf(bestC), e, Wp.buf, best, lane, 32);
         }
         Px *dst = (Px *)F.rec[0] + (size_t)y * F.rpitch[0] + x;
-        rc_reconstruct<BD, Px>(txSz, bestT, best, F.dcQ, F.acQ, rfOf(bestC), dst, F.rpitch[0], Wp.res);
+        rc_reconstruct<BD, Px>(txSz, bestT, best, F.dcQ, F.acQ, rfOf(bestC), dst, F.rpitch[0], Wp.buf);
         eobY = rc_record<Px>(F, sb, 0, txSz, bestT, x >> 2, y >> 2, best, txbBase, coefBase);
         yMode = cand_mode(bestC);
         yDelta = cand_delta(bestC);
@@ -400,19 +414,29 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
             if (c == 255) return res_cfl<Px>(sP[pl], F.spitch[pl], lw, lh, dcv[pl], Wp.cfl, alpha[pl], cflAvg, (1 << BD) - 1);
             return res_mode<Px>(sP[pl], F.spitch[pl], A[pl], L[pl], cand_mode(c), cand_delta(c), lw, lh, dcv[pl]);
         };
-        int16_t *cur[2] = {Wp.qa[0], Wp.qa[1]}, *best[2] = {Wp.qb[0], Wp.qb[1]};
+        // (candidate, plane) tasks in rounds of 32 / G; each candidate's cost = U + V + lambda * its mode bits; the
+        // winner's two planes are evaluated once more for their levels
+        const int G = grp_size(txSz), ng = 32 / G, grp = lane / G, g = lane & (G - 1);
+        const int nq = min(W, 32) * min(H, 32);
+        int32_t *tb = Wp.buf + grp * task_buf_ints(txSz);
+        int16_t *tq = Wp.q + grp * nq;
+        i64 pj[2 * (UV_K + 1)];
+        const int ntask = 2 * nch;
+        for (int r0 = 0; r0 < ntask; r0 += ng) {
+            const int k = min(r0 + grp, ntask - 1), c = chosen[k >> 1], pl = 1 + (k & 1);
+            const int txType = chroma_tx_type(txSz, c == 255 ? AV1G_UV_CFL_PRED : cand_mode(c));
+            const EvalIn e{txType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, C};
+            const EvalOut o = grp_eval<BD, Px>(txSz, rfOf(pl, c), e, tb, tq, g, G);
+            if (g == 0 && r0 + grp < ntask) Wp.taskJ[grp] = o.D + F.lam * o.R;
+            __syncwarp();
+            for (int u = 0; u < ng && r0 + u < ntask; u++) pj[r0 + u] = Wp.taskJ[u];
+            __syncwarp();
+        }
         i64 bJ = INF;
         int bestC = cand_pack(AV1G_DC_PRED, 0);
         for (int k = 0; k < nch; k++) {
             const int c = chosen[k];
-            const int mode = c == 255 ? AV1G_UV_CFL_PRED : cand_mode(c);
-            const int txType = chroma_tx_type(txSz, mode);
-            i64 J = 0;
-            for (int pl = 1; pl <= 2; pl++) {
-                const EvalIn e{txType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, C};
-                const EvalOut o = rc_eval<BD, Px>(txSz, rfOf(pl, c), e, Wp.res, Wp.tmp, cur[pl - 1]);
-                J += o.D + F.lam * o.R;
-            }
+            i64 J = pj[2 * k] + pj[2 * k + 1];
             int b;
             if (c == 255) {
                 const int a1 = alpha[1], a2 = alpha[2];
@@ -424,9 +448,20 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
                 b = uvcbits(c);
             }
             J += F.lam * b;
-            if (J < bJ) {
-                bJ = J; bestC = c;
-                for (int p = 0; p < 2; p++) { int16_t *s = cur[p]; cur[p] = best[p]; best[p] = s; }
+            if (J < bJ) { bJ = J; bestC = c; }
+        }
+        int16_t *best[2] = {Wp.qb[0], Wp.qb[1]};
+        {   // the winner's U and V levels (two tasks: one round when the warp holds two groups)
+            const int ntk = 2;
+            for (int r0 = 0; r0 < ntk; r0 += ng) {
+                const int k = min(r0 + grp, ntk - 1), pl = 1 + k;
+                const int txType = chroma_tx_type(txSz, bestC == 255 ? AV1G_UV_CFL_PRED : cand_mode(bestC));
+                const EvalIn e{txType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, C};
+                grp_eval<BD, Px>(txSz, rfOf(pl, bestC), e, tb, tq, g, G);
+                __syncwarp();
+                for (int u = 0; u < ng && r0 + u < ntk; u++)
+                    for (int i = lane; i < nq; i += 32) best[r0 + u][i] = Wp.q[u * nq + i];
+                __syncwarp();
             }
         }
         const bool cfl = bestC == 255;
@@ -434,7 +469,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
         const int uvType = chroma_tx_type(txSz, uv);
         for (int pl = 1; pl <= 2; pl++) {
             Px *dst = (Px *)F.rec[pl] + (size_t)cy * F.rpitch[pl] + cx;
-            rc_reconstruct<BD, Px>(txSz, uvType, best[pl - 1], F.dcQ, F.acQ, rfOf(pl, bestC), dst, F.rpitch[pl], Wp.res);
+            rc_reconstruct<BD, Px>(txSz, uvType, best[pl - 1], F.dcQ, F.acQ, rfOf(pl, bestC), dst, F.rpitch[pl], Wp.buf);
             const int yt = AV1G_T(Max_Tx_Size_Rect)[bsize];
             const int off = coefBase + min(txw(yt), 32) * min(txh(yt), 32) + (pl - 1) * min(W, 32) * min(H, 32);
             const int e = rc_record<Px>(F, sb, pl, txSz, uvType, cx4, cy4, best[pl - 1], txbBase + pl, off);

@@ -4,10 +4,10 @@
 
 namespace {
 
-struct TestScr { int16_t res[4096]; int32_t tmp[32 * 65]; int16_t q[1024]; };
+struct TestScr { int32_t buf[64 * 65]; int16_t q[1024]; };
 
-// one warp per block: the search's own rc_eval with a residual array as the source; the coefficients are read back
-// from the scratch before quantisation overwrote nothing of them (quantisation writes q only)
+// one warp per block: the search's own grp_eval (one task, 32 lanes) with a residual array as the source; the
+// coefficients are read back from the scratch (quantisation writes only the levels)
 __global__ void k_test_fwd_quant(int n, const int32_t *res, int txSz, int txType, int plane, int dcQ, int acQ, int qctx, int skipCtx,
                                  int dcCtx, int intraDir, int32_t *coef, int16_t *lv, long long *D, long long *R, int32_t *eob) {
     extern __shared__ __align__(16) unsigned char tsm[];
@@ -17,9 +17,9 @@ __global__ void k_test_fwd_quant(int n, const int32_t *res, int txSz, int txType
     const int W = txw(txSz), H = txh(txSz), tw = min(W, 32), th = min(H, 32), nc = tw * th, lw = 31 - __clz(W);
     const EvalIn e{txType, plane, skipCtx, dcCtx, intraDir, dcQ, acQ, g_cost[qctx]};
     ResFn<uint8_t> rf{nullptr, 0, nullptr, nullptr, 0, 0, lw, 31 - __clz(H), 0, nullptr, 0, 0, 0, res + (size_t)b * W * H};
-    const EvalOut o = rc_eval<8, uint8_t>(txSz, rf, e, S.res, S.tmp, S.q);
+    const EvalOut o = grp_eval<8, uint8_t>(txSz, rf, e, S.buf, S.q, lane_id(), 32);
     for (int idx = lane_id(); idx < nc; idx += 32) {
-        coef[(size_t)b * nc + idx] = S.tmp[(idx / tw) * (W + 1) + idx % tw];
+        coef[(size_t)b * nc + idx] = S.buf[(idx / tw) * (W + 1) + idx % tw];
         lv[(size_t)b * nc + idx] = S.q[idx];
     }
     (void)th;
@@ -27,14 +27,13 @@ __global__ void k_test_fwd_quant(int n, const int32_t *res, int txSz, int txType
 }
 
 __global__ void k_test_inverse(int n, const int16_t *lv, int txSz, int txType, int dcQ, int acQ, int32_t *res, uint32_t *flags) {
-    __shared__ int16_t S[4][4096];
-    const int b = blockIdx.x * 4 + (threadIdx.x >> 5);
+    extern __shared__ __align__(16) unsigned char tsm[];
+    TestScr &S = reinterpret_cast<TestScr *>(tsm)[threadIdx.x >> 5];
+    const int b = blockIdx.x * 2 + (threadIdx.x >> 5);
     if (b >= n) return;
     const int W = txw(txSz), H = txh(txSz), nc = min(W, 32) * min(H, 32);
-    int16_t *r = S[threadIdx.x >> 5];
-    uint32_t f = 0;
-    f = rc_inverse<8>(txSz, lv + (size_t)b * nc, txType, dcQ, acQ, r);
-    for (int p = lane_id(); p < W * H; p += 32) res[(size_t)b * W * H + p] = r[p];
+    const uint32_t f = grp_inverse<8>(txSz, lv + (size_t)b * nc, txType, dcQ, acQ, S.buf, lane_id(), 32);
+    for (int p = lane_id(); p < W * H; p += 32) res[(size_t)b * W * H + p] = S.buf[(p / W) * (W + 1) + p % W];
     if (lane_id() == 0) flags[b] = f;
 }
 
@@ -107,7 +106,8 @@ int is_test_inverse(is_handle *h, int n, const int16_t *levels, int txSz, int tx
     if (!rc) rc = dev_upload<int32_t>(h, &dres, nullptr, (size_t)n * W * H);
     if (!rc) rc = dev_upload<uint32_t>(h, &dfl, nullptr, n);
     if (!rc) {
-        k_test_inverse<<<(n + 3) / 4, 128>>>(n, dlv, txSz, txType, AV1G_T(Dc_Qlookup)[0][qindex], AV1G_T(Ac_Qlookup)[0][qindex], dres, dfl);
+        cudaFuncSetAttribute(k_test_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (int)sizeof(TestScr));
+        k_test_inverse<<<(n + 1) / 2, 64, 2 * sizeof(TestScr)>>>(n, dlv, txSz, txType, AV1G_T(Dc_Qlookup)[0][qindex], AV1G_T(Ac_Qlookup)[0][qindex], dres, dfl);
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) rc = h->setErr(IS_ERR_CUDA, "k_test_inverse: %s", cudaGetErrorString(e));
     }

@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--qindex", type=int, default=120)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", default=None, help="WxH of a smaller image (profiling cases; not a bench number)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling cases)")
     return ap.parse_args()
 
 
@@ -117,7 +119,10 @@ def cpu_reference(args, planes, rank):
 
 
 def main():
+    global W_IMG, H_IMG
     args = parse()
+    if args.size:
+        W_IMG, H_IMG = (int(v) for v in args.size.lower().split("x"))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -180,7 +185,7 @@ def main():
         # ---- end to end through the host API ----
         barrier()
         e2e_ms = []
-        for _ in range(args.steps):
+        for _ in range(0 if args.no_e2e else args.steps):
             flush.zero_()
             barrier()
             t0 = time.perf_counter()
@@ -188,7 +193,7 @@ def main():
             rec = enc.fetch(W_IMG, H_IMG, args.qindex, out)
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
     step_ms = float(np.mean(ms))
-    e2e_step = float(np.mean(e2e_ms))
+    e2e_step = float(np.mean(e2e_ms)) if e2e_ms else float("nan")
     if world > 1:
         tt = torch.tensor([step_ms, e2e_step], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
