@@ -15,9 +15,9 @@
 
 namespace is {
 
-// Two kernels share the block search: k_analysis for the 836 blocks of the shapes up to 32 samples a side (12 warps,
-// 2 CTAs per SM), k_analysis_big for the 13 blocks with a 64-sample side (4 warps with the larger scratch).
-constexpr int AN_WARPS = 12, ANB_WARPS = 4;
+// Two kernels share the block search: k_analysis for the 836 blocks of the shapes up to 32 samples a side (8 warps,
+// 3 CTAs per SM), k_analysis_big for the 13 blocks with a 64-sample side (4 warps with the larger scratch).
+constexpr int AN_WARPS = 8, ANB_WARPS = 4;
 constexpr int AN_TASKS = 836, ANB_TASKS = 13;
 constexpr int AN_BUF_INTS = 1088;             // evaluation scratch per warp: 32 / G tasks of H x (W + 1) int32 (<= 32x32)
 constexpr int ANB_BUF_INTS = 64 * 65;
@@ -27,6 +27,8 @@ __constant__ uint8_t c_anTaskBig[ANB_TASKS][3];
 template <typename Px, int BUFI> struct AnWarp {
     int32_t buf[BUFI];
     int16_t q[1024];
+    Px pred[BUFI > 2048 ? 4096 : 1024];   // predictions of the tasks' candidates, W x H per group
+    int predC[8];                         // candidate whose prediction a group's slice holds (-1: none)
     i64 taskJ[8];
     Px ea[EDGE_LEN], el[EDGE_LEN];
     int satd[32];
@@ -90,13 +92,13 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
             int t = 0;
             if (it < items) {
                 const int sb = it & (nsub - 1), sx = (sb & (nsx - 1)) * 4, sy = (sb >> lnsx) * 4;
-                const int c = S.cand[ci], m = cand_mode(c), pa = pangle(m, cand_delta(c));
+                const int c = S.cand[ci], m = cand_mode(c);
                 int d[16];
+                pred4(m, pangle(m, cand_delta(c)), sy, sx, lw, lh, A, L, dcv, d);
 #pragma unroll
                 for (int i = 0; i < 4; i++)
 #pragma unroll
-                    for (int j = 0; j < 4; j++)
-                        d[i * 4 + j] = (int)src[(sy + i) * TW + sx + j] - pred_px(m, pa, sy + i, sx + j, lw, lh, A, L, dcv);
+                    for (int j = 0; j < 4; j++) d[i * 4 + j] = (int)src[(sy + i) * TW + sx + j] - d[i * 4 + j];
                 t = hadamard4_sum(d);
             }
 #pragma unroll
@@ -140,14 +142,25 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
     const int bufInts = task_buf_ints(txSz), nq = min(W, 32) * min(H, 32);
     int32_t *tb = S.buf + grp * bufInts;
     int16_t *tq = S.q + grp * nq;
+    Px *tp = S.pred + grp * (W * H);
+    if (lane < 8) S.predC[lane] = -1;
+    __syncwarp();
+    // the group's task: its candidate's prediction into the group's slice (kept while the candidate repeats)
+    auto evalc = [&](int c, int t) -> EvalOut {
+        const int m = cand_mode(c);
+        if (S.predC[grp] != c) grp_predict(m, pangle(m, cand_delta(c)), lw, lh, A, L, dcv, tp, g, G);
+        __syncwarp();
+        if (g == 0) S.predC[grp] = c;
+        const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, C};
+        return grp_eval<BD, Px>(txSz, ResFn<Px>{src, TW, tp, lw, nullptr}, e, tb, tq, g, G);
+    };
     i64 bestJ = INF;
     int bestK = 0, bestTx = AV1G_DCT_DCT;
     // stage 1: candidates top[0 .. nK) with DCT_DCT
     for (int r0 = 0; r0 < nK; r0 += ng) {
         const int k = min(r0 + grp, nK - 1);   // groups past the end repeat the last task (their results are unused)
-        const int c = S.cand[top[k]], m = cand_mode(c);
-        const EvalIn e{AV1G_DCT_DCT, 0, 0, 0, m, F.dcQ, F.acQ, C};
-        const EvalOut o = grp_eval<BD, Px>(txSz, res_mode<Px>(src, TW, A, L, m, cand_delta(c), lw, lh, dcv), e, tb, tq, g, G);
+        const int c = S.cand[top[k]];
+        const EvalOut o = evalc(c, AV1G_DCT_DCT);
         if (g == 0 && r0 + grp < nK) S.taskJ[grp] = o.D + F.lam * (o.R + mbits(c) + overhead);
         __syncwarp();
         for (int t = 0; t < ng && r0 + t < nK; t++)
@@ -158,11 +171,10 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
     if (set != AV1G_TX_SET_DCTONLY) {
         int types[8], nt = 0;
         for (int t = 1; t < 16; t++) if (tx_in_set(set, t)) types[nt++] = t;
-        const int c = S.cand[top[bestK]], m = cand_mode(c);
+        const int c = S.cand[top[bestK]];
         for (int r0 = 0; r0 < nt; r0 += ng) {
             const int tt = types[min(r0 + grp, nt - 1)];
-            const EvalIn e{tt, 0, 0, 0, m, F.dcQ, F.acQ, C};
-            const EvalOut o = grp_eval<BD, Px>(txSz, res_mode<Px>(src, TW, A, L, m, cand_delta(c), lw, lh, dcv), e, tb, tq, g, G);
+            const EvalOut o = evalc(c, tt);
             if (g == 0 && r0 + grp < nt) S.taskJ[grp] = o.D + F.lam * (o.R + mbits(c) + overhead);
             __syncwarp();
             for (int t = 0; t < ng && r0 + t < nt; t++)
@@ -222,7 +234,7 @@ __device__ __forceinline__ void an_sb(const FrameDesc &F, unsigned char *smem_ra
 }
 
 template <int BD>
-__global__ void __launch_bounds__(AN_WARPS * 32, 2) k_analysis(const FrameDesc *__restrict__ Fp) {
+__global__ void __launch_bounds__(AN_WARPS * 32, 3) k_analysis(const FrameDesc *__restrict__ Fp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     an_sb<BD, AN_WARPS, AN_BUF_INTS, false>(*Fp, smem_raw);
 }

@@ -291,7 +291,13 @@ size_t layout(int W, int H, uint8_t *base, FrameDesc &F, int &nSb) {
     F.oCoeffs = (int16_t *)take((size_t)nSb * SB_MAX_COEF * 2);
     F.sbCount = (SbCount *)take((size_t)nSb * sizeof(SbCount));
     F.sbOrder = (const uint32_t *)take((size_t)nSb * 4);
-    F.sbDone = (int *)take((size_t)nSb * 4);
+    F.ordmap = take((size_t)nSb * 256);
+    F.leafTxb = (uint16_t *)take((size_t)nSb * SB_MAX_LEAVES * 2);
+    F.leafCoef = (uint16_t *)take((size_t)nSb * SB_MAX_LEAVES * 2);
+    F.leafDone = (int *)take((size_t)nSb * SB_MAX_LEAVES * 4);
+    F.leafStart = (uint32_t *)take((size_t)nSb * 4);
+    F.leafQueue = (uint32_t *)take((size_t)nSb * SB_MAX_LEAVES * 4);
+    F.leafTotal = (uint32_t *)take(4);
     F.queue = (int *)take(4);
     F.err = (int *)take(4);
     F.sbDecodeOrder = (uint32_t *)take((size_t)nSb * 4);
@@ -431,7 +437,6 @@ static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) 
         const int pw = ((F.sbCols + 1) * 64) >> ss, ph = (F.sbRows * 64) >> ss;
         k_pad<uint8_t><<<dim3(1, ph), 128, 0, st>>>(dst, F.spitch[p], vw, vh, pw, ph);
     }
-    IS_CK(cudaMemsetAsync(F.sbDone, 0, (size_t)nSb * 4, st));
     IS_CK(cudaMemsetAsync(F.queue, 0, 4, st));
     IS_CK(cudaMemsetAsync(F.err, 0, 4, st));
     IS_CK(cudaEventRecord(h->ev[1], st));
@@ -442,12 +447,14 @@ static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) 
     k_dp<<<(nSb + 63) / 64, 64, 0, st>>>(h->dF, nSb);
     IS_CK(cudaGetLastError());
     IS_CK(cudaEventRecord(h->ev[3], st));
+    k_leaf_prep<<<nSb, 256, 0, st>>>(h->dF, nSb);
+    k_leaf_queue_scan<<<1, 1024, 0, st>>>(h->dF, nSb);
+    k_leaf_queue_fill<<<nSb, 256, 0, st>>>(h->dF, nSb);
+    IS_CK(cudaGetLastError());
     {
         const FrameDesc *a0 = h->dF;
-        int a1 = nSb;
-        void *args[2] = {(void *)&a0, (void *)&a1};
-        const int grid = std::min(h->rcGrid, nSb);
-        IS_CK(cudaLaunchCooperativeKernel((const void *)k_recon<8>, dim3(grid), dim3(RC_WARPS * 32), args, h->smemRc, st));
+        void *args[1] = {(void *)&a0};
+        IS_CK(cudaLaunchCooperativeKernel((const void *)k_recon<8>, dim3(h->rcGrid), dim3(RC_WARPS * 32), args, h->smemRc, st));
     }
     IS_CK(cudaEventRecord(h->ev[4], st));
     k_pack_scan<<<1, 1024, 0, st>>>(h->dF, nSb);

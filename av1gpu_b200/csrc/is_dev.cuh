@@ -260,6 +260,114 @@ __device__ __forceinline__ int pred_px(int mode, int pAng, int i, int j, int lw,
     return (wx[j] * L[i] + (256 - wx[j]) * A[w - 1] + 128) >> 8;   // SMOOTH_H
 }
 
+// One 4x4 sub-block (rows sy.., cols sx..) of a block's prediction into p[16], the values of pred_px with the mode
+// dispatch hoisted out of the samples (one branch per sub-block instead of per sample).
+template <typename P>
+__device__ __forceinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, int lh, const P *A, const P *L, int dcv, int *p) {
+    const int w = 1 << lw, h = 1 << lh;
+    if (mode == AV1G_DC_PRED) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) p[k] = dcv;
+        return;
+    }
+    if (is_dir(mode)) {
+        if (pAng == 90) {
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) p[i * 4 + j] = A[sx + j];
+        } else if (pAng == 180) {
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) p[i * 4 + j] = L[sy + i];
+        } else if (pAng < 90) {
+            const int dx = AV1G_T(Dr_Intra_Derivative)[pAng], maxBaseX = w + h - 1;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int idx = (sy + i + 1) * dx, base = (idx >> 6) + sx, sh = (idx >> 1) & 0x1F;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int k = base + j;
+                    p[i * 4 + j] = k < maxBaseX ? (A[k] * (32 - sh) + A[k + 1] * sh + 16) >> 5 : A[maxBaseX];
+                }
+            }
+        } else if (pAng > 180) {
+            const int dy = AV1G_T(Dr_Intra_Derivative)[270 - pAng];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int idx = (sx + j + 1) * dy, base = (idx >> 6) + sy, sh = (idx >> 1) & 0x1F;
+#pragma unroll
+                for (int i = 0; i < 4; i++) p[i * 4 + j] = (L[base + i] * (32 - sh) + L[base + i + 1] * sh + 16) >> 5;
+            }
+        } else {
+            const int dx = AV1G_T(Dr_Intra_Derivative)[180 - pAng], dy = AV1G_T(Dr_Intra_Derivative)[pAng - 90];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    int idx = ((sx + j) << 6) - (sy + i + 1) * dx;
+                    const P *E = A;
+                    if ((idx >> 6) < -1) { idx = ((sy + i) << 6) - (sx + j + 1) * dy; E = L; }
+                    const int b = idx >> 6, sh = (idx >> 1) & 0x1F;
+                    p[i * 4 + j] = (E[b] * (32 - sh) + E[b + 1] * sh + 16) >> 5;
+                }
+        }
+        return;
+    }
+    if (mode == AV1G_PAETH_PRED) {
+        const int tl = A[-1];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int a = A[sx + j], l = L[sy + i], base = a + l - tl;
+                const int pL = abs(base - l), pT = abs(base - a), pTL = abs(base - tl);
+                p[i * 4 + j] = (pL <= pT && pL <= pTL) ? l : pT <= pTL ? a : tl;
+            }
+        return;
+    }
+    // SMOOTH / SMOOTH_V / SMOOTH_H: sum of the vertical and horizontal terms of the modes that use them
+    const uint8_t *wx = (lw == 2 ? AV1G_T(Sm_Weights_Tx_4x4) : lw == 3 ? AV1G_T(Sm_Weights_Tx_8x8) : lw == 4 ? AV1G_T(Sm_Weights_Tx_16x16)
+                       : lw == 5 ? AV1G_T(Sm_Weights_Tx_32x32) : AV1G_T(Sm_Weights_Tx_64x64)) + sx;
+    const uint8_t *wy = (lh == 2 ? AV1G_T(Sm_Weights_Tx_4x4) : lh == 3 ? AV1G_T(Sm_Weights_Tx_8x8) : lh == 4 ? AV1G_T(Sm_Weights_Tx_16x16)
+                       : lh == 5 ? AV1G_T(Sm_Weights_Tx_32x32) : AV1G_T(Sm_Weights_Tx_64x64)) + sy;
+    const int bl = L[h - 1], tr = A[w - 1];
+    const int sh = mode == AV1G_SMOOTH_PRED ? 9 : 8, useV = mode != AV1G_SMOOTH_H_PRED, useH = mode != AV1G_SMOOTH_V_PRED;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int v = useV ? wy[i] * A[sx + j] + (256 - wy[i]) * bl : 0;
+            const int hz = useH ? wx[j] * L[sy + i] + (256 - wx[j]) * tr : 0;
+            p[i * 4 + j] = (v + hz + (1 << (sh - 1))) >> sh;
+        }
+}
+
+// the whole prediction of a W x H block into out (row stride W), 4x4 sub-blocks over the G lanes of a group
+template <typename P, typename O>
+__device__ __forceinline__ void grp_predict(int mode, int pAng, int lw, int lh, const P *A, const P *L, int dcv, O *out, int g, int G) {
+    const int nsx = 1 << (lw - 2), nsub = 1 << (lw + lh - 4);
+    for (int sb = g; sb < nsub; sb += G) {
+        const int sx = (sb & (nsx - 1)) * 4, sy = (sb >> (lw - 2)) * 4;
+        int p[16];
+        pred4(mode, pAng, sy, sx, lw, lh, A, L, dcv, p);
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) out[((sy + i) << lw) + sx + j] = (O)p[i * 4 + j];
+    }
+}
+// CfL prediction (spec 7.11.5 with the DC prediction dcv) of a W x H chroma block into out (row stride W)
+template <typename O>
+__device__ __forceinline__ void grp_predict_cfl(int lw, int lh, int dcv, const int16_t *cfl, int alpha, int avg, int maxv, O *out, int g, int G) {
+    for (int p = g; p < (1 << (lw + lh)); p += G) {
+        const int v = alpha * (cfl[p] - avg);
+        const int s = v >= 0 ? (v + 32) >> 6 : -((-v + 32) >> 6);
+        out[p] = (O)min(max(dcv + s, 0), maxv);
+    }
+}
+
 // AboveRow / LeftCol preparation (spec 7.11.2, "intra edge" arrays): lanes t = 0..nt-1 of a group fill
 // A[-1 .. w+h-1] / L[-1 .. w+h-1] from a plane (pointer at sample (0, 0), pitch in samples).
 template <int BD, typename P>
@@ -396,35 +504,19 @@ __device__ __forceinline__ TxRt tx_rt(int txSz, int bd) {
     return d;
 }
 
-// Residual source of an evaluation: src - prediction (a mode with edges, or CfL), computed per sample; or a given
+// Residual source of an evaluation: src - a prediction already in shared memory (row stride 1 << lw), or a given
 // residual array (kernel tests).
 template <typename P>
 struct ResFn {
     const P *src;        // sample (0, 0) of the block
     int sp;
-    const P *A, *L;      // edges (index 0 = AboveRow[0] / LeftCol[0])
-    int mode, pAng, lw, lh, dcv;
-    const int16_t *cfl;  // CfL luma values (nullptr: not CfL), row stride 1 << lw
-    int alpha, avg, maxv;
+    const P *pred;       // the prediction, W x H
+    int lw;
     const int32_t *arr;  // residual array (H x W row-major) instead of src - prediction
-    __device__ __forceinline__ int pred(int i, int j) const {
-        if (cfl) {
-            const int v = alpha * (cfl[(i << lw) + j] - avg);
-            const int s = v >= 0 ? (v + 32) >> 6 : -((-v + 32) >> 6);
-            return min(max(dcv + s, 0), maxv);
-        }
-        return pred_px(mode, pAng, i, j, lw, lh, A, L, dcv);
+    __device__ __forceinline__ int operator()(int i, int j) const {
+        return arr ? arr[(i << lw) + j] : (int)src[i * sp + j] - (int)pred[(i << lw) + j];
     }
-    __device__ __forceinline__ int operator()(int i, int j) const { return arr ? arr[(i << lw) + j] : (int)src[i * sp + j] - pred(i, j); }
 };
-template <typename P>
-__device__ __forceinline__ ResFn<P> res_mode(const P *src, int sp, const P *A, const P *L, int mode, int delta, int lw, int lh, int dcv) {
-    return ResFn<P>{src, sp, A, L, mode, pangle(mode, delta), lw, lh, dcv, nullptr, 0, 0, 0, nullptr};
-}
-template <typename P>
-__device__ __forceinline__ ResFn<P> res_cfl(const P *src, int sp, int lw, int lh, int dcv, const int16_t *cfl, int alpha, int avg, int maxv) {
-    return ResFn<P>{src, sp, nullptr, nullptr, AV1G_DC_PRED, 0, lw, lh, dcv, cfl, alpha, avg, maxv, nullptr};
-}
 
 // ---- lane groups: G lanes (a power of two) evaluate one task; reductions stay inside the aligned group ----
 __device__ __forceinline__ int grp_sum(int v, int G) {

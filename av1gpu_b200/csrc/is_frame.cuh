@@ -51,8 +51,13 @@ struct FrameDesc {
     int16_t *oCoeffs;                         // [nSb * SB_MAX_COEF]
     SbCount *sbCount;                         // [nSb]
     const uint32_t *sbOrder;                  // [nSb] SBs sorted by wavefront step (tile-local c + 2 r)
-    int *sbDone;                              // [nSb] 1 once the SB's reconstruction and maps are complete
-    int *queue;                               // [1] next index into sbOrder
+    uint8_t *ordmap;                          // [nSb * 256] leaf index covering each luma 4x4 unit of an SB (255: none)
+    uint16_t *leafTxb, *leafCoef;             // [nSb * 256] first tx block / coefficient (SB-local) of each leaf
+    int *leafDone;                            // [nSb * 256] 1 once the leaf's reconstruction, maps and record are written
+    uint32_t *leafStart;                      // [nSb] first queue position of each SB's leaves
+    uint32_t *leafQueue;                      // [nSb * 256] (sb << 8 | leaf) in topological order
+    uint32_t *leafTotal;                      // [1] leaves in the queue
+    int *queue;                               // [1] next queue position
     int *err;                                 // [1] error status (0 = ok)
     // pack output (DecisionRecord arrays in decode order) and per-SB offsets
     uint32_t *sbDecodeOrder;                  // [nSb] SBs in decode order (tiles raster, SB raster inside a tile)
@@ -65,8 +70,7 @@ struct FrameDesc {
 };
 
 // error codes written to FrameDesc::err by the kernels
-constexpr int KERR_WAIT_SB = 1;      // a wavefront dependency wait ran out of its iteration budget
-constexpr int KERR_WAIT_LEAF = 2;    // an intra-SB leaf dependency wait ran out
+constexpr int KERR_WAIT_LEAF = 2;    // a leaf dependency wait of the closed loop ran out of its iteration budget
 constexpr int KERR_CAPACITY = 3;     // per-SB output slots exceeded
 
 }  // namespace is

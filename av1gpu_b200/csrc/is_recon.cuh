@@ -1,49 +1,46 @@
-// is_recon.cuh - closed-loop decision + reconstruction: a persistent, dependency-driven SB wavefront.
+// is_recon.cuh - closed-loop decision + reconstruction: warps as independent workers over a global leaf queue.
 //
-// Grid: one CTA per SM (co-resident, cooperative launch), 8 warps.  CTAs take superblocks from a global queue ordered
-// by wavefront step (tile-local col + 2 row: the left and above-right SBs of an SB come earlier), wait - with a bounded
-// spin on an acquire load - for those two SBs to be complete, and run the SB.  Inside an SB the leaves (the DP's
-// blocks in decode order) are claimed by warps in decode order; a warp waits only for the earlier leaves whose area
-// meets its leaf's neighbourhood (edges, above-right / below-left reach, coefficient and mode contexts, 4:2:0 chroma
-// pairs), so independent leaves run concurrently while every leaf still sees exactly the state of a sequential
-// decode-order pass.  Per leaf (one warp; the reference's rc_luma / rc_chroma, encoder/src/k_recon.cuh:822-1686):
+// The leaves (the DP's blocks) of every SB form one global queue in topological order - SBs by wavefront step
+// (tile-local col + 2 row), the leaves of an SB in decode order - so every leaf a leaf depends on comes earlier.  A
+// persistent grid of warps (co-resident: cooperative launch) takes leaves from the queue; a warp waits - bounded spins
+// on acquire loads of per-leaf done flags - only for the earlier leaves whose area meets its leaf's neighbourhood
+// (edges with their above-right / below-left reach, coefficient and mode contexts, 4:2:0 chroma pairs), in its own SB
+// or in the SBs above, above-right and left.  Leaves of neighbouring superblocks therefore overlap, and every leaf still
+// sees exactly the state of a sequential decode-order pass.  Data written by other warps (reconstruction, maps) is read
+// with L1-bypassing loads after the acquire.  Per leaf (one warp; the reference's rc_luma / rc_chroma,
+// encoder/src/k_recon.cuh:822-1686):
 //   luma    real edges from the reconstruction, exact contexts; pass 1 = the analysis' top-2 with DCT_DCT (+ its winner
-//           with its tx type), pass 2 = the other tx types of the pass-1 winner; final levels -> exact inverse (with the
-//           conformance repair) -> reconstruction, record
+//           with its tx type), pass 2 = the other tx types of the pass-1 winner; tasks in lane groups; final levels ->
+//           exact inverse (with the conformance repair) -> reconstruction, record
 //   chroma  CfL luma from the reconstruction, least-squares alpha + +-1 refinement; SATD screening of 13 UV modes
 //           (+ +-1..3 around the best directional one); top-2 + CfL through the exact RD of U and V; final U, V
-// The BlockDecoded state of the spec is derived from a per-4x4 map of the leaf index (a unit is decoded for leaf li
-// iff its leaf index is below li), the SB border rules of clear_block_decoded_flags outside it.
+// The BlockDecoded state of the spec is derived from the SB's map of leaf indices (a unit is decoded for leaf li iff its
+// leaf index is below li) and the SB border rules of clear_block_decoded_flags outside it.
 #pragma once
 #include "is_dev.cuh"
 #include "is_frame.cuh"
 
 namespace is {
 
-constexpr int RC_WARPS = 8;
-// bounded spins: a wait that runs out records an error and moves on instead of hanging, and once any error is recorded
-// no further wait starts (the kernel then finishes with wrong data, which the host discards)
-constexpr int SB_WAIT_ITERS = 1 << 20;
-constexpr int LEAF_WAIT_ITERS = 1 << 20;
+constexpr int RC_WARPS = 7;                // warps per CTA (independent workers; shared memory bounds the count)
+constexpr int LEAF_WAIT_ITERS = 1 << 20;   // bounded spins: a wait that runs out records an error and moves on, and
+                                           // once any error is recorded no further wait starts (the host discards the
+                                           // result)
 
-template <typename Px> struct RcSmem {
-    uint8_t ordmap[16][16];        // leaf index covering each luma 4x4 unit of the SB (255: none)
-    int leafDone[SB_MAX_LEAVES];
-    Leaf lv[SB_MAX_LEAVES];
-    uint16_t leafTxb[SB_MAX_LEAVES + 1];
-    uint16_t leafCoef[SB_MAX_LEAVES + 1];
-    int next, sbIdx;
-    struct Warp {
-        int32_t buf[64 * 65];      // evaluation scratch (32 / G tasks) and the inverse transform's residual
-        int16_t q[1024];           // levels of the tasks of a round
-        int16_t qb[2][1024];       // best levels (chroma: U, V)
-        i64 taskJ[8];
-        Px ea[3][EDGE_LEN], el[3][EDGE_LEN];
-        int16_t cfl[256];
-        int satd[32];
-        int cand[32];
-    } w[RC_WARPS];
+template <typename Px> struct RcWarp {
+    int32_t buf[64 * 65];      // evaluation scratch (32 / G tasks) and the inverse transform's residual
+    int16_t q[1024];           // levels of the tasks of a round
+    int16_t qb[2][1024];       // best levels (chroma: U, V)
+    Px pred[4096];             // predictions of the tasks (W x H per group); the final prediction
+    i64 taskJ[8];
+    int predC[8];
+    Px ea[3][EDGE_LEN], el[3][EDGE_LEN];
+    int16_t cfl[256];
+    int satd[32];
+    int cand[32];
+    int job;
 };
+template <typename Px> struct RcSmem { RcWarp<Px> w[RC_WARPS]; };
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
     int v;
@@ -51,11 +48,40 @@ __device__ __forceinline__ int ld_acquire(const int *p) {
     return v;
 }
 __device__ __forceinline__ void st_release(int *p, int v) { asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
+template <typename P> __device__ __forceinline__ P ldcg(const P *p);
+template <> __device__ __forceinline__ uint8_t ldcg<uint8_t>(const uint8_t *p) { return __ldcg(p); }
+template <> __device__ __forceinline__ uint16_t ldcg<uint16_t>(const uint16_t *p) { return __ldcg(p); }
+
+// AboveRow / LeftCol from the reconstruction (other warps' data: L1-bypassing loads), as build_edges
+template <int BD, typename P>
+__device__ __forceinline__ void rec_edges(const P *plane, int pitch, int x, int y, int w, int h, int haveL, int haveA, int haveAR,
+                                          int haveBL, int maxX, int maxY, P *A, P *L) {
+    const int t = lane_id(), n = w + h;
+    const int alim = min(x + (haveAR ? 2 * w : w) - 1, maxX), llim = min(y + (haveBL ? 2 * h : h) - 1, maxY);
+    for (int i = t; i < n; i += 32) {
+        P a, l;
+        if (haveA) a = ldcg(plane + (size_t)(y - 1) * pitch + min(x + i, alim));
+        else a = haveL ? ldcg(plane + (size_t)y * pitch + x - 1) : (P)((1 << (BD - 1)) - 1);
+        if (haveL) l = ldcg(plane + (size_t)min(y + i, llim) * pitch + x - 1);
+        else l = haveA ? ldcg(plane + (size_t)(y - 1) * pitch + x) : (P)((1 << (BD - 1)) + 1);
+        A[i] = a;
+        L[i] = l;
+    }
+    if (t == 0) {
+        P c;
+        if (haveA && haveL) c = ldcg(plane + (size_t)(y - 1) * pitch + x - 1);
+        else if (haveA) c = ldcg(plane + (size_t)(y - 1) * pitch + x);
+        else if (haveL) c = ldcg(plane + (size_t)y * pitch + x - 1);
+        else c = (P)(1 << (BD - 1));
+        A[-1] = c;
+        L[-1] = c;
+    }
+}
 
 // exact inverse + reconstruction of a tx block (warp), the levels halved until conformant (AV1G_ENC_FIX_RANGE's
 // repair, the reference's cta_inverse_add, k_recon.cuh:140-197); writes prediction + residual into the plane
 template <int BD, typename Px>
-__device__ void rc_reconstruct(int txSz, int txType, int16_t *q, int dcQ, int acQ, const ResFn<Px> &rf, Px *dst, int pitch, int32_t *buf) {
+__device__ void rc_reconstruct(int txSz, int txType, int16_t *q, int dcQ, int acQ, const Px *pred, Px *dst, int pitch, int32_t *buf) {
     const int lane = lane_id();
     const int W = txw(txSz), H = txh(txSz), n = min(W, 32) * min(H, 32), TS = W + 1;
     bool any = false;
@@ -71,7 +97,7 @@ __device__ void rc_reconstruct(int txSz, int txType, int16_t *q, int dcQ, int ac
     const int lw = 31 - __clz(W);
     for (int p = lane; p < W * H; p += 32) {
         const int i = p >> lw, j = p & (W - 1);
-        int v = rf.pred(i, j) + (any ? buf[i * TS + j] : 0);
+        int v = (int)pred[p] + (any ? buf[i * TS + j] : 0);
         v = min(max(v, 0), (1 << BD) - 1);
         dst[(size_t)i * pitch + j] = (Px)v;
     }
@@ -79,7 +105,6 @@ __device__ void rc_reconstruct(int txSz, int txType, int16_t *q, int dcQ, int ac
 }
 
 // record a finished tx block: eob, culLevel / dc category into the context maps, the txb entry and its levels
-template <typename Px>
 __device__ int rc_record(const FrameDesc &F, int sb, int plane, int txSz, int txType, int x4, int y4, const int16_t *q, int txbIdx, int coefOff) {
     const int lane = lane_id();
     const int W = txw(txSz), H = txh(txSz), n = min(W, 32) * min(H, 32);
@@ -126,8 +151,9 @@ __device__ __forceinline__ void rc_txb_ctx(const FrameDesc &F, int plane, int tx
     const bool hasAbove = y4 > (tileY4 >> ss), hasLeft = x4 > (tileX4 >> ss);
     const int w = txw(txSz), h = txh(txSz), w4 = w >> 2, h4 = h >> 2;
     const bool a = hasAbove && lane < w4 && x4 + lane < maxX4, l = hasLeft && lane < h4 && y4 + lane < maxY4;
-    const int la = a ? F.cLvl[plane][(size_t)(y4 - 1) * stride + x4 + lane] : 0, da = a ? F.cDc[plane][(size_t)(y4 - 1) * stride + x4 + lane] : 0;
-    const int ll = l ? F.cLvl[plane][(size_t)(y4 + lane) * stride + x4 - 1] : 0, dl = l ? F.cDc[plane][(size_t)(y4 + lane) * stride + x4 - 1] : 0;
+    const uint8_t *Lv = F.cLvl[plane], *Dc = F.cDc[plane];
+    const int la = a ? __ldcg(Lv + (size_t)(y4 - 1) * stride + x4 + lane) : 0, da = a ? __ldcg(Dc + (size_t)(y4 - 1) * stride + x4 + lane) : 0;
+    const int ll = l ? __ldcg(Lv + (size_t)(y4 + lane) * stride + x4 - 1) : 0, dl = l ? __ldcg(Dc + (size_t)(y4 + lane) * stride + x4 - 1) : 0;
     const bool nzA = __any_sync(0xffffffffu, plane ? (la | da) != 0 : la != 0);
     const bool nzL = __any_sync(0xffffffffu, plane ? (ll | dl) != 0 : ll != 0);
     const int dcSign = warp_sum((da == 2) - (da == 1) + (dl == 2) - (dl == 1));
@@ -147,33 +173,43 @@ __device__ __forceinline__ void rc_txb_ctx(const FrameDesc &F, int plane, int tx
 }
 
 template <int BD, typename Px>
-__device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::Warp &Wp, int sb, int sbr, int sbc, int li,
-                        int tR0, int tR1, int tC0, int tC1) {
+__device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li) {
     const int lane = lane_id();
-    const Leaf lf = S.lv[li];
+    const Leaf lf = F.leaves[(size_t)sb * SB_MAX_LEAVES + li];
     const int bsize = lf.bsize;
+    const int sbr = sb / F.sbCols, sbc = sb % F.sbCols;
     const int sbx = sbc * 64, sby = sbr * 64;
     const int x = sbx + lf.x4 * 4, y = sby + lf.y4 * 4, mi_row = y >> 2, mi_col = x >> 2;
     const int bw = bw4(bsize), bh = bh4(bsize);
     const int ss = F.ssx;
-    // ---- wait for the earlier leaves of the neighbourhood ----
+    const uint8_t *ordmap = F.ordmap + (size_t)sb * 256;
+    int tc = 0, tr = 0;
+    while (tc + 1 < F.tileCols && mi_col >= F.tileColStart[tc + 1]) tc++;
+    while (tr + 1 < F.tileRows && mi_row >= F.tileRowStart[tr + 1]) tr++;
+    const int tC0 = F.tileColStart[tc], tC1 = F.tileColStart[tc + 1], tR0 = F.tileRowStart[tr], tR1 = F.tileRowStart[tr + 1];
+    // ---- wait for the earlier leaves of the neighbourhood (this SB, and the SBs above, above-right and left) ----
     {
-        const int r0 = max(0, lf.y4 - 2), r1 = min(16, lf.y4 + max(2 * bh, 4));
-        const int c0 = max(0, lf.x4 - 2), c1 = min(16, lf.x4 + max(2 * bw, 4));
+        const int r0 = lf.y4 - 2, r1 = min(16, lf.y4 + max(2 * bh, 4));
+        const int c0 = lf.x4 - 2, c1 = lf.x4 + max(2 * bw, 4);
         const int nc = c1 - c0, nu = (r1 - r0) * nc;
         bool ok = true;
         for (int u = lane; u < nu; u += 32) {
-            const int o = S.ordmap[r0 + u / nc][c0 + u % nc];
-            if (o < li) {
-                int it = 0;
-                while (!*(volatile int *)&S.leafDone[o]) {
-                    if (++it > LEAF_WAIT_ITERS || *(volatile int *)F.err) { ok = false; break; }
-                    __nanosleep(32);
-                }
+            const int yy = r0 + u / nc, xx = c0 + u % nc;
+            const int Y = sbr * 16 + yy, X = sbc * 16 + xx;        // luma 4x4 unit, frame coordinates
+            if (Y < tR0 || X < tC0 || X >= tC1 || Y >= F.MiRows || X >= F.MiCols) continue;   // outside the tile / frame
+            if (yy >= 0 && xx >= 16) continue;                      // the SB to the right: decoded later
+            int osb = sb, oy = yy, ox = xx;
+            if (yy < 0 || xx < 0 || xx >= 16) { osb = (Y >> 4) * F.sbCols + (X >> 4); oy = Y & 15; ox = X & 15; }
+            const int o = F.ordmap[(size_t)osb * 256 + oy * 16 + ox];
+            if (o == 255 || (osb == sb && o >= li)) continue;
+            const int *flag = F.leafDone + (size_t)osb * SB_MAX_LEAVES + o;
+            int it = 0;
+            while (!ld_acquire(flag)) {
+                if (++it > LEAF_WAIT_ITERS || *(volatile int *)F.err) { ok = false; break; }
+                __nanosleep(64);
             }
         }
         if (!__all_sync(0xffffffffu, ok) && lane == 0) atomicExch(F.err, KERR_WAIT_LEAF);
-        __threadfence_block();
         __syncwarp();
     }
     const int availU = mi_row - 1 >= tR0, availL = mi_col - 1 >= tC0;
@@ -181,7 +217,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
     const int availUC = (ss && bh == 1) ? (mi_row - 2 >= tR0) : availU;
     const int availLC = (ss && bw == 1) ? (mi_col - 2 >= tC0) : availL;
     const uint16_t *C = g_cost[F.qctx];
-    const int txbBase = S.leafTxb[li], coefBase = S.leafCoef[li];
+    const int txbBase = F.leafTxb[(size_t)sb * SB_MAX_LEAVES + li], coefBase = F.leafCoef[(size_t)sb * SB_MAX_LEAVES + li];
     // BlockDecoded of a 4x4 unit (SB-relative, plane units; ps = 0 luma, ss chroma) for this leaf
     auto decoded = [&](int ps, int yy, int xx) -> bool {
         const int sz = 16 >> ps;
@@ -189,7 +225,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
         if (yy < 0) return xx < sbW4;
         if (xx < 0) return yy < sbH4 && yy != sz;
         if (yy >= sz || xx >= sz) return false;
-        const int o = ps ? S.ordmap[(yy << ps) + 1][(xx << ps) + 1] : S.ordmap[yy][xx];
+        const int o = ps ? ordmap[((yy << ps) + 1) * 16 + (xx << ps) + 1] : ordmap[yy * 16 + xx];
         return o < li;
     };
     // ================= luma =================
@@ -199,15 +235,14 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
         const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
         const int haveAR = decoded(0, lf.y4 - 1, lf.x4 + (W >> 2)), haveBL = decoded(0, lf.y4 + (H >> 2), lf.x4 - 1);
         Px *A = Wp.ea[0] + EDGE_OFF, *L = Wp.el[0] + EDGE_OFF;
-        const Px *rec = (const Px *)F.rec[0];
-        build_edges<BD>(rec, F.rpitch[0], x, y, W, H, availL, availU, haveAR, haveBL, F.MiCols * 4 - 1, F.MiRows * 4 - 1, A, L, lane, 32);
+        rec_edges<BD>((const Px *)F.rec[0], F.rpitch[0], x, y, W, H, availL, availU, haveAR, haveBL, F.MiCols * 4 - 1, F.MiRows * 4 - 1, A, L);
         __syncwarp();
         const int dcv = warp_dc<BD>(A, L, availL, availU, lw, lh);
         const BlockRes br = F.blk[F.shOff[bsize] + (uint32_t)(y / H) * F.shNbx[bsize] + x / W];
         int skipCtx, dcCtx;
         rc_txb_ctx(F, 0, txSz, x >> 2, y >> 2, bsize, tC0, tR0, &skipCtx, &dcCtx);
-        const int am = AV1G_T(Intra_Mode_Context)[availU ? F.mYMode[(size_t)(mi_row - 1) * F.MiCols + mi_col] : AV1G_DC_PRED];
-        const int lm = AV1G_T(Intra_Mode_Context)[availL ? F.mYMode[(size_t)mi_row * F.MiCols + mi_col - 1] : AV1G_DC_PRED];
+        const int am = AV1G_T(Intra_Mode_Context)[availU ? __ldcg(F.mYMode + (size_t)(mi_row - 1) * F.MiCols + mi_col) : AV1G_DC_PRED];
+        const int lm = AV1G_T(Intra_Mode_Context)[availL ? __ldcg(F.mYMode + (size_t)mi_row * F.MiCols + mi_col - 1) : AV1G_DC_PRED];
         auto mbits = [&](int c) -> int {
             const int m = cand_mode(c);
             int b = C[ci_y_mode(am, lm) + m];
@@ -215,43 +250,45 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
             return b;
         };
         const Px *src = (const Px *)F.src[0] + (size_t)y * F.spitch[0] + x;
-        auto rfOf = [&](int c) {
-            const int m = cand_mode(c);
-            return res_mode<Px>(src, F.spitch[0], A, L, m, cand_delta(c), lw, lh, dcv);
-        };
         const int set = tx_set_intra(txSz);
         const int G = grp_size(txSz), ng = 32 / G, grp = lane / G, g = lane & (G - 1);
         const int nq = min(W, 32) * min(H, 32);
         int32_t *tb = Wp.buf + grp * task_buf_ints(txSz);
         int16_t *tq = Wp.q + grp * nq;
+        Px *tp = Wp.pred + grp * (W * H);
         int16_t *best = Wp.qb[0];
+        if (lane < 8) Wp.predC[lane] = -1;
+        __syncwarp();
         i64 bestJ = INF;
         int bestC = br.cand[0], bestT = br.tx;
         bool have = false;
         // tasks (candidate, tx type) in rounds of 32 / G; costs compared in task order (first of equal costs wins);
         // the round's winner, if it beats the best so far, leaves its levels in `best`
-        auto run = [&](const int *tc, const int *tt, int n) {
+        auto run = [&](const int *tcand, const int *ttype, int n) {
             for (int r0 = 0; r0 < n; r0 += ng) {
                 const int k = min(r0 + grp, n - 1);
-                const int c = tc[k], t = tt[k];
-                const EvalIn e{t, 0, skipCtx, dcCtx, cand_mode(c), F.dcQ, F.acQ, C};
-                const EvalOut o = grp_eval<BD, Px>(txSz, rfOf(c), e, tb, tq, g, G);
+                const int c = tcand[k], t = ttype[k], m = cand_mode(c);
+                if (Wp.predC[grp] != c) grp_predict(m, pangle(m, cand_delta(c)), lw, lh, A, L, dcv, tp, g, G);
+                __syncwarp();
+                if (g == 0) Wp.predC[grp] = c;
+                const EvalIn e{t, 0, skipCtx, dcCtx, m, F.dcQ, F.acQ, C};
+                const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{src, F.spitch[0], tp, lw, nullptr}, e, tb, tq, g, G);
                 if (g == 0 && r0 + grp < n) Wp.taskJ[grp] = o.D + F.lam * (o.R + mbits(c));
                 __syncwarp();
                 int win = -1;
                 for (int u = 0; u < ng && r0 + u < n; u++)
-                    if (Wp.taskJ[u] < bestJ) { bestJ = Wp.taskJ[u]; bestC = tc[r0 + u]; bestT = tt[r0 + u]; win = u; have = true; }
+                    if (Wp.taskJ[u] < bestJ) { bestJ = Wp.taskJ[u]; bestC = tcand[r0 + u]; bestT = ttype[r0 + u]; win = u; have = true; }
                 if (win >= 0)
                     for (int i = lane; i < nq; i += 32) best[i] = Wp.q[win * nq + i];
                 __syncwarp();
             }
         };
         const int nc = max(1, min((int)br.ncand, K_RECHECK));
-        int tc[8], tt[8], n1 = 0;
-        for (int k = 0; k < nc; k++) { tc[n1] = br.cand[k]; tt[n1] = AV1G_DCT_DCT; n1++; }
-        if (br.tx != AV1G_DCT_DCT) { tc[n1] = br.cand[0]; tt[n1] = br.tx; n1++; }
+        int tcand[8], ttype[8], n1 = 0;
+        for (int k = 0; k < nc; k++) { tcand[n1] = br.cand[k]; ttype[n1] = AV1G_DCT_DCT; n1++; }
+        if (br.tx != AV1G_DCT_DCT) { tcand[n1] = br.cand[0]; ttype[n1] = br.tx; n1++; }
         const bool skip1 = n1 == 1;
-        if (!skip1) run(tc, tt, n1);
+        if (!skip1) run(tcand, ttype, n1);
         else { bestC = br.cand[0]; bestT = AV1G_DCT_DCT; }
         if (set != AV1G_TX_SET_DCTONLY) {
             const int c1 = bestC;
@@ -260,20 +297,23 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
             for (int t = 0; t < 16; t++) {
                 if (!tx_in_set(set, t)) continue;
                 if (!skip1 && (t == AV1G_DCT_DCT || (isC0 && t == br.tx))) continue;
-                tc[n2] = c1; tt[n2] = t; n2++;
+                tcand[n2] = c1; ttype[n2] = t; n2++;
             }
-            run(tc, tt, n2);
+            run(tcand, ttype, n2);
         }
-        if (!have) {   // one candidate, DCT only: its levels
-            const EvalIn e{bestT, 0, skipCtx, dcCtx, cand_mode(bestC), F.dcQ, F.acQ, C};
-            grp_eval<BD, Px>(txSz, rfOf(bestC), e, Wp.buf, best, lane, 32);
+        // the winner's prediction (whole warp) for its levels (single-candidate case) and the reconstruction
+        const int bm = cand_mode(bestC);
+        grp_predict(bm, pangle(bm, cand_delta(bestC)), lw, lh, A, L, dcv, Wp.pred, lane, 32);
+        __syncwarp();
+        if (!have) {
+            const EvalIn e{bestT, 0, skipCtx, dcCtx, bm, F.dcQ, F.acQ, C};
+            grp_eval<BD, Px>(txSz, ResFn<Px>{src, F.spitch[0], Wp.pred, lw, nullptr}, e, Wp.buf, best, lane, 32);
         }
         Px *dst = (Px *)F.rec[0] + (size_t)y * F.rpitch[0] + x;
-        rc_reconstruct<BD, Px>(txSz, bestT, best, F.dcQ, F.acQ, rfOf(bestC), dst, F.rpitch[0], Wp.buf);
-        eobY = rc_record<Px>(F, sb, 0, txSz, bestT, x >> 2, y >> 2, best, txbBase, coefBase);
-        yMode = cand_mode(bestC);
+        rc_reconstruct<BD, Px>(txSz, bestT, best, F.dcQ, F.acQ, Wp.pred, dst, F.rpitch[0], Wp.buf);
+        eobY = rc_record(F, sb, 0, txSz, bestT, x >> 2, y >> 2, best, txbBase, coefBase);
+        yMode = bm;
         yDelta = cand_delta(bestC);
-        // y mode map (the context of later blocks)
         for (int k = lane; k < bw * bh; k += 32) {
             const int r = mi_row + k / bw, c = mi_col + k % bw;
             if (r < F.MiRows && c < F.MiCols) F.mYMode[(size_t)r * F.MiCols + c] = (uint8_t)yMode;
@@ -292,7 +332,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
         int dcv[3];
         for (int pl = 1; pl <= 2; pl++) {
             A[pl] = Wp.ea[pl] + EDGE_OFF; L[pl] = Wp.el[pl] + EDGE_OFF;
-            build_edges<BD>((const Px *)F.rec[pl], F.rpitch[pl], cx, cy, W, H, availLC, availUC, haveAR, haveBL, maxX, maxY, A[pl], L[pl], lane, 32);
+            rec_edges<BD>((const Px *)F.rec[pl], F.rpitch[pl], cx, cy, W, H, availLC, availUC, haveAR, haveBL, maxX, maxY, A[pl], L[pl]);
         }
         __syncwarp();
         for (int pl = 1; pl <= 2; pl++) dcv[pl] = warp_dc<BD>(A[pl], L[pl], availLC, availUC, lw, lh);
@@ -317,9 +357,10 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
                 int v;
                 if (ss) {
                     const int ly = min((cy + i) << 1, maxLumaH - 2), lx = min((cx + j) << 1, maxLumaW - 2);
-                    v = (luma[(size_t)ly * lp + lx] + luma[(size_t)ly * lp + lx + 1] + luma[(size_t)(ly + 1) * lp + lx] + luma[(size_t)(ly + 1) * lp + lx + 1]) << 1;
+                    v = ((int)ldcg(luma + (size_t)ly * lp + lx) + ldcg(luma + (size_t)ly * lp + lx + 1) + ldcg(luma + (size_t)(ly + 1) * lp + lx) +
+                         ldcg(luma + (size_t)(ly + 1) * lp + lx + 1)) << 1;
                 } else {
-                    v = luma[(size_t)min(cy + i, maxLumaH - 1) * lp + min(cx + j, maxLumaW - 1)] << 3;
+                    v = (int)ldcg(luma + (size_t)min(cy + i, maxLumaH - 1) * lp + min(cx + j, maxLumaW - 1)) << 3;
                 }
                 Wp.cfl[p] = (int16_t)v;
                 sum += v;
@@ -373,13 +414,13 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
                 if (it < items) {
                     const int r = it % nsub2, pl = 1 + (r >= (nsub2 >> 1)), sbk = r % (nsub2 >> 1);
                     const int sx = (sbk % nsx) * 4, sy = (sbk / nsx) * 4;
-                    const int c = Wp.cand[ci], m = cand_mode(c), pa = pangle(m, cand_delta(c));
+                    const int c = Wp.cand[ci], m = cand_mode(c);
                     int d[16];
+                    pred4(m, pangle(m, cand_delta(c)), sy, sx, lw, lh, A[pl], L[pl], dcv[pl], d);
 #pragma unroll
                     for (int i = 0; i < 4; i++)
 #pragma unroll
-                        for (int j = 0; j < 4; j++)
-                            d[i * 4 + j] = (int)sP[pl][(sy + i) * F.spitch[pl] + sx + j] - pred_px(m, pa, sy + i, sx + j, lw, lh, A[pl], L[pl], dcv[pl]);
+                        for (int j = 0; j < 4; j++) d[i * 4 + j] = (int)sP[pl][(sy + i) * F.spitch[pl] + sx + j] - d[i * 4 + j];
                     t = hadamard4_sum(d);
                 }
                 for (int o = 16; o > 0; o >>= 1)
@@ -410,9 +451,10 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
         if (cflAllowed && (alpha[1] || alpha[2])) chosen[nch++] = 255;
         int skipCtx[3], dcCtx[3];
         for (int pl = 1; pl <= 2; pl++) rc_txb_ctx(F, pl, txSz, cx4, cy4, bsize, tC0, tR0, &skipCtx[pl], &dcCtx[pl]);
-        auto rfOf = [&](int pl, int c) {
-            if (c == 255) return res_cfl<Px>(sP[pl], F.spitch[pl], lw, lh, dcv[pl], Wp.cfl, alpha[pl], cflAvg, (1 << BD) - 1);
-            return res_mode<Px>(sP[pl], F.spitch[pl], A[pl], L[pl], cand_mode(c), cand_delta(c), lw, lh, dcv[pl]);
+        // prediction of (plane, candidate) by a group of G lanes into out
+        auto predict = [&](int pl, int c, Px *out, int g, int G) {
+            if (c == 255) grp_predict_cfl(lw, lh, dcv[pl], Wp.cfl, alpha[pl], cflAvg, (1 << BD) - 1, out, g, G);
+            else grp_predict(cand_mode(c), pangle(cand_mode(c), cand_delta(c)), lw, lh, A[pl], L[pl], dcv[pl], out, g, G);
         };
         // (candidate, plane) tasks in rounds of 32 / G; each candidate's cost = U + V + lambda * its mode bits; the
         // winner's two planes are evaluated once more for their levels
@@ -420,13 +462,16 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
         const int nq = min(W, 32) * min(H, 32);
         int32_t *tb = Wp.buf + grp * task_buf_ints(txSz);
         int16_t *tq = Wp.q + grp * nq;
+        Px *tp = Wp.pred + grp * (W * H);
         i64 pj[2 * (UV_K + 1)];
         const int ntask = 2 * nch;
         for (int r0 = 0; r0 < ntask; r0 += ng) {
             const int k = min(r0 + grp, ntask - 1), c = chosen[k >> 1], pl = 1 + (k & 1);
+            predict(pl, c, tp, g, G);
+            __syncwarp();
             const int txType = chroma_tx_type(txSz, c == 255 ? AV1G_UV_CFL_PRED : cand_mode(c));
             const EvalIn e{txType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, C};
-            const EvalOut o = grp_eval<BD, Px>(txSz, rfOf(pl, c), e, tb, tq, g, G);
+            const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{sP[pl], F.spitch[pl], tp, lw, nullptr}, e, tb, tq, g, G);
             if (g == 0 && r0 + grp < ntask) Wp.taskJ[grp] = o.D + F.lam * o.R;
             __syncwarp();
             for (int u = 0; u < ng && r0 + u < ntask; u++) pj[r0 + u] = Wp.taskJ[u];
@@ -450,30 +495,21 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
             J += F.lam * b;
             if (J < bJ) { bJ = J; bestC = c; }
         }
-        int16_t *best[2] = {Wp.qb[0], Wp.qb[1]};
-        {   // the winner's U and V levels (two tasks: one round when the warp holds two groups)
-            const int ntk = 2;
-            for (int r0 = 0; r0 < ntk; r0 += ng) {
-                const int k = min(r0 + grp, ntk - 1), pl = 1 + k;
-                const int txType = chroma_tx_type(txSz, bestC == 255 ? AV1G_UV_CFL_PRED : cand_mode(bestC));
-                const EvalIn e{txType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, C};
-                grp_eval<BD, Px>(txSz, rfOf(pl, bestC), e, tb, tq, g, G);
-                __syncwarp();
-                for (int u = 0; u < ng && r0 + u < ntk; u++)
-                    for (int i = lane; i < nq; i += 32) best[r0 + u][i] = Wp.q[u * nq + i];
-                __syncwarp();
-            }
-        }
         const bool cfl = bestC == 255;
         uv = cfl ? AV1G_UV_CFL_PRED : cand_mode(bestC);
         const int uvType = chroma_tx_type(txSz, uv);
         for (int pl = 1; pl <= 2; pl++) {
+            predict(pl, bestC, Wp.pred, lane, 32);
+            __syncwarp();
+            const EvalIn e{uvType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, C};
+            int16_t *lv = Wp.qb[pl - 1];
+            grp_eval<BD, Px>(txSz, ResFn<Px>{sP[pl], F.spitch[pl], Wp.pred, lw, nullptr}, e, Wp.buf, lv, lane, 32);
             Px *dst = (Px *)F.rec[pl] + (size_t)cy * F.rpitch[pl] + cx;
-            rc_reconstruct<BD, Px>(txSz, uvType, best[pl - 1], F.dcQ, F.acQ, rfOf(pl, bestC), dst, F.rpitch[pl], Wp.buf);
+            rc_reconstruct<BD, Px>(txSz, uvType, lv, F.dcQ, F.acQ, Wp.pred, dst, F.rpitch[pl], Wp.buf);
             const int yt = AV1G_T(Max_Tx_Size_Rect)[bsize];
-            const int off = coefBase + min(txw(yt), 32) * min(txh(yt), 32) + (pl - 1) * min(W, 32) * min(H, 32);
-            const int e = rc_record<Px>(F, sb, pl, txSz, uvType, cx4, cy4, best[pl - 1], txbBase + pl, off);
-            if (pl == 1) eobU = e; else eobV = e;
+            const int off = coefBase + min(txw(yt), 32) * min(txh(yt), 32) + (pl - 1) * nq;
+            const int e2 = rc_record(F, sb, pl, txSz, uvType, cx4, cy4, lv, txbBase + pl, off);
+            if (pl == 1) eobU = e2; else eobV = e2;
         }
         duv = cfl ? 0 : cand_delta(bestC);
         aU = cfl ? alpha[1] : 0;
@@ -494,90 +530,104 @@ __device__ void rc_leaf(const FrameDesc &F, RcSmem<Px> &S, typename RcSmem<Px>::
         F.oBlocks[(size_t)sb * SB_MAX_LEAVES + li] = b;
         F.oBlockTxb[(size_t)sb * SB_MAX_LEAVES + li] = (uint16_t)txbBase;
     }
-    __threadfence_block();
     __syncwarp();
-    if (lane == 0) *(volatile int *)&S.leafDone[li] = 1;
+    if (lane == 0) {
+        __threadfence();
+        st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 1);
+    }
 }
 
+// persistent grid of independent warps over the global leaf queue
 template <int BD>
-__global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__restrict__ Fp, int nSb) {
+__global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__restrict__ Fp) {
     typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RcSmem<Px> &S = *reinterpret_cast<RcSmem<Px> *>(smem_raw);
     const FrameDesc &F = *Fp;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    RcWarp<Px> &Wp = S.w[threadIdx.x >> 5];
+    const int lane = lane_id();
+    const uint32_t total = *F.leafTotal;
     for (;;) {
-        if (tid == 0) S.sbIdx = atomicAdd(F.queue, 1);
-        __syncthreads();
-        const int idx = S.sbIdx;
-        if (idx >= nSb) break;
-        const int sb = (int)F.sbOrder[idx], sbr = sb / F.sbCols, sbc = sb % F.sbCols;
-        int tc = 0, tr = 0;
-        while (tc + 1 < F.tileCols && sbc * 16 >= F.tileColStart[tc + 1]) tc++;
-        while (tr + 1 < F.tileRows && sbr * 16 >= F.tileRowStart[tr + 1]) tr++;
-        const int tC0 = F.tileColStart[tc], tC1 = F.tileColStart[tc + 1], tR0 = F.tileRowStart[tr], tR1 = F.tileRowStart[tr + 1];
-        // wait for the left and the above-right (above at the tile's right edge) SBs of the same tile
-        if (tid == 0) {
-            const int sbC0 = tC0 >> 4, sbR0 = tR0 >> 4, sbC1 = (tC1 + 15) >> 4;
-            int dep[2], nd = 0;
-            if (sbc > sbC0) dep[nd++] = sb - 1;
-            if (sbr > sbR0) dep[nd++] = (sbr - 1) * F.sbCols + min(sbc + 1, sbC1 - 1);
-            for (int k = 0; k < nd; k++) {
-                int it = 0;
-                while (!ld_acquire(F.sbDone + dep[k])) {
-                    if (++it > SB_WAIT_ITERS) { atomicExch(F.err, KERR_WAIT_SB); break; }
-                    if (*(volatile int *)F.err) break;
-                    __nanosleep(128);
-                }
-            }
-        }
-        // leaves, the 4x4 leaf-index map, per-leaf output offsets
-        const int nl = F.nLeaves[sb];
-        if (tid < 256) { S.ordmap[tid >> 4][tid & 15] = 255; S.leafDone[tid] = 0; }
-        if (tid < nl) S.lv[tid] = F.leaves[(size_t)sb * SB_MAX_LEAVES + tid];
-        __syncthreads();
-        if (tid < nl) {
-            const Leaf l = S.lv[tid];
-            const int w4 = bw4(l.bsize), h4 = bh4(l.bsize);
-            for (int r = l.y4; r < min(16, l.y4 + h4); r++)
-                for (int c = l.x4; c < min(16, l.x4 + w4); c++) S.ordmap[r][c] = (uint8_t)tid;
-        }
-        if (tid == 0) {
-            int nt = 0, ncf = 0;
-            for (int i = 0; i < nl; i++) {
-                S.leafTxb[i] = (uint16_t)nt;
-                S.leafCoef[i] = (uint16_t)ncf;
-                const Leaf l = S.lv[i];
-                const int yt = AV1G_T(Max_Tx_Size_Rect)[l.bsize];
-                nt += 1;
-                ncf += min(txw(yt), 32) * min(txh(yt), 32);
-                if (has_chroma(l.bsize, sbr * 16 + l.y4, sbc * 16 + l.x4, F.ssx)) {
-                    const int ut = uv_tx_size(l.bsize, F.ssx);
-                    nt += 2;
-                    ncf += 2 * min(txw(ut), 32) * min(txh(ut), 32);
-                }
-            }
-            S.leafTxb[nl] = (uint16_t)nt;
-            S.leafCoef[nl] = (uint16_t)ncf;
-            S.next = RC_WARPS;
-        }
-        __syncthreads();
-        int li = warp;
-        while (li < nl) {
-            rc_leaf<BD, Px>(F, S, S.w[warp], sb, sbr, sbc, li, tR0, tR1, tC0, tC1);
-            int n = 0;
-            if (lane == 0) n = atomicAdd(&S.next, 1);
-            li = __shfl_sync(0xffffffffu, n, 0);
-        }
-        __syncthreads();
-        if (tid == 0) {
-            SbCount c;
-            c.nBlocks = (uint32_t)nl; c.nTxb = S.leafTxb[nl]; c.nCoeffs = S.leafCoef[nl]; c.pad = 0;
-            F.sbCount[sb] = c;
-            __threadfence();
-            st_release(F.sbDone + sb, 1);
-        }
+        if (lane == 0) Wp.job = atomicAdd(F.queue, 1);
+        __syncwarp();
+        const uint32_t qi = (uint32_t)Wp.job;
+        __syncwarp();
+        if (qi >= total) break;
+        const uint32_t e = F.leafQueue[qi];
+        rc_leaf<BD, Px>(F, Wp, (int)(e >> 8), (int)(e & 255));
     }
+}
+
+// ---- before the closed loop: per SB the map of leaf indices, per leaf its first tx block and coefficient (SB-local),
+// per SB the output counts; then the global leaf queue (SBs in wavefront order, leaves in decode order) ----
+__global__ void k_leaf_prep(const FrameDesc *__restrict__ Fp, int nSb) {
+    const FrameDesc &F = *Fp;
+    const int sb = blockIdx.x, tid = threadIdx.x;
+    if (sb >= nSb) return;
+    __shared__ uint8_t om[256];
+    const int nl = F.nLeaves[sb];
+    om[tid] = 255;
+    F.leafDone[(size_t)sb * SB_MAX_LEAVES + tid] = 0;
+    __syncthreads();
+    if (tid < nl) {
+        const Leaf l = F.leaves[(size_t)sb * SB_MAX_LEAVES + tid];
+        const int w4 = bw4(l.bsize), h4 = bh4(l.bsize);
+        for (int r = l.y4; r < min(16, l.y4 + h4); r++)
+            for (int c = l.x4; c < min(16, l.x4 + w4); c++) om[r * 16 + c] = (uint8_t)tid;
+    }
+    __syncthreads();
+    F.ordmap[(size_t)sb * 256 + tid] = om[tid];
+    if (tid == 0) {
+        const int sbr = sb / F.sbCols, sbc = sb % F.sbCols;
+        int nt = 0, ncf = 0;
+        for (int i = 0; i < nl; i++) {
+            F.leafTxb[(size_t)sb * SB_MAX_LEAVES + i] = (uint16_t)nt;
+            F.leafCoef[(size_t)sb * SB_MAX_LEAVES + i] = (uint16_t)ncf;
+            const Leaf l = F.leaves[(size_t)sb * SB_MAX_LEAVES + i];
+            const int yt = AV1G_T(Max_Tx_Size_Rect)[l.bsize];
+            nt += 1;
+            ncf += min(txw(yt), 32) * min(txh(yt), 32);
+            if (has_chroma(l.bsize, sbr * 16 + l.y4, sbc * 16 + l.x4, F.ssx)) {
+                const int ut = uv_tx_size(l.bsize, F.ssx);
+                nt += 2;
+                ncf += 2 * min(txw(ut), 32) * min(txh(ut), 32);
+            }
+        }
+        SbCount c;
+        c.nBlocks = (uint32_t)nl; c.nTxb = (uint32_t)nt; c.nCoeffs = (uint32_t)ncf; c.pad = 0;
+        F.sbCount[sb] = c;
+    }
+}
+// exclusive prefix of the leaf counts over the wavefront order (one CTA of 1024 threads), then every SB's leaves into
+// the queue
+__global__ void k_leaf_queue_scan(const FrameDesc *__restrict__ Fp, int nSb) {
+    const FrameDesc &F = *Fp;
+    __shared__ uint32_t sN[1024];
+    const int tid = threadIdx.x;
+    const int per = (nSb + 1023) / 1024, i0 = min(nSb, tid * per), i1 = min(nSb, i0 + per);
+    uint32_t n = 0;
+    for (int i = i0; i < i1; i++) n += F.nLeaves[F.sbOrder[i]];
+    sN[tid] = n;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const uint32_t v = tid >= o ? sN[tid - o] : 0;
+        __syncthreads();
+        sN[tid] += v;
+        __syncthreads();
+    }
+    uint32_t at = sN[tid] - n;
+    for (int i = i0; i < i1; i++) {
+        const uint32_t sb = F.sbOrder[i];
+        F.leafStart[sb] = at;
+        at += F.nLeaves[sb];
+    }
+    if (tid == 1023) *F.leafTotal = sN[1023];
+}
+__global__ void k_leaf_queue_fill(const FrameDesc *__restrict__ Fp, int nSb) {
+    const FrameDesc &F = *Fp;
+    const int sb = blockIdx.x, tid = threadIdx.x;
+    if (sb >= nSb) return;
+    if (tid < F.nLeaves[sb]) F.leafQueue[F.leafStart[sb] + tid] = ((uint32_t)sb << 8) | (uint32_t)tid;
 }
 
 // ---- pack: per-SB slots -> DecisionRecord arrays in decode order ----
