@@ -200,6 +200,9 @@ struct is_handle {
     uint64_t nCoeffs = 0;
     int qidx = 0;
     is_times times;
+    bool trace = false;
+    unsigned long long *traceBuf = nullptr;
+    size_t traceCap = 0;
     cudaEvent_t ev[6];
     void *hostSmall = nullptr;   // pinned 64 bytes for the counts / error readback
     int setErr(int code, const char *fmt, ...) {
@@ -298,6 +301,7 @@ size_t layout(int W, int H, uint8_t *base, FrameDesc &F, int &nSb) {
     F.leafStart = (uint32_t *)take((size_t)nSb * 4);
     F.leafQueue = (uint32_t *)take((size_t)nSb * SB_MAX_LEAVES * 4);
     F.leafTotal = (uint32_t *)take(4);
+    F.leafTrace = nullptr;   // set per encode when tracing is on (is_set_trace)
     F.queue = (int *)take(4);
     F.err = (int *)take(4);
     F.sbDecodeOrder = (uint32_t *)take((size_t)nSb * 4);
@@ -360,6 +364,7 @@ void is_destroy(is_handle *h) {
     if (h->own) cudaStreamDestroy(h->own);
     if (h->hostSmall) cudaFreeHost(h->hostSmall);
     if (h->hFpinned) cudaFreeHost(h->hFpinned);
+    if (h->traceBuf) cudaFree(h->traceBuf);
     delete h;
 }
 
@@ -412,6 +417,15 @@ static int prepare(is_handle *h, const is_frame *f) {
         IS_CK(cudaMemcpy(F.sbDecodeOrder, dec.data(), dec.size() * 4, cudaMemcpyHostToDevice));
         h->geomW = f->width;
         h->geomH = f->height;
+    }
+    if (h->trace) {
+        const size_t need = (size_t)nSb * SB_MAX_LEAVES * 4;
+        if (need > h->traceCap) {
+            if (h->traceBuf) cudaFree(h->traceBuf);
+            IS_CK(cudaMalloc(&h->traceBuf, need * 8));
+            h->traceCap = need;
+        }
+        F.leafTrace = h->traceBuf;
     }
     h->F = F;
     h->nSb = nSb;

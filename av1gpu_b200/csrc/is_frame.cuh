@@ -59,6 +59,7 @@ struct FrameDesc {
     uint32_t *leafTotal;                      // [1] leaves in the queue
     int *queue;                               // [1] next queue position
     int *err;                                 // [1] error status (0 = ok)
+    unsigned long long *leafTrace;            // [leaves * 4] optional (debug): claimed / ready / luma done / done (ns)
     // pack output (DecisionRecord arrays in decode order) and per-SB offsets
     uint32_t *sbDecodeOrder;                  // [nSb] SBs in decode order (tiles raster, SB raster inside a tile)
     uint32_t *offBlk, *offTxb;                // [nSb + 1] exclusive prefix sums in decode order

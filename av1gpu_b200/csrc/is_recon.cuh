@@ -172,8 +172,14 @@ __device__ __forceinline__ void rc_txb_ctx(const FrameDesc &F, int plane, int tx
     }
 }
 
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
 template <int BD, typename Px>
-__device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li) {
+__device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li, unsigned long long *trace) {
     const int lane = lane_id();
     const Leaf lf = F.leaves[(size_t)sb * SB_MAX_LEAVES + li];
     const int bsize = lf.bsize;
@@ -212,6 +218,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li) {
         if (!__all_sync(0xffffffffu, ok) && lane == 0) atomicExch(F.err, KERR_WAIT_LEAF);
         __syncwarp();
     }
+    if (trace && lane == 0) trace[1] = gtimer();
     const int availU = mi_row - 1 >= tR0, availL = mi_col - 1 >= tC0;
     const bool hasC = has_chroma(bsize, mi_row, mi_col, ss);
     const int availUC = (ss && bh == 1) ? (mi_row - 2 >= tR0) : availU;
@@ -319,6 +326,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li) {
             if (r < F.MiRows && c < F.MiCols) F.mYMode[(size_t)r * F.MiCols + c] = (uint8_t)yMode;
         }
     }
+    if (trace && lane == 0) trace[2] = gtimer();
     // ================= chroma =================
     int uv = 0, duv = 0, aU = 0, aV = 0, eobU = 0, eobV = 0;
     if (hasC) {
@@ -534,6 +542,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li) {
     if (lane == 0) {
         __threadfence();
         st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 1);
+        if (trace) trace[3] = gtimer();
     }
 }
 
@@ -554,7 +563,9 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
         __syncwarp();
         if (qi >= total) break;
         const uint32_t e = F.leafQueue[qi];
-        rc_leaf<BD, Px>(F, Wp, (int)(e >> 8), (int)(e & 255));
+        unsigned long long *trace = F.leafTrace ? F.leafTrace + (size_t)qi * 4 : nullptr;
+        if (trace && lane == 0) trace[0] = gtimer();
+        rc_leaf<BD, Px>(F, Wp, (int)(e >> 8), (int)(e & 255), trace);
     }
 }
 

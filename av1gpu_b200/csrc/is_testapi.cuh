@@ -243,3 +243,19 @@ extern "C" int is_probe_int32(int device, double *gops, float *ms) {
     *ms = best;
     return IS_OK;
 }
+
+// ---- closed-loop trace (debug): per queued leaf the globaltimer at claim, dependencies ready, luma done, done ----
+extern "C" int is_set_trace(is_handle *h, int on) {
+    if (!h) return IS_ERR_INVALID;
+    h->trace = on != 0;
+    return IS_OK;
+}
+extern "C" int is_get_trace(is_handle *h, unsigned long long *out, size_t cap, uint32_t *n) {
+    if (!h || !h->have || !h->F.leafTrace) return IS_ERR_STATE;
+    uint32_t tot = 0;
+    IS_CK(cudaMemcpy(&tot, h->F.leafTotal, 4, cudaMemcpyDeviceToHost));
+    *n = tot;
+    const size_t m = std::min(cap, (size_t)tot * 4);
+    IS_CK(cudaMemcpy(out, h->F.leafTrace, m * 8, cudaMemcpyDeviceToHost));
+    return IS_OK;
+}

@@ -44,7 +44,7 @@ class IsTimes(C.Structure):
 # every entry point declared in include/is_api.h
 EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_encode_host", "is_record_counts",
            "is_record_copy", "is_record_device", "is_times_get", "is_test_fwd_quant", "is_test_inverse",
-           "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32"]
+           "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32", "is_set_trace", "is_get_trace"]
 
 _lib = None
 
@@ -77,6 +77,8 @@ def load_library():
     L.is_debug_tables.argtypes = [vp, C.c_int, vp, C.c_size_t, vp, vp, vp, C.c_int, C.POINTER(C.c_int64),
                                   C.POINTER(C.c_int64)]
     L.is_probe_int32.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]
+    L.is_set_trace.argtypes = [C.c_void_p, C.c_int]
+    L.is_get_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32)]
     _lib = L
     return L
 
@@ -239,6 +241,17 @@ class Encoder:
         nc, tx = np.zeros(n, np.uint8), np.zeros(n, np.uint8)
         self.L.is_debug_analysis(self.h, bsize, J.ctypes.data, cand.ctypes.data, nc.ctypes.data, tx.ctypes.data)
         return J, cand, nc, tx
+
+    def set_trace(self, on=True):
+        self._check(self.L.is_set_trace(self.h, 1 if on else 0), "is_set_trace")
+
+    def trace(self):
+        """Per queued leaf of the last encode: (claimed, ready, luma done, done) globaltimer ns, queue order."""
+        nb, _, _ = self.counts()
+        out = np.zeros(nb * 4 + 4, np.uint64)
+        n = C.c_uint32()
+        self._check(self.L.is_get_trace(self.h, out.ctypes.data, out.size, C.byref(n)), "is_get_trace")
+        return out[:n.value * 4].reshape(-1, 4)
 
     def debug_leaves(self, sb):
         b, x, y = (np.zeros(256, np.uint8) for _ in range(3))

@@ -103,6 +103,12 @@ int is_debug_leaves(is_handle *h, uint32_t sb, uint8_t *bsize, uint8_t *x4, uint
 int is_debug_tables(is_handle *h, int qctx, uint16_t *cost, size_t cap, int32_t *avgY13, int32_t *avgPart50,
                     int32_t *avgSkip0, int qindex, int64_t *lam, int64_t *sqrtlam);
 
+/* Closed-loop trace (debug): is_set_trace(h, 1) before an encode records, per queued leaf, the globaltimer (ns) when a
+ * warp claimed it, when its dependencies were ready, when its luma was done and when it was done; is_get_trace copies
+ * n x 4 values (queue order). */
+int is_set_trace(is_handle *h, int on);
+int is_get_trace(is_handle *h, unsigned long long *out, size_t cap, uint32_t *n);
+
 /* INT32 issue-rate probe: the measured INT32 instruction throughput of the device (Gop/s, multiply-add + logic chains
  * over every SM) and the best kernel time, the roofline denominator of this integer path. */
 int is_probe_int32(int device, double *gops, float *ms);
