@@ -75,7 +75,8 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
     __syncwarp();
     const int dcv = warp_dc<BD>(A, L, haveL, haveA, lw, lh);
     const Px *src = tile + ly * TW + lx;
-    const uint16_t *C = g_cost[F.qctx];
+    const RateTabs T = rate_tabs_global(F.qctx);
+    const uint16_t *C = T.cost;
     auto mbits = [&](int c) -> int {
         const int m = cand_mode(c);
         int b = c_avgY[m];
@@ -151,7 +152,7 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
         if (S.predC[grp] != c) grp_predict(m, pangle(m, cand_delta(c)), lw, lh, A, L, dcv, tp, g, G);
         __syncwarp();
         if (g == 0) S.predC[grp] = c;
-        const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, C};
+        const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, T};
         return grp_eval<BD, Px>(txSz, ResFn<Px>{src, TW, tp, lw, nullptr}, e, tb, tq, g, G);
     };
     i64 bestJ = INF;

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "is_api.h"
+#include "av1g/dsp.h"
 #include "is_dev.cuh"
 #include "is_frame.cuh"
 #include "is_analysis.cuh"
@@ -238,6 +239,31 @@ int upload_tables(int dev) {
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgY, T.avgY, sizeof T.avgY);
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgPart, T.avgPart, sizeof T.avgPart);
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgSkip0, &T.avgSkip0, sizeof T.avgSkip0);
+        // scans packed per (tx size, class), one copy of each distinct table; the 2-D base-context offsets
+        std::vector<uint16_t> pack;
+        std::vector<const uint16_t *> seen;
+        std::vector<uint16_t> seenOff;
+        uint16_t off[19][3];
+        for (int t = 0; t < 19; t++) {
+            const int n = std::min<int>(AV1G_T(Tx_Width)[t], 32) * std::min<int>(AV1G_T(Tx_Height)[t], 32);
+            const bool oneD = AV1G_T(Tx_Width)[t] <= 16 && AV1G_T(Tx_Height)[t] <= 16;
+            const int types[3] = {AV1G_DCT_DCT, AV1G_H_DCT, AV1G_V_DCT};   // class 2D, HORIZ, VERT
+            for (int c = 0; c < 3; c++) {
+                const uint16_t *sc = av1g_get_scan(t, (c == 0 || !oneD) ? AV1G_DCT_DCT : types[c]);
+                size_t k = 0;
+                while (k < seen.size() && seen[k] != sc) k++;
+                if (k == seen.size()) {
+                    seen.push_back(sc);
+                    seenOff.push_back((uint16_t)pack.size());
+                    pack.insert(pack.end(), sc, sc + n);
+                }
+                off[t][c] = seenOff[k];
+            }
+        }
+        if (e == cudaSuccess) e = pack.size() == (size_t)SCAN_PACK ? cudaMemcpyToSymbol(g_scanPack, pack.data(), pack.size() * 2)
+                                                                  : cudaErrorInvalidValue;
+        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_scanOff, off, sizeof off);
+        if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_baseCtx, &AV1G_T(Coeff_Base_Ctx_Offset)[0][0][0], 19 * 25);
         if (e == cudaSuccess && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3) {
             e = cudaMemcpyToSymbol(c_anTask, tasks.data(), tasks.size());
             if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anTaskBig, tasksBig.data(), tasksBig.size());

@@ -38,6 +38,33 @@ __constant__ int c_avgY[13];           // y_mode bits averaged over its 25 conte
 __constant__ int c_avgPart[5][10];     // partition bits averaged over contexts, per block-size level
 __constant__ int c_avgSkip0;           // skip = 0 averaged over contexts
 
+// ---- the tables of the rate loop: the cost table of the image's q-context, every scan of the intra tx sizes /
+// classes (packed), the 2-D base-context offsets.  A kernel whose few warps each run a long dependent chain (the
+// closed loop) stages them once per CTA in shared memory (RateStage); the others read them from global memory. ----
+constexpr int SCAN_PACK = 4912;
+__device__ uint16_t g_scanPack[SCAN_PACK];     // the scans, packed (host-built from the spec tables)
+__device__ uint8_t g_baseCtx[19 * 25];         // Coeff_Base_Ctx_Offset
+__constant__ uint16_t c_scanOff[19][3];        // offset of the scan of (tx size, class 2D / VERT / HORIZ) in the pack
+struct RateTabs {
+    const uint16_t *cost, *scan;
+    const uint8_t *baseCtx;                    // [19][5][5]
+};
+struct RateStage {
+    uint16_t cost[NCDF];
+    uint16_t scan[SCAN_PACK];
+    uint8_t baseCtx[19 * 25];
+    uint8_t pad[13];
+};
+__device__ __forceinline__ RateTabs rate_tabs_global(int qctx) { return RateTabs{g_cost[qctx], g_scanPack, g_baseCtx}; }
+// all threads of the CTA; followed by __syncthreads() at the caller
+__device__ __forceinline__ RateTabs rate_tabs_stage(RateStage &T, int qctx, int tid, int nt) {
+    const uint4 *c = reinterpret_cast<const uint4 *>(g_cost[qctx]);
+    for (int i = tid; i < NCDF / 8; i += nt) reinterpret_cast<uint4 *>(T.cost)[i] = c[i];
+    for (int i = tid; i < SCAN_PACK / 8; i += nt) reinterpret_cast<uint4 *>(T.scan)[i] = reinterpret_cast<const uint4 *>(g_scanPack)[i];
+    for (int i = tid; i < 19 * 25; i += nt) T.baseCtx[i] = g_baseCtx[i];
+    return RateTabs{T.cost, T.scan, T.baseCtx};
+}
+
 // ---- index of an entry of av1g_cdfs (uint16 units) ----
 #define IS_CB(f) ((int)(offsetof(av1g_cdfs, f) / 2))
 #define IS_CD(f, d) ((int)std::extent<decltype(av1g_cdfs::f), d>::value)
@@ -134,54 +161,10 @@ __device__ __forceinline__ int chroma_tx_type(int uvTx, int uvMode) {
     const int t = AV1G_T(Mode_To_Txfm)[uvMode];
     return tx_in_set(tx_set_intra(uvTx), t) ? t : AV1G_DCT_DCT;
 }
-// get_scan() (spec 5.11.41), intra types only (no flips)
-__device__ __forceinline__ const uint16_t *get_scan(int txSz, int txType) {
-    if (txSz == AV1G_TX_16X64) return AV1G_T(Default_Scan_16x32);
-    if (txSz == AV1G_TX_64X16) return AV1G_T(Default_Scan_32x16);
-    if (AV1G_T(Tx_Size_Sqr_Up)[txSz] == AV1G_TX_64X64) return AV1G_T(Default_Scan_32x32);
-    const int cls = txType == AV1G_IDTX ? AV1G_TX_CLASS_2D : tx_class(txType);
-    if (cls == AV1G_TX_CLASS_VERT) {
-        switch (txSz) {
-        case AV1G_TX_4X4: return AV1G_T(Mrow_Scan_4x4);
-        case AV1G_TX_4X8: return AV1G_T(Mrow_Scan_4x8);
-        case AV1G_TX_8X4: return AV1G_T(Mrow_Scan_8x4);
-        case AV1G_TX_8X8: return AV1G_T(Mrow_Scan_8x8);
-        case AV1G_TX_8X16: return AV1G_T(Mrow_Scan_8x16);
-        case AV1G_TX_16X8: return AV1G_T(Mrow_Scan_16x8);
-        case AV1G_TX_16X16: return AV1G_T(Mrow_Scan_16x16);
-        case AV1G_TX_4X16: return AV1G_T(Mrow_Scan_4x16);
-        default: return AV1G_T(Mrow_Scan_16x4);
-        }
-    }
-    if (cls == AV1G_TX_CLASS_HORIZ) {
-        switch (txSz) {
-        case AV1G_TX_4X4: return AV1G_T(Mcol_Scan_4x4);
-        case AV1G_TX_4X8: return AV1G_T(Mcol_Scan_4x8);
-        case AV1G_TX_8X4: return AV1G_T(Mcol_Scan_8x4);
-        case AV1G_TX_8X8: return AV1G_T(Mcol_Scan_8x8);
-        case AV1G_TX_8X16: return AV1G_T(Mcol_Scan_8x16);
-        case AV1G_TX_16X8: return AV1G_T(Mcol_Scan_16x8);
-        case AV1G_TX_16X16: return AV1G_T(Mcol_Scan_16x16);
-        case AV1G_TX_4X16: return AV1G_T(Mcol_Scan_4x16);
-        default: return AV1G_T(Mcol_Scan_16x4);
-        }
-    }
-    switch (txSz) {
-    case AV1G_TX_4X4: return AV1G_T(Default_Scan_4x4);
-    case AV1G_TX_4X8: return AV1G_T(Default_Scan_4x8);
-    case AV1G_TX_8X4: return AV1G_T(Default_Scan_8x4);
-    case AV1G_TX_8X8: return AV1G_T(Default_Scan_8x8);
-    case AV1G_TX_8X16: return AV1G_T(Default_Scan_8x16);
-    case AV1G_TX_16X8: return AV1G_T(Default_Scan_16x8);
-    case AV1G_TX_16X16: return AV1G_T(Default_Scan_16x16);
-    case AV1G_TX_16X32: return AV1G_T(Default_Scan_16x32);
-    case AV1G_TX_32X16: return AV1G_T(Default_Scan_32x16);
-    case AV1G_TX_4X16: return AV1G_T(Default_Scan_4x16);
-    case AV1G_TX_16X4: return AV1G_T(Default_Scan_16x4);
-    case AV1G_TX_8X32: return AV1G_T(Default_Scan_8x32);
-    case AV1G_TX_32X8: return AV1G_T(Default_Scan_32x8);
-    default: return AV1G_T(Default_Scan_32x32);
-    }
+// get_scan() (spec 5.11.41), intra types only (no flips): the scan of the size's class in the packed tables
+__device__ __forceinline__ const uint16_t *get_scan(const RateTabs &T, int txSz, int txType) {
+    const int cls = txType == AV1G_IDTX ? 0 : tx_class(txType);
+    return T.scan + c_scanOff[txSz][cls];
 }
 __device__ __forceinline__ int dq_denom(int txSz) {
     if (txSz == AV1G_TX_32X32 || txSz == AV1G_TX_16X32 || txSz == AV1G_TX_32X16 || txSz == AV1G_TX_16X64 || txSz == AV1G_TX_64X16) return 2;
@@ -545,7 +528,7 @@ __device__ __forceinline__ int task_buf_ints(int txSz) { return txh(txSz) * (txw
 // ---------------------------------------------------------------------------------------------------------------
 struct EvalIn {
     int txType, plane, skipCtx, dcCtx, intraDir, dcQ, acQ;
-    const uint16_t *C;   // cost table of the image's q-context
+    RateTabs T;          // cost table of the image's q-context, scans, base-context offsets
 };
 struct EvalOut { i64 D, R; int eob; };
 
@@ -558,7 +541,7 @@ __device__ __forceinline__ int tx_index_in_set(int set, int t) {
 // txb_skip, tx type, eob position bits
 __device__ __noinline__ i64 base_bits(int txSz, const EvalIn &e, int eob) {
     const int txSzCtx = (AV1G_T(Tx_Size_Sqr)[txSz] + AV1G_T(Tx_Size_Sqr_Up)[txSz] + 1) >> 1;
-    const uint16_t *C = e.C;
+    const uint16_t *C = e.T.cost;
     if (eob == 0) return C[ci_txb_skip(txSzCtx, e.skipCtx) + 1];
     i64 b = C[ci_txb_skip(txSzCtx, e.skipCtx)];
     const int ptype = e.plane > 0;
@@ -582,7 +565,8 @@ __device__ __noinline__ i64 base_bits(int txSz, const EvalIn &e, int eob) {
 
 // bits of the coefficient at scan position c < eob (levels q natural order, row stride = adjusted width)
 __device__ __forceinline__ int coeff_bits(int c, int eob, const int16_t *q, const uint16_t *scan, int txSz, int txClass, int ptype,
-                                          int dcCtx, const uint16_t *C) {
+                                          int dcCtx, const RateTabs &T) {
+    const uint16_t *C = T.cost;
     const int txSzCtx = (AV1G_T(Tx_Size_Sqr)[txSz] + AV1G_T(Tx_Size_Sqr_Up)[txSz] + 1) >> 1;
     const int adj = AV1G_T(Adjusted_Tx_Size)[txSz];
     const int bwl = AV1G_T(Tx_Width_Log2)[adj];
@@ -603,7 +587,7 @@ __device__ __forceinline__ int coeff_bits(int c, int eob, const int16_t *q, cons
             if (rr < height && cc < width) mag += min(abs((int)q[(rr << bwl) + cc]), 3);
         }
         int bctx = min((mag + 1) >> 1, 4);
-        if (txClass == AV1G_TX_CLASS_2D) bctx = (row == 0 && col == 0) ? 0 : bctx + AV1G_T(Coeff_Base_Ctx_Offset)[txSz][min(row, 4)][min(col, 4)];
+        if (txClass == AV1G_TX_CLASS_2D) bctx = (row == 0 && col == 0) ? 0 : bctx + T.baseCtx[txSz * 25 + min(row, 4) * 5 + min(col, 4)];
         else bctx += AV1G_T(Coeff_Base_Pos_Ctx_Offset)[min(txClass == AV1G_TX_CLASS_VERT ? row : col, 2)];
         b = C[ci_base(txSzCtx, ptype, bctx) + min(level, 3)];
     }
@@ -672,14 +656,14 @@ __device__ __noinline__ EvalOut grp_eval(int txSz, const ResFn<Px> &rf, const Ev
     }
     dist = grp_sum64(dist, G);
     __syncwarp();
-    const uint16_t *scan = get_scan(txSz, e.txType);
+    const uint16_t *scan = get_scan(e.T, txSz, e.txType);
     int last = 0;
     for (int c = g; c < d.n; c += G)
         if (q[scan[c]]) last = c + 1;
     const int eob = grp_max(last, G);
     int b = 0;
     const int cls = tx_class(e.txType);
-    for (int c = g; c < eob; c += G) b += coeff_bits(c, eob, q, scan, txSz, cls, e.plane > 0, e.dcCtx, e.C);
+    for (int c = g; c < eob; c += G) b += coeff_bits(c, eob, q, scan, txSz, cls, e.plane > 0, e.dcCtx, e.T);
     EvalOut o;
     o.R = grp_sum(b, G) + base_bits(txSz, e, eob);
     o.D = dist << d.dsh;

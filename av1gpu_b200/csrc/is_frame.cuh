@@ -53,7 +53,7 @@ struct FrameDesc {
     const uint32_t *sbOrder;                  // [nSb] SBs sorted by wavefront step (tile-local c + 2 r)
     uint8_t *ordmap;                          // [nSb * 256] leaf index covering each luma 4x4 unit of an SB (255: none)
     uint16_t *leafTxb, *leafCoef;             // [nSb * 256] first tx block / coefficient (SB-local) of each leaf
-    int *leafDone;                            // [nSb * 256] 1 once the leaf's reconstruction, maps and record are written
+    int *leafDone;                            // [nSb * 256] 1 once the leaf's luma (reconstruction, maps) is written, 2 once all is
     uint32_t *leafStart;                      // [nSb] first queue position of each SB's leaves
     uint32_t *leafQueue;                      // [nSb * 256] (sb << 8 | leaf) in topological order
     uint32_t *leafTotal;                      // [1] leaves in the queue

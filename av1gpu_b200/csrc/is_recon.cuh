@@ -40,7 +40,10 @@ template <typename Px> struct RcWarp {
     int cand[32];
     int job;
 };
-template <typename Px> struct RcSmem { RcWarp<Px> w[RC_WARPS]; };
+template <typename Px> struct RcSmem {
+    RateStage T;
+    RcWarp<Px> w[RC_WARPS];
+};
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
     int v;
@@ -105,10 +108,11 @@ __device__ void rc_reconstruct(int txSz, int txType, int16_t *q, int dcQ, int ac
 }
 
 // record a finished tx block: eob, culLevel / dc category into the context maps, the txb entry and its levels
-__device__ int rc_record(const FrameDesc &F, int sb, int plane, int txSz, int txType, int x4, int y4, const int16_t *q, int txbIdx, int coefOff) {
+__device__ int rc_record(const FrameDesc &F, const RateTabs &T, int sb, int plane, int txSz, int txType, int x4, int y4, const int16_t *q,
+                         int txbIdx, int coefOff) {
     const int lane = lane_id();
     const int W = txw(txSz), H = txh(txSz), n = min(W, 32) * min(H, 32);
-    const uint16_t *scan = get_scan(txSz, txType);
+    const uint16_t *scan = get_scan(T, txSz, txType);
     int last = 0;
     for (int c = lane; c < n; c += 32) if (q[scan[c]]) last = c + 1;
     const int eob = warp_max(last);
@@ -178,8 +182,40 @@ __device__ __forceinline__ unsigned long long gtimer() {
     return t;
 }
 
+// Wait until the leaves decoded before leaf li of SB sb that cover the luma 4x4 units of two strips have published
+// flag >= level: the row rTop, columns c0, c0 + st, ... < c1, and the column cLeft, rows r0, r0 + st, ... < r1 (SB-local
+// units; negative / >= 16 reach the SBs above, above-right and left).  Units outside the tile or the frame, in the SB to
+// the right, below the SB, or of this SB's later leaves are not waited on.  Returns false when a wait ran out of its
+// budget or another warp reported an error (F.err set); the leaf is then abandoned.
+__device__ __noinline__ bool rc_wait(const FrameDesc &F, int sb, int li, int sbr, int sbc, int rTop, int c0, int c1, int cLeft, int r0,
+                                     int r1, int st, int level, int tC0, int tC1, int tR0) {
+    const int lane = lane_id();
+    const int nTop = c1 > c0 ? (c1 - c0 + st - 1) / st : 0, nLeft = r1 > r0 ? (r1 - r0 + st - 1) / st : 0;
+    bool ok = true;
+    for (int u = lane; u < nTop + nLeft; u += 32) {
+        const int yy = u < nTop ? rTop : r0 + (u - nTop) * st, xx = u < nTop ? c0 + u * st : cLeft;
+        const int Y = sbr * 16 + yy, X = sbc * 16 + xx;        // luma 4x4 unit, frame coordinates
+        if (Y < tR0 || X < tC0 || X >= tC1 || Y >= F.MiRows || X >= F.MiCols) continue;   // outside the tile / frame
+        if (yy >= 16 || (yy >= 0 && xx >= 16)) continue;       // the SBs below / to the right: decoded later
+        int osb = sb, oy = yy, ox = xx;
+        if (yy < 0 || xx < 0 || xx >= 16) { osb = (Y >> 4) * F.sbCols + (X >> 4); oy = Y & 15; ox = X & 15; }
+        const int o = F.ordmap[(size_t)osb * 256 + oy * 16 + ox];
+        if (o == 255 || (osb == sb && o >= li)) continue;
+        const int *flag = F.leafDone + (size_t)osb * SB_MAX_LEAVES + o;
+        int it = 0;
+        while (ld_acquire(flag) < level) {
+            if (++it > LEAF_WAIT_ITERS || *(volatile int *)F.err) { ok = false; break; }
+            __nanosleep(64);
+        }
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    if (!ok && lane == 0) atomicCAS(F.err, 0, KERR_WAIT_LEAF);
+    __syncwarp();
+    return ok;
+}
+
 template <int BD, typename Px>
-__device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li, unsigned long long *trace) {
+__device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, int sb, int li, unsigned long long *trace) {
     const int lane = lane_id();
     const Leaf lf = F.leaves[(size_t)sb * SB_MAX_LEAVES + li];
     const int bsize = lf.bsize;
@@ -193,37 +229,15 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li, unsi
     while (tc + 1 < F.tileCols && mi_col >= F.tileColStart[tc + 1]) tc++;
     while (tr + 1 < F.tileRows && mi_row >= F.tileRowStart[tr + 1]) tr++;
     const int tC0 = F.tileColStart[tc], tC1 = F.tileColStart[tc + 1], tR0 = F.tileRowStart[tr], tR1 = F.tileRowStart[tr + 1];
-    // ---- wait for the earlier leaves of the neighbourhood (this SB, and the SBs above, above-right and left) ----
-    {
-        const int r0 = lf.y4 - 2, r1 = min(16, lf.y4 + max(2 * bh, 4));
-        const int c0 = lf.x4 - 2, c1 = lf.x4 + max(2 * bw, 4);
-        const int nc = c1 - c0, nu = (r1 - r0) * nc;
-        bool ok = true;
-        for (int u = lane; u < nu; u += 32) {
-            const int yy = r0 + u / nc, xx = c0 + u % nc;
-            const int Y = sbr * 16 + yy, X = sbc * 16 + xx;        // luma 4x4 unit, frame coordinates
-            if (Y < tR0 || X < tC0 || X >= tC1 || Y >= F.MiRows || X >= F.MiCols) continue;   // outside the tile / frame
-            if (yy >= 0 && xx >= 16) continue;                      // the SB to the right: decoded later
-            int osb = sb, oy = yy, ox = xx;
-            if (yy < 0 || xx < 0 || xx >= 16) { osb = (Y >> 4) * F.sbCols + (X >> 4); oy = Y & 15; ox = X & 15; }
-            const int o = F.ordmap[(size_t)osb * 256 + oy * 16 + ox];
-            if (o == 255 || (osb == sb && o >= li)) continue;
-            const int *flag = F.leafDone + (size_t)osb * SB_MAX_LEAVES + o;
-            int it = 0;
-            while (!ld_acquire(flag)) {
-                if (++it > LEAF_WAIT_ITERS || *(volatile int *)F.err) { ok = false; break; }
-                __nanosleep(64);
-            }
-        }
-        if (!__all_sync(0xffffffffu, ok) && lane == 0) atomicExch(F.err, KERR_WAIT_LEAF);
-        __syncwarp();
-    }
+    // ---- luma neighbourhood: the earlier leaves of the above row (from the above-left corner to the above-right reach of
+    // 2 x width) and of the left column (to the below-left reach of 2 x height) have published their luma (flag >= 1) ----
+    if (!rc_wait(F, sb, li, sbr, sbc, lf.y4 - 1, lf.x4 - 1, lf.x4 + 2 * bw, lf.x4 - 1, lf.y4, lf.y4 + 2 * bh, 1, 1, tC0, tC1, tR0)) return;
     if (trace && lane == 0) trace[1] = gtimer();
     const int availU = mi_row - 1 >= tR0, availL = mi_col - 1 >= tC0;
     const bool hasC = has_chroma(bsize, mi_row, mi_col, ss);
     const int availUC = (ss && bh == 1) ? (mi_row - 2 >= tR0) : availU;
     const int availLC = (ss && bw == 1) ? (mi_col - 2 >= tC0) : availL;
-    const uint16_t *C = g_cost[F.qctx];
+    const uint16_t *C = T.cost;
     const int txbBase = F.leafTxb[(size_t)sb * SB_MAX_LEAVES + li], coefBase = F.leafCoef[(size_t)sb * SB_MAX_LEAVES + li];
     // BlockDecoded of a 4x4 unit (SB-relative, plane units; ps = 0 luma, ss chroma) for this leaf
     auto decoded = [&](int ps, int yy, int xx) -> bool {
@@ -278,7 +292,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li, unsi
                 if (Wp.predC[grp] != c) grp_predict(m, pangle(m, cand_delta(c)), lw, lh, A, L, dcv, tp, g, G);
                 __syncwarp();
                 if (g == 0) Wp.predC[grp] = c;
-                const EvalIn e{t, 0, skipCtx, dcCtx, m, F.dcQ, F.acQ, C};
+                const EvalIn e{t, 0, skipCtx, dcCtx, m, F.dcQ, F.acQ, T};
                 const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{src, F.spitch[0], tp, lw, nullptr}, e, tb, tq, g, G);
                 if (g == 0 && r0 + grp < n) Wp.taskJ[grp] = o.D + F.lam * (o.R + mbits(c));
                 __syncwarp();
@@ -313,12 +327,12 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li, unsi
         grp_predict(bm, pangle(bm, cand_delta(bestC)), lw, lh, A, L, dcv, Wp.pred, lane, 32);
         __syncwarp();
         if (!have) {
-            const EvalIn e{bestT, 0, skipCtx, dcCtx, bm, F.dcQ, F.acQ, C};
+            const EvalIn e{bestT, 0, skipCtx, dcCtx, bm, F.dcQ, F.acQ, T};
             grp_eval<BD, Px>(txSz, ResFn<Px>{src, F.spitch[0], Wp.pred, lw, nullptr}, e, Wp.buf, best, lane, 32);
         }
         Px *dst = (Px *)F.rec[0] + (size_t)y * F.rpitch[0] + x;
         rc_reconstruct<BD, Px>(txSz, bestT, best, F.dcQ, F.acQ, Wp.pred, dst, F.rpitch[0], Wp.buf);
-        eobY = rc_record(F, sb, 0, txSz, bestT, x >> 2, y >> 2, best, txbBase, coefBase);
+        eobY = rc_record(F, T, sb, 0, txSz, bestT, x >> 2, y >> 2, best, txbBase, coefBase);
         yMode = bm;
         yDelta = cand_delta(bestC);
         for (int k = lane; k < bw * bh; k += 32) {
@@ -326,10 +340,25 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li, unsi
             if (r < F.MiRows && c < F.MiCols) F.mYMode[(size_t)r * F.MiCols + c] = (uint8_t)yMode;
         }
     }
-    if (trace && lane == 0) trace[2] = gtimer();
+    // publish the luma (reconstruction, y modes, luma coefficient contexts) for the luma of the later leaves
+    __syncwarp();
+    if (lane == 0) {
+        __threadfence();
+        st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 1);
+        if (trace) trace[2] = gtimer();
+    }
     // ================= chroma =================
     int uv = 0, duv = 0, aU = 0, aV = 0, eobU = 0, eobV = 0;
     if (hasC) {
+        // chroma neighbourhood: the leaves carrying the chroma units above (from the above-left corner to the above-right
+        // reach of 2 x chroma width) and left (to the below-left reach of 2 x chroma height) are done (flag 2); with
+        // subsampling a chroma unit's carrier covers the bottom-right luma unit of its 2 x 2 area
+        if (ss) {
+            const int cx0 = lf.x4 & ~1, cy0 = lf.y4 & ~1, cw = max(bw, 2), ch = max(bh, 2);
+            if (!rc_wait(F, sb, li, sbr, sbc, cy0 - 1, cx0 - 1, cx0 + 2 * cw, cx0 - 1, cy0 + 1, cy0 + 2 * ch, 2, 2, tC0, tC1, tR0)) return;
+        } else {
+            if (!rc_wait(F, sb, li, sbr, sbc, lf.y4 - 1, lf.x4 - 1, lf.x4 + 2 * bw, lf.x4 - 1, lf.y4, lf.y4 + 2 * bh, 1, 2, tC0, tC1, tR0)) return;
+        }
         const int txSz = uv_tx_size(bsize, ss);
         const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
         const int cx = (mi_col >> ss) * 4, cy = (mi_row >> ss) * 4, cx4 = cx >> 2, cy4 = cy >> 2;
@@ -478,7 +507,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li, unsi
             predict(pl, c, tp, g, G);
             __syncwarp();
             const int txType = chroma_tx_type(txSz, c == 255 ? AV1G_UV_CFL_PRED : cand_mode(c));
-            const EvalIn e{txType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, C};
+            const EvalIn e{txType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, T};
             const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{sP[pl], F.spitch[pl], tp, lw, nullptr}, e, tb, tq, g, G);
             if (g == 0 && r0 + grp < ntask) Wp.taskJ[grp] = o.D + F.lam * o.R;
             __syncwarp();
@@ -509,14 +538,14 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li, unsi
         for (int pl = 1; pl <= 2; pl++) {
             predict(pl, bestC, Wp.pred, lane, 32);
             __syncwarp();
-            const EvalIn e{uvType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, C};
+            const EvalIn e{uvType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, T};
             int16_t *lv = Wp.qb[pl - 1];
             grp_eval<BD, Px>(txSz, ResFn<Px>{sP[pl], F.spitch[pl], Wp.pred, lw, nullptr}, e, Wp.buf, lv, lane, 32);
             Px *dst = (Px *)F.rec[pl] + (size_t)cy * F.rpitch[pl] + cx;
             rc_reconstruct<BD, Px>(txSz, uvType, lv, F.dcQ, F.acQ, Wp.pred, dst, F.rpitch[pl], Wp.buf);
             const int yt = AV1G_T(Max_Tx_Size_Rect)[bsize];
             const int off = coefBase + min(txw(yt), 32) * min(txh(yt), 32) + (pl - 1) * nq;
-            const int e2 = rc_record(F, sb, pl, txSz, uvType, cx4, cy4, lv, txbBase + pl, off);
+            const int e2 = rc_record(F, T, sb, pl, txSz, uvType, cx4, cy4, lv, txbBase + pl, off);
             if (pl == 1) eobU = e2; else eobV = e2;
         }
         duv = cfl ? 0 : cand_delta(bestC);
@@ -541,7 +570,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, int sb, int li, unsi
     __syncwarp();
     if (lane == 0) {
         __threadfence();
-        st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 1);
+        st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 2);
         if (trace) trace[3] = gtimer();
     }
 }
@@ -555,6 +584,8 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
     const FrameDesc &F = *Fp;
     RcWarp<Px> &Wp = S.w[threadIdx.x >> 5];
     const int lane = lane_id();
+    const RateTabs T = rate_tabs_stage(S.T, F.qctx, threadIdx.x, blockDim.x);
+    __syncthreads();
     const uint32_t total = *F.leafTotal;
     for (;;) {
         if (lane == 0) Wp.job = atomicAdd(F.queue, 1);
@@ -565,7 +596,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
         const uint32_t e = F.leafQueue[qi];
         unsigned long long *trace = F.leafTrace ? F.leafTrace + (size_t)qi * 4 : nullptr;
         if (trace && lane == 0) trace[0] = gtimer();
-        rc_leaf<BD, Px>(F, Wp, (int)(e >> 8), (int)(e & 255), trace);
+        rc_leaf<BD, Px>(F, Wp, T, (int)(e >> 8), (int)(e & 255), trace);
     }
 }
 

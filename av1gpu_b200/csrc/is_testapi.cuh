@@ -15,7 +15,7 @@ __global__ void k_test_fwd_quant(int n, const int32_t *res, int txSz, int txType
     const int b = blockIdx.x * 2 + (threadIdx.x >> 5);
     if (b >= n) return;
     const int W = txw(txSz), H = txh(txSz), tw = min(W, 32), th = min(H, 32), nc = tw * th, lw = 31 - __clz(W);
-    const EvalIn e{txType, plane, skipCtx, dcCtx, intraDir, dcQ, acQ, g_cost[qctx]};
+    const EvalIn e{txType, plane, skipCtx, dcCtx, intraDir, dcQ, acQ, rate_tabs_global(qctx)};
     ResFn<uint8_t> rf{nullptr, 0, nullptr, lw, res + (size_t)b * W * H};
     const EvalOut o = grp_eval<8, uint8_t>(txSz, rf, e, S.buf, S.q, lane_id(), 32);
     for (int idx = lane_id(); idx < nc; idx += 32) {
