@@ -597,3 +597,4 @@ int is_times_get(const is_handle *h, is_times *t) {
 }  // extern "C"
 
 #include "is_testapi.cuh"
+#include "is_noalloc.cuh"

@@ -44,7 +44,8 @@ class IsTimes(C.Structure):
 # every entry point declared in include/is_api.h
 EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_encode_host", "is_record_counts",
            "is_record_copy", "is_record_device", "is_times_get", "is_test_fwd_quant", "is_test_inverse",
-           "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32", "is_set_trace", "is_get_trace"]
+           "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32", "is_set_trace", "is_get_trace",
+           "is_fwd_quant_static"]
 
 _lib = None
 
@@ -79,6 +80,7 @@ def load_library():
     L.is_probe_int32.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]
     L.is_set_trace.argtypes = [C.c_void_p, C.c_int]
     L.is_get_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32)]
+    L.is_fwd_quant_static.argtypes = [C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp]
     _lib = L
     return L
 

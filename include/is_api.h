@@ -35,6 +35,7 @@ extern "C" {
 #define IS_ERR_OOM -3       /* device allocation failed */
 #define IS_ERR_TIMEOUT -4   /* a wavefront dependency wait of the closed loop ran out of its budget (no hang) */
 #define IS_ERR_STATE -5     /* no encode result to read */
+#define IS_ERR_TOO_LARGE -6 /* the request does not fit the fixed scratch of is_fwd_quant_static */
 
 typedef struct is_params {
     int32_t bit_depth;      /* 8 */
@@ -112,6 +113,28 @@ int is_get_trace(is_handle *h, unsigned long long *out, size_t cap, uint32_t *n)
 /* INT32 issue-rate probe: the measured INT32 instruction throughput of the device (Gop/s, multiply-add + logic chains
  * over every SM) and the best kernel time, the roofline denominator of this integer path. */
 int is_probe_int32(int device, double *gops, float *ms);
+
+/* Forward transform + quantisation + rate of n residual blocks (the same computation and arguments as
+ * is_test_fwd_quant) without any device allocation: no handle, and no cudaMalloc / cudaFree or other allocating call.
+ * No counterpart in the reference.  For callers that may not allocate device memory (memory owned by a pool or
+ * budgeted elsewhere, or code that must not meet the allocator's implicit synchronisation).  The kernel's buffers live
+ * in one static scratch of IS_STATIC_SCRATCH_BYTES per device, reserved with the library's module.
+ *  - The first call on a device does one-time setup (the search's tables, the scratch address): make it before any
+ *    stream capture.  Nothing is claimed about calls inside a capture.
+ *  - n blocks of W x H need n * (4 W H + 6 nc + 20) bytes, each of the six sections rounded up to 256 bytes
+ *    (nc = min(W, 32) * min(H, 32)); a request that does not fit returns IS_ERR_TOO_LARGE before any GPU work (for
+ *    example at most 186 blocks of 64x64, 1625 of 16x16).  Bad arguments return IS_ERR_INVALID, CUDA failures
+ *    IS_ERR_CUDA (no message: there is no handle).
+ *  - Nothing in the scratch has to start at zero: the call copies its residuals in before the launch and the kernel
+ *    writes every output word the call reads back.
+ *  - Calls on one device share the scratch: they must not overlap.  Two calls in flight at once on the same device
+ *    (from other threads or streams) race on it and can return each other's results.
+ * Host arrays in and out (as is_test_fwd_quant); stream: a cudaStream_t (NULL = the legacy default stream); returns
+ * after the results are in the host arrays.  The calling thread's current device is restored. */
+#define IS_STATIC_SCRATCH_BYTES (4u << 20)
+int is_fwd_quant_static(int device, int n, const int32_t *res, int tx_size, int tx_type, int plane, int qindex,
+                        const int32_t ctx[3], int32_t *coef, int16_t *levels, int64_t *D, int64_t *R, int32_t *eob,
+                        void *stream);
 
 #ifdef __cplusplus
 }
