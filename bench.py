@@ -32,6 +32,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 W_IMG, H_IMG, SEED = 4000, 3000, 12
+# kernels of one search: k_pad x 3 planes, k_analysis_big, k_analysis, k_dp, k_leaf_prep, k_leaf_queue_scan,
+# k_leaf_queue_fill, k_recon, k_pack_scan, k_pack
+LAUNCHES_PER_STEP = 12
 
 
 def parse():
@@ -212,7 +215,7 @@ def main():
                 "config": {"workload": "plain intra RD search, 4000x3000 8-bit 4:2:0 synthetic (seeded), qindex %d" % args.qindex,
                            "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas" if world > 1 else "1 gpu"},
                 "e2e": {"value": round(e2e_value, 3), "unit": "MP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "gpu_launches": 8 * args.steps,
+                "gpu_launches": LAUNCHES_PER_STEP * args.steps,
                 "stage_ms": {k: round(v, 3) for k, v in kernel_ms.items()},
                 "clocks": clk.summary()}
         line["roofline"] = roofline.report(enc, kernel_ms, mp)
