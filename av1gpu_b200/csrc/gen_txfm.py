@@ -226,7 +226,13 @@ def emit_fwd(name, ops, n0):
 
 
 def emit_inv(name, ops, n0):
-    """Inverse with the spec's checks: B outputs must fit r bits (flag 1), H results are clamped to r bits."""
+    """Inverse with the spec's checks: B outputs must fit r bits (flag 1), H results are clamped to r bits.
+
+    32-bit arithmetic is exact for every transform that ends with the flag clear: its inputs are within r bits
+    (dequantised values are clipped to BitDepth + 8 bits, the column inputs to the column clamp range), so while no
+    rotation has left r bits every rotation input is within r bits (H results are clamped; a permutation negation
+    adds at most 1) and |T[a] c - T[b] s| + 2048 < 2^(r + 13) <= 2^31 for r <= 18 (bit depth <= 10).  After the
+    first out-of-range rotation the flag is set and the caller discards the values."""
     out = ['__host__ __device__ __forceinline__ uint32_t %s(int32_t *T, int r) {' % name,
            '    uint32_t e_ = 0;',
            '    const int32_t lo_ = -(1 << (r - 1)), hi_ = (1 << (r - 1)) - 1;']
@@ -236,16 +242,16 @@ def emit_inv(name, ops, n0):
         elif op[0] == 'B':
             _, a, b, ang, fl = op
             c, s = cos128(ang), sin128(ang)
-            x = 'rnd12w((int64_t)T[%d] * %d - (int64_t)T[%d] * %d)' % (a, c, b, s)
-            y = 'rnd12w((int64_t)T[%d] * %d + (int64_t)T[%d] * %d)' % (a, s, b, c)
+            x = 'rnd12(T[%d] * %d - T[%d] * %d)' % (a, c, b, s)
+            y = 'rnd12(T[%d] * %d + T[%d] * %d)' % (a, s, b, c)
             dst = (b, a) if fl else (a, b)
-            out.append('    { const int64_t x_ = %s, y_ = %s; e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); '
-                       'T[%d] = (int32_t)x_; T[%d] = (int32_t)y_; }' % (x, y, dst[0], dst[1]))
+            out.append('    { const int32_t x_ = %s, y_ = %s; e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); '
+                       'T[%d] = x_; T[%d] = y_; }' % (x, y, dst[0], dst[1]))
         else:
             _, a, b, fl = op
             if fl:
                 a, b = b, a
-            out.append('    { const int64_t x_ = T[%d], y_ = T[%d]; T[%d] = clampr(x_ + y_, lo_, hi_); '
+            out.append('    { const int32_t x_ = T[%d], y_ = T[%d]; T[%d] = clampr(x_ + y_, lo_, hi_); '
                        'T[%d] = clampr(x_ - y_, lo_, hi_); }' % (a, b, a, b))
     out.append('    return e_;')
     out.append('}')
@@ -264,9 +270,8 @@ def main():
            '#define __forceinline__ inline',
            '#endif',
            '__host__ __device__ __forceinline__ int32_t rnd12(int32_t x) { return (x + 2048) >> 12; }',
-           '__host__ __device__ __forceinline__ int64_t rnd12w(int64_t x) { return (x + 2048) >> 12; }',
-           '__host__ __device__ __forceinline__ int32_t clampr(int64_t v, int32_t lo, int32_t hi) '
-           '{ return (int32_t)(v < lo ? lo : (v > hi ? hi : v)); }',
+           '__host__ __device__ __forceinline__ int32_t clampr(int32_t v, int32_t lo, int32_t hi) '
+           '{ return v < lo ? lo : (v > hi ? hi : v); }',
            '']
     for n in range(2, 7):
         out += emit_fwd('fwd_dct%d' % (1 << n), idct_ops(n), 1 << n)

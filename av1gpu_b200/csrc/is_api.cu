@@ -328,7 +328,12 @@ size_t layout(int W, int H, uint8_t *base, FrameDesc &F, int &nSb) {
     F.leafQueue = (uint32_t *)take((size_t)nSb * SB_MAX_LEAVES * 4);
     F.leafTotal = (uint32_t *)take(4);
     F.leafTrace = nullptr;   // set per encode when tracing is on (is_set_trace)
-    F.queue = (int *)take(4);
+    F.queue = (int *)take(16);
+    F.depCnt = (int *)take((size_t)nSb * SB_MAX_LEAVES * 4);
+    F.revCnt = (int *)take((size_t)nSb * SB_MAX_LEAVES * 4);
+    F.revFill = (int *)take((size_t)nSb * SB_MAX_LEAVES * 4);
+    F.revOff = (uint32_t *)take((size_t)nSb * SB_MAX_LEAVES * 4);
+    F.revList = (uint32_t *)take((size_t)nSb * REV_PER_SB * 4);
     F.err = (int *)take(4);
     F.sbDecodeOrder = (uint32_t *)take((size_t)nSb * 4);
     F.offBlk = (uint32_t *)take((size_t)(nSb + 1) * 4);
@@ -477,7 +482,7 @@ static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) 
         const int pw = ((F.sbCols + 1) * 64) >> ss, ph = (F.sbRows * 64) >> ss;
         k_pad<uint8_t><<<dim3(1, ph), 128, 0, st>>>(dst, F.spitch[p], vw, vh, pw, ph);
     }
-    IS_CK(cudaMemsetAsync(F.queue, 0, 4, st));
+    IS_CK(cudaMemsetAsync(F.queue, 0, 16, st));
     IS_CK(cudaMemsetAsync(F.err, 0, 4, st));
     IS_CK(cudaEventRecord(h->ev[1], st));
     k_analysis_big<8><<<nSb, ANB_WARPS * 32, h->smemAnBig, st>>>(h->dF);
@@ -489,7 +494,9 @@ static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) 
     IS_CK(cudaEventRecord(h->ev[3], st));
     k_leaf_prep<<<nSb, 256, 0, st>>>(h->dF, nSb);
     k_leaf_queue_scan<<<1, 1024, 0, st>>>(h->dF, nSb);
-    k_leaf_queue_fill<<<nSb, 256, 0, st>>>(h->dF, nSb);
+    k_leaf_deps<0><<<nSb, 256, 0, st>>>(h->dF, nSb);
+    k_leaf_deps<1><<<nSb, 256, 0, st>>>(h->dF, nSb);
+    k_leaf_deps<2><<<nSb, 256, 0, st>>>(h->dF, nSb);
     IS_CK(cudaGetLastError());
     {
         const FrameDesc *a0 = h->dF;

@@ -244,9 +244,11 @@ __device__ __forceinline__ int pred_px(int mode, int pAng, int i, int j, int lw,
 }
 
 // One 4x4 sub-block (rows sy.., cols sx..) of a block's prediction into p[16], the values of pred_px with the mode
-// dispatch hoisted out of the samples (one branch per sub-block instead of per sample).
+// dispatch hoisted out of the samples (one branch per sub-block instead of per sample).  Not inlined: one copy
+// (~30 KB of code) serves every caller of a kernel instead of one per call site, which keeps the kernels' hot code
+// within reach of the instruction caches.
 template <typename P>
-__device__ __forceinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, int lh, const P *A, const P *L, int dcv, int *p) {
+__device__ __noinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, int lh, const P *A, const P *L, int dcv, int *p) {
     const int w = 1 << lw, h = 1 << lh;
     if (mode == AV1G_DC_PRED) {
 #pragma unroll
@@ -329,7 +331,7 @@ __device__ __forceinline__ void pred4(int mode, int pAng, int sy, int sx, int lw
 
 // the whole prediction of a W x H block into out (row stride W), 4x4 sub-blocks over the G lanes of a group
 template <typename P, typename O>
-__device__ __forceinline__ void grp_predict(int mode, int pAng, int lw, int lh, const P *A, const P *L, int dcv, O *out, int g, int G) {
+__device__ __noinline__ void grp_predict(int mode, int pAng, int lw, int lh, const P *A, const P *L, int dcv, O *out, int g, int G) {
     const int nsx = 1 << (lw - 2), nsub = 1 << (lw + lh - 4);
     for (int sb = g; sb < nsub; sb += G) {
         const int sx = (sb & (nsx - 1)) * 4, sy = (sb >> (lw - 2)) * 4;

@@ -18,6 +18,9 @@ constexpr int SRC_MARGIN_X = 16, SRC_MARGIN_Y = 1;
 constexpr int SB_MAX_LEAVES = 256;
 constexpr int SB_MAX_TXB = 768;      // luma 256 + chroma 2 x 256 (4:4:4 bound)
 constexpr int SB_MAX_COEF = 12288;   // 3 x 64 x 64
+// dependency entries per SB: a leaf of bw x bh luma 4x4 units has at most 2 bw + 1 + 2 bh luma dependencies, which is
+// at most 5 bw bh, so the leaves of one SB have at most 5 x 256 between them
+constexpr int REV_PER_SB = 1280;
 
 struct BlockRes {      // analysis result of one (shape, position): 16 bytes
     long long J;       // best open-loop RD cost (J units)
@@ -54,10 +57,16 @@ struct FrameDesc {
     uint8_t *ordmap;                          // [nSb * 256] leaf index covering each luma 4x4 unit of an SB (255: none)
     uint16_t *leafTxb, *leafCoef;             // [nSb * 256] first tx block / coefficient (SB-local) of each leaf
     int *leafDone;                            // [nSb * 256] 1 once the leaf's luma (reconstruction, maps) is written, 2 once all is
-    uint32_t *leafStart;                      // [nSb] first queue position of each SB's leaves
-    uint32_t *leafQueue;                      // [nSb * 256] (sb << 8 | leaf) in topological order
-    uint32_t *leafTotal;                      // [1] leaves in the queue
-    int *queue;                               // [1] next queue position
+    uint32_t *leafStart;                      // [nSb] first position of each SB's leaves in the wavefront order
+    uint32_t *leafQueue;                      // [nSb * 256] ready queue: 1 + (sb << 8 | leaf) in the order leaves became
+                                              // ready (0: slot not written yet)
+    uint32_t *leafTotal;                      // [1] leaves of the image
+    int *queue;                               // [4] ready-queue head (next slot to take), tail (next slot to write),
+                                              // next free entry of revList
+    int *depCnt;                              // [nSb * 256] luma dependencies of each leaf not yet published
+    int *revCnt, *revFill;                    // [nSb * 256] dependents of each leaf; entries written so far
+    uint32_t *revOff;                         // [nSb * 256] first entry of each leaf's dependents in revList
+    uint32_t *revList;                        // [nSb * REV_PER_SB] dependents (sb << 8 | leaf), grouped per leaf
     int *err;                                 // [1] error status (0 = ok)
     unsigned long long *leafTrace;            // [leaves * 4] optional (debug): claimed / ready / luma done / done (ns)
     // pack output (DecisionRecord arrays in decode order) and per-SB offsets

@@ -182,11 +182,24 @@ __device__ __forceinline__ unsigned long long gtimer() {
     return t;
 }
 
+// The leaf decoded before leaf li of SB sb that covers the luma 4x4 unit (yy, xx) (SB-local; negative / >= 16 reach
+// the SBs above, above-right and left) as sb << 8 | leaf, or -1: outside the tile or the frame, in the SBs below or to
+// the right (decoded later), uncovered, or a later leaf of this SB.
+__device__ __forceinline__ int unit_leaf(const FrameDesc &F, int sb, int li, int sbr, int sbc, int yy, int xx, int tC0, int tC1, int tR0) {
+    const int Y = sbr * 16 + yy, X = sbc * 16 + xx;            // luma 4x4 unit, frame coordinates
+    if (Y < tR0 || X < tC0 || X >= tC1 || Y >= F.MiRows || X >= F.MiCols) return -1;
+    if (yy >= 16 || (yy >= 0 && xx >= 16)) return -1;
+    int osb = sb, oy = yy, ox = xx;
+    if (yy < 0 || xx < 0 || xx >= 16) { osb = (Y >> 4) * F.sbCols + (X >> 4); oy = Y & 15; ox = X & 15; }
+    const int o = F.ordmap[(size_t)osb * 256 + oy * 16 + ox];
+    if (o == 255 || (osb == sb && o >= li)) return -1;
+    return osb * SB_MAX_LEAVES + o;
+}
+
 // Wait until the leaves decoded before leaf li of SB sb that cover the luma 4x4 units of two strips have published
-// flag >= level: the row rTop, columns c0, c0 + st, ... < c1, and the column cLeft, rows r0, r0 + st, ... < r1 (SB-local
-// units; negative / >= 16 reach the SBs above, above-right and left).  Units outside the tile or the frame, in the SB to
-// the right, below the SB, or of this SB's later leaves are not waited on.  Returns false when a wait ran out of its
-// budget or another warp reported an error (F.err set); the leaf is then abandoned.
+// flag >= level: the row rTop, columns c0, c0 + st, ... < c1, and the column cLeft, rows r0, r0 + st, ... < r1 (the
+// unit_leaf rule).  Returns false when a wait ran out of its budget or another warp reported an error (F.err set); the
+// leaf is then abandoned.
 __device__ __noinline__ bool rc_wait(const FrameDesc &F, int sb, int li, int sbr, int sbc, int rTop, int c0, int c1, int cLeft, int r0,
                                      int r1, int st, int level, int tC0, int tC1, int tR0) {
     const int lane = lane_id();
@@ -194,14 +207,9 @@ __device__ __noinline__ bool rc_wait(const FrameDesc &F, int sb, int li, int sbr
     bool ok = true;
     for (int u = lane; u < nTop + nLeft; u += 32) {
         const int yy = u < nTop ? rTop : r0 + (u - nTop) * st, xx = u < nTop ? c0 + u * st : cLeft;
-        const int Y = sbr * 16 + yy, X = sbc * 16 + xx;        // luma 4x4 unit, frame coordinates
-        if (Y < tR0 || X < tC0 || X >= tC1 || Y >= F.MiRows || X >= F.MiCols) continue;   // outside the tile / frame
-        if (yy >= 16 || (yy >= 0 && xx >= 16)) continue;       // the SBs below / to the right: decoded later
-        int osb = sb, oy = yy, ox = xx;
-        if (yy < 0 || xx < 0 || xx >= 16) { osb = (Y >> 4) * F.sbCols + (X >> 4); oy = Y & 15; ox = X & 15; }
-        const int o = F.ordmap[(size_t)osb * 256 + oy * 16 + ox];
-        if (o == 255 || (osb == sb && o >= li)) continue;
-        const int *flag = F.leafDone + (size_t)osb * SB_MAX_LEAVES + o;
+        const int id = unit_leaf(F, sb, li, sbr, sbc, yy, xx, tC0, tC1, tR0);
+        if (id < 0) continue;
+        const int *flag = F.leafDone + id;
         int it = 0;
         while (ld_acquire(flag) < level) {
             if (++it > LEAF_WAIT_ITERS || *(volatile int *)F.err) { ok = false; break; }
@@ -212,6 +220,42 @@ __device__ __noinline__ bool rc_wait(const FrameDesc &F, int sb, int li, int sbr
     if (!ok && lane == 0) atomicCAS(F.err, 0, KERR_WAIT_LEAF);
     __syncwarp();
     return ok;
+}
+
+// tile box (mi units) of the 4x4 unit (mi_row, mi_col)
+__device__ __forceinline__ void tile_box(const FrameDesc &F, int mi_row, int mi_col, int &tC0, int &tC1, int &tR0, int &tR1) {
+    int tc = 0, tr = 0;
+    while (tc + 1 < F.tileCols && mi_col >= F.tileColStart[tc + 1]) tc++;
+    while (tr + 1 < F.tileRows && mi_row >= F.tileRowStart[tr + 1]) tr++;
+    tC0 = F.tileColStart[tc]; tC1 = F.tileColStart[tc + 1]; tR0 = F.tileRowStart[tr]; tR1 = F.tileRowStart[tr + 1];
+}
+
+// Luma dependencies of leaf li of SB sb: the distinct leaves (unit_leaf rule) covering a unit of its above strip (row
+// y4 - 1 from the above-left corner to the above-right reach x4 + 2 bw) or of its left strip (column x4 - 1 down to the
+// below-left reach y4 + 2 bh) - every sample its luma prediction and its luma contexts read.  At most 2 bw + 1 + 2 bh.
+__device__ int luma_deps(const FrameDesc &F, int sb, int li, uint32_t *out) {
+    const Leaf lf = F.leaves[(size_t)sb * SB_MAX_LEAVES + li];
+    const int bw = bw4(lf.bsize), bh = bh4(lf.bsize);
+    const int sbr = sb / F.sbCols, sbc = sb % F.sbCols;
+    int tC0, tC1, tR0, tR1;
+    tile_box(F, sbr * 16 + lf.y4, sbc * 16 + lf.x4, tC0, tC1, tR0, tR1);
+    const int nTop = 2 * bw + 1, nLeft = 2 * bh;
+    int n = 0;
+    for (int u = 0; u < nTop + nLeft; u++) {
+        const int yy = u < nTop ? lf.y4 - 1 : lf.y4 + (u - nTop), xx = u < nTop ? lf.x4 - 1 + u : lf.x4 - 1;
+        const int id = unit_leaf(F, sb, li, sbr, sbc, yy, xx, tC0, tC1, tR0);
+        if (id < 0 || (n > 0 && out[n - 1] == (uint32_t)id)) continue;
+        bool seen = false;
+        for (int k = 0; k < n; k++) seen |= out[k] == (uint32_t)id;
+        if (!seen) out[n++] = (uint32_t)id;
+    }
+    return n;
+}
+
+// append leaf id to the ready queue
+__device__ __forceinline__ void push_ready(const FrameDesc &F, uint32_t id) {
+    const int pos = atomicAdd(F.queue + 1, 1);
+    st_release((int *)F.leafQueue + pos, (int)id + 1);
 }
 
 template <int BD, typename Px>
@@ -225,14 +269,9 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
     const int bw = bw4(bsize), bh = bh4(bsize);
     const int ss = F.ssx;
     const uint8_t *ordmap = F.ordmap + (size_t)sb * 256;
-    int tc = 0, tr = 0;
-    while (tc + 1 < F.tileCols && mi_col >= F.tileColStart[tc + 1]) tc++;
-    while (tr + 1 < F.tileRows && mi_row >= F.tileRowStart[tr + 1]) tr++;
-    const int tC0 = F.tileColStart[tc], tC1 = F.tileColStart[tc + 1], tR0 = F.tileRowStart[tr], tR1 = F.tileRowStart[tr + 1];
-    // ---- luma neighbourhood: the earlier leaves of the above row (from the above-left corner to the above-right reach of
-    // 2 x width) and of the left column (to the below-left reach of 2 x height) have published their luma (flag >= 1) ----
-    if (!rc_wait(F, sb, li, sbr, sbc, lf.y4 - 1, lf.x4 - 1, lf.x4 + 2 * bw, lf.x4 - 1, lf.y4, lf.y4 + 2 * bh, 1, 1, tC0, tC1, tR0)) return;
-    if (trace && lane == 0) trace[1] = gtimer();
+    int tC0, tC1, tR0, tR1;
+    tile_box(F, mi_row, mi_col, tC0, tC1, tR0, tR1);
+    // (the leaf came from the ready queue: the luma of every leaf of luma_deps() is published)
     const int availU = mi_row - 1 >= tR0, availL = mi_col - 1 >= tC0;
     const bool hasC = has_chroma(bsize, mi_row, mi_col, ss);
     const int availUC = (ss && bh == 1) ? (mi_row - 2 >= tR0) : availU;
@@ -346,6 +385,19 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
         __threadfence();
         st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 1);
         if (trace) trace[2] = gtimer();
+    }
+    {   // the dependents whose last luma dependency this was enter the ready queue
+        const uint32_t me = (uint32_t)sb * SB_MAX_LEAVES + li;
+        const int n = F.revCnt[me];
+        const uint32_t o = F.revOff[me];
+        __threadfence();
+        for (int k = lane; k < n; k += 32) {
+            const uint32_t d = F.revList[o + k];
+            if (atomicSub(F.depCnt + d, 1) == 1) {
+                __threadfence();
+                push_ready(F, d);
+            }
+        }
     }
     // ================= chroma =================
     int uv = 0, duv = 0, aU = 0, aV = 0, eobU = 0, eobV = 0;
@@ -575,7 +627,9 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
     }
 }
 
-// persistent grid of independent warps over the global leaf queue
+// persistent grid of independent warps over the ready queue: a warp takes the next slot, waits until a leaf has been
+// written there (bounded in time), and runs it
+constexpr unsigned long long READY_WAIT_NS = 4000000000ull;
 template <int BD>
 __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__restrict__ Fp) {
     typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
@@ -586,17 +640,29 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
     const int lane = lane_id();
     const RateTabs T = rate_tabs_stage(S.T, F.qctx, threadIdx.x, blockDim.x);
     __syncthreads();
-    const uint32_t total = *F.leafTotal;
+    const int total = (int)*F.leafTotal;
     for (;;) {
-        if (lane == 0) Wp.job = atomicAdd(F.queue, 1);
-        __syncwarp();
-        const uint32_t qi = (uint32_t)Wp.job;
-        __syncwarp();
-        if (qi >= total) break;
-        const uint32_t e = F.leafQueue[qi];
-        unsigned long long *trace = F.leafTrace ? F.leafTrace + (size_t)qi * 4 : nullptr;
-        if (trace && lane == 0) trace[0] = gtimer();
-        rc_leaf<BD, Px>(F, Wp, T, (int)(e >> 8), (int)(e & 255), trace);
+        int e = 0, h = 0;
+        if (lane == 0) {
+            h = atomicAdd(F.queue, 1);
+            if (h >= total) {
+                e = -1;
+            } else {
+                const unsigned long long t0 = gtimer();
+                while ((e = ld_acquire((const int *)F.leafQueue + h)) == 0) {
+                    if (gtimer() - t0 > READY_WAIT_NS || *(volatile int *)F.err) break;
+                    __nanosleep(128);
+                }
+                if (e == 0) { atomicCAS(F.err, 0, KERR_WAIT_LEAF); e = -1; }
+                if (F.leafTrace) { F.leafTrace[(size_t)h * 4] = t0; F.leafTrace[(size_t)h * 4 + 1] = gtimer(); }
+            }
+        }
+        e = __shfl_sync(0xffffffffu, e, 0);
+        h = __shfl_sync(0xffffffffu, h, 0);
+        if (e < 0) break;
+        const uint32_t id = (uint32_t)e - 1;
+        unsigned long long *trace = F.leafTrace ? F.leafTrace + (size_t)h * 4 : nullptr;
+        rc_leaf<BD, Px>(F, Wp, T, (int)(id >> 8), (int)(id & 255), trace);
     }
 }
 
@@ -610,6 +676,9 @@ __global__ void k_leaf_prep(const FrameDesc *__restrict__ Fp, int nSb) {
     const int nl = F.nLeaves[sb];
     om[tid] = 255;
     F.leafDone[(size_t)sb * SB_MAX_LEAVES + tid] = 0;
+    F.revCnt[(size_t)sb * SB_MAX_LEAVES + tid] = 0;
+    F.revFill[(size_t)sb * SB_MAX_LEAVES + tid] = 0;
+    F.leafQueue[(size_t)sb * SB_MAX_LEAVES + tid] = 0;
     __syncthreads();
     if (tid < nl) {
         const Leaf l = F.leaves[(size_t)sb * SB_MAX_LEAVES + tid];
@@ -665,11 +734,34 @@ __global__ void k_leaf_queue_scan(const FrameDesc *__restrict__ Fp, int nSb) {
     }
     if (tid == 1023) *F.leafTotal = sN[1023];
 }
-__global__ void k_leaf_queue_fill(const FrameDesc *__restrict__ Fp, int nSb) {
+// The dataflow graph of the closed loop, one thread per leaf, in three passes: 0 counts each leaf's luma dependencies
+// and its dependents, 1 gives each leaf its range of revList and queues the leaves without dependencies, 2 writes the
+// dependents.
+template <int PASS>
+__global__ void k_leaf_deps(const FrameDesc *__restrict__ Fp, int nSb) {
     const FrameDesc &F = *Fp;
     const int sb = blockIdx.x, tid = threadIdx.x;
-    if (sb >= nSb) return;
-    if (tid < F.nLeaves[sb]) F.leafQueue[F.leafStart[sb] + tid] = ((uint32_t)sb << 8) | (uint32_t)tid;
+    if (sb >= nSb || tid >= F.nLeaves[sb]) return;
+    const uint32_t me = (uint32_t)sb * SB_MAX_LEAVES + tid;
+    const uint32_t cap = (uint32_t)nSb * REV_PER_SB;   // never reached (see REV_PER_SB); checked all the same
+    if (PASS == 1) {
+        const uint32_t off = (uint32_t)atomicAdd(F.queue + 2, F.revCnt[me]);
+        F.revOff[me] = off;
+        if (off + (uint32_t)F.revCnt[me] > cap) atomicCAS(F.err, 0, KERR_CAPACITY);
+        if (F.depCnt[me] == 0) push_ready(F, me);
+        return;
+    }
+    uint32_t d[72];
+    const int n = luma_deps(F, sb, tid, d);
+    if (PASS == 0) F.depCnt[me] = n;
+    for (int k = 0; k < n; k++) {
+        if (PASS == 0) {
+            atomicAdd(F.revCnt + d[k], 1);
+        } else {
+            const uint32_t at = F.revOff[d[k]] + (uint32_t)atomicAdd(F.revFill + d[k], 1);
+            if (at < cap) F.revList[at] = me;
+        }
+    }
 }
 
 // ---- pack: per-SB slots -> DecisionRecord arrays in decode order ----

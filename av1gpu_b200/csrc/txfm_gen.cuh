@@ -9,8 +9,7 @@
 #define __forceinline__ inline
 #endif
 __host__ __device__ __forceinline__ int32_t rnd12(int32_t x) { return (x + 2048) >> 12; }
-__host__ __device__ __forceinline__ int64_t rnd12w(int64_t x) { return (x + 2048) >> 12; }
-__host__ __device__ __forceinline__ int32_t clampr(int64_t v, int32_t lo, int32_t hi) { return (int32_t)(v < lo ? lo : (v > hi ? hi : v)); }
+__host__ __device__ __forceinline__ int32_t clampr(int32_t v, int32_t lo, int32_t hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 __host__ __device__ __forceinline__ void fwd_dct4(int32_t *T) {
     { const int32_t x_ = T[1], y_ = T[2]; T[1] = x_ + y_; T[2] = x_ - y_; }
@@ -37,10 +36,10 @@ __host__ __device__ __forceinline__ uint32_t inv_dct4(int32_t *T, int r) {
         T[2] = c_[1];
         T[3] = c_[3];
     }
-    { const int64_t x_ = rnd12w((int64_t)T[0] * 2896 - (int64_t)T[1] * 2896), y_ = rnd12w((int64_t)T[0] * 2896 + (int64_t)T[1] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = (int32_t)x_; T[0] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[2] * 1567 - (int64_t)T[3] * 3784), y_ = rnd12w((int64_t)T[2] * 3784 + (int64_t)T[3] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[2] = (int32_t)x_; T[3] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[3]; T[0] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[2]; T[1] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[0] * 2896 - T[1] * 2896), y_ = rnd12(T[0] * 2896 + T[1] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = x_; T[0] = y_; }
+    { const int32_t x_ = rnd12(T[2] * 1567 - T[3] * 3784), y_ = rnd12(T[2] * 3784 + T[3] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[2] = x_; T[3] = y_; }
+    { const int32_t x_ = T[0], y_ = T[3]; T[0] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[2]; T[1] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
     return e_;
 }
 __host__ __device__ __forceinline__ void fwd_dct8(int32_t *T) {
@@ -85,19 +84,19 @@ __host__ __device__ __forceinline__ uint32_t inv_dct8(int32_t *T, int r) {
         T[6] = c_[3];
         T[7] = c_[7];
     }
-    { const int64_t x_ = rnd12w((int64_t)T[4] * 799 - (int64_t)T[7] * 4017), y_ = rnd12w((int64_t)T[4] * 4017 + (int64_t)T[7] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[4] = (int32_t)x_; T[7] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[5] * 3406 - (int64_t)T[6] * 2276), y_ = rnd12w((int64_t)T[5] * 2276 + (int64_t)T[6] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[0] * 2896 - (int64_t)T[1] * 2896), y_ = rnd12w((int64_t)T[0] * 2896 + (int64_t)T[1] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = (int32_t)x_; T[0] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[2] * 1567 - (int64_t)T[3] * 3784), y_ = rnd12w((int64_t)T[2] * 3784 + (int64_t)T[3] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[2] = (int32_t)x_; T[3] = (int32_t)y_; }
-    { const int64_t x_ = T[4], y_ = T[5]; T[4] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[6]; T[7] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[0], y_ = T[3]; T[0] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[2]; T[1] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[6] * 2896 - (int64_t)T[5] * 2896), y_ = rnd12w((int64_t)T[6] * 2896 + (int64_t)T[5] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[7]; T[0] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[6]; T[1] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[5]; T[2] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[4]; T[3] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[4] * 799 - T[7] * 4017), y_ = rnd12(T[4] * 4017 + T[7] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[4] = x_; T[7] = y_; }
+    { const int32_t x_ = rnd12(T[5] * 3406 - T[6] * 2276), y_ = rnd12(T[5] * 2276 + T[6] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[6] = y_; }
+    { const int32_t x_ = rnd12(T[0] * 2896 - T[1] * 2896), y_ = rnd12(T[0] * 2896 + T[1] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = x_; T[0] = y_; }
+    { const int32_t x_ = rnd12(T[2] * 1567 - T[3] * 3784), y_ = rnd12(T[2] * 3784 + T[3] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[2] = x_; T[3] = y_; }
+    { const int32_t x_ = T[4], y_ = T[5]; T[4] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[6]; T[7] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[0], y_ = T[3]; T[0] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[2]; T[1] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[6] * 2896 - T[5] * 2896), y_ = rnd12(T[6] * 2896 + T[5] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[6] = y_; }
+    { const int32_t x_ = T[0], y_ = T[7]; T[0] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[6]; T[1] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[5]; T[2] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[4]; T[3] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
     return e_;
 }
 __host__ __device__ __forceinline__ void fwd_dct16(int32_t *T) {
@@ -182,43 +181,43 @@ __host__ __device__ __forceinline__ uint32_t inv_dct16(int32_t *T, int r) {
         T[14] = c_[7];
         T[15] = c_[15];
     }
-    { const int64_t x_ = rnd12w((int64_t)T[8] * 401 - (int64_t)T[15] * 4076), y_ = rnd12w((int64_t)T[8] * 4076 + (int64_t)T[15] * 401); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[8] = (int32_t)x_; T[15] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[9] * 3166 - (int64_t)T[14] * 2598), y_ = rnd12w((int64_t)T[9] * 2598 + (int64_t)T[14] * 3166); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = (int32_t)x_; T[14] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[10] * 1931 - (int64_t)T[13] * 3612), y_ = rnd12w((int64_t)T[10] * 3612 + (int64_t)T[13] * 1931); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = (int32_t)x_; T[13] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[11] * 3920 - (int64_t)T[12] * 1189), y_ = rnd12w((int64_t)T[11] * 1189 + (int64_t)T[12] * 3920); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = (int32_t)x_; T[12] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[4] * 799 - (int64_t)T[7] * 4017), y_ = rnd12w((int64_t)T[4] * 4017 + (int64_t)T[7] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[4] = (int32_t)x_; T[7] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[5] * 3406 - (int64_t)T[6] * 2276), y_ = rnd12w((int64_t)T[5] * 2276 + (int64_t)T[6] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = T[8], y_ = T[9]; T[8] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[11], y_ = T[10]; T[11] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[12], y_ = T[13]; T[12] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[15], y_ = T[14]; T[15] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[0] * 2896 - (int64_t)T[1] * 2896), y_ = rnd12w((int64_t)T[0] * 2896 + (int64_t)T[1] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = (int32_t)x_; T[0] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[2] * 1567 - (int64_t)T[3] * 3784), y_ = rnd12w((int64_t)T[2] * 3784 + (int64_t)T[3] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[2] = (int32_t)x_; T[3] = (int32_t)y_; }
-    { const int64_t x_ = T[4], y_ = T[5]; T[4] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[6]; T[7] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[14] * 1567 - (int64_t)T[9] * 3784), y_ = rnd12w((int64_t)T[14] * 3784 + (int64_t)T[9] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = (int32_t)x_; T[14] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[13] * -3784 - (int64_t)T[10] * 1567), y_ = rnd12w((int64_t)T[13] * 1567 + (int64_t)T[10] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = (int32_t)x_; T[13] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[3]; T[0] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[2]; T[1] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[6] * 2896 - (int64_t)T[5] * 2896), y_ = rnd12w((int64_t)T[6] * 2896 + (int64_t)T[5] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = T[8], y_ = T[11]; T[8] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[9], y_ = T[10]; T[9] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[15], y_ = T[12]; T[15] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[14], y_ = T[13]; T[14] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[0], y_ = T[7]; T[0] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[6]; T[1] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[5]; T[2] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[4]; T[3] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[13] * 2896 - (int64_t)T[10] * 2896), y_ = rnd12w((int64_t)T[13] * 2896 + (int64_t)T[10] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = (int32_t)x_; T[13] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[12] * 2896 - (int64_t)T[11] * 2896), y_ = rnd12w((int64_t)T[12] * 2896 + (int64_t)T[11] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = (int32_t)x_; T[12] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[15]; T[0] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[14]; T[1] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[13]; T[2] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[12]; T[3] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[4], y_ = T[11]; T[4] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[5], y_ = T[10]; T[5] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[6], y_ = T[9]; T[6] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[8]; T[7] = clampr(x_ + y_, lo_, hi_); T[8] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[8] * 401 - T[15] * 4076), y_ = rnd12(T[8] * 4076 + T[15] * 401); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[8] = x_; T[15] = y_; }
+    { const int32_t x_ = rnd12(T[9] * 3166 - T[14] * 2598), y_ = rnd12(T[9] * 2598 + T[14] * 3166); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = x_; T[14] = y_; }
+    { const int32_t x_ = rnd12(T[10] * 1931 - T[13] * 3612), y_ = rnd12(T[10] * 3612 + T[13] * 1931); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = x_; T[13] = y_; }
+    { const int32_t x_ = rnd12(T[11] * 3920 - T[12] * 1189), y_ = rnd12(T[11] * 1189 + T[12] * 3920); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = x_; T[12] = y_; }
+    { const int32_t x_ = rnd12(T[4] * 799 - T[7] * 4017), y_ = rnd12(T[4] * 4017 + T[7] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[4] = x_; T[7] = y_; }
+    { const int32_t x_ = rnd12(T[5] * 3406 - T[6] * 2276), y_ = rnd12(T[5] * 2276 + T[6] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[6] = y_; }
+    { const int32_t x_ = T[8], y_ = T[9]; T[8] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[11], y_ = T[10]; T[11] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[12], y_ = T[13]; T[12] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[15], y_ = T[14]; T[15] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[0] * 2896 - T[1] * 2896), y_ = rnd12(T[0] * 2896 + T[1] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = x_; T[0] = y_; }
+    { const int32_t x_ = rnd12(T[2] * 1567 - T[3] * 3784), y_ = rnd12(T[2] * 3784 + T[3] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[2] = x_; T[3] = y_; }
+    { const int32_t x_ = T[4], y_ = T[5]; T[4] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[6]; T[7] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[14] * 1567 - T[9] * 3784), y_ = rnd12(T[14] * 3784 + T[9] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = x_; T[14] = y_; }
+    { const int32_t x_ = rnd12(T[13] * -3784 - T[10] * 1567), y_ = rnd12(T[13] * 1567 + T[10] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = x_; T[13] = y_; }
+    { const int32_t x_ = T[0], y_ = T[3]; T[0] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[2]; T[1] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[6] * 2896 - T[5] * 2896), y_ = rnd12(T[6] * 2896 + T[5] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[6] = y_; }
+    { const int32_t x_ = T[8], y_ = T[11]; T[8] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[9], y_ = T[10]; T[9] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[15], y_ = T[12]; T[15] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[14], y_ = T[13]; T[14] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[0], y_ = T[7]; T[0] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[6]; T[1] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[5]; T[2] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[4]; T[3] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[13] * 2896 - T[10] * 2896), y_ = rnd12(T[13] * 2896 + T[10] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = x_; T[13] = y_; }
+    { const int32_t x_ = rnd12(T[12] * 2896 - T[11] * 2896), y_ = rnd12(T[12] * 2896 + T[11] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = x_; T[12] = y_; }
+    { const int32_t x_ = T[0], y_ = T[15]; T[0] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[14]; T[1] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[13]; T[2] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[12]; T[3] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[4], y_ = T[11]; T[4] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[5], y_ = T[10]; T[5] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[6], y_ = T[9]; T[6] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[8]; T[7] = clampr(x_ + y_, lo_, hi_); T[8] = clampr(x_ - y_, lo_, hi_); }
     return e_;
 }
 __host__ __device__ __forceinline__ void fwd_dct32(int32_t *T) {
@@ -395,103 +394,103 @@ __host__ __device__ __forceinline__ uint32_t inv_dct32(int32_t *T, int r) {
         T[30] = c_[15];
         T[31] = c_[31];
     }
-    { const int64_t x_ = rnd12w((int64_t)T[16] * 201 - (int64_t)T[31] * 4091), y_ = rnd12w((int64_t)T[16] * 4091 + (int64_t)T[31] * 201); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[16] = (int32_t)x_; T[31] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[17] * 3035 - (int64_t)T[30] * 2751), y_ = rnd12w((int64_t)T[17] * 2751 + (int64_t)T[30] * 3035); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[17] = (int32_t)x_; T[30] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[18] * 1751 - (int64_t)T[29] * 3703), y_ = rnd12w((int64_t)T[18] * 3703 + (int64_t)T[29] * 1751); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = (int32_t)x_; T[29] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[19] * 3857 - (int64_t)T[28] * 1380), y_ = rnd12w((int64_t)T[19] * 1380 + (int64_t)T[28] * 3857); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[19] = (int32_t)x_; T[28] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[20] * 995 - (int64_t)T[27] * 3973), y_ = rnd12w((int64_t)T[20] * 3973 + (int64_t)T[27] * 995); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = (int32_t)x_; T[27] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[21] * 3513 - (int64_t)T[26] * 2106), y_ = rnd12w((int64_t)T[21] * 2106 + (int64_t)T[26] * 3513); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = (int32_t)x_; T[26] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[22] * 2440 - (int64_t)T[25] * 3290), y_ = rnd12w((int64_t)T[22] * 3290 + (int64_t)T[25] * 2440); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = (int32_t)x_; T[25] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[23] * 4052 - (int64_t)T[24] * 601), y_ = rnd12w((int64_t)T[23] * 601 + (int64_t)T[24] * 4052); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[23] = (int32_t)x_; T[24] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[8] * 401 - (int64_t)T[15] * 4076), y_ = rnd12w((int64_t)T[8] * 4076 + (int64_t)T[15] * 401); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[8] = (int32_t)x_; T[15] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[9] * 3166 - (int64_t)T[14] * 2598), y_ = rnd12w((int64_t)T[9] * 2598 + (int64_t)T[14] * 3166); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = (int32_t)x_; T[14] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[10] * 1931 - (int64_t)T[13] * 3612), y_ = rnd12w((int64_t)T[10] * 3612 + (int64_t)T[13] * 1931); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = (int32_t)x_; T[13] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[11] * 3920 - (int64_t)T[12] * 1189), y_ = rnd12w((int64_t)T[11] * 1189 + (int64_t)T[12] * 3920); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = (int32_t)x_; T[12] = (int32_t)y_; }
-    { const int64_t x_ = T[16], y_ = T[17]; T[16] = clampr(x_ + y_, lo_, hi_); T[17] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[19], y_ = T[18]; T[19] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[20], y_ = T[21]; T[20] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[23], y_ = T[22]; T[23] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[24], y_ = T[25]; T[24] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[27], y_ = T[26]; T[27] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[28], y_ = T[29]; T[28] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[31], y_ = T[30]; T[31] = clampr(x_ + y_, lo_, hi_); T[30] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[4] * 799 - (int64_t)T[7] * 4017), y_ = rnd12w((int64_t)T[4] * 4017 + (int64_t)T[7] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[4] = (int32_t)x_; T[7] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[5] * 3406 - (int64_t)T[6] * 2276), y_ = rnd12w((int64_t)T[5] * 2276 + (int64_t)T[6] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = T[8], y_ = T[9]; T[8] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[11], y_ = T[10]; T[11] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[12], y_ = T[13]; T[12] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[15], y_ = T[14]; T[15] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[30] * 799 - (int64_t)T[17] * 4017), y_ = rnd12w((int64_t)T[30] * 4017 + (int64_t)T[17] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[17] = (int32_t)x_; T[30] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[29] * -4017 - (int64_t)T[18] * 799), y_ = rnd12w((int64_t)T[29] * 799 + (int64_t)T[18] * -4017); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = (int32_t)x_; T[29] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[26] * 3406 - (int64_t)T[21] * 2276), y_ = rnd12w((int64_t)T[26] * 2276 + (int64_t)T[21] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = (int32_t)x_; T[26] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[25] * -2276 - (int64_t)T[22] * 3406), y_ = rnd12w((int64_t)T[25] * 3406 + (int64_t)T[22] * -2276); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = (int32_t)x_; T[25] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[0] * 2896 - (int64_t)T[1] * 2896), y_ = rnd12w((int64_t)T[0] * 2896 + (int64_t)T[1] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = (int32_t)x_; T[0] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[2] * 1567 - (int64_t)T[3] * 3784), y_ = rnd12w((int64_t)T[2] * 3784 + (int64_t)T[3] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[2] = (int32_t)x_; T[3] = (int32_t)y_; }
-    { const int64_t x_ = T[4], y_ = T[5]; T[4] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[6]; T[7] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[14] * 1567 - (int64_t)T[9] * 3784), y_ = rnd12w((int64_t)T[14] * 3784 + (int64_t)T[9] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = (int32_t)x_; T[14] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[13] * -3784 - (int64_t)T[10] * 1567), y_ = rnd12w((int64_t)T[13] * 1567 + (int64_t)T[10] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = (int32_t)x_; T[13] = (int32_t)y_; }
-    { const int64_t x_ = T[16], y_ = T[19]; T[16] = clampr(x_ + y_, lo_, hi_); T[19] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[17], y_ = T[18]; T[17] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[23], y_ = T[20]; T[23] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[22], y_ = T[21]; T[22] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[24], y_ = T[27]; T[24] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[25], y_ = T[26]; T[25] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[31], y_ = T[28]; T[31] = clampr(x_ + y_, lo_, hi_); T[28] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[30], y_ = T[29]; T[30] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[0], y_ = T[3]; T[0] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[2]; T[1] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[6] * 2896 - (int64_t)T[5] * 2896), y_ = rnd12w((int64_t)T[6] * 2896 + (int64_t)T[5] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = T[8], y_ = T[11]; T[8] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[9], y_ = T[10]; T[9] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[15], y_ = T[12]; T[15] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[14], y_ = T[13]; T[14] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[29] * 1567 - (int64_t)T[18] * 3784), y_ = rnd12w((int64_t)T[29] * 3784 + (int64_t)T[18] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = (int32_t)x_; T[29] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[28] * 1567 - (int64_t)T[19] * 3784), y_ = rnd12w((int64_t)T[28] * 3784 + (int64_t)T[19] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[19] = (int32_t)x_; T[28] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[27] * -3784 - (int64_t)T[20] * 1567), y_ = rnd12w((int64_t)T[27] * 1567 + (int64_t)T[20] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = (int32_t)x_; T[27] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[26] * -3784 - (int64_t)T[21] * 1567), y_ = rnd12w((int64_t)T[26] * 1567 + (int64_t)T[21] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = (int32_t)x_; T[26] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[7]; T[0] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[6]; T[1] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[5]; T[2] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[4]; T[3] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[13] * 2896 - (int64_t)T[10] * 2896), y_ = rnd12w((int64_t)T[13] * 2896 + (int64_t)T[10] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = (int32_t)x_; T[13] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[12] * 2896 - (int64_t)T[11] * 2896), y_ = rnd12w((int64_t)T[12] * 2896 + (int64_t)T[11] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = (int32_t)x_; T[12] = (int32_t)y_; }
-    { const int64_t x_ = T[16], y_ = T[23]; T[16] = clampr(x_ + y_, lo_, hi_); T[23] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[17], y_ = T[22]; T[17] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[18], y_ = T[21]; T[18] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[19], y_ = T[20]; T[19] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[31], y_ = T[24]; T[31] = clampr(x_ + y_, lo_, hi_); T[24] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[30], y_ = T[25]; T[30] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[29], y_ = T[26]; T[29] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[28], y_ = T[27]; T[28] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[0], y_ = T[15]; T[0] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[14]; T[1] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[13]; T[2] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[12]; T[3] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[4], y_ = T[11]; T[4] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[5], y_ = T[10]; T[5] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[6], y_ = T[9]; T[6] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[8]; T[7] = clampr(x_ + y_, lo_, hi_); T[8] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[27] * 2896 - (int64_t)T[20] * 2896), y_ = rnd12w((int64_t)T[27] * 2896 + (int64_t)T[20] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = (int32_t)x_; T[27] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[26] * 2896 - (int64_t)T[21] * 2896), y_ = rnd12w((int64_t)T[26] * 2896 + (int64_t)T[21] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = (int32_t)x_; T[26] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[25] * 2896 - (int64_t)T[22] * 2896), y_ = rnd12w((int64_t)T[25] * 2896 + (int64_t)T[22] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = (int32_t)x_; T[25] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[24] * 2896 - (int64_t)T[23] * 2896), y_ = rnd12w((int64_t)T[24] * 2896 + (int64_t)T[23] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[23] = (int32_t)x_; T[24] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[31]; T[0] = clampr(x_ + y_, lo_, hi_); T[31] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[30]; T[1] = clampr(x_ + y_, lo_, hi_); T[30] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[29]; T[2] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[28]; T[3] = clampr(x_ + y_, lo_, hi_); T[28] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[4], y_ = T[27]; T[4] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[5], y_ = T[26]; T[5] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[6], y_ = T[25]; T[6] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[24]; T[7] = clampr(x_ + y_, lo_, hi_); T[24] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[8], y_ = T[23]; T[8] = clampr(x_ + y_, lo_, hi_); T[23] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[9], y_ = T[22]; T[9] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[10], y_ = T[21]; T[10] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[11], y_ = T[20]; T[11] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[12], y_ = T[19]; T[12] = clampr(x_ + y_, lo_, hi_); T[19] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[13], y_ = T[18]; T[13] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[14], y_ = T[17]; T[14] = clampr(x_ + y_, lo_, hi_); T[17] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[15], y_ = T[16]; T[15] = clampr(x_ + y_, lo_, hi_); T[16] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[16] * 201 - T[31] * 4091), y_ = rnd12(T[16] * 4091 + T[31] * 201); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[16] = x_; T[31] = y_; }
+    { const int32_t x_ = rnd12(T[17] * 3035 - T[30] * 2751), y_ = rnd12(T[17] * 2751 + T[30] * 3035); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[17] = x_; T[30] = y_; }
+    { const int32_t x_ = rnd12(T[18] * 1751 - T[29] * 3703), y_ = rnd12(T[18] * 3703 + T[29] * 1751); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = x_; T[29] = y_; }
+    { const int32_t x_ = rnd12(T[19] * 3857 - T[28] * 1380), y_ = rnd12(T[19] * 1380 + T[28] * 3857); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[19] = x_; T[28] = y_; }
+    { const int32_t x_ = rnd12(T[20] * 995 - T[27] * 3973), y_ = rnd12(T[20] * 3973 + T[27] * 995); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = x_; T[27] = y_; }
+    { const int32_t x_ = rnd12(T[21] * 3513 - T[26] * 2106), y_ = rnd12(T[21] * 2106 + T[26] * 3513); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = x_; T[26] = y_; }
+    { const int32_t x_ = rnd12(T[22] * 2440 - T[25] * 3290), y_ = rnd12(T[22] * 3290 + T[25] * 2440); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = x_; T[25] = y_; }
+    { const int32_t x_ = rnd12(T[23] * 4052 - T[24] * 601), y_ = rnd12(T[23] * 601 + T[24] * 4052); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[23] = x_; T[24] = y_; }
+    { const int32_t x_ = rnd12(T[8] * 401 - T[15] * 4076), y_ = rnd12(T[8] * 4076 + T[15] * 401); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[8] = x_; T[15] = y_; }
+    { const int32_t x_ = rnd12(T[9] * 3166 - T[14] * 2598), y_ = rnd12(T[9] * 2598 + T[14] * 3166); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = x_; T[14] = y_; }
+    { const int32_t x_ = rnd12(T[10] * 1931 - T[13] * 3612), y_ = rnd12(T[10] * 3612 + T[13] * 1931); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = x_; T[13] = y_; }
+    { const int32_t x_ = rnd12(T[11] * 3920 - T[12] * 1189), y_ = rnd12(T[11] * 1189 + T[12] * 3920); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = x_; T[12] = y_; }
+    { const int32_t x_ = T[16], y_ = T[17]; T[16] = clampr(x_ + y_, lo_, hi_); T[17] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[19], y_ = T[18]; T[19] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[20], y_ = T[21]; T[20] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[23], y_ = T[22]; T[23] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[24], y_ = T[25]; T[24] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[27], y_ = T[26]; T[27] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[28], y_ = T[29]; T[28] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[31], y_ = T[30]; T[31] = clampr(x_ + y_, lo_, hi_); T[30] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[4] * 799 - T[7] * 4017), y_ = rnd12(T[4] * 4017 + T[7] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[4] = x_; T[7] = y_; }
+    { const int32_t x_ = rnd12(T[5] * 3406 - T[6] * 2276), y_ = rnd12(T[5] * 2276 + T[6] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[6] = y_; }
+    { const int32_t x_ = T[8], y_ = T[9]; T[8] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[11], y_ = T[10]; T[11] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[12], y_ = T[13]; T[12] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[15], y_ = T[14]; T[15] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[30] * 799 - T[17] * 4017), y_ = rnd12(T[30] * 4017 + T[17] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[17] = x_; T[30] = y_; }
+    { const int32_t x_ = rnd12(T[29] * -4017 - T[18] * 799), y_ = rnd12(T[29] * 799 + T[18] * -4017); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = x_; T[29] = y_; }
+    { const int32_t x_ = rnd12(T[26] * 3406 - T[21] * 2276), y_ = rnd12(T[26] * 2276 + T[21] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = x_; T[26] = y_; }
+    { const int32_t x_ = rnd12(T[25] * -2276 - T[22] * 3406), y_ = rnd12(T[25] * 3406 + T[22] * -2276); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = x_; T[25] = y_; }
+    { const int32_t x_ = rnd12(T[0] * 2896 - T[1] * 2896), y_ = rnd12(T[0] * 2896 + T[1] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = x_; T[0] = y_; }
+    { const int32_t x_ = rnd12(T[2] * 1567 - T[3] * 3784), y_ = rnd12(T[2] * 3784 + T[3] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[2] = x_; T[3] = y_; }
+    { const int32_t x_ = T[4], y_ = T[5]; T[4] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[6]; T[7] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[14] * 1567 - T[9] * 3784), y_ = rnd12(T[14] * 3784 + T[9] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = x_; T[14] = y_; }
+    { const int32_t x_ = rnd12(T[13] * -3784 - T[10] * 1567), y_ = rnd12(T[13] * 1567 + T[10] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = x_; T[13] = y_; }
+    { const int32_t x_ = T[16], y_ = T[19]; T[16] = clampr(x_ + y_, lo_, hi_); T[19] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[17], y_ = T[18]; T[17] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[23], y_ = T[20]; T[23] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[22], y_ = T[21]; T[22] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[24], y_ = T[27]; T[24] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[25], y_ = T[26]; T[25] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[31], y_ = T[28]; T[31] = clampr(x_ + y_, lo_, hi_); T[28] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[30], y_ = T[29]; T[30] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[0], y_ = T[3]; T[0] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[2]; T[1] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[6] * 2896 - T[5] * 2896), y_ = rnd12(T[6] * 2896 + T[5] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[6] = y_; }
+    { const int32_t x_ = T[8], y_ = T[11]; T[8] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[9], y_ = T[10]; T[9] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[15], y_ = T[12]; T[15] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[14], y_ = T[13]; T[14] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[29] * 1567 - T[18] * 3784), y_ = rnd12(T[29] * 3784 + T[18] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = x_; T[29] = y_; }
+    { const int32_t x_ = rnd12(T[28] * 1567 - T[19] * 3784), y_ = rnd12(T[28] * 3784 + T[19] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[19] = x_; T[28] = y_; }
+    { const int32_t x_ = rnd12(T[27] * -3784 - T[20] * 1567), y_ = rnd12(T[27] * 1567 + T[20] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = x_; T[27] = y_; }
+    { const int32_t x_ = rnd12(T[26] * -3784 - T[21] * 1567), y_ = rnd12(T[26] * 1567 + T[21] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = x_; T[26] = y_; }
+    { const int32_t x_ = T[0], y_ = T[7]; T[0] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[6]; T[1] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[5]; T[2] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[4]; T[3] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[13] * 2896 - T[10] * 2896), y_ = rnd12(T[13] * 2896 + T[10] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = x_; T[13] = y_; }
+    { const int32_t x_ = rnd12(T[12] * 2896 - T[11] * 2896), y_ = rnd12(T[12] * 2896 + T[11] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = x_; T[12] = y_; }
+    { const int32_t x_ = T[16], y_ = T[23]; T[16] = clampr(x_ + y_, lo_, hi_); T[23] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[17], y_ = T[22]; T[17] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[18], y_ = T[21]; T[18] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[19], y_ = T[20]; T[19] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[31], y_ = T[24]; T[31] = clampr(x_ + y_, lo_, hi_); T[24] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[30], y_ = T[25]; T[30] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[29], y_ = T[26]; T[29] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[28], y_ = T[27]; T[28] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[0], y_ = T[15]; T[0] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[14]; T[1] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[13]; T[2] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[12]; T[3] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[4], y_ = T[11]; T[4] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[5], y_ = T[10]; T[5] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[6], y_ = T[9]; T[6] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[8]; T[7] = clampr(x_ + y_, lo_, hi_); T[8] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[27] * 2896 - T[20] * 2896), y_ = rnd12(T[27] * 2896 + T[20] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = x_; T[27] = y_; }
+    { const int32_t x_ = rnd12(T[26] * 2896 - T[21] * 2896), y_ = rnd12(T[26] * 2896 + T[21] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = x_; T[26] = y_; }
+    { const int32_t x_ = rnd12(T[25] * 2896 - T[22] * 2896), y_ = rnd12(T[25] * 2896 + T[22] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = x_; T[25] = y_; }
+    { const int32_t x_ = rnd12(T[24] * 2896 - T[23] * 2896), y_ = rnd12(T[24] * 2896 + T[23] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[23] = x_; T[24] = y_; }
+    { const int32_t x_ = T[0], y_ = T[31]; T[0] = clampr(x_ + y_, lo_, hi_); T[31] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[30]; T[1] = clampr(x_ + y_, lo_, hi_); T[30] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[29]; T[2] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[28]; T[3] = clampr(x_ + y_, lo_, hi_); T[28] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[4], y_ = T[27]; T[4] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[5], y_ = T[26]; T[5] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[6], y_ = T[25]; T[6] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[24]; T[7] = clampr(x_ + y_, lo_, hi_); T[24] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[8], y_ = T[23]; T[8] = clampr(x_ + y_, lo_, hi_); T[23] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[9], y_ = T[22]; T[9] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[10], y_ = T[21]; T[10] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[11], y_ = T[20]; T[11] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[12], y_ = T[19]; T[12] = clampr(x_ + y_, lo_, hi_); T[19] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[13], y_ = T[18]; T[13] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[14], y_ = T[17]; T[14] = clampr(x_ + y_, lo_, hi_); T[17] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[15], y_ = T[16]; T[15] = clampr(x_ + y_, lo_, hi_); T[16] = clampr(x_ - y_, lo_, hi_); }
     return e_;
 }
 __host__ __device__ __forceinline__ void fwd_dct64(int32_t *T) {
@@ -876,247 +875,247 @@ __host__ __device__ __forceinline__ uint32_t inv_dct64(int32_t *T, int r) {
         T[62] = c_[31];
         T[63] = c_[63];
     }
-    { const int64_t x_ = rnd12w((int64_t)T[32] * 101 - (int64_t)T[63] * 4095), y_ = rnd12w((int64_t)T[32] * 4095 + (int64_t)T[63] * 101); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[32] = (int32_t)x_; T[63] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[33] * 2967 - (int64_t)T[62] * 2824), y_ = rnd12w((int64_t)T[33] * 2824 + (int64_t)T[62] * 2967); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[33] = (int32_t)x_; T[62] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[34] * 1660 - (int64_t)T[61] * 3745), y_ = rnd12w((int64_t)T[34] * 3745 + (int64_t)T[61] * 1660); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[34] = (int32_t)x_; T[61] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[35] * 3822 - (int64_t)T[60] * 1474), y_ = rnd12w((int64_t)T[35] * 1474 + (int64_t)T[60] * 3822); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[35] = (int32_t)x_; T[60] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[36] * 897 - (int64_t)T[59] * 3996), y_ = rnd12w((int64_t)T[36] * 3996 + (int64_t)T[59] * 897); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[36] = (int32_t)x_; T[59] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[37] * 3461 - (int64_t)T[58] * 2191), y_ = rnd12w((int64_t)T[37] * 2191 + (int64_t)T[58] * 3461); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[37] = (int32_t)x_; T[58] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[38] * 2359 - (int64_t)T[57] * 3349), y_ = rnd12w((int64_t)T[38] * 3349 + (int64_t)T[57] * 2359); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[38] = (int32_t)x_; T[57] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[39] * 4036 - (int64_t)T[56] * 700), y_ = rnd12w((int64_t)T[39] * 700 + (int64_t)T[56] * 4036); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[39] = (int32_t)x_; T[56] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[40] * 501 - (int64_t)T[55] * 4065), y_ = rnd12w((int64_t)T[40] * 4065 + (int64_t)T[55] * 501); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[40] = (int32_t)x_; T[55] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[41] * 3229 - (int64_t)T[54] * 2520), y_ = rnd12w((int64_t)T[41] * 2520 + (int64_t)T[54] * 3229); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[41] = (int32_t)x_; T[54] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[42] * 2019 - (int64_t)T[53] * 3564), y_ = rnd12w((int64_t)T[42] * 3564 + (int64_t)T[53] * 2019); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[42] = (int32_t)x_; T[53] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[43] * 3948 - (int64_t)T[52] * 1092), y_ = rnd12w((int64_t)T[43] * 1092 + (int64_t)T[52] * 3948); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[43] = (int32_t)x_; T[52] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[44] * 1285 - (int64_t)T[51] * 3889), y_ = rnd12w((int64_t)T[44] * 3889 + (int64_t)T[51] * 1285); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[44] = (int32_t)x_; T[51] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[45] * 3659 - (int64_t)T[50] * 1842), y_ = rnd12w((int64_t)T[45] * 1842 + (int64_t)T[50] * 3659); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[45] = (int32_t)x_; T[50] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[46] * 2675 - (int64_t)T[49] * 3102), y_ = rnd12w((int64_t)T[46] * 3102 + (int64_t)T[49] * 2675); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[46] = (int32_t)x_; T[49] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[47] * 4085 - (int64_t)T[48] * 301), y_ = rnd12w((int64_t)T[47] * 301 + (int64_t)T[48] * 4085); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[47] = (int32_t)x_; T[48] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[16] * 201 - (int64_t)T[31] * 4091), y_ = rnd12w((int64_t)T[16] * 4091 + (int64_t)T[31] * 201); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[16] = (int32_t)x_; T[31] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[17] * 3035 - (int64_t)T[30] * 2751), y_ = rnd12w((int64_t)T[17] * 2751 + (int64_t)T[30] * 3035); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[17] = (int32_t)x_; T[30] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[18] * 1751 - (int64_t)T[29] * 3703), y_ = rnd12w((int64_t)T[18] * 3703 + (int64_t)T[29] * 1751); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = (int32_t)x_; T[29] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[19] * 3857 - (int64_t)T[28] * 1380), y_ = rnd12w((int64_t)T[19] * 1380 + (int64_t)T[28] * 3857); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[19] = (int32_t)x_; T[28] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[20] * 995 - (int64_t)T[27] * 3973), y_ = rnd12w((int64_t)T[20] * 3973 + (int64_t)T[27] * 995); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = (int32_t)x_; T[27] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[21] * 3513 - (int64_t)T[26] * 2106), y_ = rnd12w((int64_t)T[21] * 2106 + (int64_t)T[26] * 3513); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = (int32_t)x_; T[26] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[22] * 2440 - (int64_t)T[25] * 3290), y_ = rnd12w((int64_t)T[22] * 3290 + (int64_t)T[25] * 2440); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = (int32_t)x_; T[25] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[23] * 4052 - (int64_t)T[24] * 601), y_ = rnd12w((int64_t)T[23] * 601 + (int64_t)T[24] * 4052); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[23] = (int32_t)x_; T[24] = (int32_t)y_; }
-    { const int64_t x_ = T[32], y_ = T[33]; T[32] = clampr(x_ + y_, lo_, hi_); T[33] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[35], y_ = T[34]; T[35] = clampr(x_ + y_, lo_, hi_); T[34] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[36], y_ = T[37]; T[36] = clampr(x_ + y_, lo_, hi_); T[37] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[39], y_ = T[38]; T[39] = clampr(x_ + y_, lo_, hi_); T[38] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[40], y_ = T[41]; T[40] = clampr(x_ + y_, lo_, hi_); T[41] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[43], y_ = T[42]; T[43] = clampr(x_ + y_, lo_, hi_); T[42] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[44], y_ = T[45]; T[44] = clampr(x_ + y_, lo_, hi_); T[45] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[47], y_ = T[46]; T[47] = clampr(x_ + y_, lo_, hi_); T[46] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[48], y_ = T[49]; T[48] = clampr(x_ + y_, lo_, hi_); T[49] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[51], y_ = T[50]; T[51] = clampr(x_ + y_, lo_, hi_); T[50] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[52], y_ = T[53]; T[52] = clampr(x_ + y_, lo_, hi_); T[53] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[55], y_ = T[54]; T[55] = clampr(x_ + y_, lo_, hi_); T[54] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[56], y_ = T[57]; T[56] = clampr(x_ + y_, lo_, hi_); T[57] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[59], y_ = T[58]; T[59] = clampr(x_ + y_, lo_, hi_); T[58] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[60], y_ = T[61]; T[60] = clampr(x_ + y_, lo_, hi_); T[61] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[63], y_ = T[62]; T[63] = clampr(x_ + y_, lo_, hi_); T[62] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[8] * 401 - (int64_t)T[15] * 4076), y_ = rnd12w((int64_t)T[8] * 4076 + (int64_t)T[15] * 401); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[8] = (int32_t)x_; T[15] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[9] * 3166 - (int64_t)T[14] * 2598), y_ = rnd12w((int64_t)T[9] * 2598 + (int64_t)T[14] * 3166); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = (int32_t)x_; T[14] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[10] * 1931 - (int64_t)T[13] * 3612), y_ = rnd12w((int64_t)T[10] * 3612 + (int64_t)T[13] * 1931); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = (int32_t)x_; T[13] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[11] * 3920 - (int64_t)T[12] * 1189), y_ = rnd12w((int64_t)T[11] * 1189 + (int64_t)T[12] * 3920); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = (int32_t)x_; T[12] = (int32_t)y_; }
-    { const int64_t x_ = T[16], y_ = T[17]; T[16] = clampr(x_ + y_, lo_, hi_); T[17] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[19], y_ = T[18]; T[19] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[20], y_ = T[21]; T[20] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[23], y_ = T[22]; T[23] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[24], y_ = T[25]; T[24] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[27], y_ = T[26]; T[27] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[28], y_ = T[29]; T[28] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[31], y_ = T[30]; T[31] = clampr(x_ + y_, lo_, hi_); T[30] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[62] * 401 - (int64_t)T[33] * 4076), y_ = rnd12w((int64_t)T[62] * 4076 + (int64_t)T[33] * 401); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[33] = (int32_t)x_; T[62] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[61] * -4076 - (int64_t)T[34] * 401), y_ = rnd12w((int64_t)T[61] * 401 + (int64_t)T[34] * -4076); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[34] = (int32_t)x_; T[61] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[58] * 3166 - (int64_t)T[37] * 2598), y_ = rnd12w((int64_t)T[58] * 2598 + (int64_t)T[37] * 3166); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[37] = (int32_t)x_; T[58] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[57] * -2598 - (int64_t)T[38] * 3166), y_ = rnd12w((int64_t)T[57] * 3166 + (int64_t)T[38] * -2598); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[38] = (int32_t)x_; T[57] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[54] * 1931 - (int64_t)T[41] * 3612), y_ = rnd12w((int64_t)T[54] * 3612 + (int64_t)T[41] * 1931); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[41] = (int32_t)x_; T[54] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[53] * -3612 - (int64_t)T[42] * 1931), y_ = rnd12w((int64_t)T[53] * 1931 + (int64_t)T[42] * -3612); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[42] = (int32_t)x_; T[53] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[50] * 3920 - (int64_t)T[45] * 1189), y_ = rnd12w((int64_t)T[50] * 1189 + (int64_t)T[45] * 3920); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[45] = (int32_t)x_; T[50] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[49] * -1189 - (int64_t)T[46] * 3920), y_ = rnd12w((int64_t)T[49] * 3920 + (int64_t)T[46] * -1189); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[46] = (int32_t)x_; T[49] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[4] * 799 - (int64_t)T[7] * 4017), y_ = rnd12w((int64_t)T[4] * 4017 + (int64_t)T[7] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[4] = (int32_t)x_; T[7] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[5] * 3406 - (int64_t)T[6] * 2276), y_ = rnd12w((int64_t)T[5] * 2276 + (int64_t)T[6] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = T[8], y_ = T[9]; T[8] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[11], y_ = T[10]; T[11] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[12], y_ = T[13]; T[12] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[15], y_ = T[14]; T[15] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[30] * 799 - (int64_t)T[17] * 4017), y_ = rnd12w((int64_t)T[30] * 4017 + (int64_t)T[17] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[17] = (int32_t)x_; T[30] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[29] * -4017 - (int64_t)T[18] * 799), y_ = rnd12w((int64_t)T[29] * 799 + (int64_t)T[18] * -4017); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = (int32_t)x_; T[29] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[26] * 3406 - (int64_t)T[21] * 2276), y_ = rnd12w((int64_t)T[26] * 2276 + (int64_t)T[21] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = (int32_t)x_; T[26] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[25] * -2276 - (int64_t)T[22] * 3406), y_ = rnd12w((int64_t)T[25] * 3406 + (int64_t)T[22] * -2276); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = (int32_t)x_; T[25] = (int32_t)y_; }
-    { const int64_t x_ = T[32], y_ = T[35]; T[32] = clampr(x_ + y_, lo_, hi_); T[35] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[33], y_ = T[34]; T[33] = clampr(x_ + y_, lo_, hi_); T[34] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[39], y_ = T[36]; T[39] = clampr(x_ + y_, lo_, hi_); T[36] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[38], y_ = T[37]; T[38] = clampr(x_ + y_, lo_, hi_); T[37] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[40], y_ = T[43]; T[40] = clampr(x_ + y_, lo_, hi_); T[43] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[41], y_ = T[42]; T[41] = clampr(x_ + y_, lo_, hi_); T[42] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[47], y_ = T[44]; T[47] = clampr(x_ + y_, lo_, hi_); T[44] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[46], y_ = T[45]; T[46] = clampr(x_ + y_, lo_, hi_); T[45] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[48], y_ = T[51]; T[48] = clampr(x_ + y_, lo_, hi_); T[51] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[49], y_ = T[50]; T[49] = clampr(x_ + y_, lo_, hi_); T[50] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[55], y_ = T[52]; T[55] = clampr(x_ + y_, lo_, hi_); T[52] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[54], y_ = T[53]; T[54] = clampr(x_ + y_, lo_, hi_); T[53] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[56], y_ = T[59]; T[56] = clampr(x_ + y_, lo_, hi_); T[59] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[57], y_ = T[58]; T[57] = clampr(x_ + y_, lo_, hi_); T[58] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[63], y_ = T[60]; T[63] = clampr(x_ + y_, lo_, hi_); T[60] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[62], y_ = T[61]; T[62] = clampr(x_ + y_, lo_, hi_); T[61] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[0] * 2896 - (int64_t)T[1] * 2896), y_ = rnd12w((int64_t)T[0] * 2896 + (int64_t)T[1] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = (int32_t)x_; T[0] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[2] * 1567 - (int64_t)T[3] * 3784), y_ = rnd12w((int64_t)T[2] * 3784 + (int64_t)T[3] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[2] = (int32_t)x_; T[3] = (int32_t)y_; }
-    { const int64_t x_ = T[4], y_ = T[5]; T[4] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[6]; T[7] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[14] * 1567 - (int64_t)T[9] * 3784), y_ = rnd12w((int64_t)T[14] * 3784 + (int64_t)T[9] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = (int32_t)x_; T[14] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[13] * -3784 - (int64_t)T[10] * 1567), y_ = rnd12w((int64_t)T[13] * 1567 + (int64_t)T[10] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = (int32_t)x_; T[13] = (int32_t)y_; }
-    { const int64_t x_ = T[16], y_ = T[19]; T[16] = clampr(x_ + y_, lo_, hi_); T[19] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[17], y_ = T[18]; T[17] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[23], y_ = T[20]; T[23] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[22], y_ = T[21]; T[22] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[24], y_ = T[27]; T[24] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[25], y_ = T[26]; T[25] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[31], y_ = T[28]; T[31] = clampr(x_ + y_, lo_, hi_); T[28] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[30], y_ = T[29]; T[30] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[61] * 799 - (int64_t)T[34] * 4017), y_ = rnd12w((int64_t)T[61] * 4017 + (int64_t)T[34] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[34] = (int32_t)x_; T[61] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[60] * 799 - (int64_t)T[35] * 4017), y_ = rnd12w((int64_t)T[60] * 4017 + (int64_t)T[35] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[35] = (int32_t)x_; T[60] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[59] * -4017 - (int64_t)T[36] * 799), y_ = rnd12w((int64_t)T[59] * 799 + (int64_t)T[36] * -4017); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[36] = (int32_t)x_; T[59] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[58] * -4017 - (int64_t)T[37] * 799), y_ = rnd12w((int64_t)T[58] * 799 + (int64_t)T[37] * -4017); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[37] = (int32_t)x_; T[58] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[53] * 3406 - (int64_t)T[42] * 2276), y_ = rnd12w((int64_t)T[53] * 2276 + (int64_t)T[42] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[42] = (int32_t)x_; T[53] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[52] * 3406 - (int64_t)T[43] * 2276), y_ = rnd12w((int64_t)T[52] * 2276 + (int64_t)T[43] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[43] = (int32_t)x_; T[52] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[51] * -2276 - (int64_t)T[44] * 3406), y_ = rnd12w((int64_t)T[51] * 3406 + (int64_t)T[44] * -2276); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[44] = (int32_t)x_; T[51] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[50] * -2276 - (int64_t)T[45] * 3406), y_ = rnd12w((int64_t)T[50] * 3406 + (int64_t)T[45] * -2276); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[45] = (int32_t)x_; T[50] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[3]; T[0] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[2]; T[1] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[6] * 2896 - (int64_t)T[5] * 2896), y_ = rnd12w((int64_t)T[6] * 2896 + (int64_t)T[5] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = T[8], y_ = T[11]; T[8] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[9], y_ = T[10]; T[9] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[15], y_ = T[12]; T[15] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[14], y_ = T[13]; T[14] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[29] * 1567 - (int64_t)T[18] * 3784), y_ = rnd12w((int64_t)T[29] * 3784 + (int64_t)T[18] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = (int32_t)x_; T[29] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[28] * 1567 - (int64_t)T[19] * 3784), y_ = rnd12w((int64_t)T[28] * 3784 + (int64_t)T[19] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[19] = (int32_t)x_; T[28] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[27] * -3784 - (int64_t)T[20] * 1567), y_ = rnd12w((int64_t)T[27] * 1567 + (int64_t)T[20] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = (int32_t)x_; T[27] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[26] * -3784 - (int64_t)T[21] * 1567), y_ = rnd12w((int64_t)T[26] * 1567 + (int64_t)T[21] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = (int32_t)x_; T[26] = (int32_t)y_; }
-    { const int64_t x_ = T[32], y_ = T[39]; T[32] = clampr(x_ + y_, lo_, hi_); T[39] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[33], y_ = T[38]; T[33] = clampr(x_ + y_, lo_, hi_); T[38] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[34], y_ = T[37]; T[34] = clampr(x_ + y_, lo_, hi_); T[37] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[35], y_ = T[36]; T[35] = clampr(x_ + y_, lo_, hi_); T[36] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[47], y_ = T[40]; T[47] = clampr(x_ + y_, lo_, hi_); T[40] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[46], y_ = T[41]; T[46] = clampr(x_ + y_, lo_, hi_); T[41] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[45], y_ = T[42]; T[45] = clampr(x_ + y_, lo_, hi_); T[42] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[44], y_ = T[43]; T[44] = clampr(x_ + y_, lo_, hi_); T[43] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[48], y_ = T[55]; T[48] = clampr(x_ + y_, lo_, hi_); T[55] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[49], y_ = T[54]; T[49] = clampr(x_ + y_, lo_, hi_); T[54] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[50], y_ = T[53]; T[50] = clampr(x_ + y_, lo_, hi_); T[53] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[51], y_ = T[52]; T[51] = clampr(x_ + y_, lo_, hi_); T[52] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[63], y_ = T[56]; T[63] = clampr(x_ + y_, lo_, hi_); T[56] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[62], y_ = T[57]; T[62] = clampr(x_ + y_, lo_, hi_); T[57] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[61], y_ = T[58]; T[61] = clampr(x_ + y_, lo_, hi_); T[58] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[60], y_ = T[59]; T[60] = clampr(x_ + y_, lo_, hi_); T[59] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[0], y_ = T[7]; T[0] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[6]; T[1] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[5]; T[2] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[4]; T[3] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[13] * 2896 - (int64_t)T[10] * 2896), y_ = rnd12w((int64_t)T[13] * 2896 + (int64_t)T[10] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = (int32_t)x_; T[13] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[12] * 2896 - (int64_t)T[11] * 2896), y_ = rnd12w((int64_t)T[12] * 2896 + (int64_t)T[11] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = (int32_t)x_; T[12] = (int32_t)y_; }
-    { const int64_t x_ = T[16], y_ = T[23]; T[16] = clampr(x_ + y_, lo_, hi_); T[23] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[17], y_ = T[22]; T[17] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[18], y_ = T[21]; T[18] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[19], y_ = T[20]; T[19] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[31], y_ = T[24]; T[31] = clampr(x_ + y_, lo_, hi_); T[24] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[30], y_ = T[25]; T[30] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[29], y_ = T[26]; T[29] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[28], y_ = T[27]; T[28] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[59] * 1567 - (int64_t)T[36] * 3784), y_ = rnd12w((int64_t)T[59] * 3784 + (int64_t)T[36] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[36] = (int32_t)x_; T[59] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[58] * 1567 - (int64_t)T[37] * 3784), y_ = rnd12w((int64_t)T[58] * 3784 + (int64_t)T[37] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[37] = (int32_t)x_; T[58] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[57] * 1567 - (int64_t)T[38] * 3784), y_ = rnd12w((int64_t)T[57] * 3784 + (int64_t)T[38] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[38] = (int32_t)x_; T[57] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[56] * 1567 - (int64_t)T[39] * 3784), y_ = rnd12w((int64_t)T[56] * 3784 + (int64_t)T[39] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[39] = (int32_t)x_; T[56] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[55] * -3784 - (int64_t)T[40] * 1567), y_ = rnd12w((int64_t)T[55] * 1567 + (int64_t)T[40] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[40] = (int32_t)x_; T[55] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[54] * -3784 - (int64_t)T[41] * 1567), y_ = rnd12w((int64_t)T[54] * 1567 + (int64_t)T[41] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[41] = (int32_t)x_; T[54] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[53] * -3784 - (int64_t)T[42] * 1567), y_ = rnd12w((int64_t)T[53] * 1567 + (int64_t)T[42] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[42] = (int32_t)x_; T[53] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[52] * -3784 - (int64_t)T[43] * 1567), y_ = rnd12w((int64_t)T[52] * 1567 + (int64_t)T[43] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[43] = (int32_t)x_; T[52] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[15]; T[0] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[14]; T[1] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[13]; T[2] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[12]; T[3] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[4], y_ = T[11]; T[4] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[5], y_ = T[10]; T[5] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[6], y_ = T[9]; T[6] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[8]; T[7] = clampr(x_ + y_, lo_, hi_); T[8] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[27] * 2896 - (int64_t)T[20] * 2896), y_ = rnd12w((int64_t)T[27] * 2896 + (int64_t)T[20] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = (int32_t)x_; T[27] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[26] * 2896 - (int64_t)T[21] * 2896), y_ = rnd12w((int64_t)T[26] * 2896 + (int64_t)T[21] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = (int32_t)x_; T[26] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[25] * 2896 - (int64_t)T[22] * 2896), y_ = rnd12w((int64_t)T[25] * 2896 + (int64_t)T[22] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = (int32_t)x_; T[25] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[24] * 2896 - (int64_t)T[23] * 2896), y_ = rnd12w((int64_t)T[24] * 2896 + (int64_t)T[23] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[23] = (int32_t)x_; T[24] = (int32_t)y_; }
-    { const int64_t x_ = T[32], y_ = T[47]; T[32] = clampr(x_ + y_, lo_, hi_); T[47] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[63], y_ = T[48]; T[63] = clampr(x_ + y_, lo_, hi_); T[48] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[33], y_ = T[46]; T[33] = clampr(x_ + y_, lo_, hi_); T[46] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[62], y_ = T[49]; T[62] = clampr(x_ + y_, lo_, hi_); T[49] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[34], y_ = T[45]; T[34] = clampr(x_ + y_, lo_, hi_); T[45] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[61], y_ = T[50]; T[61] = clampr(x_ + y_, lo_, hi_); T[50] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[35], y_ = T[44]; T[35] = clampr(x_ + y_, lo_, hi_); T[44] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[60], y_ = T[51]; T[60] = clampr(x_ + y_, lo_, hi_); T[51] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[36], y_ = T[43]; T[36] = clampr(x_ + y_, lo_, hi_); T[43] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[59], y_ = T[52]; T[59] = clampr(x_ + y_, lo_, hi_); T[52] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[37], y_ = T[42]; T[37] = clampr(x_ + y_, lo_, hi_); T[42] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[58], y_ = T[53]; T[58] = clampr(x_ + y_, lo_, hi_); T[53] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[38], y_ = T[41]; T[38] = clampr(x_ + y_, lo_, hi_); T[41] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[57], y_ = T[54]; T[57] = clampr(x_ + y_, lo_, hi_); T[54] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[39], y_ = T[40]; T[39] = clampr(x_ + y_, lo_, hi_); T[40] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[56], y_ = T[55]; T[56] = clampr(x_ + y_, lo_, hi_); T[55] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[0], y_ = T[31]; T[0] = clampr(x_ + y_, lo_, hi_); T[31] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[30]; T[1] = clampr(x_ + y_, lo_, hi_); T[30] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[29]; T[2] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[28]; T[3] = clampr(x_ + y_, lo_, hi_); T[28] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[4], y_ = T[27]; T[4] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[5], y_ = T[26]; T[5] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[6], y_ = T[25]; T[6] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[24]; T[7] = clampr(x_ + y_, lo_, hi_); T[24] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[8], y_ = T[23]; T[8] = clampr(x_ + y_, lo_, hi_); T[23] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[9], y_ = T[22]; T[9] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[10], y_ = T[21]; T[10] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[11], y_ = T[20]; T[11] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[12], y_ = T[19]; T[12] = clampr(x_ + y_, lo_, hi_); T[19] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[13], y_ = T[18]; T[13] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[14], y_ = T[17]; T[14] = clampr(x_ + y_, lo_, hi_); T[17] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[15], y_ = T[16]; T[15] = clampr(x_ + y_, lo_, hi_); T[16] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[55] * 2896 - (int64_t)T[40] * 2896), y_ = rnd12w((int64_t)T[55] * 2896 + (int64_t)T[40] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[40] = (int32_t)x_; T[55] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[54] * 2896 - (int64_t)T[41] * 2896), y_ = rnd12w((int64_t)T[54] * 2896 + (int64_t)T[41] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[41] = (int32_t)x_; T[54] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[53] * 2896 - (int64_t)T[42] * 2896), y_ = rnd12w((int64_t)T[53] * 2896 + (int64_t)T[42] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[42] = (int32_t)x_; T[53] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[52] * 2896 - (int64_t)T[43] * 2896), y_ = rnd12w((int64_t)T[52] * 2896 + (int64_t)T[43] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[43] = (int32_t)x_; T[52] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[51] * 2896 - (int64_t)T[44] * 2896), y_ = rnd12w((int64_t)T[51] * 2896 + (int64_t)T[44] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[44] = (int32_t)x_; T[51] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[50] * 2896 - (int64_t)T[45] * 2896), y_ = rnd12w((int64_t)T[50] * 2896 + (int64_t)T[45] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[45] = (int32_t)x_; T[50] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[49] * 2896 - (int64_t)T[46] * 2896), y_ = rnd12w((int64_t)T[49] * 2896 + (int64_t)T[46] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[46] = (int32_t)x_; T[49] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[48] * 2896 - (int64_t)T[47] * 2896), y_ = rnd12w((int64_t)T[48] * 2896 + (int64_t)T[47] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[47] = (int32_t)x_; T[48] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[63]; T[0] = clampr(x_ + y_, lo_, hi_); T[63] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[62]; T[1] = clampr(x_ + y_, lo_, hi_); T[62] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[61]; T[2] = clampr(x_ + y_, lo_, hi_); T[61] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[60]; T[3] = clampr(x_ + y_, lo_, hi_); T[60] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[4], y_ = T[59]; T[4] = clampr(x_ + y_, lo_, hi_); T[59] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[5], y_ = T[58]; T[5] = clampr(x_ + y_, lo_, hi_); T[58] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[6], y_ = T[57]; T[6] = clampr(x_ + y_, lo_, hi_); T[57] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[56]; T[7] = clampr(x_ + y_, lo_, hi_); T[56] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[8], y_ = T[55]; T[8] = clampr(x_ + y_, lo_, hi_); T[55] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[9], y_ = T[54]; T[9] = clampr(x_ + y_, lo_, hi_); T[54] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[10], y_ = T[53]; T[10] = clampr(x_ + y_, lo_, hi_); T[53] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[11], y_ = T[52]; T[11] = clampr(x_ + y_, lo_, hi_); T[52] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[12], y_ = T[51]; T[12] = clampr(x_ + y_, lo_, hi_); T[51] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[13], y_ = T[50]; T[13] = clampr(x_ + y_, lo_, hi_); T[50] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[14], y_ = T[49]; T[14] = clampr(x_ + y_, lo_, hi_); T[49] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[15], y_ = T[48]; T[15] = clampr(x_ + y_, lo_, hi_); T[48] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[16], y_ = T[47]; T[16] = clampr(x_ + y_, lo_, hi_); T[47] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[17], y_ = T[46]; T[17] = clampr(x_ + y_, lo_, hi_); T[46] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[18], y_ = T[45]; T[18] = clampr(x_ + y_, lo_, hi_); T[45] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[19], y_ = T[44]; T[19] = clampr(x_ + y_, lo_, hi_); T[44] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[20], y_ = T[43]; T[20] = clampr(x_ + y_, lo_, hi_); T[43] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[21], y_ = T[42]; T[21] = clampr(x_ + y_, lo_, hi_); T[42] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[22], y_ = T[41]; T[22] = clampr(x_ + y_, lo_, hi_); T[41] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[23], y_ = T[40]; T[23] = clampr(x_ + y_, lo_, hi_); T[40] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[24], y_ = T[39]; T[24] = clampr(x_ + y_, lo_, hi_); T[39] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[25], y_ = T[38]; T[25] = clampr(x_ + y_, lo_, hi_); T[38] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[26], y_ = T[37]; T[26] = clampr(x_ + y_, lo_, hi_); T[37] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[27], y_ = T[36]; T[27] = clampr(x_ + y_, lo_, hi_); T[36] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[28], y_ = T[35]; T[28] = clampr(x_ + y_, lo_, hi_); T[35] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[29], y_ = T[34]; T[29] = clampr(x_ + y_, lo_, hi_); T[34] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[30], y_ = T[33]; T[30] = clampr(x_ + y_, lo_, hi_); T[33] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[31], y_ = T[32]; T[31] = clampr(x_ + y_, lo_, hi_); T[32] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[32] * 101 - T[63] * 4095), y_ = rnd12(T[32] * 4095 + T[63] * 101); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[32] = x_; T[63] = y_; }
+    { const int32_t x_ = rnd12(T[33] * 2967 - T[62] * 2824), y_ = rnd12(T[33] * 2824 + T[62] * 2967); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[33] = x_; T[62] = y_; }
+    { const int32_t x_ = rnd12(T[34] * 1660 - T[61] * 3745), y_ = rnd12(T[34] * 3745 + T[61] * 1660); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[34] = x_; T[61] = y_; }
+    { const int32_t x_ = rnd12(T[35] * 3822 - T[60] * 1474), y_ = rnd12(T[35] * 1474 + T[60] * 3822); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[35] = x_; T[60] = y_; }
+    { const int32_t x_ = rnd12(T[36] * 897 - T[59] * 3996), y_ = rnd12(T[36] * 3996 + T[59] * 897); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[36] = x_; T[59] = y_; }
+    { const int32_t x_ = rnd12(T[37] * 3461 - T[58] * 2191), y_ = rnd12(T[37] * 2191 + T[58] * 3461); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[37] = x_; T[58] = y_; }
+    { const int32_t x_ = rnd12(T[38] * 2359 - T[57] * 3349), y_ = rnd12(T[38] * 3349 + T[57] * 2359); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[38] = x_; T[57] = y_; }
+    { const int32_t x_ = rnd12(T[39] * 4036 - T[56] * 700), y_ = rnd12(T[39] * 700 + T[56] * 4036); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[39] = x_; T[56] = y_; }
+    { const int32_t x_ = rnd12(T[40] * 501 - T[55] * 4065), y_ = rnd12(T[40] * 4065 + T[55] * 501); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[40] = x_; T[55] = y_; }
+    { const int32_t x_ = rnd12(T[41] * 3229 - T[54] * 2520), y_ = rnd12(T[41] * 2520 + T[54] * 3229); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[41] = x_; T[54] = y_; }
+    { const int32_t x_ = rnd12(T[42] * 2019 - T[53] * 3564), y_ = rnd12(T[42] * 3564 + T[53] * 2019); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[42] = x_; T[53] = y_; }
+    { const int32_t x_ = rnd12(T[43] * 3948 - T[52] * 1092), y_ = rnd12(T[43] * 1092 + T[52] * 3948); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[43] = x_; T[52] = y_; }
+    { const int32_t x_ = rnd12(T[44] * 1285 - T[51] * 3889), y_ = rnd12(T[44] * 3889 + T[51] * 1285); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[44] = x_; T[51] = y_; }
+    { const int32_t x_ = rnd12(T[45] * 3659 - T[50] * 1842), y_ = rnd12(T[45] * 1842 + T[50] * 3659); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[45] = x_; T[50] = y_; }
+    { const int32_t x_ = rnd12(T[46] * 2675 - T[49] * 3102), y_ = rnd12(T[46] * 3102 + T[49] * 2675); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[46] = x_; T[49] = y_; }
+    { const int32_t x_ = rnd12(T[47] * 4085 - T[48] * 301), y_ = rnd12(T[47] * 301 + T[48] * 4085); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[47] = x_; T[48] = y_; }
+    { const int32_t x_ = rnd12(T[16] * 201 - T[31] * 4091), y_ = rnd12(T[16] * 4091 + T[31] * 201); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[16] = x_; T[31] = y_; }
+    { const int32_t x_ = rnd12(T[17] * 3035 - T[30] * 2751), y_ = rnd12(T[17] * 2751 + T[30] * 3035); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[17] = x_; T[30] = y_; }
+    { const int32_t x_ = rnd12(T[18] * 1751 - T[29] * 3703), y_ = rnd12(T[18] * 3703 + T[29] * 1751); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = x_; T[29] = y_; }
+    { const int32_t x_ = rnd12(T[19] * 3857 - T[28] * 1380), y_ = rnd12(T[19] * 1380 + T[28] * 3857); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[19] = x_; T[28] = y_; }
+    { const int32_t x_ = rnd12(T[20] * 995 - T[27] * 3973), y_ = rnd12(T[20] * 3973 + T[27] * 995); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = x_; T[27] = y_; }
+    { const int32_t x_ = rnd12(T[21] * 3513 - T[26] * 2106), y_ = rnd12(T[21] * 2106 + T[26] * 3513); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = x_; T[26] = y_; }
+    { const int32_t x_ = rnd12(T[22] * 2440 - T[25] * 3290), y_ = rnd12(T[22] * 3290 + T[25] * 2440); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = x_; T[25] = y_; }
+    { const int32_t x_ = rnd12(T[23] * 4052 - T[24] * 601), y_ = rnd12(T[23] * 601 + T[24] * 4052); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[23] = x_; T[24] = y_; }
+    { const int32_t x_ = T[32], y_ = T[33]; T[32] = clampr(x_ + y_, lo_, hi_); T[33] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[35], y_ = T[34]; T[35] = clampr(x_ + y_, lo_, hi_); T[34] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[36], y_ = T[37]; T[36] = clampr(x_ + y_, lo_, hi_); T[37] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[39], y_ = T[38]; T[39] = clampr(x_ + y_, lo_, hi_); T[38] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[40], y_ = T[41]; T[40] = clampr(x_ + y_, lo_, hi_); T[41] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[43], y_ = T[42]; T[43] = clampr(x_ + y_, lo_, hi_); T[42] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[44], y_ = T[45]; T[44] = clampr(x_ + y_, lo_, hi_); T[45] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[47], y_ = T[46]; T[47] = clampr(x_ + y_, lo_, hi_); T[46] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[48], y_ = T[49]; T[48] = clampr(x_ + y_, lo_, hi_); T[49] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[51], y_ = T[50]; T[51] = clampr(x_ + y_, lo_, hi_); T[50] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[52], y_ = T[53]; T[52] = clampr(x_ + y_, lo_, hi_); T[53] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[55], y_ = T[54]; T[55] = clampr(x_ + y_, lo_, hi_); T[54] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[56], y_ = T[57]; T[56] = clampr(x_ + y_, lo_, hi_); T[57] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[59], y_ = T[58]; T[59] = clampr(x_ + y_, lo_, hi_); T[58] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[60], y_ = T[61]; T[60] = clampr(x_ + y_, lo_, hi_); T[61] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[63], y_ = T[62]; T[63] = clampr(x_ + y_, lo_, hi_); T[62] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[8] * 401 - T[15] * 4076), y_ = rnd12(T[8] * 4076 + T[15] * 401); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[8] = x_; T[15] = y_; }
+    { const int32_t x_ = rnd12(T[9] * 3166 - T[14] * 2598), y_ = rnd12(T[9] * 2598 + T[14] * 3166); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = x_; T[14] = y_; }
+    { const int32_t x_ = rnd12(T[10] * 1931 - T[13] * 3612), y_ = rnd12(T[10] * 3612 + T[13] * 1931); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = x_; T[13] = y_; }
+    { const int32_t x_ = rnd12(T[11] * 3920 - T[12] * 1189), y_ = rnd12(T[11] * 1189 + T[12] * 3920); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = x_; T[12] = y_; }
+    { const int32_t x_ = T[16], y_ = T[17]; T[16] = clampr(x_ + y_, lo_, hi_); T[17] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[19], y_ = T[18]; T[19] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[20], y_ = T[21]; T[20] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[23], y_ = T[22]; T[23] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[24], y_ = T[25]; T[24] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[27], y_ = T[26]; T[27] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[28], y_ = T[29]; T[28] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[31], y_ = T[30]; T[31] = clampr(x_ + y_, lo_, hi_); T[30] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[62] * 401 - T[33] * 4076), y_ = rnd12(T[62] * 4076 + T[33] * 401); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[33] = x_; T[62] = y_; }
+    { const int32_t x_ = rnd12(T[61] * -4076 - T[34] * 401), y_ = rnd12(T[61] * 401 + T[34] * -4076); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[34] = x_; T[61] = y_; }
+    { const int32_t x_ = rnd12(T[58] * 3166 - T[37] * 2598), y_ = rnd12(T[58] * 2598 + T[37] * 3166); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[37] = x_; T[58] = y_; }
+    { const int32_t x_ = rnd12(T[57] * -2598 - T[38] * 3166), y_ = rnd12(T[57] * 3166 + T[38] * -2598); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[38] = x_; T[57] = y_; }
+    { const int32_t x_ = rnd12(T[54] * 1931 - T[41] * 3612), y_ = rnd12(T[54] * 3612 + T[41] * 1931); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[41] = x_; T[54] = y_; }
+    { const int32_t x_ = rnd12(T[53] * -3612 - T[42] * 1931), y_ = rnd12(T[53] * 1931 + T[42] * -3612); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[42] = x_; T[53] = y_; }
+    { const int32_t x_ = rnd12(T[50] * 3920 - T[45] * 1189), y_ = rnd12(T[50] * 1189 + T[45] * 3920); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[45] = x_; T[50] = y_; }
+    { const int32_t x_ = rnd12(T[49] * -1189 - T[46] * 3920), y_ = rnd12(T[49] * 3920 + T[46] * -1189); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[46] = x_; T[49] = y_; }
+    { const int32_t x_ = rnd12(T[4] * 799 - T[7] * 4017), y_ = rnd12(T[4] * 4017 + T[7] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[4] = x_; T[7] = y_; }
+    { const int32_t x_ = rnd12(T[5] * 3406 - T[6] * 2276), y_ = rnd12(T[5] * 2276 + T[6] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[6] = y_; }
+    { const int32_t x_ = T[8], y_ = T[9]; T[8] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[11], y_ = T[10]; T[11] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[12], y_ = T[13]; T[12] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[15], y_ = T[14]; T[15] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[30] * 799 - T[17] * 4017), y_ = rnd12(T[30] * 4017 + T[17] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[17] = x_; T[30] = y_; }
+    { const int32_t x_ = rnd12(T[29] * -4017 - T[18] * 799), y_ = rnd12(T[29] * 799 + T[18] * -4017); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = x_; T[29] = y_; }
+    { const int32_t x_ = rnd12(T[26] * 3406 - T[21] * 2276), y_ = rnd12(T[26] * 2276 + T[21] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = x_; T[26] = y_; }
+    { const int32_t x_ = rnd12(T[25] * -2276 - T[22] * 3406), y_ = rnd12(T[25] * 3406 + T[22] * -2276); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = x_; T[25] = y_; }
+    { const int32_t x_ = T[32], y_ = T[35]; T[32] = clampr(x_ + y_, lo_, hi_); T[35] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[33], y_ = T[34]; T[33] = clampr(x_ + y_, lo_, hi_); T[34] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[39], y_ = T[36]; T[39] = clampr(x_ + y_, lo_, hi_); T[36] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[38], y_ = T[37]; T[38] = clampr(x_ + y_, lo_, hi_); T[37] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[40], y_ = T[43]; T[40] = clampr(x_ + y_, lo_, hi_); T[43] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[41], y_ = T[42]; T[41] = clampr(x_ + y_, lo_, hi_); T[42] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[47], y_ = T[44]; T[47] = clampr(x_ + y_, lo_, hi_); T[44] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[46], y_ = T[45]; T[46] = clampr(x_ + y_, lo_, hi_); T[45] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[48], y_ = T[51]; T[48] = clampr(x_ + y_, lo_, hi_); T[51] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[49], y_ = T[50]; T[49] = clampr(x_ + y_, lo_, hi_); T[50] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[55], y_ = T[52]; T[55] = clampr(x_ + y_, lo_, hi_); T[52] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[54], y_ = T[53]; T[54] = clampr(x_ + y_, lo_, hi_); T[53] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[56], y_ = T[59]; T[56] = clampr(x_ + y_, lo_, hi_); T[59] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[57], y_ = T[58]; T[57] = clampr(x_ + y_, lo_, hi_); T[58] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[63], y_ = T[60]; T[63] = clampr(x_ + y_, lo_, hi_); T[60] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[62], y_ = T[61]; T[62] = clampr(x_ + y_, lo_, hi_); T[61] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[0] * 2896 - T[1] * 2896), y_ = rnd12(T[0] * 2896 + T[1] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = x_; T[0] = y_; }
+    { const int32_t x_ = rnd12(T[2] * 1567 - T[3] * 3784), y_ = rnd12(T[2] * 3784 + T[3] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[2] = x_; T[3] = y_; }
+    { const int32_t x_ = T[4], y_ = T[5]; T[4] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[6]; T[7] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[14] * 1567 - T[9] * 3784), y_ = rnd12(T[14] * 3784 + T[9] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = x_; T[14] = y_; }
+    { const int32_t x_ = rnd12(T[13] * -3784 - T[10] * 1567), y_ = rnd12(T[13] * 1567 + T[10] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = x_; T[13] = y_; }
+    { const int32_t x_ = T[16], y_ = T[19]; T[16] = clampr(x_ + y_, lo_, hi_); T[19] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[17], y_ = T[18]; T[17] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[23], y_ = T[20]; T[23] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[22], y_ = T[21]; T[22] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[24], y_ = T[27]; T[24] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[25], y_ = T[26]; T[25] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[31], y_ = T[28]; T[31] = clampr(x_ + y_, lo_, hi_); T[28] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[30], y_ = T[29]; T[30] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[61] * 799 - T[34] * 4017), y_ = rnd12(T[61] * 4017 + T[34] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[34] = x_; T[61] = y_; }
+    { const int32_t x_ = rnd12(T[60] * 799 - T[35] * 4017), y_ = rnd12(T[60] * 4017 + T[35] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[35] = x_; T[60] = y_; }
+    { const int32_t x_ = rnd12(T[59] * -4017 - T[36] * 799), y_ = rnd12(T[59] * 799 + T[36] * -4017); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[36] = x_; T[59] = y_; }
+    { const int32_t x_ = rnd12(T[58] * -4017 - T[37] * 799), y_ = rnd12(T[58] * 799 + T[37] * -4017); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[37] = x_; T[58] = y_; }
+    { const int32_t x_ = rnd12(T[53] * 3406 - T[42] * 2276), y_ = rnd12(T[53] * 2276 + T[42] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[42] = x_; T[53] = y_; }
+    { const int32_t x_ = rnd12(T[52] * 3406 - T[43] * 2276), y_ = rnd12(T[52] * 2276 + T[43] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[43] = x_; T[52] = y_; }
+    { const int32_t x_ = rnd12(T[51] * -2276 - T[44] * 3406), y_ = rnd12(T[51] * 3406 + T[44] * -2276); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[44] = x_; T[51] = y_; }
+    { const int32_t x_ = rnd12(T[50] * -2276 - T[45] * 3406), y_ = rnd12(T[50] * 3406 + T[45] * -2276); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[45] = x_; T[50] = y_; }
+    { const int32_t x_ = T[0], y_ = T[3]; T[0] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[2]; T[1] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[6] * 2896 - T[5] * 2896), y_ = rnd12(T[6] * 2896 + T[5] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[6] = y_; }
+    { const int32_t x_ = T[8], y_ = T[11]; T[8] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[9], y_ = T[10]; T[9] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[15], y_ = T[12]; T[15] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[14], y_ = T[13]; T[14] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[29] * 1567 - T[18] * 3784), y_ = rnd12(T[29] * 3784 + T[18] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[18] = x_; T[29] = y_; }
+    { const int32_t x_ = rnd12(T[28] * 1567 - T[19] * 3784), y_ = rnd12(T[28] * 3784 + T[19] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[19] = x_; T[28] = y_; }
+    { const int32_t x_ = rnd12(T[27] * -3784 - T[20] * 1567), y_ = rnd12(T[27] * 1567 + T[20] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = x_; T[27] = y_; }
+    { const int32_t x_ = rnd12(T[26] * -3784 - T[21] * 1567), y_ = rnd12(T[26] * 1567 + T[21] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = x_; T[26] = y_; }
+    { const int32_t x_ = T[32], y_ = T[39]; T[32] = clampr(x_ + y_, lo_, hi_); T[39] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[33], y_ = T[38]; T[33] = clampr(x_ + y_, lo_, hi_); T[38] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[34], y_ = T[37]; T[34] = clampr(x_ + y_, lo_, hi_); T[37] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[35], y_ = T[36]; T[35] = clampr(x_ + y_, lo_, hi_); T[36] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[47], y_ = T[40]; T[47] = clampr(x_ + y_, lo_, hi_); T[40] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[46], y_ = T[41]; T[46] = clampr(x_ + y_, lo_, hi_); T[41] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[45], y_ = T[42]; T[45] = clampr(x_ + y_, lo_, hi_); T[42] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[44], y_ = T[43]; T[44] = clampr(x_ + y_, lo_, hi_); T[43] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[48], y_ = T[55]; T[48] = clampr(x_ + y_, lo_, hi_); T[55] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[49], y_ = T[54]; T[49] = clampr(x_ + y_, lo_, hi_); T[54] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[50], y_ = T[53]; T[50] = clampr(x_ + y_, lo_, hi_); T[53] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[51], y_ = T[52]; T[51] = clampr(x_ + y_, lo_, hi_); T[52] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[63], y_ = T[56]; T[63] = clampr(x_ + y_, lo_, hi_); T[56] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[62], y_ = T[57]; T[62] = clampr(x_ + y_, lo_, hi_); T[57] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[61], y_ = T[58]; T[61] = clampr(x_ + y_, lo_, hi_); T[58] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[60], y_ = T[59]; T[60] = clampr(x_ + y_, lo_, hi_); T[59] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[0], y_ = T[7]; T[0] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[6]; T[1] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[5]; T[2] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[4]; T[3] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[13] * 2896 - T[10] * 2896), y_ = rnd12(T[13] * 2896 + T[10] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[10] = x_; T[13] = y_; }
+    { const int32_t x_ = rnd12(T[12] * 2896 - T[11] * 2896), y_ = rnd12(T[12] * 2896 + T[11] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = x_; T[12] = y_; }
+    { const int32_t x_ = T[16], y_ = T[23]; T[16] = clampr(x_ + y_, lo_, hi_); T[23] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[17], y_ = T[22]; T[17] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[18], y_ = T[21]; T[18] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[19], y_ = T[20]; T[19] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[31], y_ = T[24]; T[31] = clampr(x_ + y_, lo_, hi_); T[24] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[30], y_ = T[25]; T[30] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[29], y_ = T[26]; T[29] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[28], y_ = T[27]; T[28] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[59] * 1567 - T[36] * 3784), y_ = rnd12(T[59] * 3784 + T[36] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[36] = x_; T[59] = y_; }
+    { const int32_t x_ = rnd12(T[58] * 1567 - T[37] * 3784), y_ = rnd12(T[58] * 3784 + T[37] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[37] = x_; T[58] = y_; }
+    { const int32_t x_ = rnd12(T[57] * 1567 - T[38] * 3784), y_ = rnd12(T[57] * 3784 + T[38] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[38] = x_; T[57] = y_; }
+    { const int32_t x_ = rnd12(T[56] * 1567 - T[39] * 3784), y_ = rnd12(T[56] * 3784 + T[39] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[39] = x_; T[56] = y_; }
+    { const int32_t x_ = rnd12(T[55] * -3784 - T[40] * 1567), y_ = rnd12(T[55] * 1567 + T[40] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[40] = x_; T[55] = y_; }
+    { const int32_t x_ = rnd12(T[54] * -3784 - T[41] * 1567), y_ = rnd12(T[54] * 1567 + T[41] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[41] = x_; T[54] = y_; }
+    { const int32_t x_ = rnd12(T[53] * -3784 - T[42] * 1567), y_ = rnd12(T[53] * 1567 + T[42] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[42] = x_; T[53] = y_; }
+    { const int32_t x_ = rnd12(T[52] * -3784 - T[43] * 1567), y_ = rnd12(T[52] * 1567 + T[43] * -3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[43] = x_; T[52] = y_; }
+    { const int32_t x_ = T[0], y_ = T[15]; T[0] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[14]; T[1] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[13]; T[2] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[12]; T[3] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[4], y_ = T[11]; T[4] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[5], y_ = T[10]; T[5] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[6], y_ = T[9]; T[6] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[8]; T[7] = clampr(x_ + y_, lo_, hi_); T[8] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[27] * 2896 - T[20] * 2896), y_ = rnd12(T[27] * 2896 + T[20] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[20] = x_; T[27] = y_; }
+    { const int32_t x_ = rnd12(T[26] * 2896 - T[21] * 2896), y_ = rnd12(T[26] * 2896 + T[21] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[21] = x_; T[26] = y_; }
+    { const int32_t x_ = rnd12(T[25] * 2896 - T[22] * 2896), y_ = rnd12(T[25] * 2896 + T[22] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[22] = x_; T[25] = y_; }
+    { const int32_t x_ = rnd12(T[24] * 2896 - T[23] * 2896), y_ = rnd12(T[24] * 2896 + T[23] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[23] = x_; T[24] = y_; }
+    { const int32_t x_ = T[32], y_ = T[47]; T[32] = clampr(x_ + y_, lo_, hi_); T[47] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[63], y_ = T[48]; T[63] = clampr(x_ + y_, lo_, hi_); T[48] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[33], y_ = T[46]; T[33] = clampr(x_ + y_, lo_, hi_); T[46] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[62], y_ = T[49]; T[62] = clampr(x_ + y_, lo_, hi_); T[49] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[34], y_ = T[45]; T[34] = clampr(x_ + y_, lo_, hi_); T[45] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[61], y_ = T[50]; T[61] = clampr(x_ + y_, lo_, hi_); T[50] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[35], y_ = T[44]; T[35] = clampr(x_ + y_, lo_, hi_); T[44] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[60], y_ = T[51]; T[60] = clampr(x_ + y_, lo_, hi_); T[51] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[36], y_ = T[43]; T[36] = clampr(x_ + y_, lo_, hi_); T[43] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[59], y_ = T[52]; T[59] = clampr(x_ + y_, lo_, hi_); T[52] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[37], y_ = T[42]; T[37] = clampr(x_ + y_, lo_, hi_); T[42] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[58], y_ = T[53]; T[58] = clampr(x_ + y_, lo_, hi_); T[53] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[38], y_ = T[41]; T[38] = clampr(x_ + y_, lo_, hi_); T[41] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[57], y_ = T[54]; T[57] = clampr(x_ + y_, lo_, hi_); T[54] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[39], y_ = T[40]; T[39] = clampr(x_ + y_, lo_, hi_); T[40] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[56], y_ = T[55]; T[56] = clampr(x_ + y_, lo_, hi_); T[55] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[0], y_ = T[31]; T[0] = clampr(x_ + y_, lo_, hi_); T[31] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[30]; T[1] = clampr(x_ + y_, lo_, hi_); T[30] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[29]; T[2] = clampr(x_ + y_, lo_, hi_); T[29] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[28]; T[3] = clampr(x_ + y_, lo_, hi_); T[28] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[4], y_ = T[27]; T[4] = clampr(x_ + y_, lo_, hi_); T[27] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[5], y_ = T[26]; T[5] = clampr(x_ + y_, lo_, hi_); T[26] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[6], y_ = T[25]; T[6] = clampr(x_ + y_, lo_, hi_); T[25] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[24]; T[7] = clampr(x_ + y_, lo_, hi_); T[24] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[8], y_ = T[23]; T[8] = clampr(x_ + y_, lo_, hi_); T[23] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[9], y_ = T[22]; T[9] = clampr(x_ + y_, lo_, hi_); T[22] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[10], y_ = T[21]; T[10] = clampr(x_ + y_, lo_, hi_); T[21] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[11], y_ = T[20]; T[11] = clampr(x_ + y_, lo_, hi_); T[20] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[12], y_ = T[19]; T[12] = clampr(x_ + y_, lo_, hi_); T[19] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[13], y_ = T[18]; T[13] = clampr(x_ + y_, lo_, hi_); T[18] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[14], y_ = T[17]; T[14] = clampr(x_ + y_, lo_, hi_); T[17] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[15], y_ = T[16]; T[15] = clampr(x_ + y_, lo_, hi_); T[16] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[55] * 2896 - T[40] * 2896), y_ = rnd12(T[55] * 2896 + T[40] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[40] = x_; T[55] = y_; }
+    { const int32_t x_ = rnd12(T[54] * 2896 - T[41] * 2896), y_ = rnd12(T[54] * 2896 + T[41] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[41] = x_; T[54] = y_; }
+    { const int32_t x_ = rnd12(T[53] * 2896 - T[42] * 2896), y_ = rnd12(T[53] * 2896 + T[42] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[42] = x_; T[53] = y_; }
+    { const int32_t x_ = rnd12(T[52] * 2896 - T[43] * 2896), y_ = rnd12(T[52] * 2896 + T[43] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[43] = x_; T[52] = y_; }
+    { const int32_t x_ = rnd12(T[51] * 2896 - T[44] * 2896), y_ = rnd12(T[51] * 2896 + T[44] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[44] = x_; T[51] = y_; }
+    { const int32_t x_ = rnd12(T[50] * 2896 - T[45] * 2896), y_ = rnd12(T[50] * 2896 + T[45] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[45] = x_; T[50] = y_; }
+    { const int32_t x_ = rnd12(T[49] * 2896 - T[46] * 2896), y_ = rnd12(T[49] * 2896 + T[46] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[46] = x_; T[49] = y_; }
+    { const int32_t x_ = rnd12(T[48] * 2896 - T[47] * 2896), y_ = rnd12(T[48] * 2896 + T[47] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[47] = x_; T[48] = y_; }
+    { const int32_t x_ = T[0], y_ = T[63]; T[0] = clampr(x_ + y_, lo_, hi_); T[63] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[62]; T[1] = clampr(x_ + y_, lo_, hi_); T[62] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[61]; T[2] = clampr(x_ + y_, lo_, hi_); T[61] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[60]; T[3] = clampr(x_ + y_, lo_, hi_); T[60] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[4], y_ = T[59]; T[4] = clampr(x_ + y_, lo_, hi_); T[59] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[5], y_ = T[58]; T[5] = clampr(x_ + y_, lo_, hi_); T[58] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[6], y_ = T[57]; T[6] = clampr(x_ + y_, lo_, hi_); T[57] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[56]; T[7] = clampr(x_ + y_, lo_, hi_); T[56] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[8], y_ = T[55]; T[8] = clampr(x_ + y_, lo_, hi_); T[55] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[9], y_ = T[54]; T[9] = clampr(x_ + y_, lo_, hi_); T[54] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[10], y_ = T[53]; T[10] = clampr(x_ + y_, lo_, hi_); T[53] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[11], y_ = T[52]; T[11] = clampr(x_ + y_, lo_, hi_); T[52] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[12], y_ = T[51]; T[12] = clampr(x_ + y_, lo_, hi_); T[51] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[13], y_ = T[50]; T[13] = clampr(x_ + y_, lo_, hi_); T[50] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[14], y_ = T[49]; T[14] = clampr(x_ + y_, lo_, hi_); T[49] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[15], y_ = T[48]; T[15] = clampr(x_ + y_, lo_, hi_); T[48] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[16], y_ = T[47]; T[16] = clampr(x_ + y_, lo_, hi_); T[47] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[17], y_ = T[46]; T[17] = clampr(x_ + y_, lo_, hi_); T[46] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[18], y_ = T[45]; T[18] = clampr(x_ + y_, lo_, hi_); T[45] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[19], y_ = T[44]; T[19] = clampr(x_ + y_, lo_, hi_); T[44] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[20], y_ = T[43]; T[20] = clampr(x_ + y_, lo_, hi_); T[43] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[21], y_ = T[42]; T[21] = clampr(x_ + y_, lo_, hi_); T[42] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[22], y_ = T[41]; T[22] = clampr(x_ + y_, lo_, hi_); T[41] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[23], y_ = T[40]; T[23] = clampr(x_ + y_, lo_, hi_); T[40] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[24], y_ = T[39]; T[24] = clampr(x_ + y_, lo_, hi_); T[39] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[25], y_ = T[38]; T[25] = clampr(x_ + y_, lo_, hi_); T[38] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[26], y_ = T[37]; T[26] = clampr(x_ + y_, lo_, hi_); T[37] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[27], y_ = T[36]; T[27] = clampr(x_ + y_, lo_, hi_); T[36] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[28], y_ = T[35]; T[28] = clampr(x_ + y_, lo_, hi_); T[35] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[29], y_ = T[34]; T[29] = clampr(x_ + y_, lo_, hi_); T[34] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[30], y_ = T[33]; T[30] = clampr(x_ + y_, lo_, hi_); T[33] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[31], y_ = T[32]; T[31] = clampr(x_ + y_, lo_, hi_); T[32] = clampr(x_ - y_, lo_, hi_); }
     return e_;
 }
 __host__ __device__ __forceinline__ void fwd_adst8(int32_t *T) {
@@ -1176,22 +1175,22 @@ __host__ __device__ __forceinline__ uint32_t inv_adst8(int32_t *T, int r) {
         T[6] = c_[1];
         T[7] = c_[6];
     }
-    { const int64_t x_ = rnd12w((int64_t)T[0] * 401 - (int64_t)T[1] * 4076), y_ = rnd12w((int64_t)T[0] * 4076 + (int64_t)T[1] * 401); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = (int32_t)x_; T[0] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[2] * 1931 - (int64_t)T[3] * 3612), y_ = rnd12w((int64_t)T[2] * 3612 + (int64_t)T[3] * 1931); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[3] = (int32_t)x_; T[2] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[4] * 3166 - (int64_t)T[5] * 2598), y_ = rnd12w((int64_t)T[4] * 2598 + (int64_t)T[5] * 3166); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[4] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[6] * 3920 - (int64_t)T[7] * 1189), y_ = rnd12w((int64_t)T[6] * 1189 + (int64_t)T[7] * 3920); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[7] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[4]; T[0] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[5]; T[1] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[6]; T[2] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[7]; T[3] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[4] * 1567 - (int64_t)T[5] * 3784), y_ = rnd12w((int64_t)T[4] * 3784 + (int64_t)T[5] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[4] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[7] * 3784 - (int64_t)T[6] * 1567), y_ = rnd12w((int64_t)T[7] * 1567 + (int64_t)T[6] * 3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[6] = (int32_t)x_; T[7] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[2]; T[0] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[4], y_ = T[6]; T[4] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[3]; T[1] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[5], y_ = T[7]; T[5] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[2] * 2896 - (int64_t)T[3] * 2896), y_ = rnd12w((int64_t)T[2] * 2896 + (int64_t)T[3] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[3] = (int32_t)x_; T[2] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[6] * 2896 - (int64_t)T[7] * 2896), y_ = rnd12w((int64_t)T[6] * 2896 + (int64_t)T[7] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[7] = (int32_t)x_; T[6] = (int32_t)y_; }
+    { const int32_t x_ = rnd12(T[0] * 401 - T[1] * 4076), y_ = rnd12(T[0] * 4076 + T[1] * 401); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = x_; T[0] = y_; }
+    { const int32_t x_ = rnd12(T[2] * 1931 - T[3] * 3612), y_ = rnd12(T[2] * 3612 + T[3] * 1931); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[3] = x_; T[2] = y_; }
+    { const int32_t x_ = rnd12(T[4] * 3166 - T[5] * 2598), y_ = rnd12(T[4] * 2598 + T[5] * 3166); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[4] = y_; }
+    { const int32_t x_ = rnd12(T[6] * 3920 - T[7] * 1189), y_ = rnd12(T[6] * 1189 + T[7] * 3920); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[7] = x_; T[6] = y_; }
+    { const int32_t x_ = T[0], y_ = T[4]; T[0] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[5]; T[1] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[6]; T[2] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[7]; T[3] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[4] * 1567 - T[5] * 3784), y_ = rnd12(T[4] * 3784 + T[5] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[4] = y_; }
+    { const int32_t x_ = rnd12(T[7] * 3784 - T[6] * 1567), y_ = rnd12(T[7] * 1567 + T[6] * 3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[6] = x_; T[7] = y_; }
+    { const int32_t x_ = T[0], y_ = T[2]; T[0] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[4], y_ = T[6]; T[4] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[3]; T[1] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[5], y_ = T[7]; T[5] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[2] * 2896 - T[3] * 2896), y_ = rnd12(T[2] * 2896 + T[3] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[3] = x_; T[2] = y_; }
+    { const int32_t x_ = rnd12(T[6] * 2896 - T[7] * 2896), y_ = rnd12(T[6] * 2896 + T[7] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[7] = x_; T[6] = y_; }
     {
         int32_t c_[8];
         c_[0] = T[0]; c_[1] = T[1]; c_[2] = T[2]; c_[3] = T[3]; c_[4] = T[4]; c_[5] = T[5]; c_[6] = T[6]; c_[7] = T[7];
@@ -1315,50 +1314,50 @@ __host__ __device__ __forceinline__ uint32_t inv_adst16(int32_t *T, int r) {
         T[14] = c_[1];
         T[15] = c_[14];
     }
-    { const int64_t x_ = rnd12w((int64_t)T[0] * 201 - (int64_t)T[1] * 4091), y_ = rnd12w((int64_t)T[0] * 4091 + (int64_t)T[1] * 201); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = (int32_t)x_; T[0] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[2] * 995 - (int64_t)T[3] * 3973), y_ = rnd12w((int64_t)T[2] * 3973 + (int64_t)T[3] * 995); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[3] = (int32_t)x_; T[2] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[4] * 1751 - (int64_t)T[5] * 3703), y_ = rnd12w((int64_t)T[4] * 3703 + (int64_t)T[5] * 1751); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[4] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[6] * 2440 - (int64_t)T[7] * 3290), y_ = rnd12w((int64_t)T[6] * 3290 + (int64_t)T[7] * 2440); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[7] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[8] * 3035 - (int64_t)T[9] * 2751), y_ = rnd12w((int64_t)T[8] * 2751 + (int64_t)T[9] * 3035); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = (int32_t)x_; T[8] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[10] * 3513 - (int64_t)T[11] * 2106), y_ = rnd12w((int64_t)T[10] * 2106 + (int64_t)T[11] * 3513); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = (int32_t)x_; T[10] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[12] * 3857 - (int64_t)T[13] * 1380), y_ = rnd12w((int64_t)T[12] * 1380 + (int64_t)T[13] * 3857); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[13] = (int32_t)x_; T[12] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[14] * 4052 - (int64_t)T[15] * 601), y_ = rnd12w((int64_t)T[14] * 601 + (int64_t)T[15] * 4052); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[15] = (int32_t)x_; T[14] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[8]; T[0] = clampr(x_ + y_, lo_, hi_); T[8] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[9]; T[1] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[10]; T[2] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[11]; T[3] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[4], y_ = T[12]; T[4] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[5], y_ = T[13]; T[5] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[6], y_ = T[14]; T[6] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[7], y_ = T[15]; T[7] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[8] * 799 - (int64_t)T[9] * 4017), y_ = rnd12w((int64_t)T[8] * 4017 + (int64_t)T[9] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = (int32_t)x_; T[8] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[13] * 4017 - (int64_t)T[12] * 799), y_ = rnd12w((int64_t)T[13] * 799 + (int64_t)T[12] * 4017); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[12] = (int32_t)x_; T[13] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[10] * 3406 - (int64_t)T[11] * 2276), y_ = rnd12w((int64_t)T[10] * 2276 + (int64_t)T[11] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = (int32_t)x_; T[10] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[15] * 2276 - (int64_t)T[14] * 3406), y_ = rnd12w((int64_t)T[15] * 3406 + (int64_t)T[14] * 2276); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[14] = (int32_t)x_; T[15] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[4]; T[0] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[8], y_ = T[12]; T[8] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[5]; T[1] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[9], y_ = T[13]; T[9] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[2], y_ = T[6]; T[2] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[10], y_ = T[14]; T[10] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[3], y_ = T[7]; T[3] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[11], y_ = T[15]; T[11] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[4] * 1567 - (int64_t)T[5] * 3784), y_ = rnd12w((int64_t)T[4] * 3784 + (int64_t)T[5] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = (int32_t)x_; T[4] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[12] * 1567 - (int64_t)T[13] * 3784), y_ = rnd12w((int64_t)T[12] * 3784 + (int64_t)T[13] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[13] = (int32_t)x_; T[12] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[7] * 3784 - (int64_t)T[6] * 1567), y_ = rnd12w((int64_t)T[7] * 1567 + (int64_t)T[6] * 3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[6] = (int32_t)x_; T[7] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[15] * 3784 - (int64_t)T[14] * 1567), y_ = rnd12w((int64_t)T[15] * 1567 + (int64_t)T[14] * 3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[14] = (int32_t)x_; T[15] = (int32_t)y_; }
-    { const int64_t x_ = T[0], y_ = T[2]; T[0] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[4], y_ = T[6]; T[4] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[8], y_ = T[10]; T[8] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[12], y_ = T[14]; T[12] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[1], y_ = T[3]; T[1] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[5], y_ = T[7]; T[5] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[9], y_ = T[11]; T[9] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = T[13], y_ = T[15]; T[13] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
-    { const int64_t x_ = rnd12w((int64_t)T[2] * 2896 - (int64_t)T[3] * 2896), y_ = rnd12w((int64_t)T[2] * 2896 + (int64_t)T[3] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[3] = (int32_t)x_; T[2] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[6] * 2896 - (int64_t)T[7] * 2896), y_ = rnd12w((int64_t)T[6] * 2896 + (int64_t)T[7] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[7] = (int32_t)x_; T[6] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[10] * 2896 - (int64_t)T[11] * 2896), y_ = rnd12w((int64_t)T[10] * 2896 + (int64_t)T[11] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = (int32_t)x_; T[10] = (int32_t)y_; }
-    { const int64_t x_ = rnd12w((int64_t)T[14] * 2896 - (int64_t)T[15] * 2896), y_ = rnd12w((int64_t)T[14] * 2896 + (int64_t)T[15] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[15] = (int32_t)x_; T[14] = (int32_t)y_; }
+    { const int32_t x_ = rnd12(T[0] * 201 - T[1] * 4091), y_ = rnd12(T[0] * 4091 + T[1] * 201); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[1] = x_; T[0] = y_; }
+    { const int32_t x_ = rnd12(T[2] * 995 - T[3] * 3973), y_ = rnd12(T[2] * 3973 + T[3] * 995); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[3] = x_; T[2] = y_; }
+    { const int32_t x_ = rnd12(T[4] * 1751 - T[5] * 3703), y_ = rnd12(T[4] * 3703 + T[5] * 1751); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[4] = y_; }
+    { const int32_t x_ = rnd12(T[6] * 2440 - T[7] * 3290), y_ = rnd12(T[6] * 3290 + T[7] * 2440); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[7] = x_; T[6] = y_; }
+    { const int32_t x_ = rnd12(T[8] * 3035 - T[9] * 2751), y_ = rnd12(T[8] * 2751 + T[9] * 3035); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = x_; T[8] = y_; }
+    { const int32_t x_ = rnd12(T[10] * 3513 - T[11] * 2106), y_ = rnd12(T[10] * 2106 + T[11] * 3513); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = x_; T[10] = y_; }
+    { const int32_t x_ = rnd12(T[12] * 3857 - T[13] * 1380), y_ = rnd12(T[12] * 1380 + T[13] * 3857); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[13] = x_; T[12] = y_; }
+    { const int32_t x_ = rnd12(T[14] * 4052 - T[15] * 601), y_ = rnd12(T[14] * 601 + T[15] * 4052); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[15] = x_; T[14] = y_; }
+    { const int32_t x_ = T[0], y_ = T[8]; T[0] = clampr(x_ + y_, lo_, hi_); T[8] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[9]; T[1] = clampr(x_ + y_, lo_, hi_); T[9] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[10]; T[2] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[11]; T[3] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[4], y_ = T[12]; T[4] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[5], y_ = T[13]; T[5] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[6], y_ = T[14]; T[6] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[7], y_ = T[15]; T[7] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[8] * 799 - T[9] * 4017), y_ = rnd12(T[8] * 4017 + T[9] * 799); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[9] = x_; T[8] = y_; }
+    { const int32_t x_ = rnd12(T[13] * 4017 - T[12] * 799), y_ = rnd12(T[13] * 799 + T[12] * 4017); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[12] = x_; T[13] = y_; }
+    { const int32_t x_ = rnd12(T[10] * 3406 - T[11] * 2276), y_ = rnd12(T[10] * 2276 + T[11] * 3406); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = x_; T[10] = y_; }
+    { const int32_t x_ = rnd12(T[15] * 2276 - T[14] * 3406), y_ = rnd12(T[15] * 3406 + T[14] * 2276); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[14] = x_; T[15] = y_; }
+    { const int32_t x_ = T[0], y_ = T[4]; T[0] = clampr(x_ + y_, lo_, hi_); T[4] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[8], y_ = T[12]; T[8] = clampr(x_ + y_, lo_, hi_); T[12] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[5]; T[1] = clampr(x_ + y_, lo_, hi_); T[5] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[9], y_ = T[13]; T[9] = clampr(x_ + y_, lo_, hi_); T[13] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[2], y_ = T[6]; T[2] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[10], y_ = T[14]; T[10] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[3], y_ = T[7]; T[3] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[11], y_ = T[15]; T[11] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[4] * 1567 - T[5] * 3784), y_ = rnd12(T[4] * 3784 + T[5] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[5] = x_; T[4] = y_; }
+    { const int32_t x_ = rnd12(T[12] * 1567 - T[13] * 3784), y_ = rnd12(T[12] * 3784 + T[13] * 1567); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[13] = x_; T[12] = y_; }
+    { const int32_t x_ = rnd12(T[7] * 3784 - T[6] * 1567), y_ = rnd12(T[7] * 1567 + T[6] * 3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[6] = x_; T[7] = y_; }
+    { const int32_t x_ = rnd12(T[15] * 3784 - T[14] * 1567), y_ = rnd12(T[15] * 1567 + T[14] * 3784); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[14] = x_; T[15] = y_; }
+    { const int32_t x_ = T[0], y_ = T[2]; T[0] = clampr(x_ + y_, lo_, hi_); T[2] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[4], y_ = T[6]; T[4] = clampr(x_ + y_, lo_, hi_); T[6] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[8], y_ = T[10]; T[8] = clampr(x_ + y_, lo_, hi_); T[10] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[12], y_ = T[14]; T[12] = clampr(x_ + y_, lo_, hi_); T[14] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[1], y_ = T[3]; T[1] = clampr(x_ + y_, lo_, hi_); T[3] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[5], y_ = T[7]; T[5] = clampr(x_ + y_, lo_, hi_); T[7] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[9], y_ = T[11]; T[9] = clampr(x_ + y_, lo_, hi_); T[11] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = T[13], y_ = T[15]; T[13] = clampr(x_ + y_, lo_, hi_); T[15] = clampr(x_ - y_, lo_, hi_); }
+    { const int32_t x_ = rnd12(T[2] * 2896 - T[3] * 2896), y_ = rnd12(T[2] * 2896 + T[3] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[3] = x_; T[2] = y_; }
+    { const int32_t x_ = rnd12(T[6] * 2896 - T[7] * 2896), y_ = rnd12(T[6] * 2896 + T[7] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[7] = x_; T[6] = y_; }
+    { const int32_t x_ = rnd12(T[10] * 2896 - T[11] * 2896), y_ = rnd12(T[10] * 2896 + T[11] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[11] = x_; T[10] = y_; }
+    { const int32_t x_ = rnd12(T[14] * 2896 - T[15] * 2896), y_ = rnd12(T[14] * 2896 + T[15] * 2896); e_ |= (x_ < lo_ || x_ > hi_ || y_ < lo_ || y_ > hi_); T[15] = x_; T[14] = y_; }
     {
         int32_t c_[16];
         c_[0] = T[0]; c_[1] = T[1]; c_[2] = T[2]; c_[3] = T[3]; c_[4] = T[4]; c_[5] = T[5]; c_[6] = T[6]; c_[7] = T[7]; c_[8] = T[8]; c_[9] = T[9]; c_[10] = T[10]; c_[11] = T[11]; c_[12] = T[12]; c_[13] = T[13]; c_[14] = T[14]; c_[15] = T[15];

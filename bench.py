@@ -33,8 +33,8 @@ sys.path.insert(0, ROOT)
 
 W_IMG, H_IMG, SEED = 4000, 3000, 12
 # kernels of one search: k_pad x 3 planes, k_analysis_big, k_analysis, k_dp, k_leaf_prep, k_leaf_queue_scan,
-# k_leaf_queue_fill, k_recon, k_pack_scan, k_pack
-LAUNCHES_PER_STEP = 12
+# k_leaf_deps x 3 passes, k_recon, k_pack_scan, k_pack
+LAUNCHES_PER_STEP = 14
 
 
 def parse():
@@ -212,7 +212,7 @@ def main():
         line = {"metric": "intra_search_mp_per_s", "value": round(value, 3), "unit": "MP/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 3), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-                "config": {"workload": "plain intra RD search, 4000x3000 8-bit 4:2:0 synthetic (seeded), qindex %d" % args.qindex,
+                "config": {"workload": "plain intra RD search, %dx%d 8-bit 4:2:0 synthetic (seeded), qindex %d" % (W_IMG, H_IMG, args.qindex),
                            "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas" if world > 1 else "1 gpu"},
                 "e2e": {"value": round(e2e_value, 3), "unit": "MP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": LAUNCHES_PER_STEP * args.steps,
