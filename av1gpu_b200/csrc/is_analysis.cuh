@@ -15,10 +15,11 @@
 
 namespace is {
 
-// Two kernels share the block search: k_analysis for the 836 blocks of the shapes up to 32 samples a side (8 warps,
-// 3 CTAs per SM), k_analysis_big for the 13 blocks with a 64-sample side (4 warps with the larger scratch).
+// Two kernels share the block search: k_analysis for the 324 blocks of the shapes up to 32 samples a side from 8x8 /
+// 4x16 / 16x4 up (8 warps, 3 CTAs per SM), k_analysis_big for the 13 blocks with a 64-sample side (4 warps with the
+// larger scratch).  The 512 blocks of 4x4, 4x8 and 8x4 have the per-thread search of is_tiny.cuh.
 constexpr int AN_WARPS = 8, ANB_WARPS = 4;
-constexpr int AN_TASKS = 836, ANB_TASKS = 13;
+constexpr int AN_TASKS = 324, ANB_TASKS = 13;
 constexpr int AN_BUF_INTS = 1088;             // evaluation scratch per warp: 32 / G tasks of H x (W + 1) int32 (<= 32x32)
 constexpr int ANB_BUF_INTS = 64 * 65;
 __constant__ uint8_t c_anTask[AN_TASKS][3];   // (bsize, x4, y4) largest area first, then shape, then raster
@@ -63,7 +64,7 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
                                       int tx0, int ty0, int tx1, int ty1) {
     constexpr int TW = 144;
     const int lane = lane_id();
-    const int txSz = AV1G_T(Max_Tx_Size_Rect)[bs];
+    const int txSz = ST(Max_Tx_Size_Rect)[bs];
     const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
     const int maxX = F.MiCols * 4 - 1, maxY = F.MiRows * 4 - 1;
     const int haveL = x > tx0, haveA = y > ty0;
@@ -235,14 +236,14 @@ __device__ __forceinline__ void an_sb(const FrameDesc &F, unsigned char *smem_ra
 }
 
 template <int BD>
-__global__ void __launch_bounds__(AN_WARPS * 32, 3) k_analysis(const FrameDesc *__restrict__ Fp) {
+__global__ void __launch_bounds__(AN_WARPS * 32, 3) k_analysis(const __grid_constant__ FrameDesc F) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    an_sb<BD, AN_WARPS, AN_BUF_INTS, false>(*Fp, smem_raw);
+    an_sb<BD, AN_WARPS, AN_BUF_INTS, false>(F, smem_raw);
 }
 template <int BD>
-__global__ void __launch_bounds__(ANB_WARPS * 32, 2) k_analysis_big(const FrameDesc *__restrict__ Fp) {
+__global__ void __launch_bounds__(ANB_WARPS * 32, 2) k_analysis_big(const __grid_constant__ FrameDesc F) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    an_sb<BD, ANB_WARPS, ANB_BUF_INTS, true>(*Fp, smem_raw);
+    an_sb<BD, ANB_WARPS, ANB_BUF_INTS, true>(F, smem_raw);
 }
 
 }  // namespace is

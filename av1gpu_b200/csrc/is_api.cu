@@ -22,6 +22,7 @@
 #include "is_dev.cuh"
 #include "is_frame.cuh"
 #include "is_analysis.cuh"
+#include "is_tiny.cuh"
 #include "is_dp.cuh"
 #include "is_recon.cuh"
 
@@ -149,7 +150,8 @@ std::vector<uint8_t> an_tasks(bool big) {
     for (int s = 0; s < AV1G_BLOCK_INVALID; s++) {
         if (s >= 13 && s <= 15) continue;
         const bool b = AV1G_T(Num_4x4_Blocks_Wide)[s] == 16 || AV1G_T(Num_4x4_Blocks_High)[s] == 16;
-        if (b == big) shapes.push_back(s);
+        // the 4x4, 4x8 and 8x4 blocks have their own kernel (k_analysis_tiny)
+        if (b == big && s != AV1G_BLOCK_4X4 && s != AV1G_BLOCK_4X8 && s != AV1G_BLOCK_8X4) shapes.push_back(s);
     }
     std::stable_sort(shapes.begin(), shapes.end(), [](int a, int b) {
         return AV1G_T(Num_4x4_Blocks_Wide)[a] * AV1G_T(Num_4x4_Blocks_High)[a] > AV1G_T(Num_4x4_Blocks_Wide)[b] * AV1G_T(Num_4x4_Blocks_High)[b];
@@ -189,9 +191,7 @@ struct is_handle {
     // workspace
     void *arena = nullptr;
     size_t arenaBytes = 0;
-    FrameDesc F;                 // host copy of the descriptor (device pointers)
-    FrameDesc *dF = nullptr;     // device copy
-    FrameDesc *hFpinned = nullptr;
+    FrameDesc F;                 // the descriptor (device pointers), passed by value to every kernel
     int nSb = 0;
     int geomW = -1, geomH = -1;
     size_t smemAn = 0, smemAnBig = 0, smemRc = 0;
@@ -263,6 +263,19 @@ int upload_tables(int dev) {
         if (e == cudaSuccess) e = pack.size() == (size_t)SCAN_PACK ? cudaMemcpyToSymbol(g_scanPack, pack.data(), pack.size() * 2)
                                                                   : cudaErrorInvalidValue;
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_scanOff, off, sizeof off);
+#define IS_UPLOAD_SPEC_TABLE(T, name, dims) \
+        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_##name, name##_host, sizeof(name##_host));
+        IS_SPEC_TABLES(IS_UPLOAD_SPEC_TABLE)
+#undef IS_UPLOAD_SPEC_TABLE
+        // the compile-time copies of spec tables in the per-thread search must equal av1core's
+        for (int c = 0; c < 3 && e == cudaSuccess; c++) {
+            for (int k = 0; k < 5; k++)
+                if (sig_ref(c, k, 0) != AV1G_T(Sig_Ref_Diff_Offset)[c][k][0] || sig_ref(c, k, 1) != AV1G_T(Sig_Ref_Diff_Offset)[c][k][1]) e = cudaErrorInvalidValue;
+            for (int k = 0; k < 3; k++)
+                if (mag_ref(c, k, 0) != AV1G_T(Mag_Ref_Offset_With_Tx_Class)[c][k][0] || mag_ref(c, k, 1) != AV1G_T(Mag_Ref_Offset_With_Tx_Class)[c][k][1])
+                    e = cudaErrorInvalidValue;
+        }
+        if (kDr23 != AV1G_T(Dr_Intra_Derivative)[23] || kDr45 != AV1G_T(Dr_Intra_Derivative)[45] || kDr67 != AV1G_T(Dr_Intra_Derivative)[67]) e = cudaErrorInvalidValue;
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_baseCtx, &AV1G_T(Coeff_Base_Ctx_Offset)[0][0][0], 19 * 25);
         if (e == cudaSuccess && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3) {
             e = cudaMemcpyToSymbol(c_anTask, tasks.data(), tasks.size());
@@ -343,7 +356,6 @@ size_t layout(int W, int H, uint8_t *base, FrameDesc &F, int &nSb) {
     F.recBlockTxb = (uint32_t *)take(((size_t)nSb * SB_MAX_LEAVES + 1) * 4);
     F.recTxb = (av1g_txb *)take((size_t)nSb * SB_MAX_TXB * sizeof(av1g_txb));
     F.recCoeffs = (int16_t *)take((size_t)nSb * SB_MAX_COEF * 2);
-    take(sizeof(FrameDesc));   // the device copy of the descriptor
     return at;
 }
 
@@ -379,7 +391,6 @@ int is_create(const is_params *p, is_handle **out) {
     for (auto &e : h->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return fail(IS_ERR_CUDA);
     if (cudaMallocHost(&h->hostSmall, 64) != cudaSuccess) return fail(IS_ERR_OOM);
-    if (cudaMallocHost(&h->hFpinned, sizeof(FrameDesc)) != cudaSuccess) return fail(IS_ERR_OOM);
     memset(&h->times, 0, sizeof h->times);
     *out = h;
     return IS_OK;
@@ -394,7 +405,6 @@ void is_destroy(is_handle *h) {
         if (e) cudaEventDestroy(e);
     if (h->own) cudaStreamDestroy(h->own);
     if (h->hostSmall) cudaFreeHost(h->hostSmall);
-    if (h->hFpinned) cudaFreeHost(h->hFpinned);
     if (h->traceBuf) cudaFree(h->traceBuf);
     delete h;
 }
@@ -416,7 +426,6 @@ static int prepare(is_handle *h, const is_frame *f) {
     }
     memset(&F, 0, sizeof F);
     layout(f->width, f->height, (uint8_t *)h->arena, F, nSb);
-    h->dF = (FrameDesc *)((uint8_t *)h->arena + need - align256(sizeof(FrameDesc)));
     // tiles, wavefront order, decode order
     std::vector<int> cs, rs;
     min_tiles(f->width, f->height, cs, rs);
@@ -468,10 +477,7 @@ static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) 
     FrameDesc &F = h->F;
     const int nSb = h->nSb;
     IS_CK(cudaEventRecord(h->ev[0], st));
-    // descriptor (pinned staging so the copy stays asynchronous)
-    IS_CK(cudaStreamSynchronize(st));   // the pinned staging copy of a previous encode must be consumed
-    *h->hFpinned = F;
-    IS_CK(cudaMemcpyAsync(h->dF, h->hFpinned, sizeof(FrameDesc), cudaMemcpyHostToDevice, st));
+    // (the descriptor travels by value in every launch's parameters: no copy, no device-side read of it)
     // planes into the padded workspace
     for (int p = 0; p < 3; p++) {
         const int ss = p ? 1 : 0;
@@ -485,27 +491,27 @@ static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) 
     IS_CK(cudaMemsetAsync(F.queue, 0, 16, st));
     IS_CK(cudaMemsetAsync(F.err, 0, 4, st));
     IS_CK(cudaEventRecord(h->ev[1], st));
-    k_analysis_big<8><<<nSb, ANB_WARPS * 32, h->smemAnBig, st>>>(h->dF);
-    k_analysis<8><<<nSb, AN_WARPS * 32, h->smemAn, st>>>(h->dF);
+    k_analysis_big<8><<<nSb, ANB_WARPS * 32, h->smemAnBig, st>>>(h->F);
+    k_analysis<8><<<nSb, AN_WARPS * 32, h->smemAn, st>>>(h->F);
+    k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem), st>>>(h->F);
     IS_CK(cudaGetLastError());
     IS_CK(cudaEventRecord(h->ev[2], st));
-    k_dp<<<(nSb + 63) / 64, 64, 0, st>>>(h->dF, nSb);
+    k_dp<<<(nSb + 63) / 64, 64, 0, st>>>(h->F, nSb);
     IS_CK(cudaGetLastError());
     IS_CK(cudaEventRecord(h->ev[3], st));
-    k_leaf_prep<<<nSb, 256, 0, st>>>(h->dF, nSb);
-    k_leaf_queue_scan<<<1, 1024, 0, st>>>(h->dF, nSb);
-    k_leaf_deps<0><<<nSb, 256, 0, st>>>(h->dF, nSb);
-    k_leaf_deps<1><<<nSb, 256, 0, st>>>(h->dF, nSb);
-    k_leaf_deps<2><<<nSb, 256, 0, st>>>(h->dF, nSb);
+    k_leaf_prep<<<nSb, 256, 0, st>>>(h->F, nSb);
+    k_leaf_queue_scan<<<1, 1024, 0, st>>>(h->F, nSb);
+    k_leaf_deps<0><<<nSb, 256, 0, st>>>(h->F, nSb);
+    k_leaf_deps<1><<<nSb, 256, 0, st>>>(h->F, nSb);
+    k_leaf_deps<2><<<nSb, 256, 0, st>>>(h->F, nSb);
     IS_CK(cudaGetLastError());
     {
-        const FrameDesc *a0 = h->dF;
-        void *args[1] = {(void *)&a0};
+        void *args[1] = {(void *)&h->F};
         IS_CK(cudaLaunchCooperativeKernel((const void *)k_recon<8>, dim3(h->rcGrid), dim3(RC_WARPS * 32), args, h->smemRc, st));
     }
     IS_CK(cudaEventRecord(h->ev[4], st));
-    k_pack_scan<<<1, 1024, 0, st>>>(h->dF, nSb);
-    k_pack<<<nSb, 256, 0, st>>>(h->dF, nSb);
+    k_pack_scan<<<1, 1024, 0, st>>>(h->F, nSb);
+    k_pack<<<nSb, 256, 0, st>>>(h->F, nSb);
     IS_CK(cudaGetLastError());
     IS_CK(cudaEventRecord(h->ev[5], st));
     // counts + error status

@@ -38,6 +38,41 @@ __constant__ int c_avgY[13];           // y_mode bits averaged over its 25 conte
 __constant__ int c_avgPart[5][10];     // partition bits averaged over contexts, per block-size level
 __constant__ int c_avgSkip0;           // skip = 0 averaged over contexts
 
+// ---- the spec tables of the device code, in constant memory (av1core spec_tables.h values, copied from its host
+// tables when the library uploads its tables): uniform-index reads hit the constant cache instead of global memory ----
+#define IS_SPEC_TABLES(X) \
+    X(uint8_t, Adjusted_Tx_Size, [19]) \
+    X(uint8_t, Coeff_Base_Pos_Ctx_Offset, [3]) \
+    X(uint16_t, Dr_Intra_Derivative, [90]) \
+    X(uint8_t, Intra_Mode_Context, [13]) \
+    X(uint8_t, Mag_Ref_Offset_With_Tx_Class, [3][3][2]) \
+    X(uint8_t, Max_Tx_Size_Rect, [22]) \
+    X(uint8_t, Mode_To_Angle, [13]) \
+    X(uint8_t, Mode_To_Txfm, [14]) \
+    X(uint8_t, Num_4x4_Blocks_High, [22]) \
+    X(uint8_t, Num_4x4_Blocks_Wide, [22]) \
+    X(uint8_t, Partition_Subsize, [10][22]) \
+    X(uint8_t, Sig_Ref_Diff_Offset, [3][5][2]) \
+    X(uint8_t, Sm_Weights_Tx_16x16, [16]) \
+    X(uint8_t, Sm_Weights_Tx_32x32, [32]) \
+    X(uint8_t, Sm_Weights_Tx_4x4, [4]) \
+    X(uint8_t, Sm_Weights_Tx_64x64, [64]) \
+    X(uint8_t, Sm_Weights_Tx_8x8, [8]) \
+    X(uint8_t, Subsampled_Size, [22][2][2]) \
+    X(uint8_t, Transform_Row_Shift, [19]) \
+    X(uint8_t, Tx_Height, [19]) \
+    X(uint8_t, Tx_Height_Log2, [19]) \
+    X(uint8_t, Tx_Size_Sqr, [19]) \
+    X(uint8_t, Tx_Size_Sqr_Up, [19]) \
+    X(uint8_t, Tx_Type_In_Set_Intra, [3][16]) \
+    X(uint8_t, Tx_Type_Intra_Inv_Set1, [7]) \
+    X(uint8_t, Tx_Type_Intra_Inv_Set2, [5]) \
+    X(uint8_t, Tx_Width, [19]) \
+    X(uint8_t, Tx_Width_Log2, [19])
+#define IS_DECL_SPEC_TABLE(T, name, dims) __constant__ T c_##name dims;
+IS_SPEC_TABLES(IS_DECL_SPEC_TABLE)
+#define ST(name) c_##name
+
 // ---- the tables of the rate loop: the cost table of the image's q-context, every scan of the intra tx sizes /
 // classes (packed), the 2-D base-context offsets.  A kernel whose few warps each run a long dependent chain (the
 // closed loop) stages them once per CTA in shared memory (RateStage); the others read them from global memory. ----
@@ -127,24 +162,24 @@ __device__ __forceinline__ int warp_argmin(i64 v, int i) {
 }
 
 // ---- geometry (spec tables) ----
-__device__ __forceinline__ int bw4(int bs) { return AV1G_T(Num_4x4_Blocks_Wide)[bs]; }
-__device__ __forceinline__ int bh4(int bs) { return AV1G_T(Num_4x4_Blocks_High)[bs]; }
-__device__ __forceinline__ int txw(int t) { return AV1G_T(Tx_Width)[t]; }
-__device__ __forceinline__ int txh(int t) { return AV1G_T(Tx_Height)[t]; }
+__device__ __forceinline__ int bw4(int bs) { return ST(Num_4x4_Blocks_Wide)[bs]; }
+__device__ __forceinline__ int bh4(int bs) { return ST(Num_4x4_Blocks_High)[bs]; }
+__device__ __forceinline__ int txw(int t) { return ST(Tx_Width)[t]; }
+__device__ __forceinline__ int txh(int t) { return ST(Tx_Height)[t]; }
 __device__ __forceinline__ bool is_dir(int m) { return m >= AV1G_V_PRED && m <= AV1G_D67_PRED; }
 __device__ __forceinline__ int cand_mode(int c) { return c >> 3; }
 __device__ __forceinline__ int cand_delta(int c) { return (c & 7) - 3; }
 __device__ __forceinline__ int cand_pack(int m, int d) { return (m << 3) | (d + 3); }
-__device__ __forceinline__ int pangle(int m, int d) { return is_dir(m) ? AV1G_T(Mode_To_Angle)[m] + d * AV1G_ANGLE_STEP : 0; }
+__device__ __forceinline__ int pangle(int m, int d) { return is_dir(m) ? ST(Mode_To_Angle)[m] + d * AV1G_ANGLE_STEP : 0; }
 
 // get_tx_set() for intra (spec 5.11.48), reduced_tx_set = 0
 __device__ __forceinline__ int tx_set_intra(int txSz) {
-    const int up = AV1G_T(Tx_Size_Sqr_Up)[txSz];
+    const int up = ST(Tx_Size_Sqr_Up)[txSz];
     if (up >= AV1G_TX_32X32) return AV1G_TX_SET_DCTONLY;
-    if (AV1G_T(Tx_Size_Sqr)[txSz] == AV1G_TX_16X16) return AV1G_TX_SET_INTRA_2;
+    if (ST(Tx_Size_Sqr)[txSz] == AV1G_TX_16X16) return AV1G_TX_SET_INTRA_2;
     return AV1G_TX_SET_INTRA_1;
 }
-__device__ __forceinline__ bool tx_in_set(int set, int t) { return AV1G_T(Tx_Type_In_Set_Intra)[set][t] != 0; }
+__device__ __forceinline__ bool tx_in_set(int set, int t) { return ST(Tx_Type_In_Set_Intra)[set][t] != 0; }
 // 1-D kinds of a 2-D type: 0 DCT, 1 ADST, 2 identity (no FLIPADST occurs in the intra sets)
 __device__ __forceinline__ int col_kind(int t) {
     return (t == AV1G_DCT_DCT || t == AV1G_DCT_ADST || t == AV1G_V_DCT) ? 0 : (t == AV1G_IDTX || t == AV1G_H_DCT) ? 2 : 1;
@@ -157,8 +192,8 @@ __device__ __forceinline__ int tx_class(int t) {
 }
 // chroma type (spec compute_tx_type for plane > 0): Mode_To_Txfm if in the set, else DCT_DCT
 __device__ __forceinline__ int chroma_tx_type(int uvTx, int uvMode) {
-    if (AV1G_T(Tx_Size_Sqr_Up)[uvTx] > AV1G_TX_32X32) return AV1G_DCT_DCT;
-    const int t = AV1G_T(Mode_To_Txfm)[uvMode];
+    if (ST(Tx_Size_Sqr_Up)[uvTx] > AV1G_TX_32X32) return AV1G_DCT_DCT;
+    const int t = ST(Mode_To_Txfm)[uvMode];
     return tx_in_set(tx_set_intra(uvTx), t) ? t : AV1G_DCT_DCT;
 }
 // get_scan() (spec 5.11.41), intra types only (no flips): the scan of the size's class in the packed tables
@@ -185,9 +220,9 @@ __device__ __forceinline__ bool has_chroma(int bs, int mi_row, int mi_col, int s
     if (ss && bw4(bs) == 1 && (mi_col & 1) == 0) return false;
     return true;
 }
-__device__ __forceinline__ int uv_bsize(int bs, int ss) { return AV1G_T(Subsampled_Size)[bs][ss][ss]; }
+__device__ __forceinline__ int uv_bsize(int bs, int ss) { return ST(Subsampled_Size)[bs][ss][ss]; }
 __device__ __forceinline__ int uv_tx_size(int bs, int ss) {
-    const int t = AV1G_T(Max_Tx_Size_Rect)[uv_bsize(bs, ss)];
+    const int t = ST(Max_Tx_Size_Rect)[uv_bsize(bs, ss)];
     const int w = txw(t), h = txh(t);
     if (w == 64 || h == 64) return w == 16 ? AV1G_TX_16X32 : h == 16 ? AV1G_TX_32X16 : AV1G_TX_32X32;
     return t;
@@ -205,26 +240,26 @@ __device__ __forceinline__ int pred_px(int mode, int pAng, int i, int j, int lw,
         if (pAng == 90) return A[j];
         if (pAng == 180) return L[i];
         if (pAng < 90) {
-            const int dx = AV1G_T(Dr_Intra_Derivative)[pAng];
+            const int dx = ST(Dr_Intra_Derivative)[pAng];
             const int idx = (i + 1) * dx, base = (idx >> 6) + j, sh = (idx >> 1) & 0x1F;
             const int maxBaseX = w + h - 1;
             return base < maxBaseX ? (A[base] * (32 - sh) + A[base + 1] * sh + 16) >> 5 : A[maxBaseX];
         }
         if (pAng < 180) {
-            const int dx = AV1G_T(Dr_Intra_Derivative)[180 - pAng];
+            const int dx = ST(Dr_Intra_Derivative)[180 - pAng];
             int idx = (j << 6) - (i + 1) * dx;
             int base = idx >> 6;
             if (base >= -1) {
                 const int sh = (idx >> 1) & 0x1F;
                 return (A[base] * (32 - sh) + A[base + 1] * sh + 16) >> 5;
             }
-            const int dy = AV1G_T(Dr_Intra_Derivative)[pAng - 90];
+            const int dy = ST(Dr_Intra_Derivative)[pAng - 90];
             idx = (i << 6) - (j + 1) * dy;
             base = idx >> 6;
             const int sh = (idx >> 1) & 0x1F;
             return (L[base] * (32 - sh) + L[base + 1] * sh + 16) >> 5;
         }
-        const int dy = AV1G_T(Dr_Intra_Derivative)[270 - pAng];
+        const int dy = ST(Dr_Intra_Derivative)[270 - pAng];
         const int idx = (j + 1) * dy, base = (idx >> 6) + i, sh = (idx >> 1) & 0x1F;
         return (L[base] * (32 - sh) + L[base + 1] * sh + 16) >> 5;
     }
@@ -233,10 +268,10 @@ __device__ __forceinline__ int pred_px(int mode, int pAng, int i, int j, int lw,
         const int pL = abs(base - l), pT = abs(base - a), pTL = abs(base - tl);
         return (pL <= pT && pL <= pTL) ? l : pT <= pTL ? a : tl;
     }
-    const uint8_t *wx = lw == 2 ? AV1G_T(Sm_Weights_Tx_4x4) : lw == 3 ? AV1G_T(Sm_Weights_Tx_8x8) : lw == 4 ? AV1G_T(Sm_Weights_Tx_16x16)
-                      : lw == 5 ? AV1G_T(Sm_Weights_Tx_32x32) : AV1G_T(Sm_Weights_Tx_64x64);
-    const uint8_t *wy = lh == 2 ? AV1G_T(Sm_Weights_Tx_4x4) : lh == 3 ? AV1G_T(Sm_Weights_Tx_8x8) : lh == 4 ? AV1G_T(Sm_Weights_Tx_16x16)
-                      : lh == 5 ? AV1G_T(Sm_Weights_Tx_32x32) : AV1G_T(Sm_Weights_Tx_64x64);
+    const uint8_t *wx = lw == 2 ? ST(Sm_Weights_Tx_4x4) : lw == 3 ? ST(Sm_Weights_Tx_8x8) : lw == 4 ? ST(Sm_Weights_Tx_16x16)
+                      : lw == 5 ? ST(Sm_Weights_Tx_32x32) : ST(Sm_Weights_Tx_64x64);
+    const uint8_t *wy = lh == 2 ? ST(Sm_Weights_Tx_4x4) : lh == 3 ? ST(Sm_Weights_Tx_8x8) : lh == 4 ? ST(Sm_Weights_Tx_16x16)
+                      : lh == 5 ? ST(Sm_Weights_Tx_32x32) : ST(Sm_Weights_Tx_64x64);
     if (mode == AV1G_SMOOTH_PRED)
         return (wy[i] * A[j] + (256 - wy[i]) * L[h - 1] + wx[j] * L[i] + (256 - wx[j]) * A[w - 1] + 256) >> 9;
     if (mode == AV1G_SMOOTH_V_PRED) return (wy[i] * A[j] + (256 - wy[i]) * L[h - 1] + 128) >> 8;
@@ -267,7 +302,7 @@ __device__ __noinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, i
 #pragma unroll
                 for (int j = 0; j < 4; j++) p[i * 4 + j] = L[sy + i];
         } else if (pAng < 90) {
-            const int dx = AV1G_T(Dr_Intra_Derivative)[pAng], maxBaseX = w + h - 1;
+            const int dx = ST(Dr_Intra_Derivative)[pAng], maxBaseX = w + h - 1;
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 const int idx = (sy + i + 1) * dx, base = (idx >> 6) + sx, sh = (idx >> 1) & 0x1F;
@@ -278,7 +313,7 @@ __device__ __noinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, i
                 }
             }
         } else if (pAng > 180) {
-            const int dy = AV1G_T(Dr_Intra_Derivative)[270 - pAng];
+            const int dy = ST(Dr_Intra_Derivative)[270 - pAng];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int idx = (sx + j + 1) * dy, base = (idx >> 6) + sy, sh = (idx >> 1) & 0x1F;
@@ -286,7 +321,7 @@ __device__ __noinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, i
                 for (int i = 0; i < 4; i++) p[i * 4 + j] = (L[base + i] * (32 - sh) + L[base + i + 1] * sh + 16) >> 5;
             }
         } else {
-            const int dx = AV1G_T(Dr_Intra_Derivative)[180 - pAng], dy = AV1G_T(Dr_Intra_Derivative)[pAng - 90];
+            const int dx = ST(Dr_Intra_Derivative)[180 - pAng], dy = ST(Dr_Intra_Derivative)[pAng - 90];
 #pragma unroll
             for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -313,10 +348,10 @@ __device__ __noinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, i
         return;
     }
     // SMOOTH / SMOOTH_V / SMOOTH_H: sum of the vertical and horizontal terms of the modes that use them
-    const uint8_t *wx = (lw == 2 ? AV1G_T(Sm_Weights_Tx_4x4) : lw == 3 ? AV1G_T(Sm_Weights_Tx_8x8) : lw == 4 ? AV1G_T(Sm_Weights_Tx_16x16)
-                       : lw == 5 ? AV1G_T(Sm_Weights_Tx_32x32) : AV1G_T(Sm_Weights_Tx_64x64)) + sx;
-    const uint8_t *wy = (lh == 2 ? AV1G_T(Sm_Weights_Tx_4x4) : lh == 3 ? AV1G_T(Sm_Weights_Tx_8x8) : lh == 4 ? AV1G_T(Sm_Weights_Tx_16x16)
-                       : lh == 5 ? AV1G_T(Sm_Weights_Tx_32x32) : AV1G_T(Sm_Weights_Tx_64x64)) + sy;
+    const uint8_t *wx = (lw == 2 ? ST(Sm_Weights_Tx_4x4) : lw == 3 ? ST(Sm_Weights_Tx_8x8) : lw == 4 ? ST(Sm_Weights_Tx_16x16)
+                       : lw == 5 ? ST(Sm_Weights_Tx_32x32) : ST(Sm_Weights_Tx_64x64)) + sx;
+    const uint8_t *wy = (lh == 2 ? ST(Sm_Weights_Tx_4x4) : lh == 3 ? ST(Sm_Weights_Tx_8x8) : lh == 4 ? ST(Sm_Weights_Tx_16x16)
+                       : lh == 5 ? ST(Sm_Weights_Tx_32x32) : ST(Sm_Weights_Tx_64x64)) + sy;
     const int bl = L[h - 1], tr = A[w - 1];
     const int sh = mode == AV1G_SMOOTH_PRED ? 9 : 8, useV = mode != AV1G_SMOOTH_H_PRED, useH = mode != AV1G_SMOOTH_V_PRED;
 #pragma unroll
@@ -476,10 +511,10 @@ struct TxRt {
 __device__ __forceinline__ TxRt tx_rt(int txSz, int bd) {
     TxRt d;
     d.W = txw(txSz); d.H = txh(txSz);
-    d.lw = AV1G_T(Tx_Width_Log2)[txSz]; d.lh = AV1G_T(Tx_Height_Log2)[txSz];
+    d.lw = ST(Tx_Width_Log2)[txSz]; d.lh = ST(Tx_Height_Log2)[txSz];
     d.tw = min(d.W, 32); d.th = min(d.H, 32); d.ltw = min(d.lw, 5); d.n = d.tw * d.th;
     d.TS = d.W + 1;
-    d.rowShift = AV1G_T(Transform_Row_Shift)[txSz];
+    d.rowShift = ST(Transform_Row_Shift)[txSz];
     d.rect = (d.lw - d.lh == 1 || d.lh - d.lw == 1) ? 1 : 0;
     const int E = d.rowShift + 4 + FB - (d.lw + d.lh - 2);
     d.s0 = max(0, 17 - bd - d.lh);
@@ -535,14 +570,14 @@ struct EvalIn {
 struct EvalOut { i64 D, R; int eob; };
 
 __device__ __forceinline__ int tx_index_in_set(int set, int t) {
-    if (set == AV1G_TX_SET_INTRA_1) { for (int i = 0; i < 7; i++) if (AV1G_T(Tx_Type_Intra_Inv_Set1)[i] == t) return i; }
-    else { for (int i = 0; i < 5; i++) if (AV1G_T(Tx_Type_Intra_Inv_Set2)[i] == t) return i; }
+    if (set == AV1G_TX_SET_INTRA_1) { for (int i = 0; i < 7; i++) if (ST(Tx_Type_Intra_Inv_Set1)[i] == t) return i; }
+    else { for (int i = 0; i < 5; i++) if (ST(Tx_Type_Intra_Inv_Set2)[i] == t) return i; }
     return 0;
 }
 
 // txb_skip, tx type, eob position bits
-__device__ __noinline__ i64 base_bits(int txSz, const EvalIn &e, int eob) {
-    const int txSzCtx = (AV1G_T(Tx_Size_Sqr)[txSz] + AV1G_T(Tx_Size_Sqr_Up)[txSz] + 1) >> 1;
+__device__ __forceinline__ i64 base_bits_inl(int txSz, const EvalIn &e, int eob) {
+    const int txSzCtx = (ST(Tx_Size_Sqr)[txSz] + ST(Tx_Size_Sqr_Up)[txSz] + 1) >> 1;
     const uint16_t *C = e.T.cost;
     if (eob == 0) return C[ci_txb_skip(txSzCtx, e.skipCtx) + 1];
     i64 b = C[ci_txb_skip(txSzCtx, e.skipCtx)];
@@ -550,11 +585,11 @@ __device__ __noinline__ i64 base_bits(int txSz, const EvalIn &e, int eob) {
     if (e.plane == 0) {
         const int set = tx_set_intra(txSz);
         if (set > 0) {
-            const int sqr = AV1G_T(Tx_Size_Sqr)[txSz], idx = tx_index_in_set(set, e.txType);
+            const int sqr = ST(Tx_Size_Sqr)[txSz], idx = tx_index_in_set(set, e.txType);
             b += set == AV1G_TX_SET_INTRA_1 ? C[ci_set1(sqr, e.intraDir) + idx] : C[ci_set2(sqr, e.intraDir) + idx];
         }
     }
-    const int ms = min((int)AV1G_T(Tx_Width_Log2)[txSz], 5) + min((int)AV1G_T(Tx_Height_Log2)[txSz], 5) - 4;
+    const int ms = min((int)ST(Tx_Width_Log2)[txSz], 5) + min((int)ST(Tx_Height_Log2)[txSz], 5) - 4;
     const int eobPt = eob <= 2 ? eob : 2 + (31 - __clz(eob - 1));
     b += C[ci_eob_pt(ms, ptype, tx_class(e.txType) == AV1G_TX_CLASS_2D ? 0 : 1) + eobPt - 1];
     if (eobPt >= 3) {
@@ -564,15 +599,16 @@ __device__ __noinline__ i64 base_bits(int txSz, const EvalIn &e, int eob) {
     }
     return b;
 }
+__device__ __noinline__ i64 base_bits(int txSz, const EvalIn &e, int eob) { return base_bits_inl(txSz, e, eob); }
 
 // bits of the coefficient at scan position c < eob (levels q natural order, row stride = adjusted width)
 __device__ __forceinline__ int coeff_bits(int c, int eob, const int16_t *q, const uint16_t *scan, int txSz, int txClass, int ptype,
                                           int dcCtx, const RateTabs &T) {
     const uint16_t *C = T.cost;
-    const int txSzCtx = (AV1G_T(Tx_Size_Sqr)[txSz] + AV1G_T(Tx_Size_Sqr_Up)[txSz] + 1) >> 1;
-    const int adj = AV1G_T(Adjusted_Tx_Size)[txSz];
-    const int bwl = AV1G_T(Tx_Width_Log2)[adj];
-    const int width = 1 << bwl, height = AV1G_T(Tx_Height)[adj];
+    const int txSzCtx = (ST(Tx_Size_Sqr)[txSz] + ST(Tx_Size_Sqr_Up)[txSz] + 1) >> 1;
+    const int adj = ST(Adjusted_Tx_Size)[txSz];
+    const int bwl = ST(Tx_Width_Log2)[adj];
+    const int width = 1 << bwl, height = ST(Tx_Height)[adj];
     const int pos = scan[c];
     const int qv = q[pos], v = abs(qv), level = min(v, 15);
     const int row = pos >> bwl, col = pos - (row << bwl);
@@ -585,19 +621,19 @@ __device__ __forceinline__ int coeff_bits(int c, int eob, const int16_t *q, cons
         int mag = 0;
 #pragma unroll
         for (int k = 0; k < 5; k++) {
-            const int rr = row + AV1G_T(Sig_Ref_Diff_Offset)[txClass][k][0], cc = col + AV1G_T(Sig_Ref_Diff_Offset)[txClass][k][1];
+            const int rr = row + ST(Sig_Ref_Diff_Offset)[txClass][k][0], cc = col + ST(Sig_Ref_Diff_Offset)[txClass][k][1];
             if (rr < height && cc < width) mag += min(abs((int)q[(rr << bwl) + cc]), 3);
         }
         int bctx = min((mag + 1) >> 1, 4);
         if (txClass == AV1G_TX_CLASS_2D) bctx = (row == 0 && col == 0) ? 0 : bctx + T.baseCtx[txSz * 25 + min(row, 4) * 5 + min(col, 4)];
-        else bctx += AV1G_T(Coeff_Base_Pos_Ctx_Offset)[min(txClass == AV1G_TX_CLASS_VERT ? row : col, 2)];
+        else bctx += ST(Coeff_Base_Pos_Ctx_Offset)[min(txClass == AV1G_TX_CLASS_VERT ? row : col, 2)];
         b = C[ci_base(txSzCtx, ptype, bctx) + min(level, 3)];
     }
     if (level > 2) {
         int mag = 0;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            const int rr = row + AV1G_T(Mag_Ref_Offset_With_Tx_Class)[txClass][k][0], cc = col + AV1G_T(Mag_Ref_Offset_With_Tx_Class)[txClass][k][1];
+            const int rr = row + ST(Mag_Ref_Offset_With_Tx_Class)[txClass][k][0], cc = col + ST(Mag_Ref_Offset_With_Tx_Class)[txClass][k][1];
             if (rr < height && cc < width) mag += min(abs((int)q[rr * width + cc]), 15);
         }
         mag = min((mag + 1) >> 1, 6);

@@ -12,17 +12,16 @@ __device__ __forceinline__ i64 sat_add(i64 a, i64 b) { return (a >= INF || b >= 
 __device__ __forceinline__ int sq_bsize(int n) {
     return n == 4 ? AV1G_BLOCK_4X4 : n == 8 ? AV1G_BLOCK_8X8 : n == 16 ? AV1G_BLOCK_16X16 : n == 32 ? AV1G_BLOCK_32X32 : AV1G_BLOCK_64X64;
 }
-__device__ __forceinline__ int sub_bsize(int p, int n) { return AV1G_T(Partition_Subsize)[p][sq_bsize(n)]; }
+__device__ __forceinline__ int sub_bsize(int p, int n) { return ST(Partition_Subsize)[p][sq_bsize(n)]; }
 
 __device__ __forceinline__ i64 dp_blockJ(const FrameDesc &F, int bs, int x, int y) {
     if (bs >= AV1G_BLOCK_INVALID || F.shNbx[bs] == 0) return INF;
     return F.blk[F.shOff[bs] + (uint32_t)(y / (4 * bh4(bs))) * F.shNbx[bs] + x / (4 * bw4(bs))].J;
 }
 
-__global__ void k_dp(const FrameDesc *__restrict__ Fp, int nSb) {
+__global__ void k_dp(const __grid_constant__ FrameDesc F, int nSb) {
     const int sb = blockIdx.x * blockDim.x + threadIdx.x;
     if (sb >= nSb) return;
-    const FrameDesc &F = *Fp;
     const int sbx = (sb % F.sbCols) * 64, sby = (sb / F.sbCols) * 64;
     const int FW = F.MiCols * 4, FH = F.MiRows * 4;
     const i64 lam = F.lam;

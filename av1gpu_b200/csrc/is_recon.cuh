@@ -22,7 +22,7 @@
 
 namespace is {
 
-constexpr int RC_WARPS = 7;                // warps per CTA (independent workers; shared memory bounds the count)
+constexpr int RC_WARPS = 4;                // warps per CTA (independent workers; shared memory bounds the count)
 constexpr int LEAF_WAIT_ITERS = 1 << 20;   // bounded spins: a wait that runs out records an error and moves on, and
                                            // once any error is recorded no further wait starts (the host discards the
                                            // result)
@@ -291,7 +291,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
     // ================= luma =================
     int yMode, yDelta, eobY;
     {
-        const int txSz = AV1G_T(Max_Tx_Size_Rect)[bsize];
+        const int txSz = ST(Max_Tx_Size_Rect)[bsize];
         const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
         const int haveAR = decoded(0, lf.y4 - 1, lf.x4 + (W >> 2)), haveBL = decoded(0, lf.y4 + (H >> 2), lf.x4 - 1);
         Px *A = Wp.ea[0] + EDGE_OFF, *L = Wp.el[0] + EDGE_OFF;
@@ -301,8 +301,8 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
         const BlockRes br = F.blk[F.shOff[bsize] + (uint32_t)(y / H) * F.shNbx[bsize] + x / W];
         int skipCtx, dcCtx;
         rc_txb_ctx(F, 0, txSz, x >> 2, y >> 2, bsize, tC0, tR0, &skipCtx, &dcCtx);
-        const int am = AV1G_T(Intra_Mode_Context)[availU ? __ldcg(F.mYMode + (size_t)(mi_row - 1) * F.MiCols + mi_col) : AV1G_DC_PRED];
-        const int lm = AV1G_T(Intra_Mode_Context)[availL ? __ldcg(F.mYMode + (size_t)mi_row * F.MiCols + mi_col - 1) : AV1G_DC_PRED];
+        const int am = ST(Intra_Mode_Context)[availU ? __ldcg(F.mYMode + (size_t)(mi_row - 1) * F.MiCols + mi_col) : AV1G_DC_PRED];
+        const int lm = ST(Intra_Mode_Context)[availL ? __ldcg(F.mYMode + (size_t)mi_row * F.MiCols + mi_col - 1) : AV1G_DC_PRED];
         auto mbits = [&](int c) -> int {
             const int m = cand_mode(c);
             int b = C[ci_y_mode(am, lm) + m];
@@ -595,7 +595,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
             grp_eval<BD, Px>(txSz, ResFn<Px>{sP[pl], F.spitch[pl], Wp.pred, lw, nullptr}, e, Wp.buf, lv, lane, 32);
             Px *dst = (Px *)F.rec[pl] + (size_t)cy * F.rpitch[pl] + cx;
             rc_reconstruct<BD, Px>(txSz, uvType, lv, F.dcQ, F.acQ, Wp.pred, dst, F.rpitch[pl], Wp.buf);
-            const int yt = AV1G_T(Max_Tx_Size_Rect)[bsize];
+            const int yt = ST(Max_Tx_Size_Rect)[bsize];
             const int off = coefBase + min(txw(yt), 32) * min(txh(yt), 32) + (pl - 1) * nq;
             const int e2 = rc_record(F, T, sb, pl, txSz, uvType, cx4, cy4, lv, txbBase + pl, off);
             if (pl == 1) eobU = e2; else eobV = e2;
@@ -631,11 +631,10 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
 // written there (bounded in time), and runs it
 constexpr unsigned long long READY_WAIT_NS = 4000000000ull;
 template <int BD>
-__global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__restrict__ Fp) {
+__global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const __grid_constant__ FrameDesc F) {
     typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RcSmem<Px> &S = *reinterpret_cast<RcSmem<Px> *>(smem_raw);
-    const FrameDesc &F = *Fp;
     RcWarp<Px> &Wp = S.w[threadIdx.x >> 5];
     const int lane = lane_id();
     const RateTabs T = rate_tabs_stage(S.T, F.qctx, threadIdx.x, blockDim.x);
@@ -668,8 +667,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
 
 // ---- before the closed loop: per SB the map of leaf indices, per leaf its first tx block and coefficient (SB-local),
 // per SB the output counts; then the global leaf queue (SBs in wavefront order, leaves in decode order) ----
-__global__ void k_leaf_prep(const FrameDesc *__restrict__ Fp, int nSb) {
-    const FrameDesc &F = *Fp;
+__global__ void k_leaf_prep(const __grid_constant__ FrameDesc F, int nSb) {
     const int sb = blockIdx.x, tid = threadIdx.x;
     if (sb >= nSb) return;
     __shared__ uint8_t om[256];
@@ -695,7 +693,7 @@ __global__ void k_leaf_prep(const FrameDesc *__restrict__ Fp, int nSb) {
             F.leafTxb[(size_t)sb * SB_MAX_LEAVES + i] = (uint16_t)nt;
             F.leafCoef[(size_t)sb * SB_MAX_LEAVES + i] = (uint16_t)ncf;
             const Leaf l = F.leaves[(size_t)sb * SB_MAX_LEAVES + i];
-            const int yt = AV1G_T(Max_Tx_Size_Rect)[l.bsize];
+            const int yt = ST(Max_Tx_Size_Rect)[l.bsize];
             nt += 1;
             ncf += min(txw(yt), 32) * min(txh(yt), 32);
             if (has_chroma(l.bsize, sbr * 16 + l.y4, sbc * 16 + l.x4, F.ssx)) {
@@ -711,8 +709,7 @@ __global__ void k_leaf_prep(const FrameDesc *__restrict__ Fp, int nSb) {
 }
 // exclusive prefix of the leaf counts over the wavefront order (one CTA of 1024 threads), then every SB's leaves into
 // the queue
-__global__ void k_leaf_queue_scan(const FrameDesc *__restrict__ Fp, int nSb) {
-    const FrameDesc &F = *Fp;
+__global__ void k_leaf_queue_scan(const __grid_constant__ FrameDesc F, int nSb) {
     __shared__ uint32_t sN[1024];
     const int tid = threadIdx.x;
     const int per = (nSb + 1023) / 1024, i0 = min(nSb, tid * per), i1 = min(nSb, i0 + per);
@@ -738,8 +735,7 @@ __global__ void k_leaf_queue_scan(const FrameDesc *__restrict__ Fp, int nSb) {
 // and its dependents, 1 gives each leaf its range of revList and queues the leaves without dependencies, 2 writes the
 // dependents.
 template <int PASS>
-__global__ void k_leaf_deps(const FrameDesc *__restrict__ Fp, int nSb) {
-    const FrameDesc &F = *Fp;
+__global__ void k_leaf_deps(const __grid_constant__ FrameDesc F, int nSb) {
     const int sb = blockIdx.x, tid = threadIdx.x;
     if (sb >= nSb || tid >= F.nLeaves[sb]) return;
     const uint32_t me = (uint32_t)sb * SB_MAX_LEAVES + tid;
@@ -765,9 +761,8 @@ __global__ void k_leaf_deps(const FrameDesc *__restrict__ Fp, int nSb) {
 }
 
 // ---- pack: per-SB slots -> DecisionRecord arrays in decode order ----
-__global__ void k_pack_scan(const FrameDesc *__restrict__ Fp, int nSb) {
+__global__ void k_pack_scan(const __grid_constant__ FrameDesc F, int nSb) {
     // exclusive prefix sums of the per-SB counts over the decode order (one CTA of 1024 threads)
-    const FrameDesc &F = *Fp;
     __shared__ uint32_t sB[1024], sT[1024];
     __shared__ unsigned long long sC[1024];
     const int tid = threadIdx.x;
@@ -797,8 +792,7 @@ __global__ void k_pack_scan(const FrameDesc *__restrict__ Fp, int nSb) {
     if (tid == 1023) { F.offBlk[nSb] = sB[1023]; F.offTxb[nSb] = sT[1023]; F.offCoef[nSb] = sC[1023]; }
 }
 
-__global__ void k_pack(const FrameDesc *__restrict__ Fp, int nSb) {
-    const FrameDesc &F = *Fp;
+__global__ void k_pack(const __grid_constant__ FrameDesc F, int nSb) {
     const int i = blockIdx.x;
     if (i >= nSb) return;
     const int sb = (int)F.sbDecodeOrder[i];
