@@ -15,11 +15,12 @@
 
 namespace is {
 
-// Two kernels share the block search: k_analysis for the 324 blocks of the shapes up to 32 samples a side from 8x8 /
-// 4x16 / 16x4 up (8 warps, 3 CTAs per SM), k_analysis_big for the 13 blocks with a 64-sample side (4 warps with the
-// larger scratch).  The 512 blocks of 4x4, 4x8 and 8x4 have the per-thread search of is_tiny.cuh.
+// Two kernels share the block search: k_analysis for the 132 blocks of the shapes up to 32 samples a side from 8x16 /
+// 16x8 / 8x32 / 32x8 up (8 warps, 3 CTAs per SM), k_analysis_big for the 13 blocks with a 64-sample side (4 warps with
+// the larger scratch).  The 704 blocks of 4x4, 4x8, 8x4, 8x8, 4x16 and 16x4 have the per-thread searches of
+// is_tiny.cuh.
 constexpr int AN_WARPS = 8, ANB_WARPS = 4;
-constexpr int AN_TASKS = 324, ANB_TASKS = 13;
+constexpr int AN_TASKS = 132, ANB_TASKS = 13;
 constexpr int AN_BUF_INTS = 1088;             // evaluation scratch per warp: 32 / G tasks of H x (W + 1) int32 (<= 32x32)
 constexpr int ANB_BUF_INTS = 64 * 65;
 __constant__ uint8_t c_anTask[AN_TASKS][3];   // (bsize, x4, y4) largest area first, then shape, then raster

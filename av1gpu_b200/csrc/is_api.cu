@@ -150,8 +150,10 @@ std::vector<uint8_t> an_tasks(bool big) {
     for (int s = 0; s < AV1G_BLOCK_INVALID; s++) {
         if (s >= 13 && s <= 15) continue;
         const bool b = AV1G_T(Num_4x4_Blocks_Wide)[s] == 16 || AV1G_T(Num_4x4_Blocks_High)[s] == 16;
-        // the 4x4, 4x8 and 8x4 blocks have their own kernel (k_analysis_tiny)
-        if (b == big && s != AV1G_BLOCK_4X4 && s != AV1G_BLOCK_4X8 && s != AV1G_BLOCK_8X4) shapes.push_back(s);
+        // the 4x4, 4x8, 8x4 (k_analysis_tiny) and 8x8, 4x16, 16x4 blocks (k_analysis_mid) have their own kernels
+        if (b == big && s != AV1G_BLOCK_4X4 && s != AV1G_BLOCK_4X8 && s != AV1G_BLOCK_8X4 && s != AV1G_BLOCK_8X8 && s != AV1G_BLOCK_4X16 &&
+            s != AV1G_BLOCK_16X4)
+            shapes.push_back(s);
     }
     std::stable_sort(shapes.begin(), shapes.end(), [](int a, int b) {
         return AV1G_T(Num_4x4_Blocks_Wide)[a] * AV1G_T(Num_4x4_Blocks_High)[a] > AV1G_T(Num_4x4_Blocks_Wide)[b] * AV1G_T(Num_4x4_Blocks_High)[b];
@@ -384,6 +386,7 @@ int is_create(const is_params *p, is_handle **out) {
     if (cudaFuncSetAttribute(k_analysis<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemAn) != cudaSuccess) return fail(IS_ERR_CUDA);
     if (cudaFuncSetAttribute(k_analysis_big<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemAnBig) != cudaSuccess) return fail(IS_ERR_CUDA);
     if (cudaFuncSetAttribute(k_recon<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemRc) != cudaSuccess) return fail(IS_ERR_CUDA);
+    if (cudaFuncSetAttribute(k_analysis_mid<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MidSmem)) != cudaSuccess) return fail(IS_ERR_CUDA);
     int per = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_recon<8>, RC_WARPS * 32, h->smemRc) != cudaSuccess || per < 1) return fail(IS_ERR_CUDA);
     h->rcGrid = per * h->nSm;
@@ -494,6 +497,7 @@ static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) 
     k_analysis_big<8><<<nSb, ANB_WARPS * 32, h->smemAnBig, st>>>(h->F);
     k_analysis<8><<<nSb, AN_WARPS * 32, h->smemAn, st>>>(h->F);
     k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem), st>>>(h->F);
+    k_analysis_mid<8><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem), st>>>(h->F);
     IS_CK(cudaGetLastError());
     IS_CK(cudaEventRecord(h->ev[2], st));
     k_dp<<<(nSb + 63) / 64, 64, 0, st>>>(h->F, nSb);

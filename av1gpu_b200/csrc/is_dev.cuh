@@ -283,7 +283,7 @@ __device__ __forceinline__ int pred_px(int mode, int pAng, int i, int j, int lw,
 // (~30 KB of code) serves every caller of a kernel instead of one per call site, which keeps the kernels' hot code
 // within reach of the instruction caches.
 template <typename P>
-__device__ __noinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, int lh, const P *A, const P *L, int dcv, int *p) {
+__device__ __forceinline__ void pred4_inl(int mode, int pAng, int sy, int sx, int lw, int lh, const P *A, const P *L, int dcv, int *p) {
     const int w = 1 << lw, h = 1 << lh;
     if (mode == AV1G_DC_PRED) {
 #pragma unroll
@@ -362,6 +362,10 @@ __device__ __noinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, i
             const int hz = useH ? wx[j] * L[sy + i] + (256 - wx[j]) * tr : 0;
             p[i * 4 + j] = (v + hz + (1 << (sh - 1))) >> sh;
         }
+}
+template <typename P>
+__device__ __noinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, int lh, const P *A, const P *L, int dcv, int *p) {
+    pred4_inl(mode, pAng, sy, sx, lw, lh, A, L, dcv, p);
 }
 
 // the whole prediction of a W x H block into out (row stride W), 4x4 sub-blocks over the G lanes of a group

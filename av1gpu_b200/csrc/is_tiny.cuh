@@ -1,4 +1,6 @@
-// is_tiny.cuh - open-loop analysis of the 4x4, 4x8 and 8x4 blocks: one thread per block, everything in registers.
+// is_tiny.cuh - open-loop analysis of the small blocks, one thread per block: 4x4, 4x8 and 8x4 with everything in
+// registers (k_analysis_tiny); 8x8, 4x16 and 16x4 with the transform in registers and edges / levels in per-thread
+// shared-memory slots (k_analysis_mid).
 //
 // The same search as an_block (the reference's k_analysis, encoder/src/k_analysis.cuh:496-689) for the three smallest
 // shapes - 512 of the 836 analysed blocks of an SB.  A warp-per-block search leaves most lanes idle or divergent on
@@ -430,6 +432,265 @@ __global__ void __launch_bounds__(TINY_THREADS, 1) k_analysis_tiny(const __grid_
     } else {           // 8x4: 8 columns x 16 rows
         const int t = tid - 128, x = sbx + (t & 7) * 8, y = sby + (t >> 3) * 4;
         if (x < FW && y < FH) tiny_block<BD, 3, 2>(F, S, T, AV1G_BLOCK_8X4, AV1G_TX_8X4, 2, x, y, sbx, sby, tx0, ty0, tx1, ty1);
+    }
+}
+
+
+// ================================================================================================================
+// 8x8, 4x16 and 16x4: one thread per block.  Angle deltas (+-1..3 around the two best directional modes) make the
+// prediction angles run-time values, so the edges live in a per-thread shared-memory slot and the prediction is
+// pred4's sub-block code; every candidate and every RD task goes through ONE loop body (one copy of the prediction, the
+// transform and the rate in the binary).  Levels go to a per-thread slot for the rate's context reads.
+// ================================================================================================================
+// One CTA runs ONE shape on the 64 blocks of each of MID_SBS superblocks, so that all its warps (and the co-resident
+// CTAs, which the grid order gives the same shape) share one instruction stream.
+constexpr int MID_SBS = 3, MID_THREADS = 64 * MID_SBS;
+struct MidSmem {
+    static constexpr int TW = 144, TH = 65;
+    uint8_t tile[MID_SBS][TH * TW];
+    uint8_t iscan[3][64];                // the shape's tx size x (2D, HORIZ, VERT)
+    uint8_t edge[MID_THREADS][2][24];    // per thread: AboveRow[-1 .. 22], LeftCol[-1 .. 22]
+    int16_t q[MID_THREADS][64];          // per thread: levels of the evaluation in progress
+    RateStage T;
+};
+
+// forward transform of an N = W x H residual block in registers (grp_eval's column and row passes with their shifts)
+template <int BD, int LW, int LH>
+__device__ __forceinline__ void thr_fwd(int txSz, int txType, const int *res, int *buf) {
+    constexpr int W = 1 << LW, H = 1 << LH;
+    const int rowShift = ST(Transform_Row_Shift)[txSz];
+    constexpr int rect = (LW - LH == 1 || LH - LW == 1) ? 1 : 0;
+    const int E = rowShift + 4 + FB - (LW + LH - 2);
+    const int s0 = max(0, 17 - BD - LH), s2 = s0 - LW - E;
+    const int ck = col_kind(txType), rk = row_kind(txType);
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+        int t[H];
+#pragma unroll
+        for (int i = 0; i < H; i++) t[i] = res[i * W + j] * (1 << s0);
+        fwd1d<H>(ck, t);
+#pragma unroll
+        for (int i = 0; i < H; i++) buf[i * W + j] = (t[i] + (1 << (LW - 1))) >> LW;
+    }
+#pragma unroll
+    for (int i = 0; i < H; i++) {
+        int t[W];
+#pragma unroll
+        for (int j = 0; j < W; j++) t[j] = buf[i * W + j];
+        fwd1d<W>(rk, t);
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            int v = t[j];
+            if (rect) v = (v * 5793 + 2048) >> 12;
+            buf[i * W + j] = s2 > 0 ? (v + (1 << (s2 - 1))) >> s2 : v * (1 << -s2);
+        }
+    }
+}
+
+// one evaluation of a <= 16-point-side block by one thread: transform in registers, levels to qs (shared memory),
+// rate by coeff_bits over the scan
+template <int BD, int LW, int LH>
+__device__ __forceinline__ EvalOut mid_eval(int txSz, const int *res, const EvalIn &e, const uint8_t (*iscan)[64], int16_t *qs) {
+    constexpr int W = 1 << LW, H = 1 << LH, N = W * H;
+    int buf[N];
+    thr_fwd<BD, LW, LH>(txSz, e.txType, res, buf);
+    const int rowShift = ST(Transform_Row_Shift)[txSz];
+    constexpr int rect = (LW - LH == 1 || LH - LW == 1) ? 1 : 0;
+    const int dsh = 16 - 2 * FB - (2 * (rowShift + 4) - (LW + LH - 2) + rect);
+    const int cls = e.txType == AV1G_IDTX ? AV1G_TX_CLASS_2D : tx_class(e.txType);
+    const uint8_t *isc = iscan[cls];
+    i64 dist = 0;
+    int eob = 0;
+#pragma unroll
+    for (int idx = 0; idx < N; idx++) {
+        const int v = buf[idx];
+        const int step = idx == 0 ? e.dcQ : e.acQ;
+        const int a = abs(v), S = step << FB;   // dequantisation denominator 1 for these sizes
+        int l = 0;
+        if (a * 32 >= 21 * S) l = min((8 * a + 3 * S) / (8 * S), 16383);
+        const int qv = v < 0 ? -l : l;
+        qs[idx] = (int16_t)qv;
+        const int dq = l ? dequant<BD>(qv, step, 1) * (1 << FB) : 0;
+        const i64 df = (i64)(v - dq);
+        dist += df * df;
+        if (qv) eob = max(eob, isc[idx] + 1);
+    }
+    const uint16_t *scan = get_scan(e.T, txSz, e.txType);
+    int b = 0;
+    for (int c = 0; c < eob; c++) b += coeff_bits(c, eob, qs, scan, txSz, cls, e.plane > 0, e.dcCtx, e.T);
+    EvalOut o;
+    o.R = b + base_bits_inl(txSz, e, eob);
+    o.D = dist << dsh;
+    o.eob = eob;
+    return o;
+}
+
+template <int BD, int LW, int LH>
+__device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const RateTabs &T, int bs, int txSz, const uint8_t *tile, int x,
+                                          int y, int sbx, int sby, int tx0, int ty0, int tx1, int ty1) {
+    constexpr int W = 1 << LW, H = 1 << LH, N = W * H, NE = W + H;
+    constexpr int TW = MidSmem::TW;
+    const int tid = threadIdx.x;
+    const int haveL = x > tx0, haveA = y > ty0;
+    const int haveAR = ol_decoded(x + W, y - 1, x, y, tx0, ty0, tx1, ty1), haveBL = ol_decoded(x - 1, y + H, x, y, tx0, ty0, tx1, ty1);
+    const int lx = x - sbx + 16, ly = y - sby + 1;
+    const int mX = F.MiCols * 4 - 1 - sbx + 16, mY = F.MiRows * 4 - 1 - sby + 1;
+    uint8_t *A = S.edge[tid][0] + 1, *L = S.edge[tid][1] + 1;
+    build_edges<BD>(tile, TW, lx, ly, W, H, haveL, haveA, haveAR, haveBL, mX, mY, A, L, 0, 1);
+    int dcv;
+    {
+        int sa = 0, sl = 0;
+#pragma unroll
+        for (int k = 0; k < W; k++) sa += A[k];
+#pragma unroll
+        for (int k = 0; k < H; k++) sl += L[k];
+        if (haveL && haveA) dcv = (sa + sl + (NE >> 1)) / NE;
+        else if (haveL) dcv = min((sl + (H >> 1)) >> LH, (1 << BD) - 1);
+        else if (haveA) dcv = min((sa + (W >> 1)) >> LW, (1 << BD) - 1);
+        else dcv = 1 << (BD - 1);
+    }
+    const uint8_t *src = tile + ly * TW + lx;
+    const uint16_t *C = T.cost;
+    auto mbits = [&](int c) -> int {
+        const int m = cand_mode(c);
+        int b = c_avgY[m];
+        if (is_dir(m)) b += C[ci_angle(m - AV1G_V_PRED) + cand_delta(c) + 3];
+        return b;
+    };
+    const bool hasC = has_chroma(bs, y >> 2, x >> 2, F.ssx);
+    const int overhead = (hasC ? UV_OVERHEAD : 0) + c_avgSkip0;
+    const uint8_t(*iscan)[64] = S.iscan;
+    int16_t *qs = S.q[tid];
+    i64 topJ[4] = {INF, INF, INF, INF};
+    int topC[4] = {0, 0, 0, 0};
+    i64 dJ0 = INF, dJ1 = INF;
+    int b0 = AV1G_V_PRED, b1 = AV1G_V_PRED;
+    i64 bestJ = INF;
+    int bestK = 0, bestTx = AV1G_DCT_DCT, winC = 0;
+    // jobs: 0-12 the 13 modes, 13-24 the deltas of the two best directional modes (SATD); 25-28 the top 4 with
+    // DCT_DCT, 29-34 the other types of TX_SET_INTRA_1 for the winner (RD)
+#pragma unroll 1
+    for (int job = 0; job < 35; job++) {
+        int c, t = AV1G_DCT_DCT;
+        if (job < 13) {
+            c = cand_pack(job, 0);
+        } else if (job < 25) {
+            const int k = job - 13, kk = k % 6;
+            c = cand_pack(k < 6 ? b0 : b1, kk < 3 ? -(kk + 1) : kk - 2);
+        } else if (job < 29) {
+            const int k = job - 25;
+            c = topC[0];
+#pragma unroll
+            for (int s = 1; s < 4; s++) if (k == s) c = topC[s];
+        } else {
+            c = winC;
+            const int k = job - 29;   // ADST_DCT, DCT_ADST, ADST_ADST, IDTX, V_DCT, H_DCT
+            t = k < 3 ? k + 1 : k + 6;
+        }
+        const int m = cand_mode(c), pa = pangle(m, cand_delta(c));
+        // the prediction, one 4x4 sub-block at a time (one copy of the predictor): SATD of the residual while screening,
+        // the prediction into the thread's slot for an RD task
+        int satd = 0;
+#pragma unroll 1
+        for (int k = 0; k < N / 16; k++) {
+            const int sy = (k >> (LW - 2)) * 4, sx = (k & ((W >> 2) - 1)) * 4;
+            int p[16];
+            pred4_inl(m, pa, sy, sx, LW, LH, A, L, dcv, p);
+            if (job < 25) {
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) p[i * 4 + j] = (int)src[(sy + i) * TW + sx + j] - p[i * 4 + j];
+                satd += hadamard4_sum(p);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) qs[(sy + i) * W + sx + j] = (int16_t)p[i * 4 + j];
+            }
+        }
+        if (job < 25) {
+            const i64 js = ((i64)satd << 14) + F.sqlam * mbits(c);
+            const int pos = (topJ[0] <= js) + (topJ[1] <= js) + (topJ[2] <= js) + (topJ[3] <= js);
+#pragma unroll
+            for (int s = 3; s >= 0; s--) {
+                if (s > pos) { topJ[s] = topJ[s > 0 ? s - 1 : 0]; topC[s] = topC[s > 0 ? s - 1 : 0]; }
+                else if (s == pos) { topJ[s] = js; topC[s] = c; }
+            }
+            if (job >= AV1G_V_PRED && job <= AV1G_D67_PRED) {   // the two best directional modes (first of equals)
+                if (js < dJ0) { dJ1 = dJ0; b1 = b0; dJ0 = js; b0 = job; }
+                else if (js < dJ1) { dJ1 = js; b1 = job; }
+            }
+        } else {
+            int res[N];
+#pragma unroll
+            for (int i = 0; i < H; i++)
+#pragma unroll
+                for (int j = 0; j < W; j++) res[i * W + j] = (int)src[i * TW + j] - qs[i * W + j];
+            const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, T};
+            const EvalOut o = mid_eval<BD, LW, LH>(txSz, res, e, iscan, qs);
+            const i64 J = o.D + F.lam * (o.R + mbits(c) + overhead);
+            if (J < bestJ) {
+                bestJ = J;
+                if (job < 29) { bestK = job - 25; winC = c; }
+                else bestTx = t;
+            }
+        }
+    }
+    BlockRes r;
+    r.J = bestJ;
+    r.tx = (uint8_t)bestTx;
+    r.cand[0] = (uint8_t)winC;
+    int n = 1;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (k != bestK) r.cand[n++ & 3] = (uint8_t)topC[k];
+    r.ncand = 4;
+    r.pad[0] = r.pad[1] = 0;
+    F.blk[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] = r;
+}
+
+// grid: 3 x ceil(nSb / MID_SBS) CTAs, shape-major (8x8, then 4x16, then 16x4)
+template <int BD>
+__global__ void __launch_bounds__(MID_THREADS, 2) k_analysis_mid(const __grid_constant__ FrameDesc F) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MidSmem &S = *reinterpret_cast<MidSmem *>(smem_raw);
+    const int nSb = F.sbCols * F.sbRows, groups = (nSb + MID_SBS - 1) / MID_SBS;
+    const int shape = blockIdx.x / groups, sb0 = (blockIdx.x % groups) * MID_SBS;
+    const int tid = threadIdx.x;
+    const int txSz = shape == 0 ? AV1G_TX_8X8 : shape == 1 ? AV1G_TX_4X16 : AV1G_TX_16X4;
+    constexpr int V = MidSmem::TW / 16;
+    for (int k = tid; k < MID_SBS * MidSmem::TH * V; k += MID_THREADS) {
+        const int u = k / (MidSmem::TH * V), r = (k / V) % MidSmem::TH, c = k % V, sb = sb0 + u;
+        if (sb >= nSb) continue;
+        const int sbx = (sb % F.sbCols) * 64, sby = (sb / F.sbCols) * 64;
+        const uint8_t *s0 = F.src[0] + (size_t)(sby - 1) * F.spitch[0] + (sbx - 16);
+        reinterpret_cast<uint4 *>(S.tile[u] + r * MidSmem::TW)[c] = __ldg(reinterpret_cast<const uint4 *>(s0 + (size_t)r * F.spitch[0]) + c);
+    }
+    const RateTabs T = rate_tabs_stage(S.T, F.qctx, tid, MID_THREADS);
+    __syncthreads();
+    for (int k = tid; k < 3 * 64; k += MID_THREADS) {
+        const int cls = k / 64, c = k % 64;
+        S.iscan[cls][T.scan[c_scanOff[txSz][cls] + c]] = (uint8_t)c;
+    }
+    __syncthreads();
+    const int u = tid >> 6, b = tid & 63, sb = sb0 + u;
+    if (sb >= nSb) return;
+    const int sbx = (sb % F.sbCols) * 64, sby = (sb / F.sbCols) * 64;
+    int tc = 0, tr = 0;
+    while (tc + 1 < F.tileCols && sbx >= F.tileColStart[tc + 1] * 4) tc++;
+    while (tr + 1 < F.tileRows && sby >= F.tileRowStart[tr + 1] * 4) tr++;
+    const int tx0 = F.tileColStart[tc] * 4, tx1 = F.tileColStart[tc + 1] * 4, ty0 = F.tileRowStart[tr] * 4, ty1 = F.tileRowStart[tr + 1] * 4;
+    const int FW = F.MiCols * 4, FH = F.MiRows * 4;
+    if (shape == 0) {          // 8x8: 8 columns x 8 rows
+        const int x = sbx + (b & 7) * 8, y = sby + (b >> 3) * 8;
+        if (x < FW && y < FH) mid_block<BD, 3, 3>(F, S, T, AV1G_BLOCK_8X8, AV1G_TX_8X8, S.tile[u], x, y, sbx, sby, tx0, ty0, tx1, ty1);
+    } else if (shape == 1) {   // 4x16: 16 columns x 4 rows
+        const int x = sbx + (b & 15) * 4, y = sby + (b >> 4) * 16;
+        if (x < FW && y < FH) mid_block<BD, 2, 4>(F, S, T, AV1G_BLOCK_4X16, AV1G_TX_4X16, S.tile[u], x, y, sbx, sby, tx0, ty0, tx1, ty1);
+    } else {                   // 16x4: 4 columns x 16 rows
+        const int x = sbx + (b & 3) * 16, y = sby + (b >> 2) * 4;
+        if (x < FW && y < FH) mid_block<BD, 4, 2>(F, S, T, AV1G_BLOCK_16X4, AV1G_TX_16X4, S.tile[u], x, y, sbx, sby, tx0, ty0, tx1, ty1);
     }
 }
 
