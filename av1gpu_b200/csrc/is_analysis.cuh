@@ -25,6 +25,10 @@ constexpr int AN_BUF_INTS = 1088;             // evaluation scratch per warp: 32
 constexpr int ANB_BUF_INTS = 64 * 65;
 __constant__ uint8_t c_anTask[AN_TASKS][3];   // (bsize, x4, y4) largest area first, then shape, then raster
 __constant__ uint8_t c_anTaskBig[ANB_TASKS][3];
+// Each CTA runs the blocks of ONE shape of one SB (grid: shapes x SBs, shape-major), so that the warps of an SM work
+// through the same code; the task ranges of the shapes in the lists above:
+constexpr int AN_SHAPES = 8, ANB_SHAPES = 5;
+__constant__ int c_anShapeStart[AN_SHAPES + 1], c_anShapeStartBig[ANB_SHAPES + 1];
 
 template <typename Px, int BUFI> struct AnWarp {
     int32_t buf[BUFI];
@@ -206,9 +210,11 @@ __device__ __forceinline__ void an_sb(const FrameDesc &F, unsigned char *smem_ra
     typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
     typedef AnSmem<Px, NW, BUFI> Sm;
     Sm &S = *reinterpret_cast<Sm *>(smem_raw);
-    const int sb = blockIdx.x, sbr = sb / F.sbCols, sbc = sb % F.sbCols;
+    const int nSb = F.sbCols * F.sbRows, shape = blockIdx.x / nSb, sb = blockIdx.x % nSb;
+    const int sbr = sb / F.sbCols, sbc = sb % F.sbCols;
     const int sbx = sbc * 64, sby = sbr * 64;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int t0 = BIG ? c_anShapeStartBig[shape] : c_anShapeStart[shape], t1 = BIG ? c_anShapeStartBig[shape + 1] : c_anShapeStart[shape + 1];
     {   // the SB tile with 128-bit loads (rows and the tile's first column are 16-byte aligned by the layout)
         constexpr int V = Sm::TW * (int)sizeof(Px) / 16;
         const Px *s0 = (const Px *)F.src[0] + (size_t)(sby - 1) * F.spitch[0] + (sbx - 16);
@@ -216,7 +222,7 @@ __device__ __forceinline__ void an_sb(const FrameDesc &F, unsigned char *smem_ra
             const int r = k / V, c = k % V;
             reinterpret_cast<uint4 *>(S.tile + r * Sm::TW)[c] = __ldg(reinterpret_cast<const uint4 *>(s0 + (size_t)r * F.spitch[0]) + c);
         }
-        if (tid == 0) S.next = NW;
+        if (tid == 0) S.next = t0 + NW;
     }
     __syncthreads();
     int tc = 0, tr = 0;
@@ -224,9 +230,8 @@ __device__ __forceinline__ void an_sb(const FrameDesc &F, unsigned char *smem_ra
     while (tr + 1 < F.tileRows && sby >= F.tileRowStart[tr + 1] * 4) tr++;
     const int tx0 = F.tileColStart[tc] * 4, tx1 = F.tileColStart[tc + 1] * 4, ty0 = F.tileRowStart[tr] * 4, ty1 = F.tileRowStart[tr + 1] * 4;
     const int FW = F.MiCols * 4, FH = F.MiRows * 4;
-    constexpr int NT = BIG ? ANB_TASKS : AN_TASKS;
-    int t = warp;
-    while (t < NT) {
+    int t = t0 + warp;
+    while (t < t1) {
         const uint8_t *tk = BIG ? c_anTaskBig[t] : c_anTask[t];
         const int bs = tk[0], x = sbx + tk[1] * 4, y = sby + tk[2] * 4;
         if (x < FW && y < FH) an_block<BD, Px, BUFI>(F, S.tile, S.w[warp], bs, x, y, sbx, sby, tx0, ty0, tx1, ty1);

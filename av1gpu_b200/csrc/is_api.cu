@@ -279,9 +279,21 @@ int upload_tables(int dev) {
         }
         if (kDr23 != AV1G_T(Dr_Intra_Derivative)[23] || kDr45 != AV1G_T(Dr_Intra_Derivative)[45] || kDr67 != AV1G_T(Dr_Intra_Derivative)[67]) e = cudaErrorInvalidValue;
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_baseCtx, &AV1G_T(Coeff_Base_Ctx_Offset)[0][0][0], 19 * 25);
-        if (e == cudaSuccess && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3) {
+        // where each shape's tasks start in the two lists
+        auto starts = [](const std::vector<uint8_t> &t, int n, int *out) {
+            int k = 0;
+            for (size_t i = 0; i < t.size() / 3; i++)
+                if (i == 0 || t[3 * i] != t[3 * i - 3]) { if (k < n) out[k] = (int)i; k++; }
+            out[n] = (int)(t.size() / 3);
+            return k == n;
+        };
+        int st[AN_SHAPES + 1], stBig[ANB_SHAPES + 1];
+        const bool okShapes = starts(tasks, AN_SHAPES, st) && starts(tasksBig, ANB_SHAPES, stBig);
+        if (e == cudaSuccess && okShapes && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3) {
             e = cudaMemcpyToSymbol(c_anTask, tasks.data(), tasks.size());
             if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anTaskBig, tasksBig.data(), tasksBig.size());
+            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStart, st, sizeof st);
+            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStartBig, stBig, sizeof stBig);
         } else if (e == cudaSuccess) {
             e = cudaErrorInvalidValue;
         }
@@ -494,8 +506,8 @@ static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) 
     IS_CK(cudaMemsetAsync(F.queue, 0, 16, st));
     IS_CK(cudaMemsetAsync(F.err, 0, 4, st));
     IS_CK(cudaEventRecord(h->ev[1], st));
-    k_analysis_big<8><<<nSb, ANB_WARPS * 32, h->smemAnBig, st>>>(h->F);
-    k_analysis<8><<<nSb, AN_WARPS * 32, h->smemAn, st>>>(h->F);
+    k_analysis_big<8><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig, st>>>(h->F);
+    k_analysis<8><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn, st>>>(h->F);
     k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem), st>>>(h->F);
     k_analysis_mid<8><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem), st>>>(h->F);
     IS_CK(cudaGetLastError());
