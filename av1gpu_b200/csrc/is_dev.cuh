@@ -84,12 +84,14 @@ struct RateTabs {
     const uint16_t *cost, *scan;
     const uint8_t *baseCtx;                    // [19][5][5]
 };
-struct RateStage {
+struct __align__(16) RateStage {
     uint16_t cost[NCDF];
     uint16_t scan[SCAN_PACK];
     uint8_t baseCtx[19 * 25];
-    uint8_t pad[13];
+    uint8_t pad[5];
 };
+// staged with 16-byte vector stores (cost, scan) and followed by 16-byte-aligned buffers in the kernels' shared memory
+static_assert(sizeof(RateStage) % 16 == 0 && (NCDF * 2) % 16 == 0 && (SCAN_PACK * 2) % 16 == 0, "RateStage layout");
 __device__ __forceinline__ RateTabs rate_tabs_global(int qctx) { return RateTabs{g_cost[qctx], g_scanPack, g_baseCtx}; }
 // all threads of the CTA; followed by __syncthreads() at the caller
 __device__ __forceinline__ RateTabs rate_tabs_stage(RateStage &T, int qctx, int tid, int nt) {

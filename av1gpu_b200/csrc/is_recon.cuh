@@ -35,6 +35,8 @@ template <typename Px> struct RcWarp {
     i64 taskJ[8];
     int predC[8];
     Px ea[3][EDGE_LEN], el[3][EDGE_LEN];
+    __align__(16) Px srcS[3][1024];   // the source of the leaf's tx blocks (Y, U, V) when <= 32 x 32, staged once per
+                                      // leaf with 16-byte vector stores
     int16_t cfl[256];
     int satd[32];
     int cand[32];
@@ -44,6 +46,8 @@ template <typename Px> struct RcSmem {
     RateStage T;
     RcWarp<Px> w[RC_WARPS];
 };
+static_assert(offsetof(RcWarp<uint8_t>, srcS) % 16 == 0 && sizeof(RcWarp<uint8_t>) % 16 == 0 && offsetof(RcSmem<uint8_t>, w) % 16 == 0,
+              "the staged sources take 16-byte vector stores");
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
     int v;
@@ -146,18 +150,28 @@ __device__ int rc_record(const FrameDesc &F, const RateTabs &T, int sb, int plan
 }
 
 // txb skip / dc-sign contexts from the 4x4 maps (spec get_tx_size_context and the reference's txb_ctx,
-// k_recon.cuh:204-238): lane k reads above entry k and left entry k (w4, h4 <= 16)
-__device__ __forceinline__ void rc_txb_ctx(const FrameDesc &F, int plane, int txSz, int x4, int y4, int bsize, int tileX4, int tileY4,
-                                           int *skipCtx, int *dcCtx) {
+// k_recon.cuh:204-238): lane k reads above entry k and left entry k (w4, h4 <= 16).  Split into the loads (issued with
+// the other loads of a leaf) and the reduction.
+struct CtxLd { int la, da, ll, dl; };
+__device__ __forceinline__ CtxLd rc_txb_ctx_load(const FrameDesc &F, int plane, int txSz, int x4, int y4, int tileX4, int tileY4) {
     const int lane = lane_id();
     const int ss = plane ? F.ssx : 0;
     const int stride = F.MiCols >> ss, maxX4 = F.MiCols >> ss, maxY4 = F.MiRows >> ss;
     const bool hasAbove = y4 > (tileY4 >> ss), hasLeft = x4 > (tileX4 >> ss);
-    const int w = txw(txSz), h = txh(txSz), w4 = w >> 2, h4 = h >> 2;
+    const int w4 = txw(txSz) >> 2, h4 = txh(txSz) >> 2;
     const bool a = hasAbove && lane < w4 && x4 + lane < maxX4, l = hasLeft && lane < h4 && y4 + lane < maxY4;
     const uint8_t *Lv = F.cLvl[plane], *Dc = F.cDc[plane];
-    const int la = a ? __ldcg(Lv + (size_t)(y4 - 1) * stride + x4 + lane) : 0, da = a ? __ldcg(Dc + (size_t)(y4 - 1) * stride + x4 + lane) : 0;
-    const int ll = l ? __ldcg(Lv + (size_t)(y4 + lane) * stride + x4 - 1) : 0, dl = l ? __ldcg(Dc + (size_t)(y4 + lane) * stride + x4 - 1) : 0;
+    CtxLd c;
+    c.la = a ? __ldcg(Lv + (size_t)(y4 - 1) * stride + x4 + lane) : 0;
+    c.da = a ? __ldcg(Dc + (size_t)(y4 - 1) * stride + x4 + lane) : 0;
+    c.ll = l ? __ldcg(Lv + (size_t)(y4 + lane) * stride + x4 - 1) : 0;
+    c.dl = l ? __ldcg(Dc + (size_t)(y4 + lane) * stride + x4 - 1) : 0;
+    return c;
+}
+__device__ __forceinline__ void rc_txb_ctx_finish(const FrameDesc &F, const CtxLd &c, int plane, int txSz, int bsize, int *skipCtx, int *dcCtx) {
+    const int ss = plane ? F.ssx : 0;
+    const int w = txw(txSz), h = txh(txSz);
+    const int la = c.la, da = c.da, ll = c.ll, dl = c.dl;
     const bool nzA = __any_sync(0xffffffffu, plane ? (la | da) != 0 : la != 0);
     const bool nzL = __any_sync(0xffffffffu, plane ? (ll | dl) != 0 : ll != 0);
     const int dcSign = warp_sum((da == 2) - (da == 1) + (dl == 2) - (dl == 1));
@@ -173,6 +187,26 @@ __device__ __forceinline__ void rc_txb_ctx(const FrameDesc &F, int plane, int tx
     } else {
         const int ub = uv_bsize(bsize, ss);
         *skipCtx = (int)nzA + (int)nzL + 7 + ((16 * bw4(ub) * bh4(ub) > w * h) ? 3 : 0);
+    }
+}
+__device__ __forceinline__ void rc_txb_ctx(const FrameDesc &F, int plane, int txSz, int x4, int y4, int bsize, int tileX4, int tileY4,
+                                           int *skipCtx, int *dcCtx) {
+    const CtxLd c = rc_txb_ctx_load(F, plane, txSz, x4, y4, tileX4, tileY4);
+    rc_txb_ctx_finish(F, c, plane, txSz, bsize, skipCtx, dcCtx);
+}
+
+// a W x H (<= 32 x 32) block of 8-bit samples at (x, y) of a plane into dst (row stride W), vector loads of up to 16
+// bytes (rows and x are aligned to the block width)
+__device__ __forceinline__ void stage_block(const uint8_t *src, int pitch, int W, int H, uint8_t *dst) {
+    const int lane = lane_id();
+    if (W >= 16) {
+        const int v = W >> 4;
+        for (int k = lane; k < v * H; k += 32)
+            reinterpret_cast<uint4 *>(dst)[k] = __ldg(reinterpret_cast<const uint4 *>(src + (size_t)(k / v) * pitch) + (k % v));
+    } else if (W == 8) {
+        for (int k = lane; k < H; k += 32) reinterpret_cast<uint2 *>(dst)[k] = __ldg(reinterpret_cast<const uint2 *>(src + (size_t)k * pitch));
+    } else {
+        for (int k = lane; k < H; k += 32) reinterpret_cast<uint32_t *>(dst)[k] = __ldg(reinterpret_cast<const uint32_t *>(src + (size_t)k * pitch));
     }
 }
 
@@ -277,7 +311,11 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
     const int availUC = (ss && bh == 1) ? (mi_row - 2 >= tR0) : availU;
     const int availLC = (ss && bw == 1) ? (mi_col - 2 >= tC0) : availL;
     const uint16_t *C = T.cost;
-    const int txbBase = F.leafTxb[(size_t)sb * SB_MAX_LEAVES + li], coefBase = F.leafCoef[(size_t)sb * SB_MAX_LEAVES + li];
+    const uint32_t me = (uint32_t)sb * SB_MAX_LEAVES + li;
+    const int txbBase = F.leafTxb[me], coefBase = F.leafCoef[me];
+    // the leaf's dependents (prefetched here, used when its luma is published)
+    const int relN = F.revCnt[me];
+    const uint32_t relOff = F.revOff[me];
     // BlockDecoded of a 4x4 unit (SB-relative, plane units; ps = 0 luma, ss chroma) for this leaf
     auto decoded = [&](int ps, int yy, int xx) -> bool {
         const int sz = 16 >> ps;
@@ -293,23 +331,60 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
     {
         const int txSz = ST(Max_Tx_Size_Rect)[bsize];
         const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
+        // ---- the luma's global loads, issued together (one round of memory latency): the raw edge samples up to the
+        //      longest reach, the analysis record, the neighbours' y modes, the coefficient-context maps, the
+        //      decoded-ness of the above-right / below-left units, the source block ----
+        const Px *recY = (const Px *)F.rec[0];
+        const int rp = F.rpitch[0], n = W + H;
+        const int aLim = min(x + 2 * W - 1, F.MiCols * 4 - 1), lLim = min(y + 2 * H - 1, F.MiRows * 4 - 1);
+        Px ra[4], rl[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int i = lane + 32 * k;
+            ra[k] = i < n ? ldcg(recY + (size_t)(y - 1) * rp + min(x + i, aLim)) : (Px)0;
+            rl[k] = i < n ? ldcg(recY + (size_t)min(y + i, lLim) * rp + x - 1) : (Px)0;
+        }
+        const Px rcorner = ldcg(recY + (size_t)(y - 1) * rp + x - 1);
+        const BlockRes br = F.blk[F.shOff[bsize] + (uint32_t)(y / H) * F.shNbx[bsize] + x / W];
+        const int ymA = availU ? __ldcg(F.mYMode + (size_t)(mi_row - 1) * F.MiCols + mi_col) : AV1G_DC_PRED;
+        const int ymL = availL ? __ldcg(F.mYMode + (size_t)mi_row * F.MiCols + mi_col - 1) : AV1G_DC_PRED;
+        const CtxLd cl = rc_txb_ctx_load(F, 0, txSz, x >> 2, y >> 2, tC0, tR0);
         const int haveAR = decoded(0, lf.y4 - 1, lf.x4 + (W >> 2)), haveBL = decoded(0, lf.y4 + (H >> 2), lf.x4 - 1);
+        const bool staged = W <= 32 && H <= 32;
+        if (staged) stage_block((const uint8_t *)F.src[0] + (size_t)y * F.spitch[0] + x, F.spitch[0], W, H, (uint8_t *)Wp.srcS[0]);
+        // ---- the edges: rec_edges' rule (availability, above-right / below-left reach, frame clamp) on the raw samples ----
         Px *A = Wp.ea[0] + EDGE_OFF, *L = Wp.el[0] + EDGE_OFF;
-        rec_edges<BD>((const Px *)F.rec[0], F.rpitch[0], x, y, W, H, availL, availU, haveAR, haveBL, F.MiCols * 4 - 1, F.MiRows * 4 - 1, A, L);
+        {
+            const Px aW = (Px)__shfl_sync(0xffffffffu, (int)(W > 32 ? ra[1] : ra[0]), (W - 1) & 31);
+            const Px lH = (Px)__shfl_sync(0xffffffffu, (int)(H > 32 ? rl[1] : rl[0]), (H - 1) & 31);
+            const Px a0 = (Px)__shfl_sync(0xffffffffu, (int)ra[0], 0), l0 = (Px)__shfl_sync(0xffffffffu, (int)rl[0], 0);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int i = lane + 32 * k;
+                if (i < n) {
+                    A[i] = availU ? ((!haveAR && i >= W) ? aW : ra[k]) : (availL ? l0 : (Px)((1 << (BD - 1)) - 1));
+                    L[i] = availL ? ((!haveBL && i >= H) ? lH : rl[k]) : (availU ? a0 : (Px)((1 << (BD - 1)) + 1));
+                }
+            }
+            if (lane == 0) {
+                const Px c = (availU && availL) ? rcorner : availU ? a0 : availL ? l0 : (Px)(1 << (BD - 1));
+                A[-1] = c;
+                L[-1] = c;
+            }
+        }
         __syncwarp();
         const int dcv = warp_dc<BD>(A, L, availL, availU, lw, lh);
-        const BlockRes br = F.blk[F.shOff[bsize] + (uint32_t)(y / H) * F.shNbx[bsize] + x / W];
         int skipCtx, dcCtx;
-        rc_txb_ctx(F, 0, txSz, x >> 2, y >> 2, bsize, tC0, tR0, &skipCtx, &dcCtx);
-        const int am = ST(Intra_Mode_Context)[availU ? __ldcg(F.mYMode + (size_t)(mi_row - 1) * F.MiCols + mi_col) : AV1G_DC_PRED];
-        const int lm = ST(Intra_Mode_Context)[availL ? __ldcg(F.mYMode + (size_t)mi_row * F.MiCols + mi_col - 1) : AV1G_DC_PRED];
+        rc_txb_ctx_finish(F, cl, 0, txSz, bsize, &skipCtx, &dcCtx);
+        const int am = ST(Intra_Mode_Context)[ymA], lm = ST(Intra_Mode_Context)[ymL];
         auto mbits = [&](int c) -> int {
             const int m = cand_mode(c);
             int b = C[ci_y_mode(am, lm) + m];
             if (bsize >= AV1G_BLOCK_8X8 && is_dir(m)) b += C[ci_angle(m - AV1G_V_PRED) + cand_delta(c) + 3];
             return b;
         };
-        const Px *src = (const Px *)F.src[0] + (size_t)y * F.spitch[0] + x;
+        const Px *src = staged ? (const Px *)Wp.srcS[0] : (const Px *)F.src[0] + (size_t)y * F.spitch[0] + x;
+        const int srcPitch = staged ? W : F.spitch[0];
         const int set = tx_set_intra(txSz);
         const int G = grp_size(txSz), ng = 32 / G, grp = lane / G, g = lane & (G - 1);
         const int nq = min(W, 32) * min(H, 32);
@@ -332,7 +407,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
                 __syncwarp();
                 if (g == 0) Wp.predC[grp] = c;
                 const EvalIn e{t, 0, skipCtx, dcCtx, m, F.dcQ, F.acQ, T};
-                const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{src, F.spitch[0], tp, lw, nullptr}, e, tb, tq, g, G);
+                const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{src, srcPitch, tp, lw, nullptr}, e, tb, tq, g, G);
                 if (g == 0 && r0 + grp < n) Wp.taskJ[grp] = o.D + F.lam * (o.R + mbits(c));
                 __syncwarp();
                 int win = -1;
@@ -367,7 +442,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
         __syncwarp();
         if (!have) {
             const EvalIn e{bestT, 0, skipCtx, dcCtx, bm, F.dcQ, F.acQ, T};
-            grp_eval<BD, Px>(txSz, ResFn<Px>{src, F.spitch[0], Wp.pred, lw, nullptr}, e, Wp.buf, best, lane, 32);
+            grp_eval<BD, Px>(txSz, ResFn<Px>{src, srcPitch, Wp.pred, lw, nullptr}, e, Wp.buf, best, lane, 32);
         }
         Px *dst = (Px *)F.rec[0] + (size_t)y * F.rpitch[0] + x;
         rc_reconstruct<BD, Px>(txSz, bestT, best, F.dcQ, F.acQ, Wp.pred, dst, F.rpitch[0], Wp.buf);
@@ -387,12 +462,9 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
         if (trace) trace[2] = gtimer();
     }
     {   // the dependents whose last luma dependency this was enter the ready queue
-        const uint32_t me = (uint32_t)sb * SB_MAX_LEAVES + li;
-        const int n = F.revCnt[me];
-        const uint32_t o = F.revOff[me];
         __threadfence();
-        for (int k = lane; k < n; k += 32) {
-            const uint32_t d = F.revList[o + k];
+        for (int k = lane; k < relN; k += 32) {
+            const uint32_t d = F.revList[relOff + k];
             if (atomicSub(F.depCnt + d, 1) == 1) {
                 __threadfence();
                 push_ready(F, d);
@@ -415,17 +487,55 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
         const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
         const int cx = (mi_col >> ss) * 4, cy = (mi_row >> ss) * 4, cx4 = cx >> 2, cy4 = cy >> 2;
         const int csr = (mi_row & 15) >> ss, csc = (mi_col & 15) >> ss;
+        // ---- the chroma's global loads, issued together: raw U / V edge samples up to the longest reach, the
+        //      coefficient-context maps, the decoded-ness of the above-right / below-left units, the U / V sources ----
+        const int n = W + H;   // <= 64
+        const int aLim = min(cx + 2 * W - 1, ((F.MiCols * 4) >> ss) - 1), lLim = min(cy + 2 * H - 1, ((F.MiRows * 4) >> ss) - 1);
+        Px ra[2][2], rl[2][2], rcorner[2];
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const Px *rp = (const Px *)F.rec[1 + q];
+            const int pitch = F.rpitch[1 + q];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int i = lane + 32 * k;
+                ra[q][k] = i < n ? ldcg(rp + (size_t)(cy - 1) * pitch + min(cx + i, aLim)) : (Px)0;
+                rl[q][k] = i < n ? ldcg(rp + (size_t)min(cy + i, lLim) * pitch + cx - 1) : (Px)0;
+            }
+            rcorner[q] = ldcg(rp + (size_t)(cy - 1) * pitch + cx - 1);
+        }
+        const CtxLd cl1 = rc_txb_ctx_load(F, 1, txSz, cx4, cy4, tC0, tR0), cl2 = rc_txb_ctx_load(F, 2, txSz, cx4, cy4, tC0, tR0);
         const int haveAR = decoded(ss, csr - 1, csc + (W >> 2)), haveBL = decoded(ss, csr + (H >> 2), csc - 1);
-        const int maxX = ((F.MiCols * 4) >> ss) - 1, maxY = ((F.MiRows * 4) >> ss) - 1;
+        stage_block((const uint8_t *)F.src[1] + (size_t)cy * F.spitch[1] + cx, F.spitch[1], W, H, (uint8_t *)Wp.srcS[1]);
+        stage_block((const uint8_t *)F.src[2] + (size_t)cy * F.spitch[2] + cx, F.spitch[2], W, H, (uint8_t *)Wp.srcS[2]);
+        // ---- the edges of U and V (rec_edges' rule on the raw samples) ----
         Px *A[3], *L[3];
         int dcv[3];
-        for (int pl = 1; pl <= 2; pl++) {
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int pl = 1 + q;
             A[pl] = Wp.ea[pl] + EDGE_OFF; L[pl] = Wp.el[pl] + EDGE_OFF;
-            rec_edges<BD>((const Px *)F.rec[pl], F.rpitch[pl], cx, cy, W, H, availLC, availUC, haveAR, haveBL, maxX, maxY, A[pl], L[pl]);
+            const Px aW = (Px)__shfl_sync(0xffffffffu, (int)(W > 32 ? ra[q][1] : ra[q][0]), (W - 1) & 31);
+            const Px lH = (Px)__shfl_sync(0xffffffffu, (int)(H > 32 ? rl[q][1] : rl[q][0]), (H - 1) & 31);
+            const Px a0 = (Px)__shfl_sync(0xffffffffu, (int)ra[q][0], 0), l0 = (Px)__shfl_sync(0xffffffffu, (int)rl[q][0], 0);
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int i = lane + 32 * k;
+                if (i < n) {
+                    A[pl][i] = availUC ? ((!haveAR && i >= W) ? aW : ra[q][k]) : (availLC ? l0 : (Px)((1 << (BD - 1)) - 1));
+                    L[pl][i] = availLC ? ((!haveBL && i >= H) ? lH : rl[q][k]) : (availUC ? a0 : (Px)((1 << (BD - 1)) + 1));
+                }
+            }
+            if (lane == 0) {
+                const Px c = (availUC && availLC) ? rcorner[q] : availUC ? a0 : availLC ? l0 : (Px)(1 << (BD - 1));
+                A[pl][-1] = c;
+                L[pl][-1] = c;
+            }
         }
         __syncwarp();
         for (int pl = 1; pl <= 2; pl++) dcv[pl] = warp_dc<BD>(A[pl], L[pl], availLC, availUC, lw, lh);
-        const Px *sP[3] = {nullptr, (const Px *)F.src[1] + (size_t)cy * F.spitch[1] + cx, (const Px *)F.src[2] + (size_t)cy * F.spitch[2] + cx};
+        // the staged sources (row stride W)
+        const Px *sP[3] = {nullptr, (const Px *)Wp.srcS[1], (const Px *)Wp.srcS[2]};
         const bool cflAllowed = bw <= 8 && bh <= 8;
         auto uvbits = [&](int m) -> int { return cflAllowed ? C[ci_uv_cfl(yMode) + m] : C[ci_uv_nocfl(yMode) + m]; };
         auto uvcbits = [&](int c) -> int {
@@ -461,8 +571,8 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
             for (int p = lane; p < W * H; p += 32) {
                 const int i = p >> lw, j = p & (W - 1);
                 const i64 l = Wp.cfl[p] - cflAvg;
-                num1 += l * ((int)sP[1][i * F.spitch[1] + j] - dcv[1]);
-                num2 += l * ((int)sP[2][i * F.spitch[2] + j] - dcv[2]);
+                num1 += l * ((int)sP[1][i * W + j] - dcv[1]);
+                num2 += l * ((int)sP[2][i * W + j] - dcv[2]);
                 den += l * l;
             }
             num1 = warp_sum64(num1); num2 = warp_sum64(num2); den = warp_sum64(den);
@@ -477,7 +587,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
                 i64 sse[3] = {0, 0, 0};
                 for (int p = lane; p < W * H; p += 32) {
                     const int i = p >> lw, j = p & (W - 1);
-                    const int l = Wp.cfl[p] - cflAvg, s = sP[pl][i * F.spitch[pl] + j];
+                    const int l = Wp.cfl[p] - cflAvg, s = sP[pl][i * W + j];
 #pragma unroll
                     for (int k = 0; k < 3; k++) {
                         const int ak = max(-16, min(16, a + k - 1));
@@ -509,7 +619,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
 #pragma unroll
                     for (int i = 0; i < 4; i++)
 #pragma unroll
-                        for (int j = 0; j < 4; j++) d[i * 4 + j] = (int)sP[pl][(sy + i) * F.spitch[pl] + sx + j] - d[i * 4 + j];
+                        for (int j = 0; j < 4; j++) d[i * 4 + j] = (int)sP[pl][(sy + i) * W + sx + j] - d[i * 4 + j];
                     t = hadamard4_sum(d);
                 }
                 for (int o = 16; o > 0; o >>= 1)
@@ -539,7 +649,8 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
         }
         if (cflAllowed && (alpha[1] || alpha[2])) chosen[nch++] = 255;
         int skipCtx[3], dcCtx[3];
-        for (int pl = 1; pl <= 2; pl++) rc_txb_ctx(F, pl, txSz, cx4, cy4, bsize, tC0, tR0, &skipCtx[pl], &dcCtx[pl]);
+        rc_txb_ctx_finish(F, cl1, 1, txSz, bsize, &skipCtx[1], &dcCtx[1]);
+        rc_txb_ctx_finish(F, cl2, 2, txSz, bsize, &skipCtx[2], &dcCtx[2]);
         // prediction of (plane, candidate) by a group of G lanes into out
         auto predict = [&](int pl, int c, Px *out, int g, int G) {
             if (c == 255) grp_predict_cfl(lw, lh, dcv[pl], Wp.cfl, alpha[pl], cflAvg, (1 << BD) - 1, out, g, G);
@@ -560,7 +671,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
             __syncwarp();
             const int txType = chroma_tx_type(txSz, c == 255 ? AV1G_UV_CFL_PRED : cand_mode(c));
             const EvalIn e{txType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, T};
-            const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{sP[pl], F.spitch[pl], tp, lw, nullptr}, e, tb, tq, g, G);
+            const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{sP[pl], W, tp, lw, nullptr}, e, tb, tq, g, G);
             if (g == 0 && r0 + grp < ntask) Wp.taskJ[grp] = o.D + F.lam * o.R;
             __syncwarp();
             for (int u = 0; u < ng && r0 + u < ntask; u++) pj[r0 + u] = Wp.taskJ[u];
@@ -592,7 +703,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
             __syncwarp();
             const EvalIn e{uvType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, T};
             int16_t *lv = Wp.qb[pl - 1];
-            grp_eval<BD, Px>(txSz, ResFn<Px>{sP[pl], F.spitch[pl], Wp.pred, lw, nullptr}, e, Wp.buf, lv, lane, 32);
+            grp_eval<BD, Px>(txSz, ResFn<Px>{sP[pl], W, Wp.pred, lw, nullptr}, e, Wp.buf, lv, lane, 32);
             Px *dst = (Px *)F.rec[pl] + (size_t)cy * F.rpitch[pl] + cx;
             rc_reconstruct<BD, Px>(txSz, uvType, lv, F.dcQ, F.acQ, Wp.pred, dst, F.rpitch[pl], Wp.buf);
             const int yt = ST(Max_Tx_Size_Rect)[bsize];

@@ -180,7 +180,7 @@ __device__ __forceinline__ int tcoeff_rate(const int *q, const uint8_t *iscan, i
 // ---- one evaluation by one thread (grp_eval's arithmetic for a 4- or 8-point tx size): forward transform of the
 // residual, dead-zone quantisation into q, transform-domain distortion, exact rate ----
 template <int BD, int LW, int LH>
-__device__ __forceinline__ EvalOut thr_eval(int txSz, const int *res, const EvalIn &e, const uint8_t (*iscan)[32], int *q) {
+__device__ __forceinline__ EvalOut thr_eval(int txSz, const int *res, const EvalIn &e, const uint8_t *iscan, int istride, int *q) {
     constexpr int W = 1 << LW, H = 1 << LH, N = W * H;
     const int rowShift = ST(Transform_Row_Shift)[txSz];
     constexpr int rect = (LW - LH == 1 || LH - LW == 1) ? 1 : 0;
@@ -212,7 +212,7 @@ __device__ __forceinline__ EvalOut thr_eval(int txSz, const int *res, const Eval
         }
     }
     const int cls = e.txType == AV1G_IDTX ? AV1G_TX_CLASS_2D : tx_class(e.txType);
-    const uint8_t *isc = iscan[cls];
+    const uint8_t *isc = iscan + cls * istride;
     i64 dist = 0;
     int eob = 0;
 #pragma unroll
@@ -346,13 +346,13 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
     // ---- RD: the top 4 with DCT_DCT, then the other types of the set for the winner (first of equal costs wins) ----
     const bool hasC = has_chroma(bs, y >> 2, x >> 2, F.ssx);
     const int overhead = (hasC ? UV_OVERHEAD : 0) + c_avgSkip0;
-    const uint8_t(*iscan)[32] = S.iscan[sizeIdx];
+    const uint8_t *iscan = &S.iscan[sizeIdx][0][0];
     auto rd = [&](const uint32_t *pw, int m, int t) -> i64 {
         int res[N], q[N];
 #pragma unroll
         for (int i = 0; i < N; i++) res[i] = src[i] - (int)((pw[i >> 2] >> (8 * (i & 3))) & 255);
         const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, T};
-        const EvalOut o = thr_eval<BD, LW, LH>(txSz, res, e, iscan, q);
+        const EvalOut o = thr_eval<BD, LW, LH>(txSz, res, e, iscan, 32, q);
         return o.D + F.lam * (o.R + c_avgY[m] + overhead);
     };
     i64 bestJ = INF;
@@ -490,7 +490,7 @@ __device__ __forceinline__ void thr_fwd(int txSz, int txType, const int *res, in
 // one evaluation of a <= 16-point-side block by one thread: transform in registers, levels to qs (shared memory),
 // rate by coeff_bits over the scan
 template <int BD, int LW, int LH>
-__device__ __forceinline__ EvalOut mid_eval(int txSz, const int *res, const EvalIn &e, const uint8_t (*iscan)[64], int16_t *qs) {
+__device__ __forceinline__ EvalOut mid_eval(int txSz, const int *res, const EvalIn &e, const uint8_t *iscan, int istride, int16_t *qs) {
     constexpr int W = 1 << LW, H = 1 << LH, N = W * H;
     int buf[N];
     thr_fwd<BD, LW, LH>(txSz, e.txType, res, buf);
@@ -498,7 +498,7 @@ __device__ __forceinline__ EvalOut mid_eval(int txSz, const int *res, const Eval
     constexpr int rect = (LW - LH == 1 || LH - LW == 1) ? 1 : 0;
     const int dsh = 16 - 2 * FB - (2 * (rowShift + 4) - (LW + LH - 2) + rect);
     const int cls = e.txType == AV1G_IDTX ? AV1G_TX_CLASS_2D : tx_class(e.txType);
-    const uint8_t *isc = iscan[cls];
+    const uint8_t *isc = iscan + cls * istride;
     i64 dist = 0;
     int eob = 0;
 #pragma unroll
@@ -559,7 +559,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
     };
     const bool hasC = has_chroma(bs, y >> 2, x >> 2, F.ssx);
     const int overhead = (hasC ? UV_OVERHEAD : 0) + c_avgSkip0;
-    const uint8_t(*iscan)[64] = S.iscan;
+    const uint8_t *iscan = &S.iscan[0][0];
     int16_t *qs = S.q[tid];
     i64 topJ[4] = {INF, INF, INF, INF};
     int topC[4] = {0, 0, 0, 0};
@@ -628,7 +628,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
 #pragma unroll
                 for (int j = 0; j < W; j++) res[i * W + j] = (int)src[i * TW + j] - qs[i * W + j];
             const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, T};
-            const EvalOut o = mid_eval<BD, LW, LH>(txSz, res, e, iscan, qs);
+            const EvalOut o = mid_eval<BD, LW, LH>(txSz, res, e, iscan, 64, qs);
             const i64 J = o.D + F.lam * (o.R + mbits(c) + overhead);
             if (J < bestJ) {
                 bestJ = J;
