@@ -68,5 +68,18 @@ def cpu_baseline(planes, qindex, crop=(2000, 1500), min_seconds=10.0):
         O.encode(sub, qindex, threads=threads)
         n += 1
     dt = (time.perf_counter() - t0) / n
-    return {"value": round(cw * ch / 1e6 / dt, 4), "unit": "MP/s", "cores": threads, "kind": "port",
-            "sample": "%dx%d crop of the 12 MP image, %d searches, %.2f s each" % (cw, ch, n, dt)}
+    out = {"value": round(cw * ch / 1e6 / dt, 4), "unit": "MP/s", "cores": threads, "kind": "port",
+           "sample": "%dx%d crop of the 12 MP image, %d searches, %.2f s each" % (cw, ch, n, dt)}
+    # beside it, on the same crop: the reference's own CPU decision engine (a simpler search, at most 4 decide threads)
+    # and av1core's av1g_encode of the oracle's record (entropy coding and reconstruction, outside the search)
+    try:
+        dec, enc = O.ref_engine_seconds(sub, qindex)
+        r = O.encode(sub, qindex, threads=threads)
+        t1 = time.perf_counter()
+        O.av1g_recon(cw, ch, qindex, r.blocks, r.block_txb, r.txb, r.coeffs)
+        out["reference_cpu_engine"] = {"decide_s": round(dec, 3), "encode_s": round(enc, 3),
+                                       "mp_per_s": round(cw * ch / 1e6 / max(dec, 1e-9), 3)}
+        out["av1g_encode_s"] = round(time.perf_counter() - t1, 3)
+    except (RuntimeError, OSError) as ex:
+        out["reference_cpu_engine"] = {"error": str(ex)[:120]}
+    return out
