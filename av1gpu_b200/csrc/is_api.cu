@@ -195,7 +195,6 @@ struct is_handle {
     size_t arenaBytes = 0;
     FrameDesc F;                 // the descriptor (device pointers), passed by value to every kernel
     int nSb = 0;
-    int geomW = -1, geomH = -1;
     size_t smemAn = 0, smemAnBig = 0, smemRc = 0;
     // last result
     bool have = false;
@@ -207,7 +206,31 @@ struct is_handle {
     unsigned long long *traceBuf = nullptr;
     size_t traceCap = 0;
     cudaEvent_t ev[6];
-    void *hostSmall = nullptr;   // pinned 64 bytes for the counts / error readback
+    void *hostSmall = nullptr;   // pinned 64 bytes (unused by the batch path; kept for the test entry points)
+    // ---- batch state: every encode is a batch (a single image is a batch of one); F / nSb / qidx above mirror
+    //      image 0 of the last batch ----
+    int bN = 0;
+    std::vector<FrameDesc> bF;
+    std::vector<int> bNsb, bQ;
+    std::vector<uint32_t> bNb, bNt;
+    std::vector<uint64_t> bNc;
+    size_t bSlots = 0;                      // ready-queue slots (sum over images of SBs x 256)
+    FrameDesc *dFs = nullptr;               // the descriptors in device memory (for the closed loop)
+    FrameDesc *hFs = nullptr;               // pinned staging of the descriptors
+    size_t hFsCap = 0;
+    uint32_t *hOrd = nullptr;               // pinned staging of every image's wavefront and decode orders
+    size_t hOrdCap = 0;
+    uint32_t *hCnt = nullptr;               // pinned readback: per image n_blocks, n_txb, n_coeffs (2 words), + err
+    size_t hCntCap = 0;
+    unsigned long long *bReadyQ = nullptr;
+    int *bRq = nullptr, *bErr = nullptr;
+    // multi-stream front end (upload, analysis, DP, dataflow graph of each image) and CUDA graph replay
+    cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t evFork = nullptr, evJoin[4] = {nullptr, nullptr, nullptr, nullptr};
+    int frontStreams = 1;                   // 1, 2 or 4 (is_autotune_batch chooses)
+    bool useGraph = false;
+    std::string graphKey;
+    cudaGraphExec_t graphExec = nullptr;
     int setErr(int code, const char *fmt, ...) {
         char b[512];
         va_list ap;
@@ -352,7 +375,6 @@ size_t layout(int W, int H, uint8_t *base, FrameDesc &F, int &nSb) {
     F.leafCoef = (uint16_t *)take((size_t)nSb * SB_MAX_LEAVES * 2);
     F.leafDone = (int *)take((size_t)nSb * SB_MAX_LEAVES * 4);
     F.leafStart = (uint32_t *)take((size_t)nSb * 4);
-    F.leafQueue = (uint32_t *)take((size_t)nSb * SB_MAX_LEAVES * 4);
     F.leafTotal = (uint32_t *)take(4);
     F.leafTrace = nullptr;   // set per encode when tracing is on (is_set_trace)
     F.queue = (int *)take(16);
@@ -406,6 +428,11 @@ int is_create(const is_params *p, is_handle **out) {
     for (auto &e : h->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return fail(IS_ERR_CUDA);
     if (cudaMallocHost(&h->hostSmall, 64) != cudaSuccess) return fail(IS_ERR_OOM);
+    for (int k = 0; k < 4; k++) {
+        if (cudaStreamCreateWithFlags(&h->aux[k], cudaStreamNonBlocking) != cudaSuccess) return fail(IS_ERR_CUDA);
+        if (cudaEventCreateWithFlags(&h->evJoin[k], cudaEventDisableTiming) != cudaSuccess) return fail(IS_ERR_CUDA);
+    }
+    if (cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming) != cudaSuccess) return fail(IS_ERR_CUDA);
     memset(&h->times, 0, sizeof h->times);
     *out = h;
     return IS_OK;
@@ -421,135 +448,309 @@ void is_destroy(is_handle *h) {
     if (h->own) cudaStreamDestroy(h->own);
     if (h->hostSmall) cudaFreeHost(h->hostSmall);
     if (h->traceBuf) cudaFree(h->traceBuf);
+    if (h->graphExec) cudaGraphExecDestroy(h->graphExec);
+    for (int k = 0; k < 4; k++) {
+        if (h->aux[k]) { cudaStreamSynchronize(h->aux[k]); cudaStreamDestroy(h->aux[k]); }
+        if (h->evJoin[k]) cudaEventDestroy(h->evJoin[k]);
+    }
+    if (h->evFork) cudaEventDestroy(h->evFork);
+    if (h->hFs) cudaFreeHost(h->hFs);
+    if (h->hOrd) cudaFreeHost(h->hOrd);
+    if (h->hCnt) cudaFreeHost(h->hCnt);
     delete h;
 }
 
 const char *is_last_error(const is_handle *h) { return h ? h->err.c_str() : "null handle"; }
 
-static int prepare(is_handle *h, const is_frame *f) {
-    if (!f || f->width < 1 || f->height < 1 || f->width > 16384 || f->height > 16384 || f->qindex < 1 || f->qindex > 255)
-        return h->setErr(IS_ERR_INVALID, "invalid frame (size %dx%d, qindex %d)", f ? f->width : 0, f ? f->height : 0, f ? f->qindex : 0);
-    FrameDesc F;
-    memset(&F, 0, sizeof F);
-    int nSb = 0;
-    const size_t need = layout(f->width, f->height, nullptr, F, nSb);
+// the wavefront order (SBs by tile-local step c + 2 r) and the decode order (tiles raster, SBs raster) of an image
+static void sb_orders(const FrameDesc &F, const std::vector<int> &cs, const std::vector<int> &rs, uint32_t *order, uint32_t *dec) {
+    struct J { uint32_t sb; int step; };
+    std::vector<J> js;
+    size_t nd = 0;
+    for (int tr = 0; tr < F.tileRows; tr++)
+        for (int tc = 0; tc < F.tileCols; tc++) {
+            const int r0 = rs[tr] >> 4, r1 = (rs[tr + 1] + 15) >> 4, c0 = cs[tc] >> 4, c1 = (cs[tc + 1] + 15) >> 4;
+            for (int r = r0; r < r1; r++)
+                for (int c = c0; c < c1; c++) {
+                    js.push_back(J{(uint32_t)(r * F.sbCols + c), (c - c0) + 2 * (r - r0)});
+                    dec[nd++] = (uint32_t)(r * F.sbCols + c);
+                }
+        }
+    std::stable_sort(js.begin(), js.end(), [](const J &a, const J &b) { return a.step < b.step; });
+    for (size_t i = 0; i < js.size(); i++) order[i] = js[i].sb;
+}
+
+extern "C++" {
+template <typename T> static int grow_pinned(is_handle *h, T **p, size_t *cap, size_t n) {
+    if (n <= *cap) return IS_OK;
+    if (*p) cudaFreeHost(*p);
+    *p = nullptr;
+    *cap = 0;
+    IS_CK(cudaMallocHost((void **)p, n * sizeof(T)));
+    *cap = n;
+    return IS_OK;
+}
+}
+
+// Lay out a batch: every image's workspace, then the shared ready queue, its counters, the error word and the device
+// copy of the descriptors, in one arena; the descriptors and SB orders in pinned staging.
+static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
+    if (!fr || n < 1 || n > 4096) return h->setErr(IS_ERR_INVALID, "invalid batch (%d images)", n);
+    for (int i = 0; i < n; i++) {
+        const is_frame *f = fr + i;
+        if (f->width < 1 || f->height < 1 || f->width > 16384 || f->height > 16384 || f->qindex < 1 || f->qindex > 255)
+            return h->setErr(IS_ERR_INVALID, "invalid frame %d (size %dx%d, qindex %d)", i, f->width, f->height, f->qindex);
+    }
+    std::vector<size_t> off(n + 1);
+    std::vector<int> nsb(n);
+    size_t at = 0, slots = 0, nOrd = 0;
+    for (int i = 0; i < n; i++) {
+        FrameDesc F;
+        memset(&F, 0, sizeof F);
+        off[i] = at;
+        at += layout(fr[i].width, fr[i].height, nullptr, F, nsb[i]);
+        slots += (size_t)nsb[i] * SB_MAX_LEAVES;
+        nOrd += 2 * (size_t)nsb[i];
+    }
+    const size_t offQ = at, offRq = offQ + align256(slots * 8), offErr = offRq + 256, offFs = offErr + 256;
+    const size_t need = offFs + align256((size_t)n * sizeof(FrameDesc));
     if (need > h->arenaBytes) {
-        if (h->arena) { cudaStreamSynchronize(h->own); cudaFree(h->arena); h->arena = nullptr; h->arenaBytes = 0; }
+        if (h->arena) { cudaStreamSynchronize(h->own); cudaDeviceSynchronize(); cudaFree(h->arena); h->arena = nullptr; h->arenaBytes = 0; }
         IS_CK(cudaMalloc(&h->arena, need));
         h->arenaBytes = need;
-        h->geomW = -1;
     }
-    memset(&F, 0, sizeof F);
-    layout(f->width, f->height, (uint8_t *)h->arena, F, nSb);
-    // tiles, wavefront order, decode order
-    std::vector<int> cs, rs;
-    min_tiles(f->width, f->height, cs, rs);
-    if (cs.size() > 65 || rs.size() > 65) return h->setErr(IS_ERR_INVALID, "too many tiles");
-    F.tileCols = (int)cs.size() - 1; F.tileRows = (int)rs.size() - 1;
-    for (size_t i = 0; i < cs.size(); i++) F.tileColStart[i] = cs[i];
-    for (size_t i = 0; i < rs.size(); i++) F.tileRowStart[i] = rs[i];
-    F.qidx = f->qindex;
-    F.qctx = av1g_coeff_cdf_q_ctx(f->qindex);
-    lambda_fx(f->qindex, 8, &F.lam, &F.sqlam);
-    F.dcQ = AV1G_T(Dc_Qlookup)[0][f->qindex];
-    F.acQ = AV1G_T(Ac_Qlookup)[0][f->qindex];
-    if (h->geomW != f->width || h->geomH != f->height) {
-        std::vector<uint32_t> order, dec;
-        struct J { uint32_t sb; int step; };
-        std::vector<J> js;
-        for (int tr = 0; tr < F.tileRows; tr++)
-            for (int tc = 0; tc < F.tileCols; tc++) {
-                const int r0 = rs[tr] >> 4, r1 = (rs[tr + 1] + 15) >> 4, c0 = cs[tc] >> 4, c1 = (cs[tc + 1] + 15) >> 4;
-                for (int r = r0; r < r1; r++)
-                    for (int c = c0; c < c1; c++) {
-                        js.push_back(J{(uint32_t)(r * F.sbCols + c), (c - c0) + 2 * (r - r0)});
-                        dec.push_back((uint32_t)(r * F.sbCols + c));
-                    }
-            }
-        std::stable_sort(js.begin(), js.end(), [](const J &a, const J &b) { return a.step < b.step; });
-        for (auto &j : js) order.push_back(j.sb);
-        IS_CK(cudaMemcpy((void *)F.sbOrder, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
-        IS_CK(cudaMemcpy(F.sbDecodeOrder, dec.data(), dec.size() * 4, cudaMemcpyHostToDevice));
-        h->geomW = f->width;
-        h->geomH = f->height;
-    }
+    uint8_t *base = (uint8_t *)h->arena;
+    h->bReadyQ = (unsigned long long *)(base + offQ);
+    h->bRq = (int *)(base + offRq);
+    h->bErr = (int *)(base + offErr);
+    h->dFs = (FrameDesc *)(base + offFs);
+    h->bSlots = slots;
+    int rc = grow_pinned(h, &h->hFs, &h->hFsCap, (size_t)n);
+    if (!rc) rc = grow_pinned(h, &h->hOrd, &h->hOrdCap, nOrd);
+    if (!rc) rc = grow_pinned(h, &h->hCnt, &h->hCntCap, (size_t)n * 4 + 4);
+    if (rc) return rc;
     if (h->trace) {
-        const size_t need = (size_t)nSb * SB_MAX_LEAVES * 4;
-        if (need > h->traceCap) {
+        const size_t needT = slots * 4;
+        if (needT > h->traceCap) {
             if (h->traceBuf) cudaFree(h->traceBuf);
-            IS_CK(cudaMalloc(&h->traceBuf, need * 8));
-            h->traceCap = need;
+            h->traceBuf = nullptr;
+            h->traceCap = 0;
+            IS_CK(cudaMalloc(&h->traceBuf, needT * 8));
+            h->traceCap = needT;
         }
-        F.leafTrace = h->traceBuf;
     }
-    h->F = F;
-    h->nSb = nSb;
-    h->qidx = f->qindex;
+    h->bF.assign(n, FrameDesc());
+    h->bNsb = nsb;
+    h->bQ.assign(n, 0);
+    h->bNb.assign(n, 0);
+    h->bNt.assign(n, 0);
+    h->bNc.assign(n, 0);
+    size_t o = 0;
+    for (int i = 0; i < n; i++) {
+        const is_frame *f = fr + i;
+        FrameDesc &F = h->bF[i];
+        memset(&F, 0, sizeof F);
+        int ns = 0;
+        layout(f->width, f->height, base + off[i], F, ns);
+        std::vector<int> cs, rs;
+        min_tiles(f->width, f->height, cs, rs);
+        if (cs.size() > 65 || rs.size() > 65) return h->setErr(IS_ERR_INVALID, "too many tiles");
+        F.tileCols = (int)cs.size() - 1; F.tileRows = (int)rs.size() - 1;
+        for (size_t k = 0; k < cs.size(); k++) F.tileColStart[k] = cs[k];
+        for (size_t k = 0; k < rs.size(); k++) F.tileRowStart[k] = rs[k];
+        F.qidx = f->qindex;
+        F.qctx = av1g_coeff_cdf_q_ctx(f->qindex);
+        lambda_fx(f->qindex, 8, &F.lam, &F.sqlam);
+        F.dcQ = AV1G_T(Dc_Qlookup)[0][f->qindex];
+        F.acQ = AV1G_T(Ac_Qlookup)[0][f->qindex];
+        F.readyQ = h->bReadyQ;
+        F.rq = h->bRq;
+        F.err = h->bErr;
+        F.img = i;
+        F.leafTrace = (h->trace && i == 0) ? h->traceBuf : nullptr;
+        sb_orders(F, cs, rs, h->hOrd + o, h->hOrd + o + ns);
+        o += 2 * (size_t)ns;
+        h->hFs[i] = F;
+        h->bQ[i] = f->qindex;
+    }
+    h->bN = n;
     return IS_OK;
 }
 
-static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) {
-    FrameDesc &F = h->F;
-    const int nSb = h->nSb;
-    IS_CK(cudaEventRecord(h->ev[0], st));
-    // (the descriptor travels by value in every launch's parameters: no copy, no device-side read of it)
-    // planes into the padded workspace
-    for (int p = 0; p < 3; p++) {
-        const int ss = p ? 1 : 0;
-        const int vw = (f->width + ss) >> ss, vh = (f->height + ss) >> ss;
-        uint8_t *dst = const_cast<uint8_t *>(F.src[p]);
-        IS_CK(cudaMemcpy2DAsync(dst, F.spitch[p], f->planes[p], f->pitch[p], vw, vh,
-                                fromHost ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
-        const int pw = ((F.sbCols + 1) * 64) >> ss, ph = (F.sbRows * 64) >> ss;
-        k_pad<uint8_t><<<dim3(1, ph), 128, 0, st>>>(dst, F.spitch[p], vw, vh, pw, ph);
-    }
-    IS_CK(cudaMemsetAsync(F.queue, 0, 16, st));
-    IS_CK(cudaMemsetAsync(F.err, 0, 4, st));
-    IS_CK(cudaEventRecord(h->ev[1], st));
-    k_analysis_big<8><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig, st>>>(h->F);
-    k_analysis<8><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn, st>>>(h->F);
-    k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem), st>>>(h->F);
-    k_analysis_mid<8><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem), st>>>(h->F);
-    IS_CK(cudaGetLastError());
-    IS_CK(cudaEventRecord(h->ev[2], st));
-    k_dp<<<(nSb + 63) / 64, 64, 0, st>>>(h->F, nSb);
-    IS_CK(cudaGetLastError());
-    IS_CK(cudaEventRecord(h->ev[3], st));
-    k_leaf_prep<<<nSb, 256, 0, st>>>(h->F, nSb);
-    k_leaf_queue_scan<<<1, 1024, 0, st>>>(h->F, nSb);
-    k_leaf_deps<0><<<nSb, 256, 0, st>>>(h->F, nSb);
-    k_leaf_deps<1><<<nSb, 256, 0, st>>>(h->F, nSb);
-    k_leaf_deps<2><<<nSb, 256, 0, st>>>(h->F, nSb);
-    IS_CK(cudaGetLastError());
+// the launch sequence of a prepared batch on stream st (capturable: no host synchronisation inside)
+static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n, bool fromHost, bool events) {
+    if (events) IS_CK(cudaEventRecord(h->ev[0], st));
+    IS_CK(cudaMemcpyAsync(h->dFs, h->hFs, (size_t)n * sizeof(FrameDesc), cudaMemcpyHostToDevice, st));
     {
-        void *args[1] = {(void *)&h->F};
-        IS_CK(cudaLaunchCooperativeKernel((const void *)k_recon<8>, dim3(h->rcGrid), dim3(RC_WARPS * 32), args, h->smemRc, st));
+        size_t o = 0;
+        for (int i = 0; i < n; i++) {
+            const FrameDesc &F = h->bF[i];
+            const int ns = h->bNsb[i];
+            IS_CK(cudaMemcpyAsync((void *)F.sbOrder, h->hOrd + o, (size_t)ns * 4, cudaMemcpyHostToDevice, st));
+            IS_CK(cudaMemcpyAsync(F.sbDecodeOrder, h->hOrd + o + ns, (size_t)ns * 4, cudaMemcpyHostToDevice, st));
+            IS_CK(cudaMemsetAsync(F.queue, 0, 16, st));
+            o += 2 * (size_t)ns;
+        }
     }
-    IS_CK(cudaEventRecord(h->ev[4], st));
-    k_pack_scan<<<1, 1024, 0, st>>>(h->F, nSb);
-    k_pack<<<nSb, 256, 0, st>>>(h->F, nSb);
+    IS_CK(cudaMemsetAsync(h->bReadyQ, 0, h->bSlots * 8, st));
+    IS_CK(cudaMemsetAsync(h->bRq, 0, 16, st));
+    IS_CK(cudaMemsetAsync(h->bErr, 0, 4, st));
+    // front end of each image: planes, analysis, DP, leaf maps and the dataflow graph (its initial ready leaves go to
+    // the shared queue); images spread over frontStreams streams
+    const int K = n > 1 ? std::max(1, std::min(h->frontStreams, 4)) : 1;
+    if (K > 1) {
+        IS_CK(cudaEventRecord(h->evFork, st));
+        for (int k = 0; k < K; k++) IS_CK(cudaStreamWaitEvent(h->aux[k], h->evFork, 0));
+    }
+    for (int i = 0; i < n; i++) {
+        const FrameDesc &F = h->bF[i];
+        const is_frame *f = fr + i;
+        const int nSb = h->bNsb[i];
+        cudaStream_t s = K > 1 ? h->aux[i % K] : st;
+        for (int p = 0; p < 3; p++) {
+            const int ss = p ? 1 : 0;
+            const int vw = (f->width + ss) >> ss, vh = (f->height + ss) >> ss;
+            uint8_t *dst = const_cast<uint8_t *>(F.src[p]);
+            IS_CK(cudaMemcpy2DAsync(dst, F.spitch[p], f->planes[p], f->pitch[p], vw, vh, fromHost ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+            const int pw = ((F.sbCols + 1) * 64) >> ss, ph = (F.sbRows * 64) >> ss;
+            k_pad<uint8_t><<<dim3(1, ph), 128, 0, s>>>(dst, F.spitch[p], vw, vh, pw, ph);
+        }
+        if (events && n == 1) IS_CK(cudaEventRecord(h->ev[1], s));
+        k_analysis_big<8><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig, s>>>(F);
+        k_analysis<8><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn, s>>>(F);
+        k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem), s>>>(F);
+        k_analysis_mid<8><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem), s>>>(F);
+        IS_CK(cudaGetLastError());
+        if (events && n == 1) IS_CK(cudaEventRecord(h->ev[2], s));
+        k_dp<<<(nSb + 63) / 64, 64, 0, s>>>(F, nSb);
+        k_leaf_prep<<<nSb, 256, 0, s>>>(F, nSb);
+        k_leaf_queue_scan<<<1, 1024, 0, s>>>(F, nSb);
+        k_leaf_deps<0><<<nSb, 256, 0, s>>>(F, nSb);
+        k_leaf_deps<1><<<nSb, 256, 0, s>>>(F, nSb);
+        k_leaf_deps<2><<<nSb, 256, 0, s>>>(F, nSb);
+        IS_CK(cudaGetLastError());
+    }
+    if (K > 1) {
+        for (int k = 0; k < K; k++) {
+            IS_CK(cudaEventRecord(h->evJoin[k], h->aux[k]));
+            IS_CK(cudaStreamWaitEvent(st, h->evJoin[k], 0));
+        }
+    }
+    if (events) IS_CK(cudaEventRecord(h->ev[3], st));
+    {   // the closed loop of every image at once: a cooperative launch (all CTAs resident: their warps wait on each
+        // other's leaves), expressed with launch attributes so that it can be captured in a graph
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(h->rcGrid);
+        cfg.blockDim = dim3(RC_WARPS * 32);
+        cfg.dynamicSmemBytes = h->smemRc;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const FrameDesc *fs = h->dFs;
+        IS_CK(cudaLaunchKernelEx(&cfg, k_recon<8>, fs, n));
+    }
+    if (events) IS_CK(cudaEventRecord(h->ev[4], st));
+    for (int i = 0; i < n; i++) {
+        const FrameDesc &F = h->bF[i];
+        k_pack_scan<<<1, 1024, 0, st>>>(F, h->bNsb[i]);
+        k_pack<<<h->bNsb[i], 256, 0, st>>>(F, h->bNsb[i]);
+    }
     IS_CK(cudaGetLastError());
-    IS_CK(cudaEventRecord(h->ev[5], st));
-    // counts + error status
-    uint32_t *hs = (uint32_t *)h->hostSmall;
-    IS_CK(cudaMemcpyAsync(hs, F.offBlk + nSb, 4, cudaMemcpyDeviceToHost, st));
-    IS_CK(cudaMemcpyAsync(hs + 1, F.offTxb + nSb, 4, cudaMemcpyDeviceToHost, st));
-    IS_CK(cudaMemcpyAsync(hs + 2, F.offCoef + nSb, 8, cudaMemcpyDeviceToHost, st));
-    IS_CK(cudaMemcpyAsync(hs + 4, F.err, 4, cudaMemcpyDeviceToHost, st));
-    IS_CK(cudaStreamSynchronize(st));
-    if (hs[4]) {
-        h->have = false;
-        return h->setErr(IS_ERR_TIMEOUT, "closed loop reported error %u (dependency wait budget exhausted)", hs[4]);
+    if (events) IS_CK(cudaEventRecord(h->ev[5], st));
+    // per image counts, then the error word
+    for (int i = 0; i < n; i++) {
+        const FrameDesc &F = h->bF[i];
+        const int nSb = h->bNsb[i];
+        IS_CK(cudaMemcpyAsync(h->hCnt + 4 * i, F.offBlk + nSb, 4, cudaMemcpyDeviceToHost, st));
+        IS_CK(cudaMemcpyAsync(h->hCnt + 4 * i + 1, F.offTxb + nSb, 4, cudaMemcpyDeviceToHost, st));
+        IS_CK(cudaMemcpyAsync(h->hCnt + 4 * i + 2, F.offCoef + nSb, 8, cudaMemcpyDeviceToHost, st));
     }
-    h->nBlocks = hs[0];
-    h->nTxb = hs[1];
-    memcpy(&h->nCoeffs, hs + 2, 8);
-    float ms[6];
-    for (int i = 1; i < 6; i++) IS_CK(cudaEventElapsedTime(&ms[i], h->ev[i - 1], h->ev[i]));
-    h->times.upload = ms[1]; h->times.analysis = ms[2]; h->times.dp = ms[3]; h->times.recon = ms[4]; h->times.pack = ms[5];
-    h->times.total = ms[1] + ms[2] + ms[3] + ms[4] + ms[5];
-    h->times.sbs = (uint32_t)nSb;
-    h->times.blocks = h->nBlocks;
+    IS_CK(cudaMemcpyAsync(h->hCnt + 4 * n, h->bErr, 4, cudaMemcpyDeviceToHost, st));
+    return IS_OK;
+}
+
+static std::string batch_key(const is_handle *h, const is_frame *fr, int n, bool fromHost) {
+    std::string k;
+    char b[160];
+    snprintf(b, sizeof b, "%p|%d|%d|%d|", h->arena, n, (int)fromHost, h->frontStreams);
+    k += b;
+    for (int i = 0; i < n; i++) {
+        snprintf(b, sizeof b, "%d,%d,%d,%p,%p,%p,%d,%d,%d;", fr[i].width, fr[i].height, fr[i].qindex, fr[i].planes[0], fr[i].planes[1],
+                 fr[i].planes[2], fr[i].pitch[0], fr[i].pitch[1], fr[i].pitch[2]);
+        k += b;
+    }
+    return k;
+}
+
+static int run_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n, bool fromHost) {
+    h->have = false;
+    int rc = prepare_batch(h, fr, n);
+    if (rc) return rc;
+    if (h->useGraph) {
+        // one CUDA graph per batch signature (sizes, qindex, plane addresses, workspace): captured once, then replayed
+        const std::string key = batch_key(h, fr, n, fromHost);
+        if (key != h->graphKey || !h->graphExec) {
+            if (h->graphExec) { cudaGraphExecDestroy(h->graphExec); h->graphExec = nullptr; }
+            h->graphKey.clear();
+            IS_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            const int lrc = launch_batch(h, st, fr, n, fromHost, false);
+            cudaGraph_t g = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(st, &g);
+            if (lrc) { if (g) cudaGraphDestroy(g); return lrc; }
+            IS_CK(ec);
+            const cudaError_t ei = cudaGraphInstantiate(&h->graphExec, g, 0);
+            cudaGraphDestroy(g);
+            IS_CK(ei);
+            h->graphKey = key;
+        }
+        IS_CK(cudaEventRecord(h->ev[0], st));   // (events recorded inside a graph cannot be timed: the whole batch)
+        IS_CK(cudaGraphLaunch(h->graphExec, st));
+        IS_CK(cudaEventRecord(h->ev[5], st));
+    } else {
+        rc = launch_batch(h, st, fr, n, fromHost, true);
+        if (rc) return rc;
+    }
+    IS_CK(cudaStreamSynchronize(st));
+    if (h->hCnt[4 * n]) return h->setErr(IS_ERR_TIMEOUT, "closed loop reported error %u (dependency wait budget exhausted)", h->hCnt[4 * n]);
+    for (int i = 0; i < n; i++) {
+        h->bNb[i] = h->hCnt[4 * i];
+        h->bNt[i] = h->hCnt[4 * i + 1];
+        memcpy(&h->bNc[i], h->hCnt + 4 * i + 2, 8);
+    }
+    float ms[6] = {0, 0, 0, 0, 0, 0};
+    memset(&h->times, 0, sizeof h->times);
+    if (h->useGraph) {
+        IS_CK(cudaEventElapsedTime(&ms[3], h->ev[0], h->ev[5]));
+    } else {
+        IS_CK(cudaEventElapsedTime(&ms[3], h->ev[0], h->ev[3]));
+        IS_CK(cudaEventElapsedTime(&ms[4], h->ev[3], h->ev[4]));
+        IS_CK(cudaEventElapsedTime(&ms[5], h->ev[4], h->ev[5]));
+    }
+    if (n == 1 && !h->useGraph) {   // single image on one stream: the front end split into its stages
+        float up = 0, an = 0, dp = 0;
+        IS_CK(cudaEventElapsedTime(&up, h->ev[0], h->ev[1]));
+        IS_CK(cudaEventElapsedTime(&an, h->ev[1], h->ev[2]));
+        IS_CK(cudaEventElapsedTime(&dp, h->ev[2], h->ev[3]));
+        h->times.upload = up; h->times.analysis = an; h->times.dp = dp;
+    } else {
+        h->times.analysis = ms[3];   // upload + analysis + DP + dataflow graph of every image
+    }
+    h->times.recon = ms[4];
+    h->times.pack = ms[5];
+    h->times.total = ms[3] + ms[4] + ms[5];
+    h->times.sbs = 0;
+    h->times.blocks = 0;
+    for (int i = 0; i < n; i++) { h->times.sbs += (uint32_t)h->bNsb[i]; h->times.blocks += h->bNb[i]; }
+    // image 0 mirrored into the single-image fields
+    h->F = h->bF[0];
+    h->nSb = h->bNsb[0];
+    h->qidx = h->bQ[0];
+    h->nBlocks = h->bNb[0];
+    h->nTxb = h->bNt[0];
+    h->nCoeffs = h->bNc[0];
     h->have = true;
     return IS_OK;
 }
@@ -557,47 +758,83 @@ static int run(is_handle *h, cudaStream_t st, const is_frame *f, bool fromHost) 
 int is_encode_device(is_handle *h, const is_frame *f, void *stream) {
     if (!h) return IS_ERR_INVALID;
     IS_CK(cudaSetDevice(h->device));
-    const int rc = prepare(h, f);
-    if (rc) return rc;
-    return run(h, stream ? (cudaStream_t)stream : h->own, f, false);
+    return run_batch(h, stream ? (cudaStream_t)stream : h->own, f, 1, false);
 }
 
 int is_encode_host(is_handle *h, const is_frame *f, void *stream) {
     if (!h) return IS_ERR_INVALID;
     IS_CK(cudaSetDevice(h->device));
-    const int rc = prepare(h, f);
-    if (rc) return rc;
-    return run(h, stream ? (cudaStream_t)stream : h->own, f, true);
+    return run_batch(h, stream ? (cudaStream_t)stream : h->own, f, 1, true);
 }
 
-int is_record_counts(const is_handle *h, uint32_t *nb, uint32_t *nt, uint64_t *nc) {
-    if (!h || !h->have) return IS_ERR_STATE;
-    if (nb) *nb = h->nBlocks;
-    if (nt) *nt = h->nTxb;
-    if (nc) *nc = h->nCoeffs;
+int is_encode_batch(is_handle *h, const is_frame *frames, int n, int from_host, void *stream) {
+    if (!h) return IS_ERR_INVALID;
+    IS_CK(cudaSetDevice(h->device));
+    return run_batch(h, stream ? (cudaStream_t)stream : h->own, frames, n, from_host != 0);
+}
+
+int is_set_batch_options(is_handle *h, int use_graph, int front_streams) {
+    if (!h || front_streams < 0 || front_streams > 4 || front_streams == 3) return IS_ERR_INVALID;
+    h->useGraph = use_graph != 0;
+    if (front_streams) h->frontStreams = front_streams;
+    if (!h->useGraph && h->graphExec) { cudaGraphExecDestroy(h->graphExec); h->graphExec = nullptr; h->graphKey.clear(); }
     return IS_OK;
 }
 
-int is_record_copy(is_handle *h, av1g_frame_params *fp, av1g_block *blocks, uint32_t *block_txb, av1g_txb *txb, int16_t *coeffs,
-                   void *recon[3], const int32_t recon_pitch[3]) {
-    if (!h || !h->have) return IS_ERR_STATE;
+int is_autotune_batch(is_handle *h, const is_frame *frames, int n, int from_host, int *front_streams, float *ms) {
+    if (!h || !frames || n < 1) return IS_ERR_INVALID;
     IS_CK(cudaSetDevice(h->device));
-    const FrameDesc &F = h->F;
+    const bool g = h->useGraph;
+    h->useGraph = false;
+    int best = 1;
+    float bestMs = 1e30f;
+    const int cand[3] = {1, 2, 4};
+    for (int c = 0; c < 3; c++) {
+        if (cand[c] > 1 && n < 2) break;
+        h->frontStreams = cand[c];
+        float t = 0;
+        for (int r = 0; r < 2; r++) {   // the second run is timed (the first warms the workspace)
+            const int rc = run_batch(h, h->own, frames, n, from_host != 0);
+            if (rc) { h->useGraph = g; return rc; }
+            t = h->times.total;
+        }
+        if (t < bestMs) { bestMs = t; best = cand[c]; }
+    }
+    h->frontStreams = best;
+    h->useGraph = g;
+    if (front_streams) *front_streams = best;
+    if (ms) *ms = bestMs;
+    return IS_OK;
+}
+
+int is_batch_counts(const is_handle *h, int i, uint32_t *nb, uint32_t *nt, uint64_t *nc) {
+    if (!h || !h->have || i < 0 || i >= h->bN) return IS_ERR_STATE;
+    if (nb) *nb = h->bNb[i];
+    if (nt) *nt = h->bNt[i];
+    if (nc) *nc = h->bNc[i];
+    return IS_OK;
+}
+
+int is_batch_copy(is_handle *h, int i, av1g_frame_params *fp, av1g_block *blocks, uint32_t *block_txb, av1g_txb *txb, int16_t *coeffs,
+                  void *recon[3], const int32_t recon_pitch[3]) {
+    if (!h || !h->have || i < 0 || i >= h->bN) return IS_ERR_STATE;
+    IS_CK(cudaSetDevice(h->device));
+    const FrameDesc &F = h->bF[i];
     cudaStream_t st = h->own;
     if (fp) {
         memset(fp, 0, sizeof *fp);
         fp->version = AV1G_DECISIONS_VERSION;
         fp->width = (uint32_t)F.W; fp->height = (uint32_t)F.H;
-        fp->base_q_idx = (uint8_t)h->qidx;
+        fp->base_q_idx = (uint8_t)h->bQ[i];
         fp->tile_cols_log2 = -1; fp->tile_rows_log2 = -1;
         fp->qm_y = fp->qm_u = fp->qm_v = 15;
         fp->chroma_format = AV1G_CHROMA_420;
         fp->bit_depth = 8;
     }
-    if (blocks) IS_CK(cudaMemcpyAsync(blocks, F.recBlocks, (size_t)h->nBlocks * sizeof(av1g_block), cudaMemcpyDeviceToHost, st));
-    if (block_txb) IS_CK(cudaMemcpyAsync(block_txb, F.recBlockTxb, ((size_t)h->nBlocks + 1) * 4, cudaMemcpyDeviceToHost, st));
-    if (txb) IS_CK(cudaMemcpyAsync(txb, F.recTxb, (size_t)h->nTxb * sizeof(av1g_txb), cudaMemcpyDeviceToHost, st));
-    if (coeffs) IS_CK(cudaMemcpyAsync(coeffs, F.recCoeffs, (size_t)h->nCoeffs * 2, cudaMemcpyDeviceToHost, st));
+    if (blocks) IS_CK(cudaMemcpyAsync(blocks, F.recBlocks, (size_t)h->bNb[i] * sizeof(av1g_block), cudaMemcpyDeviceToHost, st));
+    if (block_txb) IS_CK(cudaMemcpyAsync(block_txb, F.recBlockTxb, ((size_t)h->bNb[i] + 1) * 4, cudaMemcpyDeviceToHost, st));
+    if (txb) IS_CK(cudaMemcpyAsync(txb, F.recTxb, (size_t)h->bNt[i] * sizeof(av1g_txb), cudaMemcpyDeviceToHost, st));
+    if (coeffs) IS_CK(cudaMemcpyAsync(coeffs, F.recCoeffs, (size_t)h->bNc[i] * 2, cudaMemcpyDeviceToHost, st));
     for (int p = 0; p < 3; p++) {
         if (!recon || !recon[p]) continue;
         const int ss = p ? 1 : 0;
@@ -606,6 +843,13 @@ int is_record_copy(is_handle *h, av1g_frame_params *fp, av1g_block *blocks, uint
     }
     IS_CK(cudaStreamSynchronize(st));
     return IS_OK;
+}
+
+int is_record_counts(const is_handle *h, uint32_t *nb, uint32_t *nt, uint64_t *nc) { return is_batch_counts(h, 0, nb, nt, nc); }
+
+int is_record_copy(is_handle *h, av1g_frame_params *fp, av1g_block *blocks, uint32_t *block_txb, av1g_txb *txb, int16_t *coeffs,
+                   void *recon[3], const int32_t recon_pitch[3]) {
+    return is_batch_copy(h, 0, fp, blocks, block_txb, txb, coeffs, recon, recon_pitch);
 }
 
 int is_record_device(const is_handle *h, const av1g_block **blocks, const uint32_t **block_txb, const av1g_txb **txb, const int16_t **coeffs) {

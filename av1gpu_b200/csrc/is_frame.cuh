@@ -32,7 +32,7 @@ struct BlockRes {      // analysis result of one (shape, position): 16 bytes
 struct Leaf { uint8_t bsize, x4, y4, pad; };
 struct SbCount { uint32_t nBlocks, nTxb, nCoeffs, pad; };
 
-struct FrameDesc {
+struct __align__(16) FrameDesc {
     int W, H, MiCols, MiRows, sbCols, sbRows, ssx, ssy, bd, qidx, qctx;
     int tileCols, tileRows;
     int tileColStart[65], tileRowStart[65];   // mi units, [n] = MiCols / MiRows
@@ -58,16 +58,18 @@ struct FrameDesc {
     uint16_t *leafTxb, *leafCoef;             // [nSb * 256] first tx block / coefficient (SB-local) of each leaf
     int *leafDone;                            // [nSb * 256] 1 once the leaf's luma (reconstruction, maps) is written, 2 once all is
     uint32_t *leafStart;                      // [nSb] first position of each SB's leaves in the wavefront order
-    uint32_t *leafQueue;                      // [nSb * 256] ready queue: 1 + (sb << 8 | leaf) in the order leaves became
-                                              // ready (0: slot not written yet)
     uint32_t *leafTotal;                      // [1] leaves of the image
-    int *queue;                               // [4] ready-queue head (next slot to take), tail (next slot to write),
-                                              // next free entry of revList
+    int *queue;                               // [4] [2]: next free entry of revList
+    // the closed loop's ready queue, shared by every image of a batch: 1 + (image << 32 | sb << 8 | leaf) in the order
+    // leaves became ready (0: slot not written yet); rq[0] next slot to take, rq[1] next slot to write
+    unsigned long long *readyQ;
+    int *rq;
+    int img;                                  // index of the image in its batch
     int *depCnt;                              // [nSb * 256] luma dependencies of each leaf not yet published
     int *revCnt, *revFill;                    // [nSb * 256] dependents of each leaf; entries written so far
     uint32_t *revOff;                         // [nSb * 256] first entry of each leaf's dependents in revList
     uint32_t *revList;                        // [nSb * REV_PER_SB] dependents (sb << 8 | leaf), grouped per leaf
-    int *err;                                 // [1] error status (0 = ok)
+    int *err;                                 // [1] error status (0 = ok), shared by the images of a batch
     unsigned long long *leafTrace;            // [leaves * 4] optional (debug): claimed / ready / luma done / done (ns)
     // pack output (DecisionRecord arrays in decode order) and per-SB offsets
     uint32_t *sbDecodeOrder;                  // [nSb] SBs in decode order (tiles raster, SB raster inside a tile)

@@ -43,11 +43,14 @@ template <typename Px> struct RcWarp {
     int job;
 };
 template <typename Px> struct RcSmem {
-    RateStage T;
+    RateStage T;                         // scans, base-context offsets (and the cost table of q-context 0)
+    uint16_t cost[3][NCDF];              // the cost tables of q-contexts 1 .. 3 (the images of a batch mix qindex)
+    FrameDesc F[RC_WARPS];               // each warp's copy of the descriptor of the image it works on
     RcWarp<Px> w[RC_WARPS];
 };
-static_assert(offsetof(RcWarp<uint8_t>, srcS) % 16 == 0 && sizeof(RcWarp<uint8_t>) % 16 == 0 && offsetof(RcSmem<uint8_t>, w) % 16 == 0,
-              "the staged sources take 16-byte vector stores");
+static_assert(offsetof(RcWarp<uint8_t>, srcS) % 16 == 0 && sizeof(RcWarp<uint8_t>) % 16 == 0 && offsetof(RcSmem<uint8_t>, w) % 16 == 0 &&
+                  offsetof(RcSmem<uint8_t>, cost) % 16 == 0 && offsetof(RcSmem<uint8_t>, F) % 16 == 0 && sizeof(FrameDesc) % 16 == 0,
+              "the staged sources, tables and descriptors take 16-byte vector stores");
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
     int v;
@@ -286,10 +289,11 @@ __device__ int luma_deps(const FrameDesc &F, int sb, int li, uint32_t *out) {
     return n;
 }
 
-// append leaf id to the ready queue
+// append leaf id (sb << 8 | leaf) of the image to the batch's ready queue
 __device__ __forceinline__ void push_ready(const FrameDesc &F, uint32_t id) {
-    const int pos = atomicAdd(F.queue + 1, 1);
-    st_release((int *)F.leafQueue + pos, (int)id + 1);
+    const int pos = atomicAdd(F.rq + 1, 1);
+    const unsigned long long v = 1ull + (((unsigned long long)F.img << 32) | id);
+    asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(F.readyQ + pos), "l"(v) : "memory");
 }
 
 template <int BD, typename Px>
@@ -738,40 +742,65 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
     }
 }
 
-// persistent grid of independent warps over the ready queue: a warp takes the next slot, waits until a leaf has been
-// written there (bounded in time), and runs it
+// Persistent grid of independent warps over the ready queue of a batch of nImg images (Fs: their descriptors in
+// device memory): a warp takes the next slot, waits until a leaf has been written there (bounded in time), brings the
+// descriptor of the leaf's image into its shared copy when the image changes, and runs the leaf.
 constexpr unsigned long long READY_WAIT_NS = 4000000000ull;
 template <int BD>
-__global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const __grid_constant__ FrameDesc F) {
+__global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__restrict__ Fs, int nImg) {
     typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RcSmem<Px> &S = *reinterpret_cast<RcSmem<Px> *>(smem_raw);
-    RcWarp<Px> &Wp = S.w[threadIdx.x >> 5];
-    const int lane = lane_id();
-    const RateTabs T = rate_tabs_stage(S.T, F.qctx, threadIdx.x, blockDim.x);
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    RcWarp<Px> &Wp = S.w[warp];
+    FrameDesc &F = S.F[warp];
+    {   // all four cost tables (q-context 0 in the RateStage), the scans and base-context offsets
+        rate_tabs_stage(S.T, 0, threadIdx.x, blockDim.x);
+        for (int q = 1; q < 4; q++) {
+            const uint4 *c = reinterpret_cast<const uint4 *>(g_cost[q]);
+            for (int i = threadIdx.x; i < NCDF / 8; i += blockDim.x) reinterpret_cast<uint4 *>(S.cost[q - 1])[i] = c[i];
+        }
+    }
     __syncthreads();
-    const int total = (int)*F.leafTotal;
+    const int *rq = Fs[0].rq;
+    const unsigned long long *readyQ = Fs[0].readyQ;
+    int *err = Fs[0].err;
+    unsigned long long *traceBase = Fs[0].leafTrace;
+    int total = 0;
+    for (int i = 0; i < nImg; i++) total += (int)*Fs[i].leafTotal;
+    int cur = -1;
     for (;;) {
-        int e = 0, h = 0;
+        unsigned long long e = 0;
+        int h = 0, bad = 0;
         if (lane == 0) {
-            h = atomicAdd(F.queue, 1);
+            h = atomicAdd(const_cast<int *>(rq), 1);
             if (h >= total) {
-                e = -1;
+                bad = 1;
             } else {
                 const unsigned long long t0 = gtimer();
-                while ((e = ld_acquire((const int *)F.leafQueue + h)) == 0) {
-                    if (gtimer() - t0 > READY_WAIT_NS || *(volatile int *)F.err) break;
+                for (;;) {
+                    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(e) : "l"(readyQ + h) : "memory");
+                    if (e || gtimer() - t0 > READY_WAIT_NS || *(volatile int *)err) break;
                     __nanosleep(128);
                 }
-                if (e == 0) { atomicCAS(F.err, 0, KERR_WAIT_LEAF); e = -1; }
-                if (F.leafTrace) { F.leafTrace[(size_t)h * 4] = t0; F.leafTrace[(size_t)h * 4 + 1] = gtimer(); }
+                if (!e) { atomicCAS(err, 0, KERR_WAIT_LEAF); bad = 1; }
+                if (traceBase) { traceBase[(size_t)h * 4] = t0; traceBase[(size_t)h * 4 + 1] = gtimer(); }
             }
         }
+        if (__shfl_sync(0xffffffffu, bad, 0)) break;
         e = __shfl_sync(0xffffffffu, e, 0);
         h = __shfl_sync(0xffffffffu, h, 0);
-        if (e < 0) break;
-        const uint32_t id = (uint32_t)e - 1;
-        unsigned long long *trace = F.leafTrace ? F.leafTrace + (size_t)h * 4 : nullptr;
+        const unsigned long long v = e - 1;
+        const int img = (int)(v >> 32);
+        const uint32_t id = (uint32_t)v;
+        if (img != cur) {   // the descriptor of the leaf's image into the warp's shared copy
+            const uint4 *src = reinterpret_cast<const uint4 *>(Fs + img);
+            for (int k = lane; k < (int)(sizeof(FrameDesc) / 16); k += 32) reinterpret_cast<uint4 *>(&F)[k] = src[k];
+            __syncwarp();
+            cur = img;
+        }
+        const RateTabs T{F.qctx == 0 ? S.T.cost : S.cost[F.qctx - 1], S.T.scan, S.T.baseCtx};
+        unsigned long long *trace = traceBase ? traceBase + (size_t)h * 4 : nullptr;
         rc_leaf<BD, Px>(F, Wp, T, (int)(id >> 8), (int)(id & 255), trace);
     }
 }
@@ -787,7 +816,6 @@ __global__ void k_leaf_prep(const __grid_constant__ FrameDesc F, int nSb) {
     F.leafDone[(size_t)sb * SB_MAX_LEAVES + tid] = 0;
     F.revCnt[(size_t)sb * SB_MAX_LEAVES + tid] = 0;
     F.revFill[(size_t)sb * SB_MAX_LEAVES + tid] = 0;
-    F.leafQueue[(size_t)sb * SB_MAX_LEAVES + tid] = 0;
     __syncthreads();
     if (tid < nl) {
         const Leaf l = F.leaves[(size_t)sb * SB_MAX_LEAVES + tid];

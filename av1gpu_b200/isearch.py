@@ -45,7 +45,8 @@ class IsTimes(C.Structure):
 EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_encode_host", "is_record_counts",
            "is_record_copy", "is_record_device", "is_times_get", "is_test_fwd_quant", "is_test_inverse",
            "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32", "is_set_trace", "is_get_trace",
-           "is_fwd_quant_static"]
+           "is_fwd_quant_static", "is_encode_batch", "is_batch_counts", "is_batch_copy", "is_set_batch_options",
+           "is_autotune_batch"]
 
 _lib = None
 
@@ -81,6 +82,11 @@ def load_library():
     L.is_set_trace.argtypes = [C.c_void_p, C.c_int]
     L.is_get_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32)]
     L.is_fwd_quant_static.argtypes = [C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp]
+    L.is_encode_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, vp]
+    L.is_batch_counts.argtypes = [vp, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
+    L.is_batch_copy.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp * 3, vp]
+    L.is_set_batch_options.argtypes = [vp, C.c_int, C.c_int]
+    L.is_autotune_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
     _lib = L
     return L
 
@@ -203,6 +209,61 @@ class Encoder:
     def encode_device(self, planes, qindex):
         self.encode_device_async(planes, qindex)
         return self.fetch(planes[0].shape[1], planes[0].shape[0], qindex)
+
+    # ---- batched form ----
+    def _frames(self, images, qindices, host):
+        """is_frame array for a list of (Y, U, V) planes: numpy arrays (host) or torch CUDA tensors (device)."""
+        fr = (IsFrame * len(images))()
+        for i, (planes, q) in enumerate(zip(images, qindices)):
+            y = planes[0]
+            if host:
+                ptrs, pitches = [p.ctypes.data for p in planes], [p.strides[0] for p in planes]
+            else:
+                ptrs, pitches = [p.data_ptr() for p in planes], [p.stride(0) for p in planes]
+            fr[i] = self._frame(y.shape[1], y.shape[0], q, ptrs, pitches)
+        return fr
+
+    def encode_batch_async(self, images, qindices, host=True, stream=None):
+        """Queue one batch (host numpy planes, or torch CUDA planes with host=False); returns after the record sizes
+        of every image are known."""
+        fr = self._frames(images, qindices, host)
+        self._check(self.L.is_encode_batch(self.h, fr, len(images), 1 if host else 0, stream), "is_encode_batch")
+        return fr
+
+    def batch_counts(self, i):
+        nb, nt, nc = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        self._check(self.L.is_batch_counts(self.h, i, C.byref(nb), C.byref(nt), C.byref(nc)), "is_batch_counts")
+        return nb.value, nt.value, nc.value
+
+    def batch_fetch(self, i, width, height, qindex):
+        nb, nt, nc = self.batch_counts(i)
+        cw, ch = (width + 1) // 2, (height + 1) // 2
+        out = {"blocks": np.zeros(nb, BLOCK_DT), "block_txb": np.zeros(nb + 1, np.uint32), "txb": np.zeros(nt, TXB_DT),
+               "coeffs": np.zeros(nc, np.int16),
+               "recon": [np.zeros((height, width), np.uint8), np.zeros((ch, cw), np.uint8), np.zeros((ch, cw), np.uint8)]}
+        rp = (C.c_void_p * 3)(*[r.ctypes.data for r in out["recon"]])
+        pitches = (C.c_int32 * 3)(*[r.strides[0] for r in out["recon"]])
+        self._check(self.L.is_batch_copy(self.h, i, None, out["blocks"].ctypes.data, out["block_txb"].ctypes.data,
+                                         out["txb"].ctypes.data, out["coeffs"].ctypes.data, rp, pitches), "is_batch_copy")
+        return Record(width, height, qindex, out["blocks"], out["block_txb"], out["txb"], out["coeffs"], out["recon"],
+                      self.times())
+
+    def encode_batch(self, images, qindices):
+        """Encode a list of host images ((Y, U, V) uint8 planes) with their qindices in one batch; a list of Records."""
+        images = [[np.ascontiguousarray(p, np.uint8) for p in planes] for planes in images]
+        self.encode_batch_async(images, qindices, host=True)
+        return [self.batch_fetch(i, im[0].shape[1], im[0].shape[0], q) for i, (im, q) in enumerate(zip(images, qindices))]
+
+    def set_batch_options(self, use_graph=False, front_streams=0):
+        self._check(self.L.is_set_batch_options(self.h, 1 if use_graph else 0, front_streams), "is_set_batch_options")
+
+    def autotune_batch(self, images, qindices, host=True):
+        """Time the batch with 1 / 2 / 4 front-end streams and keep the fastest; returns (streams, ms)."""
+        fr = self._frames(images, qindices, host)
+        k, ms = C.c_int(), C.c_float()
+        self._check(self.L.is_autotune_batch(self.h, fr, len(images), 1 if host else 0, C.byref(k), C.byref(ms)),
+                    "is_autotune_batch")
+        return k.value, ms.value
 
     # ---- kernel-level entry points (parity tests) ----
     def test_fwd_quant(self, res, tx_size, tx_type, plane, qindex, ctx):

@@ -83,6 +83,22 @@ int is_record_device(const is_handle *h, const av1g_block **blocks, const uint32
                      const int16_t **coeffs);
 int is_times_get(const is_handle *h, is_times *t);
 
+/* ---- batched form: many images (uneven sizes, mixed qindex) per call ----
+ * One persistent closed-loop launch serves every image of the batch through one ready queue (the reference runs one
+ * wavefront per image and step: encoder/src/batch.cpp:1005-1029 threads GpEncoders over images).  Each image's front
+ * end (upload, analysis, DP, dataflow graph) runs on one of front_streams streams.  Results per image index; the
+ * single-image record calls read image 0.  Timing of a batch: is_times_get (analysis = the whole front end). */
+int is_encode_batch(is_handle *h, const is_frame *frames, int n, int from_host, void *stream);
+int is_batch_counts(const is_handle *h, int i, uint32_t *n_blocks, uint32_t *n_txb, uint64_t *n_coeffs);
+int is_batch_copy(is_handle *h, int i, av1g_frame_params *fp, av1g_block *blocks, uint32_t *block_txb, av1g_txb *txb,
+                  int16_t *coeffs, void *recon[3], const int32_t recon_pitch[3]);
+/* use_graph: capture each batch's launch sequence in a CUDA graph and replay it while the batch signature (sizes,
+ * qindex, plane addresses, workspace) repeats; front_streams: 1, 2 or 4 (0 keeps the current value). */
+int is_set_batch_options(is_handle *h, int use_graph, int front_streams);
+/* Autotuner: times the batch with 1, 2 and 4 front-end streams (two runs each, the second timed) and keeps the
+ * fastest for the handle; returns the choice and its time (ms). */
+int is_autotune_batch(is_handle *h, const is_frame *frames, int n, int from_host, int *front_streams, float *ms);
+
 /* ---- kernel-level entry points for the parity tests (device primitives of av1core's dsp.h API) ---- */
 /* Forward 2-D transform (this project's integer transform) + quantisation + rate of n residual blocks of one tx
  * size / type, host arrays: res [n][H*W] int32 -> coef [n][tw*th] (fixed point), levels [n][tw*th], D, R, eob per block.
