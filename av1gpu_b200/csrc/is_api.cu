@@ -228,6 +228,7 @@ struct is_handle {
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t evFork = nullptr, evJoin[4] = {nullptr, nullptr, nullptr, nullptr};
     int frontStreams = 1;                   // 1, 2 or 4 (is_autotune_batch chooses)
+    int reconCtas = 0;                      // CTAs of the closed loop (0: one per SM); fewer leave SMs to other streams
     bool useGraph = false;
     std::string graphKey;
     cudaGraphExec_t graphExec = nullptr;
@@ -640,7 +641,7 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
     {   // the closed loop of every image at once: a cooperative launch (all CTAs resident: their warps wait on each
         // other's leaves), expressed with launch attributes so that it can be captured in a graph
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(h->rcGrid);
+        cfg.gridDim = dim3(h->reconCtas > 0 && h->reconCtas < h->rcGrid ? h->reconCtas : h->rcGrid);
         cfg.blockDim = dim3(RC_WARPS * 32);
         cfg.dynamicSmemBytes = h->smemRc;
         cfg.stream = st;
@@ -675,7 +676,7 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
 static std::string batch_key(const is_handle *h, const is_frame *fr, int n, bool fromHost) {
     std::string k;
     char b[160];
-    snprintf(b, sizeof b, "%p|%d|%d|%d|", h->arena, n, (int)fromHost, h->frontStreams);
+    snprintf(b, sizeof b, "%p|%d|%d|%d|%d|", h->arena, n, (int)fromHost, h->frontStreams, h->reconCtas);
     k += b;
     for (int i = 0; i < n; i++) {
         snprintf(b, sizeof b, "%d,%d,%d,%p,%p,%p,%d,%d,%d;", fr[i].width, fr[i].height, fr[i].qindex, fr[i].planes[0], fr[i].planes[1],
@@ -755,6 +756,16 @@ static int run_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n, b
     return IS_OK;
 }
 
+int is_workspace_bytes(int width, int height, uint64_t *bytes) {
+    if (width < 1 || height < 1 || width > 16384 || height > 16384 || !bytes) return IS_ERR_INVALID;
+    FrameDesc F;
+    memset(&F, 0, sizeof F);
+    int nSb = 0;
+    const size_t ws = layout(width, height, nullptr, F, nSb);
+    *bytes = ws + (size_t)nSb * SB_MAX_LEAVES * 8 + align256(sizeof(FrameDesc)) + 512;
+    return IS_OK;
+}
+
 int is_encode_device(is_handle *h, const is_frame *f, void *stream) {
     if (!h) return IS_ERR_INVALID;
     IS_CK(cudaSetDevice(h->device));
@@ -773,10 +784,11 @@ int is_encode_batch(is_handle *h, const is_frame *frames, int n, int from_host, 
     return run_batch(h, stream ? (cudaStream_t)stream : h->own, frames, n, from_host != 0);
 }
 
-int is_set_batch_options(is_handle *h, int use_graph, int front_streams) {
-    if (!h || front_streams < 0 || front_streams > 4 || front_streams == 3) return IS_ERR_INVALID;
+int is_set_batch_options(is_handle *h, int use_graph, int front_streams, int recon_ctas) {
+    if (!h || front_streams < 0 || front_streams > 4 || front_streams == 3 || recon_ctas < 0) return IS_ERR_INVALID;
     h->useGraph = use_graph != 0;
     if (front_streams) h->frontStreams = front_streams;
+    h->reconCtas = recon_ctas;
     if (!h->useGraph && h->graphExec) { cudaGraphExecDestroy(h->graphExec); h->graphExec = nullptr; h->graphKey.clear(); }
     return IS_OK;
 }

@@ -46,7 +46,7 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_record_copy", "is_record_device", "is_times_get", "is_test_fwd_quant", "is_test_inverse",
            "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32", "is_set_trace", "is_get_trace",
            "is_fwd_quant_static", "is_encode_batch", "is_batch_counts", "is_batch_copy", "is_set_batch_options",
-           "is_autotune_batch"]
+           "is_autotune_batch", "is_workspace_bytes"]
 
 _lib = None
 
@@ -85,10 +85,19 @@ def load_library():
     L.is_encode_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, vp]
     L.is_batch_counts.argtypes = [vp, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
     L.is_batch_copy.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp * 3, vp]
-    L.is_set_batch_options.argtypes = [vp, C.c_int, C.c_int]
+    L.is_set_batch_options.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+    L.is_workspace_bytes.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64)]
     L.is_autotune_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
     _lib = L
     return L
+
+
+def workspace_bytes(width, height):
+    """Device workspace of one image in a batch (bytes); no GPU needed."""
+    b = C.c_uint64()
+    if load_library().is_workspace_bytes(width, height, C.byref(b)) != 0:
+        raise ValueError("invalid image size %dx%d" % (width, height))
+    return b.value
 
 
 def probe_int32(device=0):
@@ -254,8 +263,9 @@ class Encoder:
         self.encode_batch_async(images, qindices, host=True)
         return [self.batch_fetch(i, im[0].shape[1], im[0].shape[0], q) for i, (im, q) in enumerate(zip(images, qindices))]
 
-    def set_batch_options(self, use_graph=False, front_streams=0):
-        self._check(self.L.is_set_batch_options(self.h, 1 if use_graph else 0, front_streams), "is_set_batch_options")
+    def set_batch_options(self, use_graph=False, front_streams=0, recon_ctas=0):
+        self._check(self.L.is_set_batch_options(self.h, 1 if use_graph else 0, front_streams, recon_ctas),
+                    "is_set_batch_options")
 
     def autotune_batch(self, images, qindices, host=True):
         """Time the batch with 1 / 2 / 4 front-end streams and keep the fastest; returns (streams, ms)."""

@@ -1,0 +1,187 @@
+"""Serving loop of the intra search: continuous batching of arriving encode requests under an HBM budget.
+
+Requests (Y, U, V host planes + qindex) arrive over time.  `pipelines` worker threads each own a handle (its own
+stream and workspace).  Whenever a worker is free it takes the waiting requests in arrival order, as many as fit its
+share of the HBM budget (`is_workspace_bytes` per image) and `max_batch`, and searches them as one batch
+(`is_encode_batch`: one persistent closed loop over all of them).  Requests that arrive while batches are on the GPU
+wait for the next free worker, so two batches are in flight at once and their device work overlaps; a batch's
+closed loop can be limited to part of the SMs (`recon_ctas`) to leave room for the other worker's front end.  Each
+request's latency runs from its arrival to the moment its record and reconstruction are in host memory.
+
+The search is deterministic per image, so a request's result does not depend on the batch it ran in.
+"""
+import threading
+import time
+from collections import deque
+
+import numpy as np
+
+
+class Request:
+    """One encode request; `record` is filled when done (a Record), `t_done` with the completion time."""
+    __slots__ = ("rid", "planes", "qindex", "t_arrive", "t_start", "t_done", "record", "batch", "nbytes")
+
+    def __init__(self, rid, planes, qindex, t_arrive):
+        self.rid, self.planes, self.qindex, self.t_arrive = rid, planes, qindex, t_arrive
+        self.t_start = self.t_done = None
+        self.record = None
+        self.batch = -1
+        self.nbytes = 0
+
+    @property
+    def pixels(self):
+        return self.planes[0].shape[0] * self.planes[0].shape[1]
+
+
+def take_batch(pending, budget_bytes, max_batch):
+    """Admission: the longest arrival-order prefix of `pending` whose workspaces fit `budget_bytes` (at least one
+    request, which then runs alone even if it is larger than the budget), at most `max_batch` requests."""
+    out, used = [], 0
+    while pending and len(out) < max_batch:
+        r = pending[0]
+        if out and used + r.nbytes > budget_bytes:
+            break
+        out.append(pending.popleft())
+        used += r.nbytes
+    return out
+
+
+def latency_stats(requests):
+    lat = np.array([(r.t_done - r.t_arrive) * 1e3 for r in requests if r.t_done is not None])
+    if len(lat) == 0:
+        return {"n": 0}
+    return {"n": int(len(lat)), "p50_ms": round(float(np.percentile(lat, 50)), 2),
+            "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(lat.mean()), 2),
+            "max_ms": round(float(lat.max()), 2)}
+
+
+class Server:
+    def __init__(self, device=0, hbm_budget=None, pipelines=2, max_batch=64, recon_ctas=0, use_graph=False):
+        from .isearch import Encoder, workspace_bytes
+        import torch
+        self._wsb = workspace_bytes
+        if hbm_budget is None:   # half of the free device memory
+            free, _ = torch.cuda.mem_get_info(device)
+            hbm_budget = free // 2
+        self.budget = int(hbm_budget)
+        self.pipelines = pipelines
+        self.max_batch = max_batch
+        self.encs = [Encoder(device) for _ in range(pipelines)]
+        for e in self.encs:
+            e.set_batch_options(use_graph=use_graph, front_streams=2, recon_ctas=recon_ctas)
+        self._pending = deque()
+        self._cv = threading.Condition()
+        self._closed = False
+        self._nbatch = 0
+
+    def close(self):
+        for e in self.encs:
+            e.close()
+        self.encs = []
+
+    def submit(self, req):
+        req.nbytes = self._wsb(req.planes[0].shape[1], req.planes[0].shape[0])
+        with self._cv:
+            self._pending.append(req)
+            self._cv.notify()
+
+    def _worker(self, k):
+        enc = self.encs[k]
+        share = max(1, self.budget // self.pipelines)
+        while True:
+            with self._cv:
+                while not self._pending and not self._closed:
+                    self._cv.wait()
+                if not self._pending and self._closed:
+                    return
+                batch = take_batch(self._pending, share, self.max_batch)
+                bid = self._nbatch
+                self._nbatch += 1
+            t0 = time.perf_counter()
+            for r in batch:
+                r.t_start, r.batch = t0, bid
+            recs = enc.encode_batch([r.planes for r in batch], [r.qindex for r in batch])
+            t1 = time.perf_counter()
+            for r, rec in zip(batch, recs):
+                r.record, r.t_done = rec, t1
+
+    def run(self, arrivals):
+        """Serve a list of (arrival time in s from now, planes, qindex); returns the Requests (records filled)."""
+        reqs = [Request(i, p, q, None) for i, (_, p, q) in enumerate(arrivals)]
+        for r in reqs:
+            r.nbytes = self._wsb(r.planes[0].shape[1], r.planes[0].shape[0])
+        self._closed = False
+        workers = [threading.Thread(target=self._worker, args=(k,), daemon=True) for k in range(self.pipelines)]
+        for w in workers:
+            w.start()
+        t0 = time.perf_counter()
+        for r, (ta, _, _) in zip(reqs, arrivals):
+            now = time.perf_counter() - t0
+            if ta > now:
+                time.sleep(ta - now)
+            r.t_arrive = time.perf_counter()
+            with self._cv:
+                self._pending.append(r)
+                self._cv.notify()
+        with self._cv:
+            self._closed = True
+            self._cv.notify_all()
+        for w in workers:
+            w.join()
+        return reqs
+
+
+def poisson_arrivals(rate, n, seed=0):
+    """n arrival times (s) of a Poisson stream of `rate` requests per second."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, n))
+
+
+def _requests(n, seed, max_mp=24.0, min_mp=0.2):
+    """n seeded synthetic requests: crops (log-uniform area min_mp .. max_mp MP, aspect 1:3 .. 3:1) of one 6000x4000
+    synthetic image, qindex uniform 40 .. 220."""
+    from . import synth
+    rng = np.random.default_rng(seed)
+    y, u, v = synth.make_image(6000, 4000, seed, edges=True)
+    out = []
+    for _ in range(n):
+        area = float(np.exp(rng.uniform(np.log(min_mp * 1e6), np.log(max_mp * 1e6))))
+        ar = float(np.exp(rng.uniform(np.log(1 / 3), np.log(3))))
+        w = int(min(6000, max(16, np.sqrt(area * ar)))) & ~1
+        h = int(min(4000, max(16, np.sqrt(area / ar)))) & ~1
+        x0, y0 = int(rng.integers(0, 6000 - w + 1)) & ~1, int(rng.integers(0, 4000 - h + 1)) & ~1
+        planes = [np.ascontiguousarray(y[y0:y0 + h, x0:x0 + w]), np.ascontiguousarray(u[y0 // 2:(y0 + h) // 2, x0 // 2:(x0 + w) // 2]),
+                  np.ascontiguousarray(v[y0 // 2:(y0 + h) // 2, x0 // 2:(x0 + w) // 2])]
+        out.append((planes, int(rng.integers(40, 221))))
+    return out
+
+
+def main():
+    """python -m av1gpu_b200.serve [--rates 5,20,50,200] [--n 40]: p50 / p99 latency and MP/s per arrival rate."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rates", default="5,20,50,200")
+    ap.add_argument("--n", type=int, default=40)
+    ap.add_argument("--pipelines", type=int, default=2)
+    ap.add_argument("--recon-ctas", type=int, default=110)
+    ap.add_argument("--max-batch", type=int, default=32)
+    args = ap.parse_args()
+    reqs = _requests(args.n, 5)
+    srv = Server(pipelines=args.pipelines, max_batch=args.max_batch, recon_ctas=args.recon_ctas)
+    try:
+        srv.run([(0.0, p, q) for p, q in reqs[:4]])   # warm-up: workspaces, tables
+        for rate in [float(r) for r in args.rates.split(",")]:
+            t = poisson_arrivals(rate, len(reqs), seed=int(rate))
+            done = srv.run([(float(ti), p, q) for ti, (p, q) in zip(t, reqs)])
+            mp = sum(r.pixels for r in done) / 1e6
+            span = max(r.t_done for r in done) - min(r.t_arrive for r in done)
+            line = {"arrival_rate_per_s": rate, "requests": len(done), "mp": round(mp, 1), "mp_per_s": round(mp / span, 2),
+                    "batches": len({r.batch for r in done}), **latency_stats(done)}
+            print(json.dumps(line), flush=True)
+    finally:
+        srv.close()
+
+
+if __name__ == "__main__":
+    main()

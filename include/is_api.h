@@ -93,8 +93,12 @@ int is_batch_counts(const is_handle *h, int i, uint32_t *n_blocks, uint32_t *n_t
 int is_batch_copy(is_handle *h, int i, av1g_frame_params *fp, av1g_block *blocks, uint32_t *block_txb, av1g_txb *txb,
                   int16_t *coeffs, void *recon[3], const int32_t recon_pitch[3]);
 /* use_graph: capture each batch's launch sequence in a CUDA graph and replay it while the batch signature (sizes,
- * qindex, plane addresses, workspace) repeats; front_streams: 1, 2 or 4 (0 keeps the current value). */
-int is_set_batch_options(is_handle *h, int use_graph, int front_streams);
+ * qindex, plane addresses, workspace) repeats; front_streams: 1, 2 or 4 (0 keeps the current value); recon_ctas: CTAs
+ * of the closed loop, one per SM when 0 (fewer leave SMs to the work of other streams, e.g. another handle's batch). */
+int is_set_batch_options(is_handle *h, int use_graph, int front_streams, int recon_ctas);
+/* Device workspace of one image of width x height in a batch (bytes; host only, no GPU needed): what admission by
+ * HBM budget counts. */
+int is_workspace_bytes(int width, int height, uint64_t *bytes);
 /* Autotuner: times the batch with 1, 2 and 4 front-end streams (two runs each, the second timed) and keeps the
  * fastest for the handle; returns the choice and its time (ms). */
 int is_autotune_batch(is_handle *h, const is_frame *frames, int n, int from_host, int *front_streams, float *ms);
