@@ -25,6 +25,7 @@
 #include "is_tiny.cuh"
 #include "is_dp.cuh"
 #include "is_recon.cuh"
+#include "is_learn.cuh"
 
 using namespace is;
 
@@ -883,3 +884,4 @@ int is_times_get(const is_handle *h, is_times *t) {
 
 #include "is_testapi.cuh"
 #include "is_noalloc.cuh"
+#include "is_learn_api.cuh"

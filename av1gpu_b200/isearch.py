@@ -46,7 +46,8 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_record_copy", "is_record_device", "is_times_get", "is_test_fwd_quant", "is_test_inverse",
            "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32", "is_set_trace", "is_get_trace",
            "is_fwd_quant_static", "is_encode_batch", "is_batch_counts", "is_batch_copy", "is_set_batch_options",
-           "is_autotune_batch", "is_workspace_bytes"]
+           "is_autotune_batch", "is_workspace_bytes", "is_sl_create", "is_sl_destroy", "is_sl_set_weights",
+           "is_sl_get_weights", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset"]
 
 _lib = None
 
@@ -87,6 +88,16 @@ def load_library():
     L.is_batch_copy.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp * 3, vp]
     L.is_set_batch_options.argtypes = [vp, C.c_int, C.c_int, C.c_int]
     L.is_workspace_bytes.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64)]
+    L.is_sl_create.argtypes = [C.c_int, C.c_int, C.POINTER(vp)]
+    L.is_sl_destroy.argtypes = [vp]
+    L.is_sl_destroy.restype = None
+    L.is_sl_set_weights.argtypes = [vp, vp, vp, vp, vp]
+    L.is_sl_get_weights.argtypes = [vp, vp, vp, vp, vp]
+    L.is_sl_forward.argtypes = [vp, vp, C.c_int, vp, vp]
+    L.is_sl_grads.argtypes = [vp, vp, vp, C.c_int, vp, C.POINTER(C.c_float), C.POINTER(C.c_int)]
+    L.is_sl_train_step.argtypes = [vp, vp, vp, C.c_int, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_int)]
+    L.is_nn_gemm.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, vp]
+    L.is_sl_dataset.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int)]
     L.is_autotune_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
     _lib = L
     return L

@@ -130,6 +130,32 @@ int is_debug_tables(is_handle *h, int qctx, uint16_t *cost, size_t cap, int32_t 
 int is_set_trace(is_handle *h, int on);
 int is_get_trace(is_handle *h, unsigned long long *out, size_t cap, uint32_t *n);
 
+/* ---- learned mode shortlist: a 288 -> 128 (ReLU) -> 16 network over per-block features, trained on the GPU with
+ * the library's BF16 tensor-core kernels on labels the exhaustive search produces (no counterpart in the reference:
+ * its open-loop shortlists are hand-made, encoder/src/k_an_x.cu; the survey's ABI suggestion is is_set_shortlist_model)
+ * Features: a 16x16 luma patch resampled from the block (mean removed, / 64), an 8-bin gradient orientation histogram,
+ * the block shape one-hot (22), qindex / 255, 1.  Weights are fp32, row-major [out][in]: w1 128 x 288, b1 128,
+ * w2 16 x 128, b2 16 (scores 13 .. 15 unused). */
+typedef struct is_learner is_learner;
+int is_sl_create(int device, int max_batch, is_learner **out);   /* max_batch: a multiple of 32 */
+void is_sl_destroy(is_learner *L);
+int is_sl_set_weights(is_learner *L, const float *w1, const float *b1, const float *w2, const float *b2);
+int is_sl_get_weights(is_learner *L, float *w1, float *b1, float *w2, float *b2);
+/* scores (device, n x 16 fp32) of n feature rows (device bf16, n x 288) */
+int is_sl_forward(is_learner *L, const void *X, int n, float *S, void *stream);
+/* gradients of the mean softmax cross-entropy over the 13 modes (host, w1 | b1 | w2 | b2), loss and correct count of
+ * one batch (n a multiple of 32, device X / y), weights unchanged */
+int is_sl_grads(is_learner *L, const void *X, const int32_t *y, int n, float *grads, float *loss, int *correct);
+/* one Adam step (lr; beta 0.9 / 0.999) on a batch; the batch's mean loss and correct count */
+int is_sl_train_step(is_learner *L, const void *X, const int32_t *y, int n, float lr, float *loss, int *correct);
+/* C[M x N] = A[M x K] B[N x K]^T (+ bias, ReLU) on device bf16 operands, fp32 out (K, lda, ldb multiples of 8) */
+int is_nn_gemm(int M, int N, int K, const void *A, int lda, const void *B, int ldb, float *C, int ldc, const float *bias,
+               int relu, void *stream);
+/* training data of image i of the last search: features (device bf16, n x 288) and labels (the analysis's best mode)
+ * of its analysed blocks into buffers of capacity cap; *n = the number of blocks (also when it exceeds cap: then
+ * nothing is written) */
+int is_sl_dataset(is_handle *h, int i, void *X, int32_t *y, int cap, int *n);
+
 /* INT32 issue-rate probe: the measured INT32 instruction throughput of the device (Gop/s, multiply-add + logic chains
  * over every SM) and the best kernel time, the roofline denominator of this integer path. */
 int is_probe_int32(int device, double *gops, float *ms);
