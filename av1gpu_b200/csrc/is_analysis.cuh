@@ -115,23 +115,33 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
             __syncwarp();
         }
     };
+    // the modes screened: all 13, or the block's learned shortlist (in mode order, so ties still go to the lower mode)
+    const uint32_t recIdx = F.shOff[bs] + (uint32_t)(y / H) * F.shNbx[bs] + x / W;
+    const uint32_t mmask = F.slMask ? F.slMask[recIdx] : 0x1FFFu;
+    const int nm = __popc(mmask);
     S.satd[lane] = 0;
-    S.cand[lane] = lane < 13 ? cand_pack(lane, 0) : 0;
+    if (lane < 13 && ((mmask >> lane) & 1)) S.cand[__popc(mmask & ((1u << lane) - 1))] = cand_pack(lane, 0);
     __syncwarp();
-    screen(0, 13);
-    i64 js = lane < 13 ? ((i64)S.satd[lane] << 14) + F.sqlam * mbits(S.cand[lane]) : INF;
+    screen(0, nm);
+    i64 js = lane < nm ? ((i64)S.satd[lane] << 14) + F.sqlam * mbits(S.cand[lane]) : INF;
+    int nc = nm;
     if (bs >= AV1G_BLOCK_8X8) {
-        const i64 jd = (lane >= AV1G_V_PRED && lane <= AV1G_D67_PRED) ? js : INF;
-        const int b0 = warp_argmin(jd, lane);
-        const int b1 = warp_argmin(lane == b0 ? INF : jd, lane);
-        if (lane < 12) {
+        const i64 jd = (lane < nm && is_dir(cand_mode(S.cand[lane]))) ? js : INF;
+        const int l0 = warp_argmin(jd, lane);
+        const int l1 = warp_argmin(lane == l0 ? INF : jd, lane);
+        const int b0 = l0 >= 0 ? cand_mode(S.cand[l0]) : -1, b1 = l1 >= 0 ? cand_mode(S.cand[l1]) : -1;
+        const int nd = (b0 >= 0 ? 6 : 0) + (b1 >= 0 ? 6 : 0);   // 12 with the plain form's two directional modes
+        __syncwarp();
+        if (lane < nd) {
             const int m = lane < 6 ? b0 : b1, k = lane % 6;
-            S.cand[13 + lane] = cand_pack(m, k < 3 ? -(k + 1) : (k - 2));
+            S.cand[nm + lane] = cand_pack(m, k < 3 ? -(k + 1) : (k - 2));
         }
         __syncwarp();
-        screen(13, 25);
-        if (lane >= 13 && lane < 25) js = ((i64)S.satd[lane] << 14) + F.sqlam * mbits(S.cand[lane]);
+        screen(nm, nm + nd);
+        if (lane >= nm && lane < nm + nd) js = ((i64)S.satd[lane] << 14) + F.sqlam * mbits(S.cand[lane]);
+        nc = nm + nd;
     }
+    (void)nc;
     int top[K_TOP];
     int nK = 0;
 #pragma unroll

@@ -231,6 +231,16 @@ struct is_handle {
     int frontStreams = 1;                   // 1, 2 or 4 (is_autotune_batch chooses)
     int reconCtas = 0;                      // CTAs of the closed loop (0: one per SM); fewer leave SMs to other streams
     bool useGraph = false;
+    // learned shortlist (is_set_shortlist_model): bf16 weights, fp32 biases, mask rule; per front-end stream a chunk of
+    // features / hidden activations / scores
+    bool slOn = false;
+    __nv_bfloat16 *slW1 = nullptr, *slW2 = nullptr;
+    float *slB1 = nullptr, *slB2 = nullptr;
+    float slTau = 0.9f, slConf = 0.f;
+    int slMax = 6;
+    __nv_bfloat16 *slX[4] = {nullptr, nullptr, nullptr, nullptr}, *slH[4] = {nullptr, nullptr, nullptr, nullptr};
+    float *slS[4] = {nullptr, nullptr, nullptr, nullptr};
+    int slVersion = 0;
     std::string graphKey;
     cudaGraphExec_t graphExec = nullptr;
     int setErr(int code, const char *fmt, ...) {
@@ -364,6 +374,8 @@ size_t layout(int W, int H, uint8_t *base, FrameDesc &F, int &nSb) {
         off += (uint32_t)(F.shNbx[s] * F.shNby[s]);
     }
     F.blk = (BlockRes *)take((size_t)off * sizeof(BlockRes));
+    F.nRec = off;
+    F.slMask = (uint16_t *)take((size_t)off * 2);   // kept only while a shortlist model is set (prepare_batch)
     F.leaves = (Leaf *)take((size_t)nSb * SB_MAX_LEAVES * sizeof(Leaf));
     F.nLeaves = (uint16_t *)take((size_t)nSb * 2);
     F.oBlocks = (av1g_block *)take((size_t)nSb * SB_MAX_LEAVES * sizeof(av1g_block));
@@ -457,6 +469,10 @@ void is_destroy(is_handle *h) {
     }
     if (h->evFork) cudaEventDestroy(h->evFork);
     if (h->hFs) cudaFreeHost(h->hFs);
+    void *sl[] = {h->slW1, h->slW2, h->slB1, h->slB2, h->slX[0], h->slX[1], h->slX[2], h->slX[3], h->slH[0], h->slH[1], h->slH[2],
+                  h->slH[3], h->slS[0], h->slS[1], h->slS[2], h->slS[3]};
+    for (void *p : sl)
+        if (p) cudaFree(p);
     if (h->hOrd) cudaFreeHost(h->hOrd);
     if (h->hCnt) cudaFreeHost(h->hCnt);
     delete h;
@@ -570,6 +586,7 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         F.err = h->bErr;
         F.img = i;
         F.leafTrace = (h->trace && i == 0) ? h->traceBuf : nullptr;
+        if (!h->slOn) F.slMask = nullptr;
         sb_orders(F, cs, rs, h->hOrd + o, h->hOrd + o + ns);
         o += 2 * (size_t)ns;
         h->hFs[i] = F;
@@ -618,6 +635,19 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
             k_pad<uint8_t><<<dim3(1, ph), 128, 0, s>>>(dst, F.spitch[p], vw, vh, pw, ph);
         }
         if (events && n == 1) IS_CK(cudaEventRecord(h->ev[1], s));
+        if (h->slOn) {   // the learned shortlist: scores of every analysis record, then its mode mask
+            const int k = K > 1 ? i % K : 0;
+            for (uint32_t i0 = 0; i0 < F.nRec; i0 += SL_CHUNK) {
+                const int cn = (int)std::min<uint32_t>(SL_CHUNK, F.nRec - i0);
+                k_sl_features_rec<<<(cn + 7) / 8, 256, 0, s>>>(F, i0, cn, h->slX[k]);
+                k_gemm_abt<<<dim3((SL_HID + GT_N - 1) / GT_N, (cn + GT_M - 1) / GT_M), 128, 0, s>>>(
+                    cn, SL_HID, SL_IN, h->slX[k], SL_IN, h->slW1, SL_IN, nullptr, 0, h->slB1, 1, h->slH[k], SL_HID);
+                k_gemm_abt<<<dim3(1, (cn + GT_M - 1) / GT_M), 128, 0, s>>>(cn, SL_OUT, SL_HID, h->slH[k], SL_HID, h->slW2, SL_HID,
+                                                                          h->slS[k], SL_OUT, h->slB2, 0, nullptr, 0);
+                k_sl_mask<<<(cn + 127) / 128, 128, 0, s>>>(cn, h->slS[k], h->slTau, h->slMax, h->slConf, F.slMask + i0);
+            }
+            IS_CK(cudaGetLastError());
+        }
         k_analysis_big<8><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig, s>>>(F);
         k_analysis<8><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn, s>>>(F);
         k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem), s>>>(F);
@@ -677,7 +707,7 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
 static std::string batch_key(const is_handle *h, const is_frame *fr, int n, bool fromHost) {
     std::string k;
     char b[160];
-    snprintf(b, sizeof b, "%p|%d|%d|%d|%d|", h->arena, n, (int)fromHost, h->frontStreams, h->reconCtas);
+    snprintf(b, sizeof b, "%p|%d|%d|%d|%d|%d|", h->arena, n, (int)fromHost, h->frontStreams, h->reconCtas, h->slOn ? h->slVersion : -1);
     k += b;
     for (int i = 0; i < n; i++) {
         snprintf(b, sizeof b, "%d,%d,%d,%p,%p,%p,%d,%d,%d;", fr[i].width, fr[i].height, fr[i].qindex, fr[i].planes[0], fr[i].planes[1],
@@ -791,6 +821,39 @@ int is_set_batch_options(is_handle *h, int use_graph, int front_streams, int rec
     if (front_streams) h->frontStreams = front_streams;
     h->reconCtas = recon_ctas;
     if (!h->useGraph && h->graphExec) { cudaGraphExecDestroy(h->graphExec); h->graphExec = nullptr; h->graphKey.clear(); }
+    return IS_OK;
+}
+
+int is_set_shortlist_model(is_handle *h, const float *w1, const float *b1, const float *w2, const float *b2, float tau, int max_modes,
+                           float conf) {
+    if (!h) return IS_ERR_INVALID;
+    IS_CK(cudaSetDevice(h->device));
+    if (!w1) { h->slOn = false; return IS_OK; }
+    if (!b1 || !w2 || !b2 || max_modes < 0 || max_modes > 13 || !(tau > 0.f) || tau > 1.f) return h->setErr(IS_ERR_INVALID, "invalid shortlist model");
+    IS_CK(cudaStreamSynchronize(h->own));
+    if (!h->slW1) {
+        IS_CK(cudaMalloc(&h->slW1, (size_t)SL_HID * SL_IN * 2));
+        IS_CK(cudaMalloc(&h->slW2, (size_t)SL_OUT * SL_HID * 2));
+        IS_CK(cudaMalloc(&h->slB1, SL_HID * 4));
+        IS_CK(cudaMalloc(&h->slB2, SL_OUT * 4));
+        for (int k = 0; k < 4; k++) {
+            IS_CK(cudaMalloc(&h->slX[k], (size_t)SL_CHUNK * SL_IN * 2));
+            IS_CK(cudaMalloc(&h->slH[k], (size_t)SL_CHUNK * SL_HID * 2));
+            IS_CK(cudaMalloc(&h->slS[k], (size_t)SL_CHUNK * SL_OUT * 4));
+        }
+    }
+    std::vector<__nv_bfloat16> a((size_t)SL_HID * SL_IN), c((size_t)SL_OUT * SL_HID);
+    for (size_t k = 0; k < a.size(); k++) a[k] = __float2bfloat16(w1[k]);
+    for (size_t k = 0; k < c.size(); k++) c[k] = __float2bfloat16(w2[k]);
+    IS_CK(cudaMemcpy(h->slW1, a.data(), a.size() * 2, cudaMemcpyHostToDevice));
+    IS_CK(cudaMemcpy(h->slW2, c.data(), c.size() * 2, cudaMemcpyHostToDevice));
+    IS_CK(cudaMemcpy(h->slB1, b1, SL_HID * 4, cudaMemcpyHostToDevice));
+    IS_CK(cudaMemcpy(h->slB2, b2, SL_OUT * 4, cudaMemcpyHostToDevice));
+    h->slTau = tau;
+    h->slMax = max_modes;
+    h->slConf = conf;
+    h->slOn = true;
+    h->slVersion++;
     return IS_OK;
 }
 

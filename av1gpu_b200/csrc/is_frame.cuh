@@ -42,6 +42,8 @@ struct __align__(16) FrameDesc {
     int rpitch[3];
     uint8_t *mYMode, *cLvl[3], *cDc[3];
     BlockRes *blk;
+    uint32_t nRec;                            // analysis records (all shapes)
+    uint16_t *slMask;                         // [nRec] shortlist: modes to screen per record (bit m: mode m); null: all
     uint32_t shOff[22];
     int shNbx[22], shNby[22];
     long long lam, sqlam;                     // lambda, sqrt(lambda) in 1/256

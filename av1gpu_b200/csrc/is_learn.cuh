@@ -11,6 +11,7 @@
 namespace is {
 
 constexpr int SL_IN = 288, SL_HID = 128, SL_OUT = 16, SL_MODES = 13;
+constexpr uint32_t SL_CHUNK = 65536;   // analysis records scored per inference pass of the search
 
 // ---- C[M x N] (fp32, row stride ldc) = A[M x K] . B[N x K]^T (+ bias[N]) (ReLU if relu); optional bf16 copy ----
 // CTA tile 64 x 64, 4 warps each 32 x 32 (2 x 4 mma tiles of 16 x 8), K step 32 staged in shared memory.
@@ -119,15 +120,12 @@ namespace is {
 // the shape one-hot (22), qindex / 255, 1 ----
 struct SlBlock { uint8_t bs, x4, y4, pad; uint32_t sb; };   // block of shape bs at SB sb, 4x4-unit offset (x4, y4)
 
-__global__ void k_sl_features(const FrameDesc F, const SlBlock *__restrict__ blocks, int n, __nv_bfloat16 *__restrict__ X) {
-    const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (b >= n) return;
-    const SlBlock bl = blocks[b];
-    const int W = 4 * ST(Num_4x4_Blocks_Wide)[bl.bs], H = 4 * ST(Num_4x4_Blocks_High)[bl.bs];
-    const int x = (bl.sb % F.sbCols) * 64 + bl.x4 * 4, y = (bl.sb / F.sbCols) * 64 + bl.y4 * 4;
+// the features of a block of shape bs at (x, y) into out[288], by one warp
+__device__ __forceinline__ void sl_features_of(const FrameDesc &F, int bs, int x, int y, __nv_bfloat16 *out) {
+    const int lane = threadIdx.x & 31;
+    const int W = 4 * ST(Num_4x4_Blocks_Wide)[bs], H = 4 * ST(Num_4x4_Blocks_High)[bs];
     const uint8_t *src = F.src[0];
     const int sp = F.spitch[0];
-    __nv_bfloat16 *out = X + (size_t)b * SL_IN;
     // the patch: lane handles 8 of the 256 cells
     float cell[8], sum = 0.f;
     const int sw = max(W / 16, 1), sh = max(H / 16, 1);
@@ -177,9 +175,47 @@ __global__ void k_sl_features(const FrameDesc F, const SlBlock *__restrict__ blo
         for (int q = 0; q < 8; q++) hv = q == lane ? hist[q] : hv;
         out[256 + lane] = __float2bfloat16(hv / (tot + 1.f));
     }
-    if (lane < 22) out[264 + lane] = __float2bfloat16(lane == bl.bs ? 1.f : 0.f);
+    if (lane < 22) out[264 + lane] = __float2bfloat16(lane == bs ? 1.f : 0.f);
     if (lane == 22) out[286] = __float2bfloat16((float)F.qidx / 255.f);
     if (lane == 23) out[287] = __float2bfloat16(1.f);
+}
+
+// features of a list of blocks (training data), one warp per block
+__global__ void k_sl_features(const FrameDesc F, const SlBlock *__restrict__ blocks, int n, __nv_bfloat16 *__restrict__ X) {
+    const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (b >= n) return;
+    const SlBlock bl = blocks[b];
+    sl_features_of(F, bl.bs, (bl.sb % F.sbCols) * 64 + bl.x4 * 4, (bl.sb / F.sbCols) * 64 + bl.y4 * 4, X + (size_t)b * SL_IN);
+}
+
+// the analysis record (shape, position) of record index i; false when i is out of range or the block lies outside the
+// frame
+__device__ __forceinline__ bool sl_record_block(const FrameDesc &F, uint32_t i, int &bs, int &x, int &y) {
+    bs = -1;
+#pragma unroll 1
+    for (int s = 0; s < 22; s++) {
+        if (s >= 13 && s <= 15) continue;
+        const uint32_t n = (uint32_t)F.shNbx[s] * (uint32_t)F.shNby[s];
+        if (i >= F.shOff[s] && i < F.shOff[s] + n) { bs = s; break; }
+    }
+    if (bs < 0) return false;
+    const uint32_t k = i - F.shOff[bs];
+    x = (int)(k % (uint32_t)F.shNbx[bs]) * 4 * ST(Num_4x4_Blocks_Wide)[bs];
+    y = (int)(k / (uint32_t)F.shNbx[bs]) * 4 * ST(Num_4x4_Blocks_High)[bs];
+    return x < F.MiCols * 4 && y < F.MiRows * 4;
+}
+
+// features of the analysis records [i0, i0 + n) (zero rows for blocks outside the frame), one warp per record
+__global__ void k_sl_features_rec(const FrameDesc F, uint32_t i0, int n, __nv_bfloat16 *__restrict__ X) {
+    const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (r >= n) return;
+    int bs, x, y;
+    __nv_bfloat16 *out = X + (size_t)r * SL_IN;
+    if (sl_record_block(F, i0 + r, bs, x, y)) {
+        sl_features_of(F, bs, x, y, out);
+    } else {
+        for (int k = lane; k < SL_IN; k += 32) out[k] = __float2bfloat16(0.f);
+    }
 }
 
 // ---- softmax cross-entropy over the first SL_MODES of SL_OUT scores: loss sum (atomic) and dS = (p - onehot) / n
@@ -242,6 +278,7 @@ __global__ void k_adam(int n, float *__restrict__ p, const float *__restrict__ g
 __global__ void k_sl_mask(int n, const float *__restrict__ S, float tau, int maxModes, float conf, uint16_t *__restrict__ mask) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
+    if (maxModes <= 0) { mask[r] = 0x1FFF; return; }
     const float *s = S + (size_t)r * SL_OUT;
     float p[SL_MODES], mx = s[0], z = 0.f;
     for (int k = 1; k < SL_MODES; k++) mx = fmaxf(mx, s[k]);

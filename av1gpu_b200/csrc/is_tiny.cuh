@@ -293,8 +293,12 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
     uint32_t topP[4][N / 4];
 #pragma unroll
     for (int k = 0; k < 4; k++) { topJ[k] = INF; topM[k] = 0; }
+    // the modes screened: all 13, or the block's learned shortlist; a mode no thread of the warp screens is skipped
+    const uint32_t mmask = F.slMask ? F.slMask[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] : 0x1FFFu;
     auto screen = [&](auto modeTag) {
         constexpr int M = decltype(modeTag)::value;
+        const bool need = (mmask >> M) & 1;
+        if (!__any_sync(__activemask(), need)) return;
         int p[N];
         tpred<W, H, M>(A, L, dcv, p);
         int satd = 0;
@@ -313,8 +317,8 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
         uint32_t pk[N / 4];
 #pragma unroll
         for (int k = 0; k < N / 4; k++) pk[k] = (uint32_t)p[4 * k] | ((uint32_t)p[4 * k + 1] << 8) | ((uint32_t)p[4 * k + 2] << 16) | ((uint32_t)p[4 * k + 3] << 24);
-        // insertion: after every kept entry of cost <= js (the earlier candidate wins a tie)
-        const int pos = (topJ[0] <= js) + (topJ[1] <= js) + (topJ[2] <= js) + (topJ[3] <= js);
+        // insertion: after every kept entry of cost <= js (the earlier candidate wins a tie); none for a mode off the list
+        const int pos = need ? (topJ[0] <= js) + (topJ[1] <= js) + (topJ[2] <= js) + (topJ[3] <= js) : 4;
 #pragma unroll
         for (int s = 3; s >= 0; s--) {
             if (s > pos) {
@@ -359,6 +363,7 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
     int bestK = 0, bestTx = AV1G_DCT_DCT;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
+        if (topJ[k] == INF) continue;   // fewer than 4 modes screened (shortlist)
         const i64 j = rd(topP[k], topM[k], AV1G_DCT_DCT);
         if (j < bestJ) { bestJ = j; bestK = k; }
     }
@@ -385,11 +390,12 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
     r.J = bestJ;
     r.tx = (uint8_t)bestTx;
     r.cand[0] = (uint8_t)cand_pack(wm, 0);
+    r.cand[1] = r.cand[2] = r.cand[3] = 0;
     int n = 1;
 #pragma unroll
     for (int k = 0; k < 4; k++)
-        if (k != bestK) r.cand[n++ & 3] = (uint8_t)cand_pack(topM[k], 0);
-    r.ncand = 4;
+        if (k != bestK && topJ[k] < INF) r.cand[n++ & 3] = (uint8_t)cand_pack(topM[k], 0);
+    r.ncand = (uint8_t)n;
     r.pad[0] = r.pad[1] = 0;
     F.blk[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] = r;
 }
@@ -567,8 +573,10 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
     int b0 = AV1G_V_PRED, b1 = AV1G_V_PRED;
     i64 bestJ = INF;
     int bestK = 0, bestTx = AV1G_DCT_DCT, winC = 0;
+    // the modes screened: all 13, or the block's learned shortlist
+    const uint32_t mmask = F.slMask ? F.slMask[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] : 0x1FFFu;
     // jobs: 0-12 the 13 modes, 13-24 the deltas of the two best directional modes (SATD); 25-28 the top 4 with
-    // DCT_DCT, 29-34 the other types of TX_SET_INTRA_1 for the winner (RD)
+    // DCT_DCT, 29-34 the other types of TX_SET_INTRA_1 for the winner (RD); a job no thread of the warp needs is skipped
 #pragma unroll 1
     for (int job = 0; job < 35; job++) {
         int c, t = AV1G_DCT_DCT;
@@ -587,6 +595,9 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
             const int k = job - 29;   // ADST_DCT, DCT_ADST, ADST_ADST, IDTX, V_DCT, H_DCT
             t = k < 3 ? k + 1 : k + 6;
         }
+        const bool need = job < 13 ? ((mmask >> job) & 1) != 0 : job < 25 ? ((job - 13 < 6) ? dJ0 < INF : dJ1 < INF)
+                         : job < 29 ? topJ[job - 25] < INF : true;
+        if (!__any_sync(__activemask(), need)) continue;
         const int m = cand_mode(c), pa = pangle(m, cand_delta(c));
         // the prediction, one 4x4 sub-block at a time (one copy of the predictor): SATD of the residual while screening,
         // the prediction into the thread's slot for an RD task
@@ -611,13 +622,13 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
         }
         if (job < 25) {
             const i64 js = ((i64)satd << 14) + F.sqlam * mbits(c);
-            const int pos = (topJ[0] <= js) + (topJ[1] <= js) + (topJ[2] <= js) + (topJ[3] <= js);
+            const int pos = need ? (topJ[0] <= js) + (topJ[1] <= js) + (topJ[2] <= js) + (topJ[3] <= js) : 4;
 #pragma unroll
             for (int s = 3; s >= 0; s--) {
                 if (s > pos) { topJ[s] = topJ[s > 0 ? s - 1 : 0]; topC[s] = topC[s > 0 ? s - 1 : 0]; }
                 else if (s == pos) { topJ[s] = js; topC[s] = c; }
             }
-            if (job >= AV1G_V_PRED && job <= AV1G_D67_PRED) {   // the two best directional modes (first of equals)
+            if (need && job >= AV1G_V_PRED && job <= AV1G_D67_PRED) {   // the two best directional modes (first of equals)
                 if (js < dJ0) { dJ1 = dJ0; b1 = b0; dJ0 = js; b0 = job; }
                 else if (js < dJ1) { dJ1 = js; b1 = job; }
             }
@@ -630,7 +641,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
             const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, T};
             const EvalOut o = mid_eval<BD, LW, LH>(txSz, res, e, iscan, 64, qs);
             const i64 J = o.D + F.lam * (o.R + mbits(c) + overhead);
-            if (J < bestJ) {
+            if (need && J < bestJ) {
                 bestJ = J;
                 if (job < 29) { bestK = job - 25; winC = c; }
                 else bestTx = t;
@@ -641,11 +652,12 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
     r.J = bestJ;
     r.tx = (uint8_t)bestTx;
     r.cand[0] = (uint8_t)winC;
+    r.cand[1] = r.cand[2] = r.cand[3] = 0;
     int n = 1;
 #pragma unroll
     for (int k = 0; k < 4; k++)
-        if (k != bestK) r.cand[n++ & 3] = (uint8_t)topC[k];
-    r.ncand = 4;
+        if (k != bestK && topJ[k] < INF) r.cand[n++ & 3] = (uint8_t)topC[k];
+    r.ncand = (uint8_t)n;
     r.pad[0] = r.pad[1] = 0;
     F.blk[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] = r;
 }

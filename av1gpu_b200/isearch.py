@@ -47,7 +47,7 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32", "is_set_trace", "is_get_trace",
            "is_fwd_quant_static", "is_encode_batch", "is_batch_counts", "is_batch_copy", "is_set_batch_options",
            "is_autotune_batch", "is_workspace_bytes", "is_sl_create", "is_sl_destroy", "is_sl_set_weights",
-           "is_sl_get_weights", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset"]
+           "is_sl_get_weights", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset", "is_set_shortlist_model"]
 
 _lib = None
 
@@ -98,6 +98,7 @@ def load_library():
     L.is_sl_train_step.argtypes = [vp, vp, vp, C.c_int, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_int)]
     L.is_nn_gemm.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, vp]
     L.is_sl_dataset.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int)]
+    L.is_set_shortlist_model.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_int, C.c_float]
     L.is_autotune_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
     _lib = L
     return L
@@ -277,6 +278,16 @@ class Encoder:
     def set_batch_options(self, use_graph=False, front_streams=0, recon_ctas=0):
         self._check(self.L.is_set_batch_options(self.h, 1 if use_graph else 0, front_streams, recon_ctas),
                     "is_set_batch_options")
+
+    def set_shortlist(self, weights=None, tau=0.9, max_modes=6, conf=0.0):
+        """Use a trained shortlist network (w1, b1, w2, b2 fp32) in this handle's searches; None: the plain form."""
+        if weights is None:
+            self._check(self.L.is_set_shortlist_model(self.h, None, None, None, None, C.c_float(1.0), 0, C.c_float(0.0)),
+                        "is_set_shortlist_model")
+            return
+        w = [np.ascontiguousarray(a, np.float32) for a in weights]
+        self._check(self.L.is_set_shortlist_model(self.h, *[a.ctypes.data for a in w], C.c_float(tau), max_modes,
+                                                  C.c_float(conf)), "is_set_shortlist_model")
 
     def autotune_batch(self, images, qindices, host=True):
         """Time the batch with 1 / 2 / 4 front-end streams and keep the fastest; returns (streams, ms)."""

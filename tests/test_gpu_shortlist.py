@@ -82,3 +82,32 @@ def test_training_lowers_the_loss(enc):
         lr.close()
     assert hist[-1][0] < hist[0][0] * 0.9
     assert ev["coverage"] > ev["top1"] and ev["mean_modes"] <= 6
+
+
+def test_search_with_full_masks_equals_plain(enc):
+    im = synth.make_image(211, 149, 43, edges=True)
+    plain = enc.encode(im, 120)
+    enc.set_shortlist(SL.init_weights(1), tau=0.9, max_modes=0)   # every mask full: the plain form
+    try:
+        same = enc.encode(im, 120)
+    finally:
+        enc.set_shortlist(None)
+    assert np.array_equal(plain.blocks.view(np.uint8), same.blocks.view(np.uint8))
+    assert np.array_equal(plain.coeffs, same.coeffs)
+
+
+def test_search_with_shortlist_is_exact_and_deterministic(enc):
+    import oracle as O
+    w, h, q = 256, 160, 120
+    im = synth.make_image(w, h, 44, edges=True)
+    enc.set_shortlist(SL.init_weights(2), tau=0.6, max_modes=3)   # untrained net: arbitrary small mode sets
+    try:
+        a = enc.encode(im, q)
+        b = enc.encode(im, q)
+    finally:
+        enc.set_shortlist(None)
+    assert np.array_equal(a.blocks.view(np.uint8), b.blocks.view(np.uint8)) and np.array_equal(a.coeffs, b.coeffs)
+    rec, nbytes = O.av1g_recon(w, h, q, a.blocks, a.block_txb, a.txb, a.coeffs)
+    for p in range(3):
+        assert np.array_equal(rec[p], a.recon[p])
+    assert nbytes > 0
