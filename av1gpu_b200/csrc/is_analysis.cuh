@@ -144,10 +144,11 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
     (void)nc;
     int top[K_TOP];
     int nK = 0;
+    const int kMax = mmask != 0x1FFFu ? F.slRdK : K_TOP;   // a shortlisted block: its best slRdK candidates only
 #pragma unroll
     for (int k = 0; k < K_TOP; k++) {
         top[k] = warp_argmin(js, lane);
-        if (top[k] >= 0) nK = k + 1;
+        if (top[k] >= 0 && k < kMax) nK = k + 1;
         if (lane == top[k]) js = INF;
     }
     // ---- RD: the top-K with DCT_DCT, then the other types of the set for the winner; 32 / G tasks at a time, the

@@ -237,7 +237,7 @@ struct is_handle {
     __nv_bfloat16 *slW1 = nullptr, *slW2 = nullptr;
     float *slB1 = nullptr, *slB2 = nullptr;
     float slTau = 0.9f, slConf = 0.f;
-    int slMax = 6;
+    int slMax = 6, slRdK = 4;
     __nv_bfloat16 *slX[4] = {nullptr, nullptr, nullptr, nullptr}, *slH[4] = {nullptr, nullptr, nullptr, nullptr};
     float *slS[4] = {nullptr, nullptr, nullptr, nullptr};
     int slVersion = 0;
@@ -587,6 +587,7 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         F.img = i;
         F.leafTrace = (h->trace && i == 0) ? h->traceBuf : nullptr;
         if (!h->slOn) F.slMask = nullptr;
+        F.slRdK = h->slOn ? h->slRdK : 4;
         sb_orders(F, cs, rs, h->hOrd + o, h->hOrd + o + ns);
         o += 2 * (size_t)ns;
         h->hFs[i] = F;
@@ -825,11 +826,12 @@ int is_set_batch_options(is_handle *h, int use_graph, int front_streams, int rec
 }
 
 int is_set_shortlist_model(is_handle *h, const float *w1, const float *b1, const float *w2, const float *b2, float tau, int max_modes,
-                           float conf) {
+                           float conf, int rd_k) {
     if (!h) return IS_ERR_INVALID;
     IS_CK(cudaSetDevice(h->device));
     if (!w1) { h->slOn = false; return IS_OK; }
-    if (!b1 || !w2 || !b2 || max_modes < 0 || max_modes > 13 || !(tau > 0.f) || tau > 1.f) return h->setErr(IS_ERR_INVALID, "invalid shortlist model");
+    if (!b1 || !w2 || !b2 || max_modes < 0 || max_modes > 13 || !(tau > 0.f) || tau > 1.f || rd_k < 1 || rd_k > 4)
+        return h->setErr(IS_ERR_INVALID, "invalid shortlist model");
     IS_CK(cudaStreamSynchronize(h->own));
     if (!h->slW1) {
         IS_CK(cudaMalloc(&h->slW1, (size_t)SL_HID * SL_IN * 2));
@@ -852,6 +854,7 @@ int is_set_shortlist_model(is_handle *h, const float *w1, const float *b1, const
     h->slTau = tau;
     h->slMax = max_modes;
     h->slConf = conf;
+    h->slRdK = rd_k;
     h->slOn = true;
     h->slVersion++;
     return IS_OK;

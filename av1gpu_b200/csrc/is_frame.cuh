@@ -44,6 +44,7 @@ struct __align__(16) FrameDesc {
     BlockRes *blk;
     uint32_t nRec;                            // analysis records (all shapes)
     uint16_t *slMask;                         // [nRec] shortlist: modes to screen per record (bit m: mode m); null: all
+    int slRdK;                                // shortlist: RD candidates of a block whose list is not all 13 modes
     uint32_t shOff[22];
     int shNbx[22], shNby[22];
     long long lam, sqlam;                     // lambda, sqrt(lambda) in 1/256

@@ -362,8 +362,9 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
     i64 bestJ = INF;
     int bestK = 0, bestTx = AV1G_DCT_DCT;
 #pragma unroll
+    const int kMax = mmask != 0x1FFFu ? F.slRdK : 4;   // a shortlisted block: its best slRdK candidates only
     for (int k = 0; k < 4; k++) {
-        if (topJ[k] == INF) continue;   // fewer than 4 modes screened (shortlist)
+        if (topJ[k] == INF || k >= kMax) continue;   // fewer candidates screened or taken (shortlist)
         const i64 j = rd(topP[k], topM[k], AV1G_DCT_DCT);
         if (j < bestJ) { bestJ = j; bestK = k; }
     }
@@ -394,7 +395,7 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
     int n = 1;
 #pragma unroll
     for (int k = 0; k < 4; k++)
-        if (k != bestK && topJ[k] < INF) r.cand[n++ & 3] = (uint8_t)cand_pack(topM[k], 0);
+        if (k != bestK && topJ[k] < INF && k < kMax) r.cand[n++ & 3] = (uint8_t)cand_pack(topM[k], 0);
     r.ncand = (uint8_t)n;
     r.pad[0] = r.pad[1] = 0;
     F.blk[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] = r;
@@ -575,6 +576,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
     int bestK = 0, bestTx = AV1G_DCT_DCT, winC = 0;
     // the modes screened: all 13, or the block's learned shortlist
     const uint32_t mmask = F.slMask ? F.slMask[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] : 0x1FFFu;
+    const int kMax = mmask != 0x1FFFu ? F.slRdK : 4;   // a shortlisted block: its best slRdK candidates only
     // jobs: 0-12 the 13 modes, 13-24 the deltas of the two best directional modes (SATD); 25-28 the top 4 with
     // DCT_DCT, 29-34 the other types of TX_SET_INTRA_1 for the winner (RD); a job no thread of the warp needs is skipped
 #pragma unroll 1
@@ -596,7 +598,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
             t = k < 3 ? k + 1 : k + 6;
         }
         const bool need = job < 13 ? ((mmask >> job) & 1) != 0 : job < 25 ? ((job - 13 < 6) ? dJ0 < INF : dJ1 < INF)
-                         : job < 29 ? topJ[job - 25] < INF : true;
+                         : job < 29 ? (topJ[job - 25] < INF && job - 25 < kMax) : true;
         if (!__any_sync(__activemask(), need)) continue;
         const int m = cand_mode(c), pa = pangle(m, cand_delta(c));
         // the prediction, one 4x4 sub-block at a time (one copy of the predictor): SATD of the residual while screening,
@@ -656,7 +658,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
     int n = 1;
 #pragma unroll
     for (int k = 0; k < 4; k++)
-        if (k != bestK && topJ[k] < INF) r.cand[n++ & 3] = (uint8_t)topC[k];
+        if (k != bestK && topJ[k] < INF && k < kMax) r.cand[n++ & 3] = (uint8_t)topC[k];
     r.ncand = (uint8_t)n;
     r.pad[0] = r.pad[1] = 0;
     F.blk[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] = r;

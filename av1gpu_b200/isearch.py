@@ -98,7 +98,7 @@ def load_library():
     L.is_sl_train_step.argtypes = [vp, vp, vp, C.c_int, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_int)]
     L.is_nn_gemm.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, vp]
     L.is_sl_dataset.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int)]
-    L.is_set_shortlist_model.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_int, C.c_float]
+    L.is_set_shortlist_model.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_int, C.c_float, C.c_int]
     L.is_autotune_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
     _lib = L
     return L
@@ -279,15 +279,15 @@ class Encoder:
         self._check(self.L.is_set_batch_options(self.h, 1 if use_graph else 0, front_streams, recon_ctas),
                     "is_set_batch_options")
 
-    def set_shortlist(self, weights=None, tau=0.9, max_modes=6, conf=0.0):
+    def set_shortlist(self, weights=None, tau=0.9, max_modes=6, conf=0.0, rd_k=4):
         """Use a trained shortlist network (w1, b1, w2, b2 fp32) in this handle's searches; None: the plain form."""
         if weights is None:
-            self._check(self.L.is_set_shortlist_model(self.h, None, None, None, None, C.c_float(1.0), 0, C.c_float(0.0)),
+            self._check(self.L.is_set_shortlist_model(self.h, None, None, None, None, C.c_float(1.0), 0, C.c_float(0.0), 4),
                         "is_set_shortlist_model")
             return
         w = [np.ascontiguousarray(a, np.float32) for a in weights]
         self._check(self.L.is_set_shortlist_model(self.h, *[a.ctypes.data for a in w], C.c_float(tau), max_modes,
-                                                  C.c_float(conf)), "is_set_shortlist_model")
+                                                  C.c_float(conf), rd_k), "is_set_shortlist_model")
 
     def autotune_batch(self, images, qindices, host=True):
         """Time the batch with 1 / 2 / 4 front-end streams and keep the fastest; returns (streams, ms)."""

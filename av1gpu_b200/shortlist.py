@@ -148,3 +148,70 @@ def evaluate(learner, X, y, tau=0.9, max_modes=6, conf=0.0):
         size += int(mask.sum())
         n += Xb.shape[0]
     return {"top1": accs / n, "coverage": cover / n, "mean_modes": size / n}
+
+
+def bd_rate(rate_a, q_a, rate_b, q_b):
+    """Bjontegaard delta rate (%) of curve b against curve a: the mean log-rate difference over the overlapping
+    quality range, log rate interpolated as a monotone (PCHIP) function of quality."""
+    from scipy.interpolate import PchipInterpolator
+    ra, qa = np.log(np.asarray(rate_a, np.float64)), np.asarray(q_a, np.float64)
+    rb, qb = np.log(np.asarray(rate_b, np.float64)), np.asarray(q_b, np.float64)
+    ia, ib = np.argsort(qa), np.argsort(qb)
+    fa, fb = PchipInterpolator(qa[ia], ra[ia]), PchipInterpolator(qb[ib], rb[ib])
+    lo, hi = max(qa.min(), qb.min()), min(qa.max(), qb.max())
+    if hi <= lo:
+        return float("nan")
+    xs = np.linspace(lo, hi, 256)
+    return float((np.exp(np.mean(fb(xs) - fa(xs))) - 1.0) * 100.0)
+
+
+def training_images(n, size, seed):
+    """n seeded synthetic training images (the generator of the workloads) with qindex uniform 40 .. 220."""
+    from . import synth
+    w, h = size
+    rng = np.random.default_rng(seed)
+    return [synth.make_image(w, h, seed * 1000 + i, edges=True) for i in range(n)], [int(q) for q in rng.integers(40, 221, n)]
+
+
+def main():
+    """python -m av1gpu_b200.shortlist --images 32 --size 512x384 --epochs 10 --out shortlist_weights.npz:
+    searches the training images with the plain form, trains the network on its choices, writes the weights."""
+    import argparse
+    import json
+    import torch
+    from .isearch import Encoder
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--images", type=int, default=32)
+    ap.add_argument("--size", default="512x384")
+    ap.add_argument("--epochs", type=int, default=10)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--out", default="shortlist_weights.npz")
+    args = ap.parse_args()
+    size = tuple(int(v) for v in args.size.split("x"))
+    enc = Encoder(0)
+    ims, qs = training_images(args.images, size, args.seed)
+    X, y = dataset(enc, ims, qs)
+    n_val = X.shape[0] // 10
+    perm = torch.randperm(X.shape[0], generator=torch.Generator().manual_seed(args.seed)).cuda()
+    Xv, yv, Xt, yt = X[perm[:n_val]], y[perm[:n_val]], X[perm[n_val:]], y[perm[n_val:]]
+    lrn = Learner(max_batch=4096)
+    lrn.set_weights(init_weights(args.seed))
+    hist = train(lrn, Xt, yt, epochs=args.epochs, batch=4096, lr=args.lr, seed=args.seed, log=print)
+    w = lrn.get_weights()
+    np.savez_compressed(args.out, w1=w[0], b1=w[1], w2=w[2], b2=w[3], images=args.images, size=np.array(size), epochs=args.epochs)
+    out = {"samples": int(X.shape[0]), "final_train": hist[-1]}
+    for tau, mm in ((0.8, 4), (0.9, 6), (0.95, 8)):
+        out["val_tau%.2f_max%d" % (tau, mm)] = evaluate(lrn, Xv, yv, tau=tau, max_modes=mm)
+    print(json.dumps(out))
+    lrn.close()
+    enc.close()
+
+
+def load_weights(path):
+    d = np.load(path)
+    return [d["w1"], d["b1"], d["w2"], d["b2"]]
+
+
+if __name__ == "__main__":
+    main()

@@ -157,12 +157,13 @@ int is_nn_gemm(int M, int N, int K, const void *A, int lda, const void *B, int l
 int is_sl_dataset(is_handle *h, int i, void *X, int32_t *y, int cap, int *n);
 
 /* Use a trained shortlist in the search of this handle (w1 NULL: the plain form again).  Each analysed block screens
- * only the smallest set of most probable modes whose probabilities add up to tau, at most max_modes; a block whose most
- * probable mode has probability below conf screens all 13 (the fallback); max_modes 0 keeps all 13 for every block
- * (results identical to the plain form).  Angle deltas follow the two best screened directional modes; the rest of the
+ * only the smallest set of most probable modes whose probabilities add up to tau, at most max_modes, and takes its best
+ * rd_k (1 .. 4) screened candidates into the exact-rate RD instead of 4; a block whose most probable mode has
+ * probability below conf screens all 13 with 4 RD candidates (the fallback); max_modes 0 keeps every block on the
+ * plain form (identical results).  Angle deltas follow the two best screened directional modes; the rest of the
  * search is unchanged and the reconstruction stays exact. */
 int is_set_shortlist_model(is_handle *h, const float *w1, const float *b1, const float *w2, const float *b2, float tau,
-                           int max_modes, float conf);
+                           int max_modes, float conf, int rd_k);
 
 /* INT32 issue-rate probe: the measured INT32 instruction throughput of the device (Gop/s, multiply-add + logic chains
  * over every SM) and the best kernel time, the roofline denominator of this integer path. */
