@@ -17,8 +17,8 @@ LIB = os.path.join(HERE, "libisearch.so")
 REF = os.environ.get("AV1GPU_REF", "/root/reference")
 AV1CORE_INCLUDE = os.environ.get("AV1CORE_INCLUDE", os.path.join(REF, "av1core", "include"))
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-SOURCES = ["is_api.cu", "is_dev.cuh", "is_frame.cuh", "is_analysis.cuh", "is_dp.cuh", "is_recon.cuh", "is_testapi.cuh",
-           "txfm_gen.cuh", "gen_txfm.py"]
+# every source of the library (a change to any of them rebuilds it)
+SOURCES = sorted(f for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".py")))
 
 
 def _newer(target, deps):

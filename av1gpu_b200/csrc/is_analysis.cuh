@@ -100,13 +100,7 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
             if (it < items) {
                 const int sb = it & (nsub - 1), sx = (sb & (nsx - 1)) * 4, sy = (sb >> lnsx) * 4;
                 const int c = S.cand[ci], m = cand_mode(c);
-                int d[16];
-                pred4(m, pangle(m, cand_delta(c)), sy, sx, lw, lh, A, L, dcv, d);
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-#pragma unroll
-                    for (int j = 0; j < 4; j++) d[i * 4 + j] = (int)src[(sy + i) * TW + sx + j] - d[i * 4 + j];
-                t = hadamard4_sum(d);
+                t = pred4_satd(m, pangle(m, cand_delta(c)), sy, sx, lw, lh, A, L, dcv, src, TW);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1)

@@ -365,9 +365,48 @@ __device__ __forceinline__ void pred4_inl(int mode, int pAng, int sy, int sx, in
             p[i * 4 + j] = (v + hz + (1 << (sh - 1))) >> sh;
         }
 }
+
+// 4x4 Hadamard: sum of |coefficients| (the reference's SATD proxy, 4 x the orthonormal SATD)
+__device__ __forceinline__ int hadamard4_sum(int *d) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int *r = d + 4 * i;
+        const int s0 = r[0] + r[1], s1 = r[0] - r[1], s2 = r[2] + r[3], s3 = r[2] - r[3];
+        r[0] = s0 + s2; r[1] = s1 + s3; r[2] = s0 - s2; r[3] = s1 - s3;
+    }
+    int sum = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int s0 = d[j] + d[4 + j], s1 = d[j] - d[4 + j], s2 = d[8 + j] + d[12 + j], s3 = d[8 + j] - d[12 + j];
+        sum += abs(s0 + s2) + abs(s1 + s3) + abs(s0 - s2) + abs(s1 - s3);
+    }
+    return sum;
+}
+
+// One 4x4 sub-block of a candidate's prediction (row sy, column sx of a W x H block), kept in registers: with out, it
+// is stored there (row stride W) and 0 returned; otherwise its SATD against src (row stride sp, the block's sample
+// (0, 0)) is returned.  The one out-of-line copy of the predictor serves both the screening and whole predictions.
+template <typename P, typename O>
+__device__ __noinline__ int pred4_x(int mode, int pAng, int sy, int sx, int lw, int lh, const P *A, const P *L, int dcv, const P *src, int sp,
+                                    O *out) {
+    int d[16];
+    pred4_inl(mode, pAng, sy, sx, lw, lh, A, L, dcv, d);
+    if (out) {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) out[((sy + i) << lw) + sx + j] = (O)d[i * 4 + j];
+        return 0;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) d[i * 4 + j] = (int)src[(sy + i) * sp + sx + j] - d[i * 4 + j];
+    return hadamard4_sum(d);
+}
 template <typename P>
-__device__ __noinline__ void pred4(int mode, int pAng, int sy, int sx, int lw, int lh, const P *A, const P *L, int dcv, int *p) {
-    pred4_inl(mode, pAng, sy, sx, lw, lh, A, L, dcv, p);
+__device__ __forceinline__ int pred4_satd(int mode, int pAng, int sy, int sx, int lw, int lh, const P *A, const P *L, int dcv, const P *src, int sp) {
+    return pred4_x<P, P>(mode, pAng, sy, sx, lw, lh, A, L, dcv, src, sp, (P *)nullptr);
 }
 
 // the whole prediction of a W x H block into out (row stride W), 4x4 sub-blocks over the G lanes of a group
@@ -376,12 +415,7 @@ __device__ __noinline__ void grp_predict(int mode, int pAng, int lw, int lh, con
     const int nsx = 1 << (lw - 2), nsub = 1 << (lw + lh - 4);
     for (int sb = g; sb < nsub; sb += G) {
         const int sx = (sb & (nsx - 1)) * 4, sy = (sb >> (lw - 2)) * 4;
-        int p[16];
-        pred4(mode, pAng, sy, sx, lw, lh, A, L, dcv, p);
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) out[((sy + i) << lw) + sx + j] = (O)p[i * 4 + j];
+        pred4_x<P, O>(mode, pAng, sy, sx, lw, lh, A, L, dcv, nullptr, 0, out);
     }
 }
 // CfL prediction (spec 7.11.5 with the DC prediction dcv) of a W x H chroma block into out (row stride W)
@@ -435,22 +469,6 @@ __device__ __forceinline__ int warp_dc(const P *A, const P *L, int haveL, int ha
     return 1 << (BD - 1);
 }
 
-// 4x4 Hadamard: sum of |coefficients| (the reference's SATD proxy, 4 x the orthonormal SATD)
-__device__ __forceinline__ int hadamard4_sum(int *d) {
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        int *r = d + 4 * i;
-        const int s0 = r[0] + r[1], s1 = r[0] - r[1], s2 = r[2] + r[3], s3 = r[2] - r[3];
-        r[0] = s0 + s2; r[1] = s1 + s3; r[2] = s0 - s2; r[3] = s1 - s3;
-    }
-    int sum = 0;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        const int s0 = d[j] + d[4 + j], s1 = d[j] - d[4 + j], s2 = d[8 + j] + d[12 + j], s3 = d[8 + j] - d[12 + j];
-        sum += abs(s0 + s2) + abs(s1 + s3) + abs(s0 - s2) + abs(s1 - s3);
-    }
-    return sum;
-}
 
 // ---------------------------------------------------------------------------------------------------------------
 // 1-D transforms on a strided int32 vector in shared memory.  Each (kind, length) network exists ONCE in the binary
@@ -605,7 +623,13 @@ __device__ __forceinline__ i64 base_bits_inl(int txSz, const EvalIn &e, int eob)
     }
     return b;
 }
-__device__ __noinline__ i64 base_bits(int txSz, const EvalIn &e, int eob) { return base_bits_inl(txSz, e, eob); }
+// out of line with scalar arguments: no structure of the caller has to be written to memory for the call
+__device__ __noinline__ i64 base_bits(int txSz, int txType, int plane, int skipCtx, int intraDir, const uint16_t *cost, int eob) {
+    EvalIn e;
+    e.txType = txType; e.plane = plane; e.skipCtx = skipCtx; e.intraDir = intraDir;
+    e.T.cost = cost;
+    return base_bits_inl(txSz, e, eob);
+}
 
 // bits of the coefficient at scan position c < eob (levels q natural order, row stride = adjusted width)
 __device__ __forceinline__ int coeff_bits(int c, int eob, const int16_t *q, const uint16_t *scan, int txSz, int txClass, int ptype,
@@ -667,7 +691,15 @@ __device__ __forceinline__ int coeff_bits(int c, int eob, const int16_t *q, cons
 // the step, the reference's 0.656 / 0.375; levels capped at 16383), transform-domain distortion, exact rate.  The
 // coefficients stay in buf (th x tw, row stride W + 1).
 template <int BD, typename Px>
-__device__ __noinline__ EvalOut grp_eval(int txSz, const ResFn<Px> &rf, const EvalIn &e, int32_t *buf, int16_t *q, int g, int G) {
+__device__ __noinline__ EvalOut grp_eval_x(int txSz, const Px *rsrc, int rsp, const Px *rpred, int rlw, const int32_t *rarr, int txType,
+                                           int plane, int skipCtx, int dcCtx, int intraDir, int dcQ, int acQ, const uint16_t *cost,
+                                           const uint16_t *scanT, const uint8_t *baseCtx, int32_t *buf, int16_t *q, int g, int G) {
+    // the arguments come as scalars and the structures are rebuilt here, in registers: a structure passed by address
+    // would live in the caller's local memory and be re-read after every store through buf / q
+    const ResFn<Px> rf{rsrc, rsp, rpred, rlw, rarr};
+    EvalIn e;
+    e.txType = txType; e.plane = plane; e.skipCtx = skipCtx; e.dcCtx = dcCtx; e.intraDir = intraDir; e.dcQ = dcQ; e.acQ = acQ;
+    e.T.cost = cost; e.T.scan = scanT; e.T.baseCtx = baseCtx;
     const TxRt d = tx_rt(txSz, BD);
     const int ck = col_kind(e.txType), rk = row_kind(e.txType);
     const bool big = d.W == 64 || d.H == 64;
@@ -709,7 +741,7 @@ __device__ __noinline__ EvalOut grp_eval(int txSz, const ResFn<Px> &rf, const Ev
     const int cls = tx_class(e.txType);
     for (int c = g; c < eob; c += G) b += coeff_bits(c, eob, q, scan, txSz, cls, e.plane > 0, e.dcCtx, e.T);
     EvalOut o;
-    o.R = grp_sum(b, G) + base_bits(txSz, e, eob);
+    o.R = grp_sum(b, G) + base_bits(txSz, e.txType, e.plane, e.skipCtx, e.intraDir, e.T.cost, eob);
     o.D = dist << d.dsh;
     if (big) {
         en = grp_sum64(en, G);
@@ -719,6 +751,11 @@ __device__ __noinline__ EvalOut grp_eval(int txSz, const ResFn<Px> &rf, const Ev
     }
     o.eob = eob;
     return o;
+}
+template <int BD, typename Px>
+__device__ __forceinline__ EvalOut grp_eval(int txSz, const ResFn<Px> &rf, const EvalIn &e, int32_t *buf, int16_t *q, int g, int G) {
+    return grp_eval_x<BD, Px>(txSz, rf.src, rf.sp, rf.pred, rf.lw, rf.arr, e.txType, e.plane, e.skipCtx, e.dcCtx, e.intraDir, e.dcQ, e.acQ,
+                              e.T.cost, e.T.scan, e.T.baseCtx, buf, q, g, G);
 }
 
 // ---------------------------------------------------------------------------------------------------------------

@@ -618,13 +618,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
                     const int r = it % nsub2, pl = 1 + (r >= (nsub2 >> 1)), sbk = r % (nsub2 >> 1);
                     const int sx = (sbk % nsx) * 4, sy = (sbk / nsx) * 4;
                     const int c = Wp.cand[ci], m = cand_mode(c);
-                    int d[16];
-                    pred4(m, pangle(m, cand_delta(c)), sy, sx, lw, lh, A[pl], L[pl], dcv[pl], d);
-#pragma unroll
-                    for (int i = 0; i < 4; i++)
-#pragma unroll
-                        for (int j = 0; j < 4; j++) d[i * 4 + j] = (int)sP[pl][(sy + i) * W + sx + j] - d[i * 4 + j];
-                    t = hadamard4_sum(d);
+                    t = pred4_satd(m, pangle(m, cand_delta(c)), sy, sx, lw, lh, A[pl], L[pl], dcv[pl], sP[pl], W);
                 }
                 for (int o = 16; o > 0; o >>= 1)
                     if (o < nsub2) t += __shfl_xor_sync(0xffffffffu, t, o);

@@ -361,8 +361,8 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
     };
     i64 bestJ = INF;
     int bestK = 0, bestTx = AV1G_DCT_DCT;
-#pragma unroll
     const int kMax = mmask != 0x1FFFu ? F.slRdK : 4;   // a shortlisted block: its best slRdK candidates only
+#pragma unroll
     for (int k = 0; k < 4; k++) {
         if (topJ[k] == INF || k >= kMax) continue;   // fewer candidates screened or taken (shortlist)
         const i64 j = rd(topP[k], topM[k], AV1G_DCT_DCT);
