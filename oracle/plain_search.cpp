@@ -1158,7 +1158,7 @@ struct Engine {
         *outDelta = cand_delta(bestC);
     }
 
-    // ---- chroma of one block (k_recon.cuh:1220-1686; 4:2:0: one tx block per plane) ----
+    // ---- chroma of one block (k_recon.cuh:1220-1686) ----
     void chroma(SbState &S, std::vector<TxbOut> &txbs, int bsize, int mi_row, int mi_col, int yMode, int availUC, int availLC,
                 const TileBox &tb, int *outUv, int *outDuv, int *outAu, int *outAv, int *outEobU, int *outEobV) {
         const int txSz = av1g_uv_tx_size(bsize, ssx, ssy);
@@ -1355,6 +1355,13 @@ struct Engine {
         const bool cfl = bestC == 255;
         const int bestUv = cfl ? AV1G_UV_CFL_PRED : cand_mode(bestC);
         const int uvTxType = av1g_chroma_tx_type(txSz, bestUv, 0);
+        // chroma tx blocks per plane (k_recon.cuh:1588-1680): one in 4:2:0 and in 4:4:4 up to 32x32; 2 or 4 in raster
+        // order for a 4:4:4 block with a 64-sample side, the mode chosen on the first.  A further tx block takes its
+        // edges from the reconstruction (the block's earlier tx blocks included), its own coefficient contexts and a
+        // closed-loop quantisation of the chosen mode; tx blocks that start outside the coded area are not coded.
+        const int ub = av1g_uv_bsize(bsize, ssx, ssy);
+        const int nTxX = ssx ? 1 : std::max(1, bw_px(ub) / Wt), nTxY = ssy ? 1 : std::max(1, bh_px(ub) / Ht);
+        const int cCols4 = MiCols >> ssx, cRows4 = MiRows >> ssy;
         int eobs[3] = {0, 0, 0};
         for (int pl = 1; pl <= 2; pl++) {
             Px *dst = rec[pl].data() + (size_t)cy * pw[pl] + cx;
@@ -1367,6 +1374,29 @@ struct Engine {
             }
             inverse_add(bestQ[pl], txSz, uvTxType, pl, dst, pw[pl]);
             eobs[pl] = record_txb(S, txbs, bestQ[pl], pl, txSz, uvTxType, x4, y4, sbr4, sbc4);
+            for (int ty = 0; ty < nTxY; ty++)
+                for (int tx = 0; tx < nTxX; tx++) {
+                    if (tx == 0 && ty == 0) continue;
+                    const int ox = tx * Wt, oy = ty * Ht;
+                    if (x4 + (ox >> 2) >= cCols4 || y4 + (oy >> 2) >= cRows4) continue;
+                    const int r4 = sbr4 + (oy >> 2), c4 = sbc4 + (ox >> 2);
+                    const int haveL = availLC || tx > 0, haveA = availUC || ty > 0;
+                    const int haveAR = bd_at(S, pl, r4 - 1, c4 + (Wt >> 2)), haveBL = bd_at(S, pl, r4 + (Ht >> 2), c4 - 1);
+                    Px ea2[AV1G_EDGE_LEN], el2[AV1G_EDGE_LEN];
+                    Px *A2 = ea2 + AV1G_EDGE_OFF, *L2 = el2 + AV1G_EDGE_OFF;
+                    rec_edges(pl, cx + ox, cy + oy, lw, lh, haveL, haveA, haveAR, haveBL, A2, L2);
+                    int sc, dc;
+                    txb_ctx(pl, txSz, x4 + (ox >> 2), y4 + (oy >> 2), bsize, tb, &sc, &dc);
+                    Px *d2 = rec[pl].data() + (size_t)(cy + oy) * pw[pl] + cx + ox;
+                    av1g_predict_intra<BD>(cand_mode(bestC), cand_delta(bestC), haveL, haveA, lw, lh, A2, L2, d2, pw[pl]);
+                    const Px *s2 = sP[pl] + (size_t)oy * spP[pl] + ox;
+                    for (int i = 0; i < Ht; i++)
+                        for (int j = 0; j < Wt; j++) res[(size_t)i * Wt + j] = (int)s2[(size_t)i * spP[pl] + j] - (int)d2[(size_t)i * pw[pl] + j];
+                    int16_t q2[1024];
+                    eval(res.data(), txSz, uvTxType, pl, sc, dc, 0, 0, q2, 1, cand_mode(bestC), cand_delta(bestC));
+                    inverse_add(q2, txSz, uvTxType, pl, d2, pw[pl]);
+                    eobs[pl] |= record_txb(S, txbs, q2, pl, txSz, uvTxType, x4 + (ox >> 2), y4 + (oy >> 2), r4, c4);
+                }
         }
         *outUv = bestUv;
         *outDuv = cfl ? 0 : cand_delta(bestC);
