@@ -146,15 +146,16 @@ void min_tiles(int W, int H, std::vector<int> &cs, std::vector<int> &rs) {
 }
 
 // analysis task lists of one SB: (bsize, x4, y4) for every shape, largest area first; big = shapes with a 64 side
-std::vector<uint8_t> an_tasks(bool big) {
+// the task list of an analysis kernel (an_task<LIST>): 0 the shapes up to 32 a side from 8x16 / 16x8 up, 1 the shapes
+// with a 64-sample side, 2 the six smallest (4x4, 4x8, 8x4, 8x8, 4x16, 16x4: the per-thread kernels of 8-bit images)
+std::vector<uint8_t> an_tasks(int list) {
     std::vector<int> shapes;
     for (int s = 0; s < AV1G_BLOCK_INVALID; s++) {
         if (s >= 13 && s <= 15) continue;
         const bool b = AV1G_T(Num_4x4_Blocks_Wide)[s] == 16 || AV1G_T(Num_4x4_Blocks_High)[s] == 16;
-        // the 4x4, 4x8, 8x4 (k_analysis_tiny) and 8x8, 4x16, 16x4 blocks (k_analysis_mid) have their own kernels
-        if (b == big && s != AV1G_BLOCK_4X4 && s != AV1G_BLOCK_4X8 && s != AV1G_BLOCK_8X4 && s != AV1G_BLOCK_8X8 && s != AV1G_BLOCK_4X16 &&
-            s != AV1G_BLOCK_16X4)
-            shapes.push_back(s);
+        const bool small = s == AV1G_BLOCK_4X4 || s == AV1G_BLOCK_4X8 || s == AV1G_BLOCK_8X4 || s == AV1G_BLOCK_8X8 || s == AV1G_BLOCK_4X16 ||
+                           s == AV1G_BLOCK_16X4;
+        if (list == 2 ? small : (!small && b == (list == 1))) shapes.push_back(s);
     }
     std::stable_sort(shapes.begin(), shapes.end(), [](int a, int b) {
         return AV1G_T(Num_4x4_Blocks_Wide)[a] * AV1G_T(Num_4x4_Blocks_High)[a] > AV1G_T(Num_4x4_Blocks_Wide)[b] * AV1G_T(Num_4x4_Blocks_High)[b];
@@ -188,7 +189,7 @@ __global__ void k_pad(Px *plane, int pitch, int vw, int vh, int pw, int ph) {
 // ---------------------------------------------------------------------------------------------------------------
 struct is_handle {
     is_params p;
-    int device = 0, nSm = 0, rcGrid = 0;
+    int device = 0, nSm = 0;
     cudaStream_t own = nullptr;
     std::string err;
     // workspace
@@ -196,7 +197,9 @@ struct is_handle {
     size_t arenaBytes = 0;
     FrameDesc F;                 // the descriptor (device pointers), passed by value to every kernel
     int nSb = 0;
-    size_t smemAn = 0, smemAnBig = 0, smemRc = 0;
+    size_t smemAn = 0, smemAnBig = 0, smemAn10 = 0, smemAnBig10 = 0;
+    size_t smemRcG[4] = {0, 0, 0, 0};       // the closed loop per format group (fmt_group)
+    int rcGridG[4] = {0, 0, 0, 0};
     // last result
     bool have = false;
     uint32_t nBlocks = 0, nTxb = 0;
@@ -216,6 +219,7 @@ struct is_handle {
     std::vector<uint32_t> bNb, bNt;
     std::vector<uint64_t> bNc;
     size_t bSlots = 0;                      // ready-queue slots (sum over images of SBs x 256)
+    size_t bQBytes = 0;                     // bytes of the ready queues (all groups)
     FrameDesc *dFs = nullptr;               // the descriptors in device memory (for the closed loop)
     FrameDesc *hFs = nullptr;               // pinned staging of the descriptors
     size_t hFsCap = 0;
@@ -223,8 +227,11 @@ struct is_handle {
     size_t hOrdCap = 0;
     uint32_t *hCnt = nullptr;               // pinned readback: per image n_blocks, n_txb, n_coeffs (2 words), + err
     size_t hCntCap = 0;
-    unsigned long long *bReadyQ = nullptr;
-    int *bRq = nullptr, *bErr = nullptr;
+    unsigned long long *bReadyQ = nullptr;  // the ready queues, one per format group of the batch (fmt_group order)
+    int *bRq = nullptr, *bErr = nullptr;    // [2 g, 2 g + 1]: group g's head / tail
+    std::vector<int> bBd, bC444;            // per image (batch order)
+    std::vector<int> bPos;                  // per image: its position in the device descriptor array (groups in order)
+    int bGrpStart[5] = {0, 0, 0, 0, 0};     // group g's descriptors: [bGrpStart[g], bGrpStart[g + 1])
     // multi-stream front end (upload, analysis, DP, dataflow graph of each image) and CUDA graph replay
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t evFork = nullptr, evJoin[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -271,7 +278,7 @@ int upload_tables(int dev) {
         const HostTables &T = host_tables();
         std::vector<uint16_t> all((size_t)4 * NCDF);
         for (int q = 0; q < 4; q++) memcpy(all.data() + (size_t)q * NCDF, T.cost[q].data(), NCDF * 2);
-        const std::vector<uint8_t> tasks = an_tasks(false), tasksBig = an_tasks(true);
+        const std::vector<uint8_t> tasks = an_tasks(0), tasksBig = an_tasks(1), tasksSmall = an_tasks(2);
         cudaError_t e = cudaMemcpyToSymbol(g_cost, all.data(), all.size() * 2);
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgY, T.avgY, sizeof T.avgY);
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgPart, T.avgPart, sizeof T.avgPart);
@@ -322,11 +329,14 @@ int upload_tables(int dev) {
             out[n] = (int)(t.size() / 3);
             return k == n;
         };
-        int st[AN_SHAPES + 1], stBig[ANB_SHAPES + 1];
-        const bool okShapes = starts(tasks, AN_SHAPES, st) && starts(tasksBig, ANB_SHAPES, stBig);
-        if (e == cudaSuccess && okShapes && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3) {
+        int st[AN_SHAPES + 1], stBig[ANB_SHAPES + 1], stSmall[ANS_SHAPES + 1];
+        const bool okShapes = starts(tasks, AN_SHAPES, st) && starts(tasksBig, ANB_SHAPES, stBig) && starts(tasksSmall, ANS_SHAPES, stSmall);
+        if (e == cudaSuccess && okShapes && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3 &&
+            tasksSmall.size() == (size_t)ANS_TASKS * 3) {
             e = cudaMemcpyToSymbol(c_anTask, tasks.data(), tasks.size());
             if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anTaskBig, tasksBig.data(), tasksBig.size());
+            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anTaskSmall, tasksSmall.data(), tasksSmall.size());
+            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStartSmall, stSmall, sizeof stSmall);
             if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStart, st, sizeof st);
             if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStartBig, stBig, sizeof stBig);
         } else if (e == cudaSuccess) {
@@ -339,27 +349,41 @@ int upload_tables(int dev) {
 
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
-// lay out the workspace for an image of W x H (8-bit 4:2:0); returns bytes needed, fills F's pointers if base != 0
-size_t layout(int W, int H, uint8_t *base, FrameDesc &F, int &nSb) {
+// format groups of a batch, each with its own closed-loop instance and ready queue: 0 8-bit 4:2:0, 1 8-bit 4:4:4,
+// 2 10-bit 4:2:0, 3 10-bit 4:4:4
+int fmt_group(int bd, int c444) { return (bd == 10 ? 2 : 0) + (c444 ? 1 : 0); }
+const void *rc_kernel(int g) {
+    return g == 0 ? (const void *)k_recon<8, 1> : g == 1 ? (const void *)k_recon<8, 0> : g == 2 ? (const void *)k_recon<10, 1>
+                                                                                        : (const void *)k_recon<10, 0>;
+}
+size_t rc_smem(int g) {
+    return g == 0 ? sizeof(RcSmem<uint8_t, 1>) : g == 1 ? sizeof(RcSmem<uint8_t, 0>) : g == 2 ? sizeof(RcSmem<uint16_t, 1>)
+                                                                                        : sizeof(RcSmem<uint16_t, 0>);
+}
+
+// lay out the workspace for an image of W x H (bit depth bd, 4:4:4 or 4:2:0); returns bytes needed, fills F's
+// pointers if base != 0.  Plane pitches are in samples (a multiple of 16).
+size_t layout(int W, int H, int bd, int c444, uint8_t *base, FrameDesc &F, int &nSb) {
     F.W = W; F.H = H;
     F.MiCols = 2 * ((W + 7) >> 3); F.MiRows = 2 * ((H + 7) >> 3);
     F.sbCols = (F.MiCols + 15) >> 4; F.sbRows = (F.MiRows + 15) >> 4;
-    F.ssx = F.ssy = 1; F.bd = 8;
+    F.ssx = F.ssy = c444 ? 0 : 1; F.bd = bd;
     nSb = F.sbCols * F.sbRows;
+    const size_t px = bd > 8 ? 2 : 1;
     size_t at = 0;
     auto take = [&](size_t bytes) -> uint8_t * { uint8_t *p = base ? base + at : nullptr; at += align256(bytes); return p; };
     for (int p = 0; p < 3; p++) {
-        const int ss = p ? 1 : 0;
+        const int ss = p ? F.ssx : 0;
         const int pw = (((F.sbCols + 1) * 64) >> ss) + SRC_MARGIN_X, ph = ((F.sbRows * 64) >> ss) + SRC_MARGIN_Y;
         const int pitch = (pw + 15) & ~15;
-        uint8_t *s = take((size_t)pitch * ph), *r = take((size_t)pitch * ph);
+        uint8_t *s = take((size_t)pitch * ph * px), *r = take((size_t)pitch * ph * px);
         F.spitch[p] = F.rpitch[p] = pitch;
-        F.src[p] = s ? s + (size_t)SRC_MARGIN_Y * pitch + SRC_MARGIN_X : nullptr;
-        F.rec[p] = r ? r + (size_t)SRC_MARGIN_Y * pitch + SRC_MARGIN_X : nullptr;
+        F.src[p] = s ? s + ((size_t)SRC_MARGIN_Y * pitch + SRC_MARGIN_X) * px : nullptr;
+        F.rec[p] = r ? r + ((size_t)SRC_MARGIN_Y * pitch + SRC_MARGIN_X) * px : nullptr;
     }
     F.mYMode = take((size_t)F.MiCols * F.MiRows);
     for (int p = 0; p < 3; p++) {
-        const size_t n = (size_t)(F.MiCols >> (p ? 1 : 0)) * (F.MiRows >> (p ? 1 : 0));
+        const size_t n = (size_t)(F.MiCols >> (p ? F.ssx : 0)) * (F.MiRows >> (p ? F.ssy : 0));
         F.cLvl[p] = take(n);
         F.cDc[p] = take(n);
     }
@@ -418,7 +442,7 @@ extern "C" {
 
 int is_create(const is_params *p, is_handle **out) {
     if (!p || !out) return IS_ERR_INVALID;
-    if (p->bit_depth != 8 || p->chroma_444 != 0) return IS_ERR_INVALID;
+    if ((p->bit_depth != 8 && p->bit_depth != 10) || (p->chroma_444 != 0 && p->chroma_444 != 1)) return IS_ERR_INVALID;
     is_handle *h = new is_handle();
     h->p = *p;
     h->device = p->device;
@@ -430,14 +454,22 @@ int is_create(const is_params *p, is_handle **out) {
     h->nSm = prop.multiProcessorCount;
     h->smemAn = sizeof(AnSmem<uint8_t, AN_WARPS, AN_BUF_INTS>);
     h->smemAnBig = sizeof(AnSmem<uint8_t, ANB_WARPS, ANB_BUF_INTS>);
-    h->smemRc = sizeof(RcSmem<uint8_t>);
-    if (cudaFuncSetAttribute(k_analysis<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemAn) != cudaSuccess) return fail(IS_ERR_CUDA);
-    if (cudaFuncSetAttribute(k_analysis_big<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemAnBig) != cudaSuccess) return fail(IS_ERR_CUDA);
-    if (cudaFuncSetAttribute(k_recon<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smemRc) != cudaSuccess) return fail(IS_ERR_CUDA);
-    if (cudaFuncSetAttribute(k_analysis_mid<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MidSmem)) != cudaSuccess) return fail(IS_ERR_CUDA);
-    int per = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_recon<8>, RC_WARPS * 32, h->smemRc) != cudaSuccess || per < 1) return fail(IS_ERR_CUDA);
-    h->rcGrid = per * h->nSm;
+    h->smemAn10 = sizeof(AnSmem<uint16_t, AN_WARPS, AN_BUF_INTS>);
+    h->smemAnBig10 = sizeof(AnSmem<uint16_t, ANB_WARPS, ANB_BUF_INTS>);
+    auto attr = [](const void *k, size_t b) { return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b) == cudaSuccess; };
+    if (!attr((const void *)k_analysis<8>, h->smemAn) || !attr((const void *)k_analysis_big<8>, h->smemAnBig) ||
+        !attr((const void *)k_analysis_mid<8>, sizeof(MidSmem)) || !attr((const void *)k_analysis<10>, h->smemAn10) ||
+        !attr((const void *)k_analysis_small<10>, h->smemAn10) || !attr((const void *)k_analysis_big<10>, h->smemAnBig10))
+        return fail(IS_ERR_CUDA);
+    for (int g = 0; g < 4; g++) {   // the closed loop of each format group: shared memory and its cooperative grid
+        const void *k = rc_kernel(g);
+        h->smemRcG[g] = rc_smem(g);
+        int per = 0;
+        if (!attr(k, h->smemRcG[g]) || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, RC_WARPS * 32, h->smemRcG[g]) != cudaSuccess ||
+            per < 1)
+            return fail(IS_ERR_CUDA);
+        h->rcGridG[g] = per * h->nSm;
+    }
     if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess) return fail(IS_ERR_CUDA);
     for (auto &e : h->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return fail(IS_ERR_CUDA);
@@ -510,27 +542,50 @@ template <typename T> static int grow_pinned(is_handle *h, T **p, size_t *cap, s
 }
 }
 
-// Lay out a batch: every image's workspace, then the shared ready queue, its counters, the error word and the device
-// copy of the descriptors, in one arena; the descriptors and SB orders in pinned staging.
+// the format of a frame: its own (bit_depth 8 / 10) or the handle's (bit_depth 0)
+static void frame_format(const is_handle *h, const is_frame *f, int *bd, int *c444) {
+    *bd = f->bit_depth ? f->bit_depth : h->p.bit_depth;
+    *c444 = f->bit_depth ? f->chroma_444 : h->p.chroma_444;
+}
+
+// Lay out a batch: every image's workspace, then the ready queues (one per format group), their counters, the error
+// word and the device copy of the descriptors (grouped by format), in one arena; the descriptors and SB orders in
+// pinned staging.
 static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
     if (!fr || n < 1 || n > 4096) return h->setErr(IS_ERR_INVALID, "invalid batch (%d images)", n);
+    h->bBd.assign(n, 8);
+    h->bC444.assign(n, 0);
     for (int i = 0; i < n; i++) {
         const is_frame *f = fr + i;
         if (f->width < 1 || f->height < 1 || f->width > 16384 || f->height > 16384 || f->qindex < 1 || f->qindex > 255)
             return h->setErr(IS_ERR_INVALID, "invalid frame %d (size %dx%d, qindex %d)", i, f->width, f->height, f->qindex);
+        frame_format(h, f, &h->bBd[i], &h->bC444[i]);
+        if ((h->bBd[i] != 8 && h->bBd[i] != 10) || (h->bC444[i] != 0 && h->bC444[i] != 1))
+            return h->setErr(IS_ERR_INVALID, "invalid frame %d format (bit depth %d, chroma_444 %d)", i, h->bBd[i], h->bC444[i]);
     }
     std::vector<size_t> off(n + 1);
-    std::vector<int> nsb(n);
-    size_t at = 0, slots = 0, nOrd = 0;
+    std::vector<int> nsb(n), grp(n);
+    size_t at = 0, slotsG[4] = {0, 0, 0, 0}, nOrd = 0;
+    h->bPos.assign(n, 0);
+    int cnt[4] = {0, 0, 0, 0};
+    for (int i = 0; i < n; i++) cnt[grp[i] = fmt_group(h->bBd[i], h->bC444[i])]++;
+    h->bGrpStart[0] = 0;
+    for (int g = 0; g < 4; g++) h->bGrpStart[g + 1] = h->bGrpStart[g] + cnt[g];
+    int fill[4] = {0, 0, 0, 0};
+    for (int i = 0; i < n; i++) h->bPos[i] = h->bGrpStart[grp[i]] + fill[grp[i]]++;
     for (int i = 0; i < n; i++) {
         FrameDesc F;
         memset(&F, 0, sizeof F);
         off[i] = at;
-        at += layout(fr[i].width, fr[i].height, nullptr, F, nsb[i]);
-        slots += (size_t)nsb[i] * SB_MAX_LEAVES;
+        at += layout(fr[i].width, fr[i].height, h->bBd[i], h->bC444[i], nullptr, F, nsb[i]);
+        slotsG[grp[i]] += (size_t)nsb[i] * SB_MAX_LEAVES;
         nOrd += 2 * (size_t)nsb[i];
     }
-    const size_t offQ = at, offRq = offQ + align256(slots * 8), offErr = offRq + 256, offFs = offErr + 256;
+    const size_t slots = slotsG[0] + slotsG[1] + slotsG[2] + slotsG[3];
+    size_t offQG[4];
+    offQG[0] = at;
+    for (int g = 1; g < 4; g++) offQG[g] = offQG[g - 1] + align256(slotsG[g - 1] * 8);
+    const size_t offQ = at, offRq = offQG[3] + align256(slotsG[3] * 8), offErr = offRq + 256, offFs = offErr + 256;
     const size_t need = offFs + align256((size_t)n * sizeof(FrameDesc));
     if (need > h->arenaBytes) {
         if (h->arena) { cudaStreamSynchronize(h->own); cudaDeviceSynchronize(); cudaFree(h->arena); h->arena = nullptr; h->arenaBytes = 0; }
@@ -543,12 +598,13 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
     h->bErr = (int *)(base + offErr);
     h->dFs = (FrameDesc *)(base + offFs);
     h->bSlots = slots;
+    h->bQBytes = offRq - offQ;
     int rc = grow_pinned(h, &h->hFs, &h->hFsCap, (size_t)n);
     if (!rc) rc = grow_pinned(h, &h->hOrd, &h->hOrdCap, nOrd);
     if (!rc) rc = grow_pinned(h, &h->hCnt, &h->hCntCap, (size_t)n * 4 + 4);
     if (rc) return rc;
     if (h->trace) {
-        const size_t needT = slots * 4;
+        const size_t needT = std::max(std::max(slotsG[0], slotsG[1]), std::max(slotsG[2], slotsG[3])) * 4;
         if (needT > h->traceCap) {
             if (h->traceBuf) cudaFree(h->traceBuf);
             h->traceBuf = nullptr;
@@ -569,7 +625,7 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         FrameDesc &F = h->bF[i];
         memset(&F, 0, sizeof F);
         int ns = 0;
-        layout(f->width, f->height, base + off[i], F, ns);
+        layout(f->width, f->height, h->bBd[i], h->bC444[i], base + off[i], F, ns);
         std::vector<int> cs, rs;
         min_tiles(f->width, f->height, cs, rs);
         if (cs.size() > 65 || rs.size() > 65) return h->setErr(IS_ERR_INVALID, "too many tiles");
@@ -578,19 +634,22 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         for (size_t k = 0; k < rs.size(); k++) F.tileRowStart[k] = rs[k];
         F.qidx = f->qindex;
         F.qctx = av1g_coeff_cdf_q_ctx(f->qindex);
-        lambda_fx(f->qindex, 8, &F.lam, &F.sqlam);
-        F.dcQ = AV1G_T(Dc_Qlookup)[0][f->qindex];
-        F.acQ = AV1G_T(Ac_Qlookup)[0][f->qindex];
-        F.readyQ = h->bReadyQ;
-        F.rq = h->bRq;
+        const int bd = h->bBd[i], g10 = bd == 10;
+        lambda_fx(f->qindex, bd, &F.lam, &F.sqlam);
+        F.dcQ = AV1G_T(Dc_Qlookup)[g10][f->qindex];
+        F.acQ = AV1G_T(Ac_Qlookup)[g10][f->qindex];
+        // the image's format group: its ready queue and counters; img indexes the group's descriptors
+        F.readyQ = (unsigned long long *)(base + offQG[grp[i]]);
+        F.rq = h->bRq + 2 * grp[i];
         F.err = h->bErr;
-        F.img = i;
-        F.leafTrace = (h->trace && i == 0) ? h->traceBuf : nullptr;
-        if (!h->slOn) F.slMask = nullptr;
-        F.slRdK = h->slOn ? h->slRdK : 4;
+        F.img = h->bPos[i] - h->bGrpStart[grp[i]];
+        F.leafTrace = (h->trace && i == 0 && F.img == 0) ? h->traceBuf : nullptr;   // image 0, when its group's first
+        const bool sl = h->slOn && bd == 8;   // the shortlist network reads 8-bit luma: other images search in full
+        if (!sl) F.slMask = nullptr;
+        F.slRdK = sl ? h->slRdK : 4;
         sb_orders(F, cs, rs, h->hOrd + o, h->hOrd + o + ns);
         o += 2 * (size_t)ns;
-        h->hFs[i] = F;
+        h->hFs[h->bPos[i]] = F;
         h->bQ[i] = f->qindex;
     }
     h->bN = n;
@@ -612,8 +671,8 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
             o += 2 * (size_t)ns;
         }
     }
-    IS_CK(cudaMemsetAsync(h->bReadyQ, 0, h->bSlots * 8, st));
-    IS_CK(cudaMemsetAsync(h->bRq, 0, 16, st));
+    IS_CK(cudaMemsetAsync(h->bReadyQ, 0, h->bQBytes, st));
+    IS_CK(cudaMemsetAsync(h->bRq, 0, 32, st));
     IS_CK(cudaMemsetAsync(h->bErr, 0, 4, st));
     // front end of each image: planes, analysis, DP, leaf maps and the dataflow graph (its initial ready leaves go to
     // the shared queue); images spread over frontStreams streams
@@ -627,16 +686,19 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
         const is_frame *f = fr + i;
         const int nSb = h->bNsb[i];
         cudaStream_t s = K > 1 ? h->aux[i % K] : st;
+        const size_t px = F.bd > 8 ? 2 : 1;
         for (int p = 0; p < 3; p++) {
-            const int ss = p ? 1 : 0;
+            const int ss = p ? F.ssx : 0;
             const int vw = (f->width + ss) >> ss, vh = (f->height + ss) >> ss;
             uint8_t *dst = const_cast<uint8_t *>(F.src[p]);
-            IS_CK(cudaMemcpy2DAsync(dst, F.spitch[p], f->planes[p], f->pitch[p], vw, vh, fromHost ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+            IS_CK(cudaMemcpy2DAsync(dst, F.spitch[p] * px, f->planes[p], (size_t)f->pitch[p] * px, vw * px, vh,
+                                    fromHost ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
             const int pw = ((F.sbCols + 1) * 64) >> ss, ph = (F.sbRows * 64) >> ss;
-            k_pad<uint8_t><<<dim3(1, ph), 128, 0, s>>>(dst, F.spitch[p], vw, vh, pw, ph);
+            if (px == 1) k_pad<uint8_t><<<dim3(1, ph), 128, 0, s>>>(dst, F.spitch[p], vw, vh, pw, ph);
+            else k_pad<uint16_t><<<dim3(1, ph), 128, 0, s>>>((uint16_t *)dst, F.spitch[p], vw, vh, pw, ph);
         }
         if (events && n == 1) IS_CK(cudaEventRecord(h->ev[1], s));
-        if (h->slOn) {   // the learned shortlist: scores of every analysis record, then its mode mask
+        if (h->slOn && F.bd == 8) {   // the learned shortlist: scores of every analysis record, then its mode mask
             const int k = K > 1 ? i % K : 0;
             for (uint32_t i0 = 0; i0 < F.nRec; i0 += SL_CHUNK) {
                 const int cn = (int)std::min<uint32_t>(SL_CHUNK, F.nRec - i0);
@@ -649,10 +711,16 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
             }
             IS_CK(cudaGetLastError());
         }
-        k_analysis_big<8><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig, s>>>(F);
-        k_analysis<8><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn, s>>>(F);
-        k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem), s>>>(F);
-        k_analysis_mid<8><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem), s>>>(F);
+        if (F.bd == 8) {
+            k_analysis_big<8><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig, s>>>(F);
+            k_analysis<8><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn, s>>>(F);
+            k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem), s>>>(F);
+            k_analysis_mid<8><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem), s>>>(F);
+        } else {
+            k_analysis_big<10><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig10, s>>>(F);
+            k_analysis<10><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn10, s>>>(F);
+            k_analysis_small<10><<<ANS_SHAPES * nSb, AN_WARPS * 32, h->smemAn10, s>>>(F);
+        }
         IS_CK(cudaGetLastError());
         if (events && n == 1) IS_CK(cudaEventRecord(h->ev[2], s));
         k_dp<<<(nSb + 63) / 64, 64, 0, s>>>(F, nSb);
@@ -670,20 +738,27 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
         }
     }
     if (events) IS_CK(cudaEventRecord(h->ev[3], st));
-    {   // the closed loop of every image at once: a cooperative launch (all CTAs resident: their warps wait on each
-        // other's leaves), expressed with launch attributes so that it can be captured in a graph
+    // the closed loop of every image of a format group at once: a cooperative launch (all CTAs resident: their warps
+    // wait on each other's leaves), expressed with launch attributes so that it can be captured in a graph
+    for (int g = 0; g < 4; g++) {
+        const int gn = h->bGrpStart[g + 1] - h->bGrpStart[g];
+        if (gn == 0) continue;
+        const int grid = h->rcGridG[g];
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(h->reconCtas > 0 && h->reconCtas < h->rcGrid ? h->reconCtas : h->rcGrid);
+        cfg.gridDim = dim3(h->reconCtas > 0 && h->reconCtas < grid ? h->reconCtas : grid);
         cfg.blockDim = dim3(RC_WARPS * 32);
-        cfg.dynamicSmemBytes = h->smemRc;
+        cfg.dynamicSmemBytes = h->smemRcG[g];
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;
         attr[0].val.cooperative = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        const FrameDesc *fs = h->dFs;
-        IS_CK(cudaLaunchKernelEx(&cfg, k_recon<8>, fs, n));
+        const FrameDesc *fs = h->dFs + h->bGrpStart[g];
+        if (g == 0) IS_CK(cudaLaunchKernelEx(&cfg, k_recon<8, 1>, fs, gn));
+        else if (g == 1) IS_CK(cudaLaunchKernelEx(&cfg, k_recon<8, 0>, fs, gn));
+        else if (g == 2) IS_CK(cudaLaunchKernelEx(&cfg, k_recon<10, 1>, fs, gn));
+        else IS_CK(cudaLaunchKernelEx(&cfg, k_recon<10, 0>, fs, gn));
     }
     if (events) IS_CK(cudaEventRecord(h->ev[4], st));
     for (int i = 0; i < n; i++) {
@@ -711,8 +786,8 @@ static std::string batch_key(const is_handle *h, const is_frame *fr, int n, bool
     snprintf(b, sizeof b, "%p|%d|%d|%d|%d|%d|", h->arena, n, (int)fromHost, h->frontStreams, h->reconCtas, h->slOn ? h->slVersion : -1);
     k += b;
     for (int i = 0; i < n; i++) {
-        snprintf(b, sizeof b, "%d,%d,%d,%p,%p,%p,%d,%d,%d;", fr[i].width, fr[i].height, fr[i].qindex, fr[i].planes[0], fr[i].planes[1],
-                 fr[i].planes[2], fr[i].pitch[0], fr[i].pitch[1], fr[i].pitch[2]);
+        snprintf(b, sizeof b, "%d,%d,%d,%d,%d,%p,%p,%p,%d,%d,%d;", fr[i].width, fr[i].height, fr[i].qindex, fr[i].bit_depth, fr[i].chroma_444,
+                 fr[i].planes[0], fr[i].planes[1], fr[i].planes[2], fr[i].pitch[0], fr[i].pitch[1], fr[i].pitch[2]);
         k += b;
     }
     return k;
@@ -788,15 +863,19 @@ static int run_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n, b
     return IS_OK;
 }
 
-int is_workspace_bytes(int width, int height, uint64_t *bytes) {
-    if (width < 1 || height < 1 || width > 16384 || height > 16384 || !bytes) return IS_ERR_INVALID;
+int is_workspace_bytes_format(int width, int height, int bit_depth, int chroma_444, uint64_t *bytes) {
+    if (width < 1 || height < 1 || width > 16384 || height > 16384 || !bytes || (bit_depth != 8 && bit_depth != 10) ||
+        (chroma_444 != 0 && chroma_444 != 1))
+        return IS_ERR_INVALID;
     FrameDesc F;
     memset(&F, 0, sizeof F);
     int nSb = 0;
-    const size_t ws = layout(width, height, nullptr, F, nSb);
-    *bytes = ws + (size_t)nSb * SB_MAX_LEAVES * 8 + align256(sizeof(FrameDesc)) + 512;
+    const size_t ws = layout(width, height, bit_depth, chroma_444, nullptr, F, nSb);
+    *bytes = ws + align256((size_t)nSb * SB_MAX_LEAVES * 8) + align256(sizeof(FrameDesc)) + 768;
     return IS_OK;
 }
+
+int is_workspace_bytes(int width, int height, uint64_t *bytes) { return is_workspace_bytes_format(width, height, 8, 0, bytes); }
 
 int is_encode_device(is_handle *h, const is_frame *f, void *stream) {
     if (!h) return IS_ERR_INVALID;
@@ -907,18 +986,20 @@ int is_batch_copy(is_handle *h, int i, av1g_frame_params *fp, av1g_block *blocks
         fp->base_q_idx = (uint8_t)h->bQ[i];
         fp->tile_cols_log2 = -1; fp->tile_rows_log2 = -1;
         fp->qm_y = fp->qm_u = fp->qm_v = 15;
-        fp->chroma_format = AV1G_CHROMA_420;
-        fp->bit_depth = 8;
+        fp->chroma_format = F.ssx ? AV1G_CHROMA_420 : AV1G_CHROMA_444;
+        fp->bit_depth = (uint8_t)F.bd;
     }
     if (blocks) IS_CK(cudaMemcpyAsync(blocks, F.recBlocks, (size_t)h->bNb[i] * sizeof(av1g_block), cudaMemcpyDeviceToHost, st));
     if (block_txb) IS_CK(cudaMemcpyAsync(block_txb, F.recBlockTxb, ((size_t)h->bNb[i] + 1) * 4, cudaMemcpyDeviceToHost, st));
     if (txb) IS_CK(cudaMemcpyAsync(txb, F.recTxb, (size_t)h->bNt[i] * sizeof(av1g_txb), cudaMemcpyDeviceToHost, st));
     if (coeffs) IS_CK(cudaMemcpyAsync(coeffs, F.recCoeffs, (size_t)h->bNc[i] * 2, cudaMemcpyDeviceToHost, st));
+    const size_t px = F.bd > 8 ? 2 : 1;
     for (int p = 0; p < 3; p++) {
         if (!recon || !recon[p]) continue;
-        const int ss = p ? 1 : 0;
+        const int ss = p ? F.ssx : 0;
         const int vw = (F.W + ss) >> ss, vh = (F.H + ss) >> ss;
-        IS_CK(cudaMemcpy2DAsync(recon[p], recon_pitch ? recon_pitch[p] : vw, F.rec[p], F.rpitch[p], vw, vh, cudaMemcpyDeviceToHost, st));
+        IS_CK(cudaMemcpy2DAsync(recon[p], (recon_pitch ? recon_pitch[p] : vw) * px, F.rec[p], F.rpitch[p] * px, vw * px, vh,
+                                cudaMemcpyDeviceToHost, st));
     }
     IS_CK(cudaStreamSynchronize(st));
     return IS_OK;

@@ -27,7 +27,7 @@ constexpr int LEAF_WAIT_ITERS = 1 << 20;   // bounded spins: a wait that runs ou
                                            // once any error is recorded no further wait starts (the host discards the
                                            // result)
 
-template <typename Px> struct RcWarp {
+template <typename Px, int SS> struct RcWarp {   // SS: chroma subsampling (1 4:2:0, 0 4:4:4)
     int32_t buf[64 * 65];      // evaluation scratch (32 / G tasks) and the inverse transform's residual
     int16_t q[1024];           // levels of the tasks of a round
     int16_t qb[2][1024];       // best levels (chroma: U, V)
@@ -37,20 +37,26 @@ template <typename Px> struct RcWarp {
     Px ea[3][EDGE_LEN], el[3][EDGE_LEN];
     __align__(16) Px srcS[3][1024];   // the source of the leaf's tx blocks (Y, U, V) when <= 32 x 32, staged once per
                                       // leaf with 16-byte vector stores
-    int16_t cfl[256];
+    int16_t cfl[SS ? 256 : 1024];   // CfL luma values of a chroma block up to 16 x 16 (4:2:0) / 32 x 32 (4:4:4)
     int satd[32];
     int cand[32];
     int job;
 };
-template <typename Px> struct RcSmem {
+template <typename Px, int SS> struct RcSmem {
     RateStage T;                         // scans, base-context offsets (and the cost table of q-context 0)
     uint16_t cost[3][NCDF];              // the cost tables of q-contexts 1 .. 3 (the images of a batch mix qindex)
     FrameDesc F[RC_WARPS];               // each warp's copy of the descriptor of the image it works on
-    RcWarp<Px> w[RC_WARPS];
+    RcWarp<Px, SS> w[RC_WARPS];
 };
-static_assert(offsetof(RcWarp<uint8_t>, srcS) % 16 == 0 && sizeof(RcWarp<uint8_t>) % 16 == 0 && offsetof(RcSmem<uint8_t>, w) % 16 == 0 &&
-                  offsetof(RcSmem<uint8_t>, cost) % 16 == 0 && offsetof(RcSmem<uint8_t>, F) % 16 == 0 && sizeof(FrameDesc) % 16 == 0,
-              "the staged sources, tables and descriptors take 16-byte vector stores");
+template <typename Px, int SS> constexpr bool rc_smem_ok() {
+    typedef RcWarp<Px, SS> Wt;
+    typedef RcSmem<Px, SS> St;
+    return sizeof(St) <= 227 * 1024 && offsetof(Wt, srcS) % 16 == 0 && sizeof(Wt) % 16 == 0 && offsetof(St, w) % 16 == 0 &&
+           offsetof(St, cost) % 16 == 0 && offsetof(St, F) % 16 == 0;
+}
+static_assert(rc_smem_ok<uint8_t, 1>() && rc_smem_ok<uint8_t, 0>() && rc_smem_ok<uint16_t, 1>() && rc_smem_ok<uint16_t, 0>() &&
+                  sizeof(FrameDesc) % 16 == 0,
+              "the closed loop's shared memory: at most 227 KB, staged sources and descriptors 16-byte aligned");
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
     int v;
@@ -110,6 +116,41 @@ __device__ void rc_reconstruct(int txSz, int txType, int16_t *q, int dcQ, int ac
         int v = (int)pred[p] + (any ? buf[i * TS + j] : 0);
         v = min(max(v, 0), (1 << BD) - 1);
         dst[(size_t)i * pitch + j] = (Px)v;
+    }
+    __syncwarp();
+}
+
+// the edges of a W x H (<= 32 x 32) tx block at (px, py) of plane pl from the reconstruction, whole warp: the rule of
+// the reference's rec_edges (availability, above-right / below-left reach, frame clamp), as the leaf's first tx blocks
+template <int BD, typename Px>
+__device__ void rc_edges_rec(const FrameDesc &F, int pl, int px, int py, int W, int H, int haveL, int haveA, int haveAR, int haveBL, Px *A, Px *L) {
+    const int lane = lane_id();
+    const int ss = pl ? F.ssx : 0;
+    const Px *rp = (const Px *)F.rec[pl];
+    const int pitch = F.rpitch[pl], n = W + H;
+    const int aLim = min(px + 2 * W - 1, ((F.MiCols * 4) >> ss) - 1), lLim = min(py + 2 * H - 1, ((F.MiRows * 4) >> ss) - 1);
+    Px ra[2], rl[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const int i = lane + 32 * k;
+        ra[k] = i < n ? ldcg(rp + (size_t)(py - 1) * pitch + min(px + i, aLim)) : (Px)0;
+        rl[k] = i < n ? ldcg(rp + (size_t)min(py + i, lLim) * pitch + px - 1) : (Px)0;
+    }
+    const Px rcorner = ldcg(rp + (size_t)(py - 1) * pitch + px - 1);
+    const Px aW = (Px)__shfl_sync(0xffffffffu, (int)ra[0], W - 1), lH = (Px)__shfl_sync(0xffffffffu, (int)rl[0], H - 1);
+    const Px a0 = (Px)__shfl_sync(0xffffffffu, (int)ra[0], 0), l0 = (Px)__shfl_sync(0xffffffffu, (int)rl[0], 0);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const int i = lane + 32 * k;
+        if (i < n) {
+            A[i] = haveA ? ((!haveAR && i >= W) ? aW : ra[k]) : (haveL ? l0 : (Px)((1 << (BD - 1)) - 1));
+            L[i] = haveL ? ((!haveBL && i >= H) ? lH : rl[k]) : (haveA ? a0 : (Px)((1 << (BD - 1)) + 1));
+        }
+    }
+    if (lane == 0) {
+        const Px c = (haveA && haveL) ? rcorner : haveA ? a0 : haveL ? l0 : (Px)(1 << (BD - 1));
+        A[-1] = c;
+        L[-1] = c;
     }
     __syncwarp();
 }
@@ -198,8 +239,8 @@ __device__ __forceinline__ void rc_txb_ctx(const FrameDesc &F, int plane, int tx
     rc_txb_ctx_finish(F, c, plane, txSz, bsize, skipCtx, dcCtx);
 }
 
-// a W x H (<= 32 x 32) block of 8-bit samples at (x, y) of a plane into dst (row stride W), vector loads of up to 16
-// bytes (rows and x are aligned to the block width)
+// a block of H rows of W bytes (<= 64; a W x H <= 32 x 32 block of samples) at src (row pitch in bytes) into dst (row
+// stride W bytes), vector loads of up to 16 bytes (rows and the block's first byte are aligned to its width)
 __device__ __forceinline__ void stage_block(const uint8_t *src, int pitch, int W, int H, uint8_t *dst) {
     const int lane = lane_id();
     if (W >= 16) {
@@ -296,8 +337,60 @@ __device__ __forceinline__ void push_ready(const FrameDesc &F, uint32_t id) {
     asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(F.readyQ + pos), "l"(v) : "memory");
 }
 
+// The further chroma tx blocks of plane pl of a 4:4:4 block with a 64-sample side (2 or 4 per plane in raster order;
+// the first is coded by the caller, the block's mode bestC chosen on it): each takes its edges from the reconstruction
+// (the block's earlier tx blocks included), its own coefficient contexts and a closed-loop quantisation of the chosen
+// mode (the reference's rc_chroma, k_recon.cuh:1636-1678); tx blocks that start outside the coded area are not coded.
+// tIdx counts the leaf's coded chroma tx blocks (txb slot txb0 + tIdx, coefficients at coef0 + tIdx x the tx area).
+// Returns the OR of the eobs.
 template <int BD, typename Px>
-__device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, int sb, int li, unsigned long long *trace) {
+__device__ __noinline__ int rc_chroma_more(const FrameDesc &F, RcWarp<Px, 0> &Wp, const RateTabs &T, int sb, int li, int pl, int txSz, int uvType,
+                                           int bestC, int bsize, int cx, int cy, int csr, int csc, int nTxX, int nTxY, int availLC, int availUC,
+                                           int tC0, int tR0, int sbW4, int sbH4, int txb0, int coef0, int *tIdx) {
+    const int lane = lane_id();
+    const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H), nq = min(W, 32) * min(H, 32);
+    const int bw = bw4(bsize), bh = bh4(bsize);
+    const int cx4 = cx >> 2, cy4 = cy >> 2, cCols4 = F.MiCols, cRows4 = F.MiRows;   // 4:4:4: plane units = luma units
+    const uint8_t *ordmap = F.ordmap + (size_t)sb * 256;
+    int eobs = 0;
+    for (int t = 1; t < nTxX * nTxY; t++) {
+        const int tx = t % nTxX, ty = t / nTxX, ox = tx * W, oy = ty * H;
+        if (cx4 + (ox >> 2) >= cCols4 || cy4 + (oy >> 2) >= cRows4) continue;
+        const int r4 = csr + (oy >> 2), c4 = csc + (ox >> 2);   // SB-relative 4x4 units
+        // BlockDecoded: the leaves before this one (the SB's leaf map and its above / left rule), and this leaf's tx
+        // blocks before t
+        auto dec = [&](int yy, int xx) -> bool {
+            if (yy >= csr && xx >= csc && yy < csr + bh && xx < csc + bw) return ((yy - csr) * 4 / H) * nTxX + ((xx - csc) * 4 / W) < t;
+            if (yy < 0) return xx < sbW4;
+            if (xx < 0) return yy < sbH4 && yy != 16;
+            if (yy >= 16 || xx >= 16) return false;
+            return ordmap[yy * 16 + xx] < li;
+        };
+        const int haveL = availLC || tx > 0, haveA = availUC || ty > 0;
+        const int haveAR = dec(r4 - 1, c4 + (W >> 2)), haveBL = dec(r4 + (H >> 2), c4 - 1);
+        Px *A = Wp.ea[pl] + EDGE_OFF, *L = Wp.el[pl] + EDGE_OFF;
+        rc_edges_rec<BD, Px>(F, pl, cx + ox, cy + oy, W, H, haveL, haveA, haveAR, haveBL, A, L);
+        const int dcv = warp_dc<BD>(A, L, haveL, haveA, lw, lh);
+        const int m = cand_mode(bestC);
+        grp_predict(m, pangle(m, cand_delta(bestC)), lw, lh, A, L, dcv, Wp.pred, lane, 32);
+        __syncwarp();
+        __threadfence_block();   // the context maps of this leaf's earlier tx blocks (written by this warp)
+        int sc, dcc;
+        rc_txb_ctx(F, pl, txSz, cx4 + (ox >> 2), cy4 + (oy >> 2), bsize, tC0, tR0, &sc, &dcc);
+        const EvalIn e{uvType, pl, sc, dcc, 0, F.dcQ, F.acQ, T};
+        const Px *so = (const Px *)F.src[pl] + (size_t)(cy + oy) * F.spitch[pl] + cx + ox;
+        int16_t *lv = Wp.qb[pl - 1];
+        grp_eval<BD, Px>(txSz, ResFn<Px>{so, F.spitch[pl], Wp.pred, lw, nullptr}, e, Wp.buf, lv, lane, 32);
+        Px *dst = (Px *)F.rec[pl] + (size_t)(cy + oy) * F.rpitch[pl] + cx + ox;
+        rc_reconstruct<BD, Px>(txSz, uvType, lv, F.dcQ, F.acQ, Wp.pred, dst, F.rpitch[pl], Wp.buf);
+        eobs |= rc_record(F, T, sb, pl, txSz, uvType, cx4 + (ox >> 2), cy4 + (oy >> 2), lv, txb0 + *tIdx, coef0 + *tIdx * nq);
+        (*tIdx)++;
+    }
+    return eobs;
+}
+
+template <int BD, typename Px, int SS>
+__device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &T, int sb, int li, unsigned long long *trace) {
     const int lane = lane_id();
     const Leaf lf = F.leaves[(size_t)sb * SB_MAX_LEAVES + li];
     const int bsize = lf.bsize;
@@ -305,7 +398,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
     const int sbx = sbc * 64, sby = sbr * 64;
     const int x = sbx + lf.x4 * 4, y = sby + lf.y4 * 4, mi_row = y >> 2, mi_col = x >> 2;
     const int bw = bw4(bsize), bh = bh4(bsize);
-    const int ss = F.ssx;
+    const int ss = SS;   // (the image's F.ssx: one instance per subsampling)
     const uint8_t *ordmap = F.ordmap + (size_t)sb * 256;
     int tC0, tC1, tR0, tR1;
     tile_box(F, mi_row, mi_col, tC0, tC1, tR0, tR1);
@@ -355,7 +448,9 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
         const CtxLd cl = rc_txb_ctx_load(F, 0, txSz, x >> 2, y >> 2, tC0, tR0);
         const int haveAR = decoded(0, lf.y4 - 1, lf.x4 + (W >> 2)), haveBL = decoded(0, lf.y4 + (H >> 2), lf.x4 - 1);
         const bool staged = W <= 32 && H <= 32;
-        if (staged) stage_block((const uint8_t *)F.src[0] + (size_t)y * F.spitch[0] + x, F.spitch[0], W, H, (uint8_t *)Wp.srcS[0]);
+        if (staged)
+            stage_block((const uint8_t *)((const Px *)F.src[0] + (size_t)y * F.spitch[0] + x), F.spitch[0] * (int)sizeof(Px), W * (int)sizeof(Px), H,
+                        (uint8_t *)Wp.srcS[0]);
         // ---- the edges: rec_edges' rule (availability, above-right / below-left reach, frame clamp) on the raw samples ----
         Px *A = Wp.ea[0] + EDGE_OFF, *L = Wp.el[0] + EDGE_OFF;
         {
@@ -510,8 +605,9 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
         }
         const CtxLd cl1 = rc_txb_ctx_load(F, 1, txSz, cx4, cy4, tC0, tR0), cl2 = rc_txb_ctx_load(F, 2, txSz, cx4, cy4, tC0, tR0);
         const int haveAR = decoded(ss, csr - 1, csc + (W >> 2)), haveBL = decoded(ss, csr + (H >> 2), csc - 1);
-        stage_block((const uint8_t *)F.src[1] + (size_t)cy * F.spitch[1] + cx, F.spitch[1], W, H, (uint8_t *)Wp.srcS[1]);
-        stage_block((const uint8_t *)F.src[2] + (size_t)cy * F.spitch[2] + cx, F.spitch[2], W, H, (uint8_t *)Wp.srcS[2]);
+        for (int q = 1; q <= 2; q++)
+            stage_block((const uint8_t *)((const Px *)F.src[q] + (size_t)cy * F.spitch[q] + cx), F.spitch[q] * (int)sizeof(Px), W * (int)sizeof(Px), H,
+                        (uint8_t *)Wp.srcS[q]);
         // ---- the edges of U and V (rec_edges' rule on the raw samples) ----
         Px *A[3], *L[3];
         int dcv[3];
@@ -696,17 +792,30 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
         const bool cfl = bestC == 255;
         uv = cfl ? AV1G_UV_CFL_PRED : cand_mode(bestC);
         const int uvType = chroma_tx_type(txSz, uv);
+        // chroma tx blocks per plane (the reference's rc_chroma, k_recon.cuh:1588-1680): one in 4:2:0 and in 4:4:4 up
+        // to 32 x 32; 2 or 4 in raster order for a 4:4:4 block with a 64-sample side (rc_chroma_more codes those after
+        // the first).  Record order: U's tx blocks, then V's.
+        const int nTxX = ss ? 1 : max(1, 4 * bw / W), nTxY = ss ? 1 : max(1, 4 * bh / H);
+        const int yt = ST(Max_Tx_Size_Rect)[bsize];
+        const int lumaN = min(txw(yt), 32) * min(txh(yt), 32);
+        int tIdx = 0;   // coded chroma tx blocks so far
         for (int pl = 1; pl <= 2; pl++) {
+            Px *dst = (Px *)F.rec[pl] + (size_t)cy * F.rpitch[pl] + cx;
+            int16_t *lv = Wp.qb[pl - 1];
             predict(pl, bestC, Wp.pred, lane, 32);
             __syncwarp();
             const EvalIn e{uvType, pl, skipCtx[pl], dcCtx[pl], 0, F.dcQ, F.acQ, T};
-            int16_t *lv = Wp.qb[pl - 1];
             grp_eval<BD, Px>(txSz, ResFn<Px>{sP[pl], W, Wp.pred, lw, nullptr}, e, Wp.buf, lv, lane, 32);
-            Px *dst = (Px *)F.rec[pl] + (size_t)cy * F.rpitch[pl] + cx;
             rc_reconstruct<BD, Px>(txSz, uvType, lv, F.dcQ, F.acQ, Wp.pred, dst, F.rpitch[pl], Wp.buf);
-            const int yt = ST(Max_Tx_Size_Rect)[bsize];
-            const int off = coefBase + min(txw(yt), 32) * min(txh(yt), 32) + (pl - 1) * nq;
-            const int e2 = rc_record(F, T, sb, pl, txSz, uvType, cx4, cy4, lv, txbBase + pl, off);
+            int e2 = rc_record(F, T, sb, pl, txSz, uvType, cx4, cy4, lv, txbBase + 1 + tIdx, coefBase + lumaN + tIdx * nq);
+            tIdx++;
+            if constexpr (SS == 0) {
+                if (nTxX * nTxY > 1) {   // (4:4:4, a 64-sample side: rare, out of line)
+                    const int sbW4 = tC1 - sbc * 16, sbH4 = tR1 - sbr * 16;
+                    e2 |= rc_chroma_more<BD, Px>(F, Wp, T, sb, li, pl, txSz, uvType, bestC, bsize, cx, cy, csr, csc, nTxX, nTxY, availLC,
+                                                 availUC, tC0, tR0, sbW4, sbH4, txbBase + 1, coefBase + lumaN, &tIdx);
+                }
+            }
             if (pl == 1) eobU = e2; else eobV = e2;
         }
         duv = cfl ? 0 : cand_delta(bestC);
@@ -736,17 +845,18 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px> &Wp, const RateTabs &T, i
     }
 }
 
-// Persistent grid of independent warps over the ready queue of a batch of nImg images (Fs: their descriptors in
-// device memory): a warp takes the next slot, waits until a leaf has been written there (bounded in time), brings the
+// Persistent grid of independent warps over the ready queue of a batch of nImg images of one format (Fs: their
+// descriptors in device memory; one instance per bit depth BD and chroma subsampling SS, a batch's images run in groups
+// of one format): a warp takes the next slot, waits until a leaf has been written there (bounded in time), brings the
 // descriptor of the leaf's image into its shared copy when the image changes, and runs the leaf.
 constexpr unsigned long long READY_WAIT_NS = 4000000000ull;
-template <int BD>
+template <int BD, int SS>
 __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__restrict__ Fs, int nImg) {
     typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    RcSmem<Px> &S = *reinterpret_cast<RcSmem<Px> *>(smem_raw);
+    RcSmem<Px, SS> &S = *reinterpret_cast<RcSmem<Px, SS> *>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = lane_id();
-    RcWarp<Px> &Wp = S.w[warp];
+    RcWarp<Px, SS> &Wp = S.w[warp];
     FrameDesc &F = S.F[warp];
     {   // all four cost tables (q-context 0 in the RateStage), the scans and base-context offsets
         rate_tabs_stage(S.T, 0, threadIdx.x, blockDim.x);
@@ -795,7 +905,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
         }
         const RateTabs T{F.qctx == 0 ? S.T.cost : S.cost[F.qctx - 1], S.T.scan, S.T.baseCtx};
         unsigned long long *trace = traceBase ? traceBase + (size_t)h * 4 : nullptr;
-        rc_leaf<BD, Px>(F, Wp, T, (int)(id >> 8), (int)(id & 255), trace);
+        rc_leaf<BD, Px, SS>(F, Wp, T, (int)(id >> 8), (int)(id & 255), trace);
     }
 }
 
@@ -829,10 +939,18 @@ __global__ void k_leaf_prep(const __grid_constant__ FrameDesc F, int nSb) {
             const int yt = ST(Max_Tx_Size_Rect)[l.bsize];
             nt += 1;
             ncf += min(txw(yt), 32) * min(txh(yt), 32);
-            if (has_chroma(l.bsize, sbr * 16 + l.y4, sbc * 16 + l.x4, F.ssx)) {
-                const int ut = uv_tx_size(l.bsize, F.ssx);
-                nt += 2;
-                ncf += 2 * min(txw(ut), 32) * min(txh(ut), 32);
+            const int mi_row = sbr * 16 + l.y4, mi_col = sbc * 16 + l.x4;
+            if (has_chroma(l.bsize, mi_row, mi_col, F.ssx)) {
+                // 2 x the coded chroma tx blocks of a plane (more than one: 4:4:4 blocks with a 64-sample side)
+                const int ut = uv_tx_size(l.bsize, F.ssx), ss = F.ssx;
+                const int W = txw(ut), H = txh(ut);
+                const int nTxX = ss ? 1 : max(1, 4 * bw4(l.bsize) / W), nTxY = ss ? 1 : max(1, 4 * bh4(l.bsize) / H);
+                const int cx4 = mi_col >> ss, cy4 = mi_row >> ss, cCols4 = F.MiCols >> ss, cRows4 = F.MiRows >> ss;
+                int nc = 0;
+                for (int t = 0; t < nTxX * nTxY; t++)
+                    nc += t == 0 || (cx4 + (t % nTxX) * (W >> 2) < cCols4 && cy4 + (t / nTxX) * (H >> 2) < cRows4);
+                nt += 2 * nc;
+                ncf += 2 * nc * min(W, 32) * min(H, 32);
             }
         }
         SbCount c;

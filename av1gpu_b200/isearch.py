@@ -32,8 +32,8 @@ class IsParams(C.Structure):
 
 
 class IsFrame(C.Structure):
-    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("qindex", C.c_int32), ("pad", C.c_int32),
-                ("planes", C.c_void_p * 3), ("pitch", C.c_int32 * 3), ("pad2", C.c_int32)]
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("qindex", C.c_int32), ("bit_depth", C.c_int32),
+                ("planes", C.c_void_p * 3), ("pitch", C.c_int32 * 3), ("chroma_444", C.c_int32)]
 
 
 class IsTimes(C.Structure):
@@ -46,7 +46,7 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_record_copy", "is_record_device", "is_times_get", "is_test_fwd_quant", "is_test_inverse",
            "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32", "is_set_trace", "is_get_trace",
            "is_fwd_quant_static", "is_encode_batch", "is_batch_counts", "is_batch_copy", "is_set_batch_options",
-           "is_autotune_batch", "is_workspace_bytes", "is_sl_create", "is_sl_destroy", "is_sl_set_weights",
+           "is_autotune_batch", "is_workspace_bytes", "is_workspace_bytes_format", "is_sl_create", "is_sl_destroy", "is_sl_set_weights",
            "is_sl_get_weights", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset", "is_set_shortlist_model"]
 
 _lib = None
@@ -88,6 +88,7 @@ def load_library():
     L.is_batch_copy.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp * 3, vp]
     L.is_set_batch_options.argtypes = [vp, C.c_int, C.c_int, C.c_int]
     L.is_workspace_bytes.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64)]
+    L.is_workspace_bytes_format.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64)]
     L.is_sl_create.argtypes = [C.c_int, C.c_int, C.POINTER(vp)]
     L.is_sl_destroy.argtypes = [vp]
     L.is_sl_destroy.restype = None
@@ -104,12 +105,26 @@ def load_library():
     return L
 
 
-def workspace_bytes(width, height):
+def workspace_bytes(width, height, bit_depth=8, chroma_444=False):
     """Device workspace of one image in a batch (bytes); no GPU needed."""
     b = C.c_uint64()
-    if load_library().is_workspace_bytes(width, height, C.byref(b)) != 0:
-        raise ValueError("invalid image size %dx%d" % (width, height))
+    if load_library().is_workspace_bytes_format(width, height, bit_depth, int(bool(chroma_444)), C.byref(b)) != 0:
+        raise ValueError("invalid image %dx%d (bit depth %d, 4:4:4 %s)" % (width, height, bit_depth, chroma_444))
     return b.value
+
+
+def plane_format(planes):
+    """(bit depth, 4:4:4) of (Y, U, V) planes: 16-bit samples are 10-bit, chroma of the luma size is 4:4:4."""
+    y, u = planes[0], planes[1]
+    dt = str(y.dtype)
+    bd = 10 if ("uint16" in dt or "int16" in dt) else 8
+    return bd, tuple(u.shape) == tuple(y.shape)
+
+
+def _recon_arrays(width, height, bit_depth, chroma_444):
+    dt = np.uint16 if bit_depth == 10 else np.uint8
+    cw, ch = (width, height) if chroma_444 else ((width + 1) // 2, (height + 1) // 2)
+    return [np.zeros((height, width), dt), np.zeros((ch, cw), dt), np.zeros((ch, cw), dt)]
 
 
 def probe_int32(device=0):
@@ -136,8 +151,9 @@ def host_tables(qctx, qindex=120):
 class Record:
     """One encoded image: the DecisionRecord arrays (decode order) and the cropped reconstruction."""
 
-    def __init__(self, width, height, qindex, blocks, block_txb, txb, coeffs, recon, times):
+    def __init__(self, width, height, qindex, blocks, block_txb, txb, coeffs, recon, times, bit_depth=8, chroma_444=False):
         self.width, self.height, self.qindex = width, height, qindex
+        self.bit_depth, self.chroma_444 = bit_depth, chroma_444
         self.blocks, self.block_txb, self.txb, self.coeffs = blocks, block_txb, txb, coeffs
         self.recon = recon
         self.times = times
@@ -173,25 +189,28 @@ class Encoder:
             raise RuntimeError("%s failed (%d: %s): %s" % (what, rc, IS_ERRORS.get(rc, "?"), msg))
 
     @staticmethod
-    def _frame(width, height, qindex, ptrs, pitches):
+    def _frame(planes, qindex, host):
+        """is_frame of (Y, U, V) planes: numpy arrays (host) or torch CUDA tensors; uint8 8-bit, 16-bit samples 10-bit."""
+        y = planes[0]
+        bd, c444 = plane_format(planes)
         f = IsFrame()
-        f.width, f.height, f.qindex = width, height, qindex
+        f.width, f.height, f.qindex = y.shape[1], y.shape[0], qindex
+        f.bit_depth, f.chroma_444 = bd, int(c444)
         for p in range(3):
-            f.planes[p] = ptrs[p]
-            f.pitch[p] = pitches[p]
+            f.planes[p] = planes[p].ctypes.data if host else planes[p].data_ptr()
+            f.pitch[p] = planes[p].strides[0] // planes[p].itemsize if host else planes[p].stride(0)
         return f
 
     def encode_host_async(self, planes, qindex, stream=None):
-        """Queue an encode of host planes (Y, U, V numpy uint8, C-contiguous); returns after the record sizes are known."""
-        y = planes[0]
-        f = self._frame(y.shape[1], y.shape[0], qindex, [p.ctypes.data for p in planes], [p.strides[0] for p in planes])
+        """Queue an encode of host planes (Y, U, V numpy uint8 / uint16, row-contiguous); returns after the record sizes
+        are known."""
+        f = self._frame(planes, qindex, True)
         self._check(self.L.is_encode_host(self.h, C.byref(f), stream), "is_encode_host")
         return f
 
     def encode_device_async(self, planes, qindex, stream=None):
-        """Queue an encode of device planes (torch CUDA uint8 tensors, row-contiguous)."""
-        y = planes[0]
-        f = self._frame(y.shape[1], y.shape[0], qindex, [p.data_ptr() for p in planes], [p.stride(0) for p in planes])
+        """Queue an encode of device planes (torch CUDA uint8 / 16-bit tensors, row-contiguous)."""
+        f = self._frame(planes, qindex, False)
         self._check(self.L.is_encode_device(self.h, C.byref(f), stream), "is_encode_device")
         return f
 
@@ -205,43 +224,39 @@ class Encoder:
         self._check(self.L.is_times_get(self.h, C.byref(t)), "is_times_get")
         return {k: getattr(t, k) for k, _ in IsTimes._fields_}
 
-    def fetch(self, width, height, qindex, out=None):
+    def fetch(self, width, height, qindex, out=None, bit_depth=8, chroma_444=False):
         """Copy the last record and reconstruction to host memory (numpy arrays, or the preallocated `out` dict)."""
         nb, nt, nc = self.counts()
         if out is None:
-            cw, ch = (width + 1) // 2, (height + 1) // 2
             out = {"blocks": np.zeros(nb, BLOCK_DT), "block_txb": np.zeros(nb + 1, np.uint32),
                    "txb": np.zeros(nt, TXB_DT), "coeffs": np.zeros(nc, np.int16),
-                   "recon": [np.zeros((height, width), np.uint8), np.zeros((ch, cw), np.uint8), np.zeros((ch, cw), np.uint8)]}
+                   "recon": _recon_arrays(width, height, bit_depth, chroma_444)}
         rp = (C.c_void_p * 3)(*[r.ctypes.data for r in out["recon"]])
-        pitches = (C.c_int32 * 3)(*[r.strides[0] for r in out["recon"]])
+        pitches = (C.c_int32 * 3)(*[r.strides[0] // r.itemsize for r in out["recon"]])
         self._check(self.L.is_record_copy(self.h, None, out["blocks"].ctypes.data, out["block_txb"].ctypes.data,
                                           out["txb"].ctypes.data, out["coeffs"].ctypes.data, rp, pitches),
                     "is_record_copy")
         return Record(width, height, qindex, out["blocks"][:nb], out["block_txb"][:nb + 1], out["txb"][:nt],
-                      out["coeffs"][:nc], out["recon"], self.times())
+                      out["coeffs"][:nc], out["recon"], self.times(), bit_depth, chroma_444)
 
     def encode(self, planes, qindex):
         """Encode host planes end to end: upload, search, download of the record and the reconstruction."""
-        planes = [np.ascontiguousarray(p, np.uint8) for p in planes]
+        planes = [np.ascontiguousarray(p) for p in planes]
+        bd, c444 = plane_format(planes)
         self.encode_host_async(planes, qindex)
-        return self.fetch(planes[0].shape[1], planes[0].shape[0], qindex)
+        return self.fetch(planes[0].shape[1], planes[0].shape[0], qindex, bit_depth=bd, chroma_444=c444)
 
     def encode_device(self, planes, qindex):
+        bd, c444 = plane_format(planes)
         self.encode_device_async(planes, qindex)
-        return self.fetch(planes[0].shape[1], planes[0].shape[0], qindex)
+        return self.fetch(planes[0].shape[1], planes[0].shape[0], qindex, bit_depth=bd, chroma_444=c444)
 
     # ---- batched form ----
     def _frames(self, images, qindices, host):
         """is_frame array for a list of (Y, U, V) planes: numpy arrays (host) or torch CUDA tensors (device)."""
         fr = (IsFrame * len(images))()
         for i, (planes, q) in enumerate(zip(images, qindices)):
-            y = planes[0]
-            if host:
-                ptrs, pitches = [p.ctypes.data for p in planes], [p.strides[0] for p in planes]
-            else:
-                ptrs, pitches = [p.data_ptr() for p in planes], [p.stride(0) for p in planes]
-            fr[i] = self._frame(y.shape[1], y.shape[0], q, ptrs, pitches)
+            fr[i] = self._frame(planes, q, host)
         return fr
 
     def encode_batch_async(self, images, qindices, host=True, stream=None):
@@ -256,24 +271,27 @@ class Encoder:
         self._check(self.L.is_batch_counts(self.h, i, C.byref(nb), C.byref(nt), C.byref(nc)), "is_batch_counts")
         return nb.value, nt.value, nc.value
 
-    def batch_fetch(self, i, width, height, qindex):
+    def batch_fetch(self, i, width, height, qindex, bit_depth=8, chroma_444=False):
         nb, nt, nc = self.batch_counts(i)
-        cw, ch = (width + 1) // 2, (height + 1) // 2
         out = {"blocks": np.zeros(nb, BLOCK_DT), "block_txb": np.zeros(nb + 1, np.uint32), "txb": np.zeros(nt, TXB_DT),
-               "coeffs": np.zeros(nc, np.int16),
-               "recon": [np.zeros((height, width), np.uint8), np.zeros((ch, cw), np.uint8), np.zeros((ch, cw), np.uint8)]}
+               "coeffs": np.zeros(nc, np.int16), "recon": _recon_arrays(width, height, bit_depth, chroma_444)}
         rp = (C.c_void_p * 3)(*[r.ctypes.data for r in out["recon"]])
-        pitches = (C.c_int32 * 3)(*[r.strides[0] for r in out["recon"]])
+        pitches = (C.c_int32 * 3)(*[r.strides[0] // r.itemsize for r in out["recon"]])
         self._check(self.L.is_batch_copy(self.h, i, None, out["blocks"].ctypes.data, out["block_txb"].ctypes.data,
                                          out["txb"].ctypes.data, out["coeffs"].ctypes.data, rp, pitches), "is_batch_copy")
         return Record(width, height, qindex, out["blocks"], out["block_txb"], out["txb"], out["coeffs"], out["recon"],
-                      self.times())
+                      self.times(), bit_depth, chroma_444)
 
     def encode_batch(self, images, qindices):
-        """Encode a list of host images ((Y, U, V) uint8 planes) with their qindices in one batch; a list of Records."""
-        images = [[np.ascontiguousarray(p, np.uint8) for p in planes] for planes in images]
+        """Encode a list of host images ((Y, U, V) planes, uint8 8-bit or uint16 10-bit, 4:2:0 or 4:4:4) with their
+        qindices in one batch; a list of Records."""
+        images = [[np.ascontiguousarray(p) for p in planes] for planes in images]
         self.encode_batch_async(images, qindices, host=True)
-        return [self.batch_fetch(i, im[0].shape[1], im[0].shape[0], q) for i, (im, q) in enumerate(zip(images, qindices))]
+        out = []
+        for i, (im, q) in enumerate(zip(images, qindices)):
+            bd, c444 = plane_format(im)
+            out.append(self.batch_fetch(i, im[0].shape[1], im[0].shape[0], q, bd, c444))
+        return out
 
     def set_batch_options(self, use_graph=False, front_streams=0, recon_ctas=0):
         self._check(self.L.is_set_batch_options(self.h, 1 if use_graph else 0, front_streams, recon_ctas),

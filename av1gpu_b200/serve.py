@@ -57,9 +57,13 @@ def latency_stats(requests):
 
 class Server:
     def __init__(self, device=0, hbm_budget=None, pipelines=2, max_batch=64, recon_ctas=0, use_graph=False):
-        from .isearch import Encoder, workspace_bytes
+        from .isearch import Encoder, workspace_bytes, plane_format
         import torch
-        self._wsb = workspace_bytes
+
+        def wsb(planes):   # the workspace of an image in its own format (8 / 10-bit, 4:2:0 / 4:4:4)
+            bd, c444 = plane_format(planes)
+            return workspace_bytes(planes[0].shape[1], planes[0].shape[0], bd, c444)
+        self._wsb = wsb
         if hbm_budget is None:   # half of the free device memory
             free, _ = torch.cuda.mem_get_info(device)
             hbm_budget = free // 2
@@ -80,7 +84,7 @@ class Server:
         self.encs = []
 
     def submit(self, req):
-        req.nbytes = self._wsb(req.planes[0].shape[1], req.planes[0].shape[0])
+        req.nbytes = self._wsb(req.planes)
         with self._cv:
             self._pending.append(req)
             self._cv.notify()
@@ -109,7 +113,7 @@ class Server:
         """Serve a list of (arrival time in s from now, planes, qindex); returns the Requests (records filled)."""
         reqs = [Request(i, p, q, None) for i, (_, p, q) in enumerate(arrivals)]
         for r in reqs:
-            r.nbytes = self._wsb(r.planes[0].shape[1], r.planes[0].shape[0])
+            r.nbytes = self._wsb(r.planes)
         self._closed = False
         workers = [threading.Thread(target=self._worker, args=(k,), daemon=True) for k in range(self.pipelines)]
         for w in workers:

@@ -75,3 +75,24 @@ def make_image(width, height, seed, edges=False, bit_depth=8, chroma_444=False):
             v = np.rint(v.astype(np.float64) * 1023.0 / 255.0).astype(np.uint16)
         planes.append(np.ascontiguousarray(v))
     return tuple(planes)
+
+
+def make_smooth_image(width, height, seed, bit_depth=8, chroma_444=False):
+    """A smooth image (low-amplitude gradients and long-period waves, no noise) on which the search keeps large blocks:
+    the 64-sample-side blocks whose 4:4:4 chroma is coded in several tx blocks.  Same plane layout as make_image."""
+    rng = np.random.default_rng(np.random.PCG64(seed))
+    cw, ch = (width, height) if chroma_444 else ((width + 1) // 2, (height + 1) // 2)
+    planes = []
+    for p, (w, h) in enumerate(((width, height), (cw, ch), (cw, ch))):
+        yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+        f = np.full((h, w), 128.0 if p else rng.uniform(60, 180))
+        for _ in range(2):
+            th = rng.uniform(0, np.pi)
+            f += rng.uniform(5, 25) * ((xx - w / 2) * np.cos(th) + (yy - h / 2) * np.sin(th)) / max(w, h)
+        th, per = rng.uniform(0, np.pi), rng.uniform(60, 200)
+        f += rng.uniform(2, 8) * np.sin(2 * np.pi * (xx * np.cos(th) + yy * np.sin(th)) / per)
+        v = np.clip(np.rint(f), 0, 255).astype(np.uint8)
+        if bit_depth == 10:
+            v = np.rint(v.astype(np.float64) * 1023.0 / 255.0).astype(np.uint16)
+        planes.append(np.ascontiguousarray(v))
+    return tuple(planes)

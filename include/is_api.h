@@ -38,23 +38,25 @@ extern "C" {
 #define IS_ERR_TOO_LARGE -6 /* the request does not fit the fixed scratch of is_fwd_quant_static */
 
 typedef struct is_params {
-    int32_t bit_depth;      /* 8 */
-    int32_t chroma_444;     /* 0 (4:2:0) */
+    int32_t bit_depth;      /* 8 or 10: the format of frames whose own bit_depth is 0 */
+    int32_t chroma_444;     /* 0 (4:2:0) or 1 (4:4:4), likewise */
     int32_t device;         /* CUDA device ordinal */
     int32_t reserved[5];    /* 0 */
 } is_params;
 
 typedef struct is_handle is_handle;
 
-/* One image.  planes: Y, U, V of width x height (chroma ((width+1)/2) x ((height+1)/2)), pitch in samples.
+/* One image.  planes: Y, U, V of width x height (4:2:0 chroma ((width+1)/2) x ((height+1)/2), 4:4:4 chroma width x
+ * height), samples uint8_t (8-bit) or uint16_t (10-bit), pitch in samples.  bit_depth 0 takes the handle's format
+ * (is_params); 8 or 10 with chroma_444 0 / 1 gives the frame's own, so one batch may mix formats.
  * is_encode_device: device pointers; is_encode_host: host pointers (pinned memory gives the fastest upload). */
 typedef struct is_frame {
     int32_t width, height;
     int32_t qindex;         /* base_q_idx 1..255 */
-    int32_t pad;
+    int32_t bit_depth;      /* 0 (the handle's), 8 or 10 */
     const void *planes[3];
     int32_t pitch[3];
-    int32_t pad2;
+    int32_t chroma_444;     /* with bit_depth 8 / 10: 0 (4:2:0) or 1 (4:4:4) */
 } is_frame;
 
 /* Stage times of the last encode (ms, CUDA events on the handle's stream), cf. the reference's GpTimes
@@ -99,6 +101,8 @@ int is_set_batch_options(is_handle *h, int use_graph, int front_streams, int rec
 /* Device workspace of one image of width x height in a batch (bytes; host only, no GPU needed): what admission by
  * HBM budget counts. */
 int is_workspace_bytes(int width, int height, uint64_t *bytes);
+/* the same for a frame of the given format (bit_depth 8 / 10, chroma_444 0 / 1) */
+int is_workspace_bytes_format(int width, int height, int bit_depth, int chroma_444, uint64_t *bytes);
 /* Autotuner: times the batch with 1, 2 and 4 front-end streams (two runs each, the second timed) and keeps the
  * fastest for the handle; returns the choice and its time (ms). */
 int is_autotune_batch(is_handle *h, const is_frame *frames, int n, int from_host, int *front_streams, float *ms);

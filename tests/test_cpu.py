@@ -46,6 +46,22 @@ def test_oracle_recon_is_av1core(w, h, q, seed):
         assert np.array_equal(rec[p], r.recon[p])
 
 
+@pytest.mark.parametrize("bd,c444,w,h,q,smooth", [(10, False, 200, 136, 120, False), (8, True, 200, 136, 120, False),
+                                                  (10, True, 150, 100, 180, True), (8, True, 192, 160, 200, True)])
+def test_oracle_formats_recon_is_av1core(bd, c444, w, h, q, smooth):
+    """10-bit and 4:4:4 oracle records are valid DecisionRecords whose av1core reconstruction is the oracle's own,
+    including 4:4:4 blocks with a 64-sample side (2 or 4 chroma tx blocks per plane)."""
+    from av1gpu_b200 import synth
+    planes = (synth.make_smooth_image(w, h, 7, bd, c444) if smooth else synth.make_image(w, h, 7, edges=True, bit_depth=bd,
+                                                                                          chroma_444=c444))
+    r = O.encode(planes, q, bit_depth=bd, chroma_444=c444)
+    if smooth:
+        assert np.isin(r.blocks["bsize"], [10, 11, 12, 20, 21]).any()   # a 64-sample side
+    rec, _ = O.av1g_recon(w, h, q, r.blocks, r.block_txb, r.txb, r.coeffs, bit_depth=bd, chroma_444=c444)
+    for p in range(3):
+        assert np.array_equal(rec[p], r.recon[p])
+
+
 def test_oracle_thread_independent():
     """The wavefront over host threads gives the same record as one thread."""
     from av1gpu_b200 import synth
