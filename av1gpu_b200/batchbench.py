@@ -1,0 +1,107 @@
+"""The batched-form workload: many images of uneven size, format and qindex searched plain (one image at a time), as
+one batch, and as one batch with the learned shortlist.
+
+    python -m av1gpu_b200.batchbench [--images 256] [--max-mp 24] [--seed 3]
+
+Images are seeded crops of two synthetic 6000 x 4000 pictures (no dataset is named for this workload): log-uniform
+area 0.18 .. 24 MP, aspect 1:3 .. 3:1, 80 % 8-bit 4:2:0 and 20 % 10-bit 4:4:4, qindex uniform 40 .. 220.  Inputs are
+on the device before a timed region; the batch is captured as a CUDA graph (the captured run untimed) with the front-end
+stream count from is_autotune_batch on the first images.  One JSON line per form; MP = visible luma megapixels.
+"""
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+
+def workload(n, seed, max_mp=24.0, min_mp=0.18, frac10=0.2):
+    """n (planes, qindex) pairs: crops of an 8-bit 4:2:0 and a 10-bit 4:4:4 synthetic 6000 x 4000 picture."""
+    from . import synth
+    rng = np.random.default_rng(seed)
+    W, H = 6000, 4000
+    base8 = synth.make_image(W, H, seed, edges=True)
+    base10 = synth.make_image(W, H, seed + 1, edges=True, bit_depth=10, chroma_444=True)
+    out = []
+    for _ in range(n):
+        area = float(np.exp(rng.uniform(np.log(min_mp * 1e6), np.log(max_mp * 1e6))))
+        ar = float(np.exp(rng.uniform(np.log(1 / 3), np.log(3))))
+        w = int(min(W, max(16, np.sqrt(area * ar)))) & ~1
+        h = int(min(H, max(16, np.sqrt(area / ar)))) & ~1
+        x0, y0 = int(rng.integers(0, W - w + 1)) & ~1, int(rng.integers(0, H - h + 1)) & ~1
+        if rng.random() < frac10:
+            planes = [np.ascontiguousarray(p[y0:y0 + h, x0:x0 + w]) for p in base10]
+        else:
+            y, u, v = base8
+            planes = [np.ascontiguousarray(y[y0:y0 + h, x0:x0 + w]), np.ascontiguousarray(u[y0 // 2:(y0 + h) // 2, x0 // 2:(x0 + w) // 2]),
+                      np.ascontiguousarray(v[y0 // 2:(y0 + h) // 2, x0 // 2:(x0 + w) // 2])]
+        out.append((planes, int(rng.integers(40, 221))))
+    return out
+
+
+def main():
+    import torch
+    from .isearch import Encoder, plane_format
+    from .shortlist import load_weights
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--images", type=int, default=256)
+    ap.add_argument("--max-mp", type=float, default=24.0)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--tune-images", type=int, default=24, help="images the front-end stream count is tuned on")
+    ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "shortlist_weights.npz"))
+    ap.add_argument("--tau", type=float, default=0.9)
+    ap.add_argument("--max-modes", type=int, default=6)
+    ap.add_argument("--rd-k", type=int, default=2)
+    args = ap.parse_args()
+    t0 = time.time()
+    work = workload(args.images, args.seed, args.max_mp)
+    gen_s = time.time() - t0
+    dev = [[torch.from_numpy(p.astype(np.int16) if p.dtype == np.uint16 else p).cuda() for p in planes] for planes, _ in work]
+    qs = [q for _, q in work]
+    mp = sum(p[0].shape[0] * p[0].shape[1] for p, _ in work) / 1e6
+    fmt = [plane_format(p) for p, _ in work]
+    n10 = sum(1 for bd, _ in fmt if bd == 10)
+    enc = Encoder(0)
+    base = {"workload": "%d images, log-uniform 0.18-%g MP, aspect 1:3-3:1, %d 8-bit 4:2:0 + %d 10-bit 4:4:4, qindex 40-220"
+                        % (len(work), args.max_mp, len(work) - n10, n10), "mp": round(mp, 1), "data": "synthetic",
+            "generate_s": round(gen_s, 1)}
+
+    def plain():
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for planes, q in zip(dev, qs):
+            enc.encode_device_async(planes, q)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t
+
+    def batched():
+        k, _ = enc.autotune_batch(dev[:args.tune_images], qs[:args.tune_images], host=False)
+        enc.set_batch_options(use_graph=True, front_streams=k)
+        enc.encode_batch_async(dev, qs, host=False)   # captures the graph
+        ts = []
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            enc.encode_batch_async(dev, qs, host=False)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t)
+        enc.set_batch_options(use_graph=False, front_streams=1)
+        return min(ts), k
+
+    plain()   # warm-up (workspace, tables)
+    tp = plain()
+    print(json.dumps({**base, "form": "plain, one image at a time", "mp_per_s": round(mp / tp, 2), "s": round(tp, 3)}), flush=True)
+    tb, k = batched()
+    print(json.dumps({**base, "form": "batched (one batch, CUDA graph)", "mp_per_s": round(mp / tb, 2), "s": round(tb, 3),
+                      "front_streams": k, "x_plain": round(tp / tb, 2)}), flush=True)
+    enc.set_shortlist(load_weights(args.weights), tau=args.tau, max_modes=args.max_modes, rd_k=args.rd_k)
+    ts, k = batched()
+    enc.set_shortlist(None)
+    print(json.dumps({**base, "form": "batched + shortlist (tau %g, max %d modes, rd_k %d)" % (args.tau, args.max_modes, args.rd_k),
+                      "mp_per_s": round(mp / ts, 2), "s": round(ts, 3), "front_streams": k, "x_plain": round(tp / ts, 2)}), flush=True)
+    enc.close()
+
+
+if __name__ == "__main__":
+    main()

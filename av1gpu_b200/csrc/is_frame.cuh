@@ -18,9 +18,10 @@ constexpr int SRC_MARGIN_X = 16, SRC_MARGIN_Y = 1;
 constexpr int SB_MAX_LEAVES = 256;
 constexpr int SB_MAX_TXB = 768;      // luma 256 + chroma 2 x 256 (4:4:4 bound)
 constexpr int SB_MAX_COEF = 12288;   // 3 x 64 x 64
-// dependency entries per SB: a leaf of bw x bh luma 4x4 units has at most 2 bw + 1 + 2 bh luma dependencies, which is
-// at most 5 bw bh, so the leaves of one SB have at most 5 x 256 between them
-constexpr int REV_PER_SB = 1280;
+// dependency entries per SB: a leaf of bw x bh luma 4x4 units has at most 2 bw + 1 + 2 bh luma dependencies (at most
+// 5 bw bh) and, as a 4:2:0 chroma carrier narrower or lower than 8 samples, at most 5 more for its chroma strips; over
+// the 2 x 2 (or 2 x 1) group of such leaves that is at most 8 per unit, so the leaves of one SB have at most 8 x 256
+constexpr int REV_PER_SB = 2048;
 
 struct BlockRes {      // analysis result of one (shape, position): 16 bytes
     long long J;       // best open-loop RD cost (J units)

@@ -308,24 +308,33 @@ __device__ __forceinline__ void tile_box(const FrameDesc &F, int mi_row, int mi_
     tC0 = F.tileColStart[tc]; tC1 = F.tileColStart[tc + 1]; tR0 = F.tileRowStart[tr]; tR1 = F.tileRowStart[tr + 1];
 }
 
-// Luma dependencies of leaf li of SB sb: the distinct leaves (unit_leaf rule) covering a unit of its above strip (row
-// y4 - 1 from the above-left corner to the above-right reach x4 + 2 bw) or of its left strip (column x4 - 1 down to the
-// below-left reach y4 + 2 bh) - every sample its luma prediction and its luma contexts read.  At most 2 bw + 1 + 2 bh.
+// Dependencies of leaf li of SB sb: the distinct leaves (unit_leaf rule) covering a unit of its above strip (row y4 - 1
+// from the above-left corner to the above-right reach x4 + 2 bw) or of its left strip (column x4 - 1 down to the
+// below-left reach y4 + 2 bh) - every sample its luma prediction and its luma contexts read - and, for a 4:2:0 chroma
+// carrier, the leaves of the strips its chroma waits on (rc_leaf's chroma rc_wait; with 4:4:4 they are among the
+// first).  A leaf is queued when all of them have published their luma, so a chroma wait is always on leaves whose
+// warps are running (their chroma follows their luma in the same warp): however long the queue, waits cannot
+// accumulate on leaves that no warp has taken yet.  At most 2 bw + 1 + 2 bh + 5 (REV_PER_SB).
 __device__ int luma_deps(const FrameDesc &F, int sb, int li, uint32_t *out) {
     const Leaf lf = F.leaves[(size_t)sb * SB_MAX_LEAVES + li];
     const int bw = bw4(lf.bsize), bh = bh4(lf.bsize);
     const int sbr = sb / F.sbCols, sbc = sb % F.sbCols;
     int tC0, tC1, tR0, tR1;
     tile_box(F, sbr * 16 + lf.y4, sbc * 16 + lf.x4, tC0, tC1, tR0, tR1);
-    const int nTop = 2 * bw + 1, nLeft = 2 * bh;
     int n = 0;
-    for (int u = 0; u < nTop + nLeft; u++) {
-        const int yy = u < nTop ? lf.y4 - 1 : lf.y4 + (u - nTop), xx = u < nTop ? lf.x4 - 1 + u : lf.x4 - 1;
+    auto add = [&](int yy, int xx) {
         const int id = unit_leaf(F, sb, li, sbr, sbc, yy, xx, tC0, tC1, tR0);
-        if (id < 0 || (n > 0 && out[n - 1] == (uint32_t)id)) continue;
+        if (id < 0 || (n > 0 && out[n - 1] == (uint32_t)id)) return;
         bool seen = false;
         for (int k = 0; k < n; k++) seen |= out[k] == (uint32_t)id;
         if (!seen) out[n++] = (uint32_t)id;
+    };
+    for (int c = lf.x4 - 1; c < lf.x4 + 2 * bw; c++) add(lf.y4 - 1, c);
+    for (int r = lf.y4; r < lf.y4 + 2 * bh; r++) add(r, lf.x4 - 1);
+    if (F.ssx && has_chroma(lf.bsize, sbr * 16 + lf.y4, sbc * 16 + lf.x4, 1)) {
+        const int cx0 = lf.x4 & ~1, cy0 = lf.y4 & ~1, cw = max(bw, 2), ch = max(bh, 2);
+        for (int c = cx0 - 1; c < cx0 + 2 * cw; c += 2) add(cy0 - 1, c);
+        for (int r = cy0 + 1; r < cy0 + 2 * ch; r += 2) add(r, cx0 - 1);
     }
     return n;
 }

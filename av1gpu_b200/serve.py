@@ -142,22 +142,10 @@ def poisson_arrivals(rate, n, seed=0):
 
 
 def _requests(n, seed, max_mp=24.0, min_mp=0.2):
-    """n seeded synthetic requests: crops (log-uniform area min_mp .. max_mp MP, aspect 1:3 .. 3:1) of one 6000x4000
-    synthetic image, qindex uniform 40 .. 220."""
-    from . import synth
-    rng = np.random.default_rng(seed)
-    y, u, v = synth.make_image(6000, 4000, seed, edges=True)
-    out = []
-    for _ in range(n):
-        area = float(np.exp(rng.uniform(np.log(min_mp * 1e6), np.log(max_mp * 1e6))))
-        ar = float(np.exp(rng.uniform(np.log(1 / 3), np.log(3))))
-        w = int(min(6000, max(16, np.sqrt(area * ar)))) & ~1
-        h = int(min(4000, max(16, np.sqrt(area / ar)))) & ~1
-        x0, y0 = int(rng.integers(0, 6000 - w + 1)) & ~1, int(rng.integers(0, 4000 - h + 1)) & ~1
-        planes = [np.ascontiguousarray(y[y0:y0 + h, x0:x0 + w]), np.ascontiguousarray(u[y0 // 2:(y0 + h) // 2, x0 // 2:(x0 + w) // 2]),
-                  np.ascontiguousarray(v[y0 // 2:(y0 + h) // 2, x0 // 2:(x0 + w) // 2])]
-        out.append((planes, int(rng.integers(40, 221))))
-    return out
+    """n seeded synthetic requests: crops (log-uniform area min_mp .. max_mp MP, aspect 1:3 .. 3:1) of a 6000x4000
+    synthetic picture, 80 % 8-bit 4:2:0 and 20 % 10-bit 4:4:4, qindex uniform 40 .. 220 (batchbench.workload)."""
+    from .batchbench import workload
+    return workload(n, seed, max_mp, min_mp)
 
 
 def main():

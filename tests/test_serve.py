@@ -38,13 +38,17 @@ def test_workspace_bytes_grows_with_the_image():
     from av1gpu_b200.isearch import workspace_bytes
     a, b = workspace_bytes(640, 480), workspace_bytes(4000, 3000)
     assert 0 < a < b and b > 4000 * 3000 * 10
+    assert workspace_bytes(4000, 3000, 8, True) > b and workspace_bytes(4000, 3000, 10, True) > workspace_bytes(4000, 3000, 8, True)
 
 
 @pytest.mark.gpu
 def test_served_results_equal_alone(enc):
     sizes = [(160, 120), (96, 64), (211, 149), (64, 200), (300, 90), (128, 128), (77, 45), (256, 96)]
     qs = [60, 120, 200, 90, 150, 40, 220, 120]
-    images = [synth.make_image(w, h, 50 + i, edges=True) for i, (w, h) in enumerate(sizes)]
+    # formats mixed as requests arrive: images 2 and 5 10-bit 4:4:4, image 6 8-bit 4:4:4
+    fmts = {2: (10, True), 5: (10, True), 6: (8, True)}
+    images = [synth.make_image(w, h, 50 + i, edges=True, bit_depth=fmts.get(i, (8, False))[0], chroma_444=fmts.get(i, (8, False))[1])
+              for i, (w, h) in enumerate(sizes)]
     alone = [enc.encode(im, q) for im, q in zip(images, qs)]
     srv = serve.Server(device=0, hbm_budget=1 << 30, pipelines=2, max_batch=4, recon_ctas=96)
     try:
