@@ -644,9 +644,8 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         F.err = h->bErr;
         F.img = h->bPos[i] - h->bGrpStart[grp[i]];
         F.leafTrace = (h->trace && i == 0 && F.img == 0) ? h->traceBuf : nullptr;   // image 0, when its group's first
-        const bool sl = h->slOn && bd == 8;   // the shortlist network reads 8-bit luma: other images search in full
-        if (!sl) F.slMask = nullptr;
-        F.slRdK = sl ? h->slRdK : 4;
+        if (!h->slOn) F.slMask = nullptr;
+        F.slRdK = h->slOn ? h->slRdK : 4;
         sb_orders(F, cs, rs, h->hOrd + o, h->hOrd + o + ns);
         o += 2 * (size_t)ns;
         h->hFs[h->bPos[i]] = F;
@@ -698,7 +697,7 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
             else k_pad<uint16_t><<<dim3(1, ph), 128, 0, s>>>((uint16_t *)dst, F.spitch[p], vw, vh, pw, ph);
         }
         if (events && n == 1) IS_CK(cudaEventRecord(h->ev[1], s));
-        if (h->slOn && F.bd == 8) {   // the learned shortlist: scores of every analysis record, then its mode mask
+        if (h->slOn) {   // the learned shortlist: scores of every analysis record, then its mode mask
             const int k = K > 1 ? i % K : 0;
             for (uint32_t i0 = 0; i0 < F.nRec; i0 += SL_CHUNK) {
                 const int cn = (int)std::min<uint32_t>(SL_CHUNK, F.nRec - i0);

@@ -120,11 +120,16 @@ namespace is {
 // the shape one-hot (22), qindex / 255, 1 ----
 struct SlBlock { uint8_t bs, x4, y4, pad; uint32_t sb; };   // block of shape bs at SB sb, 4x4-unit offset (x4, y4)
 
-// the features of a block of shape bs at (x, y) into out[288], by one warp
+// the features of a block of shape bs at (x, y) into out[288], by one warp; 10-bit samples count a quarter (the
+// features stay on the 8-bit scale the network is trained on)
 __device__ __forceinline__ void sl_features_of(const FrameDesc &F, int bs, int x, int y, __nv_bfloat16 *out) {
     const int lane = threadIdx.x & 31;
     const int W = 4 * ST(Num_4x4_Blocks_Wide)[bs], H = 4 * ST(Num_4x4_Blocks_High)[bs];
-    const uint8_t *src = F.src[0];
+    const bool hi = F.bd > 8;
+    const uint8_t *src8 = F.src[0];
+    const uint16_t *src16 = reinterpret_cast<const uint16_t *>(F.src[0]);
+    auto src = [&](size_t i) -> int { return hi ? (int)src16[i] : (int)src8[i]; };
+    const float scale = hi ? 0.25f : 1.f;
     const int sp = F.spitch[0];
     // the patch: lane handles 8 of the 256 cells
     float cell[8], sum = 0.f;
@@ -135,8 +140,8 @@ __device__ __forceinline__ void sl_features_of(const FrameDesc &F, int bs, int x
         const int px = x + (cj * W) / 16, py = y + (ci * H) / 16;
         int s = 0;
         for (int i = 0; i < sh; i++)
-            for (int j = 0; j < sw; j++) s += src[(size_t)(py + i) * sp + px + j];
-        cell[k] = (float)s / (float)(sw * sh);
+            for (int j = 0; j < sw; j++) s += src((size_t)(py + i) * sp + px + j);
+        cell[k] = (float)s / (float)(sw * sh) * scale;
         sum += cell[k];
     }
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -151,8 +156,8 @@ __device__ __forceinline__ void sl_features_of(const FrameDesc &F, int bs, int x
         const int px = x + (cj * W) / 16, py = y + (ci * H) / 16;
         // central differences clamped to the block (samples of the padded source plane only)
         const int xl = max(px - 1, x), xr = min(px + 1, x + W - 1), yu = max(py - 1, y), yd = min(py + 1, y + H - 1);
-        const float gx = (float)src[(size_t)py * sp + xr] - (float)src[(size_t)py * sp + xl];
-        const float gy = (float)src[(size_t)yd * sp + px] - (float)src[(size_t)yu * sp + px];
+        const float gx = ((float)src((size_t)py * sp + xr) - (float)src((size_t)py * sp + xl)) * scale;
+        const float gy = ((float)src((size_t)yd * sp + px) - (float)src((size_t)yu * sp + px)) * scale;
         const float m = fabsf(gx) + fabsf(gy);
         // orientation in [0, 180): fold to gy >= 0, then 8 bins of 22.5 degrees by comparisons with tan(22.5/67.5)
         float ax = gx, ay = gy;

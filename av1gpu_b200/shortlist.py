@@ -88,10 +88,12 @@ class Learner:
         return loss.value, corr.value
 
 
-def dataset(enc, images, qindices):
-    """Features (torch bf16, n x 288, CUDA) and labels (torch int32) of every analysed block of the images, each
-    searched with the plain form (the labels are its choices)."""
+def dataset(enc, images, qindices, per_image=0, seed=0):
+    """Features (torch bf16, n x 288, CUDA) and labels (torch int32) of the analysed blocks of the images, each
+    searched with the plain form (the labels are its choices): every block, or per_image blocks drawn at random
+    (seeded) from each image's."""
     import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
     xs, ys = [], []
     for planes, q in zip(images, qindices):
         enc.encode(planes, q)
@@ -102,6 +104,9 @@ def dataset(enc, images, qindices):
         rc = enc.L.is_sl_dataset(enc.h, 0, _vp(X), _vp(y), n.value, C.byref(n))
         if rc != 0:
             raise RuntimeError("is_sl_dataset failed (%d)" % rc)
+        if per_image and X.shape[0] > per_image:
+            idx = torch.randperm(X.shape[0], generator=g)[:per_image].to(X.device)
+            X, y = X[idx], y[idx]
         xs.append(X)
         ys.append(y)
     return torch.cat(xs), torch.cat(ys)
@@ -129,9 +134,10 @@ def train(learner, X, y, epochs=4, batch=4096, lr=2e-3, seed=0, log=None):
 
 
 def evaluate(learner, X, y, tau=0.9, max_modes=6, conf=0.0):
-    """Top-1 accuracy, how often the label falls in the shortlist mask, and the mean mask size."""
+    """Top-1 accuracy, how often the label falls in the shortlist mask, the mean mask size, and the fallback rate (the
+    blocks whose top probability is below conf: searched in full)."""
     import torch
-    accs, cover, size, n = 0, 0, 0, 0
+    accs, cover, size, n, fb = 0, 0, 0, 0, 0
     for b0 in range(0, X.shape[0], learner.cap):
         Xb, yb = X[b0:b0 + learner.cap].contiguous(), y[b0:b0 + learner.cap]
         S = learner.forward(Xb)[:, :N_MODES]
@@ -140,14 +146,16 @@ def evaluate(learner, X, y, tau=0.9, max_modes=6, conf=0.0):
         ps = torch.gather(p, 1, order)
         keep = (torch.cumsum(ps, 1) - ps) < tau
         keep[:, max_modes:] = False
-        keep[ps[:, 0] < conf] = True
+        low = ps[:, 0] < conf
+        keep[low] = True
+        fb += int(low.sum())
         mask = torch.zeros_like(keep)
         mask.scatter_(1, order, keep)
         accs += int((order[:, 0] == yb.long()).sum())
         cover += int(mask.gather(1, yb.long()[:, None]).sum())
         size += int(mask.sum())
         n += Xb.shape[0]
-    return {"top1": accs / n, "coverage": cover / n, "mean_modes": size / n}
+    return {"top1": accs / n, "coverage": cover / n, "mean_modes": size / n, "fallback": fb / n}
 
 
 def bd_rate(rate_a, q_a, rate_b, q_b):
@@ -165,12 +173,25 @@ def bd_rate(rate_a, q_a, rate_b, q_b):
     return float((np.exp(np.mean(fb(xs) - fa(xs))) - 1.0) * 100.0)
 
 
-def training_images(n, size, seed):
-    """n seeded synthetic training images (the generator of the workloads) with qindex uniform 40 .. 220."""
+def _make(args):
     from . import synth
+    w, h, s = args
+    return synth.make_image(w, h, s, edges=True)
+
+
+def training_images(n, size, seed, workers=1):
+    """n seeded synthetic images (the generator of the workloads; image i from seed seed * 1000 + i, qindex uniform
+    40 .. 220), generated on `workers` host processes (spawned: safe before or after CUDA is initialised)."""
     w, h = size
     rng = np.random.default_rng(seed)
-    return [synth.make_image(w, h, seed * 1000 + i, edges=True) for i in range(n)], [int(q) for q in rng.integers(40, 221, n)]
+    jobs = [(w, h, seed * 1000 + i) for i in range(n)]
+    if workers > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(workers) as pool:
+            ims = pool.map(_make, jobs, chunksize=8)
+    else:
+        ims = [_make(j) for j in jobs]
+    return ims, [int(q) for q in rng.integers(40, 221, n)]
 
 
 def main():
@@ -187,22 +208,34 @@ def main():
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--out", default="shortlist_weights.npz")
+    ap.add_argument("--blocks-per-image", type=int, default=0, help="blocks drawn per image (0: all)")
+    ap.add_argument("--workers", type=int, default=0, help="host processes for the image generator (0: all cores)")
     args = ap.parse_args()
+    import os
+    import time
     size = tuple(int(v) for v in args.size.split("x"))
+    t0 = time.time()
+    ims, qs = training_images(args.images, size, args.seed, workers=args.workers or os.cpu_count() or 1)
+    t_gen = time.time() - t0
     enc = Encoder(0)
-    ims, qs = training_images(args.images, size, args.seed)
-    X, y = dataset(enc, ims, qs)
+    X, y = dataset(enc, ims, qs, per_image=args.blocks_per_image, seed=args.seed)
+    del ims
+    t_data = time.time() - t0 - t_gen
     n_val = X.shape[0] // 10
     perm = torch.randperm(X.shape[0], generator=torch.Generator().manual_seed(args.seed)).cuda()
     Xv, yv, Xt, yt = X[perm[:n_val]], y[perm[:n_val]], X[perm[n_val:]], y[perm[n_val:]]
     lrn = Learner(max_batch=4096)
     lrn.set_weights(init_weights(args.seed))
+    t1 = time.time()
     hist = train(lrn, Xt, yt, epochs=args.epochs, batch=4096, lr=args.lr, seed=args.seed, log=print)
+    t_train = time.time() - t1
     w = lrn.get_weights()
-    np.savez_compressed(args.out, w1=w[0], b1=w[1], w2=w[2], b2=w[3], images=args.images, size=np.array(size), epochs=args.epochs)
-    out = {"samples": int(X.shape[0]), "final_train": hist[-1]}
-    for tau, mm in ((0.8, 4), (0.9, 6), (0.95, 8)):
-        out["val_tau%.2f_max%d" % (tau, mm)] = evaluate(lrn, Xv, yv, tau=tau, max_modes=mm)
+    np.savez_compressed(args.out, w1=w[0], b1=w[1], w2=w[2], b2=w[3], images=args.images, size=np.array(size), epochs=args.epochs,
+                        blocks_per_image=args.blocks_per_image, seed=args.seed)
+    out = {"images": args.images, "samples": int(X.shape[0]), "final_train": hist[-1], "generate_s": round(t_gen, 1),
+           "dataset_s": round(t_data, 1), "train_s": round(t_train, 1)}
+    for tau, mm, cf in ((0.8, 4, 0.0), (0.9, 6, 0.0), (0.9, 6, 0.25), (0.95, 8, 0.0)):
+        out["val_tau%.2f_max%d_conf%.2f" % (tau, mm, cf)] = evaluate(lrn, Xv, yv, tau=tau, max_modes=mm, conf=cf)
     print(json.dumps(out))
     lrn.close()
     enc.close()
