@@ -18,18 +18,17 @@ namespace is {
 // Two kernels share the block search: k_analysis for the 132 blocks of the shapes up to 32 samples a side from 8x16 /
 // 16x8 / 8x32 / 32x8 up (8 warps, 3 CTAs per SM), k_analysis_big for the 13 blocks with a 64-sample side (4 warps with
 // the larger scratch).  The 704 blocks of 4x4, 4x8, 8x4, 8x8, 4x16 and 16x4 have the per-thread searches of
-// is_tiny.cuh for 8-bit images; for 10-bit images a third instance of the warp search, k_analysis_small, takes them.
+// is_tiny.cuh.
 constexpr int AN_WARPS = 8, ANB_WARPS = 4;
-constexpr int AN_TASKS = 132, ANB_TASKS = 13, ANS_TASKS = 704;
+constexpr int AN_TASKS = 132, ANB_TASKS = 13;
 constexpr int AN_BUF_INTS = 1088;             // evaluation scratch per warp: 32 / G tasks of H x (W + 1) int32 (<= 32x32)
 constexpr int ANB_BUF_INTS = 64 * 65;
 __constant__ uint8_t c_anTask[AN_TASKS][3];   // (bsize, x4, y4) largest area first, then shape, then raster
 __constant__ uint8_t c_anTaskBig[ANB_TASKS][3];
-__constant__ uint8_t c_anTaskSmall[ANS_TASKS][3];
 // Each CTA runs the blocks of ONE shape of one SB (grid: shapes x SBs, shape-major), so that the warps of an SM work
 // through the same code; the task ranges of the shapes in the lists above:
-constexpr int AN_SHAPES = 8, ANB_SHAPES = 5, ANS_SHAPES = 6;
-__constant__ int c_anShapeStart[AN_SHAPES + 1], c_anShapeStartBig[ANB_SHAPES + 1], c_anShapeStartSmall[ANS_SHAPES + 1];
+constexpr int AN_SHAPES = 8, ANB_SHAPES = 5;
+__constant__ int c_anShapeStart[AN_SHAPES + 1], c_anShapeStartBig[ANB_SHAPES + 1];
 
 template <typename Px, int BUFI> struct AnWarp {
     int32_t buf[BUFI];
@@ -210,13 +209,9 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
     __syncwarp();
 }
 
-// the task list of a kernel: 0 the shapes up to 32 a side, 1 those with a 64-sample side, 2 the six smallest shapes
-template <int LIST> __device__ __forceinline__ const uint8_t *an_task(int t) {
-    return LIST == 0 ? c_anTask[t] : LIST == 1 ? c_anTaskBig[t] : c_anTaskSmall[t];
-}
-template <int LIST> __device__ __forceinline__ int an_shape_start(int s) {
-    return LIST == 0 ? c_anShapeStart[s] : LIST == 1 ? c_anShapeStartBig[s] : c_anShapeStartSmall[s];
-}
+// the task list of a kernel: 0 the shapes up to 32 a side, 1 those with a 64-sample side
+template <int LIST> __device__ __forceinline__ const uint8_t *an_task(int t) { return LIST == 0 ? c_anTask[t] : c_anTaskBig[t]; }
+template <int LIST> __device__ __forceinline__ int an_shape_start(int s) { return LIST == 0 ? c_anShapeStart[s] : c_anShapeStartBig[s]; }
 
 // one CTA per SB: stage the tile, then the warps take the blocks of the task list
 template <int BD, int NW, int BUFI, int LIST>
@@ -265,10 +260,6 @@ __global__ void __launch_bounds__(ANB_WARPS * 32, 2) k_analysis_big(const __grid
     extern __shared__ __align__(16) unsigned char smem_raw[];
     an_sb<BD, ANB_WARPS, ANB_BUF_INTS, 1>(F, smem_raw);
 }
-template <int BD>
-__global__ void __launch_bounds__(AN_WARPS * 32, 3) k_analysis_small(const __grid_constant__ FrameDesc F) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    an_sb<BD, AN_WARPS, AN_BUF_INTS, 2>(F, smem_raw);
-}
+
 
 }  // namespace is

@@ -147,7 +147,7 @@ void min_tiles(int W, int H, std::vector<int> &cs, std::vector<int> &rs) {
 
 // analysis task lists of one SB: (bsize, x4, y4) for every shape, largest area first; big = shapes with a 64 side
 // the task list of an analysis kernel (an_task<LIST>): 0 the shapes up to 32 a side from 8x16 / 16x8 up, 1 the shapes
-// with a 64-sample side, 2 the six smallest (4x4, 4x8, 8x4, 8x8, 4x16, 16x4: the per-thread kernels of 8-bit images)
+// with a 64-sample side (the six smallest, 4x4, 4x8, 8x4, 8x8, 4x16 and 16x4, have the per-thread kernels)
 std::vector<uint8_t> an_tasks(int list) {
     std::vector<int> shapes;
     for (int s = 0; s < AV1G_BLOCK_INVALID; s++) {
@@ -155,7 +155,7 @@ std::vector<uint8_t> an_tasks(int list) {
         const bool b = AV1G_T(Num_4x4_Blocks_Wide)[s] == 16 || AV1G_T(Num_4x4_Blocks_High)[s] == 16;
         const bool small = s == AV1G_BLOCK_4X4 || s == AV1G_BLOCK_4X8 || s == AV1G_BLOCK_8X4 || s == AV1G_BLOCK_8X8 || s == AV1G_BLOCK_4X16 ||
                            s == AV1G_BLOCK_16X4;
-        if (list == 2 ? small : (!small && b == (list == 1))) shapes.push_back(s);
+        if (!small && b == (list == 1)) shapes.push_back(s);
     }
     std::stable_sort(shapes.begin(), shapes.end(), [](int a, int b) {
         return AV1G_T(Num_4x4_Blocks_Wide)[a] * AV1G_T(Num_4x4_Blocks_High)[a] > AV1G_T(Num_4x4_Blocks_Wide)[b] * AV1G_T(Num_4x4_Blocks_High)[b];
@@ -278,7 +278,7 @@ int upload_tables(int dev) {
         const HostTables &T = host_tables();
         std::vector<uint16_t> all((size_t)4 * NCDF);
         for (int q = 0; q < 4; q++) memcpy(all.data() + (size_t)q * NCDF, T.cost[q].data(), NCDF * 2);
-        const std::vector<uint8_t> tasks = an_tasks(0), tasksBig = an_tasks(1), tasksSmall = an_tasks(2);
+        const std::vector<uint8_t> tasks = an_tasks(0), tasksBig = an_tasks(1);
         cudaError_t e = cudaMemcpyToSymbol(g_cost, all.data(), all.size() * 2);
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgY, T.avgY, sizeof T.avgY);
         if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgPart, T.avgPart, sizeof T.avgPart);
@@ -329,14 +329,11 @@ int upload_tables(int dev) {
             out[n] = (int)(t.size() / 3);
             return k == n;
         };
-        int st[AN_SHAPES + 1], stBig[ANB_SHAPES + 1], stSmall[ANS_SHAPES + 1];
-        const bool okShapes = starts(tasks, AN_SHAPES, st) && starts(tasksBig, ANB_SHAPES, stBig) && starts(tasksSmall, ANS_SHAPES, stSmall);
-        if (e == cudaSuccess && okShapes && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3 &&
-            tasksSmall.size() == (size_t)ANS_TASKS * 3) {
+        int st[AN_SHAPES + 1], stBig[ANB_SHAPES + 1];
+        const bool okShapes = starts(tasks, AN_SHAPES, st) && starts(tasksBig, ANB_SHAPES, stBig);
+        if (e == cudaSuccess && okShapes && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3) {
             e = cudaMemcpyToSymbol(c_anTask, tasks.data(), tasks.size());
             if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anTaskBig, tasksBig.data(), tasksBig.size());
-            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anTaskSmall, tasksSmall.data(), tasksSmall.size());
-            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStartSmall, stSmall, sizeof stSmall);
             if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStart, st, sizeof st);
             if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStartBig, stBig, sizeof stBig);
         } else if (e == cudaSuccess) {
@@ -458,8 +455,9 @@ int is_create(const is_params *p, is_handle **out) {
     h->smemAnBig10 = sizeof(AnSmem<uint16_t, ANB_WARPS, ANB_BUF_INTS>);
     auto attr = [](const void *k, size_t b) { return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b) == cudaSuccess; };
     if (!attr((const void *)k_analysis<8>, h->smemAn) || !attr((const void *)k_analysis_big<8>, h->smemAnBig) ||
-        !attr((const void *)k_analysis_mid<8>, sizeof(MidSmem)) || !attr((const void *)k_analysis<10>, h->smemAn10) ||
-        !attr((const void *)k_analysis_small<10>, h->smemAn10) || !attr((const void *)k_analysis_big<10>, h->smemAnBig10))
+        !attr((const void *)k_analysis_mid<8>, sizeof(MidSmem<uint8_t>)) || !attr((const void *)k_analysis_tiny<8>, sizeof(TinySmem<uint8_t>)) ||
+        !attr((const void *)k_analysis<10>, h->smemAn10) || !attr((const void *)k_analysis_big<10>, h->smemAnBig10) ||
+        !attr((const void *)k_analysis_mid<10>, sizeof(MidSmem<uint16_t>)) || !attr((const void *)k_analysis_tiny<10>, sizeof(TinySmem<uint16_t>)))
         return fail(IS_ERR_CUDA);
     for (int g = 0; g < 4; g++) {   // the closed loop of each format group: shared memory and its cooperative grid
         const void *k = rc_kernel(g);
@@ -713,12 +711,13 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
         if (F.bd == 8) {
             k_analysis_big<8><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig, s>>>(F);
             k_analysis<8><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn, s>>>(F);
-            k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem), s>>>(F);
-            k_analysis_mid<8><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem), s>>>(F);
+            k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem<uint8_t>), s>>>(F);
+            k_analysis_mid<8><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem<uint8_t>), s>>>(F);
         } else {
             k_analysis_big<10><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig10, s>>>(F);
             k_analysis<10><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn10, s>>>(F);
-            k_analysis_small<10><<<ANS_SHAPES * nSb, AN_WARPS * 32, h->smemAn10, s>>>(F);
+            k_analysis_tiny<10><<<nSb, TINY_THREADS, sizeof(TinySmem<uint16_t>), s>>>(F);
+            k_analysis_mid<10><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem<uint16_t>), s>>>(F);
         }
         IS_CK(cudaGetLastError());
         if (events && n == 1) IS_CK(cudaEventRecord(h->ev[2], s));

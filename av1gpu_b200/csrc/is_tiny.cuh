@@ -33,9 +33,9 @@ __host__ __device__ constexpr int mag_ref(int c, int k, int d) {
 constexpr int kDr23 = 151, kDr45 = 64, kDr67 = 27;
 
 constexpr int TINY_THREADS = 256;
-struct TinySmem {
+template <typename Px> struct TinySmem {      // Px: the sample type (uint8_t 8-bit, uint16_t 10-bit)
     static constexpr int TW = 144, TH = 65;   // the SB tile of the analysis (columns sbx-16 .., rows sby-1 ..)
-    uint8_t tile[TH * TW];
+    Px tile[TH * TW];
     uint8_t iscan[3][3][32];                  // scan position of each coefficient: (4x4, 4x8, 8x4) x (2D, HORIZ, VERT)
     RateStage T;
 };
@@ -244,12 +244,15 @@ __device__ __forceinline__ EvalOut thr_eval(int txSz, const int *res, const Eval
 }
 
 // ---- the search of one W x H block (bs) at (x, y), one thread ----
-template <int BD, int LW, int LH>
-__device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S, const RateTabs &T, int bs, int txSz, int sizeIdx, int x,
+template <int BD, int LW, int LH, typename Px>
+__device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem<Px> &S, const RateTabs &T, int bs, int txSz, int sizeIdx, int x,
                                            int y, int sbx, int sby, int tx0, int ty0, int tx1, int ty1) {
     constexpr int W = 1 << LW, H = 1 << LH, N = W * H, NE = W + H;
-    constexpr int TW = TinySmem::TW;
-    const uint8_t *tile = S.tile;
+    constexpr int TW = TinySmem<Px>::TW;
+    // the kept predictions are packed PPW samples to a 32-bit word: 4 bytes (8-bit), 2 halves (10-bit)
+    constexpr int PPW = sizeof(Px) == 1 ? 4 : 2, PB = 32 / PPW, NWD = N / PPW;
+    constexpr uint32_t PMASK = (1u << PB) - 1u;
+    const Px *tile = S.tile;
     const int haveL = x > tx0, haveA = y > ty0;
     const int haveAR = ol_decoded(x + W, y - 1, x, y, tx0, ty0, tx1, ty1), haveBL = ol_decoded(x - 1, y + H, x, y, tx0, ty0, tx1, ty1);
     const int lx = x - sbx + 16, ly = y - sby + 1;
@@ -287,10 +290,10 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
     for (int i = 0; i < H; i++)
 #pragma unroll
         for (int j = 0; j < W; j++) src[i * W + j] = tile[(ly + i) * TW + lx + j];
-    // ---- SATD screening of the 13 modes; the 4 best kept in cost order with their predictions (packed bytes) ----
+    // ---- SATD screening of the 13 modes; the 4 best kept in cost order with their predictions (packed) ----
     i64 topJ[4];
     int topM[4];
-    uint32_t topP[4][N / 4];
+    uint32_t topP[4][NWD];
 #pragma unroll
     for (int k = 0; k < 4; k++) { topJ[k] = INF; topM[k] = 0; }
     // the modes screened: all 13, or the block's learned shortlist; a mode no thread of the warp screens is skipped
@@ -314,9 +317,14 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
                 satd += hadamard4_sum(d);
             }
         const i64 js = ((i64)satd << 14) + F.sqlam * c_avgY[M];
-        uint32_t pk[N / 4];
+        uint32_t pk[NWD];
 #pragma unroll
-        for (int k = 0; k < N / 4; k++) pk[k] = (uint32_t)p[4 * k] | ((uint32_t)p[4 * k + 1] << 8) | ((uint32_t)p[4 * k + 2] << 16) | ((uint32_t)p[4 * k + 3] << 24);
+        for (int k = 0; k < NWD; k++) {
+            uint32_t v = 0;
+#pragma unroll
+            for (int u = 0; u < PPW; u++) v |= (uint32_t)p[PPW * k + u] << (PB * u);
+            pk[k] = v;
+        }
         // insertion: after every kept entry of cost <= js (the earlier candidate wins a tie); none for a mode off the list
         const int pos = need ? (topJ[0] <= js) + (topJ[1] <= js) + (topJ[2] <= js) + (topJ[3] <= js) : 4;
 #pragma unroll
@@ -325,12 +333,12 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
                 topJ[s] = topJ[s - 1 < 0 ? 0 : s - 1];
                 topM[s] = topM[s - 1 < 0 ? 0 : s - 1];
 #pragma unroll
-                for (int k = 0; k < N / 4; k++) topP[s][k] = topP[s - 1 < 0 ? 0 : s - 1][k];
+                for (int k = 0; k < NWD; k++) topP[s][k] = topP[s - 1 < 0 ? 0 : s - 1][k];
             } else if (s == pos) {
                 topJ[s] = js;
                 topM[s] = M;
 #pragma unroll
-                for (int k = 0; k < N / 4; k++) topP[s][k] = pk[k];
+                for (int k = 0; k < NWD; k++) topP[s][k] = pk[k];
             }
         }
     };
@@ -354,7 +362,7 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
     auto rd = [&](const uint32_t *pw, int m, int t) -> i64 {
         int res[N], q[N];
 #pragma unroll
-        for (int i = 0; i < N; i++) res[i] = src[i] - (int)((pw[i >> 2] >> (8 * (i & 3))) & 255);
+        for (int i = 0; i < N; i++) res[i] = src[i] - (int)((pw[i / PPW] >> (PB * (i % PPW))) & PMASK);
         const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, T};
         const EvalOut o = thr_eval<BD, LW, LH>(txSz, res, e, iscan, 32, q);
         return o.D + F.lam * (o.R + c_avgY[m] + overhead);
@@ -369,16 +377,16 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
         if (j < bestJ) { bestJ = j; bestK = k; }
     }
     // the winner's prediction and mode (static register indices for the type loop)
-    uint32_t wp[N / 4];
+    uint32_t wp[NWD];
     int wm = topM[0];
 #pragma unroll
-    for (int k = 0; k < N / 4; k++) wp[k] = topP[0][k];
+    for (int k = 0; k < NWD; k++) wp[k] = topP[0][k];
 #pragma unroll
     for (int s = 1; s < 4; s++)
         if (bestK == s) {
             wm = topM[s];
 #pragma unroll
-            for (int k = 0; k < N / 4; k++) wp[k] = topP[s][k];
+            for (int k = 0; k < NWD; k++) wp[k] = topP[s][k];
         }
     // 4- and 8-point sizes are in TX_SET_INTRA_1: IDTX, DCT_DCT, V_DCT, H_DCT, ADST_ADST, ADST_DCT, DCT_ADST
 #pragma unroll 1
@@ -403,17 +411,19 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem &S
 
 template <int BD>
 __global__ void __launch_bounds__(TINY_THREADS, 1) k_analysis_tiny(const __grid_constant__ FrameDesc F) {
+    typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
+    typedef TinySmem<Px> Sm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    TinySmem &S = *reinterpret_cast<TinySmem *>(smem_raw);
+    Sm &S = *reinterpret_cast<Sm *>(smem_raw);
     const int sb = blockIdx.x, sbr = sb / F.sbCols, sbc = sb % F.sbCols;
     const int sbx = sbc * 64, sby = sbr * 64;
     const int tid = threadIdx.x;
     {   // the SB tile (as an_sb), the rate tables, the inverse scans of the three sizes
-        constexpr int V = TinySmem::TW / 16;
-        const uint8_t *s0 = F.src[0] + (size_t)(sby - 1) * F.spitch[0] + (sbx - 16);
-        for (int k = tid; k < TinySmem::TH * V; k += TINY_THREADS) {
+        constexpr int V = Sm::TW * (int)sizeof(Px) / 16;
+        const Px *s0 = (const Px *)F.src[0] + (size_t)(sby - 1) * F.spitch[0] + (sbx - 16);
+        for (int k = tid; k < Sm::TH * V; k += TINY_THREADS) {
             const int r = k / V, c = k % V;
-            reinterpret_cast<uint4 *>(S.tile + r * TinySmem::TW)[c] = __ldg(reinterpret_cast<const uint4 *>(s0 + (size_t)r * F.spitch[0]) + c);
+            reinterpret_cast<uint4 *>(S.tile + r * Sm::TW)[c] = __ldg(reinterpret_cast<const uint4 *>(s0 + (size_t)r * F.spitch[0]) + c);
         }
     }
     const RateTabs T = rate_tabs_stage(S.T, F.qctx, tid, TINY_THREADS);
@@ -452,11 +462,11 @@ __global__ void __launch_bounds__(TINY_THREADS, 1) k_analysis_tiny(const __grid_
 // One CTA runs ONE shape on the 64 blocks of each of MID_SBS superblocks, so that all its warps (and the co-resident
 // CTAs, which the grid order gives the same shape) share one instruction stream.
 constexpr int MID_SBS = 3, MID_THREADS = 64 * MID_SBS;
-struct MidSmem {
+template <typename Px> struct MidSmem {   // Px: the sample type
     static constexpr int TW = 144, TH = 65;
-    uint8_t tile[MID_SBS][TH * TW];
+    Px tile[MID_SBS][TH * TW];
     uint8_t iscan[3][64];                // the shape's tx size x (2D, HORIZ, VERT)
-    uint8_t edge[MID_THREADS][2][24];    // per thread: AboveRow[-1 .. 22], LeftCol[-1 .. 22]
+    Px edge[MID_THREADS][2][24];         // per thread: AboveRow[-1 .. 22], LeftCol[-1 .. 22]
     int16_t q[MID_THREADS][64];          // per thread: levels of the evaluation in progress
     RateStage T;
 };
@@ -532,17 +542,17 @@ __device__ __forceinline__ EvalOut mid_eval(int txSz, const int *res, const Eval
     return o;
 }
 
-template <int BD, int LW, int LH>
-__device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const RateTabs &T, int bs, int txSz, const uint8_t *tile, int x,
+template <int BD, int LW, int LH, typename Px>
+__device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem<Px> &S, const RateTabs &T, int bs, int txSz, const Px *tile, int x,
                                           int y, int sbx, int sby, int tx0, int ty0, int tx1, int ty1) {
     constexpr int W = 1 << LW, H = 1 << LH, N = W * H, NE = W + H;
-    constexpr int TW = MidSmem::TW;
+    constexpr int TW = MidSmem<Px>::TW;
     const int tid = threadIdx.x;
     const int haveL = x > tx0, haveA = y > ty0;
     const int haveAR = ol_decoded(x + W, y - 1, x, y, tx0, ty0, tx1, ty1), haveBL = ol_decoded(x - 1, y + H, x, y, tx0, ty0, tx1, ty1);
     const int lx = x - sbx + 16, ly = y - sby + 1;
     const int mX = F.MiCols * 4 - 1 - sbx + 16, mY = F.MiRows * 4 - 1 - sby + 1;
-    uint8_t *A = S.edge[tid][0] + 1, *L = S.edge[tid][1] + 1;
+    Px *A = S.edge[tid][0] + 1, *L = S.edge[tid][1] + 1;
     build_edges<BD>(tile, TW, lx, ly, W, H, haveL, haveA, haveAR, haveBL, mX, mY, A, L, 0, 1);
     int dcv;
     {
@@ -556,7 +566,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
         else if (haveA) dcv = min((sa + (W >> 1)) >> LW, (1 << BD) - 1);
         else dcv = 1 << (BD - 1);
     }
-    const uint8_t *src = tile + ly * TW + lx;
+    const Px *src = tile + ly * TW + lx;
     const uint16_t *C = T.cost;
     auto mbits = [&](int c) -> int {
         const int m = cand_mode(c);
@@ -667,19 +677,21 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem &S, const 
 // grid: 3 x ceil(nSb / MID_SBS) CTAs, shape-major (8x8, then 4x16, then 16x4)
 template <int BD>
 __global__ void __launch_bounds__(MID_THREADS, 2) k_analysis_mid(const __grid_constant__ FrameDesc F) {
+    typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
+    typedef MidSmem<Px> Sm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    MidSmem &S = *reinterpret_cast<MidSmem *>(smem_raw);
+    Sm &S = *reinterpret_cast<Sm *>(smem_raw);
     const int nSb = F.sbCols * F.sbRows, groups = (nSb + MID_SBS - 1) / MID_SBS;
     const int shape = blockIdx.x / groups, sb0 = (blockIdx.x % groups) * MID_SBS;
     const int tid = threadIdx.x;
     const int txSz = shape == 0 ? AV1G_TX_8X8 : shape == 1 ? AV1G_TX_4X16 : AV1G_TX_16X4;
-    constexpr int V = MidSmem::TW / 16;
-    for (int k = tid; k < MID_SBS * MidSmem::TH * V; k += MID_THREADS) {
-        const int u = k / (MidSmem::TH * V), r = (k / V) % MidSmem::TH, c = k % V, sb = sb0 + u;
+    constexpr int V = Sm::TW * (int)sizeof(Px) / 16;
+    for (int k = tid; k < MID_SBS * Sm::TH * V; k += MID_THREADS) {
+        const int u = k / (Sm::TH * V), r = (k / V) % Sm::TH, c = k % V, sb = sb0 + u;
         if (sb >= nSb) continue;
         const int sbx = (sb % F.sbCols) * 64, sby = (sb / F.sbCols) * 64;
-        const uint8_t *s0 = F.src[0] + (size_t)(sby - 1) * F.spitch[0] + (sbx - 16);
-        reinterpret_cast<uint4 *>(S.tile[u] + r * MidSmem::TW)[c] = __ldg(reinterpret_cast<const uint4 *>(s0 + (size_t)r * F.spitch[0]) + c);
+        const Px *s0 = (const Px *)F.src[0] + (size_t)(sby - 1) * F.spitch[0] + (sbx - 16);
+        reinterpret_cast<uint4 *>(S.tile[u] + r * Sm::TW)[c] = __ldg(reinterpret_cast<const uint4 *>(s0 + (size_t)r * F.spitch[0]) + c);
     }
     const RateTabs T = rate_tabs_stage(S.T, F.qctx, tid, MID_THREADS);
     __syncthreads();
