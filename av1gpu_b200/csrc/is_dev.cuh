@@ -409,10 +409,16 @@ __device__ __forceinline__ int pred4_satd(int mode, int pAng, int sy, int sx, in
     return pred4_x<P, P>(mode, pAng, sy, sx, lw, lh, A, L, dcv, src, sp, (P *)nullptr);
 }
 
-// the whole prediction of a W x H block into out (row stride W), 4x4 sub-blocks over the G lanes of a group
+// the whole prediction of a W x H block into out (row stride W) by the G lanes of a group: 4x4 sub-blocks over the
+// lanes, or, when the block has fewer sub-blocks than the group has lanes, samples over the lanes (pred_px: the same
+// values, the work spread over every lane instead of one lane per sub-block)
 template <typename P, typename O>
 __device__ __noinline__ void grp_predict(int mode, int pAng, int lw, int lh, const P *A, const P *L, int dcv, O *out, int g, int G) {
     const int nsx = 1 << (lw - 2), nsub = 1 << (lw + lh - 4);
+    if (nsub < G) {
+        for (int q = g; q < (1 << (lw + lh)); q += G) out[q] = (O)pred_px(mode, pAng, q >> lw, q & ((1 << lw) - 1), lw, lh, A, L, dcv);
+        return;
+    }
     for (int sb = g; sb < nsub; sb += G) {
         const int sx = (sb & (nsx - 1)) * 4, sy = (sb >> (lw - 2)) * 4;
         pred4_x<P, O>(mode, pAng, sy, sx, lw, lh, A, L, dcv, nullptr, 0, out);
@@ -580,6 +586,17 @@ __device__ __forceinline__ int grp_max(int v, int G) {
 __device__ __forceinline__ int grp_size(int txSz) {
     const int W = txw(txSz), H = txh(txSz);
     return (W >= 32 || H >= 32) ? 32 : max(max(W, H), 8);
+}
+// lanes per task for a closed-loop pass of n tasks: as few rounds of 32 / G tasks as the tx size allows - at least
+// max(W, H) / 2 lanes (two columns / rows a lane), at least 4 (32 / G <= 8 groups), and 32 / G tasks' levels within
+// one 1024-entry buffer - and no more lanes than grp_size.  The results do not depend on G: every task computes the
+// same integers, costs are compared in task order.
+__device__ __forceinline__ int round_group(int txSz, int n) {
+    const int W = txw(txSz), H = txh(txSz), nq = min(W, 32) * min(H, 32);
+    const int gmin = max(4, max(max(W, H) >> 1, nq >> 5)), gmax = grp_size(txSz);
+    int p = 1;
+    while (p < n && p < 32) p <<= 1;   // tasks rounded up to a power of two
+    return min(gmax, max(gmin, 32 / p));
 }
 // scratch of one task: int32 buffer H x (W + 1), levels tw x th
 __device__ __forceinline__ int task_buf_ints(int txSz) { return txh(txSz) * (txw(txSz) + 1); }

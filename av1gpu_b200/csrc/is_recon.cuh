@@ -494,20 +494,24 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
         const Px *src = staged ? (const Px *)Wp.srcS[0] : (const Px *)F.src[0] + (size_t)y * F.spitch[0] + x;
         const int srcPitch = staged ? W : F.spitch[0];
         const int set = tx_set_intra(txSz);
-        const int G = grp_size(txSz), ng = 32 / G, grp = lane / G, g = lane & (G - 1);
         const int nq = min(W, 32) * min(H, 32);
-        int32_t *tb = Wp.buf + grp * task_buf_ints(txSz);
-        int16_t *tq = Wp.q + grp * nq;
-        Px *tp = Wp.pred + grp * (W * H);
         int16_t *best = Wp.qb[0];
-        if (lane < 8) Wp.predC[lane] = -1;
-        __syncwarp();
         i64 bestJ = INF;
         int bestC = br.cand[0], bestT = br.tx;
         bool have = false;
-        // tasks (candidate, tx type) in rounds of 32 / G; costs compared in task order (first of equal costs wins);
-        // the round's winner, if it beats the best so far, leaves its levels in `best`
+        int curG = 0;
+        // tasks (candidate, tx type) in rounds of 32 / G (G per pass: round_group); costs compared in task order (first
+        // of equal costs wins); the round's winner, if it beats the best so far, leaves its levels in `best`
         auto run = [&](const int *tcand, const int *ttype, int n) {
+            const int G = round_group(txSz, n), ng = 32 / G, grp = lane / G, g = lane & (G - 1);
+            int32_t *tb = Wp.buf + grp * task_buf_ints(txSz);
+            int16_t *tq = Wp.q + grp * nq;
+            Px *tp = Wp.pred + grp * (W * H);
+            if (G != curG) {   // the groups' cached predictions belong to another grouping
+                if (lane < 8) Wp.predC[lane] = -1;
+                __syncwarp();
+                curG = G;
+            }
             for (int r0 = 0; r0 < n; r0 += ng) {
                 const int k = min(r0 + grp, n - 1);
                 const int c = tcand[k], t = ttype[k], m = cand_mode(c);
@@ -761,13 +765,13 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
         };
         // (candidate, plane) tasks in rounds of 32 / G; each candidate's cost = U + V + lambda * its mode bits; the
         // winner's two planes are evaluated once more for their levels
-        const int G = grp_size(txSz), ng = 32 / G, grp = lane / G, g = lane & (G - 1);
         const int nq = min(W, 32) * min(H, 32);
+        i64 pj[2 * (UV_K + 1)];
+        const int ntask = 2 * nch;
+        const int G = round_group(txSz, ntask), ng = 32 / G, grp = lane / G, g = lane & (G - 1);
         int32_t *tb = Wp.buf + grp * task_buf_ints(txSz);
         int16_t *tq = Wp.q + grp * nq;
         Px *tp = Wp.pred + grp * (W * H);
-        i64 pj[2 * (UV_K + 1)];
-        const int ntask = 2 * nch;
         for (int r0 = 0; r0 < ntask; r0 += ng) {
             const int k = min(r0 + grp, ntask - 1), c = chosen[k >> 1], pl = 1 + (k & 1);
             predict(pl, c, tp, g, G);
