@@ -16,7 +16,8 @@
 namespace is {
 
 // Two kernels share the block search: k_analysis for the 132 blocks of the shapes up to 32 samples a side from 8x16 /
-// 16x8 / 8x32 / 32x8 up (8 warps, 3 CTAs per SM), k_analysis_big for the 13 blocks with a 64-sample side (4 warps with
+// 16x8 / 8x32 / 32x8 up (8 warps, 2 CTAs per SM: 128 registers a thread; 3 CTAs with 80 registers spilled more and ran
+// 2.5 % slower), k_analysis_big for the 13 blocks with a 64-sample side (4 warps with
 // the larger scratch).  The 704 blocks of 4x4, 4x8, 8x4, 8x8, 4x16 and 16x4 have the per-thread searches of
 // is_tiny.cuh.
 constexpr int AN_WARPS = 8, ANB_WARPS = 4;
@@ -251,7 +252,7 @@ __device__ __forceinline__ void an_sb(const FrameDesc &F, unsigned char *smem_ra
 }
 
 template <int BD>
-__global__ void __launch_bounds__(AN_WARPS * 32, 3) k_analysis(const __grid_constant__ FrameDesc F) {
+__global__ void __launch_bounds__(AN_WARPS * 32, 2) k_analysis(const __grid_constant__ FrameDesc F) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     an_sb<BD, AN_WARPS, AN_BUF_INTS, 0>(F, smem_raw);
 }

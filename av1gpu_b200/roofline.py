@@ -16,7 +16,7 @@ OPS_PER_PX = {120: (16456.9, 830.3), 60: (18144.3, 984.0), 200: (14254.3, 669.4)
 BYTES_PER_PX = 6.4
 # DRAM bytes (read + write) per pixel of one launch, from ncu's dram__bytes_read.sum + dram__bytes_write.sum on a
 # 1920x1080 case (profiles/k_recon_1080p.md, profiles/k_analysis_1080p.md); traffic grows with the pixels processed
-TRAFFIC_PER_PX = {"k_recon": (12.235264e6 + 1.873920e6) / (1920 * 1080), "k_analysis": (10.287616e6 + 419.949056e6) / (1920 * 1080)}
+TRAFFIC_PER_PX = {"k_recon": (12.050432e6 + 1.372928e6) / (1920 * 1080), "k_analysis": (3.105792e6 + 3.166208e6) / (1920 * 1080)}
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 

@@ -5,11 +5,13 @@ stream and workspace).  Whenever a worker is free it takes the waiting requests 
 share of the HBM budget (`is_workspace_bytes` per image) and `max_batch`, and searches them as one batch
 (`is_encode_batch`: one persistent closed loop over all of them).  Requests that arrive while batches are on the GPU
 wait for the next free worker, so two batches are in flight at once and their device work overlaps; a batch's
-closed loop can be limited to part of the SMs (`recon_ctas`) to leave room for the other worker's front end.  Each
-request's latency runs from its arrival to the moment its record and reconstruction are in host memory.
+closed loop can be limited to part of the SMs (`recon_ctas`) to leave room for the other worker's front end.  With a
+`shortlist` (the learned mode shortlist: weights and its mask rule) every worker searches in the batched + shortlist
+form.  Each request's latency runs from its arrival to the moment its record and reconstruction are in host memory.
 
 The search is deterministic per image, so a request's result does not depend on the batch it ran in.
 """
+import os
 import threading
 import time
 from collections import deque
@@ -56,7 +58,9 @@ def latency_stats(requests):
 
 
 class Server:
-    def __init__(self, device=0, hbm_budget=None, pipelines=2, max_batch=64, recon_ctas=0, use_graph=False):
+    def __init__(self, device=0, hbm_budget=None, pipelines=2, max_batch=64, recon_ctas=0, use_graph=False, shortlist=None):
+        """shortlist: None (plain search) or a dict of Encoder.set_shortlist's arguments (weights, tau, max_modes, conf,
+        rd_k)."""
         from .isearch import Encoder, workspace_bytes, plane_format
         import torch
 
@@ -73,6 +77,8 @@ class Server:
         self.encs = [Encoder(device) for _ in range(pipelines)]
         for e in self.encs:
             e.set_batch_options(use_graph=use_graph, front_streams=2, recon_ctas=recon_ctas)
+            if shortlist is not None:
+                e.set_shortlist(**shortlist)
         self._pending = deque()
         self._cv = threading.Condition()
         self._closed = False
@@ -158,9 +164,18 @@ def main():
     ap.add_argument("--pipelines", type=int, default=2)
     ap.add_argument("--recon-ctas", type=int, default=110)
     ap.add_argument("--max-batch", type=int, default=32)
+    ap.add_argument("--plain", action="store_true", help="the plain search (default: batched + learned shortlist)")
+    ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "shortlist_weights.npz"))
+    ap.add_argument("--tau", type=float, default=0.9)
+    ap.add_argument("--max-modes", type=int, default=6)
+    ap.add_argument("--rd-k", type=int, default=2)
     args = ap.parse_args()
     reqs = _requests(args.n, 5)
-    srv = Server(pipelines=args.pipelines, max_batch=args.max_batch, recon_ctas=args.recon_ctas)
+    sl = None
+    if not args.plain:
+        from .shortlist import load_weights
+        sl = {"weights": load_weights(args.weights), "tau": args.tau, "max_modes": args.max_modes, "rd_k": args.rd_k}
+    srv = Server(pipelines=args.pipelines, max_batch=args.max_batch, recon_ctas=args.recon_ctas, shortlist=sl)
     try:
         srv.run([(0.0, p, q) for p, q in reqs[:4]])   # warm-up: workspaces, tables
         for rate in [float(r) for r in args.rates.split(",")]:
@@ -168,7 +183,8 @@ def main():
             done = srv.run([(float(ti), p, q) for ti, (p, q) in zip(t, reqs)])
             mp = sum(r.pixels for r in done) / 1e6
             span = max(r.t_done for r in done) - min(r.t_arrive for r in done)
-            line = {"arrival_rate_per_s": rate, "requests": len(done), "mp": round(mp, 1), "mp_per_s": round(mp / span, 2),
+            line = {"form": "plain" if args.plain else "batched + shortlist (tau %g, max %d modes, rd_k %d)" % (args.tau, args.max_modes, args.rd_k),
+                    "arrival_rate_per_s": rate, "requests": len(done), "mp": round(mp, 1), "mp_per_s": round(mp / span, 2),
                     "batches": len({r.batch for r in done}), **latency_stats(done)}
             print(json.dumps(line), flush=True)
     finally:

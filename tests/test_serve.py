@@ -41,16 +41,34 @@ def test_workspace_bytes_grows_with_the_image():
     assert workspace_bytes(4000, 3000, 8, True) > b and workspace_bytes(4000, 3000, 10, True) > workspace_bytes(4000, 3000, 8, True)
 
 
-@pytest.mark.gpu
-def test_served_results_equal_alone(enc):
+def _mixed_requests():
     sizes = [(160, 120), (96, 64), (211, 149), (64, 200), (300, 90), (128, 128), (77, 45), (256, 96)]
     qs = [60, 120, 200, 90, 150, 40, 220, 120]
     # formats mixed as requests arrive: images 2 and 5 10-bit 4:4:4, image 6 8-bit 4:4:4
     fmts = {2: (10, True), 5: (10, True), 6: (8, True)}
     images = [synth.make_image(w, h, 50 + i, edges=True, bit_depth=fmts.get(i, (8, False))[0], chroma_444=fmts.get(i, (8, False))[1])
               for i, (w, h) in enumerate(sizes)]
-    alone = [enc.encode(im, q) for im, q in zip(images, qs)]
-    srv = serve.Server(device=0, hbm_budget=1 << 30, pipelines=2, max_batch=4, recon_ctas=96)
+    return images, qs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("learned", [False, True])
+def test_served_results_equal_alone(enc, learned):
+    """Each served result (plain, or batched + learned shortlist) equals the same image searched alone with the same
+    search settings, whatever batch it was admitted into."""
+    images, qs = _mixed_requests()
+    sl = None
+    if learned:
+        from av1gpu_b200.shortlist import load_weights
+        import os
+        w = load_weights(os.path.join(os.path.dirname(serve.__file__), "shortlist_weights.npz"))
+        sl = {"weights": w, "tau": 0.9, "max_modes": 6, "rd_k": 2}
+        enc.set_shortlist(**sl)
+    try:
+        alone = [enc.encode(im, q) for im, q in zip(images, qs)]
+    finally:
+        enc.set_shortlist(None)
+    srv = serve.Server(device=0, hbm_budget=1 << 30, pipelines=2, max_batch=4, recon_ctas=96, shortlist=sl)
     try:
         t = serve.poisson_arrivals(400.0, len(images), seed=3)
         reqs = srv.run([(float(ti), im, q) for ti, im, q in zip(t, images, qs)])
