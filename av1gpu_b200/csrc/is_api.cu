@@ -329,13 +329,26 @@ int upload_tables(int dev) {
             out[n] = (int)(t.size() / 3);
             return k == n;
         };
-        int st[AN_SHAPES + 1], stBig[ANB_SHAPES + 1];
-        const bool okShapes = starts(tasks, AN_SHAPES, st) && starts(tasksBig, ANB_SHAPES, stBig);
+        int st[AN_SHAPES + 1], stBig[ANB_SHAPES + 1], grpBig[ANB_GROUPS + 1];
+        bool okShapes = starts(tasks, AN_SHAPES, st) && starts(tasksBig, ANB_SHAPES, stBig);
+        {   // the 64-sided list's groups: every shape of at least 2048 samples together, then one group per shape
+            int g = 0;
+            grpBig[g++] = 0;
+            for (int k = 1; k < ANB_SHAPES && okShapes; k++) {
+                const int bs = tasksBig[3 * stBig[k]];
+                if (AV1G_T(Num_4x4_Blocks_Wide)[bs] * AV1G_T(Num_4x4_Blocks_High)[bs] < 128) {
+                    if (g >= ANB_GROUPS) okShapes = false;
+                    else grpBig[g++] = stBig[k];
+                }
+            }
+            if (g != ANB_GROUPS) okShapes = false;
+            else grpBig[g] = stBig[ANB_SHAPES];
+        }
         if (e == cudaSuccess && okShapes && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3) {
             e = cudaMemcpyToSymbol(c_anTask, tasks.data(), tasks.size());
             if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anTaskBig, tasksBig.data(), tasksBig.size());
             if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStart, st, sizeof st);
-            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStartBig, stBig, sizeof stBig);
+            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStartBig, grpBig, sizeof grpBig);
         } else if (e == cudaSuccess) {
             e = cudaErrorInvalidValue;
         }
@@ -709,12 +722,12 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
             IS_CK(cudaGetLastError());
         }
         if (F.bd == 8) {
-            k_analysis_big<8><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig, s>>>(F);
+            k_analysis_big<8><<<ANB_GROUPS * nSb, ANB_WARPS * 32, h->smemAnBig, s>>>(F);
             k_analysis<8><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn, s>>>(F);
             k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem<uint8_t>), s>>>(F);
             k_analysis_mid<8><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem<uint8_t>), s>>>(F);
         } else {
-            k_analysis_big<10><<<ANB_SHAPES * nSb, ANB_WARPS * 32, h->smemAnBig10, s>>>(F);
+            k_analysis_big<10><<<ANB_GROUPS * nSb, ANB_WARPS * 32, h->smemAnBig10, s>>>(F);
             k_analysis<10><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn10, s>>>(F);
             k_analysis_tiny<10><<<nSb, TINY_THREADS, sizeof(TinySmem<uint16_t>), s>>>(F);
             k_analysis_mid<10><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem<uint16_t>), s>>>(F);
