@@ -24,14 +24,14 @@ constexpr int AN_WARPS = 8, ANB_WARPS = 4;
 constexpr int AN_TASKS = 132, ANB_TASKS = 13;
 constexpr int AN_BUF_INTS = 1088;             // evaluation scratch per warp: 32 / G tasks of H x (W + 1) int32 (<= 32x32)
 constexpr int ANB_BUF_INTS = 64 * 65;
-__constant__ uint8_t c_anTask[AN_TASKS][3];   // (bsize, x4, y4) largest area first, then shape, then raster
-__constant__ uint8_t c_anTaskBig[ANB_TASKS][3];
+static __constant__ uint8_t c_anTask[AN_TASKS][3];   // (bsize, x4, y4) largest area first, then shape, then raster
+static __constant__ uint8_t c_anTaskBig[ANB_TASKS][3];
 // Each CTA runs the blocks of ONE shape of one SB (grid: shapes x SBs, shape-major), so that the warps of an SM work
 // through the same code; the task ranges of the shapes in the lists above.  The 64-sided list runs in three groups
 // instead of its five shapes: 64x64 with 32x64 and 64x32 (5 blocks for the 4 warps; alone, 64x64 left three warps of
 // its CTA idle and 32x64 / 64x32 two), then 16x64, then 64x16 (4 blocks each).
 constexpr int AN_SHAPES = 8, ANB_SHAPES = 5, ANB_GROUPS = 3;
-__constant__ int c_anShapeStart[AN_SHAPES + 1], c_anShapeStartBig[ANB_GROUPS + 1];
+static __constant__ int c_anShapeStart[AN_SHAPES + 1], c_anShapeStartBig[ANB_GROUPS + 1];
 
 template <typename Px, int BUFI> struct AnWarp {
     int32_t buf[BUFI];

@@ -21,10 +21,10 @@
 #include "av1g/dsp.h"
 #include "is_dev.cuh"
 #include "is_frame.cuh"
-#include "is_analysis.cuh"
+#include "is_units.cuh"
 #include "is_tiny.cuh"
 #include "is_dp.cuh"
-#include "is_recon.cuh"
+#include "is_sched.cuh"
 #include "is_learn.cuh"
 
 using namespace is;
@@ -197,7 +197,6 @@ struct is_handle {
     size_t arenaBytes = 0;
     FrameDesc F;                 // the descriptor (device pointers), passed by value to every kernel
     int nSb = 0;
-    size_t smemAn = 0, smemAnBig = 0, smemAn10 = 0, smemAnBig10 = 0;
     size_t smemRcG[4] = {0, 0, 0, 0};       // the closed loop per format group (fmt_group)
     int rcGridG[4] = {0, 0, 0, 0};
     // last result
@@ -273,21 +272,19 @@ namespace {
 std::once_flag g_upload_once[64];
 int g_upload_rc[64];
 
+// the search's tables into every compilation unit's copies on device dev (once per device)
 int upload_tables(int dev) {
     std::call_once(g_upload_once[dev & 63], [dev] {
         const HostTables &T = host_tables();
-        std::vector<uint16_t> all((size_t)4 * NCDF);
-        for (int q = 0; q < 4; q++) memcpy(all.data() + (size_t)q * NCDF, T.cost[q].data(), NCDF * 2);
-        const std::vector<uint8_t> tasks = an_tasks(0), tasksBig = an_tasks(1);
-        cudaError_t e = cudaMemcpyToSymbol(g_cost, all.data(), all.size() * 2);
-        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgY, T.avgY, sizeof T.avgY);
-        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgPart, T.avgPart, sizeof T.avgPart);
-        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgSkip0, &T.avgSkip0, sizeof T.avgSkip0);
-        // scans packed per (tx size, class), one copy of each distinct table; the 2-D base-context offsets
-        std::vector<uint16_t> pack;
+        TableBlob B;
+        B.cost.assign((size_t)4 * NCDF, 0);
+        for (int q = 0; q < 4; q++) memcpy(B.cost.data() + (size_t)q * NCDF, T.cost[q].data(), NCDF * 2);
+        memcpy(B.avgY, T.avgY, sizeof B.avgY);
+        memcpy(B.avgPart, T.avgPart, sizeof B.avgPart);
+        B.avgSkip0 = T.avgSkip0;
+        // scans packed per (tx size, class), one copy of each distinct table
         std::vector<const uint16_t *> seen;
         std::vector<uint16_t> seenOff;
-        uint16_t off[19][3];
         for (int t = 0; t < 19; t++) {
             const int n = std::min<int>(AV1G_T(Tx_Width)[t], 32) * std::min<int>(AV1G_T(Tx_Height)[t], 32);
             const bool oneD = AV1G_T(Tx_Width)[t] <= 16 && AV1G_T(Tx_Height)[t] <= 16;
@@ -298,19 +295,13 @@ int upload_tables(int dev) {
                 while (k < seen.size() && seen[k] != sc) k++;
                 if (k == seen.size()) {
                     seen.push_back(sc);
-                    seenOff.push_back((uint16_t)pack.size());
-                    pack.insert(pack.end(), sc, sc + n);
+                    seenOff.push_back((uint16_t)B.scanPack.size());
+                    B.scanPack.insert(B.scanPack.end(), sc, sc + n);
                 }
-                off[t][c] = seenOff[k];
+                B.scanOff[t][c] = seenOff[k];
             }
         }
-        if (e == cudaSuccess) e = pack.size() == (size_t)SCAN_PACK ? cudaMemcpyToSymbol(g_scanPack, pack.data(), pack.size() * 2)
-                                                                  : cudaErrorInvalidValue;
-        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_scanOff, off, sizeof off);
-#define IS_UPLOAD_SPEC_TABLE(T, name, dims) \
-        if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_##name, name##_host, sizeof(name##_host));
-        IS_SPEC_TABLES(IS_UPLOAD_SPEC_TABLE)
-#undef IS_UPLOAD_SPEC_TABLE
+        cudaError_t e = cudaSuccess;
         // the compile-time copies of spec tables in the per-thread search must equal av1core's
         for (int c = 0; c < 3 && e == cudaSuccess; c++) {
             for (int k = 0; k < 5; k++)
@@ -320,38 +311,43 @@ int upload_tables(int dev) {
                     e = cudaErrorInvalidValue;
         }
         if (kDr23 != AV1G_T(Dr_Intra_Derivative)[23] || kDr45 != AV1G_T(Dr_Intra_Derivative)[45] || kDr67 != AV1G_T(Dr_Intra_Derivative)[67]) e = cudaErrorInvalidValue;
-        if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_baseCtx, &AV1G_T(Coeff_Base_Ctx_Offset)[0][0][0], 19 * 25);
-        // where each shape's tasks start in the two lists
-        auto starts = [](const std::vector<uint8_t> &t, int n, int *out) {
+        // the analysis task lists and where each shape's tasks start in them
+        B.anTask = an_tasks(0);
+        B.anTaskBig = an_tasks(1);
+        auto starts = [](const std::vector<uint8_t> &t, int n, std::vector<int> &out) {
+            out.assign(n + 1, 0);
             int k = 0;
             for (size_t i = 0; i < t.size() / 3; i++)
                 if (i == 0 || t[3 * i] != t[3 * i - 3]) { if (k < n) out[k] = (int)i; k++; }
             out[n] = (int)(t.size() / 3);
             return k == n;
         };
-        int st[AN_SHAPES + 1], stBig[ANB_SHAPES + 1], grpBig[ANB_GROUPS + 1];
-        bool okShapes = starts(tasks, AN_SHAPES, st) && starts(tasksBig, ANB_SHAPES, stBig);
+        std::vector<int> stBig;
+        bool okShapes = starts(B.anTask, AN_SHAPES, B.anShapeStart) && starts(B.anTaskBig, ANB_SHAPES, stBig);
         {   // the 64-sided list's groups: every shape of at least 2048 samples together, then one group per shape
+            B.anShapeStartBig.assign(ANB_GROUPS + 1, 0);
             int g = 0;
-            grpBig[g++] = 0;
+            B.anShapeStartBig[g++] = 0;
             for (int k = 1; k < ANB_SHAPES && okShapes; k++) {
-                const int bs = tasksBig[3 * stBig[k]];
+                const int bs = B.anTaskBig[3 * stBig[k]];
                 if (AV1G_T(Num_4x4_Blocks_Wide)[bs] * AV1G_T(Num_4x4_Blocks_High)[bs] < 128) {
                     if (g >= ANB_GROUPS) okShapes = false;
-                    else grpBig[g++] = stBig[k];
+                    else B.anShapeStartBig[g++] = stBig[k];
                 }
             }
             if (g != ANB_GROUPS) okShapes = false;
-            else grpBig[g] = stBig[ANB_SHAPES];
+            else B.anShapeStartBig[g] = stBig[ANB_SHAPES];
         }
-        if (e == cudaSuccess && okShapes && tasks.size() == (size_t)AN_TASKS * 3 && tasksBig.size() == (size_t)ANB_TASKS * 3) {
-            e = cudaMemcpyToSymbol(c_anTask, tasks.data(), tasks.size());
-            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anTaskBig, tasksBig.data(), tasksBig.size());
-            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStart, st, sizeof st);
-            if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_anShapeStartBig, grpBig, sizeof grpBig);
-        } else if (e == cudaSuccess) {
-            e = cudaErrorInvalidValue;
-        }
+        if (!okShapes) e = cudaErrorInvalidValue;
+        if (e == cudaSuccess) e = upload_common(B);
+        if (e == cudaSuccess) e = an_upload<8, 0>(B);
+        if (e == cudaSuccess) e = an_upload<8, 1>(B);
+        if (e == cudaSuccess) e = an_upload<10, 0>(B);
+        if (e == cudaSuccess) e = an_upload<10, 1>(B);
+        if (e == cudaSuccess) e = rc_upload<8, 1>(B);
+        if (e == cudaSuccess) e = rc_upload<8, 0>(B);
+        if (e == cudaSuccess) e = rc_upload<10, 1>(B);
+        if (e == cudaSuccess) e = rc_upload<10, 0>(B);
         g_upload_rc[dev & 63] = e == cudaSuccess ? 0 : (int)e;
     });
     return g_upload_rc[dev & 63];
@@ -362,15 +358,6 @@ size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 // format groups of a batch, each with its own closed-loop instance and ready queue: 0 8-bit 4:2:0, 1 8-bit 4:4:4,
 // 2 10-bit 4:2:0, 3 10-bit 4:4:4
 int fmt_group(int bd, int c444) { return (bd == 10 ? 2 : 0) + (c444 ? 1 : 0); }
-const void *rc_kernel(int g) {
-    return g == 0 ? (const void *)k_recon<8, 1> : g == 1 ? (const void *)k_recon<8, 0> : g == 2 ? (const void *)k_recon<10, 1>
-                                                                                        : (const void *)k_recon<10, 0>;
-}
-size_t rc_smem(int g) {
-    return g == 0 ? sizeof(RcSmem<uint8_t, 1>) : g == 1 ? sizeof(RcSmem<uint8_t, 0>) : g == 2 ? sizeof(RcSmem<uint16_t, 1>)
-                                                                                        : sizeof(RcSmem<uint16_t, 0>);
-}
-
 // lay out the workspace for an image of W x H (bit depth bd, 4:4:4 or 4:2:0); returns bytes needed, fills F's
 // pointers if base != 0.  Plane pitches are in samples (a multiple of 16).
 size_t layout(int W, int H, int bd, int c444, uint8_t *base, FrameDesc &F, int &nSb) {
@@ -462,23 +449,13 @@ int is_create(const is_params *p, is_handle **out) {
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) return fail(IS_ERR_CUDA);
     h->nSm = prop.multiProcessorCount;
-    h->smemAn = sizeof(AnSmem<uint8_t, AN_WARPS, AN_BUF_INTS>);
-    h->smemAnBig = sizeof(AnSmem<uint8_t, ANB_WARPS, ANB_BUF_INTS>);
-    h->smemAn10 = sizeof(AnSmem<uint16_t, AN_WARPS, AN_BUF_INTS>);
-    h->smemAnBig10 = sizeof(AnSmem<uint16_t, ANB_WARPS, ANB_BUF_INTS>);
-    auto attr = [](const void *k, size_t b) { return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b) == cudaSuccess; };
-    if (!attr((const void *)k_analysis<8>, h->smemAn) || !attr((const void *)k_analysis_big<8>, h->smemAnBig) ||
-        !attr((const void *)k_analysis_mid<8>, sizeof(MidSmem<uint8_t>)) || !attr((const void *)k_analysis_tiny<8>, sizeof(TinySmem<uint8_t>)) ||
-        !attr((const void *)k_analysis<10>, h->smemAn10) || !attr((const void *)k_analysis_big<10>, h->smemAnBig10) ||
-        !attr((const void *)k_analysis_mid<10>, sizeof(MidSmem<uint16_t>)) || !attr((const void *)k_analysis_tiny<10>, sizeof(TinySmem<uint16_t>)))
+    if (an_setup<8, 0>() != cudaSuccess || an_setup<8, 1>() != cudaSuccess || an_setup<10, 0>() != cudaSuccess || an_setup<10, 1>() != cudaSuccess)
         return fail(IS_ERR_CUDA);
     for (int g = 0; g < 4; g++) {   // the closed loop of each format group: shared memory and its cooperative grid
-        const void *k = rc_kernel(g);
-        h->smemRcG[g] = rc_smem(g);
         int per = 0;
-        if (!attr(k, h->smemRcG[g]) || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, RC_WARPS * 32, h->smemRcG[g]) != cudaSuccess ||
-            per < 1)
-            return fail(IS_ERR_CUDA);
+        const cudaError_t e = g == 0 ? rc_setup<8, 1>(&h->smemRcG[g], &per) : g == 1 ? rc_setup<8, 0>(&h->smemRcG[g], &per)
+                            : g == 2 ? rc_setup<10, 1>(&h->smemRcG[g], &per) : rc_setup<10, 0>(&h->smemRcG[g], &per);
+        if (e != cudaSuccess || per < 1) return fail(IS_ERR_CUDA);
         h->rcGridG[g] = per * h->nSm;
     }
     if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess) return fail(IS_ERR_CUDA);
@@ -721,17 +698,8 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
             }
             IS_CK(cudaGetLastError());
         }
-        if (F.bd == 8) {
-            k_analysis_big<8><<<ANB_GROUPS * nSb, ANB_WARPS * 32, h->smemAnBig, s>>>(F);
-            k_analysis<8><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn, s>>>(F);
-            k_analysis_tiny<8><<<nSb, TINY_THREADS, sizeof(TinySmem<uint8_t>), s>>>(F);
-            k_analysis_mid<8><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem<uint8_t>), s>>>(F);
-        } else {
-            k_analysis_big<10><<<ANB_GROUPS * nSb, ANB_WARPS * 32, h->smemAnBig10, s>>>(F);
-            k_analysis<10><<<AN_SHAPES * nSb, AN_WARPS * 32, h->smemAn10, s>>>(F);
-            k_analysis_tiny<10><<<nSb, TINY_THREADS, sizeof(TinySmem<uint16_t>), s>>>(F);
-            k_analysis_mid<10><<<3 * ((nSb + MID_SBS - 1) / MID_SBS), MID_THREADS, sizeof(MidSmem<uint16_t>), s>>>(F);
-        }
+        IS_CK((F.bd == 8 ? an_launch<8, 0>(F, nSb, s) : an_launch<10, 0>(F, nSb, s)));
+        IS_CK((F.bd == 8 ? an_launch<8, 1>(F, nSb, s) : an_launch<10, 1>(F, nSb, s)));
         IS_CK(cudaGetLastError());
         if (events && n == 1) IS_CK(cudaEventRecord(h->ev[2], s));
         k_dp<<<(nSb + 63) / 64, 64, 0, s>>>(F, nSb);
@@ -749,27 +717,15 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
         }
     }
     if (events) IS_CK(cudaEventRecord(h->ev[3], st));
-    // the closed loop of every image of a format group at once: a cooperative launch (all CTAs resident: their warps
-    // wait on each other's leaves), expressed with launch attributes so that it can be captured in a graph
+    // the closed loop of every image of a format group at once (one cooperative launch per group)
     for (int g = 0; g < 4; g++) {
         const int gn = h->bGrpStart[g + 1] - h->bGrpStart[g];
         if (gn == 0) continue;
-        const int grid = h->rcGridG[g];
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(h->reconCtas > 0 && h->reconCtas < grid ? h->reconCtas : grid);
-        cfg.blockDim = dim3(RC_WARPS * 32);
-        cfg.dynamicSmemBytes = h->smemRcG[g];
-        cfg.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
+        const int grid = h->reconCtas > 0 && h->reconCtas < h->rcGridG[g] ? h->reconCtas : h->rcGridG[g];
         const FrameDesc *fs = h->dFs + h->bGrpStart[g];
-        if (g == 0) IS_CK(cudaLaunchKernelEx(&cfg, k_recon<8, 1>, fs, gn));
-        else if (g == 1) IS_CK(cudaLaunchKernelEx(&cfg, k_recon<8, 0>, fs, gn));
-        else if (g == 2) IS_CK(cudaLaunchKernelEx(&cfg, k_recon<10, 1>, fs, gn));
-        else IS_CK(cudaLaunchKernelEx(&cfg, k_recon<10, 0>, fs, gn));
+        const size_t sm = h->smemRcG[g];
+        IS_CK((g == 0 ? rc_launch<8, 1>(fs, gn, grid, sm, st) : g == 1 ? rc_launch<8, 0>(fs, gn, grid, sm, st)
+               : g == 2 ? rc_launch<10, 1>(fs, gn, grid, sm, st) : rc_launch<10, 0>(fs, gn, grid, sm, st)));
     }
     if (events) IS_CK(cudaEventRecord(h->ev[4], st));
     for (int i = 0; i < n; i++) {

@@ -33,10 +33,10 @@ constexpr int UV_OVERHEAD = 384;   // uvOverheadBits 1.5 in 1/256 bit
 constexpr int EDGE_OFF = 16, EDGE_LEN = 16 + 2 * 64 + 16;
 
 // ---- fixed-point tables (host-built, uploaded once per process) ----
-__device__ uint16_t g_cost[4][NCDF];   // -log2(p) * 256 of every CDF symbol of av1g_cdfs, per coefficient q-context
-__constant__ int c_avgY[13];           // y_mode bits averaged over its 25 contexts
-__constant__ int c_avgPart[5][10];     // partition bits averaged over contexts, per block-size level
-__constant__ int c_avgSkip0;           // skip = 0 averaged over contexts
+static __device__ uint16_t g_cost[4][NCDF];   // -log2(p) * 256 of every CDF symbol of av1g_cdfs, per coefficient q-context
+static __constant__ int c_avgY[13];           // y_mode bits averaged over its 25 contexts
+static __constant__ int c_avgPart[5][10];     // partition bits averaged over contexts, per block-size level
+static __constant__ int c_avgSkip0;           // skip = 0 averaged over contexts
 
 // ---- the spec tables of the device code, in constant memory (av1core spec_tables.h values, copied from its host
 // tables when the library uploads its tables): uniform-index reads hit the constant cache instead of global memory ----
@@ -69,7 +69,7 @@ __constant__ int c_avgSkip0;           // skip = 0 averaged over contexts
     X(uint8_t, Tx_Type_Intra_Inv_Set2, [5]) \
     X(uint8_t, Tx_Width, [19]) \
     X(uint8_t, Tx_Width_Log2, [19])
-#define IS_DECL_SPEC_TABLE(T, name, dims) __constant__ T c_##name dims;
+#define IS_DECL_SPEC_TABLE(T, name, dims) static __constant__ T c_##name dims;
 IS_SPEC_TABLES(IS_DECL_SPEC_TABLE)
 #define ST(name) c_##name
 
@@ -77,9 +77,9 @@ IS_SPEC_TABLES(IS_DECL_SPEC_TABLE)
 // classes (packed), the 2-D base-context offsets.  A kernel whose few warps each run a long dependent chain (the
 // closed loop) stages them once per CTA in shared memory (RateStage); the others read them from global memory. ----
 constexpr int SCAN_PACK = 4912;
-__device__ uint16_t g_scanPack[SCAN_PACK];     // the scans, packed (host-built from the spec tables)
-__device__ uint8_t g_baseCtx[19 * 25];         // Coeff_Base_Ctx_Offset
-__constant__ uint16_t c_scanOff[19][3];        // offset of the scan of (tx size, class 2D / VERT / HORIZ) in the pack
+static __device__ uint16_t g_scanPack[SCAN_PACK];     // the scans, packed (host-built from the spec tables)
+static __device__ uint8_t g_baseCtx[19 * 25];         // Coeff_Base_Ctx_Offset
+static __constant__ uint16_t c_scanOff[19][3];        // offset of the scan of (tx size, class 2D / VERT / HORIZ) in the pack
 struct RateTabs {
     const uint16_t *cost, *scan;
     const uint8_t *baseCtx;                    // [19][5][5]
@@ -521,7 +521,7 @@ __device__ __forceinline__ void fwd_mem_n(int kind, int32_t *p, int stride, int 
         }
     }
 }
-__device__ __noinline__ void fwd1d_mem(int kind, int n, int32_t *p, int stride, int pre, int nout, int rect, int post) {
+static __device__ __noinline__ void fwd1d_mem(int kind, int n, int32_t *p, int stride, int pre, int nout, int rect, int post) {
     switch (n) {
     case 4: fwd_mem_n<4>(kind, p, stride, pre, nout, rect, post); break;
     case 8: fwd_mem_n<8>(kind, p, stride, pre, nout, rect, post); break;
@@ -641,7 +641,7 @@ __device__ __forceinline__ i64 base_bits_inl(int txSz, const EvalIn &e, int eob)
     return b;
 }
 // out of line with scalar arguments: no structure of the caller has to be written to memory for the call
-__device__ __noinline__ i64 base_bits(int txSz, int txType, int plane, int skipCtx, int intraDir, const uint16_t *cost, int eob) {
+static __device__ __noinline__ i64 base_bits(int txSz, int txType, int plane, int skipCtx, int intraDir, const uint16_t *cost, int eob) {
     EvalIn e;
     e.txType = txType; e.plane = plane; e.skipCtx = skipCtx; e.intraDir = intraDir;
     e.T.cost = cost;
@@ -838,7 +838,7 @@ __device__ __forceinline__ uint32_t inv_mem_n(int kind, int32_t *p, int stride, 
     }
     return e;
 }
-__device__ __noinline__ uint32_t inv1d_mem(int kind, int n, int32_t *p, int stride, int r, int preRect, int post, int clampBits) {
+static __device__ __noinline__ uint32_t inv1d_mem(int kind, int n, int32_t *p, int stride, int r, int preRect, int post, int clampBits) {
     switch (n) {
     case 4: return inv_mem_n<4>(kind, p, stride, r, preRect, post, clampBits);
     case 8: return inv_mem_n<8>(kind, p, stride, r, preRect, post, clampBits);

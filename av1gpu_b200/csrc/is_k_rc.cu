@@ -1,0 +1,40 @@
+// is_k_rc.cu - the closed-loop unit: k_recon of one format (IS_BD 8 / 10 and IS_SS 1 (4:2:0) / 0 (4:4:4), set on the
+// compiler command line), its table upload, occupancy and cooperative launch.
+#include "is_units.cuh"
+#include "is_recon.cuh"
+
+#if !defined(IS_BD) || !defined(IS_SS)
+#error "IS_BD (8 or 10) and IS_SS (1 or 0) must be defined"
+#endif
+
+namespace is {
+
+typedef std::conditional<IS_BD == 8, uint8_t, uint16_t>::type RcPx;
+
+template <> cudaError_t rc_upload<IS_BD, IS_SS>(const TableBlob &B) { return upload_common(B); }
+
+template <> cudaError_t rc_setup<IS_BD, IS_SS>(size_t *smem, int *ctasPerSm) {
+    const void *k = (const void *)k_recon<IS_BD, IS_SS>;
+    *smem = sizeof(RcSmem<RcPx, IS_SS>);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctasPerSm, k, RC_WARPS * 32, *smem);
+    return e;
+}
+
+// a cooperative launch (all CTAs resident: their warps wait on each other's leaves), expressed with launch attributes
+// so that it can be captured in a graph
+template <> cudaError_t rc_launch<IS_BD, IS_SS>(const FrameDesc *fs, int nImg, int grid, size_t smem, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(RC_WARPS * 32);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_recon<IS_BD, IS_SS>, fs, nImg);
+}
+
+}  // namespace is

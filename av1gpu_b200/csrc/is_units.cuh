@@ -1,0 +1,58 @@
+// is_units.cuh - the library's compilation units and what they export to the host orchestration (is_api.cu).
+//
+// The kernels are compiled in separate units so that they build in parallel: is_k_an.cu once per bit depth and kernel
+// pair (the four analysis kernels), is_k_rc.cu once per format (the closed loop), is_api.cu (host API, DP, scheduling, pack,
+// learned-shortlist and test kernels).  Device globals have internal linkage (static): every unit holds its own copy
+// of the search's tables, and upload_tables() in is_api.cu fills each unit's copy from one host-built TableBlob.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <vector>
+#include "is_dev.cuh"
+#include "is_frame.cuh"
+
+namespace is {
+
+// the host-built tables of the search (cost tables of the four q-contexts, averaged bits, packed scans, analysis task
+// lists); the spec tables of av1core are copied by each unit from av1core's host arrays
+struct TableBlob {
+    std::vector<uint16_t> cost;            // 4 x NCDF
+    int avgY[13];
+    int avgPart[5][10];
+    int avgSkip0;
+    std::vector<uint16_t> scanPack;        // SCAN_PACK entries
+    uint16_t scanOff[19][3];
+    std::vector<uint8_t> anTask, anTaskBig;
+    std::vector<int> anShapeStart, anShapeStartBig;
+};
+
+// the tables every unit indexes, into this unit's copies
+static inline cudaError_t upload_common(const TableBlob &B) {
+    cudaError_t e = B.cost.size() == (size_t)4 * NCDF && B.scanPack.size() == (size_t)SCAN_PACK ? cudaSuccess : cudaErrorInvalidValue;
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_cost, B.cost.data(), B.cost.size() * 2);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgY, B.avgY, sizeof B.avgY);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgPart, B.avgPart, sizeof B.avgPart);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_avgSkip0, &B.avgSkip0, sizeof B.avgSkip0);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_scanPack, B.scanPack.data(), B.scanPack.size() * 2);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_scanOff, B.scanOff, sizeof B.scanOff);
+#define IS_UPLOAD_SPEC_TABLE(T, name, dims) \
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_##name, name##_host, sizeof(name##_host));
+    IS_SPEC_TABLES(IS_UPLOAD_SPEC_TABLE)
+#undef IS_UPLOAD_SPEC_TABLE
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_baseCtx, &AV1G_T(Coeff_Base_Ctx_Offset)[0][0][0], 19 * 25);
+    return e;
+}
+
+// ---- analysis units (is_k_an.cu, BD 8 / 10 x PART 0: the warp-path kernels k_analysis_big and k_analysis, PART 1:
+//      the per-thread kernels k_analysis_tiny and k_analysis_mid) ----
+template <int BD, int PART> cudaError_t an_upload(const TableBlob &B);
+template <int BD, int PART> cudaError_t an_setup();   // dynamic shared memory limits of the unit's kernels
+template <int BD, int PART> cudaError_t an_launch(const FrameDesc &F, int nSb, cudaStream_t s);
+
+// ---- closed-loop unit (is_k_rc.cu, BD 8 / 10 x SS 1 (4:2:0) / 0 (4:4:4)) ----
+template <int BD, int SS> cudaError_t rc_upload(const TableBlob &B);
+// shared memory of the kernel and its co-resident CTAs per SM (the cooperative grid is that times the SM count)
+template <int BD, int SS> cudaError_t rc_setup(size_t *smem, int *ctasPerSm);
+template <int BD, int SS> cudaError_t rc_launch(const FrameDesc *fs, int nImg, int grid, size_t smem, cudaStream_t st);
+
+}  // namespace is
