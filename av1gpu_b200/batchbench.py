@@ -16,24 +16,29 @@ import time
 import numpy as np
 
 
-def workload(n, seed, max_mp=24.0, min_mp=0.18, frac10=0.2):
-    """n (planes, qindex) pairs: crops of an 8-bit 4:2:0 and a 10-bit 4:4:4 synthetic 6000 x 4000 picture."""
+def workload(n, seed, max_mp=24.0, min_mp=0.18, frac10=0.2, base8=(6000, 4000), base10=(6000, 4000)):
+    """n (planes, qindex) pairs: crops of an 8-bit 4:2:0 and a 10-bit 4:4:4 synthetic picture (6000 x 4000 each by
+    default; smaller bases clip the crops to their size)."""
     from . import synth
     rng = np.random.default_rng(seed)
-    W, H = 6000, 4000
-    base8 = synth.make_image(W, H, seed, edges=True)
-    base10 = synth.make_image(W, H, seed + 1, edges=True, bit_depth=10, chroma_444=True)
+    b8 = synth.make_image(base8[0], base8[1], seed, edges=True)
+    b10 = synth.make_image(base10[0], base10[1], seed + 1, edges=True, bit_depth=10, chroma_444=True)
     out = []
     for _ in range(n):
         area = float(np.exp(rng.uniform(np.log(min_mp * 1e6), np.log(max_mp * 1e6))))
         ar = float(np.exp(rng.uniform(np.log(1 / 3), np.log(3))))
+        W, H = base8
         w = int(min(W, max(16, np.sqrt(area * ar)))) & ~1
         h = int(min(H, max(16, np.sqrt(area / ar)))) & ~1
         x0, y0 = int(rng.integers(0, W - w + 1)) & ~1, int(rng.integers(0, H - h + 1)) & ~1
-        if rng.random() < frac10:
-            planes = [np.ascontiguousarray(p[y0:y0 + h, x0:x0 + w]) for p in base10]
+        ten = rng.random() < frac10
+        if ten and tuple(base10) != tuple(base8):   # a smaller 10-bit base: the crop clipped and moved into it
+            w, h = min(w, base10[0]) & ~1, min(h, base10[1]) & ~1
+            x0, y0 = min(x0, base10[0] - w) & ~1, min(y0, base10[1] - h) & ~1
+        if ten:
+            planes = [np.ascontiguousarray(p[y0:y0 + h, x0:x0 + w]) for p in b10]
         else:
-            y, u, v = base8
+            y, u, v = b8
             planes = [np.ascontiguousarray(y[y0:y0 + h, x0:x0 + w]), np.ascontiguousarray(u[y0 // 2:(y0 + h) // 2, x0 // 2:(x0 + w) // 2]),
                       np.ascontiguousarray(v[y0 // 2:(y0 + h) // 2, x0 // 2:(x0 + w) // 2])]
         out.append((planes, int(rng.integers(40, 221))))
@@ -53,6 +58,7 @@ def main():
     ap.add_argument("--tau", type=float, default=0.9)
     ap.add_argument("--max-modes", type=int, default=6)
     ap.add_argument("--rd-k", type=int, default=2)
+    ap.add_argument("--no-verify", action="store_true", help="skip the check that the batch equals the one-at-a-time search")
     args = ap.parse_args()
     t0 = time.time()
     work = workload(args.images, args.seed, args.max_mp)
@@ -95,6 +101,20 @@ def main():
     tb, k = batched()
     print(json.dumps({**base, "form": "batched (one batch, CUDA graph)", "mp_per_s": round(mp / tb, 2), "s": round(tb, 3),
                       "front_streams": k, "x_plain": round(tp / tb, 2)}), flush=True)
+    if not args.no_verify:   # untimed: every image of the batch bit-equal to its one-at-a-time search
+        k, _ = enc.autotune_batch(dev[:args.tune_images], qs[:args.tune_images], host=False)
+        enc.set_batch_options(use_graph=True, front_streams=k)
+        enc.encode_batch_async(dev, qs, host=False)
+        want = [enc.batch_fetch(i, p[0].shape[1], p[0].shape[0], q, *f).digest() for i, ((p, q), f) in enumerate(zip(work, fmt))]
+        enc.set_batch_options(use_graph=False, front_streams=1)
+        same = 0
+        for i, ((p, q), f) in enumerate(zip(work, fmt)):
+            enc.encode_device_async(dev[i], q)
+            same += enc.fetch(p[0].shape[1], p[0].shape[0], q, bit_depth=f[0], chroma_444=f[1]).digest() == want[i]
+        print(json.dumps({**base, "parity": "%d/%d images of the batch (CUDA graph) bit-equal to the one-at-a-time search"
+                                            % (same, len(work))}), flush=True)
+        if same != len(work):
+            raise SystemExit("batched results differ from the one-at-a-time search")
     enc.set_shortlist(load_weights(args.weights), tau=args.tau, max_modes=args.max_modes, rd_k=args.rd_k)
     ts, k = batched()
     enc.set_shortlist(None)

@@ -227,6 +227,10 @@ __device__ __forceinline__ void an_sb(const FrameDesc &F, unsigned char *smem_ra
     const int sbx = sbc * 64, sby = sbr * 64;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int t0 = an_shape_start<LIST>(shape), t1 = an_shape_start<LIST>(shape + 1);
+    if (F.poison) {
+        smem_poison(smem_raw, sizeof(Sm), tid, NW * 32);
+        __syncthreads();
+    }
     {   // the SB tile with 128-bit loads (rows and the tile's first column are 16-byte aligned by the layout)
         constexpr int V = Sm::TW * (int)sizeof(Px) / 16;
         const Px *s0 = (const Px *)F.src[0] + (size_t)(sby - 1) * F.spitch[0] + (sbx - 16);

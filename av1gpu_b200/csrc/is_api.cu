@@ -237,6 +237,12 @@ struct is_handle {
     int frontStreams = 1;                   // 1, 2 or 4 (is_autotune_batch chooses)
     int reconCtas = 0;                      // CTAs of the closed loop (0: one per SM); fewer leave SMs to other streams
     bool useGraph = false;
+    // error paths: the closed loop's wait budgets, the workspace budget, poison mode
+    int waitIters = LEAF_WAIT_ITERS;
+    long long readyWaitNs = READY_WAIT_NS;
+    uint64_t wsLimit = 0;                   // 0: no limit
+    bool poison = false;
+    size_t bNeed = 0;                       // bytes of the arena the last batch uses
     // learned shortlist (is_set_shortlist_model): bf16 weights, fp32 biases, mask rule; per front-end stream a chunk of
     // features / hidden activations / scores
     bool slOn = false;
@@ -269,12 +275,16 @@ struct is_handle {
 
 namespace {
 
-std::once_flag g_upload_once[64];
-int g_upload_rc[64];
+// per device: whether the tables are uploaded (a failed upload is retried by the next call)
+std::mutex g_upload_mu;
+bool g_uploaded[64];
 
 // the search's tables into every compilation unit's copies on device dev (once per device)
 int upload_tables(int dev) {
-    std::call_once(g_upload_once[dev & 63], [dev] {
+    if (dev < 0 || dev >= 64) return (int)cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_upload_mu);
+    if (g_uploaded[dev]) return 0;
+    {
         const HostTables &T = host_tables();
         TableBlob B;
         B.cost.assign((size_t)4 * NCDF, 0);
@@ -348,9 +358,9 @@ int upload_tables(int dev) {
         if (e == cudaSuccess) e = rc_upload<8, 0>(B);
         if (e == cudaSuccess) e = rc_upload<10, 1>(B);
         if (e == cudaSuccess) e = rc_upload<10, 0>(B);
-        g_upload_rc[dev & 63] = e == cudaSuccess ? 0 : (int)e;
-    });
-    return g_upload_rc[dev & 63];
+        g_uploaded[dev] = e == cudaSuccess;
+        return e == cudaSuccess ? 0 : (int)e;
+    }
 }
 
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -550,6 +560,11 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         frame_format(h, f, &h->bBd[i], &h->bC444[i]);
         if ((h->bBd[i] != 8 && h->bBd[i] != 10) || (h->bC444[i] != 0 && h->bC444[i] != 1))
             return h->setErr(IS_ERR_INVALID, "invalid frame %d format (bit depth %d, chroma_444 %d)", i, h->bBd[i], h->bC444[i]);
+        for (int p = 0; p < 3; p++) {   // every plane present, its rows at least as long as the plane is wide
+            const int ss = (p && !h->bC444[i]) ? 1 : 0, vw = (f->width + ss) >> ss;
+            if (!f->planes[p] || f->pitch[p] < vw)
+                return h->setErr(IS_ERR_INVALID, "invalid frame %d plane %d (pointer %p, pitch %d for width %d)", i, p, f->planes[p], f->pitch[p], vw);
+        }
     }
     std::vector<size_t> off(n + 1);
     std::vector<int> nsb(n), grp(n);
@@ -575,6 +590,10 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
     for (int g = 1; g < 4; g++) offQG[g] = offQG[g - 1] + align256(slotsG[g - 1] * 8);
     const size_t offQ = at, offRq = offQG[3] + align256(slotsG[3] * 8), offErr = offRq + 256, offFs = offErr + 256;
     const size_t need = offFs + align256((size_t)n * sizeof(FrameDesc));
+    if (h->wsLimit && need > h->wsLimit)
+        return h->setErr(IS_ERR_OOM, "the batch needs %zu bytes of workspace, over the handle's limit of %llu", need,
+                         (unsigned long long)h->wsLimit);
+    h->bNeed = need;
     if (need > h->arenaBytes) {
         if (h->arena) { cudaStreamSynchronize(h->own); cudaDeviceSynchronize(); cudaFree(h->arena); h->arena = nullptr; h->arenaBytes = 0; }
         IS_CK(cudaMalloc(&h->arena, need));
@@ -634,6 +653,9 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         F.leafTrace = (h->trace && i == 0 && F.img == 0) ? h->traceBuf : nullptr;   // image 0, when its group's first
         if (!h->slOn) F.slMask = nullptr;
         F.slRdK = h->slOn ? h->slRdK : 4;
+        F.waitIters = h->waitIters;
+        F.readyWaitNs = h->readyWaitNs;
+        F.poison = h->poison ? 1 : 0;
         sb_orders(F, cs, rs, h->hOrd + o, h->hOrd + o + ns);
         o += 2 * (size_t)ns;
         h->hFs[h->bPos[i]] = F;
@@ -646,6 +668,9 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
 // the launch sequence of a prepared batch on stream st (capturable: no host synchronisation inside)
 static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n, bool fromHost, bool events) {
     if (events) IS_CK(cudaEventRecord(h->ev[0], st));
+    // poison mode: every byte of the batch's workspace starts as garbage (whatever the launch sequence does not write
+    // before it reads would change the results)
+    if (h->poison) IS_CK(cudaMemsetAsync(h->arena, 0xA5, h->bNeed, st));
     IS_CK(cudaMemcpyAsync(h->dFs, h->hFs, (size_t)n * sizeof(FrameDesc), cudaMemcpyHostToDevice, st));
     {
         size_t o = 0;
@@ -702,7 +727,7 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
         IS_CK((F.bd == 8 ? an_launch<8, 1>(F, nSb, s) : an_launch<10, 1>(F, nSb, s)));
         IS_CK(cudaGetLastError());
         if (events && n == 1) IS_CK(cudaEventRecord(h->ev[2], s));
-        k_dp<<<(nSb + 63) / 64, 64, 0, s>>>(F, nSb);
+        k_dp<<<(nSb + DP_WARPS - 1) / DP_WARPS, DP_WARPS * 32, 0, s>>>(F, nSb);
         k_leaf_prep<<<nSb, 256, 0, s>>>(F, nSb);
         k_leaf_queue_scan<<<1, 1024, 0, s>>>(F, nSb);
         k_leaf_deps<0><<<nSb, 256, 0, s>>>(F, nSb);
@@ -750,7 +775,8 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
 static std::string batch_key(const is_handle *h, const is_frame *fr, int n, bool fromHost) {
     std::string k;
     char b[160];
-    snprintf(b, sizeof b, "%p|%d|%d|%d|%d|%d|", h->arena, n, (int)fromHost, h->frontStreams, h->reconCtas, h->slOn ? h->slVersion : -1);
+    snprintf(b, sizeof b, "%p|%d|%d|%d|%d|%d|%d|%d|%lld|", h->arena, n, (int)fromHost, h->frontStreams, h->reconCtas, h->slOn ? h->slVersion : -1,
+             (int)h->poison, h->waitIters, h->readyWaitNs);
     k += b;
     for (int i = 0; i < n; i++) {
         snprintf(b, sizeof b, "%d,%d,%d,%d,%d,%p,%p,%p,%d,%d,%d;", fr[i].width, fr[i].height, fr[i].qindex, fr[i].bit_depth, fr[i].chroma_444,
@@ -868,6 +894,25 @@ int is_set_batch_options(is_handle *h, int use_graph, int front_streams, int rec
     if (front_streams) h->frontStreams = front_streams;
     h->reconCtas = recon_ctas;
     if (!h->useGraph && h->graphExec) { cudaGraphExecDestroy(h->graphExec); h->graphExec = nullptr; h->graphKey.clear(); }
+    return IS_OK;
+}
+
+int is_set_wait_limits(is_handle *h, int leaf_wait_iters, long long ready_wait_ns) {
+    if (!h || leaf_wait_iters < 0 || leaf_wait_iters > (1 << 24) || ready_wait_ns < 0 || ready_wait_ns > 60000000000ll) return IS_ERR_INVALID;
+    h->waitIters = leaf_wait_iters ? leaf_wait_iters : LEAF_WAIT_ITERS;
+    h->readyWaitNs = ready_wait_ns ? ready_wait_ns : READY_WAIT_NS;
+    return IS_OK;
+}
+
+int is_set_workspace_limit(is_handle *h, uint64_t bytes) {
+    if (!h) return IS_ERR_INVALID;
+    h->wsLimit = bytes;
+    return IS_OK;
+}
+
+int is_set_poison(is_handle *h, int on) {
+    if (!h) return IS_ERR_INVALID;
+    h->poison = on != 0;
     return IS_OK;
 }
 

@@ -139,6 +139,13 @@ __device__ __forceinline__ int ci_br(int s, int p, int c) {
     return IS_CB(coeff_br) + ((s * IS_CD(coeff_br, 1) + p) * IS_CD(coeff_br, 2) + c) * IS_CD(coeff_br, 3);
 }
 
+// ---- shared-memory poison (is_set_poison): every word of a kernel's shared memory starts as a fixed garbage pattern,
+// so a read before the kernel's own write changes the results instead of finding a benign leftover.  The caller
+// synchronises the CTA after it. ----
+__device__ __forceinline__ void smem_poison(unsigned char *base, size_t bytes, int tid, int nt) {
+    for (size_t i = tid; i < bytes / 4; i += nt) reinterpret_cast<uint32_t *>(base)[i] = 0xA5C3E1F7u;
+}
+
 // ---- warp helpers ----
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ int warp_sum(int v) {

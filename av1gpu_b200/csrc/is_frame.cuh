@@ -83,6 +83,10 @@ struct __align__(16) FrameDesc {
     uint32_t *recBlockTxb;
     av1g_txb *recTxb;
     int16_t *recCoeffs;
+    // the closed loop's wait budgets (is_set_wait_limits): spins on a leaf flag, globaltimer ns on a ready-queue slot
+    long long readyWaitNs;
+    int waitIters;
+    int poison;                               // fill shared memory with a pattern at kernel start (is_set_poison)
 };
 
 // error codes written to FrameDesc::err by the kernels

@@ -23,9 +23,10 @@
 namespace is {
 
 constexpr int RC_WARPS = 4;                // warps per CTA (independent workers; shared memory bounds the count)
-constexpr int LEAF_WAIT_ITERS = 1 << 20;   // bounded spins: a wait that runs out records an error and moves on, and
-                                           // once any error is recorded no further wait starts (the host discards the
-                                           // result)
+// bounded waits (defaults; FrameDesc::waitIters / readyWaitNs carry the values of a run): a wait that runs out records
+// an error and moves on, and once any error is recorded no further wait starts (the host discards the result)
+constexpr int LEAF_WAIT_ITERS = 1 << 20;
+constexpr long long READY_WAIT_NS = 4000000000ll;
 
 template <typename Px, int SS> struct RcWarp {   // SS: chroma subsampling (1 4:2:0, 0 4:4:4)
     int32_t buf[64 * 65];      // evaluation scratch (32 / G tasks) and the inverse transform's residual
@@ -290,7 +291,7 @@ static __device__ __noinline__ bool rc_wait(const FrameDesc &F, int sb, int li, 
         const int *flag = F.leafDone + id;
         int it = 0;
         while (ld_acquire(flag) < level) {
-            if (++it > LEAF_WAIT_ITERS || *(volatile int *)F.err) { ok = false; break; }
+            if (++it > F.waitIters || *(volatile int *)F.err) { ok = false; break; }
             __nanosleep(64);
         }
     }
@@ -831,7 +832,6 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
 // descriptors in device memory; one instance per bit depth BD and chroma subsampling SS, a batch's images run in groups
 // of one format): a warp takes the next slot, waits until a leaf has been written there (bounded in time), brings the
 // descriptor of the leaf's image into its shared copy when the image changes, and runs the leaf.
-constexpr unsigned long long READY_WAIT_NS = 4000000000ull;
 template <int BD, int SS>
 __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__restrict__ Fs, int nImg) {
     typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
@@ -840,6 +840,10 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
     const int warp = threadIdx.x >> 5, lane = lane_id();
     RcWarp<Px, SS> &Wp = S.w[warp];
     FrameDesc &F = S.F[warp];
+    if (Fs[0].poison) {
+        smem_poison(smem_raw, sizeof(RcSmem<Px, SS>), threadIdx.x, blockDim.x);
+        __syncthreads();
+    }
     {   // all four cost tables (q-context 0 in the RateStage), the scans and base-context offsets
         rate_tabs_stage(S.T, 0, threadIdx.x, blockDim.x);
         for (int q = 1; q < 4; q++) {
@@ -851,6 +855,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
     const int *rq = Fs[0].rq;
     const unsigned long long *readyQ = Fs[0].readyQ;
     int *err = Fs[0].err;
+    const unsigned long long readyWait = (unsigned long long)Fs[0].readyWaitNs;
     unsigned long long *traceBase = Fs[0].leafTrace;
     int total = 0;
     for (int i = 0; i < nImg; i++) total += (int)*Fs[i].leafTotal;
@@ -866,7 +871,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
                 const unsigned long long t0 = gtimer();
                 for (;;) {
                     asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(e) : "l"(readyQ + h) : "memory");
-                    if (e || gtimer() - t0 > READY_WAIT_NS || *(volatile int *)err) break;
+                    if (e || gtimer() - t0 > readyWait || *(volatile int *)err) break;
                     __nanosleep(128);
                 }
                 if (!e) { atomicCAS(err, 0, KERR_WAIT_LEAF); bad = 1; }

@@ -420,6 +420,10 @@ __global__ void __launch_bounds__(TINY_THREADS, BD == 8 ? 2 : 1) k_analysis_tiny
     const int sb = blockIdx.x, sbr = sb / F.sbCols, sbc = sb % F.sbCols;
     const int sbx = sbc * 64, sby = sbr * 64;
     const int tid = threadIdx.x;
+    if (F.poison) {
+        smem_poison(smem_raw, sizeof(Sm), tid, TINY_THREADS);
+        __syncthreads();
+    }
     {   // the SB tile (as an_sb), the rate tables, the inverse scans of the three sizes
         constexpr int V = Sm::TW * (int)sizeof(Px) / 16;
         const Px *s0 = (const Px *)F.src[0] + (size_t)(sby - 1) * F.spitch[0] + (sbx - 16);
@@ -687,6 +691,10 @@ __global__ void __launch_bounds__(MID_THREADS, 2) k_analysis_mid(const __grid_co
     const int shape = blockIdx.x / groups, sb0 = (blockIdx.x % groups) * MID_SBS;
     const int tid = threadIdx.x;
     const int txSz = shape == 0 ? AV1G_TX_8X8 : shape == 1 ? AV1G_TX_4X16 : AV1G_TX_16X4;
+    if (F.poison) {
+        smem_poison(smem_raw, sizeof(Sm), tid, MID_THREADS);
+        __syncthreads();
+    }
     constexpr int V = Sm::TW * (int)sizeof(Px) / 16;
     for (int k = tid; k < MID_SBS * Sm::TH * V; k += MID_THREADS) {
         const int u = k / (Sm::TH * V), r = (k / V) % Sm::TH, c = k % V, sb = sb0 + u;

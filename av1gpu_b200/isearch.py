@@ -24,7 +24,16 @@ TXB_DT = np.dtype([("coeff_off", "<u4"), ("x4", "<u2"), ("y4", "<u2"), ("plane",
                    ("tx_type", "u1"), ("flags", "u1"), ("eob", "<u2"), ("reserved", "<u2")])
 
 IS_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "wavefront wait timeout",
-             -5: "no result"}
+             -5: "no result", -6: "too large for the static scratch"}
+IS_ERR_INVALID, IS_ERR_CUDA, IS_ERR_OOM, IS_ERR_TIMEOUT, IS_ERR_STATE, IS_ERR_TOO_LARGE = -1, -2, -3, -4, -5, -6
+
+
+class IsError(RuntimeError):
+    """A failed entry point: .code is the library's status (IS_ERR_*), the message the handle's last error."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
 
 
 class IsParams(C.Structure):
@@ -47,7 +56,8 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32", "is_set_trace", "is_get_trace",
            "is_fwd_quant_static", "is_encode_batch", "is_batch_counts", "is_batch_copy", "is_set_batch_options",
            "is_autotune_batch", "is_workspace_bytes", "is_workspace_bytes_format", "is_sl_create", "is_sl_destroy", "is_sl_set_weights",
-           "is_sl_get_weights", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset", "is_set_shortlist_model"]
+           "is_sl_get_weights", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset", "is_set_shortlist_model",
+           "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison"]
 
 _lib = None
 
@@ -101,6 +111,9 @@ def load_library():
     L.is_sl_dataset.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int)]
     L.is_set_shortlist_model.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_int, C.c_float, C.c_int]
     L.is_autotune_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
+    L.is_set_wait_limits.argtypes = [vp, C.c_int, C.c_longlong]
+    L.is_set_workspace_limit.argtypes = [vp, C.c_uint64]
+    L.is_set_poison.argtypes = [vp, C.c_int]
     _lib = L
     return L
 
@@ -158,6 +171,14 @@ class Record:
         self.recon = recon
         self.times = times
 
+    def digest(self):
+        """BLAKE2b of every record array and reconstruction plane: equal digests = bit-equal results."""
+        import hashlib
+        h = hashlib.blake2b(digest_size=20)
+        for a in (self.blocks, self.block_txb, self.txb, self.coeffs, *self.recon):
+            h.update(np.ascontiguousarray(a).view(np.uint8).tobytes())
+        return h.hexdigest()
+
 
 class Encoder:
     """GpEncoder-shaped handle (one host thread at a time)."""
@@ -169,7 +190,7 @@ class Encoder:
         h = C.c_void_p()
         rc = self.L.is_create(C.byref(p), C.byref(h))
         if rc != 0:
-            raise RuntimeError("is_create failed (%d: %s)" % (rc, IS_ERRORS.get(rc, "?")))
+            raise IsError(rc, "is_create failed (%d: %s)" % (rc, IS_ERRORS.get(rc, "?")))
         self.h = h
 
     def close(self):
@@ -186,7 +207,7 @@ class Encoder:
     def _check(self, rc, what):
         if rc != 0:
             msg = self.L.is_last_error(self.h).decode(errors="replace")
-            raise RuntimeError("%s failed (%d: %s): %s" % (what, rc, IS_ERRORS.get(rc, "?"), msg))
+            raise IsError(rc, "%s failed (%d: %s): %s" % (what, rc, IS_ERRORS.get(rc, "?"), msg))
 
     @staticmethod
     def _frame(planes, qindex, host):
@@ -292,6 +313,18 @@ class Encoder:
             bd, c444 = plane_format(im)
             out.append(self.batch_fetch(i, im[0].shape[1], im[0].shape[0], q, bd, c444))
         return out
+
+    def set_wait_limits(self, leaf_wait_iters=0, ready_wait_ns=0):
+        """Closed-loop wait budgets (0: the defaults); a wait that runs out makes the encode raise IsError(-4)."""
+        self._check(self.L.is_set_wait_limits(self.h, int(leaf_wait_iters), int(ready_wait_ns)), "is_set_wait_limits")
+
+    def set_workspace_limit(self, nbytes=0):
+        """Device-memory budget of the workspace (0: none); an encode over it raises IsError(-3) before allocating."""
+        self._check(self.L.is_set_workspace_limit(self.h, int(nbytes)), "is_set_workspace_limit")
+
+    def set_poison(self, on=True):
+        """Poison mode: workspace bytes and kernel shared memory start as garbage (results must not change)."""
+        self._check(self.L.is_set_poison(self.h, 1 if on else 0), "is_set_poison")
 
     def set_batch_options(self, use_graph=False, front_streams=0, recon_ctas=0):
         self._check(self.L.is_set_batch_options(self.h, 1 if use_graph else 0, front_streams, recon_ctas),

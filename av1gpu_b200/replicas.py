@@ -16,16 +16,24 @@ def assign(areas, world):
     return [sorted(v) for v in out]
 
 
-def run(images, encode, rank, world, group=None):
+def run(images, encode, rank, world, group=None, areas=None):
     """Encode this rank's share of `images` with `encode(i, image) -> summary` and gather every summary on every rank
-    (index -> summary).  `images` is the full list (each rank may hold only its own; others may be None)."""
+    (index -> summary).
+
+    Either every rank passes the full list of images, or the caller passes `areas` (luma samples per image, the same
+    list on every rank) and each rank loads only the images `assign(areas, world)[rank]` names, the other entries of
+    `images` being None.  A rank given None for one of its own images raises ValueError."""
     import torch.distributed as dist
-    areas = [0 if im is None else im[0].shape[0] * im[0].shape[1] for im in images]
-    if world > 1:
-        sizes = [None] * world
-        dist.all_gather_object(sizes, areas, group=group)
-        areas = [max(v) for v in zip(*sizes)]
+    if areas is None:
+        areas = [0 if im is None else im[0].shape[0] * im[0].shape[1] for im in images]
+        if world > 1:
+            sizes = [None] * world
+            dist.all_gather_object(sizes, areas, group=group)
+            areas = [max(v) for v in zip(*sizes)]
     mine = assign(areas, world)[rank]
+    missing = [i for i in mine if images[i] is None]
+    if missing:
+        raise ValueError("rank %d was not given its images %s (see assign())" % (rank, missing[:8]))
     res = {i: encode(i, images[i]) for i in mine}
     if world == 1:
         return res

@@ -14,7 +14,8 @@
  *
  * Plain form only: the reference GpConfig defaults without the speed switches (all 19 shapes, all partitions,
  * K 4 / Krecheck 2, tx-type search open and closed loop, angle deltas, CfL, uvK 2; edge filter, filter intra,
- * palette, QM, delta-q off; minimum legal tiling; tx_mode_select 0).  8-bit 4:2:0.
+ * palette, QM, delta-q off; minimum legal tiling; tx_mode_select 0).  8- and 10-bit samples, 4:2:0 and 4:4:4, chosen per
+ * frame (is_frame.bit_depth / chroma_444) or per handle (is_params).
  *
  * Status codes: IS_OK or a negative IS_ERR_*; is_last_error() returns the message of the last failure of a handle.
  * A handle serves one host thread at a time (several handles may run concurrently on different streams).
@@ -98,6 +99,23 @@ int is_batch_copy(is_handle *h, int i, av1g_frame_params *fp, av1g_block *blocks
  * qindex, plane addresses, workspace) repeats; front_streams: 1, 2 or 4 (0 keeps the current value); recon_ctas: CTAs
  * of the closed loop, one per SM when 0 (fewer leave SMs to the work of other streams, e.g. another handle's batch). */
 int is_set_batch_options(is_handle *h, int use_graph, int front_streams, int recon_ctas);
+/* ---- error paths and checks ----
+ * Closed-loop wait budgets of the handle's later encodes: spins of a wait on a neighbouring leaf's flag (each spin
+ * sleeps about 64 ns) and nanoseconds a worker waits on an empty ready-queue slot; 0 restores the defaults (2^20 spins,
+ * 4 s; at most 2^24 spins and 60 s).  A wait that runs out ends the closed loop (every worker abandons its leaf and the
+ * kernel returns) and the encode returns IS_ERR_TIMEOUT; the handle stays usable.  The reference has no counterpart
+ * (its wavefront steps are separate launches with no waits). */
+int is_set_wait_limits(is_handle *h, int leaf_wait_iters, long long ready_wait_ns);
+/* Device-memory budget of the handle's workspace in bytes (0: no limit): an encode or batch whose workspace would
+ * exceed it returns IS_ERR_OOM before any allocation (admission by HBM budget; the reference fails in cudaMalloc,
+ * pipeline.cpp:31-39). */
+int is_set_workspace_limit(is_handle *h, uint64_t bytes);
+/* Poison mode (the reference's GP_POISON / GP_POISON_SMEM, encoder/src/pipeline.cpp:311-313, k_recon.cuh:1705-1708):
+ * before each encode every byte of the workspace is set to 0xA5, and every search kernel fills its shared memory with a
+ * fixed pattern before it starts.  A read of anything the search did not write first would change the results; with
+ * poison on they must equal those without. */
+int is_set_poison(is_handle *h, int on);
+
 /* Device workspace of one image of width x height in a batch (bytes; host only, no GPU needed): what admission by
  * HBM budget counts. */
 int is_workspace_bytes(int width, int height, uint64_t *bytes);
@@ -179,7 +197,12 @@ int is_probe_int32(int device, double *gops, float *ms);
  * budgeted elsewhere, or code that must not meet the allocator's implicit synchronisation).  The kernel's buffers live
  * in one static scratch of IS_STATIC_SCRATCH_BYTES per device, reserved with the library's module.
  *  - The first call on a device does one-time setup (the search's tables, the scratch address): make it before any
- *    stream capture.  Nothing is claimed about calls inside a capture.
+ *    stream capture.  While the given stream is being captured, a call that would do the setup returns IS_ERR_INVALID
+ *    without doing anything; a setup that failed is tried again by the next call.  Nothing is claimed about calls
+ *    inside a capture.
+ *  - ctx = (skipCtx 0..12, dcCtx 0..2, intraDir 0..12), and tx_type must be one of the intra set of tx_size
+ *    (DCT_DCT alone for sizes with a 64-sample side and for 32x32, 16x32, 32x16, 8x32, 32x8); anything else returns
+ *    IS_ERR_INVALID before any GPU work.
  *  - n blocks of W x H need n * (4 W H + 6 nc + 20) bytes, each of the six sections rounded up to 256 bytes
  *    (nc = min(W, 32) * min(H, 32)); a request that does not fit returns IS_ERR_TOO_LARGE before any GPU work (for
  *    example at most 186 blocks of 64x64, 1625 of 16x16).  Bad arguments return IS_ERR_INVALID, CUDA failures

@@ -62,6 +62,27 @@ def test_oracle_formats_recon_is_av1core(bd, c444, w, h, q, smooth):
         assert np.array_equal(rec[p], r.recon[p])
 
 
+def test_oracle_reference_gate_picture():
+    """The oracle reproduces its committed records of the reference's CfL frame-edge picture (8-bit 4:2:0 planes from
+    tests/gate_images/cfl_edge_211x149.png) at qindex 60 / 120 / 200, and av1core reconstructs them exactly."""
+    z = np.load(os.path.join(ROOT, "tests", "golden", "gate_cfl_edge_211x149.npz"))
+    planes = (z["y"], z["u"], z["v"])
+    h, w = planes[0].shape
+    assert (w, h) == (211, 149)
+    for q in z["qs"]:
+        q = int(q)
+        r = O.encode(planes, q, threads=2)
+        assert np.array_equal(r.blocks.view(np.uint8), z["blocks_%d" % q]) and np.array_equal(r.block_txb, z["block_txb_%d" % q])
+        assert np.array_equal(r.txb.view(np.uint8), z["txb_%d" % q]) and np.array_equal(r.coeffs, z["coeffs_%d" % q])
+        for p, k in enumerate("yuv"):
+            assert np.array_equal(r.recon[p], z["recon_%s_%d" % (k, q)])
+        rec, nbytes = O.av1g_recon(w, h, q, r.blocks, r.block_txb, r.txb, r.coeffs)
+        assert nbytes == int(z["obu_bytes_%d" % q])
+        for p in range(3):
+            assert np.array_equal(rec[p], r.recon[p])
+    assert np.any(z["blocks_60"].reshape(-1, 16)[:, 9] == 13)   # uv_mode byte: CfL blocks at the frame edge
+
+
 def test_oracle_thread_independent():
     """The wavefront over host threads gives the same record as one thread."""
     from av1gpu_b200 import synth

@@ -56,3 +56,25 @@ def test_autotune_batch(enc):
     k, ms = enc.autotune_batch([[np.ascontiguousarray(p) for p in im] for im in images], qs)
     assert k in (1, 2, 4) and ms > 0
     enc.set_batch_options(use_graph=False, front_streams=1)
+
+
+def test_batched_workload_slice_equals_one_at_a_time(enc):
+    """A 16-image slice of the batched-form workload: the benchmark's 12 MP image plus crops of smaller 8-bit 4:2:0 and
+    10-bit 4:4:4 pictures (the workload generator with reduced base pictures), mixed qindex.  The batch, captured and
+    replayed as a CUDA graph with 4 front-end streams, gives every image bit for bit its one-at-a-time result."""
+    from av1gpu_b200 import batchbench
+    from av1gpu_b200.isearch import plane_format
+    work = batchbench.workload(15, seed=5, max_mp=2.0, frac10=0.3, base8=(2000, 1500), base10=(1600, 1000))
+    images = [synth.make_image(4000, 3000, 12, edges=True)] + [p for p, _ in work]
+    qs = [120] + [q for _, q in work]
+    assert sum(plane_format(im)[0] == 10 for im in images) >= 2 and images[0][0].size >= 12e6
+    singles = [enc.encode(im, q).digest() for im, q in zip(images, qs)]
+    enc.set_batch_options(use_graph=True, front_streams=4)
+    try:
+        enc.encode_batch(images, qs)                 # captured
+        batch = enc.encode_batch(images, qs)         # replayed
+    finally:
+        enc.set_batch_options(use_graph=False, front_streams=1)
+    for i, (s, b) in enumerate(zip(singles, batch)):
+        assert s == b.digest(), "image %d (%dx%d, q%d) of the batch differs from its one-at-a-time search" % (
+            i, images[i][0].shape[1], images[i][0].shape[0], qs[i])

@@ -1,6 +1,8 @@
 """Whole-path parity of the plain form: the GPU search (C ABI) against the CPU oracle on the same seeded synthetic
 images - analysis records of every shape, DP leaves, every DecisionRecord field, every level - and the GPU
 reconstruction against av1core's av1g_encode() of the GPU's own record.  Bit-exact."""
+import os
+
 import numpy as np
 import pytest
 
@@ -17,10 +19,14 @@ def first_diff(a, b):
     return int(idx[0]) if len(idx) else -1
 
 
-def check_image(enc, w, h, q, seed, edges=False):
-    planes = synth.make_image(w, h, seed, edges=edges)
+def check_image(enc, w, h, q, seed, edges=False, threads=None):
+    return check_planes(enc, synth.make_image(w, h, seed, edges=edges), q, threads)
+
+
+def check_planes(enc, planes, q, threads=None):
+    h, w = planes[0].shape
     g = enc.encode(planes, q)
-    o = O.encode(planes, q)
+    o = O.encode(planes, q, threads=threads)
     # analysis (every shape, every position) and leaves: localise a difference before comparing the record
     for s in SHAPES:
         gJ, gc, gn, gt = enc.debug_analysis(s)
@@ -73,6 +79,23 @@ def test_encode_two_tile_columns(enc):
 def test_encode_edges_qindex(enc, q):
     """The step-edge recipe of the 12 MP workload at its three qindex values (reduced size)."""
     check_image(enc, 640, 384, q, seed=9, edges=True)
+
+
+@pytest.mark.parametrize("q", [60, 120, 200])
+def test_encode_bench_image_full_size(enc, q):
+    """The benchmark's own image at full size (4000x3000 12 MP, seed 12, step edges) at the three qindex values of the
+    12 MP workload: every analysis record, leaf and record field against the oracle (on all host cores), and the
+    reconstruction through av1g_encode."""
+    check_image(enc, 4000, 3000, q, seed=12, edges=True, threads=os.cpu_count())
+
+
+@pytest.mark.parametrize("q", [60, 120, 200])
+def test_encode_reference_gate_picture(enc, q):
+    """The reference's own test picture for CfL at the frame edge (tests/gate_images/cfl_edge_211x149.png, converted
+    by tests/golden/make_gate_fixture.py), against the oracle and av1g_encode."""
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "gate_cfl_edge_211x149.npz"))
+    g, _ = check_planes(enc, (z["y"], z["u"], z["v"]), q)
+    assert np.array_equal(g.coeffs, z["coeffs_%d" % q]) and np.array_equal(g.blocks.view(np.uint8), z["blocks_%d" % q])
 
 
 def test_repeat_deterministic(enc):

@@ -40,3 +40,35 @@ def test_replicas_gloo_world2():
     mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
     assert out[0] == out[1]
     assert sorted(out[0]) == [0, 1, 2, 3, 4]
+
+
+def _worker_own(rank, world, port, out):
+    """Each rank loads only the images assign() gives it; the areas are known beforehand."""
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    shapes = ((64, 96), (128, 32), (8, 8), (200, 100), (16, 16))
+    areas = [h * w for h, w in shapes]
+    mine = set(replicas.assign(areas, world)[rank])
+    images = [(np.full(s, i, np.uint8),) if i in mine else None for i, s in enumerate(shapes)]
+    res = replicas.run(images, lambda i, im: (i, int(im[0].sum())), rank, world, areas=areas)
+    out[rank] = dict(res)
+    dist.destroy_process_group()
+
+
+def test_replicas_gloo_world2_own_images_only():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    manager = mp.Manager()
+    out = manager.dict()
+    mp.spawn(_worker_own, args=(2, port, out), nprocs=2, join=True)
+    assert out[0] == out[1]
+    assert out[0] == {i: (i, i * h * w) for i, (h, w) in enumerate(((64, 96), (128, 32), (8, 8), (200, 100), (16, 16)))}
+
+
+def test_replicas_missing_own_image_raises():
+    import pytest
+    with pytest.raises(ValueError):
+        replicas.run([None, (np.zeros((4, 4), np.uint8),)], lambda i, im: i, 0, 1, areas=[16, 16])
