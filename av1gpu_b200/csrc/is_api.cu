@@ -611,7 +611,7 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
     if (!rc) rc = grow_pinned(h, &h->hCnt, &h->hCntCap, (size_t)n * 4 + 4);
     if (rc) return rc;
     if (h->trace) {
-        const size_t needT = std::max(std::max(slotsG[0], slotsG[1]), std::max(slotsG[2], slotsG[3])) * 4;
+        const size_t needT = std::max(std::max(slotsG[0], slotsG[1]), std::max(slotsG[2], slotsG[3])) * TRACE_STAMPS;
         if (needT > h->traceCap) {
             if (h->traceBuf) cudaFree(h->traceBuf);
             h->traceBuf = nullptr;

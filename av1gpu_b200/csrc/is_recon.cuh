@@ -22,10 +22,17 @@
 
 namespace is {
 
-constexpr int RC_WARPS = 4;                // warps per CTA (independent workers; shared memory bounds the count)
+#ifndef IS_RC_WARPS
+#define IS_RC_WARPS 4
+#endif
+constexpr int RC_WARPS = IS_RC_WARPS;      // warps per CTA (independent workers; shared memory bounds the count)
 // bounded waits (defaults; FrameDesc::waitIters / readyWaitNs carry the values of a run): a wait that runs out records
 // an error and moves on, and once any error is recorded no further wait starts (the host discards the result)
 constexpr int LEAF_WAIT_ITERS = 1 << 20;
+// closed-loop trace (is_set_trace): per queued leaf, globaltimer ns at: 0 slot claimed, 1 slot read, 2 luma prologue
+// done (loads, edges, contexts), 3 luma pass 1 done, 4 pass 2 done, 5 luma published, 6 chroma waits done, 7 chroma
+// screening and RD done, 8 leaf done; 9 the queue entry (image << 32 | sb << 8 | leaf)
+constexpr int TRACE_STAMPS = 10;
 constexpr long long READY_WAIT_NS = 4000000000ll;
 
 template <typename Px, int SS> struct RcWarp {   // SS: chroma subsampling (1 4:2:0, 0 4:4:4)
@@ -33,7 +40,7 @@ template <typename Px, int SS> struct RcWarp {   // SS: chroma subsampling (1 4:
     int16_t q[1024];           // levels of the tasks of a round
     int16_t qb[2][1024];       // best levels (chroma: U, V)
     Px pred[4096];             // predictions of the tasks (W x H per group); the final prediction
-    i64 taskJ[8];
+    i64 taskJ[16];
     int predC[8];
     Px ea[3][EDGE_LEN], el[3][EDGE_LEN];
     __align__(16) Px srcS[3][1024];   // the source of the leaf's tx blocks (Y, U, V) when <= 32 x 32, staged once per
@@ -59,11 +66,20 @@ static_assert(rc_smem_ok<uint8_t, 1>() && rc_smem_ok<uint8_t, 0>() && rc_smem_ok
                   sizeof(FrameDesc) % 16 == 0,
               "the closed loop's shared memory: at most 227 KB, staged sources and descriptors 16-byte aligned");
 
-__device__ __forceinline__ int ld_acquire(const int *p) {
+// Waits poll with relaxed loads and acquire once, with a fence after the awaited value was seen (the acquire pattern of
+// the PTX memory model: a strong read that observes a release, then fence.acq_rel): one acquire per wait instead of one
+// per poll.
+__device__ __forceinline__ int ld_relaxed(const int *p) {
     int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_release(int *p, int v) { asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
 template <typename P> __device__ __forceinline__ P ldcg(const P *p);
 template <> __device__ __forceinline__ uint8_t ldcg<uint8_t>(const uint8_t *p) { return __ldcg(p); }
@@ -290,13 +306,14 @@ static __device__ __noinline__ bool rc_wait(const FrameDesc &F, int sb, int li, 
         if (id < 0) continue;
         const int *flag = F.leafDone + id;
         int it = 0;
-        while (ld_acquire(flag) < level) {
+        while (ld_relaxed(flag) < level) {
             if (++it > F.waitIters || *(volatile int *)F.err) { ok = false; break; }
             __nanosleep(64);
         }
     }
     ok = __all_sync(0xffffffffu, ok);
     if (!ok && lane == 0) atomicCAS(F.err, 0, KERR_WAIT_LEAF);
+    if (ok) fence_acquire();   // every lane: its awaited flags were seen, the neighbours' data may be read now
     __syncwarp();
     return ok;
 }
@@ -505,8 +522,58 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
         for (int k = 0; k < nc; k++) { tcand[n1] = br.cand[k]; ttype[n1] = AV1G_DCT_DCT; n1++; }
         if (br.tx != AV1G_DCT_DCT) { tcand[n1] = br.cand[0]; ttype[n1] = br.tx; n1++; }
         const bool skip1 = n1 == 1;
+        if (trace && lane == 0) trace[2] = gtimer();
+        if (W * H <= 64 && set != AV1G_TX_SET_DCTONLY) {
+            // Small tx sizes (4x4 .. 8x8, 4x16, 16x4; nine leaves in ten): pass 1 and the pass-2 tx types of BOTH possible
+            // pass-1 winners in one round of at most 16 tasks (2 lanes each), then the winner taken in the order of the two
+            // passes - pass 1 in task order, then pass 2 of the pass-1 winner in type order, the first of equal costs -
+            // which is exactly the result of running pass 2 after pass 1.  A round's latency hardly depends on its task
+            // count, so this saves the second round.
+            const int c0 = br.cand[0], c1 = nc >= 2 ? br.cand[1] : br.cand[0];
+            const int tt = lane & 15;   // pass-2 types: lanes 0-15 for the first candidate, 16-31 for the second
+            const bool ok = lane < 16 ? tx_in_set(set, tt) && !(!skip1 && (tt == AV1G_DCT_DCT || tt == br.tx))
+                                      : nc >= 2 && tx_in_set(set, tt) && tt != AV1G_DCT_DCT;
+            const unsigned bal = __ballot_sync(0xffffffffu, ok), m0 = bal & 0xFFFFu, m1 = bal >> 16;
+            const int p1 = skip1 ? 0 : n1, n2a = __popc(m0), n2b = __popc(m1), nt = p1 + n2a + n2b;
+            const int G = nt > 8 ? 2 : nt > 4 ? 4 : 8, grp = lane / G, g = lane & (G - 1);
+            {   // every lane takes part (the evaluation's warp-wide reductions); groups past the last task repeat it
+                const int k = min(grp, nt - 1);
+                int c, ty;
+                if (k < p1) { c = k < nc ? (int)br.cand[k] : c0; ty = k < nc ? AV1G_DCT_DCT : br.tx; }
+                else if (k < p1 + n2a) { c = c0; ty = __fns(m0, 0, k - p1 + 1); }
+                else { c = c1; ty = __fns(m1, 0, k - p1 - n2a + 1); }
+                const int m = cand_mode(c);
+                Px *tp = Wp.pred + grp * (W * H);
+                grp_predict(m, pangle(m, cand_delta(c)), lw, lh, A, L, dcv, tp, g, G);
+                __syncwarp();
+                const EvalIn e{ty, 0, skipCtx, dcCtx, m, F.dcQ, F.acQ, T};
+                const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{src, srcPitch, tp, lw, nullptr}, e, Wp.buf + grp * task_buf_ints(txSz),
+                                                   Wp.q + grp * nq, g, G);
+                if (g == 0 && grp < nt) Wp.taskJ[grp] = o.D + F.lam * (o.R + mbits(c));
+            }
+            __syncwarp();
+            int win = -1;
+            if (!skip1) {
+                for (int k = 0; k < p1; k++)
+                    if (Wp.taskJ[k] < bestJ) { bestJ = Wp.taskJ[k]; bestC = k < nc ? (int)br.cand[k] : c0; bestT = k < nc ? AV1G_DCT_DCT : br.tx; win = k; }
+            } else {
+                bestC = c0; bestT = AV1G_DCT_DCT;
+            }
+            const bool first = bestC == c0;
+            const int base = first ? p1 : p1 + n2a, cnt = first ? n2a : n2b;
+            const unsigned mk = first ? m0 : m1;
+            for (int j = 0; j < cnt; j++)
+                if (Wp.taskJ[base + j] < bestJ) { bestJ = Wp.taskJ[base + j]; bestT = __fns(mk, 0, j + 1); win = base + j; }
+            if (win >= 0) {
+                have = true;
+                for (int i = lane; i < nq; i += 32) best[i] = Wp.q[win * nq + i];
+            }
+            __syncwarp();
+            if (trace && lane == 0) trace[3] = trace[4] = gtimer();
+        } else {
         if (!skip1) run(tcand, ttype, n1);
         else { bestC = br.cand[0]; bestT = AV1G_DCT_DCT; }
+        if (trace && lane == 0) trace[3] = gtimer();
         if (set != AV1G_TX_SET_DCTONLY) {
             const int c1 = bestC;
             const bool isC0 = c1 == br.cand[0];
@@ -517,6 +584,8 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
                 tcand[n2] = c1; ttype[n2] = t; n2++;
             }
             run(tcand, ttype, n2);
+        }
+        if (trace && lane == 0) trace[4] = gtimer();
         }
         // the winner's prediction (whole warp) for its levels (single-candidate case) and the reconstruction
         const int bm = cand_mode(bestC);
@@ -541,7 +610,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
     if (lane == 0) {
         __threadfence();
         st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 1);
-        if (trace) trace[2] = gtimer();
+        if (trace) trace[5] = gtimer();
     }
     {   // the dependents whose last luma dependency this was enter the ready queue
         __threadfence();
@@ -565,6 +634,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
         } else {
             if (!rc_wait(F, sb, li, sbr, sbc, lf.y4 - 1, lf.x4 - 1, lf.x4 + 2 * bw, lf.x4 - 1, lf.y4, lf.y4 + 2 * bh, 1, 2, tC0, tC1, tR0)) return;
         }
+        if (trace && lane == 0) trace[6] = gtimer();
         const int txSz = uv_tx_size(bsize, ss);
         const int W = txw(txSz), H = txh(txSz), lw = 31 - __clz(W), lh = 31 - __clz(H);
         const int cx = (mi_col >> ss) * 4, cy = (mi_row >> ss) * 4, cx4 = cx >> 2, cy4 = cy >> 2;
@@ -772,6 +842,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
             J += F.lam * b;
             if (J < bJ) { bJ = J; bestC = c; }
         }
+        if (trace && lane == 0) trace[7] = gtimer();
         const bool cfl = bestC == 255;
         uv = cfl ? AV1G_UV_CFL_PRED : cand_mode(bestC);
         const int uvType = chroma_tx_type(txSz, uv);
@@ -824,7 +895,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
     if (lane == 0) {
         __threadfence();
         st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 2);
-        if (trace) trace[3] = gtimer();
+        if (trace) trace[8] = gtimer();
     }
 }
 
@@ -870,17 +941,22 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
             } else {
                 const unsigned long long t0 = gtimer();
                 for (;;) {
-                    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(e) : "l"(readyQ + h) : "memory");
+                    e = ld_relaxed64(readyQ + h);
                     if (e || gtimer() - t0 > readyWait || *(volatile int *)err) break;
                     __nanosleep(128);
                 }
                 if (!e) { atomicCAS(err, 0, KERR_WAIT_LEAF); bad = 1; }
-                if (traceBase) { traceBase[(size_t)h * 4] = t0; traceBase[(size_t)h * 4 + 1] = gtimer(); }
+                if (traceBase) {
+                    unsigned long long *tr = traceBase + (size_t)h * TRACE_STAMPS;
+                    tr[0] = t0; tr[1] = gtimer(); tr[9] = e - 1;
+                }
             }
         }
         if (__shfl_sync(0xffffffffu, bad, 0)) break;
         e = __shfl_sync(0xffffffffu, e, 0);
         h = __shfl_sync(0xffffffffu, h, 0);
+        fence_acquire();   // the slot's entry was released by the warp that queued the leaf: its data and that of the
+                           // leaves it waited on are visible from here on
         const unsigned long long v = e - 1;
         const int img = (int)(v >> 32);
         const uint32_t id = (uint32_t)v;
@@ -891,7 +967,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
             cur = img;
         }
         const RateTabs T{F.qctx == 0 ? S.T.cost : S.cost[F.qctx - 1], S.T.scan, S.T.baseCtx};
-        unsigned long long *trace = traceBase ? traceBase + (size_t)h * 4 : nullptr;
+        unsigned long long *trace = traceBase ? traceBase + (size_t)h * TRACE_STAMPS : nullptr;
         rc_leaf<BD, Px, SS>(F, Wp, T, (int)(id >> 8), (int)(id & 255), trace);
     }
 }

@@ -244,7 +244,7 @@ extern "C" int is_probe_int32(int device, double *gops, float *ms) {
     return IS_OK;
 }
 
-// ---- closed-loop trace (debug): per queued leaf the globaltimer at claim, dependencies ready, luma done, done ----
+// ---- closed-loop trace (debug): per queued leaf TRACE_STAMPS values (the phases' globaltimer ns and the queue entry) ----
 extern "C" int is_set_trace(is_handle *h, int on) {
     if (!h) return IS_ERR_INVALID;
     h->trace = on != 0;
@@ -255,7 +255,7 @@ extern "C" int is_get_trace(is_handle *h, unsigned long long *out, size_t cap, u
     uint32_t tot = 0;
     IS_CK(cudaMemcpy(&tot, h->F.leafTotal, 4, cudaMemcpyDeviceToHost));
     *n = tot;
-    const size_t m = std::min(cap, (size_t)tot * 4);
+    const size_t m = std::min(cap, (size_t)tot * TRACE_STAMPS);
     IS_CK(cudaMemcpy(out, h->F.leafTrace, m * 8, cudaMemcpyDeviceToHost));
     return IS_OK;
 }

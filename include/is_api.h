@@ -146,9 +146,10 @@ int is_debug_leaves(is_handle *h, uint32_t sb, uint8_t *bsize, uint8_t *x4, uint
 int is_debug_tables(is_handle *h, int qctx, uint16_t *cost, size_t cap, int32_t *avgY13, int32_t *avgPart50,
                     int32_t *avgSkip0, int qindex, int64_t *lam, int64_t *sqrtlam);
 
-/* Closed-loop trace (debug): is_set_trace(h, 1) before an encode records, per queued leaf, the globaltimer (ns) when a
- * warp claimed it, when its dependencies were ready, when its luma was done and when it was done; is_get_trace copies
- * n x 4 values (queue order). */
+/* Closed-loop trace (debug): is_set_trace(h, 1) before an encode records, per queued leaf (queue order), 10 values:
+ * the globaltimer (ns) when a worker claimed its queue slot, read the slot, finished the luma prologue (loads, edges,
+ * contexts), luma pass 1, luma pass 2, published the luma, finished its chroma waits, the chroma screening and RD, and
+ * the leaf; then the queue entry (image << 32 | sb << 8 | leaf).  is_get_trace copies n x 10 values. */
 int is_set_trace(is_handle *h, int on);
 int is_get_trace(is_handle *h, unsigned long long *out, size_t cap, uint32_t *n);
 
