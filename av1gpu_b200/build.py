@@ -105,6 +105,12 @@ def build_oracle():
     if not REF or not os.path.isdir(REF):
         return None   # the GPU host has no reference checkout: the prebuilt oracle/_ref travels with the tree
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "REF=" + REF], check=True)
+    # the reference's own GPU search (measurement only: the speed bar and its decisions for BD-rate comparisons); a
+    # failure here leaves the comparison out, not the build
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "-f", "refgpu.mk", "REF=" + REF, "-j%d" % (os.cpu_count() or 1)],
+                       capture_output=True, text=True)
+    if r.returncode:
+        print("note: the reference GPU search was not built (oracle/refgpu.mk):", (r.stderr or r.stdout)[-400:], file=sys.stderr)
     return os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
 
 

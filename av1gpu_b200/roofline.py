@@ -1,4 +1,4 @@
-"""Roofline of the intra search on B200 and the CPU baseline leg of bench.py.
+"""Roofline of the intra search on B200 (the roofline object of bench.py's JSON line).
 
 The search is integer work (prediction, 4x4 Hadamard SATD, butterfly transforms, quantisation, context-coded rates):
 its bound is the INT32 issue rate, not the tensor cores and not HBM (≈6.4 algorithmic bytes per pixel).  The
@@ -7,8 +7,6 @@ search does (oracle/count_ops.py, cost model in oracle/plain_search.cpp) - froze
 image; the denominator is the INT32 instruction rate measured on the device (is_probe_int32).
 """
 import os
-import sys
-import time
 
 # oracle/count_ops.py on the 4000x3000 seeded step-edge image (seed 12): ops per pixel (analysis, closed loop)
 OPS_PER_PX = {120: (16456.9, 830.3), 60: (18144.3, 984.0), 200: (14254.3, 669.4)}
@@ -51,35 +49,4 @@ def report(enc, stage_ms, mp, qindex=120, device=0):
                             for k, v in stages.items()},
            "hbm": {"achieved_gbs": round(hbm_gbs, 1), "peak_gbs": hbm_peak, "frac": round(hbm_gbs / hbm_peak, 5),
                    "peak_source": hbm_kind + " (MEASURED_PEAKS.json hbm_gbs)"}}
-    return out
-
-
-def cpu_baseline(planes, qindex, crop=(2000, 1500), min_seconds=10.0):
-    """The CPU oracle (the same search in integer C++) on all host cores, on a bounded crop of the workload."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
-    import oracle as O
-    cw, ch = crop
-    sub = [np.ascontiguousarray(planes[0][:ch, :cw]), np.ascontiguousarray(planes[1][:ch // 2, :cw // 2]),
-           np.ascontiguousarray(planes[2][:ch // 2, :cw // 2])]
-    threads = os.cpu_count() or 1
-    n, t0 = 0, time.perf_counter()
-    while n == 0 or time.perf_counter() - t0 < min_seconds:   # repeated searches: a sample of about 10 s
-        O.encode(sub, qindex, threads=threads)
-        n += 1
-    dt = (time.perf_counter() - t0) / n
-    out = {"value": round(cw * ch / 1e6 / dt, 4), "unit": "MP/s", "cores": threads, "kind": "port",
-           "sample": "%dx%d crop of the 12 MP image, %d searches, %.2f s each" % (cw, ch, n, dt)}
-    # beside it, on the same crop: the reference's own CPU decision engine (a simpler search, at most 4 decide threads)
-    # and av1core's av1g_encode of the oracle's record (entropy coding and reconstruction, outside the search)
-    try:
-        dec, enc = O.ref_engine_seconds(sub, qindex)
-        r = O.encode(sub, qindex, threads=threads)
-        t1 = time.perf_counter()
-        O.av1g_recon(cw, ch, qindex, r.blocks, r.block_txb, r.txb, r.coeffs)
-        out["reference_cpu_engine"] = {"decide_s": round(dec, 3), "encode_s": round(enc, 3),
-                                       "mp_per_s": round(cw * ch / 1e6 / max(dec, 1e-9), 3)}
-        out["av1g_encode_s"] = round(time.perf_counter() - t1, 3)
-    except (RuntimeError, OSError) as ex:
-        out["reference_cpu_engine"] = {"error": str(ex)[:120]}
     return out

@@ -93,6 +93,65 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(planes, qindex, crop=(2000, 1500), min_seconds=10.0):
+    """The CPU oracle (the same search in integer C++) on all host cores, on a bounded crop of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cw, ch = crop
+    sub = [np.ascontiguousarray(planes[0][:ch, :cw]), np.ascontiguousarray(planes[1][:ch // 2, :cw // 2]),
+           np.ascontiguousarray(planes[2][:ch // 2, :cw // 2])]
+    threads = os.cpu_count() or 1
+    n, t0 = 0, time.perf_counter()
+    while n == 0 or time.perf_counter() - t0 < min_seconds:   # repeated searches: a sample of about 10 s
+        O.encode(sub, qindex, threads=threads)
+        n += 1
+    dt = (time.perf_counter() - t0) / n
+    out = {"value": round(cw * ch / 1e6 / dt, 4), "unit": "MP/s", "cores": threads, "cpu_model": _cpu_model(), "kind": "port",
+           "sample": "%dx%d crop of the 12 MP image, %d searches, %.2f s each" % (cw, ch, n, dt)}
+    # beside it, on the same crop: the reference's own CPU decision engine (a simpler search, at most 4 decide threads)
+    # and av1core's av1g_encode of the oracle's record (entropy coding and reconstruction, outside the search)
+    try:
+        dec, enc = O.ref_engine_seconds(sub, qindex)
+        r = O.encode(sub, qindex, threads=threads)
+        t1 = time.perf_counter()
+        O.av1g_recon(cw, ch, qindex, r.blocks, r.block_txb, r.txb, r.coeffs)
+        out["reference_cpu_engine"] = {"decide_s": round(dec, 3), "encode_s": round(enc, 3),
+                                       "mp_per_s": round(cw * ch / 1e6 / max(dec, 1e-9), 3)}
+        out["av1g_encode_s"] = round(time.perf_counter() - t1, 3)
+    except (RuntimeError, OSError) as ex:
+        out["reference_cpu_engine"] = {"error": str(ex)[:120]}
+    return out
+
+
+def reference_gpu(planes, qindex, warmup=2, reps=5):
+    """The reference's own GPU search (maddog107/av1gpu GpEncoder::encode, plain knob set, built for sm_100 from its
+    sources by oracle/refgpu.mk) on the same image on this GPU: search time = its GpTimes setup + analysis + DP + closed
+    loop + pack (inputs on the device, record download excluded), the last of reps runs; None when not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_gpu
+    if not ref_gpu.available():
+        return None
+    ref_gpu.search(planes, qindex, reps=warmup, record=False)
+    ts = [ref_gpu.search(planes, qindex, reps=1, record=False) for _ in range(reps)]
+    ms = float(np.median([t.search_ms for t in ts]))
+    h, w = planes[0].shape
+    return {"value": round(w * h / 1e6 / (ms / 1e3), 3), "unit": "MP/s", "ms_per_search": round(ms, 2),
+            "stage_ms": {k: round(float(np.median([t.times[k] for t in ts])), 2) for k in ts[0].times},
+            "build": "reference sources for sm_100 (oracle/refgpu.mk), plain knob set, palette off",
+            "timing": "GpTimes CUDA events, median of %d runs after %d warm-up" % (reps, warmup)}
+
+
 def cpu_reference(args, planes, rank):
     """The CPU arm: the oracle (integer restatement of the reference's search) on all host cores, bounded crops."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -115,7 +174,7 @@ def cpu_reference(args, planes, rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic", "impl": "reference",
             "config": {"workload": "plain intra RD search, 4000x3000 8-bit 4:2:0 synthetic, qindex %d" % args.qindex,
                        "sample": "2000x1500 crop of the same image per step", "parallelism": "cpu threads"},
-            "cpu_baseline": {"value": round(mps, 4), "unit": "MP/s", "cores": threads, "kind": "port",
+            "cpu_baseline": {"value": round(mps, 4), "unit": "MP/s", "cores": threads, "cpu_model": _cpu_model(), "kind": "port",
                              "sample": "2000x1500 crop (3 MP) of the 12 MP image, %d steps" % args.steps},
             "e2e": {"value": round(mps, 4), "unit": "MP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -220,7 +279,13 @@ def main():
                 "clocks": clk.summary()}
         line["roofline"] = roofline.report(enc, kernel_ms, mp)
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = roofline.cpu_baseline(planes, args.qindex)
+            line["cpu_baseline"] = cpu_baseline(planes, args.qindex)
+            try:
+                rg = reference_gpu(planes, args.qindex)
+            except (RuntimeError, OSError) as ex:
+                rg = {"error": str(ex)[:160]}
+            if rg is not None:
+                line["reference_gpu"] = rg
         print(json.dumps(line), flush=True)
     enc.close()
     if world > 1:
