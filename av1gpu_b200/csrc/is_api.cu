@@ -255,6 +255,7 @@ struct is_handle {
     int slVersion = 0;
     std::string graphKey;
     cudaGraphExec_t graphExec = nullptr;
+    struct ServeSession *serve = nullptr;   // an open serving session (is_serve_open), or null
     int setErr(int code, const char *fmt, ...) {
         char b[512];
         va_list ap;
@@ -485,6 +486,7 @@ int is_create(const is_params *p, is_handle **out) {
 void is_destroy(is_handle *h) {
     if (!h) return;
     cudaSetDevice(h->device);
+    if (h->serve) is_serve_close(h);
     if (h->own) cudaStreamSynchronize(h->own);
     if (h->arena) cudaFree(h->arena);
     for (auto &e : h->ev)
@@ -648,6 +650,7 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         // the image's format group: its ready queue and counters; img indexes the group's descriptors
         F.readyQ = (unsigned long long *)(base + offQG[grp[i]]);
         F.rq = h->bRq + 2 * grp[i];
+        F.readyCap = (uint32_t)slotsG[grp[i]];
         F.err = h->bErr;
         F.img = h->bPos[i] - h->bGrpStart[grp[i]];
         F.leafTrace = (h->trace && i == 0 && F.img == 0) ? h->traceBuf : nullptr;   // image 0, when its group's first
@@ -662,6 +665,50 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         h->bQ[i] = f->qindex;
     }
     h->bN = n;
+    return IS_OK;
+}
+
+// The front end of one image on stream s: its planes into the padded workspace, the learned shortlist's mode masks
+// (with a model set; chunk buffers k), the analysis, the DP, the leaf maps and the dataflow graph, whose first ready
+// leaves go to the image's ready queue.  ev1 / ev2 (optional) are recorded after the upload and after the analysis.
+static int front_end(is_handle *h, const FrameDesc &F, const is_frame *f, int nSb, bool fromHost, cudaStream_t s, int k, cudaEvent_t ev1,
+                     cudaEvent_t ev2) {
+    const size_t px = F.bd > 8 ? 2 : 1;
+    for (int p = 0; p < 3; p++) {
+        const int ss = p ? F.ssx : 0;
+        const int vw = (f->width + ss) >> ss, vh = (f->height + ss) >> ss;
+        uint8_t *dst = const_cast<uint8_t *>(F.src[p]);
+        IS_CK(cudaMemcpy2DAsync(dst, F.spitch[p] * px, f->planes[p], (size_t)f->pitch[p] * px, vw * px, vh,
+                                fromHost ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+        const int pw = ((F.sbCols + 1) * 64) >> ss, ph = (F.sbRows * 64) >> ss;
+        if (px == 1) k_pad<uint8_t><<<dim3(1, ph), 128, 0, s>>>(dst, F.spitch[p], vw, vh, pw, ph);
+        else k_pad<uint16_t><<<dim3(1, ph), 128, 0, s>>>((uint16_t *)dst, F.spitch[p], vw, vh, pw, ph);
+    }
+    if (ev1) IS_CK(cudaEventRecord(ev1, s));
+    if (h->slOn) {   // the learned shortlist: scores of every analysis record, then its mode mask
+        for (uint32_t i0 = 0; i0 < F.nRec; i0 += SL_CHUNK) {
+            const int cn = (int)std::min<uint32_t>(SL_CHUNK, F.nRec - i0);
+            k_sl_features_rec<<<(cn + 7) / 8, 256, 0, s>>>(F, i0, cn, h->slX[k]);
+            k_gemm_abt<<<dim3((SL_HID + GT_N - 1) / GT_N, (cn + GT_M - 1) / GT_M), 128, 0, s>>>(
+                cn, SL_HID, SL_IN, h->slX[k], SL_IN, h->slW1, SL_IN, nullptr, 0, h->slB1, 1, h->slH[k], SL_HID);
+            k_gemm_abt<<<dim3(1, (cn + GT_M - 1) / GT_M), 128, 0, s>>>(cn, SL_OUT, SL_HID, h->slH[k], SL_HID, h->slW2, SL_HID,
+                                                                      h->slS[k], SL_OUT, h->slB2, 0, nullptr, 0);
+            k_sl_mask<<<(cn + 127) / 128, 128, 0, s>>>(cn, h->slS[k], h->slTau, h->slMax, h->slConf, F.slMask + i0);
+        }
+        IS_CK(cudaGetLastError());
+    }
+    IS_CK((F.bd == 8 ? an_launch<8, 0>(F, nSb, s) : an_launch<10, 0>(F, nSb, s)));
+    IS_CK((F.bd == 8 ? an_launch<8, 1>(F, nSb, s) : an_launch<10, 1>(F, nSb, s)));
+    IS_CK(cudaGetLastError());
+    if (ev2) IS_CK(cudaEventRecord(ev2, s));
+    k_dp<<<(nSb + DP_WARPS - 1) / DP_WARPS, DP_WARPS * 32, 0, s>>>(F, nSb);
+    k_leaf_prep<<<nSb, 256, 0, s>>>(F, nSb);
+    k_leaf_queue_scan<<<1, 1024, 0, s>>>(F, nSb);
+    k_leaf_deps<0><<<nSb, 256, 0, s>>>(F, nSb);
+    k_leaf_deps<1><<<nSb, 256, 0, s>>>(F, nSb);
+    k_leaf_deps<2><<<nSb, 256, 0, s>>>(F, nSb);
+    k_leaf_deps<3><<<nSb, 256, 0, s>>>(F, nSb);
+    IS_CK(cudaGetLastError());
     return IS_OK;
 }
 
@@ -694,46 +741,10 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
         for (int k = 0; k < K; k++) IS_CK(cudaStreamWaitEvent(h->aux[k], h->evFork, 0));
     }
     for (int i = 0; i < n; i++) {
-        const FrameDesc &F = h->bF[i];
-        const is_frame *f = fr + i;
-        const int nSb = h->bNsb[i];
         cudaStream_t s = K > 1 ? h->aux[i % K] : st;
-        const size_t px = F.bd > 8 ? 2 : 1;
-        for (int p = 0; p < 3; p++) {
-            const int ss = p ? F.ssx : 0;
-            const int vw = (f->width + ss) >> ss, vh = (f->height + ss) >> ss;
-            uint8_t *dst = const_cast<uint8_t *>(F.src[p]);
-            IS_CK(cudaMemcpy2DAsync(dst, F.spitch[p] * px, f->planes[p], (size_t)f->pitch[p] * px, vw * px, vh,
-                                    fromHost ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
-            const int pw = ((F.sbCols + 1) * 64) >> ss, ph = (F.sbRows * 64) >> ss;
-            if (px == 1) k_pad<uint8_t><<<dim3(1, ph), 128, 0, s>>>(dst, F.spitch[p], vw, vh, pw, ph);
-            else k_pad<uint16_t><<<dim3(1, ph), 128, 0, s>>>((uint16_t *)dst, F.spitch[p], vw, vh, pw, ph);
-        }
-        if (events && n == 1) IS_CK(cudaEventRecord(h->ev[1], s));
-        if (h->slOn) {   // the learned shortlist: scores of every analysis record, then its mode mask
-            const int k = K > 1 ? i % K : 0;
-            for (uint32_t i0 = 0; i0 < F.nRec; i0 += SL_CHUNK) {
-                const int cn = (int)std::min<uint32_t>(SL_CHUNK, F.nRec - i0);
-                k_sl_features_rec<<<(cn + 7) / 8, 256, 0, s>>>(F, i0, cn, h->slX[k]);
-                k_gemm_abt<<<dim3((SL_HID + GT_N - 1) / GT_N, (cn + GT_M - 1) / GT_M), 128, 0, s>>>(
-                    cn, SL_HID, SL_IN, h->slX[k], SL_IN, h->slW1, SL_IN, nullptr, 0, h->slB1, 1, h->slH[k], SL_HID);
-                k_gemm_abt<<<dim3(1, (cn + GT_M - 1) / GT_M), 128, 0, s>>>(cn, SL_OUT, SL_HID, h->slH[k], SL_HID, h->slW2, SL_HID,
-                                                                          h->slS[k], SL_OUT, h->slB2, 0, nullptr, 0);
-                k_sl_mask<<<(cn + 127) / 128, 128, 0, s>>>(cn, h->slS[k], h->slTau, h->slMax, h->slConf, F.slMask + i0);
-            }
-            IS_CK(cudaGetLastError());
-        }
-        IS_CK((F.bd == 8 ? an_launch<8, 0>(F, nSb, s) : an_launch<10, 0>(F, nSb, s)));
-        IS_CK((F.bd == 8 ? an_launch<8, 1>(F, nSb, s) : an_launch<10, 1>(F, nSb, s)));
-        IS_CK(cudaGetLastError());
-        if (events && n == 1) IS_CK(cudaEventRecord(h->ev[2], s));
-        k_dp<<<(nSb + DP_WARPS - 1) / DP_WARPS, DP_WARPS * 32, 0, s>>>(F, nSb);
-        k_leaf_prep<<<nSb, 256, 0, s>>>(F, nSb);
-        k_leaf_queue_scan<<<1, 1024, 0, s>>>(F, nSb);
-        k_leaf_deps<0><<<nSb, 256, 0, s>>>(F, nSb);
-        k_leaf_deps<1><<<nSb, 256, 0, s>>>(F, nSb);
-        k_leaf_deps<2><<<nSb, 256, 0, s>>>(F, nSb);
-        IS_CK(cudaGetLastError());
+        const int rc = front_end(h, h->bF[i], fr + i, h->bNsb[i], fromHost, s, K > 1 ? i % K : 0, (events && n == 1) ? h->ev[1] : nullptr,
+                                 (events && n == 1) ? h->ev[2] : nullptr);
+        if (rc) return rc;
     }
     if (K > 1) {
         for (int k = 0; k < K; k++) {
@@ -749,8 +760,18 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
         const int grid = h->reconCtas > 0 && h->reconCtas < h->rcGridG[g] ? h->reconCtas : h->rcGridG[g];
         const FrameDesc *fs = h->dFs + h->bGrpStart[g];
         const size_t sm = h->smemRcG[g];
-        IS_CK((g == 0 ? rc_launch<8, 1>(fs, gn, grid, sm, st) : g == 1 ? rc_launch<8, 0>(fs, gn, grid, sm, st)
-               : g == 2 ? rc_launch<10, 1>(fs, gn, grid, sm, st) : rc_launch<10, 0>(fs, gn, grid, sm, st)));
+        const FrameDesc &F0 = h->hFs[h->bGrpStart[g]];   // the group's first image: its queue, counters and trace
+        RcCtl ctl;
+        ctl.rq = F0.rq;
+        ctl.readyQ = F0.readyQ;
+        ctl.err = F0.err;
+        ctl.serving = 0;
+        ctl.cap = F0.readyCap;
+        ctl.readyWaitNs = (unsigned long long)h->readyWaitNs;
+        ctl.trace = F0.leafTrace;
+        ctl.poison = h->poison ? 1 : 0;
+        IS_CK((g == 0 ? rc_launch<8, 1>(fs, gn, ctl, grid, sm, st) : g == 1 ? rc_launch<8, 0>(fs, gn, ctl, grid, sm, st)
+               : g == 2 ? rc_launch<10, 1>(fs, gn, ctl, grid, sm, st) : rc_launch<10, 0>(fs, gn, ctl, grid, sm, st)));
     }
     if (events) IS_CK(cudaEventRecord(h->ev[4], st));
     for (int i = 0; i < n; i++) {
@@ -1041,6 +1062,7 @@ int is_times_get(const is_handle *h, is_times *t) {
 
 }  // extern "C"
 
+#include "is_serve.cuh"
 #include "is_testapi.cuh"
 #include "is_noalloc.cuh"
 #include "is_learn_api.cuh"

@@ -68,7 +68,12 @@ struct __align__(16) FrameDesc {
     // leaves became ready (0: slot not written yet); rq[0] next slot to take, rq[1] next slot to write
     unsigned long long *readyQ;
     int *rq;
-    int img;                                  // index of the image in its batch
+    uint32_t readyCap;                        // positions of readyQ
+    int img;                                  // the image's tag in the ready queue: its index in the descriptor array
+                                              // (low 16 bits) and, in a serving session, the generation of its slot
+    int *leafDoneCnt;                         // serving: leaves of the image finished (null in a batch)
+    volatile int *doneFlag;                   // serving: host-mapped word of the image's slot, set to img once its last
+                                              // leaf is done (null in a batch)
     int *depCnt;                              // [nSb * 256] luma dependencies of each leaf not yet published
     int *revCnt, *revFill;                    // [nSb * 256] dependents of each leaf; entries written so far
     uint32_t *revOff;                         // [nSb * 256] first entry of each leaf's dependents in revList

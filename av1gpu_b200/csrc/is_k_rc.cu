@@ -21,9 +21,11 @@ template <> cudaError_t rc_setup<IS_BD, IS_SS>(size_t *smem, int *ctasPerSm) {
     return e;
 }
 
-// a cooperative launch (all CTAs resident: their warps wait on each other's leaves), expressed with launch attributes
-// so that it can be captured in a graph
-template <> cudaError_t rc_launch<IS_BD, IS_SS>(const FrameDesc *fs, int nImg, int grid, size_t smem, cudaStream_t st) {
+// A batch's loop is a cooperative launch (all CTAs resident at once), expressed with launch attributes so that it can be
+// captured in a graph.  A serving session's loop is a plain launch: it runs next to other loops and front ends, and it
+// needs no co-residency - a queue slot is only ever claimed by a warp that is running, and every wait is on a leaf that a
+// running warp holds.
+template <> cudaError_t rc_launch<IS_BD, IS_SS>(const FrameDesc *fs, int nImg, const RcCtl &ctl, int grid, size_t smem, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(RC_WARPS * 32);
@@ -33,8 +35,8 @@ template <> cudaError_t rc_launch<IS_BD, IS_SS>(const FrameDesc *fs, int nImg, i
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_recon<IS_BD, IS_SS>, fs, nImg);
+    cfg.numAttrs = ctl.serving ? 0 : 1;
+    return cudaLaunchKernelEx(&cfg, k_recon<IS_BD, IS_SS>, fs, nImg, ctl);
 }
 
 }  // namespace is

@@ -257,17 +257,18 @@ __device__ __forceinline__ void rc_txb_ctx(const FrameDesc &F, int plane, int tx
 }
 
 // a block of H rows of W bytes (<= 64; a W x H <= 32 x 32 block of samples) at src (row pitch in bytes) into dst (row
-// stride W bytes), vector loads of up to 16 bytes (rows and the block's first byte are aligned to its width)
+// stride W bytes), vector loads of up to 16 bytes (rows and the block's first byte are aligned to its width).  Coherent
+// L2 loads, not the read-only path: a serving session's loop runs while new images are written into reused memory.
 __device__ __forceinline__ void stage_block(const uint8_t *src, int pitch, int W, int H, uint8_t *dst) {
     const int lane = lane_id();
     if (W >= 16) {
         const int v = W >> 4;
         for (int k = lane; k < v * H; k += 32)
-            reinterpret_cast<uint4 *>(dst)[k] = __ldg(reinterpret_cast<const uint4 *>(src + (size_t)(k / v) * pitch) + (k % v));
+            reinterpret_cast<uint4 *>(dst)[k] = __ldcg(reinterpret_cast<const uint4 *>(src + (size_t)(k / v) * pitch) + (k % v));
     } else if (W == 8) {
-        for (int k = lane; k < H; k += 32) reinterpret_cast<uint2 *>(dst)[k] = __ldg(reinterpret_cast<const uint2 *>(src + (size_t)k * pitch));
+        for (int k = lane; k < H; k += 32) reinterpret_cast<uint2 *>(dst)[k] = __ldcg(reinterpret_cast<const uint2 *>(src + (size_t)k * pitch));
     } else {
-        for (int k = lane; k < H; k += 32) reinterpret_cast<uint32_t *>(dst)[k] = __ldg(reinterpret_cast<const uint32_t *>(src + (size_t)k * pitch));
+        for (int k = lane; k < H; k += 32) reinterpret_cast<uint32_t *>(dst)[k] = __ldcg(reinterpret_cast<const uint32_t *>(src + (size_t)k * pitch));
     }
 }
 
@@ -326,11 +327,21 @@ __device__ __forceinline__ void tile_box(const FrameDesc &F, int mi_row, int mi_
     tC0 = F.tileColStart[tc]; tC1 = F.tileColStart[tc + 1]; tR0 = F.tileRowStart[tr]; tR1 = F.tileRowStart[tr + 1];
 }
 
-// append leaf id (sb << 8 | leaf) of the image to the batch's ready queue
+// A queue slot given up by an idle worker of a serving session (the worker claimed it and left before a leaf came).
+constexpr unsigned long long SLOT_ABANDONED = ~0ull;
+// append leaf id (sb << 8 | leaf) of the image to the ready queue, after a fence that releases everything this thread
+// wrote before (a running loop may take the leaf at once); a slot that an idle serving worker abandoned is skipped
 __device__ __forceinline__ void push_ready(const FrameDesc &F, uint32_t id) {
-    const int pos = atomicAdd(F.rq + 1, 1);
     const unsigned long long v = 1ull + (((unsigned long long)F.img << 32) | id);
-    asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(F.readyQ + pos), "l"(v) : "memory");
+    __threadfence();
+    for (;;) {
+        const int pos = atomicAdd(F.rq + 1, 1);
+        if ((uint32_t)pos >= F.readyCap) {   // the queue's positions are used up: the image cannot complete
+            atomicCAS(F.err, 0, KERR_CAPACITY);
+            return;
+        }
+        if (atomicCAS(F.readyQ + pos, 0ull, v) == 0ull) break;
+    }
 }
 
 // The further chroma tx blocks of plane pl of a 4:4:4 block with a 64-sample side (2 or 4 per plane in raster order;
@@ -896,22 +907,41 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
         __threadfence();
         st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 2);
         if (trace) trace[8] = gtimer();
+        // serving session: the image's last leaf tells the host (its record can be packed while others run on)
+        if (F.leafDoneCnt && atomicAdd(F.leafDoneCnt, 1) + 1 == (int)*F.leafTotal) {
+            __threadfence_system();
+            *F.doneFlag = F.img;
+        }
     }
 }
 
-// Persistent grid of independent warps over the ready queue of a batch of nImg images of one format (Fs: their
-// descriptors in device memory; one instance per bit depth BD and chroma subsampling SS, a batch's images run in groups
-// of one format): a warp takes the next slot, waits until a leaf has been written there (bounded in time), brings the
-// descriptor of the leaf's image into its shared copy when the image changes, and runs the leaf.
+// Persistent grid of independent warps over a ready queue (one instance per bit depth BD and chroma subsampling SS):
+// a warp takes the next slot, waits until a leaf has been written there (bounded in time), brings the descriptor of the
+// leaf's image into its shared copy when the image changes, and runs the leaf.  Two modes:
+//   batch    the nImg images of Fs (one format group of a batch): the loop ends once every leaf of them is taken;
+//   serving  (ctl.serving) images keep arriving: each submitted image's front end writes its descriptor into the table
+//            Fs and pushes its first ready leaves into the same queue while the loop runs.  A warp that finds no leaf in
+//            its slot for readyWaitNs gives the slot up and leaves: the loop ends when it is idle, and the host launches it
+//            again once an image's front end has queued leaves (the queue counters carry on).
+struct RcCtl {
+    int *rq;                       // [0] next slot to take, [1] next slot to write
+    const unsigned long long *readyQ;      // (serving: idle workers write SLOT_ABANDONED into their slots)
+    int *err;
+    int serving;                   // a serving session's loop (else a batch's)
+    uint32_t cap;                  // positions of readyQ
+    unsigned long long readyWaitNs;
+    unsigned long long *trace;     // optional leaf trace (batch mode)
+    int poison;
+};
 template <int BD, int SS>
-__global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__restrict__ Fs, int nImg) {
+__global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *Fs, int nImg, const RcCtl ctl) {
     typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RcSmem<Px, SS> &S = *reinterpret_cast<RcSmem<Px, SS> *>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = lane_id();
     RcWarp<Px, SS> &Wp = S.w[warp];
     FrameDesc &F = S.F[warp];
-    if (Fs[0].poison) {
+    if (ctl.poison) {
         smem_poison(smem_raw, sizeof(RcSmem<Px, SS>), threadIdx.x, blockDim.x);
         __syncthreads();
     }
@@ -923,19 +953,43 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
         }
     }
     __syncthreads();
-    const int *rq = Fs[0].rq;
-    const unsigned long long *readyQ = Fs[0].readyQ;
-    int *err = Fs[0].err;
-    const unsigned long long readyWait = (unsigned long long)Fs[0].readyWaitNs;
-    unsigned long long *traceBase = Fs[0].leafTrace;
-    int total = 0;
-    for (int i = 0; i < nImg; i++) total += (int)*Fs[i].leafTotal;
+    int *rq = ctl.rq;
+    const unsigned long long *readyQ = ctl.readyQ;
+    int *err = ctl.err;
+    const unsigned long long readyWait = ctl.readyWaitNs;
+    unsigned long long *traceBase = ctl.trace;
+    const bool serving = ctl.serving != 0;
+    int total = 0x7FFFFFFF;
+    if (!serving) {
+        total = 0;
+        for (int i = 0; i < nImg; i++) total += (int)*Fs[i].leafTotal;
+    }
     int cur = -1;
     for (;;) {
         unsigned long long e = 0;
         int h = 0, bad = 0;
-        if (lane == 0) {
-            h = atomicAdd(const_cast<int *>(rq), 1);
+        if (lane == 0 && serving) {
+            // serving: a ticket of its own (no two workers poll one word); a worker that finds no leaf in its slot for
+            // readyWait - or sees the stop word - gives the slot up (a producer that comes later skips it) and leaves, so
+            // the loop ends when idle (the host launches it again while images are in it; the counters carry on)
+            h = atomicAdd(rq, 1);
+            const unsigned long long t0 = gtimer();
+            if ((uint32_t)h >= ctl.cap) {   // no position left: nothing more can come
+                bad = 1;
+            } else {
+                for (;;) {
+                    e = ld_relaxed64(readyQ + h);
+                    if (e) break;
+                    if (*(volatile int *)err || gtimer() - t0 > readyWait) {
+                        e = atomicCAS(const_cast<unsigned long long *>(readyQ) + h, 0ull, SLOT_ABANDONED);
+                        if (!e) bad = 1;   // given up; otherwise a leaf came just now: take it
+                        break;
+                    }
+                    __nanosleep(128);
+                }
+            }
+        } else if (lane == 0) {
+            h = atomicAdd(rq, 1);
             if (h >= total) {
                 bad = 1;
             } else {
@@ -945,7 +999,10 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
                     if (e || gtimer() - t0 > readyWait || *(volatile int *)err) break;
                     __nanosleep(128);
                 }
-                if (!e) { atomicCAS(err, 0, KERR_WAIT_LEAF); bad = 1; }
+                if (!e) {
+                    atomicCAS(err, 0, KERR_WAIT_LEAF);
+                    bad = 1;
+                }
                 if (traceBase) {
                     unsigned long long *tr = traceBase + (size_t)h * TRACE_STAMPS;
                     tr[0] = t0; tr[1] = gtimer(); tr[9] = e - 1;
@@ -960,9 +1017,10 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *__r
         const unsigned long long v = e - 1;
         const int img = (int)(v >> 32);
         const uint32_t id = (uint32_t)v;
-        if (img != cur) {   // the descriptor of the leaf's image into the warp's shared copy
-            const uint4 *src = reinterpret_cast<const uint4 *>(Fs + img);
-            for (int k = lane; k < (int)(sizeof(FrameDesc) / 16); k += 32) reinterpret_cast<uint4 *>(&F)[k] = src[k];
+        if (img != cur) {   // the descriptor of the leaf's image into the warp's shared copy (tags differ per slot use);
+                            // coherent loads: a serving session rewrites table slots while its loop runs
+            const uint4 *src = reinterpret_cast<const uint4 *>(Fs + (img & 0xFFFF));
+            for (int k = lane; k < (int)(sizeof(FrameDesc) / 16); k += 32) reinterpret_cast<uint4 *>(&F)[k] = __ldcg(src + k);
             __syncwarp();
             cur = img;
         }

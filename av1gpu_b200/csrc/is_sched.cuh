@@ -111,9 +111,10 @@ __global__ void k_leaf_queue_scan(const __grid_constant__ FrameDesc F, int nSb) 
     }
     if (tid == 1023) *F.leafTotal = sN[1023];
 }
-// The dataflow graph of the closed loop, one thread per leaf, in three passes: 0 counts each leaf's luma dependencies
-// and its dependents, 1 gives each leaf its range of revList and queues the leaves without dependencies, 2 writes the
-// dependents.
+// The dataflow graph of the closed loop, one thread per leaf, in four passes: 0 counts each leaf's luma dependencies
+// and its dependents, 1 gives each leaf its range of revList, 2 writes the dependents, 3 queues the leaves without
+// dependencies.  The queueing comes last so that a closed loop already running (a serving session) never takes a leaf
+// whose dependents list is not written yet.
 template <int PASS>
 __global__ void k_leaf_deps(const __grid_constant__ FrameDesc F, int nSb) {
     const int sb = blockIdx.x, tid = threadIdx.x;
@@ -124,6 +125,9 @@ __global__ void k_leaf_deps(const __grid_constant__ FrameDesc F, int nSb) {
         const uint32_t off = (uint32_t)atomicAdd(F.queue + 2, F.revCnt[me]);
         F.revOff[me] = off;
         if (off + (uint32_t)F.revCnt[me] > cap) atomicCAS(F.err, 0, KERR_CAPACITY);
+        return;
+    }
+    if (PASS == 3) {
         if (F.depCnt[me] == 0) push_ready(F, me);
         return;
     }

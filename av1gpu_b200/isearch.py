@@ -24,8 +24,8 @@ TXB_DT = np.dtype([("coeff_off", "<u4"), ("x4", "<u2"), ("y4", "<u2"), ("plane",
                    ("tx_type", "u1"), ("flags", "u1"), ("eob", "<u2"), ("reserved", "<u2")])
 
 IS_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "wavefront wait timeout",
-             -5: "no result", -6: "too large for the static scratch"}
-IS_ERR_INVALID, IS_ERR_CUDA, IS_ERR_OOM, IS_ERR_TIMEOUT, IS_ERR_STATE, IS_ERR_TOO_LARGE = -1, -2, -3, -4, -5, -6
+             -5: "no result", -6: "too large for the static scratch", -7: "serving session busy"}
+IS_ERR_INVALID, IS_ERR_CUDA, IS_ERR_OOM, IS_ERR_TIMEOUT, IS_ERR_STATE, IS_ERR_TOO_LARGE, IS_ERR_BUSY = -1, -2, -3, -4, -5, -6, -7
 
 
 class IsError(RuntimeError):
@@ -57,7 +57,8 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_fwd_quant_static", "is_encode_batch", "is_batch_counts", "is_batch_copy", "is_set_batch_options",
            "is_autotune_batch", "is_workspace_bytes", "is_workspace_bytes_format", "is_sl_create", "is_sl_destroy", "is_sl_set_weights",
            "is_sl_get_weights", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset", "is_set_shortlist_model",
-           "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison"]
+           "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison", "is_serve_open", "is_serve_start", "is_serve_submit", "is_serve_poll",
+           "is_serve_counts", "is_serve_copy", "is_serve_stop", "is_serve_close"]
 
 _lib = None
 
@@ -114,6 +115,14 @@ def load_library():
     L.is_set_wait_limits.argtypes = [vp, C.c_int, C.c_longlong]
     L.is_set_workspace_limit.argtypes = [vp, C.c_uint64]
     L.is_set_poison.argtypes = [vp, C.c_int]
+    L.is_serve_open.argtypes = [vp, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_uint64, C.c_int]
+    L.is_serve_start.argtypes = [vp]
+    L.is_serve_submit.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.POINTER(C.c_int)]
+    L.is_serve_poll.argtypes = [vp, vp, C.c_int, C.POINTER(C.c_int)]
+    L.is_serve_counts.argtypes = [vp, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
+    L.is_serve_copy.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp * 3, vp]
+    L.is_serve_stop.argtypes = [vp]
+    L.is_serve_close.argtypes = [vp]
     _lib = L
     return L
 
@@ -325,6 +334,55 @@ class Encoder:
     def set_poison(self, on=True):
         """Poison mode: workspace bytes and kernel shared memory start as garbage (results must not change)."""
         self._check(self.L.is_set_poison(self.h, 1 if on else 0), "is_set_poison")
+
+    # ---- serving session: continuous admission into a running closed loop ----
+    def serve_open(self, bit_depth=8, chroma_444=False, arena_bytes=4 << 30, max_images=64, max_leaves=1 << 22, recon_ctas=0,
+                   start=True):
+        """Allocate a serving session (and start its loop; with several sessions in a process, open all with
+        start=False, then serve_start each: allocations wait for running loops)."""
+        self._check(self.L.is_serve_open(self.h, bit_depth, int(bool(chroma_444)), int(arena_bytes), max_images, int(max_leaves),
+                                         recon_ctas), "is_serve_open")
+        if start:
+            self.serve_start()
+
+    def serve_start(self):
+        self._check(self.L.is_serve_start(self.h), "is_serve_start")
+
+    def serve_submit(self, planes, qindex, host=True):
+        """Queue one image into the running closed loop; its ticket, or None when the session has no room now."""
+        f = self._frame(planes, qindex, host)
+        t = C.c_int()
+        rc = self.L.is_serve_submit(self.h, C.byref(f), 1 if host else 0, C.byref(t))
+        if rc == IS_ERR_BUSY:
+            return None
+        self._check(rc, "is_serve_submit")
+        return t.value
+
+    def serve_poll(self, cap=256):
+        """Tickets of the images whose records are ready (packed; read them with serve_fetch)."""
+        out = np.zeros(cap, np.int32)
+        n = C.c_int()
+        self._check(self.L.is_serve_poll(self.h, out.ctypes.data, cap, C.byref(n)), "is_serve_poll")
+        return [int(v) for v in out[:n.value]]
+
+    def serve_fetch(self, ticket, width, height, qindex, bit_depth=8, chroma_444=False):
+        nb, nt, nc = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        self._check(self.L.is_serve_counts(self.h, ticket, C.byref(nb), C.byref(nt), C.byref(nc)), "is_serve_counts")
+        nb, nt, nc = nb.value, nt.value, nc.value
+        out = {"blocks": np.zeros(nb, BLOCK_DT), "block_txb": np.zeros(nb + 1, np.uint32), "txb": np.zeros(nt, TXB_DT),
+               "coeffs": np.zeros(nc, np.int16), "recon": _recon_arrays(width, height, bit_depth, chroma_444)}
+        rp = (C.c_void_p * 3)(*[r.ctypes.data for r in out["recon"]])
+        pitches = (C.c_int32 * 3)(*[r.strides[0] // r.itemsize for r in out["recon"]])
+        self._check(self.L.is_serve_copy(self.h, ticket, None, out["blocks"].ctypes.data, out["block_txb"].ctypes.data,
+                                         out["txb"].ctypes.data, out["coeffs"].ctypes.data, rp, pitches), "is_serve_copy")
+        return Record(width, height, qindex, out["blocks"], out["block_txb"], out["txb"], out["coeffs"], out["recon"], {},
+                      bit_depth, chroma_444)
+
+    def serve_stop(self):
+        self._check(self.L.is_serve_stop(self.h), "is_serve_stop")
+
+    def serve_close(self):
+        self._check(self.L.is_serve_close(self.h), "is_serve_close")
 
     def set_batch_options(self, use_graph=False, front_streams=0, recon_ctas=0):
         self._check(self.L.is_set_batch_options(self.h, 1 if use_graph else 0, front_streams, recon_ctas),

@@ -141,6 +141,116 @@ class Server:
         return reqs
 
 
+class StreamServer:
+    """Continuous admission into running closed loops (is_serve_*): one serving session per image format, opened when
+    the first image of that format arrives.  An arriving request is submitted at once when its session has a free slot
+    and workspace range (else it waits in arrival order); its front end runs on a free stream and its leaves join the
+    closed loop that is already running, next to the images submitted before it.  Each request completes on its own:
+    its record is packed and read out as soon as its last leaf is done, whatever the others are doing.  Latency runs from
+    arrival to the record and reconstruction being in host memory."""
+
+    def __init__(self, device=0, hbm_budget=None, max_images=64, recon_ctas=None, shortlist=None):
+        from .isearch import Encoder, workspace_bytes, plane_format
+        import torch
+        self._Encoder, self._wsb, self._fmt = Encoder, workspace_bytes, plane_format
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info(device)
+            hbm_budget = free // 2
+        self.device, self.budget, self.max_images = device, int(hbm_budget), max_images
+        self.recon_ctas = recon_ctas or {}
+        self.shortlist = shortlist
+        self.stall_s = 60.0
+        self.encs = {}       # (bit depth, 4:4:4) -> Encoder
+        self.sessions = {}   # the formats' Encoders with an open session (during run)
+
+    def _session(self, fmt, nfmt):
+        """Allocate the session of a format (its loop is started by run, after every session is allocated)."""
+        if fmt not in self.encs:
+            e = self._Encoder(self.device)
+            if self.shortlist is not None:
+                e.set_shortlist(**self.shortlist)
+            self.encs[fmt] = e
+        e = self.encs[fmt]
+        e.serve_open(fmt[0], fmt[1], arena_bytes=self.budget // nfmt, max_images=self.max_images, max_leaves=1 << 24,
+                     recon_ctas=self.recon_ctas.get(fmt, 0), start=False)
+        self.sessions[fmt] = e
+
+    def _close_sessions(self):
+        errs = []
+        for step in ("serve_stop", "serve_close"):   # every loop stopped before anything is freed
+            for e in self.sessions.values():
+                try:
+                    getattr(e, step)()
+                except RuntimeError as ex:
+                    errs.append(ex)
+        self.sessions = {}
+        if errs:
+            raise errs[0]
+
+    def close(self):
+        try:
+            self._close_sessions()
+        finally:
+            for e in self.encs.values():
+                e.close()
+            self.encs = {}
+
+    def run(self, arrivals, poll_s=0.0002):
+        """Serve a list of (arrival time in s from now, planes, qindex); returns the Requests (records filled).  The
+        requests' planes are copied to pinned host memory and the sessions of their formats opened before the clock
+        starts (a request's data is in pinned memory when it arrives, as from a network buffer)."""
+        import torch
+        pinned = [[torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy() for a in p] for _, p, _ in arrivals]
+        reqs = [Request(i, pinned[i], q, None) for i, (_, _, q) in enumerate(arrivals)]
+        fmts = {self._fmt(p) for p in pinned}
+        for fmt in sorted(fmts):   # every session allocated first, then their loops started (allocations wait for running loops)
+            self._session(fmt, len(fmts))
+        for fmt in sorted(fmts):
+            self.sessions[fmt].serve_start()
+        try:
+            return self._serve(reqs, [ta for ta, _, _ in arrivals], poll_s)
+        finally:
+            self._close_sessions()
+
+    def _serve(self, reqs, times, poll_s):
+        pending = deque()
+        inflight = {}   # (format, ticket) -> request
+        nxt, done = 0, 0
+        t0 = time.perf_counter()
+        t_last = t0   # the last completion (a run that stops completing raises instead of waiting forever)
+        while done < len(reqs):
+            now = time.perf_counter()
+            if inflight and now - t_last > self.stall_s:
+                raise RuntimeError("serving made no progress for %.0f s (%d requests in flight)" % (self.stall_s, len(inflight)))
+            while nxt < len(reqs) and times[nxt] <= now - t0:
+                reqs[nxt].t_arrive = t0 + times[nxt]
+                pending.append(reqs[nxt])
+                nxt += 1
+            while pending:   # admission in arrival order, as slots and workspace free up
+                r = pending[0]
+                fmt = self._fmt(r.planes)
+                e = self.sessions[fmt]
+                tk = e.serve_submit(r.planes, r.qindex, host=True)
+                if tk is None:
+                    break
+                r.t_start = time.perf_counter()
+                r.batch = -1
+                inflight[(fmt, tk)] = r
+                pending.popleft()
+            for fmt, e in self.sessions.items():
+                for tk in e.serve_poll():
+                    r = inflight.pop((fmt, tk))
+                    h, w = r.planes[0].shape
+                    r.record = e.serve_fetch(tk, w, h, r.qindex, fmt[0], fmt[1])
+                    r.t_done = t_last = time.perf_counter()
+                    done += 1
+            if nxt < len(reqs) and not inflight and not pending:
+                time.sleep(max(0.0, min(times[nxt] - (time.perf_counter() - t0), 0.01)))
+            else:
+                time.sleep(poll_s)
+        return reqs
+
+
 def poisson_arrivals(rate, n, seed=0):
     """n arrival times (s) of a Poisson stream of `rate` requests per second."""
     rng = np.random.default_rng(seed)
@@ -165,6 +275,8 @@ def main():
     ap.add_argument("--recon-ctas", type=int, default=110)
     ap.add_argument("--max-batch", type=int, default=32)
     ap.add_argument("--plain", action="store_true", help="the plain search (default: batched + learned shortlist)")
+    ap.add_argument("--mode", default="stream", choices=["stream", "batch", "both"],
+                    help="stream: continuous admission into running closed loops (is_serve_*); batch: batches per worker")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "shortlist_weights.npz"))
     ap.add_argument("--tau", type=float, default=0.9)
     ap.add_argument("--max-modes", type=int, default=6)
@@ -175,20 +287,26 @@ def main():
     if not args.plain:
         from .shortlist import load_weights
         sl = {"weights": load_weights(args.weights), "tau": args.tau, "max_modes": args.max_modes, "rd_k": args.rd_k}
-    srv = Server(pipelines=args.pipelines, max_batch=args.max_batch, recon_ctas=args.recon_ctas, shortlist=sl)
-    try:
-        srv.run([(0.0, p, q) for p, q in reqs[:4]])   # warm-up: workspaces, tables
-        for rate in [float(r) for r in args.rates.split(",")]:
-            t = poisson_arrivals(rate, len(reqs), seed=int(rate))
-            done = srv.run([(float(ti), p, q) for ti, (p, q) in zip(t, reqs)])
-            mp = sum(r.pixels for r in done) / 1e6
-            span = max(r.t_done for r in done) - min(r.t_arrive for r in done)
-            line = {"form": "plain" if args.plain else "batched + shortlist (tau %g, max %d modes, rd_k %d)" % (args.tau, args.max_modes, args.rd_k),
-                    "arrival_rate_per_s": rate, "requests": len(done), "mp": round(mp, 1), "mp_per_s": round(mp / span, 2),
-                    "batches": len({r.batch for r in done}), **latency_stats(done)}
-            print(json.dumps(line), flush=True)
-    finally:
-        srv.close()
+    modes = ["stream", "batch"] if args.mode == "both" else [args.mode]
+    for mode in modes:
+        if mode == "stream":
+            srv = StreamServer(shortlist=sl, recon_ctas={(8, False): 84, (10, True): 24})
+        else:
+            srv = Server(pipelines=args.pipelines, max_batch=args.max_batch, recon_ctas=args.recon_ctas, shortlist=sl)
+        try:
+            srv.run([(0.0, p, q) for p, q in reqs[:4]])   # warm-up: workspaces, tables
+            for rate in [float(r) for r in args.rates.split(",")]:
+                t = poisson_arrivals(rate, len(reqs), seed=int(rate))
+                done = srv.run([(float(ti), p, q) for ti, (p, q) in zip(t, reqs)])
+                mp = sum(r.pixels for r in done) / 1e6
+                span = max(r.t_done for r in done) - min(r.t_arrive for r in done)
+                form = "plain" if args.plain else "batched + shortlist (tau %g, max %d modes, rd_k %d)" % (args.tau, args.max_modes, args.rd_k)
+                line = {"form": form + (", continuous admission" if mode == "stream" else ", batches per worker"),
+                        "arrival_rate_per_s": rate, "requests": len(done), "mp": round(mp, 1), "mp_per_s": round(mp / span, 2),
+                        "batches": len({r.batch for r in done}), **latency_stats(done)}
+                print(json.dumps(line), flush=True)
+        finally:
+            srv.close()
 
 
 if __name__ == "__main__":

@@ -33,8 +33,8 @@ sys.path.insert(0, ROOT)
 
 W_IMG, H_IMG, SEED = 4000, 3000, 12
 # kernels of one search: k_pad x 3 planes, k_analysis_big, k_analysis, k_analysis_tiny, k_analysis_mid, k_dp, k_leaf_prep, k_leaf_queue_scan,
-# k_leaf_deps x 3 passes, k_recon, k_pack_scan, k_pack
-LAUNCHES_PER_STEP = 16
+# k_leaf_deps x 4 passes, k_recon, k_pack_scan, k_pack
+LAUNCHES_PER_STEP = 17
 
 
 def parse():

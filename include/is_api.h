@@ -37,6 +37,7 @@ extern "C" {
 #define IS_ERR_TIMEOUT -4   /* a wavefront dependency wait of the closed loop ran out of its budget (no hang) */
 #define IS_ERR_STATE -5     /* no encode result to read */
 #define IS_ERR_TOO_LARGE -6 /* the request does not fit the fixed scratch of is_fwd_quant_static */
+#define IS_ERR_BUSY -7      /* a serving session has no room for the image now: poll, copy finished images, retry */
 
 typedef struct is_params {
     int32_t bit_depth;      /* 8 or 10: the format of frames whose own bit_depth is 0 */
@@ -124,6 +125,42 @@ int is_workspace_bytes_format(int width, int height, int bit_depth, int chroma_4
 /* Autotuner: times the batch with 1, 2 and 4 front-end streams (two runs each, the second timed) and keeps the
  * fastest for the handle; returns the choice and its time (ms). */
 int is_autotune_batch(is_handle *h, const is_frame *frames, int n, int from_host, int *front_streams, float *ms);
+
+/* ---- serving: continuous admission of images into a running closed loop ----
+ * A session (one per handle, one image format; is_serve_open allocates it, is_serve_start starts it) keeps one persistent
+ * closed loop running on recon_ctas SMs (0: three
+ * quarters of them; the rest run the front ends of arriving images and the packs of finished ones).  is_serve_submit
+ * places an image in a free range of the session's workspace arena (arena_bytes; an image needs
+ * is_workspace_bytes_format(...) bytes of it) and a free slot of max_images, and queues its front end (upload, analysis,
+ * DP, dataflow graph) on a front-end stream; its first ready leaves go into the loop that is already running, so an image
+ * submitted while others are in the closed loop is searched together with them.  Its last leaf signals the host:
+ * is_serve_poll packs the records of the images whose loop has finished and returns the tickets of those whose records
+ * are ready; is_serve_copy copies one out (as is_batch_copy) and frees its range and slot.  Each image's result is that of
+ * the same image searched alone.  Limits: max_leaves bounds the leaf positions of the whole session (each image reserves
+ * 256 per superblock; IS_ERR_STATE when used up: close and open a new session).  The loop ends by itself after 2 ms
+ * without work, and is_serve_poll launches it again once a submitted image's front end has queued leaves: the caller
+ * polls to make progress, and the loop holds its stream only while there is work.  is_serve_stop waits for the loop to
+ * end (no new launch follows); is_serve_close stops and frees the session (images not read out are lost).  While a
+ * session is open its loop occupies the device: host planes should be in pinned memory, and the process should not free
+ * device or pinned memory (cudaFree / cudaFreeHost, e.g. another handle's workspace growing), which would wait for the
+ * loop.  A running loop holds a hardware work queue: a process that opens sessions does best with more queues than the
+ * default 8 (CUDA_DEVICE_MAX_CONNECTIONS=32, which the Python package sets on import), so that fewer streams share one
+ * with a loop and wait for it to become idle.  The
+ * reference runs whole batches per GpEncoder thread (encoder/src/batch.cpp:1005-1029) and has no counterpart. */
+int is_serve_open(is_handle *h, int bit_depth, int chroma_444, uint64_t arena_bytes, int max_images, uint64_t max_leaves,
+                  int recon_ctas);
+/* starts the session's loop (allocates nothing: open every session of the process first, then start them) */
+int is_serve_start(is_handle *h);
+/* from_host: host planes (else device planes); IS_ERR_BUSY: no free slot or range now (poll / copy, then retry) */
+int is_serve_submit(is_handle *h, const is_frame *f, int from_host, int *ticket);
+int is_serve_poll(is_handle *h, int *tickets, int cap, int *n);
+int is_serve_counts(is_handle *h, int ticket, uint32_t *n_blocks, uint32_t *n_txb, uint64_t *n_coeffs);
+int is_serve_copy(is_handle *h, int ticket, av1g_frame_params *fp, av1g_block *blocks, uint32_t *block_txb, av1g_txb *txb,
+                  int16_t *coeffs, void *recon[3], const int32_t recon_pitch[3]);
+/* ends the loop without freeing (a process with several sessions stops them all, then closes them: frees wait for every
+ * running kernel); is_serve_close stops if needed and frees the session */
+int is_serve_stop(is_handle *h);
+int is_serve_close(is_handle *h);
 
 /* ---- kernel-level entry points for the parity tests (device primitives of av1core's dsp.h API) ---- */
 /* Forward 2-D transform (this project's integer transform) + quantisation + rate of n residual blocks of one tx
