@@ -39,6 +39,7 @@ template <typename Px, int BUFI> struct AnWarp {
     Px pred[BUFI > 2048 ? 4096 : 1024];   // predictions of the tasks' candidates, W x H per group
     int predC[8];                         // candidate whose prediction a group's slice holds (-1: none)
     i64 taskJ[8];
+    i64 txJ[16];                          // the winner's open-loop cost per tx type (INF: not evaluated)
     Px ea[EDGE_LEN], el[EDGE_LEN];
     int satd[32];
     int cand[32];
@@ -141,7 +142,7 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
     (void)nc;
     int top[K_TOP];
     int nK = 0;
-    const int kMax = mmask != 0x1FFFu ? F.slRdK : K_TOP;   // a shortlisted block: its best slRdK candidates only
+    const int kMax = mmask != 0x1FFFu ? F.slRdK : F.rdK;   // a shortlisted block: its best slRdK candidates only
 #pragma unroll
     for (int k = 0; k < K_TOP; k++) {
         top[k] = warp_argmin(js, lane);
@@ -183,6 +184,8 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
         __syncwarp();
     }
     // stage 2: the other tx types of the set for the winner
+    if (lane < 16) S.txJ[lane] = lane == AV1G_DCT_DCT ? bestJ : INF;   // the winner's costs per type (txKeep)
+    __syncwarp();
     if (set != AV1G_TX_SET_DCTONLY) {
         int types[8], nt = 0;
         for (int t = 1; t < 16; t++) if (tx_in_set(set, t)) types[nt++] = t;
@@ -190,11 +193,26 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
         for (int r0 = 0; r0 < nt; r0 += ng) {
             const int tt = types[min(r0 + grp, nt - 1)];
             const EvalOut o = evalc(c, tt);
-            if (g == 0 && r0 + grp < nt) S.taskJ[grp] = o.D + F.lam * (o.R + mbits(c) + overhead);
+            if (g == 0 && r0 + grp < nt) {
+                const i64 J = o.D + F.lam * (o.R + mbits(c) + overhead);
+                S.taskJ[grp] = J;
+                S.txJ[tt] = J;
+            }
             __syncwarp();
             for (int t = 0; t < ng && r0 + t < nt; t++)
                 if (S.taskJ[t] < bestJ) { bestJ = S.taskJ[t]; bestTx = types[r0 + t]; }
             __syncwarp();
+        }
+    }
+    // the txKeep best types by cost (the lower type of equal costs: the one evaluated first)
+    uint32_t txMask = 0;
+    if (F.txKeep && set != AV1G_TX_SET_DCTONLY) {
+        i64 v = lane < 16 ? S.txJ[lane] : INF;
+        for (int k = 0; k < F.txKeep; k++) {
+            const int b = warp_argmin(v, lane);
+            if (b < 0) break;
+            txMask |= 1u << b;
+            if (lane == b) v = INF;
         }
     }
     if (lane == 0) {
@@ -206,7 +224,7 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
         for (int k = 0; k < nK; k++) if (k != bestK) r.cand[n++] = (uint8_t)S.cand[top[k]];
         for (int k = n; k < 4; k++) r.cand[k] = 0;
         r.ncand = (uint8_t)n;
-        r.pad[0] = r.pad[1] = 0;
+        r.txMask = (uint16_t)txMask;
         F.blk[F.shOff[bs] + (uint32_t)(y / H) * F.shNbx[bs] + x / W] = r;
     }
     __syncwarp();

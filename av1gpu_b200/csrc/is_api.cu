@@ -243,6 +243,8 @@ struct is_handle {
     uint64_t wsLimit = 0;                   // 0: no limit
     bool poison = false;
     size_t bNeed = 0;                       // bytes of the arena the last batch uses
+    // non-learned pruning (is_set_search_options): RD candidates per block, tx types the closed loop keeps per block
+    int rdK = K_TOP, txKeep = 0;
     // learned shortlist (is_set_shortlist_model): bf16 weights, fp32 biases, mask rule; per front-end stream a chunk of
     // features / hidden activations / scores
     bool slOn = false;
@@ -656,6 +658,8 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         F.leafTrace = (h->trace && i == 0 && F.img == 0) ? h->traceBuf : nullptr;   // image 0, when its group's first
         if (!h->slOn) F.slMask = nullptr;
         F.slRdK = h->slOn ? h->slRdK : 4;
+        F.rdK = h->rdK;
+        F.txKeep = h->txKeep;
         F.waitIters = h->waitIters;
         F.readyWaitNs = h->readyWaitNs;
         F.poison = h->poison ? 1 : 0;
@@ -796,8 +800,8 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
 static std::string batch_key(const is_handle *h, const is_frame *fr, int n, bool fromHost) {
     std::string k;
     char b[160];
-    snprintf(b, sizeof b, "%p|%d|%d|%d|%d|%d|%d|%d|%lld|", h->arena, n, (int)fromHost, h->frontStreams, h->reconCtas, h->slOn ? h->slVersion : -1,
-             (int)h->poison, h->waitIters, h->readyWaitNs);
+    snprintf(b, sizeof b, "%p|%d|%d|%d|%d|%d|%d|%d|%lld|%d|%d|", h->arena, n, (int)fromHost, h->frontStreams, h->reconCtas,
+             h->slOn ? h->slVersion : -1, (int)h->poison, h->waitIters, h->readyWaitNs, h->rdK, h->txKeep);
     k += b;
     for (int i = 0; i < n; i++) {
         snprintf(b, sizeof b, "%d,%d,%d,%d,%d,%p,%p,%p,%d,%d,%d;", fr[i].width, fr[i].height, fr[i].qindex, fr[i].bit_depth, fr[i].chroma_444,
@@ -934,6 +938,14 @@ int is_set_workspace_limit(is_handle *h, uint64_t bytes) {
 int is_set_poison(is_handle *h, int on) {
     if (!h) return IS_ERR_INVALID;
     h->poison = on != 0;
+    return IS_OK;
+}
+
+int is_set_search_options(is_handle *h, int rd_k, int tx_keep) {
+    if (!h) return IS_ERR_INVALID;
+    if (rd_k < 0 || rd_k > K_TOP || tx_keep < 0 || tx_keep > 3) return h->setErr(IS_ERR_INVALID, "invalid search options");
+    h->rdK = rd_k ? rd_k : K_TOP;
+    h->txKeep = tx_keep;
     return IS_OK;
 }
 

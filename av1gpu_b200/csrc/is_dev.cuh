@@ -170,6 +170,29 @@ __device__ __forceinline__ int warp_argmin(i64 v, int i) {
     return v < INF ? i : -1;
 }
 
+// The best (at most 3) tx types of an analysed block by open-loop RD cost, the first evaluated of equal costs ahead:
+// the tx types FrameDesc::txKeep lets the closed loop's second pass try (BlockRes::txMask).
+struct TxRank {
+    i64 j[3];
+    int t[3];
+    __device__ __forceinline__ TxRank() : j{INF, INF, INF}, t{0, 0, 0} {}
+    __device__ __forceinline__ void add(i64 v, int ty) {   // after every kept entry of cost <= v
+        const int pos = (j[0] <= v) + (j[1] <= v) + (j[2] <= v);
+#pragma unroll
+        for (int s = 2; s >= 0; s--) {
+            if (s > pos) { j[s] = j[s > 0 ? s - 1 : 0]; t[s] = t[s > 0 ? s - 1 : 0]; }
+            else if (s == pos) { j[s] = v; t[s] = ty; }
+        }
+    }
+    __device__ __forceinline__ uint16_t mask(int keep) const {   // 0 (every type) when keep is 0
+        uint32_t m = 0;
+#pragma unroll
+        for (int s = 0; s < 3; s++)
+            if (s < keep && j[s] < INF) m |= 1u << t[s];
+        return (uint16_t)m;
+    }
+};
+
 // ---- geometry (spec tables) ----
 __device__ __forceinline__ int bw4(int bs) { return ST(Num_4x4_Blocks_Wide)[bs]; }
 __device__ __forceinline__ int bh4(int bs) { return ST(Num_4x4_Blocks_High)[bs]; }

@@ -28,7 +28,7 @@ struct BlockRes {      // analysis result of one (shape, position): 16 bytes
     uint8_t cand[4];   // candidates (mode << 3 | delta + 3), best first
     uint8_t ncand;
     uint8_t tx;        // best tx type of cand[0]
-    uint8_t pad[2];
+    uint16_t txMask;   // tx types the closed loop's second pass may try for cand[0] (bit t: type t); 0: every type
 };
 struct Leaf { uint8_t bsize, x4, y4, pad; };
 struct SbCount { uint32_t nBlocks, nTxb, nCoeffs, pad; };
@@ -46,6 +46,8 @@ struct __align__(16) FrameDesc {
     uint32_t nRec;                            // analysis records (all shapes)
     uint16_t *slMask;                         // [nRec] shortlist: modes to screen per record (bit m: mode m); null: all
     int slRdK;                                // shortlist: RD candidates of a block whose list is not all 13 modes
+    int rdK;                                  // RD candidates of every other block (1 .. 4; the plain form: 4)
+    int txKeep;                               // 0, or the tx types (best analysis cost first) a block's txMask keeps
     uint32_t shOff[22];
     int shNbx[22], shNby[22];
     long long lam, sqlam;                     // lambda, sqrt(lambda) in 1/256

@@ -529,6 +529,8 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
             }
         };
         const int nc = max(1, min((int)br.ncand, K_RECHECK));
+        // the types pass 2 may try for cand[0]: its open-loop shortlist (with DCT_DCT and the analysis' type), or all
+        const uint32_t txAllow = br.txMask ? (uint32_t)br.txMask | (1u << AV1G_DCT_DCT) | (1u << br.tx) : 0xFFFFu;
         int tcand[8], ttype[8], n1 = 0;
         for (int k = 0; k < nc; k++) { tcand[n1] = br.cand[k]; ttype[n1] = AV1G_DCT_DCT; n1++; }
         if (br.tx != AV1G_DCT_DCT) { tcand[n1] = br.cand[0]; ttype[n1] = br.tx; n1++; }
@@ -542,7 +544,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
             // count, so this saves the second round.
             const int c0 = br.cand[0], c1 = nc >= 2 ? br.cand[1] : br.cand[0];
             const int tt = lane & 15;   // pass-2 types: lanes 0-15 for the first candidate, 16-31 for the second
-            const bool ok = lane < 16 ? tx_in_set(set, tt) && !(!skip1 && (tt == AV1G_DCT_DCT || tt == br.tx))
+            const bool ok = lane < 16 ? tx_in_set(set, tt) && ((txAllow >> tt) & 1) && !(!skip1 && (tt == AV1G_DCT_DCT || tt == br.tx))
                                       : nc >= 2 && tx_in_set(set, tt) && tt != AV1G_DCT_DCT;
             const unsigned bal = __ballot_sync(0xffffffffu, ok), m0 = bal & 0xFFFFu, m1 = bal >> 16;
             const int p1 = skip1 ? 0 : n1, n2a = __popc(m0), n2b = __popc(m1), nt = p1 + n2a + n2b;
@@ -592,6 +594,7 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
             for (int t = 0; t < 16; t++) {
                 if (!tx_in_set(set, t)) continue;
                 if (!skip1 && (t == AV1G_DCT_DCT || (isC0 && t == br.tx))) continue;
+                if (isC0 && !((txAllow >> t) & 1)) continue;
                 tcand[n2] = c1; ttype[n2] = t; n2++;
             }
             run(tcand, ttype, n2);

@@ -263,6 +263,8 @@ int is_serve_submit(is_handle *h, const is_frame *f, int from_host, int *ticket)
     F.leafTrace = nullptr;
     if (!h->slOn) F.slMask = nullptr;
     F.slRdK = h->slOn ? h->slRdK : 4;
+    F.rdK = h->rdK;
+    F.txKeep = h->txKeep;
     F.waitIters = h->waitIters;
     F.readyWaitNs = h->readyWaitNs;
     F.poison = 0;

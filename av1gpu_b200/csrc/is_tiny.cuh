@@ -369,7 +369,7 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem<Px
     };
     i64 bestJ = INF;
     int bestK = 0, bestTx = AV1G_DCT_DCT;
-    const int kMax = mmask != 0x1FFFu ? F.slRdK : 4;   // a shortlisted block: its best slRdK candidates only
+    const int kMax = mmask != 0x1FFFu ? F.slRdK : F.rdK;   // a shortlisted block: its best slRdK candidates only
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         if (topJ[k] == INF || k >= kMax) continue;   // fewer candidates screened or taken (shortlist)
@@ -389,11 +389,14 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem<Px
             for (int k = 0; k < NWD; k++) wp[k] = topP[s][k];
         }
     // 4- and 8-point sizes are in TX_SET_INTRA_1: IDTX, DCT_DCT, V_DCT, H_DCT, ADST_ADST, ADST_DCT, DCT_ADST
+    TxRank rank;
+    rank.add(bestJ, AV1G_DCT_DCT);
 #pragma unroll 1
     for (int t = 1; t < 16; t++) {
         if (!tx_in_set(AV1G_TX_SET_INTRA_1, t)) continue;
         const i64 j = rd(wp, wm, t);
         if (j < bestJ) { bestJ = j; bestTx = t; }
+        rank.add(j, t);
     }
     BlockRes r;
     r.J = bestJ;
@@ -405,7 +408,7 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem<Px
     for (int k = 0; k < 4; k++)
         if (k != bestK && topJ[k] < INF && k < kMax) r.cand[n++ & 3] = (uint8_t)cand_pack(topM[k], 0);
     r.ncand = (uint8_t)n;
-    r.pad[0] = r.pad[1] = 0;
+    r.txMask = rank.mask(F.txKeep);
     F.blk[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] = r;
 }
 
@@ -592,7 +595,8 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem<Px> &S, co
     int bestK = 0, bestTx = AV1G_DCT_DCT, winC = 0;
     // the modes screened: all 13, or the block's learned shortlist
     const uint32_t mmask = F.slMask ? F.slMask[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] : 0x1FFFu;
-    const int kMax = mmask != 0x1FFFu ? F.slRdK : 4;   // a shortlisted block: its best slRdK candidates only
+    const int kMax = mmask != 0x1FFFu ? F.slRdK : F.rdK;   // a shortlisted block: its best slRdK candidates only
+    TxRank rank;   // the winner's types by cost (txKeep)
     // jobs: 0-12 the 13 modes, 13-24 the deltas of the two best directional modes (SATD); 25-28 the top 4 with
     // DCT_DCT, 29-34 the other types of TX_SET_INTRA_1 for the winner (RD); a job no thread of the warp needs is skipped
 #pragma unroll 1
@@ -659,6 +663,8 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem<Px> &S, co
             const EvalIn e{t, 0, 0, 0, m, F.dcQ, F.acQ, T};
             const EvalOut o = mid_eval<BD, LW, LH>(txSz, res, e, iscan, 64, qs);
             const i64 J = o.D + F.lam * (o.R + mbits(c) + overhead);
+            if (need && job == 29) rank.add(bestJ, AV1G_DCT_DCT);   // the winner's DCT_DCT cost, before its other types
+            if (need && job >= 29) rank.add(J, t);
             if (need && J < bestJ) {
                 bestJ = J;
                 if (job < 29) { bestK = job - 25; winC = c; }
@@ -676,7 +682,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem<Px> &S, co
     for (int k = 0; k < 4; k++)
         if (k != bestK && topJ[k] < INF && k < kMax) r.cand[n++ & 3] = (uint8_t)topC[k];
     r.ncand = (uint8_t)n;
-    r.pad[0] = r.pad[1] = 0;
+    r.txMask = rank.mask(F.txKeep);
     F.blk[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] = r;
 }
 

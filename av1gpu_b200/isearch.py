@@ -57,7 +57,7 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_fwd_quant_static", "is_encode_batch", "is_batch_counts", "is_batch_copy", "is_set_batch_options",
            "is_autotune_batch", "is_workspace_bytes", "is_workspace_bytes_format", "is_sl_create", "is_sl_destroy", "is_sl_set_weights",
            "is_sl_get_weights", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset", "is_set_shortlist_model",
-           "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison", "is_serve_open", "is_serve_start", "is_serve_submit", "is_serve_poll",
+           "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison", "is_set_search_options", "is_serve_open", "is_serve_start", "is_serve_submit", "is_serve_poll",
            "is_serve_counts", "is_serve_copy", "is_serve_stop", "is_serve_close"]
 
 _lib = None
@@ -115,6 +115,7 @@ def load_library():
     L.is_set_wait_limits.argtypes = [vp, C.c_int, C.c_longlong]
     L.is_set_workspace_limit.argtypes = [vp, C.c_uint64]
     L.is_set_poison.argtypes = [vp, C.c_int]
+    L.is_set_search_options.argtypes = [vp, C.c_int, C.c_int]
     L.is_serve_open.argtypes = [vp, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_uint64, C.c_int]
     L.is_serve_start.argtypes = [vp]
     L.is_serve_submit.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.POINTER(C.c_int)]
@@ -334,6 +335,11 @@ class Encoder:
     def set_poison(self, on=True):
         """Poison mode: workspace bytes and kernel shared memory start as garbage (results must not change)."""
         self._check(self.L.is_set_poison(self.h, 1 if on else 0), "is_set_poison")
+
+    def set_search_options(self, rd_k=4, tx_keep=0):
+        """Non-learned pruning: RD candidates per analysed block (1 .. 4) and the tx types (0 = all, 1 .. 3 best by the
+        analysis' cost) the closed loop's tx-type pass keeps per block.  The defaults are the plain form."""
+        self._check(self.L.is_set_search_options(self.h, rd_k, tx_keep), "is_set_search_options")
 
     # ---- serving session: continuous admission into a running closed loop ----
     def serve_open(self, bit_depth=8, chroma_444=False, arena_bytes=4 << 30, max_images=64, max_leaves=1 << 22, recon_ctas=0,

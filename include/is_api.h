@@ -117,6 +117,14 @@ int is_set_workspace_limit(is_handle *h, uint64_t bytes);
  * poison on they must equal those without. */
 int is_set_poison(is_handle *h, int on);
 
+/* Non-learned pruning of the handle's later encodes (the plain form: rd_k 4, tx_keep 0).  rd_k (1 .. 4; 0 = 4): every
+ * analysed block takes its best rd_k screened candidates into the exact-rate RD (the reference's K, GpParams::K,
+ * encoder/src/gp.h); tx_keep (0 .. 3): each analysed block keeps its tx_keep best tx types by open-loop RD cost, and the
+ * closed loop's tx-type pass for that block's first candidate tries only those (with DCT_DCT and the analysis' type) -
+ * the reference's open-loop tx shortlist (GpParams::txShortlist, encoder/src/k_leafprep.cu:292-360), ranked here by the
+ * analysis' own exact-rate costs instead of a transform-domain L1 after the DP.  0 keeps every type.  Decisions change,
+ * the reconstruction stays exact. */
+int is_set_search_options(is_handle *h, int rd_k, int tx_keep);
 /* Device workspace of one image of width x height in a batch (bytes; host only, no GPU needed): what admission by
  * HBM budget counts. */
 int is_workspace_bytes(int width, int height, uint64_t *bytes);
