@@ -48,7 +48,7 @@ def workload(n, seed, max_mp=24.0, min_mp=0.18, frac10=0.2, base8=(6000, 4000), 
 def main():
     import torch
     from .isearch import Encoder, plane_format
-    from .shortlist import load_weights
+    from .shortlist import load_params
     ap = argparse.ArgumentParser()
     ap.add_argument("--images", type=int, default=256)
     ap.add_argument("--max-mp", type=float, default=24.0)
@@ -56,8 +56,13 @@ def main():
     ap.add_argument("--tune-images", type=int, default=24, help="images the front-end stream count is tuned on")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "shortlist_weights.npz"))
     ap.add_argument("--tau", type=float, default=0.9)
-    ap.add_argument("--max-modes", type=int, default=6)
+    ap.add_argument("--max-cand", type=int, default=8)
+    ap.add_argument("--conf", type=float, default=0.0)
     ap.add_argument("--rd-k", type=int, default=2)
+    ap.add_argument("--tx-tau", type=float, default=0.9)
+    ap.add_argument("--max-tx", type=int, default=2)
+    ap.add_argument("--nl-rd-k", type=int, default=0, help="also time the non-learned pruning with this RD count (0: no)")
+    ap.add_argument("--nl-tx-keep", type=int, default=2, help="tx types the non-learned pruning keeps per block")
     ap.add_argument("--no-verify", action="store_true", help="skip the check that the batch equals the one-at-a-time search")
     args = ap.parse_args()
     t0 = time.time()
@@ -115,11 +120,19 @@ def main():
                                             % (same, len(work))}), flush=True)
         if same != len(work):
             raise SystemExit("batched results differ from the one-at-a-time search")
-    enc.set_shortlist(load_weights(args.weights), tau=args.tau, max_modes=args.max_modes, rd_k=args.rd_k)
+    enc.set_shortlist(load_params(args.weights), tau=args.tau, max_cand=args.max_cand, conf=args.conf, rd_k=args.rd_k,
+                      tx_tau=args.tx_tau, max_tx=args.max_tx)
     ts, k = batched()
     enc.set_shortlist(None)
-    print(json.dumps({**base, "form": "batched + shortlist (tau %g, max %d modes, rd_k %d)" % (args.tau, args.max_modes, args.rd_k),
+    print(json.dumps({**base, "form": "batched + learned shortlist (tau %g, max %d candidates, conf %g, rd_k %d, tx tau %g, max %d tx)"
+                                      % (args.tau, args.max_cand, args.conf, args.rd_k, args.tx_tau, args.max_tx),
                       "mp_per_s": round(mp / ts, 2), "s": round(ts, 3), "front_streams": k, "x_plain": round(tp / ts, 2)}), flush=True)
+    if args.nl_rd_k:
+        enc.set_search_options(rd_k=args.nl_rd_k, tx_keep=args.nl_tx_keep)
+        tn, k = batched()
+        enc.set_search_options()
+        print(json.dumps({**base, "form": "batched + non-learned pruning (rd_k %d, tx_keep %d)" % (args.nl_rd_k, args.nl_tx_keep),
+                          "mp_per_s": round(mp / tn, 2), "s": round(tn, 3), "front_streams": k, "x_plain": round(tp / tn, 2)}), flush=True)
     enc.close()
 
 

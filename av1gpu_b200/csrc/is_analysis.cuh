@@ -113,17 +113,20 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
             __syncwarp();
         }
     };
-    // the modes screened: all 13, or the block's learned shortlist (in mode order, so ties still go to the lower mode)
-    const uint32_t recIdx = F.shOff[bs] + (uint32_t)(y / H) * F.shNbx[bs] + x / W;
-    const uint32_t mmask = F.slMask ? F.slMask[recIdx] : 0x1FFFu;
-    const int nm = __popc(mmask);
+    // the candidates screened: a block with a learned shortlist screens its list (most probable first, so ties go to
+    // the more probable one); the others the 13 modes, then +-1..3 around the two best directional modes
+    const uint32_t recIdx = (uint32_t)(y / H) * F.shNbx[bs] + x / W;
+    const SlCand *slc = (F.slCand && F.slIdx[bs] >= 0) ? F.slCand + F.slIdx[bs] + recIdx : nullptr;
+    const int nsl = slc ? slc->n : 0;
+    const uint32_t slTx = slc ? slc->txMask : 0u;
+    const int nm = nsl > 0 ? nsl : 13;
     S.satd[lane] = 0;
-    if (lane < 13 && ((mmask >> lane) & 1)) S.cand[__popc(mmask & ((1u << lane) - 1))] = cand_pack(lane, 0);
+    if (lane < nm) S.cand[lane] = nsl > 0 ? (int)slc->c[lane] : cand_pack(lane, 0);
     __syncwarp();
     screen(0, nm);
     i64 js = lane < nm ? ((i64)S.satd[lane] << 14) + F.sqlam * mbits(S.cand[lane]) : INF;
     int nc = nm;
-    if (bs >= AV1G_BLOCK_8X8) {
+    if (nsl == 0 && bs >= AV1G_BLOCK_8X8) {
         const i64 jd = (lane < nm && is_dir(cand_mode(S.cand[lane]))) ? js : INF;
         const int l0 = warp_argmin(jd, lane);
         const int l1 = warp_argmin(lane == l0 ? INF : jd, lane);
@@ -142,7 +145,7 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
     (void)nc;
     int top[K_TOP];
     int nK = 0;
-    const int kMax = mmask != 0x1FFFu ? F.slRdK : F.rdK;   // a shortlisted block: its best slRdK candidates only
+    const int kMax = nsl > 0 ? F.slRdK : F.rdK;   // a shortlisted block: its best slRdK candidates only
 #pragma unroll
     for (int k = 0; k < K_TOP; k++) {
         top[k] = warp_argmin(js, lane);
@@ -188,7 +191,8 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
     __syncwarp();
     if (set != AV1G_TX_SET_DCTONLY) {
         int types[8], nt = 0;
-        for (int t = 1; t < 16; t++) if (tx_in_set(set, t)) types[nt++] = t;
+        for (int t = 1; t < 16; t++)   // a shortlisted block: the types of its list
+            if (tx_in_set(set, t) && (!slTx || ((slTx >> t) & 1))) types[nt++] = t;
         const int c = S.cand[top[bestK]];
         for (int r0 = 0; r0 < nt; r0 += ng) {
             const int tt = types[min(r0 + grp, nt - 1)];
@@ -224,7 +228,7 @@ __device__ __noinline__ void an_block(const FrameDesc &F, const Px *tile, AnWarp
         for (int k = 0; k < nK; k++) if (k != bestK) r.cand[n++] = (uint8_t)S.cand[top[k]];
         for (int k = n; k < 4; k++) r.cand[k] = 0;
         r.ncand = (uint8_t)n;
-        r.txMask = (uint16_t)txMask;
+        r.txMask = (uint16_t)(txMask ? txMask : slTx);
         F.blk[F.shOff[bs] + (uint32_t)(y / H) * F.shNbx[bs] + x / W] = r;
     }
     __syncwarp();

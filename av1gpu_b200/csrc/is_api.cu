@@ -199,6 +199,7 @@ struct is_handle {
     int nSb = 0;
     size_t smemRcG[4] = {0, 0, 0, 0};       // the closed loop per format group (fmt_group)
     int rcGridG[4] = {0, 0, 0, 0};
+    int rcWarpsG[4] = {0, 0, 0, 0};         // its warps per CTA
     // last result
     bool have = false;
     uint32_t nBlocks = 0, nTxb = 0;
@@ -245,15 +246,14 @@ struct is_handle {
     size_t bNeed = 0;                       // bytes of the arena the last batch uses
     // non-learned pruning (is_set_search_options): RD candidates per block, tx types the closed loop keeps per block
     int rdK = K_TOP, txKeep = 0;
-    // learned shortlist (is_set_shortlist_model): bf16 weights, fp32 biases, mask rule; per front-end stream a chunk of
-    // features / hidden activations / scores
+    // learned shortlist (is_set_shortlist_model): the parameters (fp32) and their bf16 copies, the selection rule
     bool slOn = false;
-    __nv_bfloat16 *slW1 = nullptr, *slW2 = nullptr;
-    float *slB1 = nullptr, *slB2 = nullptr;
-    float slTau = 0.9f, slConf = 0.f;
-    int slMax = 6, slRdK = 4;
-    __nv_bfloat16 *slX[4] = {nullptr, nullptr, nullptr, nullptr}, *slH[4] = {nullptr, nullptr, nullptr, nullptr};
-    float *slS[4] = {nullptr, nullptr, nullptr, nullptr};
+    float *slParams = nullptr;
+    SlNet slNet{};
+    __nv_bfloat16 *slZ[4] = {nullptr, nullptr, nullptr, nullptr}, *slH[4] = {nullptr, nullptr, nullptr, nullptr};   // chunk buffers
+    float *slS[4] = {nullptr, nullptr, nullptr, nullptr};                                                         // per front stream
+    SlSel slSel{0.9f, 0.f, 0.9f, 8, 2};
+    int slRdK = 4;
     int slVersion = 0;
     std::string graphKey;
     cudaGraphExec_t graphExec = nullptr;
@@ -409,7 +409,8 @@ size_t layout(int W, int H, int bd, int c444, uint8_t *base, FrameDesc &F, int &
     }
     F.blk = (BlockRes *)take((size_t)off * sizeof(BlockRes));
     F.nRec = off;
-    F.slMask = (uint16_t *)take((size_t)off * 2);   // kept only while a shortlist model is set (prepare_batch)
+    const uint32_t nScored = sl_scored_layout(F, F.slIdx);
+    F.slCand = (SlCand *)take((size_t)nScored * sizeof(SlCand));   // kept only while a shortlist model is set (prepare_batch)
     F.leaves = (Leaf *)take((size_t)nSb * SB_MAX_LEAVES * sizeof(Leaf));
     F.nLeaves = (uint16_t *)take((size_t)nSb * 2);
     F.oBlocks = (av1g_block *)take((size_t)nSb * SB_MAX_LEAVES * sizeof(av1g_block));
@@ -464,12 +465,14 @@ int is_create(const is_params *p, is_handle **out) {
     h->nSm = prop.multiProcessorCount;
     if (an_setup<8, 0>() != cudaSuccess || an_setup<8, 1>() != cudaSuccess || an_setup<10, 0>() != cudaSuccess || an_setup<10, 1>() != cudaSuccess)
         return fail(IS_ERR_CUDA);
-    for (int g = 0; g < 4; g++) {   // the closed loop of each format group: shared memory and its cooperative grid
-        int per = 0;
-        const cudaError_t e = g == 0 ? rc_setup<8, 1>(&h->smemRcG[g], &per) : g == 1 ? rc_setup<8, 0>(&h->smemRcG[g], &per)
-                            : g == 2 ? rc_setup<10, 1>(&h->smemRcG[g], &per) : rc_setup<10, 0>(&h->smemRcG[g], &per);
+    for (int g = 0; g < 4; g++) {   // the closed loop of each format group: shared memory, warps, its cooperative grid
+        int per = 0, nw = 0;
+        size_t *sm = &h->smemRcG[g];
+        const cudaError_t e = g == 0 ? rc_setup<8, 1>(sm, &per, &nw) : g == 1 ? rc_setup<8, 0>(sm, &per, &nw)
+                            : g == 2 ? rc_setup<10, 1>(sm, &per, &nw) : rc_setup<10, 0>(sm, &per, &nw);
         if (e != cudaSuccess || per < 1) return fail(IS_ERR_CUDA);
         h->rcGridG[g] = per * h->nSm;
+        h->rcWarpsG[g] = nw;
     }
     if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess) return fail(IS_ERR_CUDA);
     for (auto &e : h->ev)
@@ -503,8 +506,8 @@ void is_destroy(is_handle *h) {
     }
     if (h->evFork) cudaEventDestroy(h->evFork);
     if (h->hFs) cudaFreeHost(h->hFs);
-    void *sl[] = {h->slW1, h->slW2, h->slB1, h->slB2, h->slX[0], h->slX[1], h->slX[2], h->slX[3], h->slH[0], h->slH[1], h->slH[2],
-                  h->slH[3], h->slS[0], h->slS[1], h->slS[2], h->slS[3]};
+    void *sl[] = {h->slParams, h->slNet.c1, h->slNet.c2, h->slNet.c3, h->slNet.f1, h->slNet.f2, h->slZ[0], h->slZ[1], h->slZ[2], h->slZ[3],
+                  h->slH[0], h->slH[1], h->slH[2], h->slH[3], h->slS[0], h->slS[1], h->slS[2], h->slS[3]};
     for (void *p : sl)
         if (p) cudaFree(p);
     if (h->hOrd) cudaFreeHost(h->hOrd);
@@ -656,7 +659,7 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         F.err = h->bErr;
         F.img = h->bPos[i] - h->bGrpStart[grp[i]];
         F.leafTrace = (h->trace && i == 0 && F.img == 0) ? h->traceBuf : nullptr;   // image 0, when its group's first
-        if (!h->slOn) F.slMask = nullptr;
+        if (!h->slOn) F.slCand = nullptr;
         F.slRdK = h->slOn ? h->slRdK : 4;
         F.rdK = h->rdK;
         F.txKeep = h->txKeep;
@@ -672,9 +675,10 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
     return IS_OK;
 }
 
-// The front end of one image on stream s: its planes into the padded workspace, the learned shortlist's mode masks
-// (with a model set; chunk buffers k), the analysis, the DP, the leaf maps and the dataflow graph, whose first ready
-// leaves go to the image's ready queue.  ev1 / ev2 (optional) are recorded after the upload and after the analysis.
+// The front end of one image on stream s: its planes into the padded workspace, the learned shortlist of every scored
+// block (with a model set: the fused inference kernel), the analysis, the DP, the leaf maps and the dataflow graph,
+// whose first ready leaves go to the image's ready queue.  ev1 / ev2 (optional) are recorded after the upload and after
+// the analysis.
 static int front_end(is_handle *h, const FrameDesc &F, const is_frame *f, int nSb, bool fromHost, cudaStream_t s, int k, cudaEvent_t ev1,
                      cudaEvent_t ev2) {
     const size_t px = F.bd > 8 ? 2 : 1;
@@ -689,18 +693,8 @@ static int front_end(is_handle *h, const FrameDesc &F, const is_frame *f, int nS
         else k_pad<uint16_t><<<dim3(1, ph), 128, 0, s>>>((uint16_t *)dst, F.spitch[p], vw, vh, pw, ph);
     }
     if (ev1) IS_CK(cudaEventRecord(ev1, s));
-    if (h->slOn) {   // the learned shortlist: scores of every analysis record, then its mode mask
-        for (uint32_t i0 = 0; i0 < F.nRec; i0 += SL_CHUNK) {
-            const int cn = (int)std::min<uint32_t>(SL_CHUNK, F.nRec - i0);
-            k_sl_features_rec<<<(cn + 7) / 8, 256, 0, s>>>(F, i0, cn, h->slX[k]);
-            k_gemm_abt<<<dim3((SL_HID + GT_N - 1) / GT_N, (cn + GT_M - 1) / GT_M), 128, 0, s>>>(
-                cn, SL_HID, SL_IN, h->slX[k], SL_IN, h->slW1, SL_IN, nullptr, 0, h->slB1, 1, h->slH[k], SL_HID);
-            k_gemm_abt<<<dim3(1, (cn + GT_M - 1) / GT_M), 128, 0, s>>>(cn, SL_OUT, SL_HID, h->slH[k], SL_HID, h->slW2, SL_HID,
-                                                                      h->slS[k], SL_OUT, h->slB2, 0, nullptr, 0);
-            k_sl_mask<<<(cn + 127) / 128, 128, 0, s>>>(cn, h->slS[k], h->slTau, h->slMax, h->slConf, F.slMask + i0);
-        }
-        IS_CK(cudaGetLastError());
-    }
+    if (h->slOn && F.slCand)   // the learned shortlist of every scored block (chunk buffers k)
+        IS_CK(sl_infer_image(F, h->slNet, h->slSel, h->nSm, h->slZ[k], h->slH[k], h->slS[k], F.slCand, nullptr, s));
     IS_CK((F.bd == 8 ? an_launch<8, 0>(F, nSb, s) : an_launch<10, 0>(F, nSb, s)));
     IS_CK((F.bd == 8 ? an_launch<8, 1>(F, nSb, s) : an_launch<10, 1>(F, nSb, s)));
     IS_CK(cudaGetLastError());
@@ -949,35 +943,35 @@ int is_set_search_options(is_handle *h, int rd_k, int tx_keep) {
     return IS_OK;
 }
 
-int is_set_shortlist_model(is_handle *h, const float *w1, const float *b1, const float *w2, const float *b2, float tau, int max_modes,
-                           float conf, int rd_k) {
+int is_set_shortlist_model(is_handle *h, const float *params, float tau, int max_cand, float conf, int rd_k, float tx_tau, int max_tx) {
     if (!h) return IS_ERR_INVALID;
     IS_CK(cudaSetDevice(h->device));
-    if (!w1) { h->slOn = false; return IS_OK; }
-    if (!b1 || !w2 || !b2 || max_modes < 0 || max_modes > 13 || !(tau > 0.f) || tau > 1.f || rd_k < 1 || rd_k > 4)
+    if (!params) { h->slOn = false; return IS_OK; }
+    if (max_cand < 1 || max_cand > 8 || !(tau > 0.f) || tau > 1.f || !(conf >= 0.f) || conf > 1.f || rd_k < 1 || rd_k > 4 ||
+        max_tx < 0 || max_tx > 16 || !(tx_tau > 0.f) || tx_tau > 1.f)
         return h->setErr(IS_ERR_INVALID, "invalid shortlist model");
     IS_CK(cudaStreamSynchronize(h->own));
-    if (!h->slW1) {
-        IS_CK(cudaMalloc(&h->slW1, (size_t)SL_HID * SL_IN * 2));
-        IS_CK(cudaMalloc(&h->slW2, (size_t)SL_OUT * SL_HID * 2));
-        IS_CK(cudaMalloc(&h->slB1, SL_HID * 4));
-        IS_CK(cudaMalloc(&h->slB2, SL_OUT * 4));
+    if (!h->slParams) {
+        IS_CK(cudaMalloc(&h->slParams, SL_NPARAM * 4));
+        IS_CK(cudaMalloc(&h->slNet.c1, SL_C1 * SL_K1P * 2));
+        IS_CK(cudaMalloc(&h->slNet.c2, SL_C2 * SL_K2 * 2));
+        IS_CK(cudaMalloc(&h->slNet.c3, SL_C3 * SL_K3 * 2));
+        IS_CK(cudaMalloc(&h->slNet.f1, SL_HID * SL_Z * 2));
+        IS_CK(cudaMalloc(&h->slNet.f2, SL_OUT * SL_HID * 2));
+        h->slNet.b1 = h->slParams + SLP_C1B; h->slNet.b2 = h->slParams + SLP_C2B; h->slNet.b3 = h->slParams + SLP_C3B;
+        h->slNet.bf1 = h->slParams + SLP_F1B; h->slNet.bf2 = h->slParams + SLP_F2B;
         for (int k = 0; k < 4; k++) {
-            IS_CK(cudaMalloc(&h->slX[k], (size_t)SL_CHUNK * SL_IN * 2));
+            IS_CK(cudaMalloc(&h->slZ[k], (size_t)SL_CHUNK * SL_Z * 2));
             IS_CK(cudaMalloc(&h->slH[k], (size_t)SL_CHUNK * SL_HID * 2));
             IS_CK(cudaMalloc(&h->slS[k], (size_t)SL_CHUNK * SL_OUT * 4));
         }
+        IS_CK(cudaFuncSetAttribute(k_sl_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SlcSmem)));
     }
-    std::vector<__nv_bfloat16> a((size_t)SL_HID * SL_IN), c((size_t)SL_OUT * SL_HID);
-    for (size_t k = 0; k < a.size(); k++) a[k] = __float2bfloat16(w1[k]);
-    for (size_t k = 0; k < c.size(); k++) c[k] = __float2bfloat16(w2[k]);
-    IS_CK(cudaMemcpy(h->slW1, a.data(), a.size() * 2, cudaMemcpyHostToDevice));
-    IS_CK(cudaMemcpy(h->slW2, c.data(), c.size() * 2, cudaMemcpyHostToDevice));
-    IS_CK(cudaMemcpy(h->slB1, b1, SL_HID * 4, cudaMemcpyHostToDevice));
-    IS_CK(cudaMemcpy(h->slB2, b2, SL_OUT * 4, cudaMemcpyHostToDevice));
-    h->slTau = tau;
-    h->slMax = max_modes;
-    h->slConf = conf;
+    IS_CK(cudaMemcpy(h->slParams, params, SL_NPARAM * 4, cudaMemcpyHostToDevice));
+    k_sl_weights<<<(SL_HID * SL_Z + 255) / 256, 256, 0, h->own>>>(h->slParams, h->slNet);
+    IS_CK(cudaGetLastError());
+    IS_CK(cudaStreamSynchronize(h->own));
+    h->slSel = SlSel{tau, conf, tx_tau, max_cand, max_tx};
     h->slRdK = rd_k;
     h->slOn = true;
     h->slVersion++;

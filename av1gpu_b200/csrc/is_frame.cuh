@@ -30,6 +30,13 @@ struct BlockRes {      // analysis result of one (shape, position): 16 bytes
     uint8_t tx;        // best tx type of cand[0]
     uint16_t txMask;   // tx types the closed loop's second pass may try for cand[0] (bit t: type t); 0: every type
 };
+// a block's learned shortlist (k_sl_select): its candidates, most probable first, and the tx types worth a try
+struct SlCand {
+    uint8_t c[8];      // (mode, delta) candidate codes
+    uint16_t txMask;   // tx types (bit t) the analysis and the closed loop try beyond DCT_DCT; 0: every type
+    uint8_t n;         // candidates; 0: the block falls back to the full search (top probability below conf)
+    uint8_t pad[5];
+};
 struct Leaf { uint8_t bsize, x4, y4, pad; };
 struct SbCount { uint32_t nBlocks, nTxb, nCoeffs, pad; };
 
@@ -44,8 +51,9 @@ struct __align__(16) FrameDesc {
     uint8_t *mYMode, *cLvl[3], *cDc[3];
     BlockRes *blk;
     uint32_t nRec;                            // analysis records (all shapes)
-    uint16_t *slMask;                         // [nRec] shortlist: modes to screen per record (bit m: mode m); null: all
-    int slRdK;                                // shortlist: RD candidates of a block whose list is not all 13 modes
+    SlCand *slCand;                           // learned shortlist of the scored records (compact order); null: none
+    int slIdx[22];                            // first compact index of each scored shape, -1 for the others
+    int slRdK;                                // RD candidates of a block with a learned shortlist
     int rdK;                                  // RD candidates of every other block (1 .. 4; the plain form: 4)
     int txKeep;                               // 0, or the tx types (best analysis cost first) a block's txMask keeps
     uint32_t shOff[22];

@@ -9,15 +9,17 @@
 
 namespace is {
 
-typedef std::conditional<IS_BD == 8, uint8_t, uint16_t>::type RcPx;
+typedef RcPxOf<IS_BD> RcPx;
+constexpr int RcNW = rc_warps_of<IS_BD, IS_SS>();
 
 template <> cudaError_t rc_upload<IS_BD, IS_SS>(const TableBlob &B) { return upload_common(B); }
 
-template <> cudaError_t rc_setup<IS_BD, IS_SS>(size_t *smem, int *ctasPerSm) {
+template <> cudaError_t rc_setup<IS_BD, IS_SS>(size_t *smem, int *ctasPerSm, int *warps) {
     const void *k = (const void *)k_recon<IS_BD, IS_SS>;
-    *smem = sizeof(RcSmem<RcPx, IS_SS>);
+    *smem = sizeof(RcSmem<RcPx, IS_SS, RcNW>);
+    *warps = RcNW;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctasPerSm, k, RC_WARPS * 32, *smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctasPerSm, k, RcNW * 32, *smem);
     return e;
 }
 
@@ -28,7 +30,7 @@ template <> cudaError_t rc_setup<IS_BD, IS_SS>(size_t *smem, int *ctasPerSm) {
 template <> cudaError_t rc_launch<IS_BD, IS_SS>(const FrameDesc *fs, int nImg, const RcCtl &ctl, int grid, size_t smem, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(RC_WARPS * 32);
+    cfg.blockDim = dim3(RcNW * 32);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];

@@ -22,10 +22,13 @@
 
 namespace is {
 
-#ifndef IS_RC_WARPS
-#define IS_RC_WARPS 4
-#endif
-constexpr int RC_WARPS = IS_RC_WARPS;      // warps per CTA (independent workers; shared memory bounds the count)
+// warps per CTA: independent workers, as many as the shared memory of one CTA per SM holds (at most 8; rc_warps below)
+constexpr int RC_MAX_WARPS = 8;
+// per-warp scratch: a task round of tx sizes up to 32 x 32 (32 / G tasks of H x (W + 1) int32: at most 16 x 80 in the
+// small sizes' single round (G >= 2, 4x16), 4 x 272 / 2 x 544 / 1 x 1056 in the others (round_group's G)) and
+// predictions up to 32 x 32 (16 x 64 in the single round); the luma of a leaf with a 64-sample side (rare: large flat
+// blocks) uses the CTA's one large buffer (RcBig) instead, under a lock
+constexpr int RC_BUF_INTS = 1280;
 // bounded waits (defaults; FrameDesc::waitIters / readyWaitNs carry the values of a run): a wait that runs out records
 // an error and moves on, and once any error is recorded no further wait starts (the host discards the result)
 constexpr int LEAF_WAIT_ITERS = 1 << 20;
@@ -36,10 +39,10 @@ constexpr int TRACE_STAMPS = 10;
 constexpr long long READY_WAIT_NS = 4000000000ll;
 
 template <typename Px, int SS> struct RcWarp {   // SS: chroma subsampling (1 4:2:0, 0 4:4:4)
-    int32_t buf[64 * 65];      // evaluation scratch (32 / G tasks) and the inverse transform's residual
+    int32_t buf[RC_BUF_INTS];  // evaluation scratch (32 / G tasks) and the inverse transform's residual (tx <= 32 x 32)
     int16_t q[1024];           // levels of the tasks of a round
     int16_t qb[2][1024];       // best levels (chroma: U, V)
-    Px pred[4096];             // predictions of the tasks (W x H per group); the final prediction
+    Px pred[1024];             // predictions of the tasks (W x H per group); the final prediction (tx <= 32 x 32)
     i64 taskJ[16];
     int predC[8];
     Px ea[3][EDGE_LEN], el[3][EDGE_LEN];
@@ -50,21 +53,35 @@ template <typename Px, int SS> struct RcWarp {   // SS: chroma subsampling (1 4:
     int cand[32];
     int job;
 };
-template <typename Px, int SS> struct RcSmem {
-    RateStage T;                         // scans, base-context offsets (and the cost table of q-context 0)
-    uint16_t cost[3][NCDF];              // the cost tables of q-contexts 1 .. 3 (the images of a batch mix qindex)
-    FrameDesc F[RC_WARPS];               // each warp's copy of the descriptor of the image it works on
-    RcWarp<Px, SS> w[RC_WARPS];
+template <typename Px> struct RcBig {   // the CTA's scratch for luma tx sizes with a 64-sample side
+    int32_t buf[64 * 65];
+    Px pred[64 * 64];
+    int lock;                           // 0 free, 1 taken
+    int pad[3];
 };
+template <typename Px, int SS, int NW> struct RcSmem {
+    RateStage T;                         // scans, base-context offsets (and the cost table of q-context 0)
+    RcBig<Px> big;
+    uint16_t cost[3][NCDF];              // the cost tables of q-contexts 1 .. 3 (the images of a batch mix qindex)
+    FrameDesc F[NW];                     // each warp's copy of the descriptor of the image it works on
+    RcWarp<Px, SS> w[NW];
+};
+// the most warps (<= RC_MAX_WARPS) whose shared memory fits one CTA (8 for 8-bit 4:2:0, fewer for the larger formats)
+template <typename Px, int SS> constexpr int rc_warps() {
+    return sizeof(RcSmem<Px, SS, 8>) <= 227 * 1024 ? 8 : sizeof(RcSmem<Px, SS, 7>) <= 227 * 1024 ? 7
+         : sizeof(RcSmem<Px, SS, 6>) <= 227 * 1024 ? 6 : sizeof(RcSmem<Px, SS, 5>) <= 227 * 1024 ? 5 : 4;
+}
 template <typename Px, int SS> constexpr bool rc_smem_ok() {
     typedef RcWarp<Px, SS> Wt;
-    typedef RcSmem<Px, SS> St;
+    typedef RcSmem<Px, SS, rc_warps<Px, SS>()> St;
     return sizeof(St) <= 227 * 1024 && offsetof(Wt, srcS) % 16 == 0 && sizeof(Wt) % 16 == 0 && offsetof(St, w) % 16 == 0 &&
            offsetof(St, cost) % 16 == 0 && offsetof(St, F) % 16 == 0;
 }
 static_assert(rc_smem_ok<uint8_t, 1>() && rc_smem_ok<uint8_t, 0>() && rc_smem_ok<uint16_t, 1>() && rc_smem_ok<uint16_t, 0>() &&
                   sizeof(FrameDesc) % 16 == 0,
               "the closed loop's shared memory: at most 227 KB, staged sources and descriptors 16-byte aligned");
+static_assert(rc_warps<uint8_t, 1>() == 8 && rc_warps<uint8_t, 0>() >= 7 && rc_warps<uint16_t, 1>() >= 6 && rc_warps<uint16_t, 0>() >= 5,
+              "closed-loop warps per CTA");
 
 // Waits poll with relaxed loads and acquire once, with a fence after the awaited value was seen (the acquire pattern of
 // the PTX memory model: a strong read that observes a release, then fence.acq_rel): one acquire per wait instead of one
@@ -319,6 +336,24 @@ static __device__ __noinline__ bool rc_wait(const FrameDesc &F, int sb, int li, 
     return ok;
 }
 
+// Take the CTA's large buffer (RcBig; its holder gives it back right after its evaluation and waits on nothing while it
+// holds it): a spin of at most F.waitIters polls.  False when it ran out or another warp reported an error (F.err set);
+// the leaf is then abandoned.
+__device__ __forceinline__ bool rc_big_lock(const FrameDesc &F, int &lock) {
+    int ok = 1;
+    if (lane_id() == 0) {
+        int it = 0;
+        while (atomicCAS(&lock, 0, 1) != 0) {
+            if (++it > F.waitIters || *(volatile int *)F.err) { ok = 0; break; }
+            __nanosleep(64);
+        }
+        if (!ok) atomicCAS(F.err, 0, KERR_WAIT_LEAF);
+        __threadfence_block();   // the buffer's previous holder is done with it
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    return ok != 0;
+}
+
 // tile box (mi units) of the 4x4 unit (mi_row, mi_col)
 __device__ __forceinline__ void tile_box(const FrameDesc &F, int mi_row, int mi_col, int &tC0, int &tC1, int &tR0, int &tR1) {
     int tc = 0, tr = 0;
@@ -397,7 +432,7 @@ __device__ __noinline__ int rc_chroma_more(const FrameDesc &F, RcWarp<Px, 0> &Wp
 }
 
 template <int BD, typename Px, int SS>
-__device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &T, int sb, int li, unsigned long long *trace) {
+__device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, RcBig<Px> &Big, const RateTabs &T, int sb, int li, unsigned long long *trace) {
     const int lane = lane_id();
     const Leaf lf = F.leaves[(size_t)sb * SB_MAX_LEAVES + li];
     const int bsize = lf.bsize;
@@ -493,6 +528,13 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
         const int srcPitch = staged ? W : F.spitch[0];
         const int set = tx_set_intra(txSz);
         const int nq = min(W, 32) * min(H, 32);
+        // scratch of the evaluation rounds, the prediction and the inverse: the warp's own, or for a tx size with a
+        // 64-sample side the CTA's large buffer, taken under its lock for the evaluation only (its holder waits on
+        // nothing until it gives it back)
+        const bool bigTx = W == 64 || H == 64;
+        if (bigTx && !rc_big_lock(F, Big.lock)) return;   // (the wait ran out: the error is recorded)
+        int32_t *lbuf = bigTx ? Big.buf : Wp.buf;
+        Px *lpred = bigTx ? Big.pred : Wp.pred;
         int16_t *best = Wp.qb[0];
         i64 bestJ = INF;
         int bestC = br.cand[0], bestT = br.tx;
@@ -502,9 +544,9 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
         // of equal costs wins); the round's winner, if it beats the best so far, leaves its levels in `best`
         auto run = [&](const int *tcand, const int *ttype, int n) {
             const int G = round_group(txSz, n), ng = 32 / G, grp = lane / G, g = lane & (G - 1);
-            int32_t *tb = Wp.buf + grp * task_buf_ints(txSz);
+            int32_t *tb = lbuf + grp * task_buf_ints(txSz);
             int16_t *tq = Wp.q + grp * nq;
-            Px *tp = Wp.pred + grp * (W * H);
+            Px *tp = lpred + grp * (W * H);
             if (G != curG) {   // the groups' cached predictions belong to another grouping
                 if (lane < 8) Wp.predC[lane] = -1;
                 __syncwarp();
@@ -556,11 +598,11 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
                 else if (k < p1 + n2a) { c = c0; ty = __fns(m0, 0, k - p1 + 1); }
                 else { c = c1; ty = __fns(m1, 0, k - p1 - n2a + 1); }
                 const int m = cand_mode(c);
-                Px *tp = Wp.pred + grp * (W * H);
+                Px *tp = lpred + grp * (W * H);
                 grp_predict(m, pangle(m, cand_delta(c)), lw, lh, A, L, dcv, tp, g, G);
                 __syncwarp();
                 const EvalIn e{ty, 0, skipCtx, dcCtx, m, F.dcQ, F.acQ, T};
-                const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{src, srcPitch, tp, lw, nullptr}, e, Wp.buf + grp * task_buf_ints(txSz),
+                const EvalOut o = grp_eval<BD, Px>(txSz, ResFn<Px>{src, srcPitch, tp, lw, nullptr}, e, lbuf + grp * task_buf_ints(txSz),
                                                    Wp.q + grp * nq, g, G);
                 if (g == 0 && grp < nt) Wp.taskJ[grp] = o.D + F.lam * (o.R + mbits(c));
             }
@@ -603,14 +645,21 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, const RateTabs &
         }
         // the winner's prediction (whole warp) for its levels (single-candidate case) and the reconstruction
         const int bm = cand_mode(bestC);
-        grp_predict(bm, pangle(bm, cand_delta(bestC)), lw, lh, A, L, dcv, Wp.pred, lane, 32);
+        grp_predict(bm, pangle(bm, cand_delta(bestC)), lw, lh, A, L, dcv, lpred, lane, 32);
         __syncwarp();
         if (!have) {
             const EvalIn e{bestT, 0, skipCtx, dcCtx, bm, F.dcQ, F.acQ, T};
-            grp_eval<BD, Px>(txSz, ResFn<Px>{src, srcPitch, Wp.pred, lw, nullptr}, e, Wp.buf, best, lane, 32);
+            grp_eval<BD, Px>(txSz, ResFn<Px>{src, srcPitch, lpred, lw, nullptr}, e, lbuf, best, lane, 32);
         }
         Px *dst = (Px *)F.rec[0] + (size_t)y * F.rpitch[0] + x;
-        rc_reconstruct<BD, Px>(txSz, bestT, best, F.dcQ, F.acQ, Wp.pred, dst, F.rpitch[0], Wp.buf);
+        rc_reconstruct<BD, Px>(txSz, bestT, best, F.dcQ, F.acQ, lpred, dst, F.rpitch[0], lbuf);
+        if (bigTx) {   // the large buffer back (the reconstruction is written; the levels are in the warp's own qb)
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                atomicExch(&Big.lock, 0);
+            }
+        }
         eobY = rc_record(F, T, sb, 0, txSz, bestT, x >> 2, y >> 2, best, txbBase, coefBase);
         yMode = bm;
         yDelta = cand_delta(bestC);
@@ -936,16 +985,20 @@ struct RcCtl {
     unsigned long long *trace;     // optional leaf trace (batch mode)
     int poison;
 };
+template <int BD> using RcPxOf = typename std::conditional<BD == 8, uint8_t, uint16_t>::type;
+template <int BD, int SS> constexpr int rc_warps_of() { return rc_warps<RcPxOf<BD>, SS>(); }
 template <int BD, int SS>
-__global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *Fs, int nImg, const RcCtl ctl) {
-    typedef typename std::conditional<BD == 8, uint8_t, uint16_t>::type Px;
+__global__ void __launch_bounds__(rc_warps_of<BD, SS>() * 32, 1) k_recon(const FrameDesc *Fs, int nImg, const RcCtl ctl) {
+    typedef RcPxOf<BD> Px;
+    constexpr int NW = rc_warps_of<BD, SS>();
+    typedef RcSmem<Px, SS, NW> Sm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    RcSmem<Px, SS> &S = *reinterpret_cast<RcSmem<Px, SS> *>(smem_raw);
+    Sm &S = *reinterpret_cast<Sm *>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = lane_id();
     RcWarp<Px, SS> &Wp = S.w[warp];
     FrameDesc &F = S.F[warp];
     if (ctl.poison) {
-        smem_poison(smem_raw, sizeof(RcSmem<Px, SS>), threadIdx.x, blockDim.x);
+        smem_poison(smem_raw, sizeof(Sm), threadIdx.x, blockDim.x);
         __syncthreads();
     }
     {   // all four cost tables (q-context 0 in the RateStage), the scans and base-context offsets
@@ -955,6 +1008,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *Fs,
             for (int i = threadIdx.x; i < NCDF / 8; i += blockDim.x) reinterpret_cast<uint4 *>(S.cost[q - 1])[i] = c[i];
         }
     }
+    if (threadIdx.x == 0) S.big.lock = 0;
     __syncthreads();
     int *rq = ctl.rq;
     const unsigned long long *readyQ = ctl.readyQ;
@@ -1029,7 +1083,7 @@ __global__ void __launch_bounds__(RC_WARPS * 32, 1) k_recon(const FrameDesc *Fs,
         }
         const RateTabs T{F.qctx == 0 ? S.T.cost : S.cost[F.qctx - 1], S.T.scan, S.T.baseCtx};
         unsigned long long *trace = traceBase ? traceBase + (size_t)h * TRACE_STAMPS : nullptr;
-        rc_leaf<BD, Px, SS>(F, Wp, T, (int)(id >> 8), (int)(id & 255), trace);
+        rc_leaf<BD, Px, SS>(F, Wp, S.big, T, (int)(id >> 8), (int)(id & 255), trace);
     }
 }
 

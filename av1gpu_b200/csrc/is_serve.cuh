@@ -23,7 +23,7 @@ struct ServeSlot {
 };
 
 struct ServeSession {
-    int bd = 8, c444 = 0, g = 0, grid = 0;
+    int bd = 8, c444 = 0, g = 0, grid = 0, warps = 0;   // format, its group; the loop's CTAs and warps per CTA
     uint8_t *arena = nullptr;
     size_t arenaBytes = 0;
     std::vector<std::pair<size_t, size_t>> freeList;   // (offset, bytes), sorted by offset
@@ -131,7 +131,8 @@ int is_serve_open(is_handle *h, int bit_depth, int chroma_444, uint64_t arena_by
     S->arenaBytes = align256(arena_bytes);
     // queue positions: the leaves of every image the session will take, plus the slots idle workers give up (one per
     // worker each time the loop ends; max_leaves covers both, submit checks the leaves' share)
-    S->queueCap = (size_t)max_leaves + (size_t)S->grid * RC_WARPS + 64;
+    S->warps = h->rcWarpsG[S->g];
+    S->queueCap = (size_t)max_leaves + (size_t)S->grid * S->warps + 64;
     S->slots.resize(max_images);
     IS_SCK(cudaMalloc(&S->arena, S->arenaBytes));
     S->freeList.push_back(std::make_pair((size_t)0, S->arenaBytes));
@@ -235,7 +236,7 @@ int is_serve_submit(is_handle *h, const is_frame *f, int from_host, int *ticket)
     IS_CK(cudaMemcpyAsync(S->hErr + 4, S->dCtl, 8, cudaMemcpyDeviceToHost, S->pst));
     IS_CK(cudaStreamSynchronize(S->pst));
     taken = std::max<int64_t>(S->hErr[4], S->hErr[5]);
-    if ((size_t)taken + S->inflightLeaves + (size_t)maxLeaves + 2 * (size_t)S->grid * RC_WARPS + 64 > S->queueCap)
+    if ((size_t)taken + S->inflightLeaves + (size_t)maxLeaves + 2 * (size_t)S->grid * S->warps + 64 > S->queueCap)
         return h->setErr(IS_ERR_STATE, "the session's queue positions are used up (close and open a new session)");
     size_t off = 0;
     if (!serve_alloc(S, bytes, &off)) return h->setErr(IS_ERR_BUSY, "no free workspace range of %zu bytes", bytes);
@@ -261,7 +262,7 @@ int is_serve_submit(is_handle *h, const is_frame *f, int from_host, int *ticket)
     F.leafDoneCnt = F.queue + 3;
     F.doneFlag = S->dFlags + slot;
     F.leafTrace = nullptr;
-    if (!h->slOn) F.slMask = nullptr;
+    if (!h->slOn) F.slCand = nullptr;
     F.slRdK = h->slOn ? h->slRdK : 4;
     F.rdK = h->rdK;
     F.txKeep = h->txKeep;

@@ -144,7 +144,7 @@ int is_test_predict(is_handle *h, int n, const uint8_t *plane, int w, int hgt, c
     return rc;
 }
 
-int is_debug_analysis(is_handle *h, int bs, int64_t *J, uint8_t *cand, uint8_t *ncand, uint8_t *tx) {
+int is_debug_analysis(is_handle *h, int bs, int64_t *J, uint8_t *cand, uint8_t *ncand, uint8_t *tx, uint16_t *tx_mask) {
     if (!h || !h->have || bs < 0 || bs >= 22) return IS_ERR_STATE;
     const FrameDesc &F = h->F;
     const size_t n = (size_t)F.shNbx[bs] * F.shNby[bs];
@@ -156,6 +156,7 @@ int is_debug_analysis(is_handle *h, int bs, int64_t *J, uint8_t *cand, uint8_t *
         if (cand) memcpy(cand + 4 * i, v[i].cand, 4);
         if (ncand) ncand[i] = v[i].ncand;
         if (tx) tx[i] = v[i].tx;
+        if (tx_mask) tx_mask[i] = v[i].txMask;
     }
     return (int)n;
 }

@@ -296,12 +296,8 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem<Px
     uint32_t topP[4][NWD];
 #pragma unroll
     for (int k = 0; k < 4; k++) { topJ[k] = INF; topM[k] = 0; }
-    // the modes screened: all 13, or the block's learned shortlist; a mode no thread of the warp screens is skipped
-    const uint32_t mmask = F.slMask ? F.slMask[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] : 0x1FFFu;
     auto screen = [&](auto modeTag) {
         constexpr int M = decltype(modeTag)::value;
-        const bool need = (mmask >> M) & 1;
-        if (!__any_sync(__activemask(), need)) return;
         int p[N];
         tpred<W, H, M>(A, L, dcv, p);
         int satd = 0;
@@ -325,8 +321,8 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem<Px
             for (int u = 0; u < PPW; u++) v |= (uint32_t)p[PPW * k + u] << (PB * u);
             pk[k] = v;
         }
-        // insertion: after every kept entry of cost <= js (the earlier candidate wins a tie); none for a mode off the list
-        const int pos = need ? (topJ[0] <= js) + (topJ[1] <= js) + (topJ[2] <= js) + (topJ[3] <= js) : 4;
+        // insertion: after every kept entry of cost <= js (the earlier candidate wins a tie)
+        const int pos = (topJ[0] <= js) + (topJ[1] <= js) + (topJ[2] <= js) + (topJ[3] <= js);
 #pragma unroll
         for (int s = 3; s >= 0; s--) {
             if (s > pos) {
@@ -369,7 +365,7 @@ __device__ __forceinline__ void tiny_block(const FrameDesc &F, const TinySmem<Px
     };
     i64 bestJ = INF;
     int bestK = 0, bestTx = AV1G_DCT_DCT;
-    const int kMax = mmask != 0x1FFFu ? F.slRdK : F.rdK;   // a shortlisted block: its best slRdK candidates only
+    const int kMax = F.rdK;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         if (topJ[k] == INF || k >= kMax) continue;   // fewer candidates screened or taken (shortlist)
@@ -593,17 +589,24 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem<Px> &S, co
     int b0 = AV1G_V_PRED, b1 = AV1G_V_PRED;
     i64 bestJ = INF;
     int bestK = 0, bestTx = AV1G_DCT_DCT, winC = 0;
-    // the modes screened: all 13, or the block's learned shortlist
-    const uint32_t mmask = F.slMask ? F.slMask[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] : 0x1FFFu;
-    const int kMax = mmask != 0x1FFFu ? F.slRdK : F.rdK;   // a shortlisted block: its best slRdK candidates only
+    // a block with a learned shortlist screens its (mode, delta) list (most probable first) instead of the 13 modes and
+    // the deltas, and tries only its list's tx types
+    const SlCand *slc = (F.slCand && F.slIdx[bs] >= 0) ? F.slCand + F.slIdx[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW) : nullptr;
+    const uint2 slw = slc ? *reinterpret_cast<const uint2 *>(slc->c) : make_uint2(0u, 0u);
+    const int nsl = slc ? slc->n : 0;
+    const uint32_t slTx = slc ? slc->txMask : 0u;
+    const int kMax = nsl > 0 ? F.slRdK : F.rdK;
     TxRank rank;   // the winner's types by cost (txKeep)
-    // jobs: 0-12 the 13 modes, 13-24 the deltas of the two best directional modes (SATD); 25-28 the top 4 with
-    // DCT_DCT, 29-34 the other types of TX_SET_INTRA_1 for the winner (RD); a job no thread of the warp needs is skipped
+    // jobs: 0-12 the 13 modes (a shortlisted block: its list's entries 0-7), 13-24 the deltas of the two best
+    // directional modes (SATD); 25-28 the top 4 with DCT_DCT, 29-34 the other types of TX_SET_INTRA_1 for the winner (a
+    // shortlisted block: the types of its list, in type order) (RD); a job no thread of the warp needs is skipped
 #pragma unroll 1
     for (int job = 0; job < 35; job++) {
         int c, t = AV1G_DCT_DCT;
+        bool need;
         if (job < 13) {
-            c = cand_pack(job, 0);
+            c = nsl > 0 ? (int)(((job < 4 ? slw.x >> (8 * job) : slw.y >> (8 * (job - 4)))) & 0xFFu) : cand_pack(job, 0);
+            need = nsl > 0 ? job < nsl && job < 8 : true;
         } else if (job < 25) {
             const int k = job - 13, kk = k % 6;
             c = cand_pack(k < 6 ? b0 : b1, kk < 3 ? -(kk + 1) : kk - 2);
@@ -616,10 +619,15 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem<Px> &S, co
             c = winC;
             const int k = job - 29;   // ADST_DCT, DCT_ADST, ADST_ADST, IDTX, V_DCT, H_DCT
             t = k < 3 ? k + 1 : k + 6;
+            if (slTx) {   // the k-th type of the list beyond DCT_DCT
+                const uint32_t m = slTx & ~1u;
+                t = k < __popc(m) ? (int)__fns(m, 0, k + 1) : -1;
+            }
         }
-        const bool need = job < 13 ? ((mmask >> job) & 1) != 0 : job < 25 ? ((job - 13 < 6) ? dJ0 < INF : dJ1 < INF)
-                         : job < 29 ? (topJ[job - 25] < INF && job - 25 < kMax) : true;
+        if (job >= 13)
+            need = job < 25 ? ((job - 13 < 6) ? dJ0 < INF : dJ1 < INF) : job < 29 ? (topJ[job - 25] < INF && job - 25 < kMax) : t >= 0;
         if (!__any_sync(__activemask(), need)) continue;
+        if (t < 0) t = AV1G_DCT_DCT;   // (a thread past its list's types: its result is not used)
         const int m = cand_mode(c), pa = pangle(m, cand_delta(c));
         // the prediction, one 4x4 sub-block at a time (one copy of the predictor): SATD of the residual while screening,
         // the prediction into the thread's slot for an RD task
@@ -650,7 +658,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem<Px> &S, co
                 if (s > pos) { topJ[s] = topJ[s > 0 ? s - 1 : 0]; topC[s] = topC[s > 0 ? s - 1 : 0]; }
                 else if (s == pos) { topJ[s] = js; topC[s] = c; }
             }
-            if (need && job >= AV1G_V_PRED && job <= AV1G_D67_PRED) {   // the two best directional modes (first of equals)
+            if (need && nsl == 0 && job >= AV1G_V_PRED && job <= AV1G_D67_PRED) {   // the two best directional modes (first of equals)
                 if (js < dJ0) { dJ1 = dJ0; b1 = b0; dJ0 = js; b0 = job; }
                 else if (js < dJ1) { dJ1 = js; b1 = job; }
             }
@@ -672,6 +680,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem<Px> &S, co
             }
         }
     }
+    if (rank.j[0] >= INF) rank.add(bestJ, bestTx);   // no type job ran for this block: its own type only
     BlockRes r;
     r.J = bestJ;
     r.tx = (uint8_t)bestTx;
@@ -682,7 +691,7 @@ __device__ __forceinline__ void mid_block(const FrameDesc &F, MidSmem<Px> &S, co
     for (int k = 0; k < 4; k++)
         if (k != bestK && topJ[k] < INF && k < kMax) r.cand[n++ & 3] = (uint8_t)topC[k];
     r.ncand = (uint8_t)n;
-    r.txMask = rank.mask(F.txKeep);
+    r.txMask = F.txKeep ? rank.mask(F.txKeep) : (uint16_t)slTx;
     F.blk[F.shOff[bs] + (uint32_t)(y >> LH) * F.shNbx[bs] + (x >> LW)] = r;
 }
 

@@ -52,7 +52,7 @@ template <int BD, int PART> cudaError_t an_launch(const FrameDesc &F, int nSb, c
 // ---- closed-loop unit (is_k_rc.cu, BD 8 / 10 x SS 1 (4:2:0) / 0 (4:4:4)) ----
 template <int BD, int SS> cudaError_t rc_upload(const TableBlob &B);
 // shared memory of the kernel and its co-resident CTAs per SM (the cooperative grid is that times the SM count)
-template <int BD, int SS> cudaError_t rc_setup(size_t *smem, int *ctasPerSm);
+template <int BD, int SS> cudaError_t rc_setup(size_t *smem, int *ctasPerSm, int *warps);
 struct RcCtl;
 template <int BD, int SS> cudaError_t rc_launch(const FrameDesc *fs, int nImg, const RcCtl &ctl, int grid, size_t smem, cudaStream_t st);
 

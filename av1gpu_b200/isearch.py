@@ -55,8 +55,9 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_record_copy", "is_record_device", "is_times_get", "is_test_fwd_quant", "is_test_inverse",
            "is_test_predict", "is_debug_analysis", "is_debug_leaves", "is_debug_tables", "is_probe_int32", "is_set_trace", "is_get_trace",
            "is_fwd_quant_static", "is_encode_batch", "is_batch_counts", "is_batch_copy", "is_set_batch_options",
-           "is_autotune_batch", "is_workspace_bytes", "is_workspace_bytes_format", "is_sl_create", "is_sl_destroy", "is_sl_set_weights",
-           "is_sl_get_weights", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset", "is_set_shortlist_model",
+           "is_autotune_batch", "is_workspace_bytes", "is_workspace_bytes_format", "is_sl_create", "is_sl_destroy", "is_sl_set_params",
+           "is_sl_get_params", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset", "is_sl_infer",
+           "is_set_shortlist_model",
            "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison", "is_set_search_options", "is_serve_open", "is_serve_start", "is_serve_submit", "is_serve_poll",
            "is_serve_counts", "is_serve_copy", "is_serve_stop", "is_serve_close"]
 
@@ -86,7 +87,7 @@ def load_library():
     L.is_test_fwd_quant.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp]
     L.is_test_inverse.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, vp]
     L.is_test_predict.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, vp, vp]
-    L.is_debug_analysis.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+    L.is_debug_analysis.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
     L.is_debug_leaves.argtypes = [vp, C.c_uint32, vp, vp, vp]
     L.is_debug_tables.argtypes = [vp, C.c_int, vp, C.c_size_t, vp, vp, vp, C.c_int, C.POINTER(C.c_int64),
                                   C.POINTER(C.c_int64)]
@@ -103,14 +104,15 @@ def load_library():
     L.is_sl_create.argtypes = [C.c_int, C.c_int, C.POINTER(vp)]
     L.is_sl_destroy.argtypes = [vp]
     L.is_sl_destroy.restype = None
-    L.is_sl_set_weights.argtypes = [vp, vp, vp, vp, vp]
-    L.is_sl_get_weights.argtypes = [vp, vp, vp, vp, vp]
+    L.is_sl_set_params.argtypes = [vp, vp]
+    L.is_sl_get_params.argtypes = [vp, vp]
     L.is_sl_forward.argtypes = [vp, vp, C.c_int, vp, vp]
     L.is_sl_grads.argtypes = [vp, vp, vp, C.c_int, vp, C.POINTER(C.c_float), C.POINTER(C.c_int)]
     L.is_sl_train_step.argtypes = [vp, vp, vp, C.c_int, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_int)]
     L.is_nn_gemm.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, vp]
     L.is_sl_dataset.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int)]
-    L.is_set_shortlist_model.argtypes = [vp, vp, vp, vp, vp, C.c_float, C.c_int, C.c_float, C.c_int]
+    L.is_sl_infer.argtypes = [vp, vp, C.c_int, vp, C.c_int, C.POINTER(C.c_int)]
+    L.is_set_shortlist_model.argtypes = [vp, vp, C.c_float, C.c_int, C.c_float, C.c_int, C.c_float, C.c_int]
     L.is_autotune_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
     L.is_set_wait_limits.argtypes = [vp, C.c_int, C.c_longlong]
     L.is_set_workspace_limit.argtypes = [vp, C.c_uint64]
@@ -394,15 +396,19 @@ class Encoder:
         self._check(self.L.is_set_batch_options(self.h, 1 if use_graph else 0, front_streams, recon_ctas),
                     "is_set_batch_options")
 
-    def set_shortlist(self, weights=None, tau=0.9, max_modes=6, conf=0.0, rd_k=4):
-        """Use a trained shortlist network (w1, b1, w2, b2 fp32) in this handle's searches; None: the plain form."""
-        if weights is None:
-            self._check(self.L.is_set_shortlist_model(self.h, None, None, None, None, C.c_float(1.0), 0, C.c_float(0.0), 4),
+    def set_shortlist(self, params=None, tau=0.9, max_cand=8, conf=0.0, rd_k=2, tx_tau=0.9, max_tx=2):
+        """Use a trained shortlist network (IS_SL_PARAMS fp32 parameters) in this handle's searches; None: the plain
+        form.  Candidates per scored block: the most probable (mode, delta) pairs covering tau (at most max_cand), the
+        best rd_k of them by SATD into the RD, the tx types covering tx_tau (at most max_tx); blocks whose top
+        probability is below conf search in full."""
+        if params is None:
+            self._check(self.L.is_set_shortlist_model(self.h, None, C.c_float(1.0), 1, C.c_float(0.0), 4, C.c_float(1.0), 0),
                         "is_set_shortlist_model")
             return
-        w = [np.ascontiguousarray(a, np.float32) for a in weights]
-        self._check(self.L.is_set_shortlist_model(self.h, *[a.ctypes.data for a in w], C.c_float(tau), max_modes,
-                                                  C.c_float(conf), rd_k), "is_set_shortlist_model")
+        p = np.ascontiguousarray(params, np.float32).ravel()
+        self._keep_params = p
+        self._check(self.L.is_set_shortlist_model(self.h, p.ctypes.data, C.c_float(tau), max_cand, C.c_float(conf), rd_k,
+                                                  C.c_float(tx_tau), max_tx), "is_set_shortlist_model")
 
     def autotune_batch(self, images, qindices, host=True):
         """Time the batch with 1 / 2 / 4 front-end streams and keep the fastest; returns (streams, ms)."""
@@ -443,14 +449,15 @@ class Encoder:
                                            params.ctypes.data, out.ctypes.data), "is_test_predict")
         return out
 
-    def debug_analysis(self, bsize):
-        n = self.L.is_debug_analysis(self.h, bsize, None, None, None, None)
+    def debug_analysis(self, bsize, tx_mask=False):
+        """Analysis records of one shape of the last encode: J, cand [n x 4], ncand, tx (and the closed loop's tx masks)."""
+        n = self.L.is_debug_analysis(self.h, bsize, None, None, None, None, None)
         if n < 0:
             raise RuntimeError("is_debug_analysis failed")
         J, cand = np.zeros(n, np.int64), np.zeros((n, 4), np.uint8)
-        nc, tx = np.zeros(n, np.uint8), np.zeros(n, np.uint8)
-        self.L.is_debug_analysis(self.h, bsize, J.ctypes.data, cand.ctypes.data, nc.ctypes.data, tx.ctypes.data)
-        return J, cand, nc, tx
+        nc, tx, tm = np.zeros(n, np.uint8), np.zeros(n, np.uint8), np.zeros(n, np.uint16)
+        self.L.is_debug_analysis(self.h, bsize, J.ctypes.data, cand.ctypes.data, nc.ctypes.data, tx.ctypes.data, tm.ctypes.data)
+        return (J, cand, nc, tx, tm) if tx_mask else (J, cand, nc, tx)
 
     def set_trace(self, on=True):
         self._check(self.L.is_set_trace(self.h, 1 if on else 0), "is_set_trace")

@@ -59,8 +59,8 @@ def latency_stats(requests):
 
 class Server:
     def __init__(self, device=0, hbm_budget=None, pipelines=2, max_batch=64, recon_ctas=0, use_graph=False, shortlist=None):
-        """shortlist: None (plain search) or a dict of Encoder.set_shortlist's arguments (weights, tau, max_modes, conf,
-        rd_k)."""
+        """shortlist: None (plain search) or a dict of Encoder.set_shortlist's arguments (params, tau, max_cand, conf, rd_k,
+        tx_tau, max_tx)."""
         from .isearch import Encoder, workspace_bytes, plane_format
         import torch
 
@@ -279,14 +279,18 @@ def main():
                     help="stream: continuous admission into running closed loops (is_serve_*); batch: batches per worker")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "shortlist_weights.npz"))
     ap.add_argument("--tau", type=float, default=0.9)
-    ap.add_argument("--max-modes", type=int, default=6)
+    ap.add_argument("--max-cand", type=int, default=8)
+    ap.add_argument("--conf", type=float, default=0.0)
     ap.add_argument("--rd-k", type=int, default=2)
+    ap.add_argument("--tx-tau", type=float, default=0.9)
+    ap.add_argument("--max-tx", type=int, default=2)
     args = ap.parse_args()
     reqs = _requests(args.n, 5)
     sl = None
     if not args.plain:
-        from .shortlist import load_weights
-        sl = {"weights": load_weights(args.weights), "tau": args.tau, "max_modes": args.max_modes, "rd_k": args.rd_k}
+        from .shortlist import load_params
+        sl = {"params": load_params(args.weights), "tau": args.tau, "max_cand": args.max_cand, "conf": args.conf, "rd_k": args.rd_k,
+              "tx_tau": args.tx_tau, "max_tx": args.max_tx}
     modes = ["stream", "batch"] if args.mode == "both" else [args.mode]
     for mode in modes:
         if mode == "stream":
@@ -300,7 +304,8 @@ def main():
                 done = srv.run([(float(ti), p, q) for ti, (p, q) in zip(t, reqs)])
                 mp = sum(r.pixels for r in done) / 1e6
                 span = max(r.t_done for r in done) - min(r.t_arrive for r in done)
-                form = "plain" if args.plain else "batched + shortlist (tau %g, max %d modes, rd_k %d)" % (args.tau, args.max_modes, args.rd_k)
+                form = "plain" if args.plain else ("batched + learned shortlist (tau %g, max %d candidates, conf %g, rd_k %d, tx tau %g, max %d tx)"
+                                                   % (args.tau, args.max_cand, args.conf, args.rd_k, args.tx_tau, args.max_tx))
                 line = {"form": form + (", continuous admission" if mode == "stream" else ", batches per worker"),
                         "arrival_rate_per_s": rate, "requests": len(done), "mp": round(mp, 1), "mp_per_s": round(mp / span, 2),
                         "batches": len({r.batch for r in done}), **latency_stats(done)}

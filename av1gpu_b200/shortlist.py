@@ -1,10 +1,12 @@
-"""Learned mode shortlist: dataset from the search, training with the library's BF16 tensor-core kernels, evaluation.
+"""Learned shortlist: dataset from the search, training with the library's BF16 tensor-core kernels, evaluation.
 
-The network (include/is_api.h, is_sl_*) maps 288 per-block features to scores over the 13 intra modes.  Labels are
-the exhaustive search's own choices (the best mode of each analysed block), so the network learns which modes the
-full search keeps.  Used in the search (`Encoder.set_shortlist`), it restricts the screened modes of a block to the
-smallest most-probable set covering a probability `tau` (at most `max_modes`), and falls back to all 13 modes when
-its top probability is below `conf`.
+The network (include/is_api.h, is_sl_*) maps a block's 32 x 32 luma patch and 32 extras (gradient-orientation
+histogram, shape, qindex) through three 3x3 convolutions and two fully connected layers to 80 scores: 61 (mode, angle
+delta) classes and 16 tx types.  Labels are the exhaustive search's own choices (the analysis' best (mode, delta) of
+each scored block and its tx type), so the network learns which candidates the full search keeps.  Used in the search
+(`Encoder.set_shortlist`), it replaces a block's SATD screening of 13 modes and 12 angle deltas by its most probable
+(mode, delta) candidates and its tx-type search by the most probable types; blocks whose top probability is below
+`conf` keep the full search.
 """
 import ctypes as C
 
@@ -12,16 +14,37 @@ import numpy as np
 
 from .isearch import load_library
 
-N_IN, N_HID, N_OUT, N_MODES = 288, 128, 16, 13
-SHAPES = (N_HID * N_IN, N_HID, N_OUT * N_HID, N_OUT)
+N_FEAT, N_OUT, N_MD, TX0 = 1056, 80, 61, 64
+C1, C2, C3, HID, NZ = 8, 16, 16, 160, 288
+SHAPES = (("c1w", (C1, 9)), ("c1b", (C1,)), ("c2w", (C2, 9 * C1)), ("c2b", (C2,)), ("c3w", (C3, 9 * C2)), ("c3b", (C3,)),
+          ("f1w", (HID, NZ)), ("f1b", (HID,)), ("f2w", (N_OUT, HID)), ("f2b", (N_OUT,)))
+N_PARAMS = sum(int(np.prod(s)) for _, s in SHAPES)
+# (mode, delta) class k -> candidate code (mode << 3 | delta + 3), as the library numbers them
+CLASS_CAND = np.array([(0 << 3 | 3), (9 << 3 | 3), (10 << 3 | 3), (11 << 3 | 3), (12 << 3 | 3)]
+                      + [(1 + (k // 7)) << 3 | (k % 7) for k in range(56)], np.int32)
 
 
-def init_weights(seed=0):
-    """He-initialised fp32 weights (w1 [128 x 288], b1, w2 [16 x 128], b2), seeded."""
+def init_params(seed=0):
+    """He-initialised parameters (flat fp32, the library's order), seeded; biases 0."""
     rng = np.random.default_rng(seed)
-    w1 = (rng.standard_normal((N_HID, N_IN)) * np.sqrt(2.0 / N_IN)).astype(np.float32)
-    w2 = (rng.standard_normal((N_OUT, N_HID)) * np.sqrt(1.0 / N_HID)).astype(np.float32)
-    return w1, np.zeros(N_HID, np.float32), w2, np.zeros(N_OUT, np.float32)
+    parts = []
+    for name, shp in SHAPES:
+        if name.endswith("b"):
+            parts.append(np.zeros(shp, np.float32))
+        else:
+            fan_in = shp[1]
+            scale = np.sqrt((1.0 if name == "f2w" else 2.0) / fan_in)
+            parts.append((rng.standard_normal(shp) * scale).astype(np.float32))
+    return np.concatenate([p.ravel() for p in parts])
+
+
+def unpack(p):
+    out, o = {}, 0
+    for name, shp in SHAPES:
+        n = int(np.prod(shp))
+        out[name] = p[o:o + n].reshape(shp)
+        o += n
+    return out
 
 
 def _vp(t):
@@ -29,7 +52,7 @@ def _vp(t):
 
 
 class Learner:
-    """The device-side network: weights, Adam state and training buffers (is_sl_create)."""
+    """The device-side network: master weights, Adam state and training buffers (is_sl_create)."""
 
     def __init__(self, device=0, max_batch=4096):
         self.L = load_library()
@@ -44,41 +67,39 @@ class Learner:
             self.L.is_sl_destroy(self.h)
             self.h = None
 
-    def set_weights(self, w):
-        w = [np.ascontiguousarray(a, np.float32) for a in w]
-        rc = self.L.is_sl_set_weights(self.h, *[a.ctypes.data for a in w])
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == N_PARAMS
+        rc = self.L.is_sl_set_params(self.h, p.ctypes.data)
         if rc != 0:
-            raise RuntimeError("is_sl_set_weights failed (%d)" % rc)
+            raise RuntimeError("is_sl_set_params failed (%d)" % rc)
 
-    def get_weights(self):
-        w = [np.zeros((N_HID, N_IN), np.float32), np.zeros(N_HID, np.float32), np.zeros((N_OUT, N_HID), np.float32),
-             np.zeros(N_OUT, np.float32)]
-        rc = self.L.is_sl_get_weights(self.h, *[a.ctypes.data for a in w])
+    def get_params(self):
+        p = np.zeros(N_PARAMS, np.float32)
+        rc = self.L.is_sl_get_params(self.h, p.ctypes.data)
         if rc != 0:
-            raise RuntimeError("is_sl_get_weights failed (%d)" % rc)
-        return w
+            raise RuntimeError("is_sl_get_params failed (%d)" % rc)
+        return p
 
     def forward(self, X):
-        """Scores (torch float32, n x 16) of feature rows X (torch bf16 CUDA, n x 288)."""
+        """Scores (torch float32, n x 80) of feature rows X (torch bf16 CUDA, n x 1056), in chunks of the capacity."""
         import torch
         S = torch.empty((X.shape[0], N_OUT), dtype=torch.float32, device=X.device)
-        rc = self.L.is_sl_forward(self.h, _vp(X), X.shape[0], C.c_void_p(S.data_ptr()), None)
-        if rc != 0:
-            raise RuntimeError("is_sl_forward failed (%d)" % rc)
+        for b0 in range(0, X.shape[0], self.cap):
+            Xb = X[b0:b0 + self.cap].contiguous()
+            rc = self.L.is_sl_forward(self.h, _vp(Xb), Xb.shape[0], C.c_void_p(S[b0:].data_ptr()), None)
+            if rc != 0:
+                raise RuntimeError("is_sl_forward failed (%d)" % rc)
         torch.cuda.synchronize()
         return S
 
     def grads(self, X, y):
-        g = np.zeros(sum(SHAPES), np.float32)
+        g = np.zeros(N_PARAMS, np.float32)
         loss, corr = C.c_float(), C.c_int()
         rc = self.L.is_sl_grads(self.h, _vp(X), _vp(y), X.shape[0], g.ctypes.data, C.byref(loss), C.byref(corr))
         if rc != 0:
             raise RuntimeError("is_sl_grads failed (%d)" % rc)
-        out, o = [], 0
-        for shp, n in zip(((N_HID, N_IN), (N_HID,), (N_OUT, N_HID), (N_OUT,)), SHAPES):
-            out.append(g[o:o + n].reshape(shp))
-            o += n
-        return out, loss.value, corr.value
+        return g, loss.value, corr.value
 
     def train_step(self, X, y, lr):
         loss, corr = C.c_float(), C.c_int()
@@ -88,22 +109,33 @@ class Learner:
         return loss.value, corr.value
 
 
+def image_rows(enc, i=0, keep_outside=False):
+    """Feature rows (torch bf16, n x 1056, CUDA) and labels (torch int32, n x 3) of image i of the encoder's last
+    search (its scored blocks in the library's compact order; with keep_outside the rows of records outside the frame
+    stay, with class -1)."""
+    import torch
+    n = C.c_int()
+    enc.L.is_sl_dataset(enc.h, i, None, None, 0, C.byref(n))
+    X = torch.empty((n.value, N_FEAT), dtype=torch.bfloat16, device="cuda")
+    y = torch.empty((n.value, 3), dtype=torch.int32, device="cuda")
+    rc = enc.L.is_sl_dataset(enc.h, i, _vp(X), _vp(y), n.value, C.byref(n))
+    if rc != 0:
+        raise RuntimeError("is_sl_dataset failed (%d)" % rc)
+    if not keep_outside:
+        keep = y[:, 0] >= 0
+        X, y = X[keep], y[keep]
+    return X, y
+
+
 def dataset(enc, images, qindices, per_image=0, seed=0):
-    """Features (torch bf16, n x 288, CUDA) and labels (torch int32) of the analysed blocks of the images, each
-    searched with the plain form (the labels are its choices): every block, or per_image blocks drawn at random
-    (seeded) from each image's."""
+    """Feature rows and labels of the scored blocks of the images, each searched with the plain form (the labels are its
+    choices): every block, or per_image blocks drawn at random (seeded) from each image's."""
     import torch
     g = torch.Generator(device="cpu").manual_seed(seed)
     xs, ys = [], []
     for planes, q in zip(images, qindices):
         enc.encode(planes, q)
-        n = C.c_int()
-        enc.L.is_sl_dataset(enc.h, 0, None, None, 0, C.byref(n))
-        X = torch.empty((n.value, N_IN), dtype=torch.bfloat16, device="cuda")
-        y = torch.empty(n.value, dtype=torch.int32, device="cuda")
-        rc = enc.L.is_sl_dataset(enc.h, 0, _vp(X), _vp(y), n.value, C.byref(n))
-        if rc != 0:
-            raise RuntimeError("is_sl_dataset failed (%d)" % rc)
+        X, y = image_rows(enc)
         if per_image and X.shape[0] > per_image:
             idx = torch.randperm(X.shape[0], generator=g)[:per_image].to(X.device)
             X, y = X[idx], y[idx]
@@ -112,8 +144,9 @@ def dataset(enc, images, qindices, per_image=0, seed=0):
     return torch.cat(xs), torch.cat(ys)
 
 
-def train(learner, X, y, epochs=4, batch=4096, lr=2e-3, seed=0, log=None):
-    """Adam over shuffled mini-batches (the tail that does not fill a batch of a multiple of 32 is dropped)."""
+def train(learner, X, y, epochs=4, batch=4096, lr=2e-3, seed=0, log=None, lr_decay=1.0):
+    """Adam over shuffled mini-batches (the tail that does not fill a batch is dropped); the learning rate is multiplied
+    by lr_decay after each epoch."""
     import torch
     g = torch.Generator(device="cpu").manual_seed(seed)
     n = X.shape[0]
@@ -129,33 +162,50 @@ def train(learner, X, y, epochs=4, batch=4096, lr=2e-3, seed=0, log=None):
             tn += batch
         hist.append((tl / max(tn, 1), tc / max(tn, 1)))
         if log:
-            log("epoch %d: loss %.4f top-1 %.3f" % (ep, hist[-1][0], hist[-1][1]))
+            log("epoch %d: loss %.4f top-1 %.3f (lr %.2e)" % (ep, hist[-1][0], hist[-1][1], lr))
+        lr *= lr_decay
     return hist
 
 
-def evaluate(learner, X, y, tau=0.9, max_modes=6, conf=0.0):
-    """Top-1 accuracy, how often the label falls in the shortlist mask, the mean mask size, and the fallback rate (the
-    blocks whose top probability is below conf: searched in full)."""
+def select(S, y_valid, tau=0.9, max_cand=8, conf=0.0, tx_tau=0.9, max_tx=2):
+    """The library's selection rule on scores S (torch, n x 80): the candidate mask over the 61 classes, the fallback
+    rows, and the tx mask over the 16 types (within each row's set y_valid)."""
     import torch
-    accs, cover, size, n, fb = 0, 0, 0, 0, 0
-    for b0 in range(0, X.shape[0], learner.cap):
-        Xb, yb = X[b0:b0 + learner.cap].contiguous(), y[b0:b0 + learner.cap]
-        S = learner.forward(Xb)[:, :N_MODES]
-        p = torch.softmax(S, dim=1)
-        order = torch.argsort(p, dim=1, descending=True)
-        ps = torch.gather(p, 1, order)
-        keep = (torch.cumsum(ps, 1) - ps) < tau
-        keep[:, max_modes:] = False
-        low = ps[:, 0] < conf
-        keep[low] = True
-        fb += int(low.sum())
-        mask = torch.zeros_like(keep)
-        mask.scatter_(1, order, keep)
-        accs += int((order[:, 0] == yb.long()).sum())
-        cover += int(mask.gather(1, yb.long()[:, None]).sum())
-        size += int(mask.sum())
-        n += Xb.shape[0]
-    return {"top1": accs / n, "coverage": cover / n, "mean_modes": size / n, "fallback": fb / n}
+    p = torch.softmax(S[:, :N_MD], dim=1)
+    order = torch.argsort(p, dim=1, descending=True, stable=True)
+    ps = torch.gather(p, 1, order)
+    keep = (torch.cumsum(ps, 1) - ps) < tau
+    keep[:, max_cand:] = False
+    fb = ps[:, 0] < conf
+    mask = torch.zeros_like(keep)
+    mask.scatter_(1, order, keep)
+    bits = ((y_valid[:, None].long() >> torch.arange(16, device=S.device)[None, :]) & 1).bool()
+    t = S[:, TX0:TX0 + 16].masked_fill(~bits, float("-inf"))
+    q = torch.softmax(t, dim=1).nan_to_num(0.0)
+    torder = torch.argsort(q, dim=1, descending=True, stable=True)
+    qs = torch.gather(q, 1, torder)
+    tkeep = ((torch.cumsum(qs, 1) - qs) < tx_tau) & (qs > 0)
+    tkeep[:, max_tx:] = False
+    tmask = torch.zeros_like(tkeep)
+    tmask.scatter_(1, torder, tkeep)
+    return mask, fb, tmask
+
+
+def evaluate(learner, X, y, tau=0.9, max_cand=8, conf=0.0, tx_tau=0.9, max_tx=2):
+    """Top-1 of the (mode, delta) head, how often the label is in the candidate list (fallback rows count as covered:
+    they search in full), the mean list size, the fallback rate, and how often the tx label is DCT_DCT or in the tx
+    list (rows with a tx search)."""
+    S = learner.forward(X)
+    mask, fb, tmask = select(S, y[:, 2], tau, max_cand, conf, tx_tau, max_tx)
+    lab = y[:, 0].long()
+    top1 = float((S[:, :N_MD].argmax(1) == lab).float().mean())
+    cover = mask.gather(1, lab[:, None])[:, 0] | fb
+    has_tx = y[:, 1] >= 0
+    tl = y[:, 1].clamp(min=0).long()
+    tx_ok = (tmask.gather(1, tl[:, None])[:, 0] | (tl == 0) | fb)[has_tx]
+    return {"top1": top1, "coverage": float(cover.float().mean()), "mean_cand": float(mask[~fb].sum(1).float().mean()) if (~fb).any() else 0.0,
+            "fallback": float(fb.float().mean()), "tx_coverage": float(tx_ok.float().mean()) if has_tx.any() else 1.0,
+            "mean_tx": float(tmask[has_tx & ~fb].sum(1).float().mean()) if (has_tx & ~fb).any() else 0.0}
 
 
 def bd_rate(rate_a, q_a, rate_b, q_b):
@@ -195,24 +245,26 @@ def training_images(n, size, seed, workers=1):
 
 
 def main():
-    """python -m av1gpu_b200.shortlist --images 32 --size 512x384 --epochs 10 --out shortlist_weights.npz:
-    searches the training images with the plain form, trains the network on its choices, writes the weights."""
+    """python -m av1gpu_b200.shortlist --images 2000 --size 512x384 --epochs 8 --out shortlist_weights.npz:
+    searches the training images with the plain form, trains the network on its choices, writes the parameters."""
     import argparse
     import json
+    import os
+    import time
     import torch
     from .isearch import Encoder
     ap = argparse.ArgumentParser()
     ap.add_argument("--images", type=int, default=32)
     ap.add_argument("--size", default="512x384")
-    ap.add_argument("--epochs", type=int, default=10)
+    ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr-decay", type=float, default=0.7)
+    ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--out", default="shortlist_weights.npz")
     ap.add_argument("--blocks-per-image", type=int, default=0, help="blocks drawn per image (0: all)")
     ap.add_argument("--workers", type=int, default=0, help="host processes for the image generator (0: all cores)")
     args = ap.parse_args()
-    import os
-    import time
     size = tuple(int(v) for v in args.size.split("x"))
     t0 = time.time()
     ims, qs = training_images(args.images, size, args.seed, workers=args.workers or os.cpu_count() or 1)
@@ -224,26 +276,25 @@ def main():
     n_val = X.shape[0] // 10
     perm = torch.randperm(X.shape[0], generator=torch.Generator().manual_seed(args.seed)).cuda()
     Xv, yv, Xt, yt = X[perm[:n_val]], y[perm[:n_val]], X[perm[n_val:]], y[perm[n_val:]]
-    lrn = Learner(max_batch=4096)
-    lrn.set_weights(init_weights(args.seed))
+    lrn = Learner(max_batch=args.batch)
+    lrn.set_params(init_params(args.seed))
     t1 = time.time()
-    hist = train(lrn, Xt, yt, epochs=args.epochs, batch=4096, lr=args.lr, seed=args.seed, log=print)
+    hist = train(lrn, Xt, yt, epochs=args.epochs, batch=args.batch, lr=args.lr, seed=args.seed, log=print, lr_decay=args.lr_decay)
     t_train = time.time() - t1
-    w = lrn.get_weights()
-    np.savez_compressed(args.out, w1=w[0], b1=w[1], w2=w[2], b2=w[3], images=args.images, size=np.array(size), epochs=args.epochs,
+    p = lrn.get_params()
+    np.savez_compressed(args.out, params=p, images=args.images, size=np.array(size), epochs=args.epochs,
                         blocks_per_image=args.blocks_per_image, seed=args.seed)
     out = {"images": args.images, "samples": int(X.shape[0]), "final_train": hist[-1], "generate_s": round(t_gen, 1),
            "dataset_s": round(t_data, 1), "train_s": round(t_train, 1)}
-    for tau, mm, cf in ((0.8, 4, 0.0), (0.9, 6, 0.0), (0.9, 6, 0.25), (0.95, 8, 0.0)):
-        out["val_tau%.2f_max%d_conf%.2f" % (tau, mm, cf)] = evaluate(lrn, Xv, yv, tau=tau, max_modes=mm, conf=cf)
+    for tau, mc, cf, tt, mt in ((0.8, 4, 0.0, 0.8, 1), (0.9, 6, 0.0, 0.9, 2), (0.95, 8, 0.0, 0.95, 3), (0.9, 6, 0.25, 0.9, 2)):
+        out["val_tau%.2f_max%d_conf%.2f_tx%.2f_%d" % (tau, mc, cf, tt, mt)] = evaluate(lrn, Xv, yv, tau, mc, cf, tt, mt)
     print(json.dumps(out))
     lrn.close()
     enc.close()
 
 
-def load_weights(path):
-    d = np.load(path)
-    return [d["w1"], d["b1"], d["w2"], d["b2"]]
+def load_params(path):
+    return np.load(path)["params"].astype(np.float32)
 
 
 if __name__ == "__main__":

@@ -182,8 +182,9 @@ int is_test_inverse(is_handle *h, int n, const int16_t *levels, int tx_size, int
 /* Intra prediction (av1g_build_edges + av1g_predict_intra semantics) of n blocks on an 8-bit plane (host, w x h):
  * params [n][10] = {x, y, log2W, log2H, haveLeft, haveAbove, haveAR, haveBL, mode, delta}, out [n][64*64]. */
 int is_test_predict(is_handle *h, int n, const uint8_t *plane, int w, int hgt, const int32_t *params, uint8_t *out);
-/* Analysis records of one shape of the last encode: J, cand[4], ncand, tx per block; returns the count or < 0. */
-int is_debug_analysis(is_handle *h, int bsize, int64_t *J, uint8_t *cand, uint8_t *ncand, uint8_t *tx);
+/* Analysis records of one shape of the last encode: J, cand[4], ncand, tx and the closed loop's tx mask per block (0:
+ * every type); returns the count or < 0. */
+int is_debug_analysis(is_handle *h, int bsize, int64_t *J, uint8_t *cand, uint8_t *ncand, uint8_t *tx, uint16_t *tx_mask);
 /* Leaves of SB sb of the last encode (bsize, x4, y4); returns the count or < 0. */
 int is_debug_leaves(is_handle *h, uint32_t sb, uint8_t *bsize, uint8_t *x4, uint8_t *y4);
 /* Fixed-point tables as uploaded: cost table of q-context qctx (n entries), averaged bits, lambda of a qindex.  Host
@@ -198,40 +199,61 @@ int is_debug_tables(is_handle *h, int qctx, uint16_t *cost, size_t cap, int32_t 
 int is_set_trace(is_handle *h, int on);
 int is_get_trace(is_handle *h, unsigned long long *out, size_t cap, uint32_t *n);
 
-/* ---- learned mode shortlist: a 288 -> 128 (ReLU) -> 16 network over per-block features, trained on the GPU with
- * the library's BF16 tensor-core kernels on labels the exhaustive search produces (no counterpart in the reference:
- * its open-loop shortlists are hand-made, encoder/src/k_an_x.cu; the survey's ABI suggestion is is_set_shortlist_model)
- * Features: a 16x16 luma patch resampled from the block (mean removed, / 64), an 8-bin gradient orientation histogram,
- * the block shape one-hot (22), qindex / 255, 1.  Weights are fp32, row-major [out][in]: w1 128 x 288, b1 128,
- * w2 16 x 128, b2 16 (scores 13 .. 15 unused). */
+/* ---- learned shortlist: a small BF16 conv / MLP network scoring (mode, angle delta, tx type) candidates per block,
+ * trained on the GPU with the library's BF16 tensor-core kernels on labels the exhaustive search produces.  It plays the
+ * role of the reference's external-screener hook (GpBatch::extCand / GpExtCand {J, mode, delta, tx},
+ * encoder/src/gp.h:136-143,164-170, consumed in place of the SATD screening at encoder/src/k_analysis.cuh:586-606), which
+ * nothing in the reference fills; its hand-made pruning is the staged analysis and the open-loop shortlists
+ * (encoder/src/an_stage.h, k_leafprep.cu).
+ * Scored blocks: the 16 shapes of at least 64 samples (8x8 .. 64x64, 4x16, 16x4; not 4x4, 4x8, 8x4), in the order
+ * 8x8 8x16 16x8 16x16 16x32 32x16 32x32 32x64 64x32 64x64 4x16 16x4 8x32 32x8 16x64 64x16.  Input (IS_SL_FEAT bf16 per
+ * block): a 32 x 32 luma patch resampled from the block and a margin of ceil(side / 8) samples above and left (box
+ * averages, mean removed, / 64; 10-bit samples count a quarter), then 32 extras: an 8-bin gradient-orientation histogram
+ * of the patch, the shape one-hot (16), qindex / 255, 1, zeros.  Layers: conv 3x3 stride 2 1 -> 8 (16 x 16), 8 -> 16
+ * (8 x 8), 16 -> 16 (4 x 4), each ReLU; fc 288 (the 256 conv outputs, position-major, then the 32 extras) -> 160 ReLU;
+ * fc 160 -> 80 scores: [0, 61) the (mode, delta) classes (DC, SMOOTH, SMOOTH_V, SMOOTH_H, PAETH, then V .. D67 x delta
+ * -3 .. 3), [64, 80) the 16 tx types.  Parameters: IS_SL_PARAMS fp32 in the order conv1 w [8][9] b [8], conv2 w [16][72]
+ * b [16], conv3 w [16][144] b [16], fc1 w [160][288] b [160], fc2 w [80][160] b [80] (a conv weight's column is
+ * tap * in_channels + channel, tap = 3 ky + kx). */
+#define IS_SL_FEAT 1056
+#define IS_SL_OUT 80
+#define IS_SL_PARAMS 62688
 typedef struct is_learner is_learner;
-int is_sl_create(int device, int max_batch, is_learner **out);   /* max_batch: a multiple of 32 */
+int is_sl_create(int device, int max_batch, is_learner **out);   /* max_batch: a multiple of 32, at most 65536 */
 void is_sl_destroy(is_learner *L);
-int is_sl_set_weights(is_learner *L, const float *w1, const float *b1, const float *w2, const float *b2);
-int is_sl_get_weights(is_learner *L, float *w1, float *b1, float *w2, float *b2);
-/* scores (device, n x 16 fp32) of n feature rows (device bf16, n x 288) */
+int is_sl_set_params(is_learner *L, const float *params);   /* also resets the Adam state */
+int is_sl_get_params(is_learner *L, float *params);
+/* scores (device, n x IS_SL_OUT fp32) of n feature rows (device bf16, n x IS_SL_FEAT), through the GEMM path */
 int is_sl_forward(is_learner *L, const void *X, int n, float *S, void *stream);
-/* gradients of the mean softmax cross-entropy over the 13 modes (host, w1 | b1 | w2 | b2), loss and correct count of
- * one batch (n a multiple of 32, device X / y), weights unchanged */
+/* gradients (host, IS_SL_PARAMS floats in parameter order) of the mean loss of one batch (n a multiple of 32; device X,
+ * labels y n x 3 int32: (mode, delta) class, tx type or -1, the tx set's types as a bit mask), its mean loss and the
+ * count of rows whose best-scored class is the label; weights unchanged.  Loss: softmax cross-entropy of the (mode,
+ * delta) head plus that of the tx head restricted to the block's set (no tx term where the tx label is -1). */
 int is_sl_grads(is_learner *L, const void *X, const int32_t *y, int n, float *grads, float *loss, int *correct);
 /* one Adam step (lr; beta 0.9 / 0.999) on a batch; the batch's mean loss and correct count */
 int is_sl_train_step(is_learner *L, const void *X, const int32_t *y, int n, float lr, float *loss, int *correct);
 /* C[M x N] = A[M x K] B[N x K]^T (+ bias, ReLU) on device bf16 operands, fp32 out (K, lda, ldb multiples of 8) */
 int is_nn_gemm(int M, int N, int K, const void *A, int lda, const void *B, int ldb, float *C, int ldc, const float *bias,
                int relu, void *stream);
-/* training data of image i of the last search: features (device bf16, n x 288) and labels (the analysis's best mode)
- * of its analysed blocks into buffers of capacity cap; *n = the number of blocks (also when it exceeds cap: then
- * nothing is written) */
+/* training rows of image i of the last search: features (device bf16, n x IS_SL_FEAT) and labels (device int32, n x 3)
+ * of its scored records (shape by shape, records in analysis order; a record outside the frame has class -1 and zero
+ * features), the labels being the analysis' choices (best (mode, delta), its tx type); *n = the number of records (also
+ * when it exceeds cap: then nothing is written) */
 int is_sl_dataset(is_handle *h, int i, void *X, int32_t *y, int cap, int *n);
+/* the search's fused inference kernel (source plane -> candidates in one kernel) on image i of the last search with the
+ * learner's weights: scores (device fp32, n x IS_SL_OUT) of the same rows as is_sl_dataset (rows outside the frame are
+ * not written) */
+int is_sl_infer(is_handle *h, is_learner *L, int i, float *S, int cap, int *n);
 
-/* Use a trained shortlist in the search of this handle (w1 NULL: the plain form again).  Each analysed block screens
- * only the smallest set of most probable modes whose probabilities add up to tau, at most max_modes, and takes its best
- * rd_k (1 .. 4) screened candidates into the exact-rate RD instead of 4; a block whose most probable mode has
- * probability below conf screens all 13 with 4 RD candidates (the fallback); max_modes 0 keeps every block on the
- * plain form (identical results).  Angle deltas follow the two best screened directional modes; the rest of the
- * search is unchanged and the reconstruction stays exact. */
-int is_set_shortlist_model(is_handle *h, const float *w1, const float *b1, const float *w2, const float *b2, float tau,
-                           int max_modes, float conf, int rd_k);
+/* Use a trained shortlist in the search of this handle (params NULL: the plain form again).  Before each image's
+ * analysis the fused kernel scores every scored block; a block whose most probable (mode, delta) has probability below
+ * conf falls back to the full search; the others screen only the smallest set of most probable (mode, delta) candidates
+ * whose probabilities add up to tau (at most max_cand, 1 .. 8), with no separate angle-delta search, take their best
+ * rd_k (1 .. 4) into the exact-rate RD, and try beyond DCT_DCT only the tx types of the block's set that cover tx_tau of
+ * the tx head's probability (at most max_tx; 0: none) - in the analysis and in the closed loop's tx-type pass.  The
+ * chosen modes are still coded and reconstructed exactly. */
+int is_set_shortlist_model(is_handle *h, const float *params, float tau, int max_cand, float conf, int rd_k, float tx_tau,
+                           int max_tx);
 
 /* INT32 issue-rate probe: the measured INT32 instruction throughput of the device (Gop/s, multiply-add + logic chains
  * over every SM) and the best kernel time, the roofline denominator of this integer path. */

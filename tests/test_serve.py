@@ -59,10 +59,10 @@ def test_served_results_equal_alone(enc, learned):
     images, qs = _mixed_requests()
     sl = None
     if learned:
-        from av1gpu_b200.shortlist import load_weights
+        from av1gpu_b200.shortlist import load_params
         import os
-        w = load_weights(os.path.join(os.path.dirname(serve.__file__), "shortlist_weights.npz"))
-        sl = {"weights": w, "tau": 0.9, "max_modes": 6, "rd_k": 2}
+        w = load_params(os.path.join(os.path.dirname(serve.__file__), "shortlist_weights.npz"))
+        sl = {"params": w, "tau": 0.9, "max_cand": 8, "rd_k": 2, "tx_tau": 0.9, "max_tx": 2}
         enc.set_shortlist(**sl)
     try:
         alone = [enc.encode(im, q) for im, q in zip(images, qs)]
