@@ -87,7 +87,7 @@ def main():
         return time.perf_counter() - t
 
     def batched():
-        k, _ = enc.autotune_batch(dev[:args.tune_images], qs[:args.tune_images], host=False)
+        k, w, _ = enc.autotune_batch(dev[:args.tune_images], qs[:args.tune_images], host=False, with_warps=True)
         enc.set_batch_options(use_graph=True, front_streams=k)
         enc.encode_batch_async(dev, qs, host=False)   # captures the graph
         ts = []
@@ -98,14 +98,15 @@ def main():
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t)
         enc.set_batch_options(use_graph=False, front_streams=1)
-        return min(ts), k
+        enc.set_closed_loop_warps(0)
+        return min(ts), (k, w)
 
     plain()   # warm-up (workspace, tables)
     tp = plain()
     print(json.dumps({**base, "form": "plain, one image at a time", "mp_per_s": round(mp / tp, 2), "s": round(tp, 3)}), flush=True)
     tb, k = batched()
     print(json.dumps({**base, "form": "batched (one batch, CUDA graph)", "mp_per_s": round(mp / tb, 2), "s": round(tb, 3),
-                      "front_streams": k, "x_plain": round(tp / tb, 2)}), flush=True)
+                      "front_streams": k[0], "closed_loop_warps": k[1] or "all", "x_plain": round(tp / tb, 2)}), flush=True)
     if not args.no_verify:   # untimed: every image of the batch bit-equal to its one-at-a-time search
         k, _ = enc.autotune_batch(dev[:args.tune_images], qs[:args.tune_images], host=False)
         enc.set_batch_options(use_graph=True, front_streams=k)
@@ -126,13 +127,15 @@ def main():
     enc.set_shortlist(None)
     print(json.dumps({**base, "form": "batched + learned shortlist (tau %g, max %d candidates, conf %g, rd_k %d, tx tau %g, max %d tx)"
                                       % (args.tau, args.max_cand, args.conf, args.rd_k, args.tx_tau, args.max_tx),
-                      "mp_per_s": round(mp / ts, 2), "s": round(ts, 3), "front_streams": k, "x_plain": round(tp / ts, 2)}), flush=True)
+                      "mp_per_s": round(mp / ts, 2), "s": round(ts, 3), "front_streams": k[0], "closed_loop_warps": k[1] or "all",
+                      "x_plain": round(tp / ts, 2)}), flush=True)
     if args.nl_rd_k:
         enc.set_search_options(rd_k=args.nl_rd_k, tx_keep=args.nl_tx_keep)
         tn, k = batched()
         enc.set_search_options()
         print(json.dumps({**base, "form": "batched + non-learned pruning (rd_k %d, tx_keep %d)" % (args.nl_rd_k, args.nl_tx_keep),
-                          "mp_per_s": round(mp / tn, 2), "s": round(tn, 3), "front_streams": k, "x_plain": round(tp / tn, 2)}), flush=True)
+                          "mp_per_s": round(mp / tn, 2), "s": round(tn, 3), "front_streams": k[0], "closed_loop_warps": k[1] or "all",
+                          "x_plain": round(tp / tn, 2)}), flush=True)
     enc.close()
 
 

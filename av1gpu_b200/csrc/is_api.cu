@@ -200,6 +200,7 @@ struct is_handle {
     size_t smemRcG[4] = {0, 0, 0, 0};       // the closed loop per format group (fmt_group)
     int rcGridG[4] = {0, 0, 0, 0};
     int rcWarpsG[4] = {0, 0, 0, 0};         // its warps per CTA
+    int reconWarps = 0;                     // warps per CTA the closed loop uses (0: all; is_set_closed_loop_warps)
     // last result
     bool have = false;
     uint32_t nBlocks = 0, nTxb = 0;
@@ -768,6 +769,7 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
         ctl.readyWaitNs = (unsigned long long)h->readyWaitNs;
         ctl.trace = F0.leafTrace;
         ctl.poison = h->poison ? 1 : 0;
+        ctl.warps = h->reconWarps > 0 ? std::min(h->reconWarps, h->rcWarpsG[g]) : h->rcWarpsG[g];
         IS_CK((g == 0 ? rc_launch<8, 1>(fs, gn, ctl, grid, sm, st) : g == 1 ? rc_launch<8, 0>(fs, gn, ctl, grid, sm, st)
                : g == 2 ? rc_launch<10, 1>(fs, gn, ctl, grid, sm, st) : rc_launch<10, 0>(fs, gn, ctl, grid, sm, st)));
     }
@@ -794,8 +796,8 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
 static std::string batch_key(const is_handle *h, const is_frame *fr, int n, bool fromHost) {
     std::string k;
     char b[160];
-    snprintf(b, sizeof b, "%p|%d|%d|%d|%d|%d|%d|%d|%lld|%d|%d|", h->arena, n, (int)fromHost, h->frontStreams, h->reconCtas,
-             h->slOn ? h->slVersion : -1, (int)h->poison, h->waitIters, h->readyWaitNs, h->rdK, h->txKeep);
+    snprintf(b, sizeof b, "%p|%d|%d|%d|%d|%d|%d|%d|%lld|%d|%d|%d|", h->arena, n, (int)fromHost, h->frontStreams, h->reconCtas,
+             h->slOn ? h->slVersion : -1, (int)h->poison, h->waitIters, h->readyWaitNs, h->rdK, h->txKeep, h->reconWarps);
     k += b;
     for (int i = 0; i < n; i++) {
         snprintf(b, sizeof b, "%d,%d,%d,%d,%d,%p,%p,%p,%d,%d,%d;", fr[i].width, fr[i].height, fr[i].qindex, fr[i].bit_depth, fr[i].chroma_444,
@@ -978,28 +980,39 @@ int is_set_shortlist_model(is_handle *h, const float *params, float tau, int max
     return IS_OK;
 }
 
-int is_autotune_batch(is_handle *h, const is_frame *frames, int n, int from_host, int *front_streams, float *ms) {
+int is_set_closed_loop_warps(is_handle *h, int warps) {
+    if (!h || warps < 0 || warps > RC_MAX_WARPS) return IS_ERR_INVALID;
+    h->reconWarps = warps;
+    return IS_OK;
+}
+
+int is_autotune_batch(is_handle *h, const is_frame *frames, int n, int from_host, int *front_streams, int *recon_warps, float *ms) {
     if (!h || !frames || n < 1) return IS_ERR_INVALID;
     IS_CK(cudaSetDevice(h->device));
     const bool g = h->useGraph;
     h->useGraph = false;
-    int best = 1;
+    int best = 1, bestW = 0;
     float bestMs = 1e30f;
-    const int cand[3] = {1, 2, 4};
+    const int cand[3] = {1, 2, 4}, wcand[3] = {4, 6, 0};   // front-end streams x closed-loop warps per CTA (0: all)
     for (int c = 0; c < 3; c++) {
         if (cand[c] > 1 && n < 2) break;
-        h->frontStreams = cand[c];
-        float t = 0;
-        for (int r = 0; r < 2; r++) {   // the second run is timed (the first warms the workspace)
-            const int rc = run_batch(h, h->own, frames, n, from_host != 0);
-            if (rc) { h->useGraph = g; return rc; }
-            t = h->times.total;
+        for (int w = 0; w < 3; w++) {
+            h->frontStreams = cand[c];
+            h->reconWarps = wcand[w];
+            float t = 0;
+            for (int r = 0; r < 2; r++) {   // the second run is timed (the first warms the workspace)
+                const int rc = run_batch(h, h->own, frames, n, from_host != 0);
+                if (rc) { h->useGraph = g; return rc; }
+                t = h->times.total;
+            }
+            if (t < bestMs) { bestMs = t; best = cand[c]; bestW = wcand[w]; }
         }
-        if (t < bestMs) { bestMs = t; best = cand[c]; }
     }
     h->frontStreams = best;
+    h->reconWarps = bestW;
     h->useGraph = g;
     if (front_streams) *front_streams = best;
+    if (recon_warps) *recon_warps = bestW;
     if (ms) *ms = bestMs;
     return IS_OK;
 }

@@ -238,7 +238,7 @@ __device__ __forceinline__ void sl_cells(const FrameDesc &F, int bs, int x, int 
 // (lanes write their own entries).  Histogram: central differences on the cell grid (clamped at its border),
 // orientation mod 180 degrees in 8 bins of 22.5 degrees, |gx| + |gy| weighted, divided by (sum + 1).
 template <typename PatchFn, typename ExtraFn>
-__device__ __forceinline__ void sl_features(const FrameDesc &F, int bs, const float (&v)[32], PatchFn patch, ExtraFn extra) {
+__device__ __forceinline__ void sl_features(const FrameDesc &F, int bs, const float (&v)[32], float *hs, PatchFn patch, ExtraFn extra) {
     const int lane = threadIdx.x & 31;
     float sum = 0.f;
 #pragma unroll
@@ -247,7 +247,9 @@ __device__ __forceinline__ void sl_features(const FrameDesc &F, int bs, const fl
     const float mean = sum / 1024.f;
 #pragma unroll
     for (int i = 0; i < 32; i++) patch(i, lane, __float2bfloat16((v[i] - mean) / 64.f));
-    float hist[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    float *hr = hs + lane * 9;   // the lane's 8 bins in shared memory (row stride 9: distinct banks)
+#pragma unroll
+    for (int q = 0; q < 8; q++) hr[q] = 0.f;
 #pragma unroll
     for (int i = 0; i < 32; i++) {
         const float l = __shfl_sync(0xffffffffu, v[i], max(lane - 1, 0)), r = __shfl_sync(0xffffffffu, v[i], min(lane + 1, 31));
@@ -258,9 +260,11 @@ __device__ __forceinline__ void sl_features(const FrameDesc &F, int bs, const fl
         int bin;
         if (ax >= 0.f) bin = ay <= 0.41421356f * ax ? 0 : ay <= ax ? 1 : ay <= 2.41421356f * ax ? 2 : 3;
         else bin = ay >= -2.41421356f * ax ? 4 : ay >= -ax ? 5 : ay >= -0.41421356f * ax ? 6 : 7;
-#pragma unroll
-        for (int q = 0; q < 8; q++) hist[q] += q == bin ? m : 0.f;
+        hr[bin] += m;
     }
+    float hist[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) hist[q] = hr[q];
     float tot = 0.f;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -324,9 +328,10 @@ __global__ void k_sl_dataset(const FrameDesc F, uint32_t i0, int n, __nv_bfloat1
         if (lane == 0) { y[3 * r] = -1; y[3 * r + 1] = -1; y[3 * r + 2] = 0; }
         return;
     }
+    __shared__ float hs[8][32 * 9];   // (256 threads: 8 warps)
     float v[32];
     sl_cells(F, bs, x, yy, v);
-    sl_features(F, bs, v, [&](int i, int j, __nv_bfloat16 b) { out[i * SL_PATCH + j] = b; },
+    sl_features(F, bs, v, hs[(threadIdx.x >> 5) & 7], [&](int i, int j, __nv_bfloat16 b) { out[i * SL_PATCH + j] = b; },
                 [&](int k, __nv_bfloat16 b) { out[SL_NPIX + k] = b; });
     if (lane == 0) {
         const BlockRes br = F.blk[F.shOff[bs] + rec];
@@ -499,6 +504,7 @@ struct SlcWarp {
     __nv_bfloat16 patch[SL_PATCH * SLI_PS];   // 32 x 32 (+ pad)
     __nv_bfloat16 act1[256 * SL_C1];          // 16 x 16 x 8
     __nv_bfloat16 act2[64 * SL_C2];           // 8 x 8 x 16
+    float hist[32 * 9];                       // the lanes' orientation-histogram bins
 };
 struct SlcSmem {
     __nv_bfloat16 w1[SL_C1 * SLI_W1S], w2[SL_C2 * SLI_W2S], w3[SL_C3 * SLI_W3S];
@@ -567,7 +573,7 @@ __global__ void __launch_bounds__(SLC_WARPS * 32, 2) k_sl_conv(const __grid_cons
         {
             float v[32];
             sl_cells(F, bs, x, y, v);
-            sl_features(F, bs, v, [&](int i, int j, __nv_bfloat16 val) { Wp.patch[i * SLI_PS + j] = val; },
+            sl_features(F, bs, v, Wp.hist, [&](int i, int j, __nv_bfloat16 val) { Wp.patch[i * SLI_PS + j] = val; },
                         [&](int k, __nv_bfloat16 val) { zr[256 + k] = val; });
         }
         __syncwarp();

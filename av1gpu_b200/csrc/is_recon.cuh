@@ -984,6 +984,7 @@ struct RcCtl {
     unsigned long long readyWaitNs;
     unsigned long long *trace;     // optional leaf trace (batch mode)
     int poison;
+    int warps;                     // warps per CTA that work (the rest leave after the CTA's staging); at most NW
 };
 template <int BD> using RcPxOf = typename std::conditional<BD == 8, uint8_t, uint16_t>::type;
 template <int BD, int SS> constexpr int rc_warps_of() { return rc_warps<RcPxOf<BD>, SS>(); }
@@ -1010,6 +1011,7 @@ __global__ void __launch_bounds__(rc_warps_of<BD, SS>() * 32, 1) k_recon(const F
     }
     if (threadIdx.x == 0) S.big.lock = 0;
     __syncthreads();
+    if (warp >= ctl.warps) return;   // (uniform per warp; no CTA barrier follows)
     int *rq = ctl.rq;
     const unsigned long long *readyQ = ctl.readyQ;
     int *err = ctl.err;

@@ -177,6 +177,7 @@ static int serve_launch(is_handle *h) {
     ctl.readyWaitNs = SERVE_IDLE_NS;
     ctl.trace = nullptr;
     ctl.poison = h->poison ? 1 : 0;
+    ctl.warps = h->reconWarps > 0 ? std::min(h->reconWarps, S->warps) : S->warps;
     const size_t sm = h->smemRcG[S->g];
     const FrameDesc *fs = S->dTable;
     const int g = S->g, grid = S->grid;

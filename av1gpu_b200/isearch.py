@@ -58,7 +58,7 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_autotune_batch", "is_workspace_bytes", "is_workspace_bytes_format", "is_sl_create", "is_sl_destroy", "is_sl_set_params",
            "is_sl_get_params", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset", "is_sl_infer",
            "is_set_shortlist_model",
-           "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison", "is_set_search_options", "is_serve_open", "is_serve_start", "is_serve_submit", "is_serve_poll",
+           "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison", "is_set_search_options", "is_set_closed_loop_warps", "is_serve_open", "is_serve_start", "is_serve_submit", "is_serve_poll",
            "is_serve_counts", "is_serve_copy", "is_serve_stop", "is_serve_close"]
 
 _lib = None
@@ -113,7 +113,8 @@ def load_library():
     L.is_sl_dataset.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_int)]
     L.is_sl_infer.argtypes = [vp, vp, C.c_int, vp, C.c_int, C.POINTER(C.c_int)]
     L.is_set_shortlist_model.argtypes = [vp, vp, C.c_float, C.c_int, C.c_float, C.c_int, C.c_float, C.c_int]
-    L.is_autotune_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
+    L.is_autotune_batch.argtypes = [vp, C.POINTER(IsFrame), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]
+    L.is_set_closed_loop_warps.argtypes = [vp, C.c_int]
     L.is_set_wait_limits.argtypes = [vp, C.c_int, C.c_longlong]
     L.is_set_workspace_limit.argtypes = [vp, C.c_uint64]
     L.is_set_poison.argtypes = [vp, C.c_int]
@@ -410,13 +411,18 @@ class Encoder:
         self._check(self.L.is_set_shortlist_model(self.h, p.ctypes.data, C.c_float(tau), max_cand, C.c_float(conf), rd_k,
                                                   C.c_float(tx_tau), max_tx), "is_set_shortlist_model")
 
-    def autotune_batch(self, images, qindices, host=True):
-        """Time the batch with 1 / 2 / 4 front-end streams and keep the fastest; returns (streams, ms)."""
+    def autotune_batch(self, images, qindices, host=True, with_warps=False):
+        """Time the batch with 1 / 2 / 4 front-end streams x 4 / 6 / all closed-loop warps per CTA and keep the fastest
+        for the handle; returns (streams, ms), or (streams, warps, ms) with with_warps (warps 0: all)."""
         fr = self._frames(images, qindices, host)
-        k, ms = C.c_int(), C.c_float()
-        self._check(self.L.is_autotune_batch(self.h, fr, len(images), 1 if host else 0, C.byref(k), C.byref(ms)),
+        k, w, ms = C.c_int(), C.c_int(), C.c_float()
+        self._check(self.L.is_autotune_batch(self.h, fr, len(images), 1 if host else 0, C.byref(k), C.byref(w), C.byref(ms)),
                     "is_autotune_batch")
-        return k.value, ms.value
+        return (k.value, w.value, ms.value) if with_warps else (k.value, ms.value)
+
+    def set_closed_loop_warps(self, warps=0):
+        """Warps per CTA of the closed loop (0: all the shared memory holds)."""
+        self._check(self.L.is_set_closed_loop_warps(self.h, warps), "is_set_closed_loop_warps")
 
     # ---- kernel-level entry points (parity tests) ----
     def test_fwd_quant(self, res, tx_size, tx_type, plane, qindex, ctx):

@@ -130,9 +130,13 @@ int is_set_search_options(is_handle *h, int rd_k, int tx_keep);
 int is_workspace_bytes(int width, int height, uint64_t *bytes);
 /* the same for a frame of the given format (bit_depth 8 / 10, chroma_444 0 / 1) */
 int is_workspace_bytes_format(int width, int height, int bit_depth, int chroma_444, uint64_t *bytes);
-/* Autotuner: times the batch with 1, 2 and 4 front-end streams (two runs each, the second timed) and keeps the
- * fastest for the handle; returns the choice and its time (ms). */
-int is_autotune_batch(is_handle *h, const is_frame *frames, int n, int from_host, int *front_streams, float *ms);
+/* Warps per CTA the closed loop runs (0: all the shared memory of a CTA holds - 8 for 8-bit 4:2:0, fewer for the
+ * larger formats; 1 .. 8 caps it).  More warps per SM raise the loop's throughput when many leaves are ready at once (a
+ * batch, a serving session); a single image's loop is bound by its dependency chain. */
+int is_set_closed_loop_warps(is_handle *h, int warps);
+/* Autotuner: times the batch with 1, 2 and 4 front-end streams x 4, 6 and all closed-loop warps per CTA (two runs each,
+ * the second timed) and keeps the fastest for the handle; returns the choice and its time (ms). */
+int is_autotune_batch(is_handle *h, const is_frame *frames, int n, int from_host, int *front_streams, int *recon_warps, float *ms);
 
 /* ---- serving: continuous admission of images into a running closed loop ----
  * A session (one per handle, one image format; is_serve_open allocates it, is_serve_start starts it) keeps one persistent

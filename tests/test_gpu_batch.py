@@ -52,10 +52,21 @@ def test_batch_streams_and_graph_replay(enc):
 
 
 def test_autotune_batch(enc):
+    """The autotuner's choice (front-end streams x closed-loop warps per CTA) changes the speed, not the results."""
     images, qs = _images()
-    k, ms = enc.autotune_batch([[np.ascontiguousarray(p) for p in im] for im in images], qs)
-    assert k in (1, 2, 4) and ms > 0
-    enc.set_batch_options(use_graph=False, front_streams=1)
+    planes = [[np.ascontiguousarray(p) for p in im] for im in images]
+    ref = [enc.encode(im, q) for im, q in zip(images, qs)]
+    k, w, ms = enc.autotune_batch(planes, qs, with_warps=True)
+    assert k in (1, 2, 4) and w in (0, 4, 6) and ms > 0
+    try:
+        for warps in (1, 3):
+            enc.set_closed_loop_warps(warps)
+            got = enc.encode_batch(planes, qs)
+            for i in range(len(images)):
+                assert _same(ref[i], got[i]), (warps, i)
+    finally:
+        enc.set_closed_loop_warps(0)
+        enc.set_batch_options(use_graph=False, front_streams=1)
 
 
 def test_batched_workload_slice_equals_one_at_a_time(enc):
