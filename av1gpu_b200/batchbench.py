@@ -1,12 +1,13 @@
 """The batched-form workload: many images of uneven size, format and qindex searched plain (one image at a time), as
-one batch, and as one batch with the learned shortlist.
+one batch, as one batch with the learned shortlist, and (with --nl-rd-k) as one batch with the non-learned pruning.
 
-    python -m av1gpu_b200.batchbench [--images 256] [--max-mp 24] [--seed 3]
+    python -m av1gpu_b200.batchbench [--images 256] [--max-mp 24] [--seed 3] [--nl-rd-k 2]
 
 Images are seeded crops of two synthetic 6000 x 4000 pictures (no dataset is named for this workload): log-uniform
 area 0.18 .. 24 MP, aspect 1:3 .. 3:1, 80 % 8-bit 4:2:0 and 20 % 10-bit 4:4:4, qindex uniform 40 .. 220.  Inputs are
 on the device before a timed region; the batch is captured as a CUDA graph (the captured run untimed) with the front-end
-stream count from is_autotune_batch on the first images.  One JSON line per form; MP = visible luma megapixels.
+stream count and the closed loop's warps per CTA from is_autotune_batch on the first images.  One JSON line per form;
+MP = visible luma megapixels.
 """
 import argparse
 import json
@@ -53,13 +54,14 @@ def main():
     ap.add_argument("--images", type=int, default=256)
     ap.add_argument("--max-mp", type=float, default=24.0)
     ap.add_argument("--seed", type=int, default=3)
-    ap.add_argument("--tune-images", type=int, default=24, help="images the front-end stream count is tuned on")
+    ap.add_argument("--tune-images", type=int, default=24, help="images the autotuner runs on")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "shortlist_weights.npz"))
-    ap.add_argument("--tau", type=float, default=0.9)
-    ap.add_argument("--max-cand", type=int, default=8)
+    ap.add_argument("--tau", type=float, default=0.8)
+    ap.add_argument("--max-cand", type=int, default=4)
     ap.add_argument("--conf", type=float, default=0.0)
     ap.add_argument("--rd-k", type=int, default=2)
     ap.add_argument("--tx-tau", type=float, default=0.9)
+    ap.add_argument("--rd-k-other", type=int, default=2, help="RD candidates of the blocks the network does not score")
     ap.add_argument("--max-tx", type=int, default=2)
     ap.add_argument("--nl-rd-k", type=int, default=0, help="also time the non-learned pruning with this RD count (0: no)")
     ap.add_argument("--nl-tx-keep", type=int, default=2, help="tx types the non-learned pruning keeps per block")
@@ -123,10 +125,13 @@ def main():
             raise SystemExit("batched results differ from the one-at-a-time search")
     enc.set_shortlist(load_params(args.weights), tau=args.tau, max_cand=args.max_cand, conf=args.conf, rd_k=args.rd_k,
                       tx_tau=args.tx_tau, max_tx=args.max_tx)
+    enc.set_search_options(rd_k=args.rd_k_other)
     ts, k = batched()
     enc.set_shortlist(None)
-    print(json.dumps({**base, "form": "batched + learned shortlist (tau %g, max %d candidates, conf %g, rd_k %d, tx tau %g, max %d tx)"
-                                      % (args.tau, args.max_cand, args.conf, args.rd_k, args.tx_tau, args.max_tx),
+    enc.set_search_options()
+    print(json.dumps({**base, "form": "batched + learned shortlist (tau %g, max %d candidates, conf %g, rd_k %d, tx tau %g, max %d tx;"
+                                      " other blocks rd_k %d)" % (args.tau, args.max_cand, args.conf, args.rd_k, args.tx_tau, args.max_tx,
+                                                                   args.rd_k_other),
                       "mp_per_s": round(mp / ts, 2), "s": round(ts, 3), "front_streams": k[0], "closed_loop_warps": k[1] or "all",
                       "x_plain": round(tp / ts, 2)}), flush=True)
     if args.nl_rd_k:

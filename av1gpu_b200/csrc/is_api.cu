@@ -676,6 +676,17 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
     return IS_OK;
 }
 
+// The closed loop's working warps per CTA for a launch over n images of format group g: the handle's setting, else 4
+// for one image (its loop is bound by its dependency chain, and fewer warps leave the SM a larger L1) and all the shared
+// memory holds for a batch; and that launch's dynamic shared memory.
+static int rc_warps_for(const is_handle *h, int g, int n) {
+    const int all = h->rcWarpsG[g];
+    return h->reconWarps > 0 ? std::min(h->reconWarps, all) : n == 1 ? std::min(4, all) : all;
+}
+static size_t rc_launch_smem(int g, int warps) {
+    return g == 0 ? rc_smem<8, 1>(warps) : g == 1 ? rc_smem<8, 0>(warps) : g == 2 ? rc_smem<10, 1>(warps) : rc_smem<10, 0>(warps);
+}
+
 // The front end of one image on stream s: its planes into the padded workspace, the learned shortlist of every scored
 // block (with a model set: the fused inference kernel), the analysis, the DP, the leaf maps and the dataflow graph,
 // whose first ready leaves go to the image's ready queue.  ev1 / ev2 (optional) are recorded after the upload and after
@@ -758,7 +769,6 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
         if (gn == 0) continue;
         const int grid = h->reconCtas > 0 && h->reconCtas < h->rcGridG[g] ? h->reconCtas : h->rcGridG[g];
         const FrameDesc *fs = h->dFs + h->bGrpStart[g];
-        const size_t sm = h->smemRcG[g];
         const FrameDesc &F0 = h->hFs[h->bGrpStart[g]];   // the group's first image: its queue, counters and trace
         RcCtl ctl;
         ctl.rq = F0.rq;
@@ -769,7 +779,8 @@ static int launch_batch(is_handle *h, cudaStream_t st, const is_frame *fr, int n
         ctl.readyWaitNs = (unsigned long long)h->readyWaitNs;
         ctl.trace = F0.leafTrace;
         ctl.poison = h->poison ? 1 : 0;
-        ctl.warps = h->reconWarps > 0 ? std::min(h->reconWarps, h->rcWarpsG[g]) : h->rcWarpsG[g];
+        ctl.warps = rc_warps_for(h, g, gn);
+        const size_t sm = rc_launch_smem(g, ctl.warps);
         IS_CK((g == 0 ? rc_launch<8, 1>(fs, gn, ctl, grid, sm, st) : g == 1 ? rc_launch<8, 0>(fs, gn, ctl, grid, sm, st)
                : g == 2 ? rc_launch<10, 1>(fs, gn, ctl, grid, sm, st) : rc_launch<10, 0>(fs, gn, ctl, grid, sm, st)));
     }

@@ -14,6 +14,8 @@ constexpr int RcNW = rc_warps_of<IS_BD, IS_SS>();
 
 template <> cudaError_t rc_upload<IS_BD, IS_SS>(const TableBlob &B) { return upload_common(B); }
 
+template <> size_t rc_smem<IS_BD, IS_SS>(int warps) { return rc_smem_bytes<RcPx, IS_SS>(warps); }
+
 template <> cudaError_t rc_setup<IS_BD, IS_SS>(size_t *smem, int *ctasPerSm, int *warps) {
     const void *k = (const void *)k_recon<IS_BD, IS_SS>;
     *smem = sizeof(RcSmem<RcPx, IS_SS, RcNW>);

@@ -59,13 +59,23 @@ template <typename Px> struct RcBig {   // the CTA's scratch for luma tx sizes w
     int lock;                           // 0 free, 1 taken
     int pad[3];
 };
+template <typename Px, int SS> struct RcSlot {   // one warp's part: its copy of its image's descriptor, its scratch
+    FrameDesc F;
+    RcWarp<Px, SS> w;
+};
+// The warps' parts come last: a launch with fewer working warps allocates only theirs (rc_smem_bytes), which leaves the
+// SM a larger L1 for the warps' stacks.
 template <typename Px, int SS, int NW> struct RcSmem {
     RateStage T;                         // scans, base-context offsets (and the cost table of q-context 0)
     RcBig<Px> big;
     uint16_t cost[3][NCDF];              // the cost tables of q-contexts 1 .. 3 (the images of a batch mix qindex)
-    FrameDesc F[NW];                     // each warp's copy of the descriptor of the image it works on
-    RcWarp<Px, SS> w[NW];
+    RcSlot<Px, SS> ws[NW];
 };
+template <typename Px, int SS> constexpr size_t rc_smem_bytes(int warps) {
+    typedef RcSmem<Px, SS, 1> S1;
+    typedef RcSlot<Px, SS> Slot;
+    return offsetof(S1, ws) + (size_t)warps * sizeof(Slot);
+}
 // the most warps (<= RC_MAX_WARPS) whose shared memory fits one CTA (8 for 8-bit 4:2:0, fewer for the larger formats)
 template <typename Px, int SS> constexpr int rc_warps() {
     return sizeof(RcSmem<Px, SS, 8>) <= 227 * 1024 ? 8 : sizeof(RcSmem<Px, SS, 7>) <= 227 * 1024 ? 7
@@ -74,8 +84,10 @@ template <typename Px, int SS> constexpr int rc_warps() {
 template <typename Px, int SS> constexpr bool rc_smem_ok() {
     typedef RcWarp<Px, SS> Wt;
     typedef RcSmem<Px, SS, rc_warps<Px, SS>()> St;
-    return sizeof(St) <= 227 * 1024 && offsetof(Wt, srcS) % 16 == 0 && sizeof(Wt) % 16 == 0 && offsetof(St, w) % 16 == 0 &&
-           offsetof(St, cost) % 16 == 0 && offsetof(St, F) % 16 == 0;
+    typedef RcSlot<Px, SS> Sl;
+    return sizeof(St) <= 227 * 1024 && offsetof(Wt, srcS) % 16 == 0 && sizeof(Wt) % 16 == 0 && offsetof(St, ws) % 16 == 0 &&
+           offsetof(St, cost) % 16 == 0 && sizeof(Sl) % 16 == 0 && offsetof(Sl, w) % 16 == 0 &&
+           rc_smem_bytes<Px, SS>(rc_warps<Px, SS>()) == sizeof(St);
 }
 static_assert(rc_smem_ok<uint8_t, 1>() && rc_smem_ok<uint8_t, 0>() && rc_smem_ok<uint16_t, 1>() && rc_smem_ok<uint16_t, 0>() &&
                   sizeof(FrameDesc) % 16 == 0,
@@ -97,6 +109,10 @@ __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long l
     return v;
 }
 __device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+// the release side: the writes before it (the thread's own, and those ordered before it by a warp barrier) are visible
+// to a thread that acquires a later relaxed store or atomic of this thread (an acquire-release fence, not the
+// sequentially consistent one of __threadfence, which costs a global ordering step)
+__device__ __forceinline__ void fence_release() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_release(int *p, int v) { asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
 template <typename P> __device__ __forceinline__ P ldcg(const P *p);
 template <> __device__ __forceinline__ uint8_t ldcg<uint8_t>(const uint8_t *p) { return __ldcg(p); }
@@ -368,7 +384,7 @@ constexpr unsigned long long SLOT_ABANDONED = ~0ull;
 // wrote before (a running loop may take the leaf at once); a slot that an idle serving worker abandoned is skipped
 __device__ __forceinline__ void push_ready(const FrameDesc &F, uint32_t id) {
     const unsigned long long v = 1ull + (((unsigned long long)F.img << 32) | id);
-    __threadfence();
+    fence_release();
     for (;;) {
         const int pos = atomicAdd(F.rq + 1, 1);
         if ((uint32_t)pos >= F.readyCap) {   // the queue's positions are used up: the image cannot complete
@@ -670,19 +686,16 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, RcBig<Px> &Big, 
     }
     // publish the luma (reconstruction, y modes, luma coefficient contexts) for the luma of the later leaves
     __syncwarp();
-    if (lane == 0) {
-        __threadfence();
+    if (lane == 0) {   // (the release store is cumulative: it also releases the other lanes' writes, ordered by the barrier)
         st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 1);
         if (trace) trace[5] = gtimer();
     }
-    {   // the dependents whose last luma dependency this was enter the ready queue
-        __threadfence();
+    {   // the dependents whose last luma dependency this was enter the ready queue (the taker of a leaf acquires each of
+        // its dependencies' flags itself before it reads their data; push_ready releases what this thread wrote)
+        __syncwarp();
         for (int k = lane; k < relN; k += 32) {
             const uint32_t d = F.revList[relOff + k];
-            if (atomicSub(F.depCnt + d, 1) == 1) {
-                __threadfence();
-                push_ready(F, d);
-            }
+            if (atomicSub(F.depCnt + d, 1) == 1) push_ready(F, d);
         }
     }
     // ================= chroma =================
@@ -956,7 +969,6 @@ __device__ void rc_leaf(const FrameDesc &F, RcWarp<Px, SS> &Wp, RcBig<Px> &Big, 
     }
     __syncwarp();
     if (lane == 0) {
-        __threadfence();
         st_release(F.leafDone + (size_t)sb * SB_MAX_LEAVES + li, 2);
         if (trace) trace[8] = gtimer();
         // serving session: the image's last leaf tells the host (its record can be packed while others run on)
@@ -996,10 +1008,10 @@ __global__ void __launch_bounds__(rc_warps_of<BD, SS>() * 32, 1) k_recon(const F
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Sm &S = *reinterpret_cast<Sm *>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = lane_id();
-    RcWarp<Px, SS> &Wp = S.w[warp];
-    FrameDesc &F = S.F[warp];
-    if (ctl.poison) {
-        smem_poison(smem_raw, sizeof(Sm), threadIdx.x, blockDim.x);
+    RcWarp<Px, SS> &Wp = S.ws[warp].w;
+    FrameDesc &F = S.ws[warp].F;
+    if (ctl.poison) {   // (the shared memory of the launch: the working warps' parts only)
+        smem_poison(smem_raw, rc_smem_bytes<Px, SS>(ctl.warps), threadIdx.x, blockDim.x);
         __syncthreads();
     }
     {   // all four cost tables (q-context 0 in the RateStage), the scans and base-context offsets

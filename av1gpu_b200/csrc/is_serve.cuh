@@ -177,8 +177,8 @@ static int serve_launch(is_handle *h) {
     ctl.readyWaitNs = SERVE_IDLE_NS;
     ctl.trace = nullptr;
     ctl.poison = h->poison ? 1 : 0;
-    ctl.warps = h->reconWarps > 0 ? std::min(h->reconWarps, S->warps) : S->warps;
-    const size_t sm = h->smemRcG[S->g];
+    ctl.warps = rc_warps_for(h, S->g, 2);   // (a session's loop serves many images)
+    const size_t sm = rc_launch_smem(S->g, ctl.warps);
     const FrameDesc *fs = S->dTable;
     const int g = S->g, grid = S->grid;
     IS_CK((g == 0 ? rc_launch<8, 1>(fs, 0, ctl, grid, sm, S->kst) : g == 1 ? rc_launch<8, 0>(fs, 0, ctl, grid, sm, S->kst)

@@ -253,9 +253,10 @@ extern "C" int is_set_trace(is_handle *h, int on) {
 }
 extern "C" int is_get_trace(is_handle *h, unsigned long long *out, size_t cap, uint32_t *n) {
     if (!h || !h->have || !h->F.leafTrace) return IS_ERR_STATE;
-    uint32_t tot = 0;
-    IS_CK(cudaMemcpy(&tot, h->F.leafTotal, 4, cudaMemcpyDeviceToHost));
-    *n = tot;
+    // the leaves of the ready queue image 0 took part in: its own, or those of its format group in a batch
+    int tot = 0;
+    IS_CK(cudaMemcpy(&tot, h->F.rq + 1, 4, cudaMemcpyDeviceToHost));
+    *n = (uint32_t)tot;
     const size_t m = std::min(cap, (size_t)tot * TRACE_STAMPS);
     IS_CK(cudaMemcpy(out, h->F.leafTrace, m * 8, cudaMemcpyDeviceToHost));
     return IS_OK;

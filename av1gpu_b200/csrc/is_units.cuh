@@ -53,6 +53,7 @@ template <int BD, int PART> cudaError_t an_launch(const FrameDesc &F, int nSb, c
 template <int BD, int SS> cudaError_t rc_upload(const TableBlob &B);
 // shared memory of the kernel and its co-resident CTAs per SM (the cooperative grid is that times the SM count)
 template <int BD, int SS> cudaError_t rc_setup(size_t *smem, int *ctasPerSm, int *warps);
+template <int BD, int SS> size_t rc_smem(int warps);   // dynamic shared memory of a launch with that many working warps
 struct RcCtl;
 template <int BD, int SS> cudaError_t rc_launch(const FrameDesc *fs, int nImg, const RcCtl &ctl, int grid, size_t smem, cudaStream_t st);
 

@@ -471,15 +471,15 @@ class Encoder:
     TRACE_STAMPS = 10
 
     def trace(self):
-        """Per queued leaf of the last encode (queue order), 10 values: globaltimer ns at slot claimed, slot read, luma
-        prologue done, luma pass 1 done, pass 2 done, luma published, chroma waits done, chroma RD done, leaf done; then
-        the queue entry (image << 32 | sb << 8 | leaf)."""
-        nb, _, _ = self.counts()
+        """Per queued leaf of the last encode (queue order; in a batch, image 0's format group), 10 values: globaltimer ns
+        at slot claimed, slot read, luma prologue done, luma pass 1 done, pass 2 done, luma published, chroma waits done,
+        chroma RD done, leaf done; then the queue entry (image << 32 | sb << 8 | leaf)."""
         k = self.TRACE_STAMPS
-        out = np.zeros(nb * k + k, np.uint64)
         n = C.c_uint32()
+        self._check(self.L.is_get_trace(self.h, None, 0, C.byref(n)), "is_get_trace")
+        out = np.zeros(n.value * k, np.uint64)
         self._check(self.L.is_get_trace(self.h, out.ctypes.data, out.size, C.byref(n)), "is_get_trace")
-        return out[:n.value * k].reshape(-1, k)
+        return out.reshape(-1, k)
 
     def debug_leaves(self, sb):
         b, x, y = (np.zeros(256, np.uint8) for _ in range(3))

@@ -20,6 +20,9 @@ SHAPES = (("c1w", (C1, 9)), ("c1b", (C1,)), ("c2w", (C2, 9 * C1)), ("c2b", (C2,)
           ("f1w", (HID, NZ)), ("f1b", (HID,)), ("f2w", (N_OUT, HID)), ("f2b", (N_OUT,)))
 N_PARAMS = sum(int(np.prod(s)) for _, s in SHAPES)
 # (mode, delta) class k -> candidate code (mode << 3 | delta + 3), as the library numbers them
+# the learned form of the batched workload: the selection rule, and the RD count of the blocks the network does not score
+LEARNED = dict(tau=0.8, max_cand=4, conf=0.0, rd_k=2, tx_tau=0.9, max_tx=2)
+LEARNED_OTHER = dict(rd_k=2)
 CLASS_CAND = np.array([(0 << 3 | 3), (9 << 3 | 3), (10 << 3 | 3), (11 << 3 | 3), (12 << 3 | 3)]
                       + [(1 + (k // 7)) << 3 | (k % 7) for k in range(56)], np.int32)
 
@@ -264,7 +267,21 @@ def main():
     ap.add_argument("--out", default="shortlist_weights.npz")
     ap.add_argument("--blocks-per-image", type=int, default=0, help="blocks drawn per image (0: all)")
     ap.add_argument("--workers", type=int, default=0, help="host processes for the image generator (0: all cores)")
+    ap.add_argument("--search", default="", help="WxH: only search the seeded synthetic picture of that size twice with the "
+                                                "shipped weights (the learned form) and print the stage times (profiling)")
     args = ap.parse_args()
+    if args.search:
+        from . import synth
+        w, h = (int(v) for v in args.search.lower().split("x"))
+        enc = Encoder(0)
+        enc.set_shortlist(load_params(os.path.join(os.path.dirname(os.path.abspath(__file__)), "shortlist_weights.npz")), **LEARNED)
+        enc.set_search_options(**LEARNED_OTHER)
+        planes = synth.make_image(w, h, 5, edges=True)
+        for _ in range(2):
+            enc.encode(planes, 120)
+        print(json.dumps(enc.times()))
+        enc.close()
+        return
     size = tuple(int(v) for v in args.size.split("x"))
     t0 = time.time()
     ims, qs = training_images(args.images, size, args.seed, workers=args.workers or os.cpu_count() or 1)

@@ -130,9 +130,9 @@ int is_set_search_options(is_handle *h, int rd_k, int tx_keep);
 int is_workspace_bytes(int width, int height, uint64_t *bytes);
 /* the same for a frame of the given format (bit_depth 8 / 10, chroma_444 0 / 1) */
 int is_workspace_bytes_format(int width, int height, int bit_depth, int chroma_444, uint64_t *bytes);
-/* Warps per CTA the closed loop runs (0: all the shared memory of a CTA holds - 8 for 8-bit 4:2:0, fewer for the
- * larger formats; 1 .. 8 caps it).  More warps per SM raise the loop's throughput when many leaves are ready at once (a
- * batch, a serving session); a single image's loop is bound by its dependency chain. */
+/* Warps per CTA the closed loop runs: 1 .. 8 caps it at the most the shared memory of a CTA holds (8 for 8-bit 4:2:0,
+ * fewer for the larger formats); 0 (the default) takes 4 for a single image - its loop is bound by its dependency chain,
+ * and fewer warps leave the SM a larger L1 - and all of them for a batch or a serving session. */
 int is_set_closed_loop_warps(is_handle *h, int warps);
 /* Autotuner: times the batch with 1, 2 and 4 front-end streams x 4, 6 and all closed-loop warps per CTA (two runs each,
  * the second timed) and keeps the fastest for the handle; returns the choice and its time (ms). */
@@ -199,7 +199,8 @@ int is_debug_tables(is_handle *h, int qctx, uint16_t *cost, size_t cap, int32_t 
 /* Closed-loop trace (debug): is_set_trace(h, 1) before an encode records, per queued leaf (queue order), 10 values:
  * the globaltimer (ns) when a worker claimed its queue slot, read the slot, finished the luma prologue (loads, edges,
  * contexts), luma pass 1, luma pass 2, published the luma, finished its chroma waits, the chroma screening and RD, and
- * the leaf; then the queue entry (image << 32 | sb << 8 | leaf).  is_get_trace copies n x 10 values. */
+ * the leaf; then the queue entry (image << 32 | sb << 8 | leaf).  The queue is image 0's: in a batch, that of image 0's
+ * format group (every image of the group).  is_get_trace copies up to cap / 10 leaves and sets n to the queue's leaves. */
 int is_set_trace(is_handle *h, int on);
 int is_get_trace(is_handle *h, unsigned long long *out, size_t cap, uint32_t *n);
 

@@ -16,8 +16,8 @@ pytestmark = pytest.mark.gpu
 WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "av1gpu_b200", "shortlist_weights.npz")
 QS = (40, 80, 120, 160, 200)
 # the learned form of the batched + shortlist workload, and the non-learned pruning it is compared with
-LEARNED = dict(tau=0.9, max_cand=6, conf=0.0, rd_k=2, tx_tau=0.9, max_tx=2)
-LEARNED_NL = dict(rd_k=2)           # the blocks the network does not score (4x4, 4x8, 8x4)
+LEARNED = SL.LEARNED                # the selection rule
+LEARNED_NL = SL.LEARNED_OTHER       # the blocks the network does not score (4x4, 4x8, 8x4)
 NONLEARNED = dict(rd_k=2)           # the same RD count for every block, no network
 
 
