@@ -60,12 +60,14 @@ def main():
     ap.add_argument("--max-cand", type=int, default=4)
     ap.add_argument("--conf", type=float, default=0.0)
     ap.add_argument("--rd-k", type=int, default=2)
-    ap.add_argument("--tx-tau", type=float, default=0.9)
+    ap.add_argument("--tx-tau", type=float, default=0.95)
     ap.add_argument("--rd-k-other", type=int, default=2, help="RD candidates of the blocks the network does not score")
-    ap.add_argument("--max-tx", type=int, default=2)
+    ap.add_argument("--max-tx", type=int, default=3)
     ap.add_argument("--nl-rd-k", type=int, default=0, help="also time the non-learned pruning with this RD count (0: no)")
     ap.add_argument("--nl-tx-keep", type=int, default=2, help="tx types the non-learned pruning keeps per block")
     ap.add_argument("--no-verify", action="store_true", help="skip the check that the batch equals the one-at-a-time search")
+    ap.add_argument("--profile", action="store_true", help="only search the 8-bit 4:2:0 images twice as one batch (2 front-end "
+                                                          "streams, every closed-loop warp, no graph) and print the stage times")
     args = ap.parse_args()
     t0 = time.time()
     work = workload(args.images, args.seed, args.max_mp)
@@ -103,6 +105,15 @@ def main():
         enc.set_closed_loop_warps(0)
         return min(ts), (k, w)
 
+    if args.profile:
+        idx = [i for i, f in enumerate(fmt) if f == (8, False)]
+        enc.set_batch_options(use_graph=False, front_streams=2)
+        for _ in range(2):
+            enc.encode_batch_async([dev[i] for i in idx], [qs[i] for i in idx], host=False)
+            torch.cuda.synchronize()
+        print(json.dumps({**base, "form": "profile: the %d 8-bit 4:2:0 images as one batch" % len(idx), "times": enc.times()}))
+        enc.close()
+        return
     plain()   # warm-up (workspace, tables)
     tp = plain()
     print(json.dumps({**base, "form": "plain, one image at a time", "mp_per_s": round(mp / tp, 2), "s": round(tp, 3)}), flush=True)

@@ -278,12 +278,12 @@ def main():
     ap.add_argument("--mode", default="stream", choices=["stream", "batch", "both"],
                     help="stream: continuous admission into running closed loops (is_serve_*); batch: batches per worker")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "shortlist_weights.npz"))
-    ap.add_argument("--tau", type=float, default=0.9)
-    ap.add_argument("--max-cand", type=int, default=8)
+    ap.add_argument("--tau", type=float, default=0.8)
+    ap.add_argument("--max-cand", type=int, default=4)
     ap.add_argument("--conf", type=float, default=0.0)
     ap.add_argument("--rd-k", type=int, default=2)
-    ap.add_argument("--tx-tau", type=float, default=0.9)
-    ap.add_argument("--max-tx", type=int, default=2)
+    ap.add_argument("--tx-tau", type=float, default=0.95)
+    ap.add_argument("--max-tx", type=int, default=3)
     args = ap.parse_args()
     reqs = _requests(args.n, 5)
     sl = None

@@ -21,7 +21,7 @@ SHAPES = (("c1w", (C1, 9)), ("c1b", (C1,)), ("c2w", (C2, 9 * C1)), ("c2b", (C2,)
 N_PARAMS = sum(int(np.prod(s)) for _, s in SHAPES)
 # (mode, delta) class k -> candidate code (mode << 3 | delta + 3), as the library numbers them
 # the learned form of the batched workload: the selection rule, and the RD count of the blocks the network does not score
-LEARNED = dict(tau=0.8, max_cand=4, conf=0.0, rd_k=2, tx_tau=0.9, max_tx=2)
+LEARNED = dict(tau=0.8, max_cand=4, conf=0.0, rd_k=2, tx_tau=0.95, max_tx=3)
 LEARNED_OTHER = dict(rd_k=2)
 CLASS_CAND = np.array([(0 << 3 | 3), (9 << 3 | 3), (10 << 3 | 3), (11 << 3 | 3), (12 << 3 | 3)]
                       + [(1 + (k // 7)) << 3 | (k % 7) for k in range(56)], np.int32)
