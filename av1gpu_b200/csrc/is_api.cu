@@ -259,6 +259,10 @@ struct is_handle {
     std::string graphKey;
     cudaGraphExec_t graphExec = nullptr;
     struct ServeSession *serve = nullptr;   // an open serving session (is_serve_open), or null
+    // entropy coding of the records (is_encode_obu): device scratch, pinned result staging, timing events
+    void *entScratch = nullptr;
+    size_t entBytes = 0;
+    cudaEvent_t entEv[2] = {nullptr, nullptr};
     int setErr(int code, const char *fmt, ...) {
         char b[512];
         va_list ap;
@@ -362,6 +366,7 @@ int upload_tables(int dev) {
         if (e == cudaSuccess) e = rc_upload<8, 0>(B);
         if (e == cudaSuccess) e = rc_upload<10, 1>(B);
         if (e == cudaSuccess) e = rc_upload<10, 0>(B);
+        if (e == cudaSuccess) e = ent_upload(B);
         g_uploaded[dev] = e == cudaSuccess;
         return e == cudaSuccess ? 0 : (int)e;
     }
@@ -495,6 +500,9 @@ void is_destroy(is_handle *h) {
     if (h->serve) is_serve_close(h);
     if (h->own) cudaStreamSynchronize(h->own);
     if (h->arena) cudaFree(h->arena);
+    if (h->entScratch) cudaFree(h->entScratch);
+    for (auto &e : h->entEv)
+        if (e) cudaEventDestroy(e);
     for (auto &e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->own) cudaStreamDestroy(h->own);
@@ -1082,6 +1090,112 @@ int is_record_device(const is_handle *h, const av1g_block **blocks, const uint32
     if (txb) *txb = h->F.recTxb;
     if (coeffs) *coeffs = h->F.recCoeffs;
     return IS_OK;
+}
+
+// the frame parameters of image i of the last batch (as is_batch_copy writes them)
+static void batch_fp(const is_handle *h, int i, av1g_frame_params *fp) {
+    const FrameDesc &F = h->bF[i];
+    memset(fp, 0, sizeof *fp);
+    fp->version = AV1G_DECISIONS_VERSION;
+    fp->width = (uint32_t)F.W; fp->height = (uint32_t)F.H;
+    fp->base_q_idx = (uint8_t)h->bQ[i];
+    fp->tile_cols_log2 = -1; fp->tile_rows_log2 = -1;
+    fp->qm_y = fp->qm_u = fp->qm_v = 15;
+    fp->chroma_format = F.ssx ? AV1G_CHROMA_420 : AV1G_CHROMA_444;
+    fp->bit_depth = (uint8_t)F.bd;
+}
+
+int is_entropy_scratch_bytes(const is_ent_frame *frames, int n, uint64_t cap, uint64_t *bytes) {
+    if (!bytes) return IS_ERR_INVALID;
+    size_t b = 0;
+    const int rc = ent_scratch(frames, n, cap, &b, nullptr);
+    if (rc == IS_OK) *bytes = b;
+    return rc;
+}
+
+int is_entropy_batch(int device, const is_ent_frame *frames, int n, uint64_t cap, void *scratch, uint64_t scratchBytes, void *stream,
+                     is_ent_out *out, uint32_t *frameTile0) {
+    if (!out) return IS_ERR_INVALID;
+    int nDev = 0;
+    if (cudaGetDeviceCount(&nDev) != cudaSuccess || device < 0 || device >= nDev) return IS_ERR_INVALID;
+    if (cudaSetDevice(device) != cudaSuccess || upload_tables(device)) return IS_ERR_CUDA;
+    return ent_launch(frames, n, cap, scratch, (size_t)scratchBytes, (cudaStream_t)stream, out, frameTile0, nullptr);
+}
+
+int is_obu_assemble(const av1g_frame_params *fp, const uint8_t *payload, const uint64_t *off, uint32_t nTiles, uint8_t *out, uint64_t cap,
+                    uint64_t *size) {
+    if (!fp || !payload || !off || !size || !nTiles) return IS_ERR_INVALID;
+    std::vector<uint8_t> o;
+    const int rc = obu_assemble(*fp, payload, off, nTiles, o, nullptr);
+    if (rc != IS_OK) return rc;
+    *size = o.size();
+    if (!out || cap < o.size()) return IS_ERR_TOO_LARGE;
+    memcpy(out, o.data(), o.size());
+    return IS_OK;
+}
+
+int is_encode_obu(is_handle *h, int first, int n, uint8_t *out, uint64_t cap, uint64_t *offsets, float *device_ms) {
+    if (!h || !h->have || first < 0 || n < 1 || first + n > h->bN) return h ? h->setErr(IS_ERR_STATE, "no such images") : IS_ERR_STATE;
+    if (!offsets) return h->setErr(IS_ERR_INVALID, "offsets missing");
+    IS_CK(cudaSetDevice(h->device));
+    std::vector<is_ent_frame> fr(n);
+    for (int k = 0; k < n; k++) {
+        const int i = first + k;
+        const FrameDesc &F = h->bF[i];
+        batch_fp(h, i, &fr[k].fp);
+        fr[k].blocks = F.recBlocks; fr[k].block_txb = F.recBlockTxb; fr[k].txb = F.recTxb; fr[k].coeffs = F.recCoeffs;
+        fr[k].n_blocks = h->bNb[i]; fr[k].n_txb = h->bNt[i];
+    }
+    for (auto &e : h->entEv)
+        if (!e) IS_CK(cudaEventCreate(&e));
+    uint64_t cap0 = 0;
+    std::vector<uint8_t> head;
+    is_ent_out eo;
+    std::vector<uint32_t> t0(n + 1);
+    for (int attempt = 0; attempt < 2; attempt++) {
+        size_t need = 0;
+        int rc = ent_scratch(fr.data(), n, cap0, &need, &h->err);
+        if (rc != IS_OK) return rc;
+        if (need > h->entBytes) {
+            if (h->entScratch) IS_CK(cudaFree(h->entScratch));
+            h->entScratch = nullptr;
+            h->entBytes = 0;
+            IS_CK(cudaMalloc(&h->entScratch, need));
+            h->entBytes = need;
+        }
+        IS_CK(cudaEventRecord(h->entEv[0], h->own));
+        rc = ent_launch(fr.data(), n, cap0, h->entScratch, h->entBytes, h->own, &eo, t0.data(), &h->err);
+        if (rc != IS_OK) return rc;
+        IS_CK(cudaEventRecord(h->entEv[1], h->own));
+        head.resize(eo.result_bytes);
+        IS_CK(cudaMemcpyAsync(head.data(), eo.result, eo.result_bytes, cudaMemcpyDeviceToHost, h->own));
+        IS_CK(cudaStreamSynchronize(h->own));
+        const is_ent_status *st = (const is_ent_status *)head.data();
+        if (st->error == IS_ENT_ERR_SYMBOLS && attempt == 0) { cap0 = st->symbols; continue; }
+        if (st->error) return h->setErr(IS_ERR_INVALID, "entropy coding failed: error bits %d (symbols %llu)", st->error,
+                                        (unsigned long long)st->symbols);
+        break;
+    }
+    if (device_ms) IS_CK(cudaEventElapsedTime(device_ms, h->entEv[0], h->entEv[1]));
+    const is_ent_status *st = (const is_ent_status *)head.data();
+    const uint64_t *toff = (const uint64_t *)(head.data() + sizeof(is_ent_status));
+    std::vector<uint8_t> pay(st->bytes);
+    if (st->bytes) IS_CK(cudaMemcpy(pay.data(), eo.payload, st->bytes, cudaMemcpyDeviceToHost));
+    uint64_t pos = 0;
+    std::vector<uint8_t> obu;
+    bool fits = true;
+    for (int k = 0; k < n; k++) {
+        std::vector<uint64_t> rel;
+        for (uint32_t t = t0[k]; t <= t0[k + 1]; t++) rel.push_back(toff[t] - toff[t0[k]]);
+        const int rc = obu_assemble(fr[k].fp, pay.data() + toff[t0[k]], rel.data(), t0[k + 1] - t0[k], obu, &h->err);
+        if (rc != IS_OK) return rc;
+        offsets[k] = pos;
+        if (out && pos + obu.size() <= cap) memcpy(out + pos, obu.data(), obu.size());
+        else fits = false;
+        pos += obu.size();
+    }
+    offsets[n] = pos;
+    return fits ? IS_OK : h->setErr(IS_ERR_TOO_LARGE, "the OBU streams need %llu bytes", (unsigned long long)pos);
 }
 
 int is_times_get(const is_handle *h, is_times *t) {

@@ -1,13 +1,15 @@
 // is_units.cuh - the library's compilation units and what they export to the host orchestration (is_api.cu).
 //
 // The kernels are compiled in separate units so that they build in parallel: is_k_an.cu once per bit depth and kernel
-// pair (the four analysis kernels), is_k_rc.cu once per format (the closed loop), is_api.cu (host API, DP, scheduling, pack,
-// learned-shortlist and test kernels).  Device globals have internal linkage (static): every unit holds its own copy
+// pair (the four analysis kernels), is_k_rc.cu once per format (the closed loop), is_k_ent.cu (entropy coding of the
+// records), is_api.cu (host API, DP, scheduling, pack, learned-shortlist and test kernels).  Device globals have internal linkage (static): every unit holds its own copy
 // of the search's tables, and upload_tables() in is_api.cu fills each unit's copy from one host-built TableBlob.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string>
 #include <vector>
+#include "is_api.h"
 #include "is_dev.cuh"
 #include "is_frame.cuh"
 
@@ -56,5 +58,17 @@ template <int BD, int SS> cudaError_t rc_setup(size_t *smem, int *ctasPerSm, int
 template <int BD, int SS> size_t rc_smem(int warps);   // dynamic shared memory of a launch with that many working warps
 struct RcCtl;
 template <int BD, int SS> cudaError_t rc_launch(const FrameDesc *fs, int nImg, const RcCtl &ctl, int grid, size_t smem, cudaStream_t st);
+
+// ---- entropy unit (is_k_ent.cu): records on the device -> tile payloads; OBU framing on the host ----
+struct TileGeom {   // uniform tile spacing (spec 5.9.15): log2 counts, their legal ranges, tile sizes in SBs, counts
+    int minLog2Cols, maxLog2Cols, minLog2Rows, maxLog2Rows, colsLog2, rowsLog2, wSb, hSb, cols, rows;
+};
+bool tile_info(int W, int H, int colsLog2, int rowsLog2, TileGeom &t);
+cudaError_t ent_upload(const TableBlob &B);
+int ent_scratch(const is_ent_frame *frames, int n, uint64_t cap, size_t *bytes, std::string *err);
+int ent_launch(const is_ent_frame *frames, int n, uint64_t cap, void *scratch, size_t scratchBytes, cudaStream_t s, is_ent_out *out,
+               uint32_t *frameTile0, std::string *err);
+int obu_assemble(const av1g_frame_params &fp, const uint8_t *payload, const uint64_t *off, uint32_t nTiles, std::vector<uint8_t> &o,
+                 std::string *err);
 
 }  // namespace is

@@ -23,6 +23,11 @@ BLOCK_DT = np.dtype([("mi_row", "<u2"), ("mi_col", "<u2"), ("bsize", "u1"), ("sk
 TXB_DT = np.dtype([("coeff_off", "<u4"), ("x4", "<u2"), ("y4", "<u2"), ("plane", "u1"), ("tx_size", "u1"),
                    ("tx_type", "u1"), ("flags", "u1"), ("eob", "<u2"), ("reserved", "<u2")])
 
+# av1g_frame_params (av1core/include/av1g/decisions.h:254-296): 88 bytes; the offsets of the fields the bindings write
+FRAME_PARAMS_BYTES = 88
+FP_BASE_Q_IDX, FP_TILE_LOG2, FP_QM, FP_CHROMA_FORMAT, FP_BIT_DEPTH = 13, 16, 28, 72, 73
+AV1G_DECISIONS_VERSION = 5
+
 IS_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "wavefront wait timeout",
              -5: "no result", -6: "too large for the static scratch", -7: "serving session busy"}
 IS_ERR_INVALID, IS_ERR_CUDA, IS_ERR_OOM, IS_ERR_TIMEOUT, IS_ERR_STATE, IS_ERR_TOO_LARGE, IS_ERR_BUSY = -1, -2, -3, -4, -5, -6, -7
@@ -59,7 +64,8 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_sl_get_params", "is_sl_forward", "is_sl_grads", "is_sl_train_step", "is_nn_gemm", "is_sl_dataset", "is_sl_infer",
            "is_set_shortlist_model",
            "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison", "is_set_search_options", "is_set_closed_loop_warps", "is_serve_open", "is_serve_start", "is_serve_submit", "is_serve_poll",
-           "is_serve_counts", "is_serve_copy", "is_serve_stop", "is_serve_close"]
+           "is_serve_counts", "is_serve_copy", "is_serve_stop", "is_serve_close", "is_entropy_scratch_bytes", "is_entropy_batch",
+           "is_obu_assemble", "is_encode_obu"]
 
 _lib = None
 
@@ -127,6 +133,10 @@ def load_library():
     L.is_serve_copy.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp * 3, vp]
     L.is_serve_stop.argtypes = [vp]
     L.is_serve_close.argtypes = [vp]
+    L.is_entropy_scratch_bytes.argtypes = [vp, C.c_int, C.c_uint64, C.POINTER(C.c_uint64)]
+    L.is_entropy_batch.argtypes = [C.c_int, vp, C.c_int, C.c_uint64, vp, C.c_uint64, vp, vp, vp]
+    L.is_obu_assemble.argtypes = [vp, vp, vp, C.c_uint32, vp, C.c_uint64, C.POINTER(C.c_uint64)]
+    L.is_encode_obu.argtypes = [vp, C.c_int, C.c_int, vp, C.c_uint64, vp, C.POINTER(C.c_float)]
     _lib = L
     return L
 
@@ -137,6 +147,35 @@ def workspace_bytes(width, height, bit_depth=8, chroma_444=False):
     if load_library().is_workspace_bytes_format(width, height, bit_depth, int(bool(chroma_444)), C.byref(b)) != 0:
         raise ValueError("invalid image %dx%d (bit depth %d, 4:4:4 %s)" % (width, height, bit_depth, chroma_444))
     return b.value
+
+
+def frame_params(width, height, qindex, bit_depth=8, chroma_444=False):
+    """The av1g_frame_params bytes the search writes for an image (is_batch_copy's fp)."""
+    fp = np.zeros(FRAME_PARAMS_BYTES, np.uint8)
+    fp[:12].view(np.uint32)[:] = (AV1G_DECISIONS_VERSION, width, height)
+    fp[FP_BASE_Q_IDX] = qindex
+    fp[FP_TILE_LOG2:FP_TILE_LOG2 + 2] = 0xFF        # tile_cols_log2 = tile_rows_log2 = -1: the minimum legal tiling
+    fp[FP_QM:FP_QM + 3] = 15                        # qm_y, qm_u, qm_v
+    fp[FP_CHROMA_FORMAT] = 1 if chroma_444 else 0
+    fp[FP_BIT_DEPTH] = bit_depth
+    return fp
+
+
+def obu_assemble(fp, payload, tile_offsets):
+    """The OBU stream (sequence header + frame OBU) of a frame from its tile payloads (host bytes) and offsets."""
+    L = load_library()
+    pay = np.frombuffer(bytes(payload), np.uint8) if not isinstance(payload, np.ndarray) else np.ascontiguousarray(payload, np.uint8)
+    off = np.ascontiguousarray(tile_offsets, np.uint64)
+    size = C.c_uint64()
+    fp = np.ascontiguousarray(fp, np.uint8)
+    rc = L.is_obu_assemble(fp.ctypes.data, pay.ctypes.data, off.ctypes.data, len(off) - 1, None, 0, C.byref(size))
+    if rc not in (0, IS_ERR_TOO_LARGE):
+        raise IsError(rc, "is_obu_assemble failed (%d)" % rc)
+    out = np.zeros(size.value, np.uint8)
+    rc = L.is_obu_assemble(fp.ctypes.data, pay.ctypes.data, off.ctypes.data, len(off) - 1, out.ctypes.data, size.value, C.byref(size))
+    if rc != 0:
+        raise IsError(rc, "is_obu_assemble failed (%d)" % rc)
+    return out.tobytes()
 
 
 def plane_format(planes):
@@ -326,6 +365,19 @@ class Encoder:
             bd, c444 = plane_format(im)
             out.append(self.batch_fetch(i, im[0].shape[1], im[0].shape[0], q, bd, c444))
         return out
+
+    def obu(self, first=0, n=1, timed=False):
+        """Images first .. first + n - 1 of the last encode entropy-coded on the device in one batch: a list of OBU
+        streams (bytes, av1g_encode()'s obu), and with timed=True also the device time of the coding (ms)."""
+        offs = np.zeros(n + 1, np.uint64)
+        ms = C.c_float()
+        rc = self.L.is_encode_obu(self.h, first, n, None, 0, offs.ctypes.data, C.byref(ms))
+        if rc != IS_ERR_TOO_LARGE:
+            self._check(rc, "is_encode_obu")
+        buf = np.zeros(int(offs[n]), np.uint8)
+        self._check(self.L.is_encode_obu(self.h, first, n, buf.ctypes.data, buf.size, offs.ctypes.data, C.byref(ms)), "is_encode_obu")
+        out = [buf[int(offs[k]):int(offs[k + 1])].tobytes() for k in range(n)]
+        return (out, ms.value) if timed else out
 
     def set_wait_limits(self, leaf_wait_iters=0, ready_wait_ns=0):
         """Closed-loop wait budgets (0: the defaults); a wait that runs out makes the encode raise IsError(-4)."""

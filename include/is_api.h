@@ -36,7 +36,7 @@ extern "C" {
 #define IS_ERR_OOM -3       /* device allocation failed */
 #define IS_ERR_TIMEOUT -4   /* a wavefront dependency wait of the closed loop ran out of its budget (no hang) */
 #define IS_ERR_STATE -5     /* no encode result to read */
-#define IS_ERR_TOO_LARGE -6 /* the request does not fit the fixed scratch of is_fwd_quant_static */
+#define IS_ERR_TOO_LARGE -6 /* the request does not fit the fixed scratch of is_fwd_quant_static, or an output buffer */
 #define IS_ERR_BUSY -7      /* a serving session has no room for the image now: poll, copy finished images, retry */
 
 typedef struct is_params {
@@ -173,6 +173,57 @@ int is_serve_copy(is_handle *h, int ticket, av1g_frame_params *fp, av1g_block *b
  * running kernel); is_serve_close stops if needed and frees the session */
 int is_serve_stop(is_handle *h);
 int is_serve_close(is_handle *h);
+
+/* ---- entropy coding on the device: records -> AV1 bitstream ----
+ * Replaces av1core's GPU entropy coder av1g_gpu::run_batch_device_scratch_bytes / run_batch_device
+ * (av1core/include/av1g/gpu_entropy.h:73-147) and the OBU assembly after it (Encoder::write_headers,
+ * av1core/src/encoder.cpp:1317-1441, and the framing of Encoder::run, :1571-1600).  The payloads are byte for byte those
+ * of av1g_encode() on the same records.  Records of the search's toolset: lossy, 4:2:0 or 4:4:4, 8- or 10-bit, tx_depth
+ * 0, no delta-q / CDEF / palette / filter intra / reduced tx set (IS_ERR_INVALID otherwise); header-only fields (tiling,
+ * delta_q_* of the planes, quantizer matrices, loop-filter levels, colour description) are free. */
+typedef struct is_ent_frame {
+    av1g_frame_params fp;        /* host copy of the frame parameters */
+    const av1g_block *blocks;    /* device: n_blocks blocks in decode order */
+    const uint32_t *block_txb;   /* device: n_blocks + 1 entries (the av1g_layout() of the blocks) */
+    const av1g_txb *txb;         /* device: n_txb tx blocks; the chroma tx_type and eob fields are not read (derived) */
+    const int16_t *coeffs;       /* device: the levels, txb[].coeff_off relative to this pointer */
+    uint32_t n_blocks, n_txb;
+} is_ent_frame;
+#define IS_ENT_ERR_SYMBOLS 1     /* more symbols than the capacity: status.symbols is the count needed (rerun with it) */
+#define IS_ENT_ERR_OUTPUT 2      /* a tile's payload outgrew its buffer */
+#define IS_ENT_ERR_RECORD 4      /* blocks out of decode order, a partition the syntax cannot code, a field out of range */
+typedef struct is_ent_status {   /* the head of the device result */
+    int32_t error;               /* 0 or IS_ENT_ERR_* bits; the payloads are valid only for 0 */
+    int32_t reserved;
+    uint64_t symbols;            /* symbols of the batch (also when it exceeded the capacity) */
+    uint64_t capacity;
+    uint64_t bytes;              /* payload bytes of every tile */
+} is_ent_status;
+typedef struct is_ent_out {
+    const void *result;          /* device: is_ent_status, then uint64_t tile_offset[n_tiles + 1] (one download) */
+    uint64_t result_bytes;
+    const uint8_t *payload;      /* device: tile i of the batch = payload[tile_offset[i] .. tile_offset[i + 1]) */
+    uint64_t payload_capacity;
+    uint32_t n_tiles;            /* frame f owns tiles frame_tile0[f] .. frame_tile0[f + 1] - 1 (raster order) */
+} is_ent_out;
+/* Scratch the batch needs with a symbol capacity (0: a default bound from the frames' sizes). */
+int is_entropy_scratch_bytes(const is_ent_frame *frames, int n, uint64_t symbol_capacity, uint64_t *bytes);
+/* Enqueue the coding of n frames on stream (a cudaStream_t; NULL = the legacy default stream of device): no allocation,
+ * no synchronisation.  scratch: device memory of at least is_entropy_scratch_bytes(), 256-byte aligned; it and the
+ * out pointers belong to the call until the stream has passed it.  frame_tile0: n + 1 entries (host) or NULL. */
+int is_entropy_batch(int device, const is_ent_frame *frames, int n, uint64_t symbol_capacity, void *scratch, uint64_t scratch_bytes,
+                     void *stream, is_ent_out *out, uint32_t *frame_tile0);
+/* The OBU stream of one frame (sequence header OBU + frame OBU, no temporal delimiter; av1g_encode()'s obu bytes) from
+ * its tile payloads (host memory, tile i = payload[tile_offset[i] .. tile_offset[i + 1])).  *size gets the length;
+ * IS_ERR_TOO_LARGE when cap is smaller (nothing written). */
+int is_obu_assemble(const av1g_frame_params *fp, const uint8_t *payload, const uint64_t *tile_offset, uint32_t n_tiles, uint8_t *out,
+                    uint64_t cap, uint64_t *size);
+/* Images first .. first + n - 1 of the handle's last encode (batch order; a single image is image 0) coded on the device
+ * in one batch and returned as OBU streams back to back: image k at out[offsets[k] .. offsets[k + 1]).  The handle keeps
+ * the scratch; a symbol count above the default capacity reruns once with the exact count.  device_ms (may be NULL):
+ * the device time of the coding kernels.  IS_ERR_TOO_LARGE when cap is smaller than the streams (offsets[n] = the bytes
+ * needed). */
+int is_encode_obu(is_handle *h, int first, int n, uint8_t *out, uint64_t cap, uint64_t *offsets, float *device_ms);
 
 /* ---- kernel-level entry points for the parity tests (device primitives of av1core's dsp.h API) ---- */
 /* Forward 2-D transform (this project's integer transform) + quantisation + rate of n residual blocks of one tx

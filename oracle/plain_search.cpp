@@ -1677,6 +1677,46 @@ extern "C" int orc_av1g_recon_arrays(int width, int height, int qindex, int bd, 
     return orc_av1g_recon(&rec, recon, err, errlen, obu_bytes);
 }
 
+// av1g_encode()'s OBU stream of a record (the bitstream only) and, from av1g_parse() of it, where each tile payload lies
+extern "C" int orc_av1g_obu_arrays(int width, int height, int qindex, int bd, int chroma_444, uint32_t n_blocks, av1g_block *blocks,
+                                   uint32_t *block_txb, uint32_t n_txb, av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs, uint8_t *obu,
+                                   uint64_t cap, uint64_t *size, uint32_t *n_tiles, uint64_t *tile_off, uint32_t *tile_bytes, uint32_t tile_cap,
+                                   char *err, size_t errlen) {
+    av1g_decision_record rec;
+    memset(&rec, 0, sizeof rec);
+    rec.fp.version = AV1G_DECISIONS_VERSION;
+    rec.fp.width = (uint32_t)width;
+    rec.fp.height = (uint32_t)height;
+    rec.fp.base_q_idx = (uint8_t)qindex;
+    rec.fp.tile_cols_log2 = -1;
+    rec.fp.tile_rows_log2 = -1;
+    rec.fp.qm_y = rec.fp.qm_u = rec.fp.qm_v = 15;
+    rec.fp.chroma_format = chroma_444 ? AV1G_CHROMA_444 : AV1G_CHROMA_420;
+    rec.fp.bit_depth = (uint8_t)bd;
+    rec.n_blocks = n_blocks;
+    rec.blocks = blocks;
+    rec.block_txb = block_txb;
+    rec.n_txb = n_txb;
+    rec.txb = txb;
+    rec.n_coeffs = n_coeffs;
+    rec.coeffs = coeffs;
+    av1g_encode_opts o = {AV1G_ENC_BITSTREAM_ONLY, -1};
+    av1g_output out;
+    memset(&out, 0, sizeof out);
+    int rc = av1g_encode(&rec, &o, &out);
+    if (rc != AV1G_OK) { if (err) snprintf(err, errlen, "%s", out.error); av1g_output_free(&out); return rc; }
+    *size = out.obu_size;
+    if (obu && cap >= out.obu_size) memcpy(obu, out.obu, out.obu_size);
+    av1g_parsed *ps = nullptr;
+    rc = av1g_parse(out.obu, out.obu_size, &ps);
+    av1g_output_free(&out);
+    if (rc != AV1G_OK) { if (err) snprintf(err, errlen, "av1g_parse %d: %s", rc, ps ? ps->error : ""); av1g_parsed_free(ps); return rc; }
+    *n_tiles = ps->n_tiles;
+    for (uint32_t i = 0; i < ps->n_tiles && i < tile_cap; i++) { tile_off[i] = ps->tile_offsets[i]; tile_bytes[i] = ps->tile_bytes[i]; }
+    av1g_parsed_free(ps);
+    return 0;
+}
+
 extern "C" void orc_qstep(int qindex, int bd, int *dcq, int *acq) {
     *dcq = av1g_dc_q_bd(qindex, bd);
     *acq = av1g_ac_q_bd(qindex, bd);
