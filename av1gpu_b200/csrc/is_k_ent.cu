@@ -5,7 +5,7 @@
 //
 // Every context of the intra syntax is a function of the record alone (neighbouring blocks' sizes, modes and skip
 // flags, neighbouring tx blocks' cumulative levels and DC signs), never of the adapted CDF values, so the symbols are
-// made in parallel and only the range coder with its CDF adaptation runs in order, one warp per tile:
+// made in parallel and only the range coder with its CDF adaptation runs in order, per tile:
 //   k_ent_blocks  one thread per block: the 4x4 mode-info maps (size, luma mode, skip), each SB's first block, the
 //                 owner block of each tx block
 //   k_ent_txb     one thread per tx block: end of block, cumulative level and DC category (into per-plane 4x4 maps),
@@ -15,8 +15,9 @@
 //   scans         exclusive sums of the blocks' and tx blocks' symbol counts: where each block's and tx block's
 //                 symbols start in the batch's stream, which is in bitstream order
 //   k_ent_emit_*  the symbols into the stream (one thread per block / tx block)
-//   k_ent_code    one warp per tile: the CDF state in shared memory, the warp stages the tile's symbols in chunks,
-//                 lane 0 adapts and range-codes them, then resolves the carries
+//   k_ent_code    two warps per tile: the CDF state in shared memory; one warp adapts the CDFs and works out the
+//                 symbols' interval bounds 32 at a time, one lane range-codes the bounds of the batch before, then
+//                 resolves the carries
 //   k_ent_pack    the tiles' payloads back to back, offsets in the result head
 // A symbol is one 32-bit word: kind (adaptive / equiprobable bit / split-or-horizontal / split-or-vertical), alphabet
 // size, value and the CDF's offset inside av1g_cdfs.
@@ -35,7 +36,6 @@ static __device__ uint16_t g_cdfInit[4][NCDF];   // av1g_cdfs of each coefficien
 
 constexpr uint32_t NONE32 = 0xFFFFFFFFu;
 constexpr int HEAD_WORDS = 12;   // partition symbols (at most 4: 64, 32, 16, 8) + mode info (at most 8) of a block
-constexpr int CODE_CHUNK = 2048; // symbols a coding warp stages at a time
 enum { SYM_ADAPT = 0, SYM_BIT = 1, SYM_SPLIT_H = 2, SYM_SPLIT_V = 3 };
 
 __device__ __forceinline__ uint32_t sym_word(int kind, int cdf, int s, int N) {
@@ -431,6 +431,7 @@ __global__ void k_ent_tiles(EntArgs A) {
         if (total > A.cap) ent_fail(A, IS_ENT_ERR_SYMBOLS);
     }
     if (g >= A.nTiles) return;
+    if (A.status->error & IS_ENT_ERR_RECORD) { A.symBegin[g] = 0; return; }   // a bad record's offsets are not trusted
     const EntFrameD &F = A.fr[ent_find(A.fTile, A.nF, g)];
     const int t = (int)(g - F.tileBase), tr = t / F.tileCols, tc = t - tr * F.tileCols;
     const uint32_t gb = A.sbFirst[F.sbBase + tr * F.tileHSb * F.sbCols + tc * F.tileWSb];
@@ -582,8 +583,8 @@ __global__ void k_ent_emit_txb(EntArgs A) {
 }
 
 // ---- the range coder: AV1's multi-symbol arithmetic coder (spec 8.2.6 read_symbol, from the encoder's side; the
-// interval split, renormalisation and flush follow libaom's od_ec_encode_q15 / od_ec_enc_done, which the decoder's
-// arithmetic fixes to the bit).  Output goes to a precarry buffer of 16-bit entries (a byte plus a possible carry);
+// interval split (15-bit probabilities, 4 per symbol reserved), renormalisation and flush follow libaom's
+// od_ec_encode_q15 / od_ec_enc_done, which the decoder's arithmetic fixes to the bit).  Output goes to a precarry buffer of 16-bit entries (a byte plus a possible carry);
 // the carries are resolved backwards when the tile is done. ----
 struct RangeEnc {
     uint32_t low, rng;
@@ -596,34 +597,31 @@ struct RangeEnc {
         if (n < cap) pre[n] = (uint16_t)v; else over = true;
         n++;
     }
-    // symbol s of an alphabet of nm1 + 1 symbols; fl / fh: 32768 x the probability of the symbols after s - 1 / s
-    __device__ __forceinline__ void code(uint32_t fl, uint32_t fh, int s, int nm1) {
-        uint32_t l = low, r = rng;
-        const uint32_t r8 = r >> 8;
-        const uint32_t v = ((r8 * (fh >> 6)) >> 1) + 4u * (uint32_t)(nm1 - s);
-        if (fl < 32768u) {
-            const uint32_t u = ((r8 * (fl >> 6)) >> 1) + 4u * (uint32_t)(nm1 - s + 1);
-            l += r - u;
-            r = u - v;
-        } else {
-            r -= v;
-        }
-        // renormalise r to 16 bits; every 8 bits of low that pass the window go out
-        const int d = __clz(r) - 16;
-        int s2 = cnt + d;
-        if (s2 >= 0) {
+    // one symbol from its packed step (pack_step): the interval split of the symbol, then renormalisation of the range
+    // to 16 bits, where every 8 bits of low that pass the window go out.  The arithmetic chain through the range is
+    // kept short: the probability terms come precomputed.
+    __device__ __forceinline__ void step(uint32_t e) {
+        const uint32_t r = rng, r8 = r >> 8;
+        const uint32_t ev = (e >> 20) & 63u;
+        const uint32_t v = ((r8 * ((e >> 10) & 0x3FFu)) >> 1) + ev;
+        const uint32_t u = (e >> 26) ? r : ((r8 * (e & 0x3FFu)) >> 1) + ev + 4u;
+        uint32_t l = low + (r - u);
+        const uint32_t rn = u - v;
+        const int d = __clz(rn) - 16;
+        int s = cnt + d;
+        if (s >= 0) {
             int c = cnt + 16;
-            const int bytes = s2 >= 8 ? 2 : 1;
+            const int bytes = s >= 8 ? 2 : 1;
             for (int i = 0; i < bytes; i++) {
                 out(l >> c);
                 l &= (1u << c) - 1;
                 c -= 8;
             }
-            s2 = c + d - 16;
+            s = c + d - 16;
         }
         low = l << d;
-        rng = r << d;
-        cnt = s2;
+        rng = rn << d;
+        cnt = s;
     }
     // flush: the shortest tail that keeps the final interval decodable, then the carries; returns the byte count
     __device__ uint32_t finish(uint8_t *bytes) {
@@ -649,6 +647,11 @@ struct RangeEnc {
         return n;
     }
 };
+// the coder's inputs of symbol s of an alphabet of nm1 + 1 symbols with bounds fl / fh (32768 x the probability of the
+// symbols after s - 1 / after s): fl >> 6, fh >> 6, 4 (nm1 - s), and whether fl is the whole range
+__device__ __forceinline__ uint32_t pack_step(uint32_t fl, uint32_t fh, int s, int nm1) {
+    return (fl >> 6) | ((fh >> 6) << 10) | ((uint32_t)(4 * (nm1 - s)) << 20) | ((fl >= 32768u ? 1u : 0u) << 26);
+}
 
 // CDF adaptation (spec 8.2.6 symbol decoding process, disable_cdf_update 0): spec-format CDF (cumulative, last
 // entry 32768) followed by its counter
@@ -672,48 +675,122 @@ __device__ __forceinline__ uint32_t split_mass(const uint16_t *pc, bool vert) {
                       P(AV1G_PARTITION_VERT_B) + P(AV1G_PARTITION_VERT_4);
 }
 
-__global__ void __launch_bounds__(32) k_ent_code(EntArgs A) {
+// Two warps per tile.  Warp 0 turns the symbols into coder inputs 32 at a time: a symbol's interval bounds (fl, fh)
+// depend on its CDF as the earlier symbols left it, so the symbols of a window that share a CDF form a group (lanes
+// with equal CDF offsets) whose lowest lane walks them in order, adapting the CDF - in registers for alphabets of up
+// to 4 symbols (the coefficient CDFs, which carry long runs), in shared memory otherwise; groups and the equiprobable
+// bits proceed side by side; each symbol leaves its coder step (pack_step).  Lane 0 of warp 1 runs only the range
+// coder's arithmetic over the previous batch of steps, so the two overlap batch by batch.
+constexpr int CODE_BATCH = 1024;   // symbols per batch (a multiple of 32)
+
+// the coder step of symbol s of a CDF of up to 4 symbols held as c0..c2 (the last entry is 32768), then its adaptation
+__device__ __forceinline__ uint32_t bounds_small(uint32_t c[3], uint32_t &count, int s, int N) {
+    const uint32_t cs = s == 0 ? c[0] : s == 1 ? (N > 2 ? c[1] : 32768u) : s == 2 ? (N > 3 ? c[2] : 32768u) : 32768u;
+    const uint32_t cp = s == 1 ? c[0] : s == 2 ? c[1] : c[2];
+    const uint32_t fl = s ? 32768u - cp : 32768u, fh = 32768u - cs;
+    const int rate = 3 + (count > 15) + (count > 31) + (N > 3 ? 2 : 1);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+        if (i < N - 1) c[i] = i < s ? c[i] - (c[i] >> rate) : c[i] + ((32768u - c[i]) >> rate);
+    count += count < 32;
+    return pack_step(fl, fh, s, N - 1);
+}
+
+__global__ void __launch_bounds__(64) k_ent_code(EntArgs A) {
     __shared__ __align__(16) uint16_t cdf[NCDF];
-    __shared__ uint32_t buf[CODE_CHUNK];
+    __shared__ uint32_t bnd[2][CODE_BATCH];   // the coder steps (pack_step)
+    __shared__ uint32_t words[CODE_BATCH];    // warp 0's batch of symbol words
     const uint32_t g = blockIdx.x;
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (A.status->error) return;
     const EntFrameD &F = A.fr[ent_find(A.fTile, A.nF, g)];
     {
         const uint4 *src = reinterpret_cast<const uint4 *>(g_cdfInit[F.qctx]);
-        for (int i = lane; i < NCDF / 8; i += 32) reinterpret_cast<uint4 *>(cdf)[i] = src[i];
+        for (int i = threadIdx.x; i < NCDF / 8; i += 64) reinterpret_cast<uint4 *>(cdf)[i] = src[i];
     }
     const uint64_t s0 = A.symBegin[g], s1 = A.symBegin[g + 1];
     const uint64_t base = 2 * s0 + 16 * (uint64_t)g;
+    const uint32_t nb = (uint32_t)((s1 - s0 + CODE_BATCH - 1) / CODE_BATCH);
     RangeEnc E;
     E.init(A.pre + base, (uint32_t)(2 * (s1 - s0) + 16));
-    __syncwarp();
-    for (uint64_t i = s0; i < s1; i += CODE_CHUNK) {
-        const int n = (int)min((uint64_t)CODE_CHUNK, s1 - i);
-        for (int j = lane; j < n; j += 32) buf[j] = A.syms[i + j];
-        __syncwarp();
-        if (lane == 0) {
-            for (int j = 0; j < n; j++) {
-                const uint32_t w = buf[j];
+    __syncthreads();
+    for (uint32_t b = 0; b <= nb; b++) {
+        if (warp == 0 && b < nb) {
+            const uint64_t at = s0 + (uint64_t)b * CODE_BATCH;
+            const int n = (int)min((uint64_t)CODE_BATCH, s1 - at);
+            uint32_t *pb = bnd[b & 1];
+#pragma unroll 8
+            for (int j = lane; j < n; j += 32) words[j] = A.syms[at + j];   // the batch's loads in flight together
+            __syncwarp();
+            for (int j = 0; j < n; j += 32) {
+                const bool live = j + lane < n;
+                const uint32_t w = live ? words[j + lane] : (uint32_t)SYM_BIT;
                 const int kind = w & 3, nm1 = (w >> 2) & 15, s = (w >> 6) & 15;
-                uint16_t *c = cdf + (w >> 16);
-                if (kind == SYM_ADAPT) {
-                    E.code(s ? 32768u - c[s - 1] : 32768u, 32768u - c[s], s, nm1);
-                    adapt(c, s, nm1 + 1);
-                } else if (kind == SYM_BIT) {
-                    E.code(s ? 16384u : 32768u, s ? 0u : 16384u, s, 1);
-                } else {
-                    const uint32_t m = split_mass(c, kind == SYM_SPLIT_V);
-                    E.code(s ? m : 32768u, s ? 0u : m, s, 1);
+                const uint32_t key = kind == SYM_BIT ? 0x80000000u | lane : (w >> 16);
+                const uint32_t same = __match_any_sync(0xffffffffu, key);
+                if (live) {
+                    if (kind == SYM_BIT) {
+                        pb[j + lane] = pack_step(s ? 16384u : 32768u, s ? 0u : 16384u, s, 1);
+                    } else if (lane == __ffs(same) - 1) {   // the group's leader walks its members in order
+                        uint16_t *c = cdf + (w >> 16);
+                        const uint32_t m = same;   // only live lanes carry CDF keys
+                        bool small = kind == SYM_ADAPT && nm1 < 4;
+                        for (uint32_t t = m; t && small; t &= t - 1) small = (words[j + __ffs(t) - 1] & 3) == SYM_ADAPT;
+                        if (small) {
+                            const int N = nm1 + 1;
+                            uint32_t cv[3] = {c[0], N > 2 ? c[1] : 0u, N > 3 ? c[2] : 0u};
+                            uint32_t count = c[N];
+                            int k = j + __ffs(m) - 1;
+                            uint32_t wk = words[k];
+                            for (uint32_t t = m; t;) {   // the next member's word is loaded while this one is coded
+                                const uint32_t tn = t & (t - 1);
+                                const int kn = tn ? j + __ffs(tn) - 1 : k;
+                                const uint32_t wn = words[kn];
+                                pb[k] = bounds_small(cv, count, (wk >> 6) & 15, N);
+                                t = tn;
+                                k = kn;
+                                wk = wn;
+                            }
+                            c[0] = (uint16_t)cv[0];
+                            if (N > 2) c[1] = (uint16_t)cv[1];
+                            if (N > 3) c[2] = (uint16_t)cv[2];
+                            c[N] = (uint16_t)count;
+                        } else {
+                            for (uint32_t t = m; t; t &= t - 1) {
+                                const int k = j + __ffs(t) - 1;
+                                const uint32_t wk = words[k];
+                                const int kk = wk & 3, nk = (wk >> 2) & 15, sk = (wk >> 6) & 15;
+                                uint32_t fl, fh;
+                                if (kk == SYM_ADAPT) {
+                                    fl = sk ? 32768u - c[sk - 1] : 32768u;
+                                    fh = 32768u - c[sk];
+                                    adapt(c, sk, nk + 1);
+                                } else {
+                                    const uint32_t ms = split_mass(c, kk == SYM_SPLIT_V);
+                                    fl = sk ? ms : 32768u;
+                                    fh = sk ? 0u : ms;
+                                }
+                                pb[k] = pack_step(fl, fh, sk, nk);
+                            }
+                        }
+                    }
                 }
+                __syncwarp();
             }
         }
-        __syncwarp();
+        if (warp == 1 && lane == 0 && b > 0) {
+            const uint64_t at = s0 + (uint64_t)(b - 1) * CODE_BATCH;
+            const int n = (int)min((uint64_t)CODE_BATCH, s1 - at);
+            const uint32_t *pb = bnd[(b - 1) & 1];
+#pragma unroll 4
+            for (int j = 0; j < n; j++) E.step(pb[j]);
+        }
+        __syncthreads();
     }
-    if (lane == 0) {
-        const uint32_t nb = E.finish(A.tbytes + base);
+    if (warp == 1 && lane == 0) {
+        const uint32_t bytes = E.finish(A.tbytes + base);
         if (E.over) ent_fail(A, IS_ENT_ERR_OUTPUT);
-        A.tileBytes[g] = nb;
+        A.tileBytes[g] = bytes;
     }
 }
 
@@ -978,7 +1055,7 @@ int ent_launch(const is_ent_frame *frames, int n, uint64_t cap, void *scratch, s
         k_ent_tiles<<<grid(P.nTiles, 128), 128, 0, s>>>(A);
         k_ent_emit_head<<<grid(P.nB, 256), 256, 0, s>>>(A);
         if (P.nT) k_ent_emit_txb<<<grid(P.nT, 128), 128, 0, s>>>(A);
-        k_ent_code<<<P.nTiles, 32, 0, s>>>(A);
+        k_ent_code<<<P.nTiles, 64, 0, s>>>(A);
         k_ent_offsets<<<1, SCAN_T, 0, s>>>(A);
         k_ent_pack<<<P.nTiles, 256, 0, s>>>(A);
         e = cudaGetLastError();

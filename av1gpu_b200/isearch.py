@@ -371,11 +371,16 @@ class Encoder:
         streams (bytes, av1g_encode()'s obu), and with timed=True also the device time of the coding (ms)."""
         offs = np.zeros(n + 1, np.uint64)
         ms = C.c_float()
-        rc = self.L.is_encode_obu(self.h, first, n, None, 0, offs.ctypes.data, C.byref(ms))
-        if rc != IS_ERR_TOO_LARGE:
-            self._check(rc, "is_encode_obu")
-        buf = np.zeros(int(offs[n]), np.uint8)
-        self._check(self.L.is_encode_obu(self.h, first, n, buf.ctypes.data, buf.size, offs.ctypes.data, C.byref(ms)), "is_encode_obu")
+        px = 0
+        for i in range(first, first + n):
+            nb, _, nc = self.batch_counts(i)
+            px += nc + 16 * nb
+        buf = np.empty(8 * px + 65536, np.uint8)   # above any stream of these records: one coding in the common case
+        rc = self.L.is_encode_obu(self.h, first, n, buf.ctypes.data, buf.size, offs.ctypes.data, C.byref(ms))
+        if rc == IS_ERR_TOO_LARGE:
+            buf = np.empty(int(offs[n]), np.uint8)
+            rc = self.L.is_encode_obu(self.h, first, n, buf.ctypes.data, buf.size, offs.ctypes.data, C.byref(ms))
+        self._check(rc, "is_encode_obu")
         out = [buf[int(offs[k]):int(offs[k + 1])].tobytes() for k in range(n)]
         return (out, ms.value) if timed else out
 

@@ -82,12 +82,13 @@ int orc_av1g_recon_arrays(int width, int height, int qindex, int bd, int chroma_
                           uint32_t *block_txb, uint32_t n_txb, av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs,
                           void *recon[3], char *err, size_t errlen, uint64_t *obu_bytes);
 
-/* av1g_encode()'s OBU stream of such a record (bitstream only; obu may be NULL to ask for the size) and where av1g_parse()
- * finds each tile payload in it (offsets from the start of the stream, byte counts; tile_cap entries at most). */
+/* av1g_encode()'s OBU stream of such a record (bitstream only; obu may be NULL to ask for the size), its symbol count, and
+ * where av1g_parse() finds each tile payload in it (offsets from the start of the stream, byte counts; tile_cap entries at
+ * most). */
 int orc_av1g_obu_arrays(int width, int height, int qindex, int bd, int chroma_444, uint32_t n_blocks, av1g_block *blocks,
                         uint32_t *block_txb, uint32_t n_txb, av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs, uint8_t *obu,
                         uint64_t cap, uint64_t *size, uint32_t *n_tiles, uint64_t *tile_off, uint32_t *tile_bytes, uint32_t tile_cap,
-                        char *err, size_t errlen);
+                        uint64_t *n_symbols, char *err, size_t errlen);
 
 #ifdef __cplusplus
 }

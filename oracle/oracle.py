@@ -45,8 +45,8 @@ def lib():
                                                             C.c_size_t, C.POINTER(C.c_uint64)]
         L.orc_av1g_obu_arrays.argtypes = [C.c_int] * 5 + [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                                           C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
-                                                          C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_uint32, C.c_char_p,
-                                                          C.c_size_t]
+                                                          C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_uint32,
+                                                          C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]
         L.orc_fwd2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.orc_inv2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.orc_inv2d.restype = C.c_uint32
@@ -158,26 +158,29 @@ def av1g_recon(width, height, qindex, blocks, block_txb, txb, coeffs, bit_depth=
     return outs, nbytes.value
 
 
-def av1g_obu(width, height, qindex, blocks, block_txb, txb, coeffs, bit_depth=8, chroma_444=False):
-    """av1g_encode()'s OBU stream of a record (bytes) and the tile payloads' (offset, size) in it, from av1g_parse()."""
+def av1g_obu(width, height, qindex, blocks, block_txb, txb, coeffs, bit_depth=8, chroma_444=False, symbols=False):
+    """av1g_encode()'s OBU stream of a record (bytes) and the tile payloads' (offset, size) in it, from av1g_parse();
+    with symbols=True also the number of symbols av1g_encode() coded."""
     blocks = np.ascontiguousarray(blocks)
     block_txb = np.ascontiguousarray(block_txb, np.uint32)
     txb = np.ascontiguousarray(txb).copy()
     coeffs = np.ascontiguousarray(coeffs, np.int16).copy()
     err = C.create_string_buffer(256)
-    size, nt = C.c_uint64(), C.c_uint32()
+    size, nt, nsym = C.c_uint64(), C.c_uint32(), C.c_uint64()
     toff, tby = np.zeros(4096, np.uint64), np.zeros(4096, np.uint32)
     args = (width, height, qindex, bit_depth, int(chroma_444), len(blocks), blocks.ctypes.data, block_txb.ctypes.data, len(txb),
             txb.ctypes.data, len(coeffs), coeffs.ctypes.data)
-    rc = lib().orc_av1g_obu_arrays(*args, None, 0, C.byref(size), C.byref(nt), toff.ctypes.data, tby.ctypes.data, 4096, err, 256)
+    rc = lib().orc_av1g_obu_arrays(*args, None, 0, C.byref(size), C.byref(nt), toff.ctypes.data, tby.ctypes.data, 4096, C.byref(nsym),
+                                   err, 256)
     if rc != 0:
         raise RuntimeError("av1g_encode rejected the record (%d): %s" % (rc, err.value.decode(errors="replace")))
     obu = np.zeros(size.value, np.uint8)
     rc = lib().orc_av1g_obu_arrays(*args, obu.ctypes.data, size.value, C.byref(size), C.byref(nt), toff.ctypes.data, tby.ctypes.data,
-                                   4096, err, 256)
+                                   4096, None, err, 256)
     if rc != 0:
         raise RuntimeError("av1g_encode rejected the record (%d): %s" % (rc, err.value.decode(errors="replace")))
-    return obu.tobytes(), [(int(toff[i]), int(tby[i])) for i in range(nt.value)]
+    tiles = [(int(toff[i]), int(tby[i])) for i in range(nt.value)]
+    return (obu.tobytes(), tiles, nsym.value) if symbols else (obu.tobytes(), tiles)
 
 
 def fwd2d(res, tx_size, tx_type, bit_depth=8):

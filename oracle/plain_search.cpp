@@ -1681,7 +1681,7 @@ extern "C" int orc_av1g_recon_arrays(int width, int height, int qindex, int bd, 
 extern "C" int orc_av1g_obu_arrays(int width, int height, int qindex, int bd, int chroma_444, uint32_t n_blocks, av1g_block *blocks,
                                    uint32_t *block_txb, uint32_t n_txb, av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs, uint8_t *obu,
                                    uint64_t cap, uint64_t *size, uint32_t *n_tiles, uint64_t *tile_off, uint32_t *tile_bytes, uint32_t tile_cap,
-                                   char *err, size_t errlen) {
+                                   uint64_t *n_symbols, char *err, size_t errlen) {
     av1g_decision_record rec;
     memset(&rec, 0, sizeof rec);
     rec.fp.version = AV1G_DECISIONS_VERSION;
@@ -1706,6 +1706,7 @@ extern "C" int orc_av1g_obu_arrays(int width, int height, int qindex, int bd, in
     int rc = av1g_encode(&rec, &o, &out);
     if (rc != AV1G_OK) { if (err) snprintf(err, errlen, "%s", out.error); av1g_output_free(&out); return rc; }
     *size = out.obu_size;
+    if (n_symbols) *n_symbols = out.n_symbols;
     if (obu && cap >= out.obu_size) memcpy(obu, out.obu, out.obu_size);
     av1g_parsed *ps = nullptr;
     rc = av1g_parse(out.obu, out.obu_size, &ps);

@@ -111,6 +111,25 @@ def test_device_entropy_batch(enc):
     assert enc.obu(3, 2) == streams[3:5]
 
 
+@pytest.mark.gpu
+def test_device_entropy_speed(enc):
+    """The 12 MP bench picture at qindex 120: the device coder's kernel time (CUDA events) against av1core's CPU writer
+    (av1g_encode, bitstream only, one host thread) on the same record; the streams are equal."""
+    import json
+    import time
+    w, h, q = 4000, 3000, 120
+    r = enc.encode(synth.make_image(w, h, 12, edges=True), q)
+    ms = min(enc.obu(timed=True)[1] for _ in range(3))
+    t0 = time.perf_counter()
+    want, tiles, nsym = O.av1g_obu(w, h, q, r.blocks, r.block_txb, r.txb, r.coeffs, symbols=True)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    assert enc.obu()[0] == want
+    print(json.dumps({"image": "%dx%d q%d" % (w, h, q), "tiles": len(tiles), "symbols": nsym, "bytes": len(want),
+                      "device_ms": round(ms, 1), "cpu_av1g_encode_ms": round(cpu_ms, 1),
+                      "ns_per_symbol_per_tile": round(ms * 1e6 / (nsym / len(tiles)), 1)}))
+    assert ms < cpu_ms
+
+
 class _DevBytes:
     """A device byte range as a __cuda_array_interface__ object (torch.as_tensor reads it without a copy)."""
 
