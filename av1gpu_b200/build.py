@@ -38,13 +38,13 @@ def gen_txfm():
 
 
 # compilation units: (source, object, defines).  The analysis unit is compiled once per bit depth and kernel pair, the
-# closed loop once per format, the entropy coder once; the units build in parallel and are linked into one library.
+# closed loop once per format, the entropy coder and the post-filters once; the units build in parallel and are linked into one library.
 UNITS = [("is_api.cu", "is_api.o", []),
          ("is_k_an.cu", "is_k_an8w.o", ["-DIS_BD=8", "-DIS_AN_PART=0"]), ("is_k_an.cu", "is_k_an8t.o", ["-DIS_BD=8", "-DIS_AN_PART=1"]),
          ("is_k_an.cu", "is_k_an10w.o", ["-DIS_BD=10", "-DIS_AN_PART=0"]), ("is_k_an.cu", "is_k_an10t.o", ["-DIS_BD=10", "-DIS_AN_PART=1"]),
          ("is_k_rc.cu", "is_k_rc8_420.o", ["-DIS_BD=8", "-DIS_SS=1"]), ("is_k_rc.cu", "is_k_rc8_444.o", ["-DIS_BD=8", "-DIS_SS=0"]),
          ("is_k_rc.cu", "is_k_rc10_420.o", ["-DIS_BD=10", "-DIS_SS=1"]), ("is_k_rc.cu", "is_k_rc10_444.o", ["-DIS_BD=10", "-DIS_SS=0"]),
-         ("is_k_ent.cu", "is_k_ent.o", [])]
+         ("is_k_ent.cu", "is_k_ent.o", []), ("is_k_pf.cu", "is_k_pf.o", [])]
 BUILD_DIR = os.path.join(HERE, "_build")
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC",
               "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]

@@ -262,6 +262,8 @@ struct is_handle {
     // entropy coding of the records (is_encode_obu): device scratch, pinned result staging, timing events
     void *entScratch = nullptr;
     size_t entBytes = 0;
+    void *pfScratch = nullptr;              // post-filters (is_postfilter)
+    size_t pfBytes = 0;
     cudaEvent_t entEv[2] = {nullptr, nullptr};
     int setErr(int code, const char *fmt, ...) {
         char b[512];
@@ -501,6 +503,7 @@ void is_destroy(is_handle *h) {
     if (h->own) cudaStreamSynchronize(h->own);
     if (h->arena) cudaFree(h->arena);
     if (h->entScratch) cudaFree(h->entScratch);
+    if (h->pfScratch) cudaFree(h->pfScratch);
     for (auto &e : h->entEv)
         if (e) cudaEventDestroy(e);
     for (auto &e : h->ev)
@@ -1196,6 +1199,46 @@ int is_encode_obu(is_handle *h, int first, int n, uint8_t *out, uint64_t cap, ui
     }
     offsets[n] = pos;
     return fits ? IS_OK : h->setErr(IS_ERR_TOO_LARGE, "the OBU streams need %llu bytes", (unsigned long long)pos);
+}
+
+int is_postfilter(is_handle *h, int i, const av1g_frame_params *fp, const int8_t *sb_cdef, float *device_ms) {
+    if (!h || !h->have || i < 0 || i >= h->bN) return h ? h->setErr(IS_ERR_STATE, "no such image") : IS_ERR_STATE;
+    const FrameDesc &F = h->bF[i];
+    if (!fp || fp->width != (uint32_t)F.W || fp->height != (uint32_t)F.H || fp->monochrome || fp->base_q_idx == 0 ||
+        (fp->chroma_format == AV1G_CHROMA_444) != (F.ssx == 0) || (fp->bit_depth == 10) != (F.bd == 10))
+        return h->setErr(IS_ERR_INVALID, "frame parameters do not describe image %d", i);
+    bool ok = fp->loop_filter_sharpness <= 7 && fp->enable_cdef <= 1 && fp->cdef_damping_minus_3 <= 3 && fp->cdef_bits <= 3;
+    for (int k = 0; k < 4; k++) ok = ok && fp->loop_filter_level[k] <= 63;
+    ok = ok && (fp->loop_filter_level[0] || fp->loop_filter_level[1] || (!fp->loop_filter_level[2] && !fp->loop_filter_level[3]));
+    for (int k = 0; k < 8; k++) {
+        auto sec = [](int v) { return v == 0 || v == 1 || v == 2 || v == 4; };
+        ok = ok && fp->cdef_y_pri[k] <= 15 && fp->cdef_uv_pri[k] <= 15 && sec(fp->cdef_y_sec[k]) && sec(fp->cdef_uv_sec[k]);
+    }
+    const size_t nSb = (size_t)F.sbCols * F.sbRows;
+    if (fp->enable_cdef && sb_cdef)
+        for (size_t k = 0; k < nSb; k++) ok = ok && sb_cdef[k] >= 0 && sb_cdef[k] < (1 << fp->cdef_bits);
+    if (!ok) return h->setErr(IS_ERR_INVALID, "post-filter parameters out of range");
+    IS_CK(cudaSetDevice(h->device));
+    const size_t need = pf_scratch_bytes(F.W, F.H, F.bd, F.ssx ? 0 : 1);
+    if (need > h->pfBytes) {
+        if (h->pfScratch) IS_CK(cudaFree(h->pfScratch));
+        h->pfScratch = nullptr;
+        h->pfBytes = 0;
+        IS_CK(cudaMalloc(&h->pfScratch, need));
+        h->pfBytes = need;
+    }
+    for (auto &e : h->entEv)
+        if (!e) IS_CK(cudaEventCreate(&e));
+    std::vector<int8_t> zero;
+    if (fp->enable_cdef && !sb_cdef) { zero.assign(nSb, 0); sb_cdef = zero.data(); }
+    IS_CK(cudaEventRecord(h->entEv[0], h->own));
+    const int rc = pf_launch(*fp, h->bF[i].recBlocks, h->bNb[i], fp->enable_cdef ? sb_cdef : nullptr, F.rec, F.rpitch, h->pfScratch,
+                             h->pfBytes, h->own, &h->err);
+    if (rc != IS_OK) return rc;
+    IS_CK(cudaEventRecord(h->entEv[1], h->own));
+    IS_CK(cudaStreamSynchronize(h->own));
+    if (device_ms) IS_CK(cudaEventElapsedTime(device_ms, h->entEv[0], h->entEv[1]));
+    return IS_OK;
 }
 
 int is_times_get(const is_handle *h, is_times *t) {

@@ -2,7 +2,7 @@
 //
 // The kernels are compiled in separate units so that they build in parallel: is_k_an.cu once per bit depth and kernel
 // pair (the four analysis kernels), is_k_rc.cu once per format (the closed loop), is_k_ent.cu (entropy coding of the
-// records), is_api.cu (host API, DP, scheduling, pack, learned-shortlist and test kernels).  Device globals have internal linkage (static): every unit holds its own copy
+// records), is_k_pf.cu (post-filters), is_api.cu (host API, DP, scheduling, pack, learned-shortlist and test kernels).  Device globals have internal linkage (static): every unit holds its own copy
 // of the search's tables, and upload_tables() in is_api.cu fills each unit's copy from one host-built TableBlob.
 #pragma once
 #include <cuda_runtime.h>
@@ -70,5 +70,10 @@ int ent_launch(const is_ent_frame *frames, int n, uint64_t cap, void *scratch, s
                uint32_t *frameTile0, std::string *err);
 int obu_assemble(const av1g_frame_params &fp, const uint8_t *payload, const uint64_t *off, uint32_t nTiles, std::vector<uint8_t> &o,
                  std::string *err);
+
+// ---- post-filter unit (is_k_pf.cu): deblocking + CDEF of a reconstruction on the device ----
+size_t pf_scratch_bytes(int W, int H, int bd, int c444);
+int pf_launch(const av1g_frame_params &fp, av1g_block *blocks, uint32_t nBlocks, const int8_t *sbCdefHost, uint8_t *const rec[3],
+              const int rpitch[3], void *scratch, size_t scratchBytes, cudaStream_t s, std::string *err);
 
 }  // namespace is

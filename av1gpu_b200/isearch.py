@@ -65,7 +65,7 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_set_shortlist_model",
            "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison", "is_set_search_options", "is_set_closed_loop_warps", "is_serve_open", "is_serve_start", "is_serve_submit", "is_serve_poll",
            "is_serve_counts", "is_serve_copy", "is_serve_stop", "is_serve_close", "is_entropy_scratch_bytes", "is_entropy_batch",
-           "is_obu_assemble", "is_encode_obu"]
+           "is_obu_assemble", "is_encode_obu", "is_postfilter"]
 
 _lib = None
 
@@ -137,6 +137,7 @@ def load_library():
     L.is_entropy_batch.argtypes = [C.c_int, vp, C.c_int, C.c_uint64, vp, C.c_uint64, vp, vp, vp]
     L.is_obu_assemble.argtypes = [vp, vp, vp, C.c_uint32, vp, C.c_uint64, C.POINTER(C.c_uint64)]
     L.is_encode_obu.argtypes = [vp, C.c_int, C.c_int, vp, C.c_uint64, vp, C.POINTER(C.c_float)]
+    L.is_postfilter.argtypes = [vp, C.c_int, vp, vp, C.POINTER(C.c_float)]
     _lib = L
     return L
 
@@ -383,6 +384,15 @@ class Encoder:
         self._check(rc, "is_encode_obu")
         out = [buf[int(offs[k]):int(offs[k + 1])].tobytes() for k in range(n)]
         return (out, ms.value) if timed else out
+
+    def postfilter(self, fp, sb_cdef=None, i=0):
+        """Deblocking + CDEF in place on image i's reconstruction (fp: av1g_frame_params bytes with the filter fields,
+        sb_cdef: int8 cdef_idx per 64x64 or None); the device time (ms)."""
+        fp = np.ascontiguousarray(fp, np.uint8)
+        sb = None if sb_cdef is None else np.ascontiguousarray(sb_cdef, np.int8)
+        ms = C.c_float()
+        self._check(self.L.is_postfilter(self.h, i, fp.ctypes.data, None if sb is None else sb.ctypes.data, C.byref(ms)), "is_postfilter")
+        return ms.value
 
     def set_wait_limits(self, leaf_wait_iters=0, ready_wait_ns=0):
         """Closed-loop wait budgets (0: the defaults); a wait that runs out makes the encode raise IsError(-4)."""

@@ -225,6 +225,17 @@ int is_obu_assemble(const av1g_frame_params *fp, const uint8_t *payload, const u
  * needed). */
 int is_encode_obu(is_handle *h, int first, int n, uint8_t *out, uint64_t cap, uint64_t *offsets, float *device_ms);
 
+/* ---- post-filters on the device ----
+ * Deblocking (spec 7.14) then CDEF (spec 7.15), as the decoder applies them, in place on image i's reconstruction of the
+ * handle's last encode (is_batch_copy / is_record_copy then return the filtered planes); replaces av1core's
+ * av1g_postfilter / av1g_postfilter16 (av1core/include/av1g/av1g.h:95-104, encoder.cpp:1998-2041) and its GPU
+ * counterpart (av1core/src/gpu_postfilter.cu).  fp: the frame's parameters with the filter fields set (effective
+ * loop_filter_level[4], loop_filter_sharpness, enable_cdef, cdef_damping_minus_3, cdef_bits and the strengths); its size and
+ * format must be the image's.  sb_cdef: the cdef_idx of every 64x64 (raster, (MiCols + 15) / 16 per row; NULL = 0), written
+ * into the record's blocks so that av1g_encode() of the record with fp reconstructs the filtered planes.  device_ms (may be
+ * NULL): device time of the filters.  Not undone by anything but a new encode. */
+int is_postfilter(is_handle *h, int i, const av1g_frame_params *fp, const int8_t *sb_cdef, float *device_ms);
+
 /* ---- kernel-level entry points for the parity tests (device primitives of av1core's dsp.h API) ---- */
 /* Forward 2-D transform (this project's integer transform) + quantisation + rate of n residual blocks of one tx
  * size / type, host arrays: res [n][H*W] int32 -> coef [n][tw*th] (fixed point), levels [n][tw*th], D, R, eob per block.

@@ -90,6 +90,13 @@ int orc_av1g_obu_arrays(int width, int height, int qindex, int bd, int chroma_44
                         uint64_t cap, uint64_t *size, uint32_t *n_tiles, uint64_t *tile_off, uint32_t *tile_bytes, uint32_t tile_cap,
                         uint64_t *n_symbols, char *err, size_t errlen);
 
+/* av1g_encode() of a record with the given frame parameters and flags (AV1G_ENC_*); recon planes as av1g_output describes
+ * them (cropped, or the unfiltered coded area with AV1G_ENC_PREFILTER_RECON). */
+int orc_av1g_encode_fp(const av1g_frame_params *fp, uint32_t flags, uint32_t n_blocks, av1g_block *blocks, uint32_t *block_txb,
+                       uint32_t n_txb, av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs, void *recon[3], char *err, size_t errlen);
+/* av1core's post-filters in place on planes of at least the coded area (strides in samples). */
+int orc_av1g_postfilter(const av1g_frame_params *fp, uint32_t n_blocks, av1g_block *blocks, void *planes[3], const int stride[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,6 +47,9 @@ def lib():
                                                           C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
                                                           C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_uint32,
                                                           C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]
+        L.orc_av1g_encode_fp.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                         C.c_uint64, C.c_void_p, C.c_void_p * 3, C.c_char_p, C.c_size_t]
+        L.orc_av1g_postfilter.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p * 3, C.c_int * 3]
         L.orc_fwd2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.orc_inv2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.orc_inv2d.restype = C.c_uint32
@@ -181,6 +184,43 @@ def av1g_obu(width, height, qindex, blocks, block_txb, txb, coeffs, bit_depth=8,
         raise RuntimeError("av1g_encode rejected the record (%d): %s" % (rc, err.value.decode(errors="replace")))
     tiles = [(int(toff[i]), int(tby[i])) for i in range(nt.value)]
     return (obu.tobytes(), tiles, nsym.value) if symbols else (obu.tobytes(), tiles)
+
+
+AV1G_ENC_PREFILTER_RECON = 0x20
+
+
+def av1g_encode_fp(fp, blocks, block_txb, txb, coeffs, prefilter=False):
+    """av1g_encode() of a record with frame parameters fp (av1g_frame_params bytes): the reconstruction planes, cropped
+    and post-filtered, or (prefilter) the unfiltered coded area (MiCols * 4 x MiRows * 4, chroma subsampled)."""
+    fp = np.ascontiguousarray(fp, np.uint8)
+    w, h = (int(v) for v in fp[4:12].view(np.uint32))
+    c444, bd = int(fp[72]) == 1, 10 if int(fp[73]) == 10 else 8
+    if prefilter:
+        w, h = 8 * ((w + 7) // 8), 8 * ((h + 7) // 8)
+    cw, ch = (w, h) if c444 else ((w + 1) // 2, (h + 1) // 2)
+    dt = np.uint16 if bd == 10 else np.uint8
+    outs = [np.zeros((h, w), dt), np.zeros((ch, cw), dt), np.zeros((ch, cw), dt)]
+    err = C.create_string_buffer(256)
+    blocks = np.ascontiguousarray(blocks)
+    txb = np.ascontiguousarray(txb).copy()
+    coeffs = np.ascontiguousarray(coeffs, np.int16).copy()
+    block_txb = np.ascontiguousarray(block_txb, np.uint32)
+    rc = lib().orc_av1g_encode_fp(fp.ctypes.data, AV1G_ENC_PREFILTER_RECON if prefilter else 0, len(blocks), blocks.ctypes.data,
+                                  block_txb.ctypes.data, len(txb), txb.ctypes.data, len(coeffs), coeffs.ctypes.data,
+                                  (C.c_void_p * 3)(*[o.ctypes.data for o in outs]), err, 256)
+    if rc != 0:
+        raise RuntimeError("av1g_encode rejected the record (%d): %s" % (rc, err.value.decode(errors="replace")))
+    return outs
+
+
+def av1g_postfilter(fp, blocks, planes):
+    """av1core's deblocking + CDEF in place on planes (numpy, at least the coded area) for the record's blocks."""
+    fp = np.ascontiguousarray(fp, np.uint8)
+    blocks = np.ascontiguousarray(blocks)
+    rc = lib().orc_av1g_postfilter(fp.ctypes.data, len(blocks), blocks.ctypes.data, (C.c_void_p * 3)(*[p.ctypes.data for p in planes]),
+                                   (C.c_int * 3)(*[p.strides[0] // p.itemsize for p in planes]))
+    if rc != 0:
+        raise RuntimeError("av1g_postfilter failed (%d)" % rc)
 
 
 def fwd2d(res, tx_size, tx_type, bit_depth=8):

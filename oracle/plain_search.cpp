@@ -1718,6 +1718,43 @@ extern "C" int orc_av1g_obu_arrays(int width, int height, int qindex, int bd, in
     return 0;
 }
 
+// av1g_encode() of a record with the given frame parameters (e.g. post-filter fields) and flags; its reconstruction
+// planes copied out (cropped, or with AV1G_ENC_PREFILTER_RECON the unfiltered coded area)
+extern "C" int orc_av1g_encode_fp(const av1g_frame_params *fp, uint32_t flags, uint32_t n_blocks, av1g_block *blocks, uint32_t *block_txb,
+                                  uint32_t n_txb, av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs, void *recon[3], char *err, size_t errlen) {
+    av1g_decision_record rec;
+    memset(&rec, 0, sizeof rec);
+    rec.fp = *fp;
+    rec.n_blocks = n_blocks;
+    rec.blocks = blocks;
+    rec.block_txb = block_txb;
+    rec.n_txb = n_txb;
+    rec.txb = txb;
+    rec.n_coeffs = n_coeffs;
+    rec.coeffs = coeffs;
+    av1g_encode_opts o = {flags, -1};
+    av1g_output out;
+    memset(&out, 0, sizeof out);
+    const int rc = av1g_encode(&rec, &o, &out);
+    if (rc != AV1G_OK) { if (err) snprintf(err, errlen, "%s", out.error); av1g_output_free(&out); return rc; }
+    for (int p = 0; p < 3; p++)
+        if (recon[p] && out.recon[p])
+            memcpy(recon[p], out.recon[p], (size_t)out.recon_w[p] * out.recon_h[p] * (fp->bit_depth == 10 ? 2 : 1));
+    av1g_output_free(&out);
+    return 0;
+}
+
+// av1core's post-filters (av1g_postfilter / av1g_postfilter16) in place on the planes, for the record's blocks and fp
+extern "C" int orc_av1g_postfilter(const av1g_frame_params *fp, uint32_t n_blocks, av1g_block *blocks, void *planes[3], const int stride[3]) {
+    av1g_decision_record rec;
+    memset(&rec, 0, sizeof rec);
+    rec.fp = *fp;
+    rec.n_blocks = n_blocks;
+    rec.blocks = blocks;
+    if (fp->bit_depth == 10) return av1g_postfilter16(&rec, (uint16_t *const *)planes, stride);
+    return av1g_postfilter(&rec, (uint8_t *const *)planes, stride);
+}
+
 extern "C" void orc_qstep(int qindex, int bd, int *dcq, int *acq) {
     *dcq = av1g_dc_q_bd(qindex, bd);
     *acq = av1g_ac_q_bd(qindex, bd);
