@@ -90,6 +90,11 @@ int orc_av1g_obu_arrays(int width, int height, int qindex, int bd, int chroma_44
                         uint64_t cap, uint64_t *size, uint32_t *n_tiles, uint64_t *tile_off, uint32_t *tile_bytes, uint32_t tile_cap,
                         uint64_t *n_symbols, char *err, size_t errlen);
 
+/* orc_av1g_obu_arrays with the record's frame parameters given. */
+int orc_av1g_obu_fp(const av1g_frame_params *fp, uint32_t n_blocks, av1g_block *blocks, uint32_t *block_txb, uint32_t n_txb,
+                    av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs, uint8_t *obu, uint64_t cap, uint64_t *size,
+                    uint32_t *n_tiles, uint64_t *tile_off, uint32_t *tile_bytes, uint32_t tile_cap, uint64_t *n_symbols,
+                    char *err, size_t errlen);
 /* av1g_encode() of a record with the given frame parameters and flags (AV1G_ENC_*); recon planes as av1g_output describes
  * them (cropped, or the unfiltered coded area with AV1G_ENC_PREFILTER_RECON). */
 int orc_av1g_encode_fp(const av1g_frame_params *fp, uint32_t flags, uint32_t n_blocks, av1g_block *blocks, uint32_t *block_txb,

@@ -47,6 +47,9 @@ def lib():
                                                           C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
                                                           C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_uint32,
                                                           C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]
+        L.orc_av1g_obu_fp.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p,
+                                      C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p,
+                                      C.c_uint32, C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]
         L.orc_av1g_encode_fp.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                          C.c_uint64, C.c_void_p, C.c_void_p * 3, C.c_char_p, C.c_size_t]
         L.orc_av1g_postfilter.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p * 3, C.c_int * 3]
@@ -187,6 +190,27 @@ def av1g_obu(width, height, qindex, blocks, block_txb, txb, coeffs, bit_depth=8,
 
 
 AV1G_ENC_PREFILTER_RECON = 0x20
+
+
+def av1g_obu_fp(fp, blocks, block_txb, txb, coeffs):
+    """av1g_encode()'s OBU stream of a record with frame parameters fp (av1g_frame_params bytes) and its tile payloads'
+    (offset, size)."""
+    fp = np.ascontiguousarray(fp, np.uint8)
+    blocks = np.ascontiguousarray(blocks)
+    block_txb = np.ascontiguousarray(block_txb, np.uint32)
+    txb = np.ascontiguousarray(txb).copy()
+    coeffs = np.ascontiguousarray(coeffs, np.int16).copy()
+    err = C.create_string_buffer(256)
+    size, nt = C.c_uint64(), C.c_uint32()
+    toff, tby = np.zeros(4096, np.uint64), np.zeros(4096, np.uint32)
+    args = (fp.ctypes.data, len(blocks), blocks.ctypes.data, block_txb.ctypes.data, len(txb), txb.ctypes.data, len(coeffs), coeffs.ctypes.data)
+    for obu in (None, True):
+        buf = np.zeros(size.value, np.uint8) if obu else None
+        rc = lib().orc_av1g_obu_fp(*args, None if buf is None else buf.ctypes.data, size.value if obu else 0, C.byref(size), C.byref(nt),
+                                   toff.ctypes.data, tby.ctypes.data, 4096, None, err, 256)
+        if rc != 0:
+            raise RuntimeError("av1g_encode rejected the record (%d): %s" % (rc, err.value.decode(errors="replace")))
+    return buf.tobytes(), [(int(toff[i]), int(tby[i])) for i in range(nt.value)]
 
 
 def av1g_encode_fp(fp, blocks, block_txb, txb, coeffs, prefilter=False):

@@ -1677,22 +1677,40 @@ extern "C" int orc_av1g_recon_arrays(int width, int height, int qindex, int bd, 
     return orc_av1g_recon(&rec, recon, err, errlen, obu_bytes);
 }
 
+extern "C" int orc_av1g_obu_fp(const av1g_frame_params *fp, uint32_t n_blocks, av1g_block *blocks, uint32_t *block_txb, uint32_t n_txb,
+                               av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs, uint8_t *obu, uint64_t cap, uint64_t *size,
+                               uint32_t *n_tiles, uint64_t *tile_off, uint32_t *tile_bytes, uint32_t tile_cap, uint64_t *n_symbols,
+                               char *err, size_t errlen);
+
 // av1g_encode()'s OBU stream of a record (the bitstream only) and, from av1g_parse() of it, where each tile payload lies
 extern "C" int orc_av1g_obu_arrays(int width, int height, int qindex, int bd, int chroma_444, uint32_t n_blocks, av1g_block *blocks,
                                    uint32_t *block_txb, uint32_t n_txb, av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs, uint8_t *obu,
                                    uint64_t cap, uint64_t *size, uint32_t *n_tiles, uint64_t *tile_off, uint32_t *tile_bytes, uint32_t tile_cap,
                                    uint64_t *n_symbols, char *err, size_t errlen) {
+    av1g_frame_params fp;
+    memset(&fp, 0, sizeof fp);
+    fp.version = AV1G_DECISIONS_VERSION;
+    fp.width = (uint32_t)width;
+    fp.height = (uint32_t)height;
+    fp.base_q_idx = (uint8_t)qindex;
+    fp.tile_cols_log2 = -1;
+    fp.tile_rows_log2 = -1;
+    fp.qm_y = fp.qm_u = fp.qm_v = 15;
+    fp.chroma_format = chroma_444 ? AV1G_CHROMA_444 : AV1G_CHROMA_420;
+    fp.bit_depth = (uint8_t)bd;
+    return orc_av1g_obu_fp(&fp, n_blocks, blocks, block_txb, n_txb, txb, n_coeffs, coeffs, obu, cap, size, n_tiles, tile_off, tile_bytes,
+                           tile_cap, n_symbols, err, errlen);
+}
+
+// the same with the record's frame parameters given (header fields: delta_q, quantizer matrices, loop-filter levels,
+// colour description, ...)
+extern "C" int orc_av1g_obu_fp(const av1g_frame_params *fp, uint32_t n_blocks, av1g_block *blocks, uint32_t *block_txb, uint32_t n_txb,
+                               av1g_txb *txb, uint64_t n_coeffs, int16_t *coeffs, uint8_t *obu, uint64_t cap, uint64_t *size,
+                               uint32_t *n_tiles, uint64_t *tile_off, uint32_t *tile_bytes, uint32_t tile_cap, uint64_t *n_symbols,
+                               char *err, size_t errlen) {
     av1g_decision_record rec;
     memset(&rec, 0, sizeof rec);
-    rec.fp.version = AV1G_DECISIONS_VERSION;
-    rec.fp.width = (uint32_t)width;
-    rec.fp.height = (uint32_t)height;
-    rec.fp.base_q_idx = (uint8_t)qindex;
-    rec.fp.tile_cols_log2 = -1;
-    rec.fp.tile_rows_log2 = -1;
-    rec.fp.qm_y = rec.fp.qm_u = rec.fp.qm_v = 15;
-    rec.fp.chroma_format = chroma_444 ? AV1G_CHROMA_444 : AV1G_CHROMA_420;
-    rec.fp.bit_depth = (uint8_t)bd;
+    rec.fp = *fp;
     rec.n_blocks = n_blocks;
     rec.blocks = blocks;
     rec.block_txb = block_txb;

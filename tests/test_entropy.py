@@ -32,6 +32,45 @@ def test_obu_framing_matches_av1core(w, h, q, bd, c444, seed):
     assert got == obu
 
 
+# av1g_frame_params offsets of the header-only fields (av1core/include/av1g/decisions.h:254-296)
+FP_DQ, FP_EDGE, FP_QM_ON, FP_QM, FP_LF, FP_SHARP, FP_CD, FP_CP, FP_TC, FP_MC = 18, 24, 27, 28, 31, 35, 74, 75, 76, 77
+
+
+@pytest.mark.parametrize("case", range(8))
+def test_obu_framing_header_fields(case):
+    """Frame parameters that change only the headers (plane delta_q values with and without separate U / V, quantizer
+    matrices, loop-filter levels and sharpness, the intra edge filter flag, colour descriptions incl. the implied-range
+    and unspecified forms, 10-bit 4:4:4): the framing still equals av1g_encode()'s stream."""
+    rng = np.random.default_rng(100 + case)
+    bd, c444 = (10, True) if case in (3, 6) else (8, False)
+    w, h, q = 72, 40, 100
+    im = synth.make_image(w, h, 900 + case, edges=True, bit_depth=bd, chroma_444=c444)
+    r = O.encode(im, q, bit_depth=bd, chroma_444=c444, threads=2)
+    fp = frame_params(w, h, q, bd, c444)
+    dq = rng.integers(-20, 21, 5).astype(np.int8)
+    if case % 2:
+        dq[3:] = dq[1:3]                    # V equal to U: no separate_uv_delta_q
+    fp[FP_DQ:FP_DQ + 5] = dq.view(np.uint8)
+    if case in (2, 5, 6):
+        fp[FP_QM_ON] = 1
+        fp[FP_QM:FP_QM + 3] = rng.integers(0, 16, 3)
+    lv = rng.integers(0, 64, 4)
+    if case == 4:
+        lv[:] = 0
+    fp[FP_LF:FP_LF + 4] = lv
+    fp[FP_SHARP] = rng.integers(0, 8)
+    fp[FP_EDGE] = case % 2
+    cicp = [(1, 13, 6), (1, 13, 0), (2, 2, 2), (9, 16, 9)][case % 4]
+    if case >= 4:
+        fp[FP_CD] = 1
+        fp[FP_CP:FP_CP + 3] = cicp
+        if cicp[2] == 0 and not c444:
+            fp[FP_CP:FP_CP + 3] = (1, 13, 6)   # identity matrix needs 4:4:4
+    want, tiles = O.av1g_obu_fp(fp, r.blocks, r.block_txb, r.txb, r.coeffs)
+    pay, off = _payloads(want, tiles)
+    assert obu_assemble(fp, pay, off) == want
+
+
 def test_obu_assemble_refusals():
     """Frames outside the coder's toolset, a tile count that does not match the tiling, and a short buffer."""
     L = load_library()
