@@ -264,6 +264,8 @@ struct is_handle {
     size_t entBytes = 0;
     void *pfScratch = nullptr;              // post-filters (is_postfilter)
     size_t pfBytes = 0;
+    std::vector<av1g_frame_params> bPf;     // per image: the frame parameters of its post-filters (is_encode_obu codes them)
+    std::vector<char> bPfSet;
     cudaEvent_t entEv[2] = {nullptr, nullptr};
     int setErr(int code, const char *fmt, ...) {
         char b[512];
@@ -640,6 +642,8 @@ static int prepare_batch(is_handle *h, const is_frame *fr, int n) {
         }
     }
     h->bF.assign(n, FrameDesc());
+    h->bPf.assign(n, av1g_frame_params());
+    h->bPfSet.assign(n, 0);
     h->bNsb = nsb;
     h->bQ.assign(n, 0);
     h->bNb.assign(n, 0);
@@ -1047,22 +1051,15 @@ int is_batch_counts(const is_handle *h, int i, uint32_t *nb, uint32_t *nt, uint6
     return IS_OK;
 }
 
+static void batch_fp(const is_handle *h, int i, av1g_frame_params *fp);
+
 int is_batch_copy(is_handle *h, int i, av1g_frame_params *fp, av1g_block *blocks, uint32_t *block_txb, av1g_txb *txb, int16_t *coeffs,
                   void *recon[3], const int32_t recon_pitch[3]) {
     if (!h || !h->have || i < 0 || i >= h->bN) return IS_ERR_STATE;
     IS_CK(cudaSetDevice(h->device));
     const FrameDesc &F = h->bF[i];
     cudaStream_t st = h->own;
-    if (fp) {
-        memset(fp, 0, sizeof *fp);
-        fp->version = AV1G_DECISIONS_VERSION;
-        fp->width = (uint32_t)F.W; fp->height = (uint32_t)F.H;
-        fp->base_q_idx = (uint8_t)h->bQ[i];
-        fp->tile_cols_log2 = -1; fp->tile_rows_log2 = -1;
-        fp->qm_y = fp->qm_u = fp->qm_v = 15;
-        fp->chroma_format = F.ssx ? AV1G_CHROMA_420 : AV1G_CHROMA_444;
-        fp->bit_depth = (uint8_t)F.bd;
-    }
+    if (fp) batch_fp(h, i, fp);
     if (blocks) IS_CK(cudaMemcpyAsync(blocks, F.recBlocks, (size_t)h->bNb[i] * sizeof(av1g_block), cudaMemcpyDeviceToHost, st));
     if (block_txb) IS_CK(cudaMemcpyAsync(block_txb, F.recBlockTxb, ((size_t)h->bNb[i] + 1) * 4, cudaMemcpyDeviceToHost, st));
     if (txb) IS_CK(cudaMemcpyAsync(txb, F.recTxb, (size_t)h->bNt[i] * sizeof(av1g_txb), cudaMemcpyDeviceToHost, st));
@@ -1095,9 +1092,10 @@ int is_record_device(const is_handle *h, const av1g_block **blocks, const uint32
     return IS_OK;
 }
 
-// the frame parameters of image i of the last batch (as is_batch_copy writes them)
+// the frame parameters of image i of the last batch (as is_batch_copy writes them; after is_postfilter, its parameters)
 static void batch_fp(const is_handle *h, int i, av1g_frame_params *fp) {
     const FrameDesc &F = h->bF[i];
+    if (i < (int)h->bPfSet.size() && h->bPfSet[i]) { *fp = h->bPf[i]; return; }
     memset(fp, 0, sizeof *fp);
     fp->version = AV1G_DECISIONS_VERSION;
     fp->width = (uint32_t)F.W; fp->height = (uint32_t)F.H;
@@ -1238,6 +1236,18 @@ int is_postfilter(is_handle *h, int i, const av1g_frame_params *fp, const int8_t
     IS_CK(cudaEventRecord(h->entEv[1], h->own));
     IS_CK(cudaStreamSynchronize(h->own));
     if (device_ms) IS_CK(cudaEventElapsedTime(device_ms, h->entEv[0], h->entEv[1]));
+    // the record now carries the filters: the bitstream is_encode_obu writes signals them
+    av1g_frame_params q;
+    batch_fp(h, i, &q);
+    memcpy(q.loop_filter_level, fp->loop_filter_level, sizeof q.loop_filter_level);
+    q.loop_filter_sharpness = fp->loop_filter_sharpness;
+    q.enable_cdef = fp->enable_cdef;
+    q.cdef_damping_minus_3 = fp->cdef_damping_minus_3;
+    q.cdef_bits = fp->cdef_bits;
+    memcpy(q.cdef_y_pri, fp->cdef_y_pri, 8); memcpy(q.cdef_y_sec, fp->cdef_y_sec, 8);
+    memcpy(q.cdef_uv_pri, fp->cdef_uv_pri, 8); memcpy(q.cdef_uv_sec, fp->cdef_uv_sec, 8);
+    h->bPf[i] = q;
+    h->bPfSet[i] = 1;
     return IS_OK;
 }
 

@@ -35,7 +35,7 @@ static __constant__ uint8_t c_miWLog2[22], c_miHLog2[22];
 static __device__ uint16_t g_cdfInit[4][NCDF];   // av1g_cdfs of each coefficient q-context at the start of a tile
 
 constexpr uint32_t NONE32 = 0xFFFFFFFFu;
-constexpr int HEAD_WORDS = 12;   // partition symbols (at most 4: 64, 32, 16, 8) + mode info (at most 8) of a block
+constexpr int HEAD_WORDS = 16;   // partition symbols (at most 4: 64, 32, 16, 8) + mode info (at most 11) of a block
 enum { SYM_ADAPT = 0, SYM_BIT = 1, SYM_SPLIT_H = 2, SYM_SPLIT_V = 3 };
 
 __device__ __forceinline__ uint32_t sym_word(int kind, int cdf, int s, int N) {
@@ -48,6 +48,7 @@ struct EntFrameD {
     const av1g_txb *txb;
     const int16_t *coeffs;
     int MiCols, MiRows, ss, qctx;
+    int cdefBits;                 // enable_cdef: the bits of a SB's cdef_idx; -1 without CDEF
     int sbCols, sbRows, tileWSb, tileHSb, tileCols, tileRows;
     uint32_t blockBase, nBlocks, txbBase, nTxb, sbBase, tileBase;
     uint64_t miBase, ctxBase[3];
@@ -175,6 +176,7 @@ struct Walk {
     int rowStart, colStart;     // the tile's first row / column (mi)
     uint32_t cur, end;          // next block (global), end of the frame's blocks
     int k;                      // words in the current block's slot
+    int cdef;                   // the SB's cdef_idx once coded (-1: not yet)
     bool bad;
 };
 
@@ -214,6 +216,13 @@ __device__ void walk_block(Walk &W, int r, int c, int bs) {
     }
     const int sctx = (aU ? mi_at(A.skip, F, r - 1, c) : 0) + (aL ? mi_at(A.skip, F, r, c - 1) : 0);
     put_word(W, sym_word(SYM_ADAPT, IS_CB(skip) + sctx * IS_CD(skip, 1), B.skip, 2));
+    if (F.cdefBits >= 0 && !B.skip) {   // read_cdef: the SB's cdef_idx with its first coded block, a literal
+        if (B.cdef_idx < 0 || B.cdef_idx >= (1 << F.cdefBits) || (W.cdef >= 0 && B.cdef_idx != W.cdef)) { W.bad = true; return; }
+        if (W.cdef < 0) {
+            for (int i = F.cdefBits - 1; i >= 0; i--) put_word(W, sym_word(SYM_BIT, 0, (B.cdef_idx >> i) & 1, 2));
+            W.cdef = B.cdef_idx;
+        }
+    }
     const int am = ST(Intra_Mode_Context)[aU ? mi_at(A.yMode, F, r - 1, c) : AV1G_DC_PRED];
     const int lm = ST(Intra_Mode_Context)[aL ? mi_at(A.yMode, F, r, c - 1) : AV1G_DC_PRED];
     put_word(W, sym_word(SYM_ADAPT, ci_y_mode(am, lm), B.y_mode, 13));
@@ -343,6 +352,7 @@ __global__ void k_ent_sb(EntArgs A) {
     W.cur = A.sbFirst[g];
     W.end = F.blockBase + F.nBlocks;
     W.k = 0;
+    W.cdef = -1;
     W.bad = W.cur == NONE32;
     if (!W.bad) walk_node(W, sr * 16, sc * 16, AV1G_BLOCK_64X64);
     // the walk must end where the next SB of the decode order starts
@@ -873,8 +883,9 @@ bool tile_info(int W, int H, int colsLog2, int rowsLog2, TileGeom &t) {
 
 namespace {
 
-// the frame parameters this coder handles: the toolset of the search's records (no delta-q, CDEF, palette, filter
-// intra, tx-size or reduced-set syntax; lossy; 4:2:0 or 4:4:4; 8- or 10-bit); header-only fields are free
+// the frame parameters this coder handles: the toolset of the search's records (no delta-q, palette, filter intra,
+// tx-size or reduced-set syntax; lossy; 4:2:0 or 4:4:4; 8- or 10-bit) with CDEF (its per-SB cdef_idx); header-only
+// fields are free
 bool frame_ok(const av1g_frame_params &fp, std::string *err) {
     const char *why = nullptr;
     if (fp.width < 1 || fp.height < 1 || fp.width > 65536 || fp.height > 65536) why = "size";
@@ -882,9 +893,9 @@ bool frame_ok(const av1g_frame_params &fp, std::string *err) {
     else if (fp.base_q_idx == 0) why = "lossless (base_q_idx 0)";
     else if (fp.bit_depth != 0 && fp.bit_depth != 8 && fp.bit_depth != 10) why = "bit_depth";
     else if (fp.chroma_format > 1) why = "chroma_format";
-    else if (fp.tx_mode_select || fp.reduced_tx_set || fp.delta_q_present || fp.enable_cdef || fp.enable_filter_intra ||
-             fp.allow_screen_content_tools)
-        why = "a coding tool outside the search's toolset (tx_mode_select, reduced_tx_set, delta_q, CDEF, filter intra, palette)";
+    else if (fp.tx_mode_select || fp.reduced_tx_set || fp.delta_q_present || fp.enable_filter_intra || fp.allow_screen_content_tools)
+        why = "a coding tool outside the search's toolset (tx_mode_select, reduced_tx_set, delta_q, filter intra, palette)";
+    else if (fp.enable_cdef > 1 || fp.cdef_bits > 3 || fp.cdef_damping_minus_3 > 3) why = "CDEF parameters";
     if (why && err) *err = std::string("frame parameters: ") + why;
     return !why;
 }
@@ -924,6 +935,7 @@ int plan(const is_ent_frame *frames, int n, uint64_t cap, Plan &P, std::string *
         D.MiCols = 2 * (((int)f.fp.width + 7) >> 3);
         D.MiRows = 2 * (((int)f.fp.height + 7) >> 3);
         D.ss = f.fp.chroma_format == AV1G_CHROMA_444 ? 0 : 1;
+        D.cdefBits = f.fp.enable_cdef ? f.fp.cdef_bits : -1;
         const int q = f.fp.base_q_idx;
         D.qctx = q <= 20 ? 0 : q <= 60 ? 1 : q <= 120 ? 2 : 3;
         D.sbCols = (D.MiCols + 15) >> 4; D.sbRows = (D.MiRows + 15) >> 4;
@@ -948,7 +960,7 @@ int plan(const is_ent_frame *frames, int n, uint64_t cap, Plan &P, std::string *
         P.nTiles += (uint32_t)(t.cols * t.rows);
         P.nMi += (uint64_t)D.MiCols * D.MiRows;
         const uint64_t px = (uint64_t)D.MiCols * D.MiRows * 16;
-        defCap += px * (D.ss ? 3 : 6) / 4 + 16ull * f.n_blocks + 8ull * f.n_txb;
+        defCap += px * (D.ss ? 2 : 4) + 16ull * f.n_blocks + 8ull * f.n_txb;
     }
     P.fBlock.push_back(P.nB); P.fTxb.push_back(P.nT); P.fSb.push_back(P.nSb); P.fTile.push_back(P.nTiles);
     P.cap = cap ? cap : defCap;
@@ -1191,6 +1203,14 @@ int obu_assemble(const av1g_frame_params &fp, const uint8_t *payload, const uint
     if (fp.loop_filter_level[0] || fp.loop_filter_level[1]) { fh.put(fp.loop_filter_level[2], 6); fh.put(fp.loop_filter_level[3], 6); }
     fh.put(fp.loop_filter_sharpness, 3);
     fh.put(0, 1);                                     // loop_filter_delta_enabled
+    if (fp.enable_cdef) {                             // cdef_params (secondary strength 4 is coded as 3)
+        fh.put(fp.cdef_damping_minus_3, 2);
+        fh.put(fp.cdef_bits, 2);
+        for (int i = 0; i < (1 << fp.cdef_bits); i++) {
+            fh.put(fp.cdef_y_pri[i], 4); fh.put(fp.cdef_y_sec[i] == 4 ? 3 : fp.cdef_y_sec[i], 2);
+            fh.put(fp.cdef_uv_pri[i], 4); fh.put(fp.cdef_uv_sec[i] == 4 ? 3 : fp.cdef_uv_sec[i], 2);
+        }
+    }
     fh.put(0, 1);                                     // tx_mode_select
     fh.put(0, 1);                                     // reduced_tx_set
     fh.align();

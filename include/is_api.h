@@ -179,8 +179,9 @@ int is_serve_close(is_handle *h);
  * (av1core/include/av1g/gpu_entropy.h:73-147) and the OBU assembly after it (Encoder::write_headers,
  * av1core/src/encoder.cpp:1317-1441, and the framing of Encoder::run, :1571-1600).  The payloads are byte for byte those
  * of av1g_encode() on the same records.  Records of the search's toolset: lossy, 4:2:0 or 4:4:4, 8- or 10-bit, tx_depth
- * 0, no delta-q / CDEF / palette / filter intra / reduced tx set (IS_ERR_INVALID otherwise); header-only fields (tiling,
- * delta_q_* of the planes, quantizer matrices, loop-filter levels, colour description) are free. */
+ * 0, no delta-q / palette / filter intra / reduced tx set (IS_ERR_INVALID otherwise), with or without CDEF (each SB's
+ * cdef_idx is coded with its first non-skip block); header-only fields (tiling, delta_q_* of the planes, quantizer
+ * matrices, loop-filter levels, colour description) are free. */
 typedef struct is_ent_frame {
     av1g_frame_params fp;        /* host copy of the frame parameters */
     const av1g_block *blocks;    /* device: n_blocks blocks in decode order */
@@ -232,8 +233,10 @@ int is_encode_obu(is_handle *h, int first, int n, uint8_t *out, uint64_t cap, ui
  * counterpart (av1core/src/gpu_postfilter.cu).  fp: the frame's parameters with the filter fields set (effective
  * loop_filter_level[4], loop_filter_sharpness, enable_cdef, cdef_damping_minus_3, cdef_bits and the strengths); its size and
  * format must be the image's.  sb_cdef: the cdef_idx of every 64x64 (raster, (MiCols + 15) / 16 per row; NULL = 0), written
- * into the record's blocks so that av1g_encode() of the record with fp reconstructs the filtered planes.  device_ms (may be
- * NULL): device time of the filters.  Not undone by anything but a new encode. */
+ * into the record's blocks so that av1g_encode() of the record with fp reconstructs the filtered planes; from then on the
+ * frame parameters is_batch_copy / is_record_copy return and the frame header is_encode_obu writes carry the filters (so
+ * the decoded stream is the filtered picture).  device_ms (may be NULL): device time of the filters.  Not undone by
+ * anything but a new encode. */
 int is_postfilter(is_handle *h, int i, const av1g_frame_params *fp, const int8_t *sb_cdef, float *device_ms);
 
 /* ---- kernel-level entry points for the parity tests (device primitives of av1core's dsp.h API) ---- */

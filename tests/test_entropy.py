@@ -71,6 +71,29 @@ def test_obu_framing_header_fields(case):
     assert obu_assemble(fp, pay, off) == want
 
 
+@pytest.mark.parametrize("bd,c444,bits,seed", [(8, False, 2, 1), (10, True, 3, 2), (8, False, 0, 3)])
+def test_obu_framing_with_post_filters(bd, c444, bits, seed):
+    """A record with deblocking levels and CDEF (presets, damping, cdef_bits, a cdef_idx per 64x64): the framing around
+    av1g_encode()'s payloads (which carry the cdef_idx literals) equals its stream, cdef_params of the frame header
+    included."""
+    rng = np.random.default_rng(seed)
+    w, h, q = 200, 136, 90
+    im = synth.make_image(w, h, 40 + seed, edges=True, bit_depth=bd, chroma_444=c444)
+    r = O.encode(im, q, bit_depth=bd, chroma_444=c444, threads=4)
+    fp = frame_params(w, h, q, bd, c444)
+    fp[FP_LF:FP_LF + 4] = rng.integers(1, 64, 4)
+    fp[36], fp[37], fp[38] = 1, rng.integers(0, 4), bits          # enable_cdef, cdef_damping_minus_3, cdef_bits
+    fp[39:47], fp[55:63] = rng.integers(0, 16, 8), rng.integers(0, 16, 8)
+    fp[47:55], fp[63:71] = rng.choice([0, 1, 2, 4], 8), rng.choice([0, 1, 2, 4], 8)
+    sbc, sbr = (2 * ((w + 7) // 8) + 15) // 16, (2 * ((h + 7) // 8) + 15) // 16
+    sb = rng.integers(0, 1 << bits, sbr * sbc)
+    blocks = r.blocks.copy()
+    blocks["cdef_idx"] = sb[(blocks["mi_row"].astype(np.int64) >> 4) * sbc + (blocks["mi_col"].astype(np.int64) >> 4)]
+    want, tiles = O.av1g_obu_fp(fp, blocks, r.block_txb, r.txb, r.coeffs)
+    pay, off = _payloads(want, tiles)
+    assert obu_assemble(fp, pay, off) == want
+
+
 def test_obu_assemble_refusals():
     """Frames outside the coder's toolset, a tile count that does not match the tiling, and a short buffer."""
     L = load_library()

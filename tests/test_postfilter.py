@@ -25,6 +25,8 @@ def filter_params(w, h, q, bd, c444, rng, cdef=True):
     lv = rng.integers(0, 64, 4)
     if rng.random() < 0.2:
         lv[1] = 0                                  # luma horizontal edges off
+    if not lv[0] and not lv[1]:
+        lv[0] = 1                                  # chroma levels need a luma level
     fp[FP_LF:FP_LF + 4] = lv
     fp[FP_SHARP] = rng.integers(0, 8)
     if cdef:
@@ -116,3 +118,20 @@ def test_device_postfilter_matches_av1core(enc, w, h, q, bd, c444, seed):
     for p in range(3):
         assert np.array_equal(got.recon[p], want[p]), (p, int(np.sum(got.recon[p] != want[p])))
     assert any(not np.array_equal(got.recon[p], r.recon[p]) for p in range(3))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("w,h,q,bd,c444,seed", [(256, 160, 110, 8, False, 21), (144, 112, 70, 10, True, 22)])
+def test_device_postfilter_then_bitstream(enc, w, h, q, bd, c444, seed):
+    """Search, post-filters, then the device entropy coder: the OBU stream signals the filters (frame header levels and
+    cdef_params, each SB's cdef_idx literal) and equals av1g_encode()'s stream of the record with the same parameters."""
+    rng = np.random.default_rng(seed)
+    im = synth.make_image(w, h, seed, edges=True, bit_depth=bd, chroma_444=c444)
+    enc.encode(im, q)
+    fp = filter_params(w, h, q, bd, c444, rng)
+    sb, sbc = sb_cdef_map(w, h, fp, rng)
+    enc.postfilter(fp, sb)
+    got = enc.fetch(w, h, q, bit_depth=bd, chroma_444=c444)
+    want, _ = O.av1g_obu_fp(fp, got.blocks, got.block_txb, got.txb, got.coeffs)
+    assert enc.obu()[0] == want
+
