@@ -1251,6 +1251,20 @@ int is_postfilter(is_handle *h, int i, const av1g_frame_params *fp, const int8_t
     return IS_OK;
 }
 
+int is_postfilter_from_q(int qindex, int bit_depth, av1g_frame_params *fp) {
+    if (!fp || qindex < 1 || qindex > 255 || (bit_depth != 8 && bit_depth != 10)) return IS_ERR_INVALID;
+    // libaom av1_pick_filter_level, LPF_PICK_FROM_Q, key frame: a linear fit of the level to the ac quantizer step
+    const int64_t ac = AV1G_T(Ac_Qlookup)[(bit_depth - 8) >> 1][qindex];
+    int g = bit_depth == 8 ? (int)((ac * 17563 - 421574 + (1 << 17)) >> 18) : (int)((ac * 20723 + 4060632 + (1 << 19)) >> 20) - 4;
+    g = std::min(std::max(g, 0), 63);
+    // the effective level of an intra block: + the intra reference delta (1) scaled by 1 << (level >> 5)
+    const int lvl = g ? std::min(g + (1 << (g >> 5)), 63) : 0;
+    for (int i = 0; i < 4; i++) fp->loop_filter_level[i] = (uint8_t)lvl;
+    fp->loop_filter_sharpness = (uint8_t)(qindex <= 120 ? 7 : qindex <= 160 ? 1 : 0);
+    fp->cdef_damping_minus_3 = (uint8_t)(qindex >> 6);
+    return IS_OK;
+}
+
 int is_times_get(const is_handle *h, is_times *t) {
     if (!h || !t) return IS_ERR_INVALID;
     *t = h->times;

@@ -65,7 +65,7 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_set_shortlist_model",
            "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison", "is_set_search_options", "is_set_closed_loop_warps", "is_serve_open", "is_serve_start", "is_serve_submit", "is_serve_poll",
            "is_serve_counts", "is_serve_copy", "is_serve_stop", "is_serve_close", "is_entropy_scratch_bytes", "is_entropy_batch",
-           "is_obu_assemble", "is_encode_obu", "is_postfilter"]
+           "is_obu_assemble", "is_encode_obu", "is_postfilter", "is_postfilter_from_q"]
 
 _lib = None
 
@@ -138,6 +138,7 @@ def load_library():
     L.is_obu_assemble.argtypes = [vp, vp, vp, C.c_uint32, vp, C.c_uint64, C.POINTER(C.c_uint64)]
     L.is_encode_obu.argtypes = [vp, C.c_int, C.c_int, vp, C.c_uint64, vp, C.POINTER(C.c_float)]
     L.is_postfilter.argtypes = [vp, C.c_int, vp, vp, C.POINTER(C.c_float)]
+    L.is_postfilter_from_q.argtypes = [C.c_int, C.c_int, vp]
     _lib = L
     return L
 
@@ -159,6 +160,15 @@ def frame_params(width, height, qindex, bit_depth=8, chroma_444=False):
     fp[FP_QM:FP_QM + 3] = 15                        # qm_y, qm_u, qm_v
     fp[FP_CHROMA_FORMAT] = 1 if chroma_444 else 0
     fp[FP_BIT_DEPTH] = bit_depth
+    return fp
+
+
+def postfilter_from_q(fp, qindex, bit_depth=8):
+    """fp (av1g_frame_params bytes) with the reference's default deblocking levels, sharpness and CDEF damping."""
+    fp = np.ascontiguousarray(fp, np.uint8).copy()
+    rc = load_library().is_postfilter_from_q(qindex, bit_depth, fp.ctypes.data)
+    if rc != 0:
+        raise IsError(rc, "is_postfilter_from_q failed (%d)" % rc)
     return fp
 
 

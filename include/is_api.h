@@ -238,6 +238,12 @@ int is_encode_obu(is_handle *h, int first, int n, uint8_t *out, uint64_t cap, ui
  * the decoded stream is the filtered picture).  device_ms (may be NULL): device time of the filters.  Not undone by
  * anything but a new encode. */
 int is_postfilter(is_handle *h, int i, const av1g_frame_params *fp, const int8_t *sb_cdef, float *device_ms);
+/* The reference's default deblocking decision for a base qindex (av1f LF_FROM_Q, av1f/include/av1f/lfsearch_gpu.h:19,
+ * av1f/include/av1f/tuneiq.h:152-199: libaom's av1_pick_filter_level LPF_PICK_FROM_Q for a key frame plus the intra
+ * delta, the tune=iq sharpness rule) into fp's loop_filter_level[4] and loop_filter_sharpness, and its CDEF damping
+ * (cdef_damping_minus_3); enable_cdef and the presets are left as they are (the reference's CDEF preset search has no
+ * counterpart here).  No GPU needed. */
+int is_postfilter_from_q(int qindex, int bit_depth, av1g_frame_params *fp);
 
 /* ---- kernel-level entry points for the parity tests (device primitives of av1core's dsp.h API) ---- */
 /* Forward 2-D transform (this project's integer transform) + quantisation + rate of n residual blocks of one tx

@@ -50,6 +50,7 @@ def lib():
         L.orc_av1g_obu_fp.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p,
                                       C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p,
                                       C.c_uint32, C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]
+        L.orc_ref_lf_from_q.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_av1g_encode_fp.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                          C.c_uint64, C.c_void_p, C.c_void_p * 3, C.c_char_p, C.c_size_t]
         L.orc_av1g_postfilter.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p * 3, C.c_int * 3]
@@ -235,6 +236,13 @@ def av1g_encode_fp(fp, blocks, block_txb, txb, coeffs, prefilter=False):
     if rc != 0:
         raise RuntimeError("av1g_encode rejected the record (%d): %s" % (rc, err.value.decode(errors="replace")))
     return outs
+
+
+def ref_lf_from_q(base, bit_depth=8):
+    """The reference's default deblocking level (effective, with the intra delta), sharpness and CDEF damping."""
+    a, b, c = C.c_int(), C.c_int(), C.c_int()
+    lib().orc_ref_lf_from_q(base, bit_depth, C.byref(a), C.byref(b), C.byref(c))
+    return a.value, b.value, c.value
 
 
 def av1g_postfilter(fp, blocks, planes):

@@ -4,6 +4,7 @@
 // TX_MODE_LARGEST, at most 4 decide threads), so only its speed is reported, never its decisions.
 #include "oracle.h"
 #include "tools.h"
+#include "av1f/tuneiq.h"
 
 #include <cstring>
 #include <string>
@@ -34,3 +35,14 @@ extern "C" int orc_ref_engine(const orc_image *img, double *sec_decide, double *
     if (sec_encode) *sec_encode = st.seconds_encode;
     return rc;
 }
+
+// The reference's frame-level post-filter decisions of its default (av1f/include/av1f/tuneiq.h av1f_tuneiq_frame_init:
+// deblocking level from Q with the intra delta, sharpness, CDEF damping), the pin of the library's is_postfilter_from_q.
+extern "C" void orc_ref_lf_from_q(int base, int bd, int *level, int *sharpness, int *damping) {
+    av1f_tuneiq_frame t;
+    av1f_tuneiq_frame_init(base, 1, 1, 0, &t, bd);
+    *level = t.lf_level;
+    *sharpness = t.lf_sharpness;
+    *damping = t.cdef_damping;
+}
+

@@ -99,6 +99,17 @@ def test_postfilter_arithmetic_matches_av1core(w, h, q, bd, c444, seed):
         assert any(not np.array_equal(want[p], pre[p]) for p in range(3))   # the filters did change the picture
 
 
+def test_postfilter_from_q_matches_reference():
+    """is_postfilter_from_q (the reference's default deblocking: level from Q with the intra delta, sharpness, CDEF
+    damping) equals the reference's own av1f_tuneiq_frame_init for every qindex at 8 and 10 bits."""
+    from av1gpu_b200.isearch import postfilter_from_q
+    for bd in (8, 10):
+        for q in range(1, 256):
+            fp = postfilter_from_q(frame_params(64, 64, q, bd), q, bd)
+            lvl, sharp, damp = O.ref_lf_from_q(q, bd)
+            assert list(fp[FP_LF:FP_LF + 4]) == [lvl] * 4 and fp[FP_SHARP] == sharp and fp[FP_DAMP] + 3 == damp, (bd, q)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("w,h,q,bd,c444,seed", [(320, 240, 120, 8, False, 11), (211, 149, 60, 8, False, 12), (192, 128, 100, 10, False, 13),
                                                 (160, 96, 80, 8, True, 14), (128, 96, 150, 10, True, 15)])
