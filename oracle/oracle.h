@@ -102,6 +102,9 @@ int orc_av1g_encode_fp(const av1g_frame_params *fp, uint32_t flags, uint32_t n_b
 /* av1core's post-filters in place on planes of at least the coded area (strides in samples). */
 int orc_av1g_postfilter(const av1g_frame_params *fp, uint32_t n_blocks, av1g_block *blocks, void *planes[3], const int stride[3]);
 
+/* Experiment switch (0 = the plain form): the chroma screening on source edges (the reference's open-loop chroma
+ * shortlist), its operations counted as open-loop work.  Process-wide; set it before orc_encode. */
+void orc_set_uv_open_loop(int on);
 /* The reference's default frame-level post-filter decisions for a base qindex (ref_shim.cpp). */
 void orc_ref_lf_from_q(int base, int bd, int *level, int *sharpness, int *damping);
 

@@ -50,6 +50,7 @@ def lib():
         L.orc_av1g_obu_fp.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p,
                                       C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p,
                                       C.c_uint32, C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]
+        L.orc_set_uv_open_loop.argtypes = [C.c_int]
         L.orc_ref_lf_from_q.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_av1g_encode_fp.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                          C.c_uint64, C.c_void_p, C.c_void_p * 3, C.c_char_p, C.c_size_t]
@@ -236,6 +237,11 @@ def av1g_encode_fp(fp, blocks, block_txb, txb, coeffs, prefilter=False):
     if rc != 0:
         raise RuntimeError("av1g_encode rejected the record (%d): %s" % (rc, err.value.decode(errors="replace")))
     return outs
+
+
+def set_uv_open_loop(on):
+    """Experiment switch of the oracle: chroma screening on source edges (the reference's open-loop chroma shortlist)."""
+    lib().orc_set_uv_open_loop(1 if on else 0)
 
 
 def ref_lf_from_q(base, bit_depth=8):

@@ -50,6 +50,10 @@ static const int NCDF = (int)(sizeof(av1g_cdfs) / 2);
 
 // plain-form knobs (pipeline.cpp:41-76)
 static const int K_TOP = 4, K_RECHECK = 2, UV_K = 2;
+// experiment switch (orc_set_uv_open_loop; the plain form is 0): the chroma screening reads its edges from the SOURCE
+// with the closed loop's availability, as the reference's open-loop chroma shortlist (k_leafprep.cu:1-30) does, so it
+// could run before the closed loop; its operations are then counted as open-loop work
+static int g_uvOpenLoop = 0;
 static const int UV_OVERHEAD = 384;     // uvOverheadBits 1.5, in 1/256 bit
 
 static inline i64 sat_add(i64 a, i64 b) { return (a >= INF || b >= INF) ? INF : std::min(a + b, INF); }
@@ -1071,6 +1075,11 @@ struct Engine {
         const int maxX = ((MiCols * 4) >> (plane ? ssx : 0)) - 1, maxY = ((MiRows * 4) >> (plane ? ssy : 0)) - 1;
         av1g_build_edges<BD>(rec[plane].data(), pw[plane], px, py, lw, lh, haveL, haveA, haveAR, haveBL, maxX, maxY, A, L);
     }
+    // the same from the source planes (the open-loop chroma screening of the experiment switch)
+    void src_edges(int plane, int px, int py, int lw, int lh, int haveL, int haveA, int haveAR, int haveBL, Px *A, Px *L) const {
+        const int maxX = ((MiCols * 4) >> (plane ? ssx : 0)) - 1, maxY = ((MiRows * 4) >> (plane ? ssy : 0)) - 1;
+        av1g_build_edges<BD>(src[plane].data(), pw[plane], px, py, lw, lh, haveL, haveA, haveAR, haveBL, maxX, maxY, A, L);
+    }
 
     // ---- luma of one block (k_recon.cuh:822-1214, tx_depth 0) ----
     void luma(SbState &S, std::vector<TxbOut> &txbs, int bsize, int x, int y, int availU, int availL, const TileBox &tb, int *outMode,
@@ -1166,14 +1175,19 @@ struct Engine {
         const int cx = (mi_col >> ssx) * 4, cy = (mi_row >> ssy) * 4;
         const int x4 = cx >> 2, y4 = cy >> 2;
         const int sbr4 = (mi_row & 15) >> ssy, sbc4 = (mi_col & 15) >> ssx;
-        Px ea[3][AV1G_EDGE_LEN], el[3][AV1G_EDGE_LEN];
-        Px *A[3], *L[3];
+        Px ea[3][AV1G_EDGE_LEN], el[3][AV1G_EDGE_LEN], oa[3][AV1G_EDGE_LEN], ol[3][AV1G_EDGE_LEN];
+        Px *A[3], *L[3], *OA[3], *OL[3];   // OA / OL: the screening's edges (the source's with the experiment switch)
         int dcv[3];
         for (int pl = 1; pl <= 2; pl++) {
             A[pl] = ea[pl] + AV1G_EDGE_OFF; L[pl] = el[pl] + AV1G_EDGE_OFF;
             const int haveAR = bd_at(S, pl, sbr4 - 1, sbc4 + (Wt >> 2)), haveBL = bd_at(S, pl, sbr4 + (Ht >> 2), sbc4 - 1);
             rec_edges(pl, cx, cy, lw, lh, availLC, availUC, haveAR, haveBL, A[pl], L[pl]);
             dcv[pl] = av1g_dc_value<BD>(A[pl], L[pl], availLC, availUC, lw, lh);
+            OA[pl] = A[pl]; OL[pl] = L[pl];
+            if (g_uvOpenLoop) {
+                OA[pl] = oa[pl] + AV1G_EDGE_OFF; OL[pl] = ol[pl] + AV1G_EDGE_OFF;
+                src_edges(pl, cx, cy, lw, lh, availLC, availUC, haveAR, haveBL, OA[pl], OL[pl]);
+            }
         }
         const Px *sU = src[1].data() + (size_t)cy * pw[1] + cx, *sV = src[2].data() + (size_t)cy * pw[2] + cx;
         const Px *sP[3] = {nullptr, sU, sV};
@@ -1260,7 +1274,7 @@ struct Engine {
             for (int ci = c0; ci < c1; ci++) {
                 i64 t = 0;
                 for (int pl = 1; pl <= 2; pl++) {
-                    av1g_predict_intra<BD>(cand_mode(uvc[ci]), cand_delta(uvc[ci]), availLC, availUC, lw, lh, A[pl], L[pl], pred.data(), Wt);
+                    av1g_predict_intra<BD>(cand_mode(uvc[ci]), cand_delta(uvc[ci]), availLC, availUC, lw, lh, OA[pl], OL[pl], pred.data(), Wt);
                     for (int sy = 0; sy < Ht; sy += 4)
                         for (int sx = 0; sx < Wt; sx += 4) {
                             int d[16];
@@ -1271,7 +1285,7 @@ struct Engine {
                         }
                 }
                 satd[ci] = t << 14;
-                count(1, 2 * (uint64_t)(npx / 16) * (16 * (uint64_t)pred_ops(cand_mode(uvc[ci]), cand_delta(uvc[ci])) + 111) + 30);
+                count(g_uvOpenLoop ? 0 : 1, 2 * (uint64_t)(npx / 16) * (16 * (uint64_t)pred_ops(cand_mode(uvc[ci]), cand_delta(uvc[ci])) + 111) + 30);
             }
         };
         screen(0, 13);
@@ -1772,6 +1786,8 @@ extern "C" int orc_av1g_postfilter(const av1g_frame_params *fp, uint32_t n_block
     if (fp->bit_depth == 10) return av1g_postfilter16(&rec, (uint16_t *const *)planes, stride);
     return av1g_postfilter(&rec, (uint8_t *const *)planes, stride);
 }
+
+extern "C" void orc_set_uv_open_loop(int on) { orc::g_uvOpenLoop = on ? 1 : 0; }
 
 extern "C" void orc_qstep(int qindex, int bd, int *dcq, int *acq) {
     *dcq = av1g_dc_q_bd(qindex, bd);
