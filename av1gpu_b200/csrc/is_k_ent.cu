@@ -35,7 +35,7 @@ static __constant__ uint8_t c_miWLog2[22], c_miHLog2[22];
 static __device__ uint16_t g_cdfInit[4][NCDF];   // av1g_cdfs of each coefficient q-context at the start of a tile
 
 constexpr uint32_t NONE32 = 0xFFFFFFFFu;
-constexpr int HEAD_WORDS = 16;   // partition symbols (at most 4: 64, 32, 16, 8) + mode info (at most 11) of a block
+constexpr int HEAD_WORDS = 16;   // partition symbols (at most 4: 64, 32, 16, 8) + mode info (at most 10) of a block
 enum { SYM_ADAPT = 0, SYM_BIT = 1, SYM_SPLIT_H = 2, SYM_SPLIT_V = 3 };
 
 __device__ __forceinline__ uint32_t sym_word(int kind, int cdf, int s, int N) {
