@@ -99,6 +99,30 @@ def test_postfilter_arithmetic_matches_av1core(w, h, q, bd, c444, seed):
         assert any(not np.array_equal(want[p], pre[p]) for p in range(3))   # the filters did change the picture
 
 
+def test_postfilter_arithmetic_bench_picture():
+    """The 12 MP bench picture (4000x3000, qindex 120, the oracle's record): deblocking with the reference's default
+    levels (level from Q) and CDEF with seeded presets, the host build of the library's functions against av1g_postfilter
+    over the whole coded area."""
+    from av1gpu_b200.isearch import postfilter_from_q
+    L = harness()
+    rng = np.random.default_rng(77)
+    w, h, q = 4000, 3000, 120
+    im = synth.make_image(w, h, 12, edges=True)
+    r = O.encode(im, q)
+    fp = filter_params(w, h, q, 8, False, rng)
+    fp = postfilter_from_q(fp, q, 8)
+    sb, sbc = sb_cdef_map(w, h, fp, rng)
+    blocks = with_cdef_idx(r.blocks, sb, sbc)
+    pre = O.av1g_encode_fp(fp, blocks, r.block_txb, r.txb, r.coeffs, prefilter=True)
+    want = [p.copy() for p in pre]
+    O.av1g_postfilter(fp, blocks, want)
+    got = [p.copy() for p in pre]
+    L.pfh_apply(fp.ctypes.data, blocks.ctypes.data, len(blocks), (C.c_void_p * 3)(*[p.ctypes.data for p in got]),
+                (C.c_int * 3)(*[p.strides[0] // p.itemsize for p in got]))
+    for p in range(3):
+        assert np.array_equal(got[p], want[p]), (p, int(np.sum(got[p] != want[p])))
+
+
 def test_postfilter_from_q_matches_reference():
     """is_postfilter_from_q (the reference's default deblocking: level from Q with the intra delta, sharpness, CDEF
     damping) equals the reference's own av1f_tuneiq_frame_init for every qindex at 8 and 10 bits."""
