@@ -1251,6 +1251,17 @@ int is_postfilter(is_handle *h, int i, const av1g_frame_params *fp, const int8_t
     return IS_OK;
 }
 
+int is_avif_mux(const av1g_frame_params *fp, const uint8_t *obu, uint64_t obu_size, uint8_t *out, uint64_t cap, uint64_t *size) {
+    if (!fp || !obu || !obu_size || !size) return IS_ERR_INVALID;
+    std::vector<uint8_t> o;
+    const int rc = avif_write(*fp, obu, (size_t)obu_size, o, nullptr);
+    if (rc != IS_OK) return rc;
+    *size = o.size();
+    if (!out || cap < o.size()) return IS_ERR_TOO_LARGE;
+    memcpy(out, o.data(), o.size());
+    return IS_OK;
+}
+
 int is_postfilter_from_q(int qindex, int bit_depth, av1g_frame_params *fp) {
     if (!fp || qindex < 1 || qindex > 255 || (bit_depth != 8 && bit_depth != 10)) return IS_ERR_INVALID;
     // libaom av1_pick_filter_level, LPF_PICK_FROM_Q, key frame: a linear fit of the level to the ac quantizer step

@@ -1232,4 +1232,88 @@ int obu_assemble(const av1g_frame_params &fp, const uint8_t *payload, const uint
     return IS_OK;
 }
 
+// ---- AVIF container (host): the still-image HEIF layout libavif writes (ftyp / meta: hdlr, pitm, iinf, iloc, iprp
+// with ispe, av1C, pixi, colr nclx / mdat), the av1C, pixi and colr values from the frame parameters the sequence header
+// was written from; av1core's av1g_mux_avif (av1core/src/avif.cpp) writes the same bytes ----
+namespace {
+struct Box {
+    std::vector<uint8_t> b;
+    void u8(uint32_t v) { b.push_back((uint8_t)v); }
+    void u16(uint32_t v) { u8(v >> 8); u8(v); }
+    void u32(uint32_t v) { u16(v >> 16); u16(v & 0xFFFF); }
+    void tag(const char *t) { for (int i = 0; i < 4; i++) u8((uint8_t)t[i]); }
+    void add(const std::vector<uint8_t> &x) { b.insert(b.end(), x.begin(), x.end()); }
+};
+// a box of type t around payload p; full boxes carry version and flags first
+std::vector<uint8_t> boxed(const char *t, const std::vector<uint8_t> &p, int version = -1, uint32_t flags = 0) {
+    Box o;
+    o.u32((uint32_t)(8 + (version >= 0 ? 4 : 0) + p.size()));
+    o.tag(t);
+    if (version >= 0) o.u32(((uint32_t)version << 24) | (flags & 0xFFFFFF));
+    o.add(p);
+    return o.b;
+}
+}  // namespace
+
+int avif_write(const av1g_frame_params &fp, const uint8_t *obu, size_t n, std::vector<uint8_t> &out, std::string *err) {
+    if (!frame_ok(fp, err)) return IS_ERR_INVALID;
+    TileGeom t;
+    if (!tile_info((int)fp.width, (int)fp.height, fp.tile_cols_log2, fp.tile_rows_log2, t)) {
+        if (err) *err = "tiling not allowed";
+        return IS_ERR_INVALID;
+    }
+    const bool c444 = fp.chroma_format == AV1G_CHROMA_444, hbd = fp.bit_depth == 10;
+    const int cp = fp.color_description ? fp.color_primaries : 1, tc = fp.color_description ? fp.transfer_characteristics : 13,
+              mc = fp.color_description ? fp.matrix_coefficients : 6;
+    // properties of the item: ispe (size), av1C (the sequence header's configuration), pixi (3 channels), colr (CICP,
+    // full range: the sequence header always codes or implies color_range 1)
+    Box ispe, av1c, pixi, colr;
+    ispe.u32(fp.width); ispe.u32(fp.height);
+    av1c.u8(0x81);                                                        // marker, version 1
+    av1c.u8(((c444 ? 1u : 0u) << 5) | (uint32_t)seq_level(fp.width, fp.height, t.cols * t.rows, t.cols));
+    av1c.u8(((hbd ? 1u : 0u) << 6) | ((c444 ? 0u : 1u) << 3) | ((c444 ? 0u : 1u) << 2));   // tier 0, mono 0, CSP unknown
+    av1c.u8(0);                                                           // no initial presentation delay
+    pixi.u8(3);
+    for (int k = 0; k < 3; k++) pixi.u8(hbd ? 10 : 8);
+    colr.tag("nclx"); colr.u16(cp); colr.u16(tc); colr.u16(mc); colr.u8(0x80);
+    Box ipco;
+    ipco.add(boxed("ispe", ispe.b, 0));
+    ipco.add(boxed("av1C", av1c.b));
+    ipco.add(boxed("pixi", pixi.b, 0));
+    ipco.add(boxed("colr", colr.b));
+    Box ipma;                                                             // item 1: ispe, av1C essential; pixi, colr
+    ipma.u32(1); ipma.u16(1); ipma.u8(4); ipma.u8(0x81); ipma.u8(0x82); ipma.u8(0x03); ipma.u8(0x04);
+    Box iprp;
+    iprp.add(boxed("ipco", ipco.b));
+    iprp.add(boxed("ipma", ipma.b, 0));
+    Box hdlr, pitm, infe, iinf;
+    hdlr.u32(0); hdlr.tag("pict"); for (int k = 0; k < 12; k++) hdlr.u8(0); hdlr.u8(0);   // no name
+    pitm.u16(1);
+    infe.u16(1); infe.u16(0); infe.tag("av01"); infe.u8(0);
+    iinf.u16(1); iinf.add(boxed("infe", infe.b, 2));
+    auto meta = [&](uint32_t dataAt) {
+        Box iloc, m;
+        iloc.u8(0x44); iloc.u8(0x00);                                     // 4-byte offsets and lengths, no base offset
+        iloc.u16(1); iloc.u16(1); iloc.u16(0); iloc.u16(1); iloc.u32(dataAt); iloc.u32((uint32_t)n);
+        m.add(boxed("hdlr", hdlr.b, 0));
+        m.add(boxed("pitm", pitm.b, 0));
+        m.add(boxed("iinf", iinf.b, 0));
+        m.add(boxed("iloc", iloc.b, 0));
+        m.add(boxed("iprp", iprp.b));
+        return boxed("meta", m.b, 0);
+    };
+    Box ftyp;
+    ftyp.tag("avif"); ftyp.u32(0); ftyp.tag("avif"); ftyp.tag("mif1");
+    const std::vector<uint8_t> ft = boxed("ftyp", ftyp.b);
+    const size_t metaBytes = meta(0).size();                              // the offset field does not change the size
+    const uint32_t at = (uint32_t)(ft.size() + metaBytes + 8);
+    Box file;
+    file.add(ft);
+    file.add(meta(at));
+    file.u32((uint32_t)(8 + n)); file.tag("mdat");
+    file.b.insert(file.b.end(), obu, obu + n);
+    out.swap(file.b);
+    return IS_OK;
+}
+
 }  // namespace is

@@ -70,6 +70,7 @@ int ent_launch(const is_ent_frame *frames, int n, uint64_t cap, void *scratch, s
                uint32_t *frameTile0, std::string *err);
 int obu_assemble(const av1g_frame_params &fp, const uint8_t *payload, const uint64_t *off, uint32_t nTiles, std::vector<uint8_t> &o,
                  std::string *err);
+int avif_write(const av1g_frame_params &fp, const uint8_t *obu, size_t n, std::vector<uint8_t> &out, std::string *err);
 
 // ---- post-filter unit (is_k_pf.cu): deblocking + CDEF of a reconstruction on the device ----
 size_t pf_scratch_bytes(int W, int H, int bd, int c444);

@@ -65,7 +65,8 @@ EXPORTS = ["is_create", "is_destroy", "is_last_error", "is_encode_device", "is_e
            "is_set_shortlist_model",
            "is_set_wait_limits", "is_set_workspace_limit", "is_set_poison", "is_set_search_options", "is_set_closed_loop_warps", "is_serve_open", "is_serve_start", "is_serve_submit", "is_serve_poll",
            "is_serve_counts", "is_serve_copy", "is_serve_stop", "is_serve_close", "is_entropy_scratch_bytes", "is_entropy_batch",
-           "is_obu_assemble", "is_encode_obu", "is_postfilter", "is_postfilter_from_q"]
+           "is_obu_assemble", "is_encode_obu", "is_postfilter", "is_postfilter_from_q",
+           "is_avif_mux"]
 
 _lib = None
 
@@ -139,6 +140,7 @@ def load_library():
     L.is_encode_obu.argtypes = [vp, C.c_int, C.c_int, vp, C.c_uint64, vp, C.POINTER(C.c_float)]
     L.is_postfilter.argtypes = [vp, C.c_int, vp, vp, C.POINTER(C.c_float)]
     L.is_postfilter_from_q.argtypes = [C.c_int, C.c_int, vp]
+    L.is_avif_mux.argtypes = [vp, vp, C.c_uint64, vp, C.c_uint64, C.POINTER(C.c_uint64)]
     _lib = L
     return L
 
@@ -161,6 +163,22 @@ def frame_params(width, height, qindex, bit_depth=8, chroma_444=False):
     fp[FP_CHROMA_FORMAT] = 1 if chroma_444 else 0
     fp[FP_BIT_DEPTH] = bit_depth
     return fp
+
+
+def avif_mux(fp, obu):
+    """The AVIF file (bytes) around an OBU stream written for fp (av1g_frame_params bytes)."""
+    L = load_library()
+    fp = np.ascontiguousarray(fp, np.uint8)
+    src = np.frombuffer(bytes(obu), np.uint8)
+    size = C.c_uint64()
+    rc = L.is_avif_mux(fp.ctypes.data, src.ctypes.data, len(src), None, 0, C.byref(size))
+    if rc not in (0, IS_ERR_TOO_LARGE):
+        raise IsError(rc, "is_avif_mux failed (%d)" % rc)
+    out = np.zeros(size.value, np.uint8)
+    rc = L.is_avif_mux(fp.ctypes.data, src.ctypes.data, len(src), out.ctypes.data, size.value, C.byref(size))
+    if rc != 0:
+        raise IsError(rc, "is_avif_mux failed (%d)" % rc)
+    return out.tobytes()
 
 
 def postfilter_from_q(fp, qindex, bit_depth=8):
@@ -394,6 +412,17 @@ class Encoder:
         self._check(rc, "is_encode_obu")
         out = [buf[int(offs[k]):int(offs[k + 1])].tobytes() for k in range(n)]
         return (out, ms.value) if timed else out
+
+    def frame_params(self, i=0):
+        """The av1g_frame_params bytes of image i of the last encode (with the post-filters once applied)."""
+        fp = np.zeros(FRAME_PARAMS_BYTES, np.uint8)
+        self._check(self.L.is_batch_copy(self.h, i, fp.ctypes.data, None, None, None, None, (C.c_void_p * 3)(), None), "is_batch_copy")
+        return fp
+
+    def avif(self, first=0, n=1):
+        """Images first .. first + n - 1 of the last encode as AVIF files (bytes): device entropy coding in one batch,
+        then the container on the host."""
+        return [avif_mux(self.frame_params(first + k), s) for k, s in enumerate(self.obu(first, n))]
 
     def postfilter(self, fp, sb_cdef=None, i=0):
         """Deblocking + CDEF in place on image i's reconstruction (fp: av1g_frame_params bytes with the filter fields,

@@ -219,6 +219,11 @@ int is_entropy_batch(int device, const is_ent_frame *frames, int n, uint64_t sym
  * IS_ERR_TOO_LARGE when cap is smaller (nothing written). */
 int is_obu_assemble(const av1g_frame_params *fp, const uint8_t *payload, const uint64_t *tile_offset, uint32_t n_tiles, uint8_t *out,
                     uint64_t cap, uint64_t *size);
+/* The AVIF file (still image, the layout libavif writes: ftyp, meta with hdlr / pitm / iinf / iloc / iprp (ispe, av1C,
+ * pixi, colr nclx), mdat) around an OBU stream written for fp (is_obu_assemble / is_encode_obu): av1core's av1g_mux_avif
+ * (av1core/include/av1g/av1g.h:128-131, av1core/src/avif.cpp) writes the same bytes.  Host only; IS_ERR_TOO_LARGE when
+ * cap is smaller (*size = the bytes needed). */
+int is_avif_mux(const av1g_frame_params *fp, const uint8_t *obu, uint64_t obu_size, uint8_t *out, uint64_t cap, uint64_t *size);
 /* Images first .. first + n - 1 of the handle's last encode (batch order; a single image is image 0) coded on the device
  * in one batch and returned as OBU streams back to back: image k at out[offsets[k] .. offsets[k + 1]).  The handle keeps
  * the scratch; a symbol count above the default capacity reruns once with the exact count.  device_ms (may be NULL):

@@ -102,6 +102,8 @@ int orc_av1g_encode_fp(const av1g_frame_params *fp, uint32_t flags, uint32_t n_b
 /* av1core's post-filters in place on planes of at least the coded area (strides in samples). */
 int orc_av1g_postfilter(const av1g_frame_params *fp, uint32_t n_blocks, av1g_block *blocks, void *planes[3], const int stride[3]);
 
+/* av1core's AVIF muxer (av1g_mux_avif) around an OBU stream; out may be NULL to ask for the size. */
+int orc_mux_avif(const uint8_t *obu, uint64_t n, uint32_t w, uint32_t h, uint8_t *out, uint64_t cap, uint64_t *size);
 /* Experiment switch (0 = the plain form): the chroma screening on source edges (the reference's open-loop chroma
  * shortlist), its operations counted as open-loop work.  Process-wide; set it before orc_encode. */
 void orc_set_uv_open_loop(int on);

@@ -51,6 +51,7 @@ def lib():
                                       C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p,
                                       C.c_uint32, C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]
         L.orc_set_uv_open_loop.argtypes = [C.c_int]
+        L.orc_mux_avif.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]
         L.orc_ref_lf_from_q.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_av1g_encode_fp.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                          C.c_uint64, C.c_void_p, C.c_void_p * 3, C.c_char_p, C.c_size_t]
@@ -237,6 +238,18 @@ def av1g_encode_fp(fp, blocks, block_txb, txb, coeffs, prefilter=False):
     if rc != 0:
         raise RuntimeError("av1g_encode rejected the record (%d): %s" % (rc, err.value.decode(errors="replace")))
     return outs
+
+
+def mux_avif(obu, width, height):
+    """av1core's AVIF file (av1g_mux_avif) around an OBU stream (bytes)."""
+    src = np.frombuffer(obu, np.uint8)
+    size = C.c_uint64()
+    rc = lib().orc_mux_avif(src.ctypes.data, len(src), width, height, None, 0, C.byref(size))
+    if rc != 0:
+        raise RuntimeError("av1g_mux_avif failed (%d)" % rc)
+    out = np.zeros(size.value, np.uint8)
+    lib().orc_mux_avif(src.ctypes.data, len(src), width, height, out.ctypes.data, size.value, C.byref(size))
+    return out.tobytes()
 
 
 def set_uv_open_loop(on):

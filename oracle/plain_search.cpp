@@ -1787,6 +1787,18 @@ extern "C" int orc_av1g_postfilter(const av1g_frame_params *fp, uint32_t n_block
     return av1g_postfilter(&rec, (uint8_t *const *)planes, stride);
 }
 
+// av1core's AVIF muxer around an OBU stream (cap 0: only the size)
+extern "C" int orc_mux_avif(const uint8_t *obu, uint64_t n, uint32_t w, uint32_t h, uint8_t *out, uint64_t cap, uint64_t *size) {
+    uint8_t *a = nullptr;
+    size_t an = 0;
+    const int rc = av1g_mux_avif(obu, (size_t)n, w, h, &a, &an);
+    if (rc != AV1G_OK) return rc;
+    *size = an;
+    if (out && cap >= an) memcpy(out, a, an);
+    free(a);
+    return 0;
+}
+
 extern "C" void orc_set_uv_open_loop(int on) { orc::g_uvOpenLoop = on ? 1 : 0; }
 
 extern "C" void orc_qstep(int qindex, int bd, int *dcq, int *acq) {

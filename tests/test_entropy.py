@@ -94,6 +94,23 @@ def test_obu_framing_with_post_filters(bd, c444, bits, seed):
     assert obu_assemble(fp, pay, off) == want
 
 
+@pytest.mark.parametrize("w,h,bd,c444,cicp,seed", [(96, 64, 8, False, None, 1), (64, 48, 10, True, None, 2), (72, 40, 8, False, (2, 2, 2), 3),
+                                                (64, 64, 8, True, (1, 13, 0), 4), (80, 56, 10, False, (9, 16, 9), 5), (4160, 40, 8, False, None, 6)])
+def test_avif_matches_av1core(w, h, bd, c444, cicp, seed):
+    """The AVIF file around av1g_encode()'s OBU stream equals av1core's av1g_mux_avif (formats, colour descriptions incl.
+    unspecified and identity, a two-tile frame's level)."""
+    from av1gpu_b200.isearch import avif_mux
+    im = synth.make_image(w, h, 60 + seed, edges=True, bit_depth=bd, chroma_444=c444)
+    q = 110
+    r = O.encode(im, q, bit_depth=bd, chroma_444=c444, threads=4)
+    fp = frame_params(w, h, q, bd, c444)
+    if cicp:
+        fp[FP_CD] = 1
+        fp[FP_CP:FP_CP + 3] = cicp
+    obu, _ = O.av1g_obu_fp(fp, r.blocks, r.block_txb, r.txb, r.coeffs)
+    assert avif_mux(fp, obu) == O.mux_avif(obu, w, h)
+
+
 def test_obu_assemble_refusals():
     """Frames outside the coder's toolset, a tile count that does not match the tiling, and a short buffer."""
     L = load_library()
@@ -171,6 +188,9 @@ def test_device_entropy_batch(enc):
         assert got == want
     # a sub-range of the batch
     assert enc.obu(3, 2) == streams[3:5]
+    # the AVIF files of the batch: av1core's container around the same streams
+    for (w, h, q, bd, c), got, f in zip(spec, streams, enc.avif(0, len(spec))):
+        assert f == O.mux_avif(got, w, h)
 
 
 @pytest.mark.gpu
