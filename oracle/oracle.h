@@ -107,6 +107,9 @@ int orc_mux_avif(const uint8_t *obu, uint64_t n, uint32_t w, uint32_t h, uint8_t
 /* Experiment switch (0 = the plain form): the chroma screening on source edges (the reference's open-loop chroma
  * shortlist), its operations counted as open-loop work.  Process-wide; set it before orc_encode. */
 void orc_set_uv_open_loop(int on);
+/* Experiment switch (0 = the plain form): the search with the intra edge filter (its records need
+ * enable_intra_edge_filter = 1).  Process-wide; set it before orc_encode. */
+void orc_set_edge_filter(int on);
 /* The reference's default frame-level post-filter decisions for a base qindex (ref_shim.cpp). */
 void orc_ref_lf_from_q(int base, int bd, int *level, int *sharpness, int *damping);
 

@@ -51,6 +51,7 @@ def lib():
                                       C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p,
                                       C.c_uint32, C.POINTER(C.c_uint64), C.c_char_p, C.c_size_t]
         L.orc_set_uv_open_loop.argtypes = [C.c_int]
+        L.orc_set_edge_filter.argtypes = [C.c_int]
         L.orc_mux_avif.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]
         L.orc_ref_lf_from_q.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_av1g_encode_fp.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
@@ -250,6 +251,11 @@ def mux_avif(obu, width, height):
     out = np.zeros(size.value, np.uint8)
     lib().orc_mux_avif(src.ctypes.data, len(src), width, height, out.ctypes.data, size.value, C.byref(size))
     return out.tobytes()
+
+
+def set_edge_filter(on):
+    """Experiment switch of the oracle: the search with the intra edge filter (records for enable_intra_edge_filter 1)."""
+    lib().orc_set_edge_filter(1 if on else 0)
 
 
 def set_uv_open_loop(on):

@@ -54,6 +54,10 @@ static const int K_TOP = 4, K_RECHECK = 2, UV_K = 2;
 // with the closed loop's availability, as the reference's open-loop chroma shortlist (k_leafprep.cu:1-30) does, so it
 // could run before the closed loop; its operations are then counted as open-loop work
 static int g_uvOpenLoop = 0;
+// experiment switch (orc_set_edge_filter; the plain form is 0): directional predictions with the intra edge filter and
+// upsampling (spec 7.11.2.11-12, enable_intra_edge_filter = 1), filter type 0 in the open-loop analysis (no neighbour
+// modes yet, as the reference's analysis) and from the neighbours' modes in the closed loop
+static int g_edgeFilter = 0;
 static const int UV_OVERHEAD = 384;     // uvOverheadBits 1.5, in 1/256 bit
 
 static inline i64 sat_add(i64 a, i64 b) { return (a >= INF || b >= INF) ? INF : std::min(a + b, INF); }
@@ -628,7 +632,7 @@ struct Engine {
     std::vector<BlockRes> blk[22];
     int shNbx[22], shNby[22];
     std::vector<std::vector<Leaf>> leaves;
-    std::vector<uint8_t> mYMode, cLvl[3], cDc[3];
+    std::vector<uint8_t> mYMode, mUVMode, cLvl[3], cDc[3];
     std::vector<SbOut> sbo;
     OpCounter *ops = nullptr;
 
@@ -674,6 +678,7 @@ struct Engine {
             blk[s].assign((size_t)shNbx[s] * shNby[s], BlockRes{INF, {0, 0, 0, 0}, 0, 0});
         }
         mYMode.assign((size_t)MiCols * MiRows, 0);
+        mUVMode.assign((size_t)MiCols * MiRows, 0);
         for (int p = 0; p < 3; p++) {
             const size_t n = (size_t)(MiCols >> (p ? ssx : 0)) * (MiRows >> (p ? ssy : 0));
             cLvl[p].assign(n, 0);
@@ -725,7 +730,7 @@ struct Engine {
             return b;
         };
         std::vector<Px> pred((size_t)w * h);
-        auto predict = [&](int c) { av1g_predict_intra<BD>(cand_mode(c), cand_delta(c), haveL, haveA, lw, lh, A, L, pred.data(), w); };
+        auto predict = [&](int c) { predictx(0, cand_mode(c), cand_delta(c), haveL, haveA, lw, lh, x, y, 0, A, L, pred.data(), w); };
         // ---- SATD screening: 13 modes at delta 0, then +-1..3 around the two best directional modes ----
         int cands[32];
         i64 js[32];
@@ -1056,7 +1061,10 @@ struct Engine {
             if (hasChroma) chroma(S, txbs, bsize, mi_row, mi_col, yMode, availUC, availLC, tb, &uv, &duv, &aU, &aV, &eobU, &eobV);
             const int skip = (eobY == 0 && eobU == 0 && eobV == 0) ? 1 : 0;
             for (int r = mi_row; r < mi_row + av1g_bh4(bsize) && r < MiRows; r++)
-                for (int c = mi_col; c < mi_col + av1g_bw4(bsize) && c < MiCols; c++) mYMode[(size_t)r * MiCols + c] = (uint8_t)yMode;
+                for (int c = mi_col; c < mi_col + av1g_bw4(bsize) && c < MiCols; c++) {
+                    mYMode[(size_t)r * MiCols + c] = (uint8_t)yMode;
+                    if (hasChroma) mUVMode[(size_t)r * MiCols + c] = (uint8_t)uv;
+                }
             av1g_block b;
             memset(&b, 0, sizeof b);
             b.mi_row = (uint16_t)mi_row; b.mi_col = (uint16_t)mi_col;
@@ -1074,6 +1082,21 @@ struct Engine {
     void rec_edges(int plane, int px, int py, int lw, int lh, int haveL, int haveA, int haveAR, int haveBL, Px *A, Px *L) const {
         const int maxX = ((MiCols * 4) >> (plane ? ssx : 0)) - 1, maxY = ((MiRows * 4) >> (plane ? ssy : 0)) - 1;
         av1g_build_edges<BD>(rec[plane].data(), pw[plane], px, py, lw, lh, haveL, haveA, haveAR, haveBL, maxX, maxY, A, L);
+    }
+    // prediction of a tx block at plane position (px, py): av1core's plain predictor, or with the edge-filter switch its
+    // predictor with the intra edge filter (on copies of the edges, which it filters in place)
+    void predictx(int plane, int mode, int delta, int haveL, int haveA, int lw, int lh, int px, int py, int filterType, const Px *A,
+                  const Px *L, Px *dst, int stride) const {
+        if (!g_edgeFilter) { av1g_predict_intra<BD>(mode, delta, haveL, haveA, lw, lh, A, L, dst, stride); return; }
+        Px ea[AV1G_EDGE_LEN], el[AV1G_EDGE_LEN];
+        memcpy(ea, A - AV1G_EDGE_OFF, sizeof ea);
+        memcpy(el, L - AV1G_EDGE_OFF, sizeof el);
+        const int maxX = ((MiCols * 4) >> (plane ? ssx : 0)) - 1, maxY = ((MiRows * 4) >> (plane ? ssy : 0)) - 1;
+        av1g_predict_intra_ex<BD>(mode, delta, -1, 1, filterType, haveL, haveA, lw, lh, px, py, maxX, maxY, ea + AV1G_EDGE_OFF,
+                                  el + AV1G_EDGE_OFF, dst, stride);
+    }
+    int filter_type(int plane, int mi_row, int mi_col, int availU, int availL) const {
+        return av1g_get_filter_type(plane, mi_row, mi_col, availU, availL, mYMode.data(), mUVMode.data(), MiCols, ssx, ssy);
     }
     // the same from the source planes (the open-loop chroma screening of the experiment switch)
     void src_edges(int plane, int px, int py, int lw, int lh, int haveL, int haveA, int haveAR, int haveBL, Px *A, Px *L) const {
@@ -1108,8 +1131,9 @@ struct Engine {
         const int set = av1g_get_tx_set_intra(txSz, 0);
         std::vector<Px> pred((size_t)Wt * Ht);
         std::vector<int32_t> res((size_t)Wt * Ht);
+        const int fType = g_edgeFilter ? filter_type(0, mi_row, mi_col, availU, availL) : 0;
         auto residual = [&](int c) -> i64 {
-            av1g_predict_intra<BD>(cand_mode(c), cand_delta(c), availL, availU, lw, lh, A, L, pred.data(), Wt);
+            predictx(0, cand_mode(c), cand_delta(c), availL, availU, lw, lh, x, y, fType, A, L, pred.data(), Wt);
             i64 e = 0;
             for (int i = 0; i < Ht; i++)
                 for (int j = 0; j < Wt; j++) {
@@ -1160,7 +1184,7 @@ struct Engine {
         }
         // final: prediction + exact inverse into the reconstruction, record
         Px *dst = rec[0].data() + (size_t)y * pw[0] + x;
-        av1g_predict_intra<BD>(cand_mode(bestC), cand_delta(bestC), availL, availU, lw, lh, A, L, dst, pw[0]);
+        predictx(0, cand_mode(bestC), cand_delta(bestC), availL, availU, lw, lh, x, y, fType, A, L, dst, pw[0]);
         inverse_add(bestQ, txSz, bestT, 0, dst, pw[0]);
         *outEob = record_txb(S, txbs, bestQ, 0, txSz, bestT, x >> 2, y >> 2, sbr4, sbc4);
         *outMode = cand_mode(bestC);
@@ -1189,6 +1213,7 @@ struct Engine {
                 src_edges(pl, cx, cy, lw, lh, availLC, availUC, haveAR, haveBL, OA[pl], OL[pl]);
             }
         }
+        const int fTypeC = g_edgeFilter ? filter_type(1, mi_row, mi_col, availUC, availLC) : 0;
         const Px *sU = src[1].data() + (size_t)cy * pw[1] + cx, *sV = src[2].data() + (size_t)cy * pw[2] + cx;
         const Px *sP[3] = {nullptr, sU, sV};
         const int spP[3] = {0, pw[1], pw[2]};
@@ -1274,7 +1299,7 @@ struct Engine {
             for (int ci = c0; ci < c1; ci++) {
                 i64 t = 0;
                 for (int pl = 1; pl <= 2; pl++) {
-                    av1g_predict_intra<BD>(cand_mode(uvc[ci]), cand_delta(uvc[ci]), availLC, availUC, lw, lh, OA[pl], OL[pl], pred.data(), Wt);
+                    predictx(pl, cand_mode(uvc[ci]), cand_delta(uvc[ci]), availLC, availUC, lw, lh, cx, cy, fTypeC, OA[pl], OL[pl], pred.data(), Wt);
                     for (int sy = 0; sy < Ht; sy += 4)
                         for (int sx = 0; sx < Wt; sx += 4) {
                             int d[16];
@@ -1331,7 +1356,7 @@ struct Engine {
                     }
                 return;
             }
-            av1g_predict_intra<BD>(cand_mode(c), cand_delta(c), availLC, availUC, lw, lh, A[pl], L[pl], pred.data(), Wt);
+            predictx(pl, cand_mode(c), cand_delta(c), availLC, availUC, lw, lh, cx, cy, fTypeC, A[pl], L[pl], pred.data(), Wt);
             for (int i = 0; i < Ht; i++)
                 for (int j = 0; j < Wt; j++) res[(size_t)i * Wt + j] = (int)sP[pl][i * spP[pl] + j] - (int)pred[(size_t)i * Wt + j];
         };
@@ -1384,7 +1409,7 @@ struct Engine {
                     for (int j = 0; j < Wt; j++)
                         dst[(size_t)i * pw[pl] + j] = (Px)av1g_clip1<BD>(dcv[pl] + av1g_round2signed(alpha[pl] * (cflL[i * Wt + j] - cflAvg), 6));
             } else {
-                av1g_predict_intra<BD>(cand_mode(bestC), cand_delta(bestC), availLC, availUC, lw, lh, A[pl], L[pl], dst, pw[pl]);
+                predictx(pl, cand_mode(bestC), cand_delta(bestC), availLC, availUC, lw, lh, cx, cy, fTypeC, A[pl], L[pl], dst, pw[pl]);
             }
             inverse_add(bestQ[pl], txSz, uvTxType, pl, dst, pw[pl]);
             eobs[pl] = record_txb(S, txbs, bestQ[pl], pl, txSz, uvTxType, x4, y4, sbr4, sbc4);
@@ -1402,7 +1427,7 @@ struct Engine {
                     int sc, dc;
                     txb_ctx(pl, txSz, x4 + (ox >> 2), y4 + (oy >> 2), bsize, tb, &sc, &dc);
                     Px *d2 = rec[pl].data() + (size_t)(cy + oy) * pw[pl] + cx + ox;
-                    av1g_predict_intra<BD>(cand_mode(bestC), cand_delta(bestC), haveL, haveA, lw, lh, A2, L2, d2, pw[pl]);
+                    predictx(pl, cand_mode(bestC), cand_delta(bestC), haveL, haveA, lw, lh, cx + ox, cy + oy, fTypeC, A2, L2, d2, pw[pl]);
                     const Px *s2 = sP[pl] + (size_t)oy * spP[pl] + ox;
                     for (int i = 0; i < Ht; i++)
                         for (int j = 0; j < Wt; j++) res[(size_t)i * Wt + j] = (int)s2[(size_t)i * spP[pl] + j] - (int)d2[(size_t)i * pw[pl] + j];
@@ -1800,6 +1825,7 @@ extern "C" int orc_mux_avif(const uint8_t *obu, uint64_t n, uint32_t w, uint32_t
 }
 
 extern "C" void orc_set_uv_open_loop(int on) { orc::g_uvOpenLoop = on ? 1 : 0; }
+extern "C" void orc_set_edge_filter(int on) { orc::g_edgeFilter = on ? 1 : 0; }
 
 extern "C" void orc_qstep(int qindex, int bd, int *dcq, int *acq) {
     *dcq = av1g_dc_q_bd(qindex, bd);
